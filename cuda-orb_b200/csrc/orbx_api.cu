@@ -1,0 +1,840 @@
+// C ABI of the sm_100a ORB library: contexts, constant tables, workspaces,
+// batch descriptors and the per-call launch sequences.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <vector>
+
+#include "orb_pattern31.h"
+#include "orbx_device.cuh"
+#include "orbx_internal.cuh"
+
+using namespace orbx;
+
+namespace {
+
+struct Workspace {
+  int w = 0, h = 0, noct_req = 0, n = 0;
+  int oszp[5 * kMaxOctaves + 1] = {0};
+  size_t obytes = 0;
+  size_t guard = 0;              // zeroed bytes before and after each pyramid
+  uint8_t* pyr_alloc = nullptr;  // guard + obytes + guard
+  uint8_t* blr_alloc = nullptr;
+  float* vmap = nullptr;
+  int* layer = nullptr;
+  unsigned long long* nms_status = nullptr;
+  int* total = nullptr;
+  int nms_strips = 0;
+};
+
+struct BatchSlot {
+  Frame* d_frames = nullptr;
+  int* d_bases = nullptr;  // 3 * (cap + 1)
+  unsigned int* d_ticket = nullptr;
+  uint8_t* h_stage = nullptr;  // pinned staging for the upload
+  int cap = 0;
+  cudaEvent_t uploaded = nullptr;
+  std::vector<uint8_t> last;
+};
+
+struct PairGraph {
+  bool valid = false;
+  std::vector<uint8_t> key;
+  cudaGraphExec_t exec = nullptr;
+  MatchWork mw{};
+};
+
+struct DeviceGuard {
+  int prev = -1;
+  explicit DeviceGuard(int dev) {
+    if (cudaGetDevice(&prev) == cudaSuccess && prev != dev) {
+      cudaSetDevice(dev);
+    } else {
+      prev = -1;
+    }
+  }
+  ~DeviceGuard() {
+    if (prev >= 0) cudaSetDevice(prev);
+  }
+};
+
+}  // namespace
+
+struct orbx_ctx {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  bool inited = false;
+  orbx_params p{};
+  float gauss[4] = {0, 0, 0, 0};
+  float scale4 = 0.f;
+  int half_k = 15;
+  int8_t* d_pattern = nullptr;
+  int* d_umax = nullptr;
+  int* d_err = nullptr;
+  Workspace ws[2];
+  BatchSlot single, pair;
+  MatchWork mw{};  // for orbx_match / orbx_match_knn2
+  PairGraph pg;
+};
+
+#define ORBX_CUDA(x)                   \
+  do {                                 \
+    cudaError_t _e = (x);              \
+    if (_e != cudaSuccess) {           \
+      (void)cudaGetLastError();        \
+      return _e == cudaErrorMemoryAllocation ? ORBX_ERR_NOMEM : ORBX_ERR_CUDA; \
+    }                                  \
+  } while (0)
+
+static inline int align_up(int a, int b) { return (a % b != 0) ? (a - a % b + b) : a; }
+static inline int div_up(int a, int b) { return (a + b - 1) / b; }
+
+// ---------------------------------------------------------------------------
+// Tables (Orbor::init, orb.cpp:32-54)
+// ---------------------------------------------------------------------------
+
+// setUmax (orbd.cu:66-92).
+static void make_umax(int patch_size, int* umax) {
+  const int half = patch_size / 2;
+  umax[half + 1] = 0;
+  const float v = half * sqrtf(2.f) / 2;
+  const int vmax = (int)floorf(v + 1);
+  const int vmin = (int)ceilf(v);
+  for (int i = 0; i <= vmax; i++) umax[i] = (int)roundf(sqrtf((float)(half * half - i * i)));
+  for (int i = half, v0 = 0; i >= vmin; --i) {
+    while (umax[v0] == umax[v0 + 1]) ++v0;
+    umax[i] = v0;
+    ++v0;
+  }
+}
+
+// setPattern (orbd.cu:95-410).  The 31x31 table is fixed; other patch sizes and
+// WTA_K 3/4 draw from the C library's rand() with the reference's seeds, so the
+// sampling points agree with a reference process on the same C library.
+static int make_pattern(int patch_size, int wta_k, int8_t* out /* [512][2] */) {
+  int base[512][2];
+  for (int i = 0; i < 512; i++) {
+    base[i][0] = kOrbPattern31[i][0];
+    base[i][1] = kOrbPattern31[i][1];
+  }
+  if (patch_size != 31) {
+    srand(0x34985739);
+    for (int i = 0; i < 512; i++) {
+      // the reference's offset is "- -patch_size / 2", i.e. + patch_size / 2 (orbd.cu:366-367)
+      base[i][0] = rand() % patch_size + patch_size / 2;
+      base[i][1] = rand() % patch_size + patch_size / 2;
+    }
+  }
+  if (wta_k == 2) {
+    for (int i = 0; i < 512; i++) {
+      out[2 * i] = (int8_t)base[i][0];
+      out[2 * i + 1] = (int8_t)base[i][1];
+    }
+    return 512;
+  }
+  srand(0x12345678);
+  const int ntuples = 128;
+  int sel[512][2];
+  for (int i = 0; i < ntuples; i++) {
+    for (int k = 0; k < wta_k; k++) {
+      for (;;) {
+        const int idx = rand() % 512;
+        int k1 = 0;
+        for (; k1 < k; k1++) {
+          if (base[idx][0] == sel[wta_k * i + k1][0] && base[idx][1] == sel[wta_k * i + k1][1]) break;
+        }
+        if (k1 == k) {
+          sel[wta_k * i + k][0] = base[idx][0];
+          sel[wta_k * i + k][1] = base[idx][1];
+          break;
+        }
+      }
+    }
+  }
+  std::memset(out, 0, 1024);
+  for (int i = 0; i < ntuples * wta_k; i++) {
+    out[2 * i] = (int8_t)sel[i][0];
+    out[2 * i + 1] = (int8_t)sel[i][1];
+  }
+  return ntuples * wta_k;
+}
+
+// setGaussianKernel (orbd.cu:413-433): host expf, sigma 2, normalised.
+static void make_gauss(float* k) {
+  const float sigma = 2.f;
+  const float svar = -1.f / (2.f * sigma * sigma);
+  float kersum = 0.f;
+  for (int i = 0; i <= 3; i++) {
+    k[i] = expf(i * i * svar);
+    kersum = kersum + (k[i] + (i == 0 ? 0 : k[i]));
+  }
+  kersum = 1.f / kersum;
+  for (int i = 0; i <= 3; i++) k[i] *= kersum;
+}
+
+// setScaleSqSq (orbd.cu:436-441).
+static float make_scale4() {
+  const float scale = 1.f / (4 * 7 * 255.f);
+  return scale * scale * scale * scale;
+}
+
+// Orbor::updateParam (orb.cpp:145-191).  Returns the octave count, or a negative status.
+static int compute_layout(int w, int h, int noctaves, int* oszp) {
+  const int m = (w < h ? w : h) / 80;
+  if (m <= 0) return -ORBX_ERR_SIZE;
+  int n = (int)log2f((float)m) + 1;
+  if (noctaves < n) n = noctaves;
+  if (n <= 0 || n > kMaxOctaves) return -ORBX_ERR_SIZE;
+  int* osizes = oszp;
+  int* widths = osizes + n;
+  int* heights = widths + n;
+  int* pitchs = heights + n;
+  int* offsets = pitchs + n;
+  widths[0] = w;
+  heights[0] = h;
+  pitchs[0] = align_up(w, 128);
+  osizes[0] = h * pitchs[0];
+  offsets[0] = 0;
+  offsets[1] = osizes[0];
+  for (int j = 1; j < n; j++) {
+    widths[j] = widths[j - 1] >> 1;
+    heights[j] = heights[j - 1] >> 1;
+    pitchs[j] = align_up(widths[j], 128);
+    osizes[j] = heights[j] * pitchs[j];
+    offsets[j + 1] = offsets[j] + osizes[j];
+  }
+  return n;
+}
+
+// ---------------------------------------------------------------------------
+// Workspaces and batches
+// ---------------------------------------------------------------------------
+// Zeroed bytes kept before octave 0 and after the last octave.  The reference
+// reads past octave edges by design: the Harris window one row above octave 0
+// (orbd.cu:651-669), the detect halo and the sampling patterns several rows
+// beyond the last octave (orbd.cu:1001-1036, 1341-1348; with the rand() pattern
+// of patch sizes other than 31 up to 64 rows).  72 rows of the widest pitch
+// cover every such read.
+static size_t pyramid_guard(int pitch0) {
+  size_t g = (size_t)72 * pitch0 + 4096;
+  if (g < kGuard) g = kGuard;
+  return (g + 255) & ~(size_t)255;
+}
+
+static void ws_free(Workspace& ws) {
+  cudaFree(ws.pyr_alloc);
+  cudaFree(ws.blr_alloc);
+  cudaFree(ws.vmap);
+  cudaFree(ws.layer);
+  cudaFree(ws.nms_status);
+  cudaFree(ws.total);
+  ws = Workspace();
+}
+
+static int ws_ensure(orbx_ctx* c, Workspace& ws, int w, int h, int noct_req = -1) {
+  if (noct_req < 0) noct_req = c->p.noctaves;
+  if (ws.pyr_alloc && ws.w == w && ws.h == h && ws.noct_req == noct_req) return ORBX_OK;
+  ws_free(ws);
+  const int n = compute_layout(w, h, noct_req, ws.oszp);
+  if (n < 0) return -n;
+  ws.n = n;
+  ws.w = w;
+  ws.h = h;
+  ws.noct_req = noct_req;
+  ws.obytes = (size_t)ws.oszp[4 * n + n];
+  ws.guard = pyramid_guard(ws.oszp[3 * n]);
+  const size_t alloc = ws.obytes + 2 * ws.guard;
+  const size_t npx = (size_t)h * ws.oszp[3 * n];
+  const int border = c->p.edge_threshold < 3 ? 3 : c->p.edge_threshold;
+  ws.nms_strips = (h - 2 * border > 0 && w - 2 * border > 0) ? div_up(h - 2 * border, kNmsRows) : 0;
+  ORBX_CUDA(cudaMalloc(&ws.pyr_alloc, alloc));
+  ORBX_CUDA(cudaMalloc(&ws.blr_alloc, alloc));
+  ORBX_CUDA(cudaMalloc(&ws.vmap, npx * sizeof(float)));
+  ORBX_CUDA(cudaMalloc(&ws.layer, npx * sizeof(int)));
+  // look-back words for the smallest border (3), so any border fits
+  const int strips_max = (h - 6 > 0) ? div_up(h - 6, kNmsRows) : 1;
+  ORBX_CUDA(cudaMalloc(&ws.nms_status, sizeof(unsigned long long) * strips_max));
+  ORBX_CUDA(cudaMalloc(&ws.total, sizeof(int)));
+  ORBX_CUDA(cudaMemsetAsync(ws.pyr_alloc, 0, alloc, c->stream));
+  ORBX_CUDA(cudaMemsetAsync(ws.blr_alloc, 0, alloc, c->stream));
+  ORBX_CUDA(cudaMemsetAsync(ws.vmap, 0, npx * sizeof(float), c->stream));
+  ORBX_CUDA(cudaMemsetAsync(ws.layer, 0, npx * sizeof(int), c->stream));
+  return ORBX_OK;
+}
+
+static void fill_frame(const orbx_ctx* c, const Workspace& ws, const uint8_t* img, int pitch_in, orbx_point* pts,
+                       uint8_t* desc, int* count, Frame& F) {
+  std::memset(&F, 0, sizeof(F));
+  const int n = ws.n;
+  F.img = img;
+  F.w = ws.w;
+  F.h = ws.h;
+  F.pitch_in = pitch_in;
+  F.n_oct = n;
+  for (int o = 0; o < n; o++) {
+    F.ow[o] = ws.oszp[n + o];
+    F.oh[o] = ws.oszp[2 * n + o];
+    F.op[o] = ws.oszp[3 * n + o];
+  }
+  for (int o = 0; o <= n; o++) F.ooff[o] = ws.oszp[4 * n + o];
+  F.pyr = ws.pyr_alloc + ws.guard;
+  F.blr = ws.blr_alloc + ws.guard;
+  F.vmap = ws.vmap;
+  F.layer = ws.layer;
+  F.pts = pts;
+  F.desc = desc;
+  F.count = count;
+  F.total = ws.total;
+  F.max_pts = c->p.max_pts;
+  F.border = c->p.edge_threshold < 3 ? 3 : c->p.edge_threshold;
+  int acc = 0;
+  for (int o = 0; o < n; o++) {
+    F.pyr_tiles_x[o] = div_up(F.ow[o], kPyrTW);
+    F.pyr_tiles_y[o] = div_up(F.oh[o], kPyrTH);
+    F.pyr_tile_base[o] = acc;
+    acc += F.pyr_tiles_x[o] * F.pyr_tiles_y[o];
+  }
+  F.pyr_tile_base[n] = acc;
+  F.det_tiles_x = div_up(F.w, kDetTW);
+  F.det_tiles_y = div_up(F.h, kDetTH);
+  F.nms_strips = ws.nms_strips;
+  F.nms_status = ws.nms_status;
+}
+
+struct LaunchPlan {
+  Batch b{};
+  int pyr_tiles = 0, det_tiles = 0, nms_strips = 0, total_max_pts = 0;
+};
+
+static int upload_batch(orbx_ctx* c, BatchSlot& bs, const std::vector<Frame>& frames, LaunchPlan* plan) {
+  const int nf = (int)frames.size();
+  if (nf <= 0 || nf > kMaxFramesPerLaunch) return ORBX_ERR_SIZE;
+  std::vector<int> bases(3 * (nf + 1));
+  int* pb = bases.data();
+  int* db = pb + nf + 1;
+  int* nb = db + nf + 1;
+  pb[0] = db[0] = nb[0] = 0;
+  long long tmp = 0;
+  for (int f = 0; f < nf; f++) {
+    const Frame& F = frames[f];
+    pb[f + 1] = pb[f] + F.pyr_tile_base[F.n_oct];
+    db[f + 1] = db[f] + F.det_tiles_x * F.det_tiles_y;
+    nb[f + 1] = nb[f] + F.nms_strips;
+    tmp += F.max_pts;
+  }
+  const size_t fbytes = sizeof(Frame) * nf;
+  const size_t bbytes = sizeof(int) * bases.size();
+  std::vector<uint8_t> blob(fbytes + bbytes);
+  std::memcpy(blob.data(), frames.data(), fbytes);
+  std::memcpy(blob.data() + fbytes, bases.data(), bbytes);
+  if (nf > bs.cap) {
+    if (bs.uploaded) cudaEventSynchronize(bs.uploaded);
+    cudaFree(bs.d_frames);
+    cudaFree(bs.d_bases);
+    cudaFreeHost(bs.h_stage);
+    bs.d_frames = nullptr;
+    bs.d_bases = nullptr;
+    bs.h_stage = nullptr;
+    bs.last.clear();
+    const int cap = nf < 4 ? 4 : nf;
+    ORBX_CUDA(cudaMalloc(&bs.d_frames, sizeof(Frame) * cap));
+    ORBX_CUDA(cudaMalloc(&bs.d_bases, sizeof(int) * 3 * (cap + 1)));
+    ORBX_CUDA(cudaMallocHost(&bs.h_stage, sizeof(Frame) * cap + sizeof(int) * 3 * (cap + 1)));
+    if (!bs.d_ticket) ORBX_CUDA(cudaMalloc(&bs.d_ticket, sizeof(unsigned int)));
+    if (!bs.uploaded) ORBX_CUDA(cudaEventCreateWithFlags(&bs.uploaded, cudaEventDisableTiming));
+    bs.cap = cap;
+  }
+  if (bs.last != blob) {
+    ORBX_CUDA(cudaEventSynchronize(bs.uploaded));  // the previous upload has left the staging buffer
+    std::memcpy(bs.h_stage, blob.data(), blob.size());
+    ORBX_CUDA(cudaMemcpyAsync(bs.d_frames, bs.h_stage, fbytes, cudaMemcpyHostToDevice, c->stream));
+    ORBX_CUDA(cudaMemcpyAsync(bs.d_bases, bs.h_stage + fbytes, bbytes, cudaMemcpyHostToDevice, c->stream));
+    ORBX_CUDA(cudaEventRecord(bs.uploaded, c->stream));
+    bs.last.swap(blob);
+  }
+  Batch& b = plan->b;
+  b.frames = bs.d_frames;
+  b.n_frames = nf;
+  b.pyr_base = bs.d_bases;
+  b.det_base = bs.d_bases + (nf + 1);
+  b.nms_base = bs.d_bases + 2 * (nf + 1);
+  b.nms_ticket = bs.d_ticket;
+  b.err = c->d_err;
+  b.fast_thr = c->p.fast_threshold;
+  b.harris = c->p.score_type == 0 ? 1 : 0;
+  b.wta_k = c->p.wta_k;
+  b.half_k = c->half_k;
+  for (int i = 0; i < 4; i++) b.gauss[i] = c->gauss[i];
+  b.harris_scale4 = c->scale4;
+  b.pattern = c->d_pattern;
+  b.umax = c->d_umax;
+  plan->pyr_tiles = pb[nf];
+  plan->det_tiles = db[nf];
+  plan->nms_strips = nb[nf];
+  plan->total_max_pts = (int)(tmp > (1 << 30) ? (1 << 30) : tmp);
+  return ORBX_OK;
+}
+
+static int launch_frames(orbx_ctx* c, const LaunchPlan& pl, bool compute_desc) {
+  ORBX_CUDA(launch_pyramid_blur(pl.b, pl.pyr_tiles, c->stream));
+  ORBX_CUDA(launch_detect(pl.b, pl.det_tiles, c->stream));
+  ORBX_CUDA(launch_nms(pl.b, pl.nms_strips, c->stream));
+  if (compute_desc) ORBX_CUDA(launch_describe(pl.b, pl.total_max_pts, c->stream));
+  return ORBX_OK;
+}
+
+static constexpr int kSplitsCap = 64;
+
+static int mw_ensure(MatchWork& mw, int nq_cap) {
+  if (mw.part && mw.nq_cap >= nq_cap) return ORBX_OK;
+  cudaFree(mw.part);
+  cudaFree(mw.tile_done);
+  mw = MatchWork();
+  const int cap = nq_cap < 128 ? 128 : nq_cap;
+  ORBX_CUDA(cudaMalloc(&mw.part, sizeof(uint32_t) * 2 * (size_t)kSplitsCap * cap));
+  ORBX_CUDA(cudaMalloc(&mw.tile_done, sizeof(unsigned int) * (size_t)div_up(cap, 128)));
+  ORBX_CUDA(cudaMemset(mw.tile_done, 0, sizeof(unsigned int) * (size_t)div_up(cap, 128)));
+  mw.nq_cap = cap;
+  mw.splits_cap = kSplitsCap;
+  return ORBX_OK;
+}
+
+static int check_image(const orbx_ctx* c, const uint8_t* img, int w, int h, int pitch) {
+  if (!c) return ORBX_ERR_ARG;
+  if (!c->inited) return ORBX_ERR_STATE;
+  if (!img || w <= 0 || h <= 0 || pitch < w) return ORBX_ERR_ARG;
+  if (w > 16384 || h > 16384) return ORBX_ERR_SIZE;
+  return ORBX_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Lower-level entry points of orbd.h (orbd.cu:1564-1793) on caller-owned
+// pyramid buffers.  The caller's buffers have no guard bytes, so each call
+// runs on the context's guarded workspace and copies between the two.
+// ---------------------------------------------------------------------------
+namespace orbx {
+
+static int lower_workspace(orbx_ctx* c, const int* oszp, int noctaves, Workspace** out) {
+  if (!c || !oszp || noctaves < 1 || noctaves > kMaxOctaves) return ORBX_ERR_ARG;
+  if (!c->inited) return ORBX_ERR_STATE;
+  const int w = oszp[noctaves], h = oszp[2 * noctaves];
+  int rc = ws_ensure(c, c->ws[0], w, h, noctaves);
+  if (rc) return rc;
+  Workspace& ws = c->ws[0];
+  if (ws.n != noctaves || std::memcmp(ws.oszp, oszp, sizeof(int) * (5 * noctaves + 1)) != 0) return ORBX_ERR_SIZE;
+  *out = &ws;
+  return ORBX_OK;
+}
+
+static int lower_run(orbx_ctx* c, Workspace& ws, Frame& F, int stage, int describe_mode, int threshold, int harris,
+                     int wta_k, int half_k, int n_pts) {
+  std::vector<Frame> frames(1, F);
+  LaunchPlan pl;
+  int rc = upload_batch(c, c->single, frames, &pl);
+  if (rc) return rc;
+  pl.b.fast_thr = threshold;
+  pl.b.harris = harris;
+  pl.b.wta_k = wta_k;
+  pl.b.half_k = half_k;
+  pl.b.describe_mode = describe_mode;
+  if (stage == 0) {
+    ORBX_CUDA(launch_pyramid_blur(pl.b, pl.pyr_tiles, c->stream));
+    ORBX_CUDA(launch_detect(pl.b, pl.det_tiles, c->stream));
+    ORBX_CUDA(launch_nms(pl.b, pl.nms_strips, c->stream));
+  } else if (stage == 1) {
+    ORBX_CUDA(launch_pyramid_blur(pl.b, pl.pyr_tiles, c->stream));
+  } else {
+    ORBX_CUDA(launch_describe(pl.b, n_pts, c->stream));
+  }
+  (void)ws;
+  return ORBX_OK;
+}
+
+int lower_detect(orbx_ctx* c, const uint8_t* image, uint8_t* octave_images, float* vmem, orbx_point* pts,
+                 int* d_count, const int* oszp, int noctaves, int threshold, int border, bool harris) {
+  Workspace* ws = nullptr;
+  int rc = lower_workspace(c, oszp, noctaves, &ws);
+  if (rc) return rc;
+  if (!image || !pts || !d_count) return ORBX_ERR_ARG;
+  Frame F;
+  fill_frame(c, *ws, image, ws->oszp[3 * noctaves], pts, nullptr, d_count, F);
+  F.border = border < 3 ? 3 : border;
+  F.nms_strips = (F.h - 2 * F.border > 0 && F.w - 2 * F.border > 0) ? div_up(F.h - 2 * F.border, kNmsRows) : 0;
+  rc = lower_run(c, *ws, F, 0, kDescribeBoth, threshold, harris ? 1 : 0, c->p.wta_k, c->half_k, 0);
+  if (rc) return rc;
+  const size_t npx = (size_t)ws->h * ws->oszp[3 * noctaves];
+  if (octave_images)
+    ORBX_CUDA(cudaMemcpyAsync(octave_images, ws->pyr_alloc + ws->guard, ws->obytes, cudaMemcpyDeviceToDevice, c->stream));
+  if (vmem) {
+    ORBX_CUDA(cudaMemcpyAsync(vmem, ws->vmap, npx * sizeof(float), cudaMemcpyDeviceToDevice, c->stream));
+    ORBX_CUDA(cudaMemcpyAsync(vmem + npx, ws->layer, npx * sizeof(int), cudaMemcpyDeviceToDevice, c->stream));
+  }
+  return ORBX_OK;
+}
+
+int lower_angle(orbx_ctx* c, const uint8_t* octave_images, orbx_point* pts, int n_pts, const int* oszp,
+                int noctaves, int patch_size, int* d_tmp_count) {
+  Workspace* ws = nullptr;
+  int rc = lower_workspace(c, oszp, noctaves, &ws);
+  if (rc) return rc;
+  if (n_pts <= 0) return ORBX_OK;
+  if (!octave_images || !pts || patch_size / 2 != c->half_k) return ORBX_ERR_ARG;
+  ORBX_CUDA(cudaMemcpyAsync(ws->pyr_alloc + ws->guard, octave_images, ws->obytes, cudaMemcpyDeviceToDevice, c->stream));
+  ORBX_CUDA(cudaMemcpyAsync(d_tmp_count, &n_pts, sizeof(int), cudaMemcpyHostToDevice, c->stream));
+  Frame F;
+  fill_frame(c, *ws, octave_images, ws->oszp[3 * noctaves], pts, nullptr, d_tmp_count, F);
+  return lower_run(c, *ws, F, 2, kDescribeAngleOnly, c->p.fast_threshold, 1, c->p.wta_k, c->half_k, n_pts);
+}
+
+int lower_blur(orbx_ctx* c, uint8_t* octave_images, const int* oszp, int noctaves, int* d_tmp_count) {
+  Workspace* ws = nullptr;
+  int rc = lower_workspace(c, oszp, noctaves, &ws);
+  if (rc) return rc;
+  if (!octave_images) return ORBX_ERR_ARG;
+  ORBX_CUDA(cudaMemcpyAsync(ws->pyr_alloc + ws->guard, octave_images, ws->obytes, cudaMemcpyDeviceToDevice, c->stream));
+  Frame F;
+  fill_frame(c, *ws, octave_images, ws->oszp[3 * noctaves], nullptr, nullptr, d_tmp_count, F);
+  F.pyr_src = ws->pyr_alloc + ws->guard;
+  rc = lower_run(c, *ws, F, 1, kDescribeBoth, c->p.fast_threshold, 1, c->p.wta_k, c->half_k, 0);
+  if (rc) return rc;
+  ORBX_CUDA(cudaMemcpyAsync(octave_images, ws->blr_alloc + ws->guard, ws->obytes, cudaMemcpyDeviceToDevice, c->stream));
+  return ORBX_OK;
+}
+
+int lower_last_layout(orbx_ctx* c, int* oszp, int noctaves) {
+  if (!c || !oszp) return ORBX_ERR_ARG;
+  const Workspace& ws = c->ws[0];
+  if (!ws.pyr_alloc || ws.n != noctaves) return ORBX_ERR_STATE;
+  std::memcpy(oszp, ws.oszp, sizeof(int) * (5 * noctaves + 1));
+  return ORBX_OK;
+}
+
+int lower_describe(orbx_ctx* c, const uint8_t* octave_images, orbx_point* pts, int n_pts, uint8_t* desc, int wta_k,
+                   const int* oszp, int noctaves, int* d_tmp_count) {
+  Workspace* ws = nullptr;
+  int rc = lower_workspace(c, oszp, noctaves, &ws);
+  if (rc) return rc;
+  if (n_pts <= 0) return ORBX_OK;
+  if (!octave_images || !pts || !desc || wta_k < 2 || wta_k > 4) return ORBX_ERR_ARG;
+  ORBX_CUDA(cudaMemcpyAsync(ws->blr_alloc + ws->guard, octave_images, ws->obytes, cudaMemcpyDeviceToDevice, c->stream));
+  ORBX_CUDA(cudaMemcpyAsync(d_tmp_count, &n_pts, sizeof(int), cudaMemcpyHostToDevice, c->stream));
+  Frame F;
+  fill_frame(c, *ws, octave_images, ws->oszp[3 * noctaves], pts, desc, d_tmp_count, F);
+  return lower_run(c, *ws, F, 2, kDescribeDescOnly, c->p.fast_threshold, 1, wta_k, c->half_k, n_pts);
+}
+
+}  // namespace orbx
+
+// ---------------------------------------------------------------------------
+// C ABI
+// ---------------------------------------------------------------------------
+extern "C" {
+
+ORBX_API const char* orbx_version(void) { return "orbx 0.1 (sm_100a)"; }
+
+ORBX_API const char* orbx_status_string(int status) {
+  switch (status) {
+    case ORBX_OK: return "ok";
+    case ORBX_ERR_ARG: return "invalid argument";
+    case ORBX_ERR_CUDA: return "CUDA runtime error";
+    case ORBX_ERR_SIZE: return "size out of supported range";
+    case ORBX_ERR_STATE: return "context not initialised";
+    case ORBX_ERR_TIMEOUT: return "device-side wait timed out";
+    case ORBX_ERR_NOMEM: return "device out of memory";
+    default: return "unknown status";
+  }
+}
+
+ORBX_API int orbx_create(orbx_ctx** out, int device) {
+  if (!out) return ORBX_ERR_ARG;
+  *out = nullptr;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || device < 0 || device >= ndev) {
+    (void)cudaGetLastError();
+    return ORBX_ERR_CUDA;
+  }
+  DeviceGuard g(device);
+  orbx_ctx* c = new orbx_ctx();
+  c->device = device;
+  if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaMalloc(&c->d_pattern, 1024) != cudaSuccess || cudaMalloc(&c->d_umax, 32 * sizeof(int)) != cudaSuccess ||
+      cudaMalloc(&c->d_err, sizeof(int)) != cudaSuccess || cudaMemset(c->d_err, 0, sizeof(int)) != cudaSuccess) {
+    (void)cudaGetLastError();
+    delete c;
+    return ORBX_ERR_CUDA;
+  }
+  c->own_stream = true;
+  *out = c;
+  return ORBX_OK;
+}
+
+ORBX_API int orbx_destroy(orbx_ctx* c) {
+  if (!c) return ORBX_ERR_ARG;
+  DeviceGuard g(c->device);
+  cudaStreamSynchronize(c->stream);
+  for (auto& ws : c->ws) ws_free(ws);
+  for (BatchSlot* bs : {&c->single, &c->pair}) {
+    cudaFree(bs->d_frames);
+    cudaFree(bs->d_bases);
+    cudaFree(bs->d_ticket);
+    cudaFreeHost(bs->h_stage);
+    if (bs->uploaded) cudaEventDestroy(bs->uploaded);
+  }
+  if (c->pg.exec) cudaGraphExecDestroy(c->pg.exec);
+  cudaFree(c->pg.mw.part);
+  cudaFree(c->pg.mw.tile_done);
+  cudaFree(c->mw.part);
+  cudaFree(c->mw.tile_done);
+  cudaFree(c->d_pattern);
+  cudaFree(c->d_umax);
+  cudaFree(c->d_err);
+  if (c->own_stream) cudaStreamDestroy(c->stream);
+  delete c;
+  return ORBX_OK;
+}
+
+ORBX_API int orbx_set_stream(orbx_ctx* c, void* stream) {
+  if (!c) return ORBX_ERR_ARG;
+  DeviceGuard g(c->device);
+  cudaStreamSynchronize(c->stream);
+  if (c->own_stream) cudaStreamDestroy(c->stream);
+  c->stream = (cudaStream_t)stream;
+  c->own_stream = false;
+  if (c->pg.exec) {
+    cudaGraphExecDestroy(c->pg.exec);
+    c->pg.exec = nullptr;
+    c->pg.valid = false;
+  }
+  return ORBX_OK;
+}
+
+ORBX_API void* orbx_get_stream(orbx_ctx* c) { return c ? (void*)c->stream : nullptr; }
+
+ORBX_API int orbx_sync(orbx_ctx* c) {
+  if (!c) return ORBX_ERR_ARG;
+  DeviceGuard g(c->device);
+  ORBX_CUDA(cudaStreamSynchronize(c->stream));
+  int err = 0;
+  ORBX_CUDA(cudaMemcpy(&err, c->d_err, sizeof(int), cudaMemcpyDeviceToHost));
+  if (err) {
+    ORBX_CUDA(cudaMemset(c->d_err, 0, sizeof(int)));
+    return ORBX_ERR_TIMEOUT;
+  }
+  return ORBX_OK;
+}
+
+ORBX_API int orbx_default_params(orbx_params* p) {
+  if (!p) return ORBX_ERR_ARG;
+  // Orbor::init defaults (orb.h:18-19)
+  p->noctaves = 5;
+  p->edge_threshold = 31;
+  p->wta_k = 2;
+  p->score_type = 0;
+  p->patch_size = 31;
+  p->fast_threshold = 20;
+  p->retain_topn = -1;
+  p->max_pts = 1000;
+  return ORBX_OK;
+}
+
+ORBX_API int orbx_init(orbx_ctx* c, const orbx_params* p) {
+  if (!c || !p) return ORBX_ERR_ARG;
+  if (p->wta_k < 2 || p->wta_k > 4 || (p->score_type != 0 && p->score_type != 1) || p->patch_size < 3 ||
+      p->patch_size > 31 || p->max_pts < 1 || p->max_pts > (1 << 22) || p->fast_threshold < 0 ||
+      p->fast_threshold > 255 || p->noctaves < 1 || p->edge_threshold < 0)
+    return ORBX_ERR_ARG;
+  DeviceGuard g(c->device);
+  ORBX_CUDA(cudaStreamSynchronize(c->stream));
+  const bool shape_change = !c->inited || c->p.noctaves != p->noctaves || c->p.edge_threshold != p->edge_threshold;
+  c->p = *p;
+  int8_t pat[1024];
+  make_pattern(p->patch_size, p->wta_k, pat);
+  int umax[32] = {0};
+  make_umax(p->patch_size, umax);
+  make_gauss(c->gauss);
+  c->scale4 = make_scale4();
+  c->half_k = p->patch_size / 2;
+  ORBX_CUDA(cudaMemcpy(c->d_pattern, pat, sizeof(pat), cudaMemcpyHostToDevice));
+  ORBX_CUDA(cudaMemcpy(c->d_umax, umax, sizeof(umax), cudaMemcpyHostToDevice));
+  if (shape_change)
+    for (auto& ws : c->ws) ws_free(ws);
+  if (c->pg.exec) {
+    cudaGraphExecDestroy(c->pg.exec);
+    c->pg.exec = nullptr;
+  }
+  c->pg.valid = false;
+  c->single.last.clear();
+  c->pair.last.clear();
+  c->inited = true;
+  return ORBX_OK;
+}
+
+ORBX_API int orbx_layout(int w, int h, int noctaves, int* oszp, int cap) {
+  if (!oszp || w <= 0 || h <= 0 || noctaves < 1) return -ORBX_ERR_ARG;
+  int buf[5 * kMaxOctaves + 1];
+  const int n = compute_layout(w, h, noctaves, buf);
+  if (n < 0) return n;
+  if (cap < 5 * n + 1) return -ORBX_ERR_ARG;
+  std::memcpy(oszp, buf, sizeof(int) * (5 * n + 1));
+  return n;
+}
+
+ORBX_API int orbx_detect_and_compute(orbx_ctx* c, const uint8_t* d_image, int w, int h, int pitch,
+                                     orbx_point* d_points, uint8_t* d_desc, int* d_num_pts, int compute_desc) {
+  int rc = check_image(c, d_image, w, h, pitch);
+  if (rc) return rc;
+  if (!d_points || !d_num_pts || (compute_desc && !d_desc)) return ORBX_ERR_ARG;
+  DeviceGuard g(c->device);
+  rc = ws_ensure(c, c->ws[0], w, h);
+  if (rc) return rc;
+  std::vector<Frame> frames(1);
+  fill_frame(c, c->ws[0], d_image, pitch, d_points, d_desc, d_num_pts, frames[0]);
+  LaunchPlan pl;
+  rc = upload_batch(c, c->single, frames, &pl);
+  if (rc) return rc;
+  return launch_frames(c, pl, compute_desc != 0);
+}
+
+static int match_common(orbx_ctx* c, MatchWork& mw, const MatchArgs& a, int nq_cap, int mode) {
+  if (mode != ORBX_MATCH_POPC && mode != ORBX_MATCH_AUTO) return ORBX_ERR_ARG;
+  int rc = mw_ensure(mw, nq_cap);
+  if (rc) return rc;
+  ORBX_CUDA(launch_match_popc(a, mw, c->stream));
+  return ORBX_OK;
+}
+
+ORBX_API int orbx_match(orbx_ctx* c, orbx_point* d_points1, const int* d_n1, const uint8_t* d_desc1,
+                        const int* d_n2, const uint8_t* d_desc2, int n1_cap, int n2_cap, int mode) {
+  if (!c || !d_points1 || !d_n1 || !d_desc1 || !d_n2 || (!d_desc2 && n2_cap > 0) || n1_cap < 0 || n2_cap < 0)
+    return ORBX_ERR_ARG;
+  if (n2_cap > (1 << 22) - 1) return ORBX_ERR_SIZE;
+  if (n1_cap == 0) return ORBX_OK;
+  DeviceGuard g(c->device);
+  MatchArgs a{};
+  a.q = d_desc1;
+  a.db = d_desc2;
+  a.nq = n1_cap;
+  a.ndb = n2_cap;
+  a.d_nq = d_n1;
+  a.d_ndb = d_n2;
+  a.pts = d_points1;
+  return match_common(c, c->mw, a, n1_cap, mode);
+}
+
+ORBX_API int orbx_match_knn2(orbx_ctx* c, const uint8_t* d_q, int nq, const uint8_t* d_db, int ndb,
+                             uint32_t* d_dist2, int32_t* d_idx2, int mode) {
+  if (!c || nq < 0 || ndb < 0 || (nq > 0 && (!d_q || !d_dist2 || !d_idx2)) || (ndb > 0 && !d_db))
+    return ORBX_ERR_ARG;
+  if (ndb > (1 << 22) - 1) return ORBX_ERR_SIZE;
+  if (nq == 0) return ORBX_OK;
+  DeviceGuard g(c->device);
+  MatchArgs a{};
+  a.q = d_q;
+  a.db = d_db;
+  a.nq = nq;
+  a.ndb = ndb;
+  a.dist2 = d_dist2;
+  a.idx2 = d_idx2;
+  return match_common(c, c->mw, a, nq, mode);
+}
+
+ORBX_API int orbx_pair(orbx_ctx* c, const uint8_t* d_img_a, const uint8_t* d_img_b, int w, int h, int pitch,
+                       orbx_point* d_pts_a, uint8_t* d_desc_a, int* d_n_a, orbx_point* d_pts_b, uint8_t* d_desc_b,
+                       int* d_n_b, int mode) {
+  int rc = check_image(c, d_img_a, w, h, pitch);
+  if (rc) return rc;
+  if (!d_img_b || !d_pts_a || !d_desc_a || !d_n_a || !d_pts_b || !d_desc_b || !d_n_b) return ORBX_ERR_ARG;
+  if (mode != ORBX_MATCH_POPC && mode != ORBX_MATCH_AUTO) return ORBX_ERR_ARG;
+  DeviceGuard g(c->device);
+  if ((rc = ws_ensure(c, c->ws[0], w, h)) != 0) return rc;
+  if ((rc = ws_ensure(c, c->ws[1], w, h)) != 0) return rc;
+  std::vector<Frame> frames(2);
+  fill_frame(c, c->ws[0], d_img_a, pitch, d_pts_a, d_desc_a, d_n_a, frames[0]);
+  fill_frame(c, c->ws[1], d_img_b, pitch, d_pts_b, d_desc_b, d_n_b, frames[1]);
+  LaunchPlan pl;
+  if ((rc = upload_batch(c, c->pair, frames, &pl)) != 0) return rc;
+  MatchArgs a{};
+  a.q = d_desc_a;
+  a.db = d_desc_b;
+  a.nq = c->p.max_pts;
+  a.ndb = c->p.max_pts;
+  a.d_nq = d_n_a;
+  a.d_ndb = d_n_b;
+  a.pts = d_pts_a;
+  // graph key: launch shapes and every pointer baked into the captured launches
+  std::vector<uint8_t> key(sizeof(Batch) + sizeof(MatchArgs) + sizeof(LaunchPlan) + sizeof(int));
+  {
+    uint8_t* k = key.data();
+    std::memcpy(k, &pl.b, sizeof(Batch));
+    std::memcpy(k + sizeof(Batch), &a, sizeof(MatchArgs));
+    LaunchPlan pz = pl;
+    std::memset(&pz.b, 0, sizeof(Batch));
+    std::memcpy(k + sizeof(Batch) + sizeof(MatchArgs), &pz, sizeof(LaunchPlan));
+    std::memcpy(k + sizeof(Batch) + sizeof(MatchArgs) + sizeof(LaunchPlan), &mode, sizeof(int));
+  }
+  PairGraph& pg = c->pg;
+  if (!(pg.valid && pg.key == key)) {
+    if (pg.exec) {
+      cudaGraphExecDestroy(pg.exec);
+      pg.exec = nullptr;
+    }
+    pg.valid = false;
+    if ((rc = mw_ensure(pg.mw, c->p.max_pts)) != 0) return rc;
+    cudaGraph_t graph = nullptr;
+    ORBX_CUDA(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+    int lrc = launch_frames(c, pl, true);
+    if (lrc == ORBX_OK) lrc = launch_match_popc(a, pg.mw, c->stream) == cudaSuccess ? ORBX_OK : ORBX_ERR_CUDA;
+    const cudaError_t ce = cudaStreamEndCapture(c->stream, &graph);
+    if (lrc != ORBX_OK) {
+      if (graph) cudaGraphDestroy(graph);
+      return lrc;
+    }
+    ORBX_CUDA(ce);
+    const cudaError_t ie = cudaGraphInstantiate(&pg.exec, graph, 0);
+    cudaGraphDestroy(graph);
+    ORBX_CUDA(ie);
+    pg.key.swap(key);
+    pg.valid = true;
+  }
+  ORBX_CUDA(cudaGraphLaunch(pg.exec, c->stream));
+  return ORBX_OK;
+}
+
+ORBX_API int orbx_debug_buffers(orbx_ctx* c, uint8_t* h_pyr, uint8_t* h_blur, float* h_vmap, int* h_layer,
+                                int* h_total) {
+  if (!c) return ORBX_ERR_ARG;
+  const Workspace& ws = c->ws[0];
+  if (!ws.pyr_alloc) return ORBX_ERR_STATE;
+  DeviceGuard g(c->device);
+  ORBX_CUDA(cudaStreamSynchronize(c->stream));
+  const size_t npx = (size_t)ws.h * ws.oszp[3 * ws.n];
+  if (h_pyr) ORBX_CUDA(cudaMemcpy(h_pyr, ws.pyr_alloc + ws.guard, ws.obytes, cudaMemcpyDeviceToHost));
+  if (h_blur) ORBX_CUDA(cudaMemcpy(h_blur, ws.blr_alloc + ws.guard, ws.obytes, cudaMemcpyDeviceToHost));
+  if (h_vmap) ORBX_CUDA(cudaMemcpy(h_vmap, ws.vmap, npx * sizeof(float), cudaMemcpyDeviceToHost));
+  if (h_layer) ORBX_CUDA(cudaMemcpy(h_layer, ws.layer, npx * sizeof(int), cudaMemcpyDeviceToHost));
+  if (h_total) ORBX_CUDA(cudaMemcpy(h_total, ws.total, sizeof(int), cudaMemcpyDeviceToHost));
+  return ORBX_OK;
+}
+
+ORBX_API long long orbx_selftest_pi_minus(uint32_t lo_bits, uint32_t hi_bits) {
+  long long bad = 0;
+  for (uint64_t b = lo_bits; b < hi_bits; b++) {
+    const uint32_t bits = (uint32_t)b;
+    float r;
+    std::memcpy(&r, &bits, 4);
+    if (!(r >= 0.f && r < 2.f)) continue;
+    const float want = (float)(3.14159265358979323846 - (double)r);
+    const float got = pi_minus_as_double(r);
+    uint32_t wb, gb;
+    std::memcpy(&wb, &want, 4);
+    std::memcpy(&gb, &got, 4);
+    bad += (wb != gb);
+  }
+  return bad;
+}
+
+}  // extern "C"

@@ -1,0 +1,113 @@
+// Internal structures shared by the sm_100a ORB kernels and the C ABI layer.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "../../include/orbx.h"
+
+namespace orbx {
+
+constexpr int kMaxOctaves = 5;        // MAX_OCTAVE, orbd.cu:18
+constexpr int kMaxFramesPerLaunch = 1024;
+constexpr size_t kGuard = 256 * 1024; // zeroed bytes before/after each pyramid
+
+// Pyramid-and-blur tile (octave pixels)
+constexpr int kPyrTW = 128;
+constexpr int kPyrTH = 32;
+// Detect tile (level-0 pixels); 32 keeps octave 4/5 tiles whole
+constexpr int kDetTW = 64;
+constexpr int kDetTH = 32;
+// NMS strip height (level-0 rows); strips span the full valid width
+constexpr int kNmsRows = 4;
+
+// Per-frame state, in device memory (one entry per frame of a launch).
+struct Frame {
+  const uint8_t* img;  // level-0 input, row pitch `pitch_in`
+  const uint8_t* pyr_src;  // optional: an existing pyramid (reference layout) to blur instead of img
+  int w, h, pitch_in;
+  int n_oct;
+  int ow[kMaxOctaves], oh[kMaxOctaves], op[kMaxOctaves];
+  long long ooff[kMaxOctaves + 1];  // octave offsets in the pyramid (orb.cpp:151-174)
+  uint8_t* pyr;  // octave 0 of the raw pyramid (kGuard zeroed bytes on both sides)
+  uint8_t* blr;  // octave 0 of the blurred pyramid (same layout and guards)
+  float* vmap;   // level-0 keyed score map, h * op[0] floats
+  int* layer;    // octave of each score map entry, h * op[0] ints
+  orbx_point* pts;
+  uint8_t* desc;
+  int* count;    // min(survivors, max_pts)
+  int* total;    // survivors before the cap (may be null)
+  int max_pts;
+  int border;    // max(edge_threshold, 3)
+  // tiling
+  int pyr_tiles_x[kMaxOctaves], pyr_tiles_y[kMaxOctaves];
+  int pyr_tile_base[kMaxOctaves + 1];  // per-octave prefix within the frame
+  int det_tiles_x, det_tiles_y;
+  int nms_strips;
+  unsigned long long* nms_status;  // look-back words, one per strip
+};
+
+// Per-launch view of a batch of frames.
+struct Batch {
+  Frame* frames;
+  int n_frames;
+  const int* pyr_base;   // [n_frames + 1] tile prefix over frames for k_pyramid_blur
+  const int* det_base;   // [n_frames + 1] for k_detect
+  const int* nms_base;   // [n_frames + 1] for k_nms
+  unsigned int* nms_ticket;  // dynamic strip ticket (reset by k_pyramid_blur)
+  int* err;              // sticky error word (bounded waits that gave up)
+  int describe_mode;     // 0: angle + descriptor, 1: angle only, 2: descriptor only
+  // parameters (Orbor::init, orb.h:18-19)
+  int fast_thr;
+  int harris;            // 1: HARRIS_SCORE, 0: FAST_SCORE
+  int wta_k;
+  int half_k;            // patch_size / 2
+  float gauss[4];        // setGaussianKernel weights (host expf, orbd.cu:413-433)
+  float harris_scale4;   // setScaleSqSq (orbd.cu:436-441)
+  const int8_t* pattern; // [512][2] sampling points (setPattern)
+  const int* umax;       // [half_k + 2] (setUmax)
+};
+
+enum : int {
+  kErrLookbackTimeout = 1,
+};
+enum : int { kDescribeBoth = 0, kDescribeAngleOnly = 1, kDescribeDescOnly = 2 };
+
+// host-side helpers implemented in orbx_api.cu
+}  // namespace orbx
+
+// kernel launchers (orbx_detect.cu / orbx_describe.cu / orbx_match.cu)
+namespace orbx {
+cudaError_t launch_pyramid_blur(const Batch& b, int total_tiles, cudaStream_t s);
+cudaError_t launch_detect(const Batch& b, int total_tiles, cudaStream_t s);
+cudaError_t launch_nms(const Batch& b, int total_strips, cudaStream_t s);
+cudaError_t launch_describe(const Batch& b, int total_max_pts, cudaStream_t s);
+
+struct MatchArgs {
+  const uint8_t* q;      // [nq][32]
+  const uint8_t* db;     // [ndb][32]
+  int nq, ndb;
+  const int* d_nq;       // optional device counts (override nq/ndb when non-null)
+  const int* d_ndb;
+  uint32_t* dist2;       // optional [nq][2]
+  int32_t* idx2;         // optional [nq][2]
+  orbx_point* pts;         // optional: reference-semantics match/distance (orbd.cu:1545-1557)
+};
+struct MatchWork {          // scratch for split-train merging
+  uint32_t* part;           // [splits_cap][nq_cap][2] partial top-2 keys
+  unsigned int* tile_done;  // [ceil(nq_cap / 128)] arrival counters, self-resetting
+  int nq_cap;               // query capacity the grid is sized for
+  int splits_cap;           // most train splits per query tile
+};
+int match_popc_blocks(int nq_cap, int splits_cap);
+
+// orbd.h lower-level entry points on caller-owned pyramid buffers (orbx_api.cu)
+int lower_detect(orbx_ctx* c, const uint8_t* image, uint8_t* octave_images, float* vmem, orbx_point* pts,
+                 int* d_count, const int* oszp, int noctaves, int threshold, int border, bool harris);
+int lower_angle(orbx_ctx* c, const uint8_t* octave_images, orbx_point* pts, int n_pts, const int* oszp,
+                int noctaves, int patch_size, int* d_tmp_count);
+int lower_blur(orbx_ctx* c, uint8_t* octave_images, const int* oszp, int noctaves, int* d_tmp_count);
+int lower_last_layout(orbx_ctx* c, int* oszp, int noctaves);
+int lower_describe(orbx_ctx* c, const uint8_t* octave_images, orbx_point* pts, int n_pts, uint8_t* desc, int wta_k,
+                   const int* oszp, int noctaves, int* d_tmp_count);
+cudaError_t launch_match_popc(const MatchArgs& a, const MatchWork& w, cudaStream_t s);
+}  // namespace orbx

@@ -1,0 +1,224 @@
+"""Python binding of liborbx.so (include/orbx.h), the sm_100a ORB library.
+
+Device memory comes from torch tensors; the library itself is the CUDA code in
+csrc/.  There is no CPU path: if the shared library is missing or fails to
+load, import raises.
+
+Keypoints are int32 tensors of shape (max_pts, 7) laid out as orb::OrbPoint
+(x, y, octave, score, angle, match, distance; score and angle are float32 bits).
+"""
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "liborbx.so")
+
+ORBX_OK = 0
+MATCH_POPC = 0
+MATCH_IMMA = 1
+MATCH_AUTO = 2
+HARRIS_SCORE = 0
+FAST_SCORE = 1
+
+POINT_FIELDS = ("x", "y", "octave", "score", "angle", "match", "distance")
+ORB_POINT_DTYPE = np.dtype([("x", "<i4"), ("y", "<i4"), ("octave", "<i4"), ("score", "<f4"),
+                            ("angle", "<f4"), ("match", "<i4"), ("distance", "<i4")])
+
+
+class OrbxError(RuntimeError):
+    def __init__(self, status, what):
+        self.status = status
+        super().__init__(f"{what}: {status_string(status)} ({status})")
+
+
+class Params(ctypes.Structure):
+    _fields_ = [("noctaves", ctypes.c_int), ("edge_threshold", ctypes.c_int), ("wta_k", ctypes.c_int),
+                ("score_type", ctypes.c_int), ("patch_size", ctypes.c_int), ("fast_threshold", ctypes.c_int),
+                ("retain_topn", ctypes.c_int), ("max_pts", ctypes.c_int)]
+
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(f"liborbx.so not built: run `python {os.path.join(HERE, 'build.py')}`")
+        L = ctypes.CDLL(LIB_PATH)
+        vp, i32 = ctypes.c_void_p, ctypes.c_int
+        L.orbx_version.restype = ctypes.c_char_p
+        L.orbx_status_string.restype = ctypes.c_char_p
+        L.orbx_status_string.argtypes = [i32]
+        L.orbx_create.argtypes = [ctypes.POINTER(vp), i32]
+        L.orbx_destroy.argtypes = [vp]
+        L.orbx_set_stream.argtypes = [vp, vp]
+        L.orbx_get_stream.argtypes = [vp]
+        L.orbx_get_stream.restype = vp
+        L.orbx_sync.argtypes = [vp]
+        L.orbx_default_params.argtypes = [ctypes.POINTER(Params)]
+        L.orbx_init.argtypes = [vp, ctypes.POINTER(Params)]
+        L.orbx_layout.argtypes = [i32, i32, i32, vp, i32]
+        L.orbx_detect_and_compute.argtypes = [vp, vp, i32, i32, i32, vp, vp, vp, i32]
+        L.orbx_match.argtypes = [vp, vp, vp, vp, vp, vp, i32, i32, i32]
+        L.orbx_match_knn2.argtypes = [vp, vp, i32, vp, i32, vp, vp, i32]
+        L.orbx_pair.argtypes = [vp, vp, vp, i32, i32, i32, vp, vp, vp, vp, vp, vp, i32]
+        L.orbx_debug_buffers.argtypes = [vp, vp, vp, vp, vp, vp]
+        L.orbx_selftest_pi_minus.argtypes = [ctypes.c_uint32, ctypes.c_uint32]
+        L.orbx_selftest_pi_minus.restype = ctypes.c_longlong
+        _lib = L
+    return _lib
+
+
+def status_string(status):
+    return lib().orbx_status_string(int(status)).decode()
+
+
+def version():
+    return lib().orbx_version().decode()
+
+
+def _check(status, what):
+    if status != ORBX_OK:
+        raise OrbxError(status, what)
+
+
+def _ptr(t):
+    if t is None:
+        return None
+    if isinstance(t, int):
+        return t
+    return t.data_ptr()
+
+
+def layout(w, h, noctaves=8):
+    buf = np.zeros(64, dtype=np.int32)
+    n = lib().orbx_layout(w, h, noctaves, buf.ctypes.data, 64)
+    if n < 0:
+        raise OrbxError(-n, "orbx_layout")
+    return n, buf[:5 * n + 1].copy()
+
+
+def default_params():
+    p = Params()
+    _check(lib().orbx_default_params(ctypes.byref(p)), "orbx_default_params")
+    return p
+
+
+def make_params(noctaves=8, edge_threshold=31, wta_k=2, score_type=HARRIS_SCORE, patch_size=31, fast_threshold=20,
+                retain_topn=-1, max_pts=10000):
+    return Params(noctaves, edge_threshold, wta_k, score_type, patch_size, fast_threshold, retain_topn, max_pts)
+
+
+class Context:
+    """An orbx context: tables, workspaces and a CUDA stream on one device."""
+
+    def __init__(self, device=0, params=None, stream=None):
+        h = ctypes.c_void_p()
+        _check(lib().orbx_create(ctypes.byref(h), device), "orbx_create")
+        self.h = h
+        self.device = device
+        self.params = None
+        if stream is not None:
+            self.set_stream(stream)
+        if params is not None:
+            self.init(params)
+
+    def close(self):
+        if self.h:
+            lib().orbx_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_stream(self, stream):
+        handle = stream.cuda_stream if hasattr(stream, "cuda_stream") else stream
+        _check(lib().orbx_set_stream(self.h, handle), "orbx_set_stream")
+
+    @property
+    def stream_handle(self):
+        return lib().orbx_get_stream(self.h)
+
+    def init(self, params):
+        _check(lib().orbx_init(self.h, ctypes.byref(params)), "orbx_init")
+        self.params = params
+
+    def sync(self):
+        _check(lib().orbx_sync(self.h), "orbx_sync")
+
+    # -- raw pointer entry points -------------------------------------------
+    def detect_and_compute_ptr(self, d_img, w, h, pitch, d_points, d_desc, d_count, compute_desc=True):
+        _check(lib().orbx_detect_and_compute(self.h, _ptr(d_img), w, h, pitch, _ptr(d_points), _ptr(d_desc),
+                                             _ptr(d_count), int(bool(compute_desc))), "orbx_detect_and_compute")
+
+    def match_ptr(self, d_points1, d_n1, d_desc1, d_n2, d_desc2, n1_cap, n2_cap, mode=MATCH_POPC):
+        _check(lib().orbx_match(self.h, _ptr(d_points1), _ptr(d_n1), _ptr(d_desc1), _ptr(d_n2), _ptr(d_desc2),
+                                n1_cap, n2_cap, mode), "orbx_match")
+
+    def knn2_ptr(self, d_q, nq, d_db, ndb, d_dist2, d_idx2, mode=MATCH_POPC):
+        _check(lib().orbx_match_knn2(self.h, _ptr(d_q), nq, _ptr(d_db), ndb, _ptr(d_dist2), _ptr(d_idx2), mode),
+               "orbx_match_knn2")
+
+    def pair_ptr(self, d_a, d_b, w, h, pitch, pa, da, na, pb, db, nb, mode=MATCH_POPC):
+        _check(lib().orbx_pair(self.h, _ptr(d_a), _ptr(d_b), w, h, pitch, _ptr(pa), _ptr(da), _ptr(na), _ptr(pb),
+                               _ptr(db), _ptr(nb), mode), "orbx_pair")
+
+    def debug_buffers(self, w, h):
+        n, oszp = layout(w, h, self.params.noctaves)
+        obytes = int(oszp[5 * n])
+        npx = int(oszp[0])
+        pyr = np.zeros(obytes, dtype=np.uint8)
+        blur = np.zeros(obytes, dtype=np.uint8)
+        vmap = np.zeros(npx, dtype=np.float32)
+        layer = np.zeros(npx, dtype=np.int32)
+        total = np.zeros(1, dtype=np.int32)
+        _check(lib().orbx_debug_buffers(self.h, pyr.ctypes.data, blur.ctypes.data, vmap.ctypes.data,
+                                        layer.ctypes.data, total.ctypes.data), "orbx_debug_buffers")
+        return {"pyr": pyr, "blur": blur, "vmap": vmap, "layer": layer, "total": int(total[0]), "n": n,
+                "oszp": oszp}
+
+
+# -- torch conveniences -------------------------------------------------------
+def _torch():
+    import torch
+    return torch
+
+
+class FrameBuffers:
+    """Device buffers for one image's keypoints, descriptors and count."""
+
+    def __init__(self, max_pts, device="cuda"):
+        torch = _torch()
+        self.max_pts = max_pts
+        self.points = torch.zeros((max_pts, 7), dtype=torch.int32, device=device)
+        self.desc = torch.zeros((max_pts, 32), dtype=torch.uint8, device=device)
+        self.count = torch.zeros(1, dtype=torch.int32, device=device)
+
+    def to_host(self):
+        n = int(self.count.item())
+        pts = self.points[:n].cpu().numpy().copy().view(ORB_POINT_DTYPE).reshape(n)
+        return pts, self.desc[:n].cpu().numpy().copy()
+
+
+def detect_and_compute(ctx, img, w, h, bufs=None, compute_desc=True):
+    """img: uint8 CUDA tensor of shape (h, pitch).  Returns FrameBuffers (asynchronous)."""
+    if bufs is None:
+        bufs = FrameBuffers(ctx.params.max_pts, img.device)
+    ctx.detect_and_compute_ptr(img, w, h, img.shape[1], bufs.points, bufs.desc, bufs.count, compute_desc)
+    return bufs
+
+
+def knn2(ctx, q, db, mode=MATCH_POPC):
+    """q, db: uint8 CUDA tensors (n, 32).  Returns (dist2 uint32 as int64, idx2 int32) CUDA tensors."""
+    torch = _torch()
+    nq, ndb = q.shape[0], db.shape[0]
+    dist = torch.empty((nq, 2), dtype=torch.int32, device=q.device)
+    idx = torch.empty((nq, 2), dtype=torch.int32, device=q.device)
+    ctx.knn2_ptr(q, nq, db if ndb else None, ndb, dist, idx, mode)
+    return dist, idx

@@ -1,0 +1,135 @@
+/* orbx -- C ABI of the sm_100a ORB detect / describe / match library.
+ *
+ * Plain pointers and sizes only.  Device pointers are prefixed d_, host
+ * pointers h_.  Every call returns an ORBX_* status; nothing exits the process.
+ * Work is queued on the context's CUDA stream and does not synchronise the
+ * host unless the call says so.
+ *
+ * Each entry point names the reference interface it replaces (CUDA-ORB,
+ * file:line).  The C++ classes of the reference (orb.h, orbd.h) are provided on
+ * top of this ABI by include/orb.h and include/orbd.h.
+ */
+#ifndef ORBX_H
+#define ORBX_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define ORBX_API __attribute__((visibility("default")))
+
+/* Same 28-byte layout and field order as orb::OrbPoint (orb_structures.h:8-17):
+ * x, y are level-0 coordinates; octave is the pyramid level; score is the Harris
+ * (or FAST) score; angle is in radians; match/distance are written by matching. */
+typedef struct orbx_point {
+  int x;
+  int y;
+  int octave;
+  float score;
+  float angle;
+  int match;
+  int distance;
+} orbx_point;
+
+/* Orbor::init arguments (orb.h:18-19, orb.cpp:32-54). */
+typedef struct orbx_params {
+  int noctaves;       /* requested levels; clamped as orb.cpp:148 does */
+  int edge_threshold; /* NMS border in level-0 pixels */
+  int wta_k;          /* 2, 3 or 4 */
+  int score_type;     /* 0 = HARRIS_SCORE, 1 = FAST_SCORE (orb_structures.h:31-35) */
+  int patch_size;     /* <= 31 */
+  int fast_threshold;
+  int retain_topn;    /* accepted and ignored, as in the reference (orb.cpp:41) */
+  int max_pts;        /* keypoint cap per image */
+} orbx_params;
+
+typedef struct orbx_ctx orbx_ctx;
+
+enum {
+  ORBX_OK = 0,
+  ORBX_ERR_ARG = 1,     /* bad argument (null pointer, negative size, ...) */
+  ORBX_ERR_CUDA = 2,    /* a CUDA runtime call failed */
+  ORBX_ERR_SIZE = 3,    /* image or set size outside the supported range */
+  ORBX_ERR_STATE = 4,   /* orbx_init not called */
+  ORBX_ERR_TIMEOUT = 5, /* a bounded device-side wait gave up */
+  ORBX_ERR_NOMEM = 6    /* device allocation failed */
+};
+
+enum {
+  ORBX_MATCH_POPC = 0, /* XOR + popcount over 32-bit words */
+  ORBX_MATCH_IMMA = 1, /* +-1 int8 tcgen05 MMA, Hamming = (256 - dot) / 2 */
+  ORBX_MATCH_AUTO = 2
+};
+
+ORBX_API const char* orbx_version(void);
+ORBX_API const char* orbx_status_string(int status);
+
+/* Context: holds what the reference keeps in process-global __constant__ and
+ * __device__ state (orbd.cu:32-41) plus its own stream and workspaces, so that
+ * several contexts can coexist.  Replaces orb::Orbor::Orbor/~Orbor (orb.cpp:14-29). */
+ORBX_API int orbx_create(orbx_ctx** ctx, int device);
+ORBX_API int orbx_destroy(orbx_ctx* ctx);
+ORBX_API int orbx_set_stream(orbx_ctx* ctx, void* cuda_stream);
+ORBX_API void* orbx_get_stream(orbx_ctx* ctx);
+ORBX_API int orbx_sync(orbx_ctx* ctx);
+
+/* Orbor::init (orb.cpp:32-54) with setMaxNumPoints, setFastThresholdLUT,
+ * setUmax, setPattern, setGaussianKernel, setScaleSqSq (orbd.cu:45-441). */
+ORBX_API int orbx_default_params(orbx_params* p);
+ORBX_API int orbx_init(orbx_ctx* ctx, const orbx_params* p);
+
+/* Orbor::updateParam sizes (orb.cpp:145-191): writes
+ * [osizes|widths|heights|pitchs|offsets] (5n+1 ints) into oszp; returns n, or a
+ * negative ORBX_* status. */
+ORBX_API int orbx_layout(int w, int h, int noctaves, int* oszp, int cap);
+
+/* Orbor::detectAndCompute (orb.cpp:57-101) = hFastDectectWithNMS +
+ * hComputeAngle + hGassianBlur + hDescribe (orbd.cu:1564-1783), for one image.
+ * d_image: w x h bytes with row pitch `pitch` (the reference requires
+ * pitch == align_up(w, 128); other pitches are accepted, their padding reads as 0).
+ * d_points: max_pts entries; d_desc: max_pts * 32 bytes; d_num_pts: 1 int.
+ * Keypoints come out in raster order (y, then x); when more than max_pts survive,
+ * the first max_pts in that order are kept and *d_num_pts = max_pts.
+ * Asynchronous: *d_num_pts stays on the device. */
+ORBX_API int orbx_detect_and_compute(orbx_ctx* ctx, const uint8_t* d_image, int w, int h, int pitch,
+                                     orbx_point* d_points, uint8_t* d_desc, int* d_num_pts, int compute_desc);
+
+/* Orbor::match / hMatch / gHammingMatch (orb.cpp:104-113, orbd.cu:1471-1559,
+ * 1786-1793): for i < *d_n1 sets d_points1[i].match = index of the nearest
+ * descriptor in d_desc2 and .distance = its Hamming distance when that nearest
+ * is unique and closer than 64, else -1 / -1.  Counts are read on the device. */
+ORBX_API int orbx_match(orbx_ctx* ctx, orbx_point* d_points1, const int* d_n1, const uint8_t* d_desc1,
+                        const int* d_n2, const uint8_t* d_desc2, int n1_cap, int n2_cap, int mode);
+
+/* Brute-force k = 2 Hamming search (the gHammingMatch reduction, orbd.cu:1489-1542,
+ * exposed as a result): d_dist2[2i], d_dist2[2i+1] and d_idx2[...] are the two
+ * nearest database rows of query i ordered by (distance, index); missing entries
+ * are (0xFFFFFFFF, -1).  Sizes up to 4,194,303 database rows. */
+ORBX_API int orbx_match_knn2(orbx_ctx* ctx, const uint8_t* d_q, int nq, const uint8_t* d_db, int ndb,
+                             uint32_t* d_dist2, int32_t* d_idx2, int mode);
+
+/* A frame pair end to end: detect + describe A and B in shared launches, then
+ * match A -> B (Orbor::detectAndCompute x2 + Orbor::match, main.cpp:233-243).
+ * Replayed from a CUDA graph cached per (shape, pointers). */
+ORBX_API int orbx_pair(orbx_ctx* ctx, const uint8_t* d_img_a, const uint8_t* d_img_b, int w, int h, int pitch,
+                       orbx_point* d_pts_a, uint8_t* d_desc_a, int* d_n_a, orbx_point* d_pts_b,
+                       uint8_t* d_desc_b, int* d_n_b, int mode);
+
+/* Debug: copy the internal buffers of the last single-image call to the host:
+ * raw pyramid, blurred pyramid (offsets[n] bytes each, reference layout),
+ * score map and octave map (h * pitch0 each).  Synchronises the stream. */
+ORBX_API int orbx_debug_buffers(orbx_ctx* ctx, uint8_t* h_pyr, uint8_t* h_blur, float* h_vmap, int* h_layer,
+                                int* h_total);
+
+/* Host self-check of the float rounding of (double)pi - r used by the angle
+ * kernel (orbd.cu:995), over every float r with bits in [lo_bits, hi_bits).
+ * Returns the number of mismatches. */
+ORBX_API long long orbx_selftest_pi_minus(uint32_t lo_bits, uint32_t hi_bits);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* ORBX_H */
