@@ -1,0 +1,480 @@
+#!/usr/bin/env python
+"""Benchmark of the sm_100a ORB library on one 1920x1080 frame pair.
+
+A step is one frame pair: detect + describe both images and match A -> B
+(noctaves 8 -> 4 levels at 1080p, edge 31, FAST 20, Harris score, patch 31,
+WTA_K 2, at most 10000 keypoints per image), synthetic images from the seeded
+generator in cuda-orb_b200/synth.py.  The L2 cache is flushed (256 MiB write)
+before every timed step; each step is timed with CUDA events on the library's
+stream.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl orbx|reference]
+
+Prints one JSON line (rank 0).  Under torchrun every rank runs its own replica
+(there is no exchange between frame pairs) and the reported time is the max
+over ranks.  --impl reference runs the reference CUDA-ORB build
+(oracle/_ref/libref_orb.so, the reference's own orbd.cu/orb.cpp compiled for
+sm_100a) through its Orbor API on the same pair and GPU.
+"""
+import argparse
+import csv
+import io
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "cuda-orb_b200"))
+sys.path.insert(0, ROOT)
+
+METRIC = "ms/1080p pair detect+match; Hamming match-pairs/s exact vs learned @recall>=0.99"
+W, H = 1920, 1080
+MAX_PTS = 10000
+L2_FLUSH_BYTES = 256 << 20
+POPC_PER_CLK_PER_SM = 16  # 32-bit population count results per clock per SM
+SMS = 148
+
+# DRAM bytes per launch measured by ncu (dram__bytes_read.sum + dram__bytes_write.sum)
+# for the same workload; see profiles/pair1080_kernels.md.  None until captured.
+NCU_TRAFFIC = {}
+
+
+def parse_args(argv=None):
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=1000)
+    p.add_argument("--warmup", type=int, default=10)
+    p.add_argument("--impl", choices=["orbx", "reference"], default="orbx")
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-match-bench", action="store_true")
+    return p.parse_args(argv)
+
+
+# ---------------------------------------------------------------------------
+# distributed plumbing (replicas only)
+# ---------------------------------------------------------------------------
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+
+        backend = "nccl" if torch.cuda.is_available() else "gloo"
+        if backend == "nccl":
+            torch.cuda.set_device(local)
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=120))
+    return world, rank, local
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+
+
+def max_over_ranks(value, world):
+    """Max of a float over all ranks (the whole-job time)."""
+    if world <= 1:
+        return float(value)
+    import torch
+    import torch.distributed as dist
+
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([float(value)], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def sum_over_ranks(value, world):
+    if world <= 1:
+        return float(value)
+    import torch
+    import torch.distributed as dist
+
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([float(value)], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return float(t.item())
+
+
+# ---------------------------------------------------------------------------
+# clocks during the timed region
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index, interval_ms=50):
+        self.gpu = gpu_index
+        self.interval = interval_ms
+        self.proc = None
+        self.out = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 f"-lms={self.interval}"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except (OSError, ValueError):
+            self.proc = None
+        time.sleep(0.15)
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"], "samples": 0}
+        self.proc.terminate()
+        try:
+            out, _ = self.proc.communicate(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+            out, _ = self.proc.communicate()
+        rows = [r for r in csv.reader(io.StringIO(out)) if len(r) >= 9]
+        sm = []
+        smax = None
+        reasons = set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            try:
+                sm.append(float(r[1]))
+                smax = float(r[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, r[5:9]):
+                if v.strip().lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------
+# per-kernel algorithmic bytes / work for the pair (two frames)
+# ---------------------------------------------------------------------------
+def stage_work(oszp, n, na, nb):
+    h0 = int(oszp[2 * n])
+    p0 = int(oszp[3 * n])
+    obytes = int(oszp[5 * n])
+    npx = h0 * p0
+    nk = na + nb
+    return {
+        # input read once, raw and blurred pyramids written
+        "pyramid_blur": 2 * (npx + 2 * obytes),
+        # raw pyramid read, score + octave map written
+        "detect": 2 * (obytes + 8 * npx),
+        # score map read, keypoints written
+        "nms": 2 * 4 * npx + nk * 28,
+        # per keypoint: point, 31x31 disc, 512 samples, angle + 32-byte descriptor
+        "describe": nk * (28 + 961 + 512 + 4 + 32),
+    }
+
+
+def load_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            pk = json.load(f)
+        return pk, "measured"
+    except (OSError, ValueError):
+        return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "sm_max_mhz": 1965.0}, "fallback"
+
+
+# ---------------------------------------------------------------------------
+# CPU baselines
+# ---------------------------------------------------------------------------
+def cpu_baseline_port(a, b, budget_s=12.0, max_reps=20):
+    """The oracle (CPU restatement) on the same pair, on this host's cores."""
+    from oracle import oracle as O
+
+    times = []
+    t_end = time.time() + budget_s
+    while len(times) < max_reps and (not times or time.time() < t_end):
+        t0 = time.perf_counter()
+        ra = O.detect_and_compute(a, W, H, max_pts=MAX_PTS)
+        rb = O.detect_and_compute(b, W, H, max_pts=MAX_PTS)
+        O.match(ra["desc"], rb["desc"])
+        times.append(time.perf_counter() - t0)
+    return {"value": 1000.0 * statistics.median(times), "unit": "ms", "cores": O.threads(), "kind": "port",
+            "sample": f"{len(times)} runs of the full 1920x1080 pair (detect+describe A and B, match A->B) "
+                      f"by the oracle restatement, median"}
+
+
+def cpu_baseline_opencv(a, b, budget_s=8.0):
+    """OpenCV cv2.ORB + BFMatcher(NORM_HAMMING) knnMatch k=2 on the host (its own algorithm, for context)."""
+    try:
+        import cv2
+    except ImportError:
+        return {"unavailable": "cv2 not importable on this host"}
+    cores = len(os.sched_getaffinity(0))
+    cv2.setNumThreads(cores)
+    orb = cv2.ORB_create(nfeatures=MAX_PTS, scaleFactor=1.2, nlevels=8, edgeThreshold=31, patchSize=31,
+                         fastThreshold=20, WTA_K=2)
+    bf = cv2.BFMatcher(cv2.NORM_HAMMING)
+    ia, ib = np.ascontiguousarray(a[:, :W]), np.ascontiguousarray(b[:, :W])
+    times = []
+    t_end = time.time() + budget_s
+    nka = nkb = 0
+    while len(times) < 20 and (not times or time.time() < t_end):
+        t0 = time.perf_counter()
+        ka, da = orb.detectAndCompute(ia, None)
+        kb, db = orb.detectAndCompute(ib, None)
+        if da is not None and db is not None:
+            bf.knnMatch(da, db, k=2)
+        times.append(time.perf_counter() - t0)
+        nka, nkb = len(ka), len(kb)
+    return {"value": 1000.0 * statistics.median(times), "unit": "ms", "cores": cores,
+            "kind": "opencv", "keypoints": [nka, nkb],
+            "sample": f"{len(times)} runs, cv2 {cv2.__version__} ORB(10000, 1.2, 8 levels) + BFMatcher knn k=2"}
+
+
+# ---------------------------------------------------------------------------
+# the library arm
+# ---------------------------------------------------------------------------
+def run_orbx(args, world, rank, local):
+    import torch
+
+    import orbx
+    import synth
+
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    a, b, _ = synth.make_pair(W, H, seed=rank)
+    pitch = a.shape[1]
+    stream = torch.cuda.Stream(device=dev)
+    ctx = orbx.Context(local, orbx.make_params(noctaves=8, edge_threshold=31, wta_k=2, score_type=0, patch_size=31,
+                                               fast_threshold=20, max_pts=MAX_PTS), stream=stream)
+    da = torch.from_numpy(a).to(dev)
+    db = torch.from_numpy(b).to(dev)
+    A, B = orbx.FrameBuffers(MAX_PTS, dev), orbx.FrameBuffers(MAX_PTS, dev)
+    flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device=dev)
+
+    def step():
+        ctx.pair_ptr(da, db, W, H, pitch, A.points, A.desc, A.count, B.points, B.desc, B.count)
+
+    with torch.cuda.stream(stream):
+        for _ in range(max(args.warmup, 3)):
+            step()
+        stream.synchronize()
+        starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+        ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+        sampler = ClockSampler(local)
+        if rank == 0:
+            sampler.start()
+        barrier(world)
+        torch.cuda.synchronize(dev)
+        for k in range(args.steps):
+            flush.zero_()
+            starts[k].record(stream)
+            step()
+            ends[k].record(stream)
+        torch.cuda.synchronize(dev)
+        barrier(world)
+        clocks = sampler.stop() if rank == 0 else None
+        step_ms = [s.elapsed_time(e) for s, e in zip(starts, ends)]
+    local_total = sum(step_ms)
+    total_ms = max_over_ranks(local_total, world)
+    na, nb = int(A.count.item()), int(B.count.item())
+    matched = int((A.points[:na, 5] >= 0).sum().item())
+
+    # end to end through the host-buffer C ABI call, pinned host images
+    ha = torch.from_numpy(a).pin_memory()
+    hb = torch.from_numpy(b).pin_memory()
+    hpa = np.zeros((MAX_PTS, 7), dtype=np.int32)
+    hpb = np.zeros((MAX_PTS, 7), dtype=np.int32)
+    hna = np.zeros(1, dtype=np.int32)
+    hnb = np.zeros(1, dtype=np.int32)
+    e2e_steps = min(args.steps, 300)
+    with torch.cuda.stream(stream):
+        for _ in range(3):
+            ctx.pair_host(ha.data_ptr(), hb.data_ptr(), W, H, pitch, hpa, hna, hpb, hnb)
+        e_ms = []
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        barrier(world)
+        for _ in range(e2e_steps):
+            flush.zero_()
+            ev0.record(stream)
+            ctx.pair_host(ha.data_ptr(), hb.data_ptr(), W, H, pitch, hpa, hna, hpb, hnb)
+            ev1.record(stream)
+            ev1.synchronize()
+            e_ms.append(ev0.elapsed_time(ev1))
+        barrier(world)
+    e2e_total = max_over_ranks(sum(e_ms), world)
+    h2d = 2 * H * pitch
+    d2h = 8 + (int(hna[0]) + int(hnb[0])) * 28
+
+    # per-kernel times (events between the five launches, same inputs, L2 flushed)
+    prof_steps = min(args.steps, 100)
+    with torch.cuda.stream(stream):
+        acc = np.zeros(5)
+        for _ in range(prof_steps):
+            flush.zero_()
+            acc += ctx.profile_pair(da, db, W, H, pitch, A.points, A.desc, A.count, B.points, B.desc, B.count)
+    stage_ms = acc / prof_steps
+    names = ["pyramid_blur", "detect", "nms", "describe", "match"]
+    n, oszp = orbx.layout(W, H, 8)
+    work = stage_work(oszp, n, na, nb)
+    peaks, peak_kind = load_peaks()
+    kernels = {}
+    for i, nm in enumerate(names):
+        ent = {"ms": float(stage_ms[i])}
+        if nm in work:
+            ent["bytes"] = work[nm]
+            ent["gbs"] = work[nm] / (stage_ms[i] * 1e-3) / 1e9
+        else:
+            ent["popc_ops"] = na * nb * 8
+        kernels[nm] = ent
+    dom = max(names, key=lambda k: kernels[k]["ms"])
+    if dom == "match":
+        clock_mhz = (clocks or {}).get("sm_mhz") or peaks.get("sm_max_mhz", 1965.0)
+        peak_ops = SMS * POPC_PER_CLK_PER_SM * peaks.get("sm_max_mhz", 1965.0) * 1e6
+        ach = kernels["match"]["popc_ops"] / (stage_ms[4] * 1e-3)
+        roofline = {"kernel": "k_match_popc", "bound": "int", "achieved": ach / 1e12, "peak": peak_ops / 1e12,
+                    "unit": "Tpopc/s", "frac": ach / peak_ops, "traffic": NCU_TRAFFIC.get("k_match_popc"),
+                    "peak_kind": "derived: 148 SMs x 16 popc/clk x max SM clock", "clock_mhz": clock_mhz}
+    else:
+        kname = {"pyramid_blur": "k_pyramid_blur", "detect": "k_detect", "nms": "k_nms",
+                 "describe": "k_describe<2>"}[dom]
+        ach = kernels[dom]["gbs"]
+        roofline = {"kernel": kname, "bound": "hbm", "achieved": ach, "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                    "frac": ach / peaks["hbm_gbs"], "traffic": NCU_TRAFFIC.get(kname),
+                    "peak_kind": f"{peak_kind} hbm_gbs", "algorithmic_bytes": work[dom]}
+
+    match_bench = None
+    if not args.no_match_bench and rank == 0:
+        match_bench = bench_knn2(ctx, stream, dev, peaks)
+
+    result = None
+    if rank == 0:
+        steps_all = args.steps * world
+        value = total_ms / steps_all
+        result = {
+            "metric": METRIC, "value": value, "unit": "ms", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": False,
+            "scaling": "weak", "vs_baseline": None, "dtype": "u8",
+            "data": "synthetic (seeded blobs + polygons + noise, homography-warped partner; cuda-orb_b200/synth.py)",
+            "config": {"workload": "1920x1080 uint8 pair: detect+describe A and B, match A->B (XOR-popc)",
+                       "levels": n, "noctaves_requested": 8, "fast_threshold": 20, "edge": 31, "wta_k": 2,
+                       "max_pts": MAX_PTS, "keypoints": [na, nb], "matches": matched,
+                       "l2": "flushed (256 MiB write) before every timed step", "parallelism": "replicas",
+                       "graph": "one CUDA graph per pair (5 kernels)"},
+            "e2e": {"value": e2e_total / (e2e_steps * world), "unit": "ms", "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h,
+                    "how": "orbx_pair_host: pinned host images in, host keypoints/matches out, CUDA events"},
+            "gpu_launches": 5 * args.steps,
+            "roofline": roofline,
+            "kernels": kernels,
+            "clocks": clocks,
+        }
+        if match_bench:
+            result["match_65536"] = match_bench
+    ctx.close()
+    return result, (a, b)
+
+
+def bench_knn2(ctx, stream, dev, peaks):
+    """Matching only: 65536 queries x 65536 database rows, k = 2 (XOR-popc form)."""
+    import torch
+
+    import orbx
+    import synth
+
+    dbh, qh, _ = synth.match_workload(65536, 65536, seed=0)
+    q = torch.from_numpy(qh).to(dev)
+    db = torch.from_numpy(dbh).to(dev)
+    with torch.cuda.stream(stream):
+        dist, idx = orbx.knn2(ctx, q, db)
+        ctx.sync()
+        ms = []
+        for _ in range(5):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            orbx.knn2(ctx, q, db)
+            e1.record(stream)
+            e1.synchronize()
+            ms.append(e0.elapsed_time(e1))
+    t = statistics.median(ms)
+    pairs = 65536.0 * 65536.0
+    peak = SMS * POPC_PER_CLK_PER_SM * peaks.get("sm_max_mhz", 1965.0) * 1e6 / 8  # pairs/s at 8 popc per pair
+    return {"form": "xor-popc", "ms": t, "pairs_per_s": pairs / (t * 1e-3), "roofline_pairs_per_s": peak,
+            "frac": pairs / (t * 1e-3) / peak,
+            "peak_kind": "derived: 148 SMs x 16 popc/clk x max SM clock / 8 popc per pair"}
+
+
+# ---------------------------------------------------------------------------
+# the reference arm
+# ---------------------------------------------------------------------------
+def run_reference(args, world, rank, local):
+    if rank != 0:
+        return None
+    from oracle import refharness as R
+
+    if not R.available():
+        return {"impl": "reference", "unavailable": "reference build oracle/_ref/libref_orb.so not built"}
+    import torch
+
+    import synth
+
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    a, b, _ = synth.make_pair(W, H, seed=rank)
+    R.init(noctaves=8, edge=31, wta_k=2, score_type=0, patch=31, fast_thr=20, retain_topn=-1, max_pts=MAX_PTS)
+    R.time_pair(a, b, W, H, max(args.warmup, 3), 1)
+    flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device=dev)
+    steps = min(args.steps, 300)
+    ms = []
+    sampler = ClockSampler(local)
+    sampler.start()
+    for _ in range(steps):
+        flush.zero_()
+        torch.cuda.synchronize(dev)
+        t, na, nb = R.time_pair(a, b, W, H, 0, 1)
+        ms.append(t)
+    clocks = sampler.stop()
+    value = sum(ms) / len(ms)
+    return {
+        "metric": METRIC, "value": value, "unit": "ms", "n_gpus": 1, "steps": steps, "warmup": args.warmup,
+        "ms_per_step": value, "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "u8",
+        "impl": "reference",
+        "data": "synthetic (same generator and seed as the library arm)",
+        "config": {"workload": "1920x1080 uint8 pair: Orbor::detectAndCompute A and B, Orbor::match A->B",
+                   "max_pts": MAX_PTS, "keypoints": [na, nb], "l2": "flushed before every step"},
+        "e2e": {"value": value, "unit": "ms", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "cpu_baseline": {"value": value, "unit": "ms", "cores": 1, "kind": "reference",
+                         "sample": f"{steps} pairs through the reference CUDA build (its orbd.cu/orb.cpp compiled "
+                                   f"for sm_100a, oracle/_ref) on cuda:{local}; the reference has no CPU "
+                                   f"implementation of the path, so its own GPU build is the arm"},
+        "clocks": clocks,
+    }
+
+
+def main(argv=None):
+    args = parse_args(argv)
+    world, rank, local = dist_setup()
+    if args.impl == "reference":
+        res = run_reference(args, world, rank, local)
+    else:
+        res, imgs = run_orbx(args, world, rank, local)
+        if rank == 0 and not args.no_cpu_baseline:
+            res["cpu_baseline"] = cpu_baseline_port(*imgs)
+            res["cpu_opencv"] = cpu_baseline_opencv(*imgs)
+    if rank == 0 and res is not None:
+        print(json.dumps(res), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

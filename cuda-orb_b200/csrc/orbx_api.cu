@@ -79,6 +79,15 @@ struct orbx_ctx {
   BatchSlot single, pair;
   MatchWork mw{};  // for orbx_match / orbx_match_knn2
   PairGraph pg;
+  // orbx_pair_host device buffers
+  uint8_t* io_img[2] = {nullptr, nullptr};
+  size_t io_img_bytes = 0;
+  orbx_point* io_pts[2] = {nullptr, nullptr};
+  uint8_t* io_desc[2] = {nullptr, nullptr};
+  int* io_count = nullptr;  // [2]
+  int* io_count_host = nullptr;  // pinned [2]
+  int io_max_pts = 0;
+  cudaEvent_t prof_ev[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
 };
 
 #define ORBX_CUDA(x)                   \
@@ -589,6 +598,15 @@ ORBX_API int orbx_destroy(orbx_ctx* c) {
   cudaFree(c->pg.mw.tile_done);
   cudaFree(c->mw.part);
   cudaFree(c->mw.tile_done);
+  for (int i = 0; i < 2; i++) {
+    cudaFree(c->io_img[i]);
+    cudaFree(c->io_pts[i]);
+    cudaFree(c->io_desc[i]);
+  }
+  cudaFree(c->io_count);
+  cudaFreeHost(c->io_count_host);
+  for (auto& e : c->prof_ev)
+    if (e) cudaEventDestroy(e);
   cudaFree(c->d_pattern);
   cudaFree(c->d_umax);
   cudaFree(c->d_err);
@@ -801,6 +819,100 @@ ORBX_API int orbx_pair(orbx_ctx* c, const uint8_t* d_img_a, const uint8_t* d_img
     pg.valid = true;
   }
   ORBX_CUDA(cudaGraphLaunch(pg.exec, c->stream));
+  return ORBX_OK;
+}
+
+ORBX_API int orbx_pair_host(orbx_ctx* c, const uint8_t* h_img_a, const uint8_t* h_img_b, int w, int h, int pitch,
+                            orbx_point* h_pts_a, int* h_n_a, orbx_point* h_pts_b, int* h_n_b, uint8_t* h_desc_a,
+                            uint8_t* h_desc_b, int mode) {
+  int rc = check_image(c, h_img_a, w, h, pitch);
+  if (rc) return rc;
+  if (!h_img_b || !h_pts_a || !h_n_a || !h_pts_b || !h_n_b) return ORBX_ERR_ARG;
+  DeviceGuard g(c->device);
+  const size_t ibytes = (size_t)h * pitch;
+  if (c->io_img_bytes < ibytes) {
+    for (auto& p : c->io_img) {
+      cudaFree(p);
+      p = nullptr;
+    }
+    c->io_img_bytes = 0;
+    for (auto& p : c->io_img) ORBX_CUDA(cudaMalloc(&p, ibytes));
+    c->io_img_bytes = ibytes;
+  }
+  if (c->io_max_pts < c->p.max_pts) {
+    for (int i = 0; i < 2; i++) {
+      cudaFree(c->io_pts[i]);
+      cudaFree(c->io_desc[i]);
+      c->io_pts[i] = nullptr;
+      c->io_desc[i] = nullptr;
+    }
+    c->io_max_pts = 0;
+    for (int i = 0; i < 2; i++) {
+      ORBX_CUDA(cudaMalloc(&c->io_pts[i], sizeof(orbx_point) * (size_t)c->p.max_pts));
+      ORBX_CUDA(cudaMalloc(&c->io_desc[i], (size_t)32 * c->p.max_pts));
+    }
+    if (!c->io_count) ORBX_CUDA(cudaMalloc(&c->io_count, 2 * sizeof(int)));
+    if (!c->io_count_host) ORBX_CUDA(cudaMallocHost(&c->io_count_host, 2 * sizeof(int)));
+    c->io_max_pts = c->p.max_pts;
+  }
+  ORBX_CUDA(cudaMemcpyAsync(c->io_img[0], h_img_a, ibytes, cudaMemcpyHostToDevice, c->stream));
+  ORBX_CUDA(cudaMemcpyAsync(c->io_img[1], h_img_b, ibytes, cudaMemcpyHostToDevice, c->stream));
+  rc = orbx_pair(c, c->io_img[0], c->io_img[1], w, h, pitch, c->io_pts[0], c->io_desc[0], c->io_count,
+                 c->io_pts[1], c->io_desc[1], c->io_count + 1, mode);
+  if (rc) return rc;
+  ORBX_CUDA(cudaMemcpyAsync(c->io_count_host, c->io_count, 2 * sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+  ORBX_CUDA(cudaStreamSynchronize(c->stream));
+  const int na = c->io_count_host[0], nb = c->io_count_host[1];
+  *h_n_a = na;
+  *h_n_b = nb;
+  if (na > 0) ORBX_CUDA(cudaMemcpyAsync(h_pts_a, c->io_pts[0], sizeof(orbx_point) * na, cudaMemcpyDeviceToHost, c->stream));
+  if (nb > 0) ORBX_CUDA(cudaMemcpyAsync(h_pts_b, c->io_pts[1], sizeof(orbx_point) * nb, cudaMemcpyDeviceToHost, c->stream));
+  if (h_desc_a && na > 0) ORBX_CUDA(cudaMemcpyAsync(h_desc_a, c->io_desc[0], (size_t)32 * na, cudaMemcpyDeviceToHost, c->stream));
+  if (h_desc_b && nb > 0) ORBX_CUDA(cudaMemcpyAsync(h_desc_b, c->io_desc[1], (size_t)32 * nb, cudaMemcpyDeviceToHost, c->stream));
+  ORBX_CUDA(cudaStreamSynchronize(c->stream));
+  return ORBX_OK;
+}
+
+ORBX_API int orbx_profile_pair(orbx_ctx* c, const uint8_t* d_img_a, const uint8_t* d_img_b, int w, int h, int pitch,
+                               orbx_point* d_pts_a, uint8_t* d_desc_a, int* d_n_a, orbx_point* d_pts_b,
+                               uint8_t* d_desc_b, int* d_n_b, int mode, float* stage_ms) {
+  int rc = check_image(c, d_img_a, w, h, pitch);
+  if (rc) return rc;
+  if (!d_img_b || !d_pts_a || !d_desc_a || !d_n_a || !d_pts_b || !d_desc_b || !d_n_b || !stage_ms)
+    return ORBX_ERR_ARG;
+  if (mode != ORBX_MATCH_POPC && mode != ORBX_MATCH_AUTO) return ORBX_ERR_ARG;
+  DeviceGuard g(c->device);
+  if ((rc = ws_ensure(c, c->ws[0], w, h)) != 0) return rc;
+  if ((rc = ws_ensure(c, c->ws[1], w, h)) != 0) return rc;
+  std::vector<Frame> frames(2);
+  fill_frame(c, c->ws[0], d_img_a, pitch, d_pts_a, d_desc_a, d_n_a, frames[0]);
+  fill_frame(c, c->ws[1], d_img_b, pitch, d_pts_b, d_desc_b, d_n_b, frames[1]);
+  LaunchPlan pl;
+  if ((rc = upload_batch(c, c->pair, frames, &pl)) != 0) return rc;
+  if ((rc = mw_ensure(c->mw, c->p.max_pts)) != 0) return rc;
+  for (auto& e : c->prof_ev)
+    if (!e) ORBX_CUDA(cudaEventCreate(&e));
+  MatchArgs a{};
+  a.q = d_desc_a;
+  a.db = d_desc_b;
+  a.nq = c->p.max_pts;
+  a.ndb = c->p.max_pts;
+  a.d_nq = d_n_a;
+  a.d_ndb = d_n_b;
+  a.pts = d_pts_a;
+  ORBX_CUDA(cudaEventRecord(c->prof_ev[0], c->stream));
+  ORBX_CUDA(launch_pyramid_blur(pl.b, pl.pyr_tiles, c->stream));
+  ORBX_CUDA(cudaEventRecord(c->prof_ev[1], c->stream));
+  ORBX_CUDA(launch_detect(pl.b, pl.det_tiles, c->stream));
+  ORBX_CUDA(cudaEventRecord(c->prof_ev[2], c->stream));
+  ORBX_CUDA(launch_nms(pl.b, pl.nms_strips, c->stream));
+  ORBX_CUDA(cudaEventRecord(c->prof_ev[3], c->stream));
+  ORBX_CUDA(launch_describe(pl.b, pl.total_max_pts, c->stream));
+  ORBX_CUDA(cudaEventRecord(c->prof_ev[4], c->stream));
+  ORBX_CUDA(launch_match_popc(a, c->mw, c->stream));
+  ORBX_CUDA(cudaEventRecord(c->prof_ev[5], c->stream));
+  ORBX_CUDA(cudaEventSynchronize(c->prof_ev[5]));
+  for (int i = 0; i < 5; i++) ORBX_CUDA(cudaEventElapsedTime(&stage_ms[i], c->prof_ev[i], c->prof_ev[i + 1]));
   return ORBX_OK;
 }
 

@@ -22,12 +22,12 @@ namespace orbx {
 // the octaves are read from an existing pyramid instead (hGassianBlur on a
 // caller's buffer, orbd.cu:1732-1773).
 // ---------------------------------------------------------------------------
-constexpr int kPyrSW = kPyrTW + 6;
+constexpr int kPyrSW = kPyrTW + 8;  // 3-pixel halo each side, padded to a multiple of 4
 constexpr int kPyrSH = kPyrTH + 6;
 
 __global__ void __launch_bounds__(256) k_pyramid_blur(Batch b) {
-  __shared__ uint8_t s_src[kPyrSH * kPyrSW];
-  __shared__ float s_row[kPyrSH * kPyrTW];
+  __shared__ __align__(16) uint8_t s_src[kPyrSH * kPyrSW];
+  __shared__ __align__(16) float s_row[kPyrSH * kPyrTW];
 
   const int t = blockIdx.x;
   const int f = find_frame(b.pyr_base, b.n_frames, t);
@@ -53,53 +53,84 @@ __global__ void __launch_bounds__(256) k_pyramid_blur(Batch b) {
   }
   if (t == 0 && threadIdx.x == 0) *b.nms_ticket = 0u;
 
+  // stage: source rows y0-3 .. y0+34, columns x0-3 .. x0+132, reflect-101 at the octave edges
   const uint8_t* __restrict__ psrc = F.pyr_src ? F.pyr_src + F.ooff[o] : nullptr;
-  for (int i = threadIdx.x; i < kPyrSH * kPyrSW; i += blockDim.x) {
-    const int r = i / kPyrSW;
-    const int c = i - r * kPyrSW;
+  constexpr int kGroups = kPyrSW / 4;
+  for (int it = threadIdx.x; it < kPyrSH * kGroups; it += blockDim.x) {
+    const int r = it / kGroups;
+    const int g = it - r * kGroups;
     const int y = reflect101(y0 - 3 + r, oh);
-    const int x = reflect101(x0 - 3 + c, ow);
-    s_src[i] = psrc ? __ldg(psrc + (size_t)y * op + x) : __ldg(img + (size_t)(y << o) * pitch_in + (x << o));
+    const uint8_t* rowp = psrc ? psrc + (size_t)y * op : img + (size_t)(y << o) * pitch_in;
+    const int sh = psrc ? 0 : o;
+    uint32_t word = 0;
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+      const int x = reflect101(x0 - 3 + 4 * g + j, ow);
+      word |= (uint32_t)__ldg(rowp + (x << sh)) << (8 * j);
+    }
+    reinterpret_cast<uint32_t*>(s_src)[it] = word;
   }
   __syncthreads();
 
   const float* k = b.gauss;
-  for (int i = threadIdx.x; i < kPyrSH * kPyrTW; i += blockDim.x) {
-    const int r = i / kPyrTW;
-    const int c = i - r * kPyrTW;
-    const uint8_t* s = s_src + r * kPyrSW + c + 3;
-    const float t0 = (float)(int)s[0];
-    const float t1 = (float)((int)s[-1] + (int)s[1]);
-    const float t2 = (float)((int)s[-2] + (int)s[2]);
-    const float t3 = (float)((int)s[-3] + (int)s[3]);
-    s_row[i] = gauss_dot4(k, t0, t1, t2, t3);
+  // horizontal pass: 4 consecutive outputs per thread from 12 staged bytes
+  for (int it = threadIdx.x; it < kPyrSH * (kPyrTW / 4); it += blockDim.x) {
+    const int r = it / (kPyrTW / 4);
+    const int g = it - r * (kPyrTW / 4);
+    const uint32_t* w = reinterpret_cast<const uint32_t*>(s_src + r * kPyrSW) + g;
+    const uint32_t w0 = w[0], w1 = w[1], w2 = w[2];
+    int p[12];
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+      p[j] = (w0 >> (8 * j)) & 0xFF;
+      p[4 + j] = (w1 >> (8 * j)) & 0xFF;
+      p[8 + j] = (w2 >> (8 * j)) & 0xFF;
+    }
+    float4 out;
+    float* op4 = &out.x;
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+      const float t0 = (float)p[j + 3];
+      const float t1 = (float)(p[j + 2] + p[j + 4]);
+      const float t2 = (float)(p[j + 1] + p[j + 5]);
+      const float t3 = (float)(p[j] + p[j + 6]);
+      op4[j] = gauss_dot4(k, t0, t1, t2, t3);
+    }
+    reinterpret_cast<float4*>(s_row + r * kPyrTW)[g] = out;
   }
   __syncthreads();
 
+  // vertical pass: 4 consecutive rows of one column per thread (10-row window)
   uint8_t* P = F.pyr + F.ooff[o];
   uint8_t* B = F.blr + F.ooff[o];
   const bool copy_pad = (o == 0) && (pitch_in == op);
-  for (int i = threadIdx.x; i < kPyrTH * kPyrTW; i += blockDim.x) {
-    const int r = i / kPyrTW;
-    const int c = i - r * kPyrTW;
-    const int y = y0 + r;
+  for (int it = threadIdx.x; it < (kPyrTH / 4) * kPyrTW; it += blockDim.x) {
+    const int rg = it / kPyrTW;
+    const int c = it - rg * kPyrTW;
     const int x = x0 + c;
-    if (y >= oh || x >= op) continue;
-    const size_t a = (size_t)y * op + x;
-    if (x < ow) {
-      const float* col = s_row + (r + 3) * kPyrTW + c;
-      const float t0 = col[0];
-      const float t1 = __fadd_rn(col[-kPyrTW], col[kPyrTW]);
-      const float t2 = __fadd_rn(col[-2 * kPyrTW], col[2 * kPyrTW]);
-      const float t3 = __fadd_rn(col[-3 * kPyrTW], col[3 * kPyrTW]);
-      B[a] = (uint8_t)__float2int_rn(gauss_dot4(k, t0, t1, t2, t3));
-      P[a] = s_src[(r + 3) * kPyrSW + c + 3];
-    } else {
-      // Row padding: octave 0 carries the caller's padding bytes (the reference
-      // copies h * pitch0 bytes, orbd.cu:1584); other octaves hold zeros.
-      const uint8_t v = psrc ? __ldg(psrc + a) : (copy_pad ? __ldg(img + (size_t)y * pitch_in + x) : (uint8_t)0);
-      P[a] = v;
-      B[a] = v;
+    if (x >= op) continue;
+    float hcol[10];
+#pragma unroll
+    for (int j = 0; j < 10; j++) hcol[j] = s_row[(4 * rg + j) * kPyrTW + c];
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+      const int y = y0 + 4 * rg + j;
+      if (y >= oh) break;
+      const size_t a = (size_t)y * op + x;
+      if (x < ow) {
+        const float t0 = hcol[j + 3];
+        const float t1 = __fadd_rn(hcol[j + 2], hcol[j + 4]);
+        const float t2 = __fadd_rn(hcol[j + 1], hcol[j + 5]);
+        const float t3 = __fadd_rn(hcol[j], hcol[j + 6]);
+        B[a] = (uint8_t)__float2int_rn(gauss_dot4(k, t0, t1, t2, t3));
+        P[a] = s_src[(4 * rg + j + 3) * kPyrSW + c + 3];
+      } else {
+        // Row padding: octave 0 carries the caller's padding bytes (the reference
+        // copies h * pitch0 bytes, orbd.cu:1584); other octaves hold zeros.
+        const uint8_t v = psrc ? __ldg(psrc + a) : (copy_pad ? __ldg(img + (size_t)y * pitch_in + x) : (uint8_t)0);
+        P[a] = v;
+        B[a] = v;
+      }
     }
   }
 }
@@ -146,7 +177,7 @@ __device__ __forceinline__ bool has_arc9(uint32_t m16) {
 // (dxx*dyy - dxy*dxy - HARRIS_K*(dsxy*dsxy)) * d_scale_sq_sq.
 __device__ __forceinline__ float harris_score(const uint8_t* c, int sw, float scale4) {
   int dxx = 0, dyy = 0, dxy = 0;
-#pragma unroll
+#pragma unroll 1
   for (int i = -3; i <= 3; i++) {
 #pragma unroll
     for (int j = -3; j <= 3; j++) {
@@ -200,10 +231,30 @@ __device__ __forceinline__ float fast_score(const int* d, int threshold) {
   return (float)(-b0 - 1);
 }
 
-__global__ void __launch_bounds__(256) k_detect(Batch b) {
-  __shared__ uint8_t s_stage[det_stage_bytes()];
+// FAST-9 segment test on a shared-memory tile of row stride sw.  The first
+// check is the reference's pre-test on ring pixels 0 and 8 (orbd.cu:700-702):
+// every run of 9 contains one of them, so most pixels stop there.
+__device__ __forceinline__ bool fast9(const uint8_t* c, int sw, int thr) {
+  const int v = c[0];
+  const int lo = v - thr, hi = v + thr;
+  const int p0 = c[3 * sw], p8 = c[-3 * sw];
+  if (!(p0 < lo || p0 > hi || p8 < lo || p8 > hi)) return false;
+  uint32_t dark = 0, bright = 0;
+#pragma unroll
+  for (int k = 0; k < 16; k++) {
+    const int p = c[c_ring[k][1] * sw + c_ring[k][0]];
+    dark |= (uint32_t)(p < lo) << k;
+    bright |= (uint32_t)(p > hi) << k;
+  }
+  return has_arc9(dark) || has_arc9(bright);
+}
+
+__global__ void __launch_bounds__(256, 4) k_detect(Batch b) {
+  __shared__ __align__(16) uint8_t s_stage[det_stage_bytes()];
   __shared__ float s_map[kDetTH * kDetTW];
-  __shared__ int s_oct[kDetTH * kDetTW];
+  __shared__ int8_t s_oct[kDetTH * kDetTW];
+  __shared__ int16_t s_cand[kDetTH * kDetTW];
+  __shared__ int s_ncand;
 
   const int t = blockIdx.x;
   const int f = find_frame(b.det_base, b.n_frames, t);
@@ -213,22 +264,27 @@ __global__ void __launch_bounds__(256) k_detect(Batch b) {
   const int Y0 = (lt / F.det_tiles_x) * kDetTH;
   const int n_oct = F.n_oct;
   const uint8_t* __restrict__ pyr = F.pyr;
+  const int lane = threadIdx.x & 31;
 
   for (int i = threadIdx.x; i < kDetTH * kDetTW; i += blockDim.x) {
     s_map[i] = 0.f;
     s_oct[i] = 0;
   }
-  // Stage every octave's tile with its halo (linear pyramid addressing).
+  // Stage every octave's tile with its halo, 4 bytes per load: octave offsets
+  // and pitches are multiples of 128 and (X0 >> o) - 4 is a multiple of 4.
   {
     int off = 0;
     for (int o = 0; o < n_oct; o++) {
       const int sw = (kDetTW >> o) + 2 * kHalo;
       const int sh = (kDetTH >> o) + 2 * kHalo;
-      const long long base = F.ooff[o] + (long long)((Y0 >> o) - kHalo) * F.op[o] + ((X0 >> o) - kHalo);
-      for (int i = threadIdx.x; i < sw * sh; i += blockDim.x) {
-        const int r = i / sw;
-        const int c = i - r * sw;
-        s_stage[off + i] = __ldg(pyr + base + (long long)r * F.op[o] + c);
+      const int sw4 = sw >> 2;
+      const int op = F.op[o];
+      const long long base = F.ooff[o] + (long long)((Y0 >> o) - kHalo) * op + ((X0 >> o) - kHalo);
+      uint32_t* dst = reinterpret_cast<uint32_t*>(s_stage + off);
+      for (int i = threadIdx.x; i < sw4 * sh; i += blockDim.x) {
+        const int r = i / sw4;
+        const int c4 = i - r * sw4;
+        dst[i] = __ldg(reinterpret_cast<const uint32_t*>(pyr + base + (long long)r * op) + c4);
       }
       off += sw * sh;
     }
@@ -243,36 +299,50 @@ __global__ void __launch_bounds__(256) k_detect(Batch b) {
     const int sw = tw + 2 * kHalo;
     const int ow = F.ow[o], oh = F.oh[o];
     const int xb = X0 >> o, yb = Y0 >> o;
-    for (int i = threadIdx.x; i < tw * th; i += blockDim.x) {
+    const uint8_t* stage = s_stage + off;
+    if (threadIdx.x == 0) s_ncand = 0;
+    __syncthreads();
+    // phase A: segment test, corners appended to a shared list
+    for (int i0 = 0; i0 < tw * th; i0 += blockDim.x) {
+      const int i = i0 + threadIdx.x;
+      bool corner = false;
+      if (i < tw * th) {
+        const int ly = i / tw;
+        const int lx = i - ly * tw;
+        const int x = xb + lx, y = yb + ly;
+        if (x >= 3 && x < ow - 3 && y >= 3 && y < oh - 3)
+          corner = fast9(stage + (ly + kHalo) * sw + (lx + kHalo), sw, thr);
+      }
+      const uint32_t m = __ballot_sync(0xffffffffu, corner);
+      if (m) {
+        int wbase = 0;
+        if (lane == 0) wbase = atomicAdd(&s_ncand, __popc(m));
+        wbase = __shfl_sync(0xffffffffu, wbase, 0);
+        if (corner) s_cand[wbase + __popc(m & ((1u << lane) - 1u))] = (int16_t)i;
+      }
+    }
+    __syncthreads();
+    // phase B: score every corner (each position once, so list order is irrelevant)
+    const int nc = s_ncand;
+    for (int j = threadIdx.x; j < nc; j += blockDim.x) {
+      const int i = s_cand[j];
       const int ly = i / tw;
       const int lx = i - ly * tw;
-      const int x = xb + lx, y = yb + ly;
-      if (x < 3 || x >= ow - 3 || y < 3 || y >= oh - 3) continue;
-      const uint8_t* c = s_stage + off + (ly + kHalo) * sw + (lx + kHalo);
-      const int v = c[0];
-      uint32_t dark = 0, bright = 0;
-      int ring[16];
-#pragma unroll
-      for (int k = 0; k < 16; k++) {
-        const int p = c[c_ring[k][1] * sw + c_ring[k][0]];
-        ring[k] = p;
-        dark |= (uint32_t)(p < v - thr) << k;
-        bright |= (uint32_t)(p > v + thr) << k;
-      }
-      if (!has_arc9(dark) && !has_arc9(bright)) continue;
+      const uint8_t* c = stage + (ly + kHalo) * sw + (lx + kHalo);
       float score;
       if (b.harris) {
         score = harris_score(c, sw, b.harris_scale4);
       } else {
+        const int v = c[0];
         int d[25];
 #pragma unroll
-        for (int k = 0; k < 25; k++) d[k] = (int)(short)(v - ring[k & 15]);
+        for (int k = 0; k < 25; k++) d[k] = (int)(short)(v - c[c_ring[k & 15][1] * sw + c_ring[k & 15][0]]);
         score = fast_score(d, thr);
       }
-      const int m = (ly << o) * kDetTW + (lx << o);
-      if (s_map[m] < score) {
-        s_map[m] = score;
-        s_oct[m] = o;
+      const int mpos = (ly << o) * kDetTW + (lx << o);
+      if (s_map[mpos] < score) {
+        s_map[mpos] = score;
+        s_oct[mpos] = (int8_t)o;
       }
     }
     off += sw * ((kDetTH >> o) + 2 * kHalo);
@@ -309,27 +379,42 @@ constexpr unsigned long long kFlagAgg = 1ull << 32;
 constexpr unsigned long long kFlagPre = 2ull << 32;
 constexpr int kLookbackSpinLimit = 1 << 22;
 
-// Neighbours are addressed linearly like the reference (a column past the
-// edge is the adjacent row's entry); positions outside the map, reachable only
-// with an edge threshold below the window radius 2^o, read as 0.
-__device__ __forceinline__ bool nms_survives(const float* __restrict__ vmap, const int* __restrict__ layer, size_t idx,
-                                             int p0, long long npx, float* v_out, int* o_out) {
-  const float v = vmap[idx];
-  if (!(v > 0.f)) return false;
-  const int o = layer[idx];
-  const int r = 1 << o;
-  for (int dy = -r; dy <= r; dy++) {
-    const long long rowi = (long long)idx + (long long)dy * p0;
-    for (int dx = -r; dx <= r; dx++) {
-      if (dx == 0 && dy == 0) continue;
-      const long long li = rowi + dx;
-      const float u = (li >= 0 && li < npx) ? vmap[li] : 0.f;
-      if (u > 0.f && (u > v || (u == v && dx <= 0 && dy <= 0))) return false;
+// Neighbour rule (gNmsUnroll4, orbd.cu:938-956): positions are addressed
+// linearly like the reference (a column past the edge is the adjacent row's
+// entry); positions outside the map, reachable only with an edge threshold
+// below the window radius 2^o, read as 0.
+
+// Warp 0 of a strip's block resolves the strip's exclusive prefix: it reads the
+// look-back words of up to 32 predecessors per round with acquire loads, and
+// stops at the nearest one that already carries an inclusive prefix.
+__device__ __forceinline__ int nms_lookback(unsigned long long* st, int s, int lane, int* err) {
+  int excl = 0;
+  int j = s - 1;
+  int spins = 0;
+  while (j >= 0) {
+    const int idx = j - lane;
+    const unsigned long long wv = (idx >= 0) ? ld_acquire_u64(&st[idx]) : kFlagPre;
+    const unsigned long long flag = wv & (3ull << 32);
+    const unsigned pre = __ballot_sync(0xffffffffu, flag == kFlagPre);
+    const unsigned notready = __ballot_sync(0xffffffffu, flag == 0ull);
+    const int first_pre = pre ? (__ffs(pre) - 1) : 32;
+    const unsigned need = (first_pre >= 31) ? 0xffffffffu : ((2u << first_pre) - 1u);
+    if (notready & need) {
+      if (++spins > kLookbackSpinLimit) {
+        if (lane == 0) atomicOr(err, kErrLookbackTimeout);
+        break;
+      }
+      __nanosleep(20);
+      continue;
     }
+    int v = ((need >> lane) & 1u) ? (int)(unsigned)wv : 0;
+#pragma unroll
+    for (int d = 16; d >= 1; d >>= 1) v += __shfl_xor_sync(0xffffffffu, v, d);
+    excl += v;
+    if (first_pre < 32) break;
+    j -= 32;
   }
-  *v_out = v;
-  *o_out = o;
-  return true;
+  return excl;
 }
 
 __global__ void __launch_bounds__(256) k_nms(Batch b) {
@@ -351,28 +436,71 @@ __global__ void __launch_bounds__(256) k_nms(Batch b) {
   const int npx = (row1 - row0) * ncols;
   const int nchunks = (npx + 255) >> 8;
   const int p0 = F.op[0];
+  const long long npx_map = (long long)F.h * p0;
+  const float* __restrict__ vmap = F.vmap;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 
-  // pass 1: survivor masks in raster order
-  for (int k = 0; k < nchunks; k++) {
-    const int p = (k << 8) + threadIdx.x;
-    bool sur = false;
-    if (p < npx) {
-      const int y = row0 + p / ncols;
-      const int x = border + p % ncols;
-      float v;
-      int o;
-      sur = nms_survives(F.vmap, F.layer, (size_t)y * p0 + x, p0, (long long)F.h * p0, &v, &o);
+  // pass 1: survivor masks in raster order.  Four chunks' centre scores are
+  // loaded together; each centre with a score is then checked by the whole warp,
+  // 32 window positions per round, so even the 33x33 window of an octave-4
+  // keypoint costs a few dependent loads.
+  for (int k0 = 0; k0 < nchunks; k0 += 4) {
+    float v[4];
+    long long idx[4];
+#pragma unroll
+    for (int u = 0; u < 4; u++) {
+      const int p = ((k0 + u) << 8) + threadIdx.x;
+      v[u] = 0.f;
+      idx[u] = 0;
+      if (k0 + u < nchunks && p < npx) {
+        const int y = row0 + p / ncols;
+        const int x = border + p % ncols;
+        idx[u] = (long long)y * p0 + x;
+        v[u] = __ldg(vmap + idx[u]);
+      }
     }
-    const uint32_t m = __ballot_sync(0xffffffffu, sur);
-    if (lane == 0) s_mask[k * 8 + warp] = m;
+#pragma unroll
+    for (int u = 0; u < 4; u++) {
+      if (k0 + u >= nchunks) break;
+      uint32_t cand = __ballot_sync(0xffffffffu, v[u] > 0.f);
+      uint32_t sur = 0;
+      while (cand) {
+        const int l = __ffs(cand) - 1;
+        cand &= cand - 1u;
+        const long long cidx = __shfl_sync(0xffffffffu, idx[u], l);
+        const float cv = __shfl_sync(0xffffffffu, v[u], l);
+        const int r = 1 << __ldg(F.layer + cidx);
+        const int side = 2 * r + 1;
+        const int npos = side * side;
+        bool sup = false;
+        for (int q0 = 0; q0 < npos; q0 += 32) {
+          const int q = q0 + lane;
+          bool s_ = false;
+          if (q < npos) {
+            const int dy = q / side - r;
+            const int dx = q - (q / side) * side - r;
+            if (dx != 0 || dy != 0) {
+              const long long li = cidx + (long long)dy * p0 + dx;
+              const float uu = (li >= 0 && li < npx_map) ? __ldg(vmap + li) : 0.f;
+              s_ = uu > 0.f && (uu > cv || (uu == cv && dx <= 0 && dy <= 0));
+            }
+          }
+          if (__any_sync(0xffffffffu, s_)) {
+            sup = true;
+            break;
+          }
+        }
+        if (!sup) sur |= 1u << l;
+      }
+      if (lane == 0) s_mask[(k0 + u) * 8 + warp] = sur;
+    }
   }
   __syncthreads();
 
   // exclusive scan of the mask popcounts, in (chunk, warp) order
   const int nent = nchunks * 8;
   const int per = (nent + 255) >> 8;
-  const int beg = min(threadIdx.x * per, nent), end = min(beg + per, nent);
+  const int beg = min((int)threadIdx.x * per, nent), end = min(beg + per, nent);
   int local = 0;
   for (int i = beg; i < end; i++) local += __popc(s_mask[i]);
   int incl = local;
@@ -393,41 +521,25 @@ __global__ void __launch_bounds__(256) k_nms(Batch b) {
   int strip_total = 0;
   for (int w2 = 0; w2 < 8; w2++) strip_total += s_warp_tot[w2];
 
-  // decoupled look-back over the frame's strips
-  if (threadIdx.x == 0) {
+  // decoupled look-back over the frame's strips (warp 0)
+  if (warp == 0) {
     unsigned long long* st = F.nms_status;
     int excl = 0;
     if (s == 0) {
-      st_release_u64(&st[0], kFlagPre | (unsigned)strip_total);
+      if (lane == 0) st_release_u64(&st[0], kFlagPre | (unsigned)strip_total);
     } else {
-      st_release_u64(&st[s], kFlagAgg | (unsigned)strip_total);
-      int j = s - 1;
-      int spins = 0;
-      while (j >= 0) {
-        const unsigned long long wv = ld_acquire_u64(&st[j]);
-        const unsigned long long flag = wv & (3ull << 32);
-        if (flag == kFlagPre) {
-          excl += (int)(unsigned)wv;
-          break;
-        }
-        if (flag == kFlagAgg) {
-          excl += (int)(unsigned)wv;
-          j--;
-          continue;
-        }
-        if (++spins > kLookbackSpinLimit) {
-          atomicOr(b.err, kErrLookbackTimeout);
-          break;
-        }
-        __nanosleep(32);
-      }
-      st_release_u64(&st[s], kFlagPre | (unsigned)(excl + strip_total));
+      if (lane == 0) st_release_u64(&st[s], kFlagAgg | (unsigned)strip_total);
+      __syncwarp();
+      excl = nms_lookback(st, s, lane, b.err);
+      if (lane == 0) st_release_u64(&st[s], kFlagPre | (unsigned)(excl + strip_total));
     }
-    s_base = excl;
-    if (s == F.nms_strips - 1) {
-      const int tot = excl + strip_total;
-      *F.count = min(tot, F.max_pts);
-      if (F.total) *F.total = tot;
+    if (lane == 0) {
+      s_base = excl;
+      if (s == F.nms_strips - 1) {
+        const int tot = excl + strip_total;
+        *F.count = min(tot, F.max_pts);
+        if (F.total) *F.total = tot;
+      }
     }
   }
   __syncthreads();
@@ -448,7 +560,7 @@ __global__ void __launch_bounds__(256) k_nms(Batch b) {
     q.x = x;
     q.y = y;
     q.octave = F.layer[idx];
-    q.score = F.vmap[idx];
+    q.score = vmap[idx];
     q.angle = 0.f;
     q.match = 0;
     q.distance = 0;

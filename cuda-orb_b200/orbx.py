@@ -66,6 +66,8 @@ def lib():
         L.orbx_match_knn2.argtypes = [vp, vp, i32, vp, i32, vp, vp, i32]
         L.orbx_pair.argtypes = [vp, vp, vp, i32, i32, i32, vp, vp, vp, vp, vp, vp, i32]
         L.orbx_debug_buffers.argtypes = [vp, vp, vp, vp, vp, vp]
+        L.orbx_pair_host.argtypes = [vp, vp, vp, i32, i32, i32, vp, vp, vp, vp, vp, vp, i32]
+        L.orbx_profile_pair.argtypes = [vp, vp, vp, i32, i32, i32, vp, vp, vp, vp, vp, vp, i32, vp]
         L.orbx_selftest_pi_minus.argtypes = [ctypes.c_uint32, ctypes.c_uint32]
         L.orbx_selftest_pi_minus.restype = ctypes.c_longlong
         _lib = L
@@ -168,6 +170,23 @@ class Context:
     def pair_ptr(self, d_a, d_b, w, h, pitch, pa, da, na, pb, db, nb, mode=MATCH_POPC):
         _check(lib().orbx_pair(self.h, _ptr(d_a), _ptr(d_b), w, h, pitch, _ptr(pa), _ptr(da), _ptr(na), _ptr(pb),
                                _ptr(db), _ptr(nb), mode), "orbx_pair")
+
+    def pair_host(self, a, b, w, h, pitch, pts_a, n_a, pts_b, n_b, desc_a=None, desc_b=None, mode=MATCH_POPC):
+        """Host-buffer pair call; a/b/pts/n/desc are host pointers (ints) or numpy arrays."""
+        def hp(x):
+            if x is None or isinstance(x, int):
+                return x
+            if hasattr(x, "ctypes"):
+                return x.ctypes.data
+            return x.data_ptr()
+        _check(lib().orbx_pair_host(self.h, hp(a), hp(b), w, h, pitch, hp(pts_a), hp(n_a), hp(pts_b), hp(n_b),
+                                    hp(desc_a), hp(desc_b), mode), "orbx_pair_host")
+
+    def profile_pair(self, d_a, d_b, w, h, pitch, pa, da, na, pb, db, nb, mode=MATCH_POPC):
+        ms = np.zeros(5, dtype=np.float32)
+        _check(lib().orbx_profile_pair(self.h, _ptr(d_a), _ptr(d_b), w, h, pitch, _ptr(pa), _ptr(da), _ptr(na),
+                                       _ptr(pb), _ptr(db), _ptr(nb), mode, ms.ctypes.data), "orbx_profile_pair")
+        return ms
 
     def debug_buffers(self, w, h):
         n, oszp = layout(w, h, self.params.noctaves)

@@ -118,6 +118,25 @@ ORBX_API int orbx_pair(orbx_ctx* ctx, const uint8_t* d_img_a, const uint8_t* d_i
                        orbx_point* d_pts_a, uint8_t* d_desc_a, int* d_n_a, orbx_point* d_pts_b,
                        uint8_t* d_desc_b, int* d_n_b, int mode);
 
+/* orbx_pair with host buffers, synchronous: copies both images (h x pitch bytes
+ * each; pinned memory makes the copies asynchronous DMA) to the device, runs the
+ * pair, and copies back the keypoint counts, the keypoints of both images
+ * (h_pts_* need max_pts entries; match/distance of A are filled) and, when the
+ * pointers are non-null, the descriptors (max_pts * 32 bytes each).  This is
+ * what Orbor::detectAndCompute x2 + Orbor::match hand back to the host
+ * (orb.cpp:95-112). */
+ORBX_API int orbx_pair_host(orbx_ctx* ctx, const uint8_t* h_img_a, const uint8_t* h_img_b, int w, int h, int pitch,
+                            orbx_point* h_pts_a, int* h_n_a, orbx_point* h_pts_b, int* h_n_b, uint8_t* h_desc_a,
+                            uint8_t* h_desc_b, int mode);
+
+/* Profiling variant of orbx_pair: the same launches without the graph, with a
+ * CUDA event between consecutive kernels; writes the milliseconds of the
+ * pyramid/blur, detect, NMS, describe and match kernels to stage_ms[0..4].
+ * Synchronises the stream. */
+ORBX_API int orbx_profile_pair(orbx_ctx* ctx, const uint8_t* d_img_a, const uint8_t* d_img_b, int w, int h, int pitch,
+                               orbx_point* d_pts_a, uint8_t* d_desc_a, int* d_n_a, orbx_point* d_pts_b,
+                               uint8_t* d_desc_b, int* d_n_b, int mode, float* stage_ms);
+
 /* Debug: copy the internal buffers of the last single-image call to the host:
  * raw pyramid, blurred pyramid (offsets[n] bytes each, reference layout),
  * score map and octave map (h * pitch0 each).  Synchronises the stream. */
