@@ -382,7 +382,7 @@ def run_orbx(args, world, rank, local):
 
 
 def bench_knn2(ctx, stream, dev, peaks):
-    """Matching only: 65536 queries x 65536 database rows, k = 2 (XOR-popc form)."""
+    """Matching only: 65536 queries x 65536 database rows, k = 2, both exact forms."""
     import torch
 
     import orbx
@@ -391,23 +391,37 @@ def bench_knn2(ctx, stream, dev, peaks):
     dbh, qh, _ = synth.match_workload(65536, 65536, seed=0)
     q = torch.from_numpy(qh).to(dev)
     db = torch.from_numpy(dbh).to(dev)
-    with torch.cuda.stream(stream):
-        dist, idx = orbx.knn2(ctx, q, db)
-        ctx.sync()
-        ms = []
-        for _ in range(5):
-            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            e0.record(stream)
-            orbx.knn2(ctx, q, db)
-            e1.record(stream)
-            e1.synchronize()
-            ms.append(e0.elapsed_time(e1))
-    t = statistics.median(ms)
     pairs = 65536.0 * 65536.0
-    peak = SMS * POPC_PER_CLK_PER_SM * peaks.get("sm_max_mhz", 1965.0) * 1e6 / 8  # pairs/s at 8 popc per pair
-    return {"form": "xor-popc", "ms": t, "pairs_per_s": pairs / (t * 1e-3), "roofline_pairs_per_s": peak,
-            "frac": pairs / (t * 1e-3) / peak,
-            "peak_kind": "derived: 148 SMs x 16 popc/clk x max SM clock / 8 popc per pair"}
+    out = {}
+    with torch.cuda.stream(stream):
+        res = {}
+        for name, mode in (("xor_popc", orbx.MATCH_POPC), ("int8_tcgen05", orbx.MATCH_IMMA)):
+            res[name] = orbx.knn2(ctx, q, db, mode)
+            ctx.sync()
+            ms = []
+            for _ in range(5):
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                orbx.knn2(ctx, q, db, mode)
+                e1.record(stream)
+                e1.synchronize()
+                ms.append(e0.elapsed_time(e1))
+            out[name] = {"ms": statistics.median(ms), "pairs_per_s": pairs / (statistics.median(ms) * 1e-3)}
+        same = bool(torch.equal(res["xor_popc"][0], res["int8_tcgen05"][0]) and
+                    torch.equal(res["xor_popc"][1], res["int8_tcgen05"][1]))
+    popc_peak = SMS * POPC_PER_CLK_PER_SM * peaks.get("sm_max_mhz", 1965.0) * 1e6 / 8
+    out["xor_popc"].update({"roofline_pairs_per_s": popc_peak, "frac": out["xor_popc"]["pairs_per_s"] / popc_peak,
+                            "peak_kind": "derived: 148 SMs x 16 popc/clk x max SM clock / 8 popc per pair"})
+    ops = pairs * 512.0  # 256 int8 multiply-adds per pair, 2 ops each
+    t = out["int8_tcgen05"]["ms"] * 1e-3
+    i8_measured = 2.0 * peaks.get("bf16_tflops", 1590.0) * 1e12
+    out["int8_tcgen05"].update({"tops": ops / t / 1e12, "peak_tops_measured_bf16x2": i8_measured / 1e12,
+                                "frac_of_measured": ops / t / i8_measured, "peak_tops_nominal_dense": 4500.0,
+                                "frac_of_nominal": ops / t / 4.5e15,
+                                "note": "int8 dense peak taken as 2x the measured cuBLAS bf16 peak; includes the "
+                                        "+-1 expansion of both 65536 x 32-byte sets"})
+    out["bit_exact_popc_vs_tcgen05"] = same
+    return out
 
 
 # ---------------------------------------------------------------------------

@@ -79,6 +79,10 @@ struct orbx_ctx {
   BatchSlot single, pair;
   MatchWork mw{};  // for orbx_match / orbx_match_knn2
   PairGraph pg;
+  // int8 tensor-core matcher scratch: +-1 expanded queries / database
+  int8_t* imma_q = nullptr;
+  int8_t* imma_db = nullptr;
+  size_t imma_q_bytes = 0, imma_db_bytes = 0;
   // orbx_pair_host device buffers
   uint8_t* io_img[2] = {nullptr, nullptr};
   size_t io_img_bytes = 0;
@@ -607,6 +611,8 @@ ORBX_API int orbx_destroy(orbx_ctx* c) {
   cudaFreeHost(c->io_count_host);
   for (auto& e : c->prof_ev)
     if (e) cudaEventDestroy(e);
+  cudaFree(c->imma_q);
+  cudaFree(c->imma_db);
   cudaFree(c->d_pattern);
   cudaFree(c->d_umax);
   cudaFree(c->d_err);
@@ -717,12 +723,59 @@ ORBX_API int orbx_detect_and_compute(orbx_ctx* c, const uint8_t* d_image, int w,
   return launch_frames(c, pl, compute_desc != 0);
 }
 
-static int match_common(orbx_ctx* c, MatchWork& mw, const MatchArgs& a, int nq_cap, int mode) {
-  if (mode != ORBX_MATCH_POPC && mode != ORBX_MATCH_AUTO) return ORBX_ERR_ARG;
+static int imma_ensure(orbx_ctx* c, int nq_cap, int ndb_cap) {
+  const size_t qb = (size_t)imma_rows_q(nq_cap < 1 ? 1 : nq_cap) * 256;
+  const size_t db = (size_t)imma_rows_db(ndb_cap < 1 ? 1 : ndb_cap) * 256;
+  if (c->imma_q_bytes < qb) {
+    cudaFree(c->imma_q);
+    c->imma_q = nullptr;
+    c->imma_q_bytes = 0;
+    ORBX_CUDA(cudaMalloc(&c->imma_q, qb));
+    c->imma_q_bytes = qb;
+  }
+  if (c->imma_db_bytes < db) {
+    cudaFree(c->imma_db);
+    c->imma_db = nullptr;
+    c->imma_db_bytes = 0;
+    ORBX_CUDA(cudaMalloc(&c->imma_db, db));
+    c->imma_db_bytes = db;
+  }
+  return ORBX_OK;
+}
+
+// AUTO picks the tensor-core form once the pair count pays for its expansion
+// pass and fixed tile cost.
+static int resolve_mode(int mode, long long nq, long long ndb) {
+  if (mode == ORBX_MATCH_AUTO) return (nq * ndb >= (1ll << 24) && nq >= 128) ? ORBX_MATCH_IMMA : ORBX_MATCH_POPC;
+  return mode;
+}
+
+static int launch_match(orbx_ctx* c, MatchWork& mw, const MatchArgs& a, int nq_cap, int ndb_cap, int mode) {
+  mode = resolve_mode(mode, nq_cap, ndb_cap);
+  if (mode != ORBX_MATCH_POPC && mode != ORBX_MATCH_IMMA) return ORBX_ERR_ARG;
   int rc = mw_ensure(mw, nq_cap);
   if (rc) return rc;
-  ORBX_CUDA(launch_match_popc(a, mw, c->stream));
+  if (mode == ORBX_MATCH_POPC) {
+    ORBX_CUDA(launch_match_popc(a, mw, c->stream));
+    return ORBX_OK;
+  }
+  if ((rc = imma_ensure(c, nq_cap, ndb_cap)) != 0) return rc;
+  ImmaLaunch L{};
+  L.args = a;
+  L.work = mw;
+  L.q_pm1 = c->imma_q;
+  L.db_pm1 = c->imma_db;
+  L.nq_cap = nq_cap;
+  L.ndb_cap = ndb_cap;
+  L.splits = imma_default_splits(nq_cap);
+  if (L.splits > mw.splits_cap) L.splits = mw.splits_cap;
+  L.err = c->d_err;
+  ORBX_CUDA(launch_match_imma(L, c->stream));
   return ORBX_OK;
+}
+
+static int match_common(orbx_ctx* c, MatchWork& mw, const MatchArgs& a, int nq_cap, int ndb_cap, int mode) {
+  return launch_match(c, mw, a, nq_cap, ndb_cap, mode);
 }
 
 ORBX_API int orbx_match(orbx_ctx* c, orbx_point* d_points1, const int* d_n1, const uint8_t* d_desc1,
@@ -740,7 +793,7 @@ ORBX_API int orbx_match(orbx_ctx* c, orbx_point* d_points1, const int* d_n1, con
   a.d_nq = d_n1;
   a.d_ndb = d_n2;
   a.pts = d_points1;
-  return match_common(c, c->mw, a, n1_cap, mode);
+  return match_common(c, c->mw, a, n1_cap, n2_cap, mode);
 }
 
 ORBX_API int orbx_match_knn2(orbx_ctx* c, const uint8_t* d_q, int nq, const uint8_t* d_db, int ndb,
@@ -757,7 +810,7 @@ ORBX_API int orbx_match_knn2(orbx_ctx* c, const uint8_t* d_q, int nq, const uint
   a.ndb = ndb;
   a.dist2 = d_dist2;
   a.idx2 = d_idx2;
-  return match_common(c, c->mw, a, nq, mode);
+  return match_common(c, c->mw, a, nq, ndb, mode);
 }
 
 ORBX_API int orbx_pair(orbx_ctx* c, const uint8_t* d_img_a, const uint8_t* d_img_b, int w, int h, int pitch,
@@ -766,10 +819,13 @@ ORBX_API int orbx_pair(orbx_ctx* c, const uint8_t* d_img_a, const uint8_t* d_img
   int rc = check_image(c, d_img_a, w, h, pitch);
   if (rc) return rc;
   if (!d_img_b || !d_pts_a || !d_desc_a || !d_n_a || !d_pts_b || !d_desc_b || !d_n_b) return ORBX_ERR_ARG;
-  if (mode != ORBX_MATCH_POPC && mode != ORBX_MATCH_AUTO) return ORBX_ERR_ARG;
+  if (mode != ORBX_MATCH_POPC && mode != ORBX_MATCH_AUTO && mode != ORBX_MATCH_IMMA) return ORBX_ERR_ARG;
+  // frame pairs hold at most max_pts keypoints each: the popcount form unless asked
+  if (mode == ORBX_MATCH_AUTO) mode = ORBX_MATCH_POPC;
   DeviceGuard g(c->device);
   if ((rc = ws_ensure(c, c->ws[0], w, h)) != 0) return rc;
   if ((rc = ws_ensure(c, c->ws[1], w, h)) != 0) return rc;
+  if (mode == ORBX_MATCH_IMMA && (rc = imma_ensure(c, c->p.max_pts, c->p.max_pts)) != 0) return rc;
   std::vector<Frame> frames(2);
   fill_frame(c, c->ws[0], d_img_a, pitch, d_pts_a, d_desc_a, d_n_a, frames[0]);
   fill_frame(c, c->ws[1], d_img_b, pitch, d_pts_b, d_desc_b, d_n_b, frames[1]);
@@ -805,7 +861,7 @@ ORBX_API int orbx_pair(orbx_ctx* c, const uint8_t* d_img_a, const uint8_t* d_img
     cudaGraph_t graph = nullptr;
     ORBX_CUDA(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
     int lrc = launch_frames(c, pl, true);
-    if (lrc == ORBX_OK) lrc = launch_match_popc(a, pg.mw, c->stream) == cudaSuccess ? ORBX_OK : ORBX_ERR_CUDA;
+    if (lrc == ORBX_OK) lrc = launch_match(c, pg.mw, a, c->p.max_pts, c->p.max_pts, mode);
     const cudaError_t ce = cudaStreamEndCapture(c->stream, &graph);
     if (lrc != ORBX_OK) {
       if (graph) cudaGraphDestroy(graph);

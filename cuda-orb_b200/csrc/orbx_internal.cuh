@@ -69,6 +69,7 @@ struct Batch {
 
 enum : int {
   kErrLookbackTimeout = 1,
+  kErrImmaTimeout = 2,
 };
 enum : int { kDescribeBoth = 0, kDescribeAngleOnly = 1, kDescribeDescOnly = 2 };
 
@@ -99,6 +100,59 @@ struct MatchWork {          // scratch for split-train merging
   int splits_cap;           // most train splits per query tile
 };
 int match_popc_blocks(int nq_cap, int splits_cap);
+
+// int8 tensor-core form (orbx_match_imma.cu)
+struct ImmaLaunch {
+  MatchArgs args;     // queries, database, counts, outputs
+  MatchWork work;     // split merging (splits_cap >= splits)
+  int8_t* q_pm1;      // [imma_rows_q(nq_cap)][256] scratch
+  int8_t* db_pm1;     // [imma_rows_db(ndb_cap)][256] scratch
+  int nq_cap, ndb_cap;
+  int splits;         // database splits per query tile
+  int* err;
+};
+int imma_rows_q(int n);
+int imma_rows_db(int n);
+int imma_default_splits(int nq_cap);
+cudaError_t launch_match_imma(const ImmaLaunch& L, cudaStream_t s);
+
+// Top-2 keys shared by both matcher forms: key = distance << 22 | index, so
+// ordering keys orders by (distance, index); 0xFFFFFFFF means "none".
+constexpr int kIdxBitsShared = 22;
+constexpr uint32_t kIdxMaskShared = (1u << kIdxBitsShared) - 1u;
+constexpr uint32_t kNoKeyShared = 0xFFFFFFFFu;
+constexpr int kMaxDistShared = 64;  // MAX_DIST, orbd.cu:26
+
+#ifdef __CUDACC__
+__device__ __forceinline__ void top2_push_shared(uint32_t& k1, uint32_t& k2, uint32_t key) {
+  k2 = min(k2, max(k1, key));
+  k1 = min(k1, key);
+}
+
+// Reference semantics of the final step (orbd.cu:1545-1557): both best scores
+// start at 256 and only strictly smaller distances replace them, so a match is
+// reported when the nearest distance is unique and below MAX_DIST.
+__device__ __forceinline__ void finish_query_shared(const MatchArgs& a, int q, uint32_t k1, uint32_t k2) {
+  const uint32_t d1 = (k1 == kNoKeyShared) ? kNoKeyShared : (k1 >> kIdxBitsShared);
+  const uint32_t d2 = (k2 == kNoKeyShared) ? kNoKeyShared : (k2 >> kIdxBitsShared);
+  const int i1 = (k1 == kNoKeyShared) ? -1 : (int)(k1 & kIdxMaskShared);
+  const int i2 = (k2 == kNoKeyShared) ? -1 : (int)(k2 & kIdxMaskShared);
+  if (a.dist2) {
+    a.dist2[2 * q] = d1;
+    a.dist2[2 * q + 1] = d2;
+  }
+  if (a.idx2) {
+    a.idx2[2 * q] = i1;
+    a.idx2[2 * q + 1] = i2;
+  }
+  if (a.pts) {
+    const uint32_t c1 = min(d1, 256u), c2 = min(d2, 256u);
+    const bool ok = (c1 < c2) && (c1 < (uint32_t)kMaxDistShared);
+    a.pts[q].match = ok ? i1 : -1;
+    a.pts[q].distance = ok ? (int)c1 : -1;
+  }
+}
+#endif
 
 // orbd.h lower-level entry points on caller-owned pyramid buffers (orbx_api.cu)
 int lower_detect(orbx_ctx* c, const uint8_t* image, uint8_t* octave_images, float* vmem, orbx_point* pts,

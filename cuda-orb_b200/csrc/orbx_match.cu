@@ -15,37 +15,12 @@ namespace orbx {
 
 constexpr int kMQ = 128;      // queries per block
 constexpr int kMChunk = 512;  // train rows per shared-memory chunk (16 KB)
-constexpr int kIdxBits = 22;
-constexpr uint32_t kIdxMask = (1u << kIdxBits) - 1u;
-constexpr uint32_t kNoKey = 0xFFFFFFFFu;
-constexpr int kMaxDist = 64;  // MAX_DIST, orbd.cu:26
+constexpr int kIdxBits = kIdxBitsShared;
+constexpr uint32_t kNoKey = kNoKeyShared;
 
-__device__ __forceinline__ void top2_push(uint32_t& k1, uint32_t& k2, uint32_t key) {
-  k2 = min(k2, max(k1, key));
-  k1 = min(k1, key);
-}
-
-// Reference semantics of the final step (orbd.cu:1545-1557): both best scores
-// start at 256 and only strictly smaller distances replace them.
+__device__ __forceinline__ void top2_push(uint32_t& k1, uint32_t& k2, uint32_t key) { top2_push_shared(k1, k2, key); }
 __device__ __forceinline__ void finish_query(const MatchArgs& a, int q, uint32_t k1, uint32_t k2) {
-  const uint32_t d1 = (k1 == kNoKey) ? kNoKey : (k1 >> kIdxBits);
-  const uint32_t d2 = (k2 == kNoKey) ? kNoKey : (k2 >> kIdxBits);
-  const int i1 = (k1 == kNoKey) ? -1 : (int)(k1 & kIdxMask);
-  const int i2 = (k2 == kNoKey) ? -1 : (int)(k2 & kIdxMask);
-  if (a.dist2) {
-    a.dist2[2 * q] = d1;
-    a.dist2[2 * q + 1] = d2;
-  }
-  if (a.idx2) {
-    a.idx2[2 * q] = i1;
-    a.idx2[2 * q + 1] = i2;
-  }
-  if (a.pts) {
-    const uint32_t c1 = min(d1, 256u), c2 = min(d2, 256u);
-    const bool ok = (c1 < c2) && (c1 < (uint32_t)kMaxDist);
-    a.pts[q].match = ok ? i1 : -1;
-    a.pts[q].distance = ok ? (int)c1 : -1;
-  }
+  finish_query_shared(a, q, k1, k2);
 }
 
 __global__ void __launch_bounds__(kMQ) k_match_popc(MatchArgs a, MatchWork w) {

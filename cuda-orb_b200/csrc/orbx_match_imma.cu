@@ -1,0 +1,505 @@
+// Brute-force k = 2 Hamming matching on the 5th-generation tensor cores.
+//
+// A 256-bit descriptor b is expanded to 256 int8 values s_k = 2*b_k - 1 (+-1),
+// so for two descriptors dot(s, t) = 256 - 2 * Hamming(s, t), computed exactly
+// by tcgen05.mma kind::i8 with int32 accumulation.  One block owns 128
+// queries (the MMA's M) and walks 256-row database tiles (the MMA's N) with
+// K = 256 = eight K=32 MMA steps per tile:
+//   warp 0     TMA producer: the query tile once, database tiles through a
+//              3-stage shared-memory ring (128-byte swizzle, no multicast);
+//   warp 1     MMA issuer: one elected thread issues the eight MMAs of a tile
+//              into one of two TMEM accumulators (2 x 256 columns) and commits
+//              them to the ring's "empty" and the accumulator's "full" barriers;
+//   warps 2-9  epilogue: each reads its 32 TMEM lanes (queries) over half of
+//              the columns, keeps a running best / second-best (dot, index)
+//              per query, and hands the accumulator back.
+// The block's result per query is the top-2 by (distance, index), the same
+// keys as the XOR-popc kernel (orbx_match.cu), so both forms agree bit for bit.
+// Every barrier wait is bounded by a clock deadline; on expiry the block
+// records kErrImmaTimeout, drains its in-flight copies, frees TMEM and exits.
+#include <cuda.h>
+#include <cudaTypedefs.h>
+
+#include "orbx_device.cuh"
+#include "orbx_internal.cuh"
+
+namespace orbx {
+
+constexpr int kIBM = 128;  // queries per block (MMA M)
+constexpr int kIBN = 256;  // database rows per tile (MMA N)
+constexpr int kIK = 256;   // bytes per expanded descriptor (MMA K)
+constexpr int kIStages = 3;
+constexpr int kIEpiWarps = 8;
+constexpr int kIThreads = (2 + kIEpiWarps) * 32;
+constexpr uint32_t kIHalfA = kIBM * 128;  // one 128-byte-wide K half of the query tile
+constexpr uint32_t kIHalfB = kIBN * 128;
+constexpr uint32_t kIATile = 2 * kIHalfA;
+constexpr uint32_t kIBTile = 2 * kIHalfB;
+constexpr uint32_t kINumBars = 1 + 2 * kIStages + 4;
+// 1024 bytes of alignment slack, the query tile, the ring, the barriers, TMEM base + abort flag;
+// the end-of-block merge scratch reuses ring stage 0 (free once the last MMA completed)
+constexpr uint32_t kISmemBytes = 1024 + kIATile + kIStages * kIBTile + 8 * kINumBars + 16;
+static_assert(kISmemBytes + 16 <= 232448, "exceeds the 227 KB shared-memory opt-in");
+static_assert(kIBM * 4 * sizeof(int) <= kIBTile, "merge scratch must fit in one ring stage");
+constexpr uint32_t kITmemCols = 512;
+constexpr long long kIDeadlineCycles = 4000000000ll;  // ~2 s at 2 GHz
+
+// instruction descriptor: S32 accumulate, S8 x S8, both K-major, N = 256, M = 128
+constexpr uint32_t kIDesc = (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(kIBN >> 3) << 17) |
+                            ((uint32_t)(kIBM >> 4) << 24);
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+// shared-memory matrix descriptor: K-major, 128-byte swizzle, 8-row groups 1024 B apart
+__device__ __forceinline__ uint64_t sw128_desc(uint32_t saddr) {
+  return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)1u << 16) | ((uint64_t)(1024u >> 4) << 32) |
+         ((uint64_t)1u << 46) | ((uint64_t)2u << 61);
+}
+
+__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive(uint32_t bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try(uint32_t bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(bar), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+
+// Bounded wait: false once the block's deadline has passed or another role aborted.
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, long long deadline,
+                                          volatile int* abort_flag) {
+  while (!mbar_try(bar, parity)) {
+    if (*abort_flag) return false;
+    if (clock64() > deadline) return false;
+  }
+  return true;
+}
+
+__device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap* map, int x, int y, uint32_t bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::"r"(
+          dst),
+      "l"(map), "r"(x), "r"(y), "r"(bar)
+      : "memory");
+}
+
+__device__ __forceinline__ void umma_i8(uint32_t tmem_d, uint64_t da, uint64_t db, uint32_t idesc, uint32_t acc) {
+  const uint32_t mask0 = 0, mask1 = 0, mask2 = 0, mask3 = 0;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}" ::"r"(tmem_d),
+      "l"(da), "l"(db), "r"(idesc), "r"(acc), "r"(mask0), "r"(mask1), "r"(mask2), "r"(mask3)
+      : "memory");
+}
+
+__device__ __forceinline__ void umma_commit(uint32_t bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar) : "memory");
+}
+
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, int* v) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
+      "{%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15, "
+      "%16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];"
+      : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
+        "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15]),
+        "=r"(v[16]), "=r"(v[17]), "=r"(v[18]), "=r"(v[19]), "=r"(v[20]), "=r"(v[21]), "=r"(v[22]), "=r"(v[23]),
+        "=r"(v[24]), "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]), "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
+      : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+
+// (dot desc, index asc) order; index -1 marks "none" and loses to anything.
+__device__ __forceinline__ bool dot_better(int d, int i, int d2, int i2) {
+  if (i < 0) return false;
+  if (i2 < 0) return true;
+  return d > d2 || (d == d2 && i < i2);
+}
+
+__device__ __forceinline__ uint32_t dot_key(int d, int i) {
+  return (i < 0) ? kNoKeyShared : ((uint32_t)((256 - d) >> 1) << kIdxBitsShared) | (uint32_t)i;
+}
+
+// Expand 256-bit descriptors to +-1 int8 rows; rows at or past the count are zero.
+__global__ void k_expand_pm1(const uint8_t* __restrict__ bits, int n_host, const int* d_n, int rows,
+                             int8_t* __restrict__ out) {
+  __shared__ unsigned long long lut[256];
+  for (int i = threadIdx.x; i < 256; i += blockDim.x) {
+    unsigned long long v = 0;
+    for (int j = 0; j < 8; j++) v |= (unsigned long long)(((i >> j) & 1) ? 0x01u : 0xFFu) << (8 * j);
+    lut[i] = v;
+  }
+  __syncthreads();
+  const int n = d_n ? min(*d_n, rows) : min(n_host, rows);
+  const long long total = (long long)rows * 32;
+  for (long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x; idx < total;
+       idx += (long long)gridDim.x * blockDim.x) {
+    const long long r = idx >> 5;
+    const unsigned long long v = (r < n) ? lut[bits[idx]] : 0ull;
+    reinterpret_cast<unsigned long long*>(out)[idx] = v;
+  }
+}
+
+// Warp-uniform bounded wait: lane 0 polls, the result is broadcast.
+__device__ __forceinline__ bool warp_wait(uint32_t bar, uint32_t parity, long long deadline,
+                                          volatile int* abort_flag) {
+  int ok = 0;
+  if ((threadIdx.x & 31) == 0) ok = mbar_wait(bar, parity, deadline, abort_flag) ? 1 : 0;
+  return __shfl_sync(0xffffffffu, ok, 0) != 0;
+}
+
+__global__ void __launch_bounds__(kIThreads, 1)
+    k_match_imma(const __grid_constant__ CUtensorMap tmQ, const __grid_constant__ CUtensorMap tmD, MatchArgs a,
+                 MatchWork w, int splits, int* err) {
+  extern __shared__ uint8_t smem_raw[];
+  const uint32_t raw = smem_u32(smem_raw);
+  uint8_t* smem = smem_raw + ((1024u - (raw & 1023u)) & 1023u);
+  uint8_t* sA = smem;
+  uint8_t* sB = sA + kIATile;
+  int* s_merge = reinterpret_cast<int*>(sB);  // used only after the last tile
+  uint64_t* bars = reinterpret_cast<uint64_t*>(sB + kIStages * kIBTile);
+  uint32_t* s_tmem = reinterpret_cast<uint32_t*>(bars + kINumBars);
+  volatile int* s_abort = reinterpret_cast<volatile int*>(s_tmem + 1);
+  __shared__ unsigned int s_last;
+
+  const int nq = min(a.d_nq ? *a.d_nq : a.nq, w.nq_cap);
+  const int ndb = a.d_ndb ? *a.d_ndb : a.ndb;
+  const int qtiles = (nq + kIBM - 1) / kIBM;
+  const int qb = blockIdx.x / splits;
+  const int sp = blockIdx.x - qb * splits;
+  if (qb >= qtiles) return;  // uniform over the block: before any barrier or TMEM use
+  const int dbtiles = (ndb + kIBN - 1) / kIBN;
+  const int t_beg = (int)((long long)dbtiles * sp / splits);
+  const int t_end = (int)((long long)dbtiles * (sp + 1) / splits);
+  const int ntiles = t_end - t_beg;
+
+  const int warp = threadIdx.x >> 5;
+  const int lane = threadIdx.x & 31;
+  const uint32_t bar0 = smem_u32(bars);
+  const uint32_t BAR_A = bar0;
+#define BAR_BFULL(s) (bar0 + 8u * (1 + (s)))
+#define BAR_BEMPTY(s) (bar0 + 8u * (1 + kIStages + (s)))
+#define BAR_ACCFULL(s) (bar0 + 8u * (1 + 2 * kIStages + (s)))
+#define BAR_ACCEMPTY(s) (bar0 + 8u * (3 + 2 * kIStages + (s)))
+
+  if (threadIdx.x == 0) {
+    mbar_init(BAR_A, 1);
+    for (int s = 0; s < kIStages; s++) {
+      mbar_init(BAR_BFULL(s), 1);
+      mbar_init(BAR_BEMPTY(s), 1);
+    }
+    for (int s = 0; s < 2; s++) {
+      mbar_init(BAR_ACCFULL(s), 1);
+      mbar_init(BAR_ACCEMPTY(s), kIEpiWarps);
+    }
+    *s_abort = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  }
+  if (warp == 1) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(s_tmem)),
+                 "r"(kITmemCols)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem_base = *s_tmem;
+  const long long deadline = clock64() + kIDeadlineCycles;
+
+  // epilogue state (warps 2..9): best and second-best (dot, index) of this row
+  const int quarter = warp & 3;
+  const int colhalf = (warp >= 2) ? ((warp - 2) >> 2) : 0;
+  int d1 = 0, i1 = -1, d2 = 0, i2 = -1;
+
+  if (warp == 0) {
+    if (lane == 0) {
+      // TMA producer
+      int issued[kIStages];
+      for (int s = 0; s < kIStages; s++) issued[s] = 0;
+      bool ok = true;
+      mbar_expect_tx(BAR_A, kIATile);
+      tma_load_2d(smem_u32(sA), &tmQ, 0, qb * kIBM, BAR_A);
+      tma_load_2d(smem_u32(sA + kIHalfA), &tmQ, 128, qb * kIBM, BAR_A);
+      for (int i = 0; i < ntiles; i++) {
+        const int s = i % kIStages;
+        const int use = i / kIStages;
+        if (use > 0 && !mbar_wait(BAR_BEMPTY(s), (use - 1) & 1, deadline, s_abort)) {
+          ok = false;
+          break;
+        }
+        const int row = (t_beg + i) * kIBN;
+        mbar_expect_tx(BAR_BFULL(s), kIBTile);
+        tma_load_2d(smem_u32(sB + s * kIBTile), &tmD, 0, row, BAR_BFULL(s));
+        tma_load_2d(smem_u32(sB + s * kIBTile + kIHalfB), &tmD, 128, row, BAR_BFULL(s));
+        issued[s]++;
+      }
+      if (!ok) {
+        *s_abort = 1;
+        atomicOr(err, kErrImmaTimeout);
+      }
+      // Drain before the block may exit: every issued copy has landed and every
+      // MMA that read a stage has completed (its commit arrived on "empty").
+      long long dl = clock64() + kIDeadlineCycles;
+      while (!mbar_try(BAR_A, 0) && clock64() < dl) {
+      }
+      for (int s = 0; s < kIStages; s++) {
+        if (issued[s] == 0) continue;
+        const uint32_t par = (uint32_t)(issued[s] - 1) & 1u;
+        dl = clock64() + kIDeadlineCycles;
+        while (!mbar_try(BAR_BFULL(s), par) && clock64() < dl) {
+        }
+        dl = clock64() + kIDeadlineCycles;
+        while (!mbar_try(BAR_BEMPTY(s), par) && clock64() < dl) {
+        }
+      }
+    }
+  } else if (warp == 1) {
+    if (lane == 0) {
+      // MMA issuer: eight K=32 steps per tile into accumulator (tile & 1)
+      bool ok = mbar_wait(BAR_A, 0, deadline, s_abort);
+      const uint32_t a_lo = smem_u32(sA);
+      for (int i = 0; ok && i < ntiles; i++) {
+        const int s = i % kIStages;
+        const int acc = i & 1;
+        if (!mbar_wait(BAR_BFULL(s), (uint32_t)(i / kIStages) & 1u, deadline, s_abort)) {
+          ok = false;
+          break;
+        }
+        if (i >= 2 && !mbar_wait(BAR_ACCEMPTY(acc), (uint32_t)((i - 2) >> 1) & 1u, deadline, s_abort)) {
+          ok = false;
+          break;
+        }
+        tc_fence_after();
+        const uint32_t d = tmem_base + (uint32_t)(acc * kIBN);
+        const uint32_t b_lo = smem_u32(sB + s * kIBTile);
+#pragma unroll
+        for (int k = 0; k < 8; k++) {
+          const int h = k >> 2, kk = k & 3;
+          const uint64_t da = sw128_desc(a_lo + h * kIHalfA) + (uint64_t)(2 * kk);
+          const uint64_t db = sw128_desc(b_lo + h * kIHalfB) + (uint64_t)(2 * kk);
+          umma_i8(d, da, db, kIDesc, k > 0 ? 1u : 0u);
+        }
+        umma_commit(BAR_BEMPTY(s));
+        umma_commit(BAR_ACCFULL(acc));
+      }
+      if (!ok) {
+        *s_abort = 1;
+        atomicOr(err, kErrImmaTimeout);
+      }
+    }
+  } else {
+    // epilogue: TMEM lanes 32*(warp&3).. (one query per lane), columns [128*colhalf, +128)
+    bool ok = true;
+    for (int i = 0; i < ntiles; i++) {
+      const int acc = i & 1;
+      if (!warp_wait(BAR_ACCFULL(acc), (uint32_t)(i >> 1) & 1u, deadline, s_abort)) {
+        ok = false;
+        break;
+      }
+      tc_fence_after();
+      const int gbase = (t_beg + i) * kIBN + colhalf * 128;
+      const uint32_t tbase =
+          tmem_base + ((uint32_t)(quarter * 32) << 16) + (uint32_t)(acc * kIBN + colhalf * 128);
+#pragma unroll 1
+      for (int c = 0; c < 4; c++) {
+        int v[32];
+        tmem_ld32(tbase + (uint32_t)(c * 32), v);
+        const int g0 = gbase + c * 32;
+        int m = v[0];
+#pragma unroll
+        for (int j = 1; j < 32; j++) m = max(m, v[j]);
+        // columns arrive in increasing index order, so only a strictly larger dot
+        // can enter the top two
+        if (__any_sync(0xffffffffu, i2 < 0 || m > d2)) {
+#pragma unroll
+          for (int j = 0; j < 32; j++) {
+            const int g = g0 + j;
+            const int dv = v[j];
+            if (g < ndb) {
+              if (i1 < 0 || dv > d1) {
+                d2 = d1;
+                i2 = i1;
+                d1 = dv;
+                i1 = g;
+              } else if (i2 < 0 || dv > d2) {
+                d2 = dv;
+                i2 = g;
+              }
+            }
+          }
+        }
+      }
+      tc_fence_before();
+      __syncwarp();
+      if (lane == 0) mbar_arrive(BAR_ACCEMPTY(acc));
+    }
+    if (!ok) {
+      *s_abort = 1;
+      if (lane == 0) atomicOr(err, kErrImmaTimeout);
+    }
+    if (colhalf == 1) {
+      int* mrow = s_merge + 4 * (quarter * 32 + lane);
+      mrow[0] = d1;
+      mrow[1] = i1;
+      mrow[2] = d2;
+      mrow[3] = i2;
+    }
+  }
+#undef BAR_BFULL
+#undef BAR_BEMPTY
+#undef BAR_ACCFULL
+#undef BAR_ACCEMPTY
+
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  if (warp == 1) {
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem_base), "r"(kITmemCols)
+                 : "memory");
+  }
+  if (warp >= 2 && colhalf == 0) {
+    // merge the two column halves of each row: top two of four by (dot desc, index asc)
+    const int row = quarter * 32 + lane;
+    const int* mrow = s_merge + 4 * row;
+    const int e1 = mrow[0], j1 = mrow[1], e2 = mrow[2], j2 = mrow[3];
+    int bd1, bi1, bd2, bi2;
+    if (dot_better(e1, j1, d1, i1)) {
+      bd1 = e1;
+      bi1 = j1;
+      const bool x = dot_better(d1, i1, e2, j2);
+      bd2 = x ? d1 : e2;
+      bi2 = x ? i1 : j2;
+    } else {
+      bd1 = d1;
+      bi1 = i1;
+      const bool x = dot_better(e1, j1, d2, i2);
+      bd2 = x ? e1 : d2;
+      bi2 = x ? j1 : i2;
+    }
+    const int q = qb * kIBM + row;
+    if (q < nq) {
+      const uint32_t k1 = dot_key(bd1, bi1), k2 = dot_key(bd2, bi2);
+      if (splits == 1)
+        finish_query_shared(a, q, k1, k2);
+      else
+        reinterpret_cast<uint2*>(w.part)[(size_t)sp * w.nq_cap + q] = make_uint2(k1, k2);
+    }
+  }
+  if (splits == 1) return;
+  // the last block of this query tile to finish merges the partial top-2 of all splits
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) s_last = (atomicAdd(&w.tile_done[qb], 1u) == (unsigned)(splits - 1)) ? 1u : 0u;
+  __syncthreads();
+  if (!s_last) return;
+  __threadfence();
+  if (threadIdx.x == 0) w.tile_done[qb] = 0u;
+  if (threadIdx.x >= kIBM) return;
+  const int q = qb * kIBM + threadIdx.x;
+  if (q >= nq) return;
+  const uint2* part = reinterpret_cast<const uint2*>(w.part);
+  uint32_t m1 = kNoKeyShared, m2 = kNoKeyShared;
+  for (int s2 = 0; s2 < splits; s2++) {
+    const uint2 pk = __ldcg(part + (size_t)s2 * w.nq_cap + q);
+    top2_push_shared(m1, m2, pk.x);
+    top2_push_shared(m1, m2, pk.y);
+  }
+  finish_query_shared(a, q, m1, m2);
+}
+
+// ---------------------------------------------------------------------------
+// host side
+// ---------------------------------------------------------------------------
+static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  if (!fn) {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+  }
+  return fn;
+}
+
+static bool make_rows_map(CUtensorMap* m, const void* base, uint64_t rows, uint32_t box_rows) {
+  auto enc = tensor_map_encoder();
+  if (!enc) return false;
+  cuuint64_t dims[2] = {(cuuint64_t)kIK, (cuuint64_t)rows};
+  cuuint64_t strides[1] = {(cuuint64_t)kIK};
+  cuuint32_t box[2] = {128u, box_rows};
+  cuuint32_t es[2] = {1u, 1u};
+  const CUresult r = enc(m, CU_TENSOR_MAP_DATA_TYPE_UINT8, 2, const_cast<void*>(base), dims, strides, box, es,
+                         CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                         CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return r == CUDA_SUCCESS;
+}
+
+int imma_rows_q(int n) { return (n + kIBM - 1) / kIBM * kIBM; }
+
+// Database splits per query tile so that the grid fills the 148 SMs in whole
+// waves (one 227 KB block per SM): 512 query tiles -> 2 splits -> 1024 blocks.
+int imma_default_splits(int nq_cap) {
+  const int qt = (nq_cap + kIBM - 1) / kIBM;
+  int best = 1;
+  double best_eff = 0.0;
+  for (int s = 1; s <= 16; s++) {
+    const long long blocks = (long long)qt * s;
+    const long long waves = (blocks + 147) / 148;
+    const double eff = (double)blocks / (double)(waves * 148);
+    if (eff > best_eff + 0.02) {
+      best_eff = eff;
+      best = s;
+    }
+  }
+  return best;
+}
+int imma_rows_db(int n) { return (n + kIBN - 1) / kIBN * kIBN; }
+
+cudaError_t launch_match_imma(const ImmaLaunch& L, cudaStream_t s) {
+  if (L.nq_cap <= 0) return cudaSuccess;
+  static bool attr_set = false;
+  if (!attr_set) {
+    cudaError_t e = cudaFuncSetAttribute(k_match_imma, cudaFuncAttributeMaxDynamicSharedMemorySize, kISmemBytes);
+    if (e != cudaSuccess) return e;
+    attr_set = true;
+  }
+  const int qrows = imma_rows_q(L.nq_cap);
+  const int dbrows = imma_rows_db(L.ndb_cap > 0 ? L.ndb_cap : 1);
+  {
+    const int blocks = 4 * 148;
+    k_expand_pm1<<<blocks, 256, 0, s>>>(L.args.q, L.args.nq, L.args.d_nq, qrows, L.q_pm1);
+    if (L.ndb_cap > 0) k_expand_pm1<<<blocks, 256, 0, s>>>(L.args.db, L.args.ndb, L.args.d_ndb, dbrows, L.db_pm1);
+  }
+  CUtensorMap tq, td;
+  if (!make_rows_map(&tq, L.q_pm1, (uint64_t)qrows, kIBM)) return cudaErrorInvalidValue;
+  if (!make_rows_map(&td, L.db_pm1, (uint64_t)dbrows, kIBN)) return cudaErrorInvalidValue;
+  const int qtiles = qrows / kIBM;
+  k_match_imma<<<qtiles * L.splits, kIThreads, kISmemBytes, s>>>(tq, td, L.args, L.work, L.splits, L.err);
+  return cudaGetLastError();
+}
+
+}  // namespace orbx

@@ -158,54 +158,58 @@ def test_against_reference_build_live(ctx, w, h, seed):
     assert np.array_equal(m_ref, m_o) and np.array_equal(d_ref, d_o)
 
 
-def _match_gpu(ctx, d1, d2):
+def _match_gpu(ctx, d1, d2, mode=orbx.MATCH_POPC):
     n1, n2 = len(d1), len(d2)
     pts = torch.zeros((max(n1, 1), 7), dtype=torch.int32, device="cuda")
     t1 = torch.from_numpy(np.ascontiguousarray(d1)).cuda() if n1 else torch.zeros((1, 32), dtype=torch.uint8,
                                                                                   device="cuda")
     t2 = torch.from_numpy(np.ascontiguousarray(d2)).cuda() if n2 else None
     cnt = torch.tensor([n1, n2], dtype=torch.int32, device="cuda")
-    ctx.match_ptr(pts, cnt[0:1].data_ptr(), t1, cnt[1:2].data_ptr(), t2, n1, n2)
+    ctx.match_ptr(pts, cnt[0:1].data_ptr(), t1, cnt[1:2].data_ptr(), t2, n1, n2, mode)
     ctx.sync()
     p = pts[:n1].cpu().numpy()
     return p[:, 5].copy(), p[:, 6].copy()
 
 
-def test_match_kat(ctx, golden):
+@pytest.mark.parametrize("mode", [orbx.MATCH_POPC, orbx.MATCH_IMMA])
+def test_match_kat(ctx, golden, mode):
     g = golden("match_kat.npz")
     for name in g["names"]:
         name = str(name)
-        m, d = _match_gpu(ctx, g[name + "_q"], g[name + "_db"])
+        m, d = _match_gpu(ctx, g[name + "_q"], g[name + "_db"], mode)
         assert np.array_equal(m, g[name + "_match"]), name
         assert np.array_equal(d, g[name + "_dist"]), name
 
 
+@pytest.mark.parametrize("mode", [orbx.MATCH_POPC, orbx.MATCH_IMMA])
 @pytest.mark.parametrize("name", ["pair_320x240_s1.npz", "pair_640x480_s2.npz"])
-def test_match_golden_pairs(ctx, golden, name):
+def test_match_golden_pairs(ctx, golden, name, mode):
     g = golden(name)
-    m, d = _match_gpu(ctx, g["A_desc"], g["B_desc"])
+    m, d = _match_gpu(ctx, g["A_desc"], g["B_desc"], mode)
     assert np.array_equal(m, g["match_rf"]) and np.array_equal(d, g["dist_rf"])
 
 
+@pytest.mark.parametrize("mode", [orbx.MATCH_POPC, orbx.MATCH_IMMA])
 @pytest.mark.parametrize("nq,ndb", [(1, 1), (5, 0), (127, 129), (1000, 1000), (3000, 200), (200, 70000),
-                                    (4096, 16384)])
-def test_knn2_vs_oracle(ctx, nq, ndb):
+                                    (4096, 16384), (333, 257)])
+def test_knn2_vs_oracle(ctx, nq, ndb, mode):
     db, q, _ = synth.match_workload(max(ndb, 1), nq, seed=nq * 7 + ndb)
     db = db[:ndb]
     dist, idx = orbx.knn2(ctx, torch.from_numpy(q).cuda(), torch.from_numpy(db).cuda() if ndb else
-                          torch.zeros((0, 32), dtype=torch.uint8, device="cuda"))
+                          torch.zeros((0, 32), dtype=torch.uint8, device="cuda"), mode)
     ctx.sync()
     od, oi = O.knn2(q, db)
     assert np.array_equal(dist.cpu().numpy().view(np.uint32), od)
     assert np.array_equal(idx.cpu().numpy(), oi)
 
 
-def test_knn2_full_size_sampled(ctx):
+@pytest.mark.parametrize("mode", [orbx.MATCH_POPC, orbx.MATCH_IMMA])
+def test_knn2_full_size_sampled(ctx, mode):
     """65536 x 65536 (the matching-only workload) on the GPU; a seeded sample of
     2048 queries is checked against the oracle, and every planted near-duplicate
     query must find its source row."""
     db, q, src = synth.match_workload(65536, 65536, seed=0)
-    dist, idx = orbx.knn2(ctx, torch.from_numpy(q).cuda(), torch.from_numpy(db).cuda())
+    dist, idx = orbx.knn2(ctx, torch.from_numpy(q).cuda(), torch.from_numpy(db).cuda(), mode)
     ctx.sync()
     dist = dist.cpu().numpy().view(np.uint32)
     idx = idx.cpu().numpy()
@@ -218,7 +222,18 @@ def test_knn2_full_size_sampled(ctx):
     assert np.all(dist[:, 0] <= dist[:, 1])
 
 
-def test_pair_api_matches_single_calls(ctx):
+def test_imma_equals_popc_full_size(ctx):
+    """Both matcher forms on the 65536 x 65536 workload: identical distances and indices."""
+    db, q, _ = synth.match_workload(65536, 65536, seed=1)
+    tq, tdb = torch.from_numpy(q).cuda(), torch.from_numpy(db).cuda()
+    d0, i0 = orbx.knn2(ctx, tq, tdb, orbx.MATCH_POPC)
+    d1, i1 = orbx.knn2(ctx, tq, tdb, orbx.MATCH_IMMA)
+    ctx.sync()
+    assert torch.equal(d0, d1) and torch.equal(i0, i1)
+
+
+@pytest.mark.parametrize("mode", [orbx.MATCH_POPC, orbx.MATCH_IMMA])
+def test_pair_api_matches_single_calls(ctx, mode):
     w, h = 1280, 720
     a, b, _ = synth.make_pair(w, h, 3)
     ctx.init(orbx.make_params(max_pts=10000))
@@ -227,7 +242,7 @@ def test_pair_api_matches_single_calls(ctx):
     A = orbx.FrameBuffers(10000)
     B = orbx.FrameBuffers(10000)
     for _ in range(3):  # first call captures the graph, later calls replay it
-        ctx.pair_ptr(da, db, w, h, a.shape[1], A.points, A.desc, A.count, B.points, B.desc, B.count)
+        ctx.pair_ptr(da, db, w, h, a.shape[1], A.points, A.desc, A.count, B.points, B.desc, B.count, mode)
         ctx.sync()
         pa, desc_a = A.to_host()
         pb, desc_b = B.to_host()
