@@ -10,9 +10,9 @@
 //   warp 1     MMA issuer: one elected thread issues the eight MMAs of a tile
 //              into one of two TMEM accumulators (2 x 256 columns) and commits
 //              them to the ring's "empty" and the accumulator's "full" barriers;
-//   warps 2-9  epilogue: each reads its 32 TMEM lanes (queries) over half of
-//              the columns, keeps a running best / second-best (dot, index)
-//              per query, and hands the accumulator back.
+//   warps 2-17 epilogue: each reads its 32 TMEM lanes (queries) over a quarter
+//              of the columns into registers, hands the accumulator straight
+//              back, and keeps a running best / second-best key per query.
 // The block's result per query is the top-2 by (distance, index), the same
 // keys as the XOR-popc kernel (orbx_match.cu), so both forms agree bit for bit.
 // Every barrier wait is bounded by a clock deadline; on expiry the block
@@ -29,7 +29,7 @@ constexpr int kIBM = 128;  // queries per block (MMA M)
 constexpr int kIBN = 256;  // database rows per tile (MMA N)
 constexpr int kIK = 256;   // bytes per expanded descriptor (MMA K)
 constexpr int kIStages = 3;
-constexpr int kIEpiWarps = 8;
+constexpr int kIEpiWarps = 16;  // four per TMEM lane quarter, 64 columns each
 constexpr int kIThreads = (2 + kIEpiWarps) * 32;
 constexpr uint32_t kIHalfA = kIBM * 128;  // one 128-byte-wide K half of the query tile
 constexpr uint32_t kIHalfB = kIBN * 128;
@@ -40,7 +40,7 @@ constexpr uint32_t kINumBars = 1 + 2 * kIStages + 4;
 // the end-of-block merge scratch reuses ring stage 0 (free once the last MMA completed)
 constexpr uint32_t kISmemBytes = 1024 + kIATile + kIStages * kIBTile + 8 * kINumBars + 16;
 static_assert(kISmemBytes + 16 <= 232448, "exceeds the 227 KB shared-memory opt-in");
-static_assert(kIBM * 4 * sizeof(int) <= kIBTile, "merge scratch must fit in one ring stage");
+static_assert(3 * kIBM * sizeof(uint2) <= kIBTile, "merge scratch must fit in one ring stage");
 constexpr uint32_t kITmemCols = 512;
 constexpr long long kIDeadlineCycles = 4000000000ll;  // ~2 s at 2 GHz
 
@@ -117,6 +117,8 @@ __device__ __forceinline__ void umma_commit(uint32_t bar) {
 __device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
 
+__device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
+
 __device__ __forceinline__ void tmem_ld32(uint32_t taddr, int* v) {
   asm volatile(
       "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
@@ -127,18 +129,16 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, int* v) {
         "=r"(v[16]), "=r"(v[17]), "=r"(v[18]), "=r"(v[19]), "=r"(v[20]), "=r"(v[21]), "=r"(v[22]), "=r"(v[23]),
         "=r"(v[24]), "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]), "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
       : "r"(taddr));
-  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 }
 
-// (dot desc, index asc) order; index -1 marks "none" and loses to anything.
-__device__ __forceinline__ bool dot_better(int d, int i, int d2, int i2) {
-  if (i < 0) return false;
-  if (i2 < 0) return true;
-  return d > d2 || (d == d2 && i < i2);
-}
+// Dot value given to database columns past the end of the set (never selected).
+constexpr int kMaskedDot = -65536;
 
-__device__ __forceinline__ uint32_t dot_key(int d, int i) {
-  return (i < 0) ? kNoKeyShared : ((uint32_t)((256 - d) >> 1) << kIdxBitsShared) | (uint32_t)i;
+// Global key (distance << 22 | index) of a chunk-local key (dot << 5 | 31 - column).
+__device__ __forceinline__ uint32_t local_to_key(int lk, int g_chunk) {
+  const int dot = lk >> 5;
+  const int col = 31 - (lk & 31);
+  return ((uint32_t)((256 - dot) >> 1) << kIdxBitsShared) | (uint32_t)(g_chunk + col);
 }
 
 // Expand 256-bit descriptors to +-1 int8 rows; rows at or past the count are zero.
@@ -229,10 +229,10 @@ __global__ void __launch_bounds__(kIThreads, 1)
   const uint32_t tmem_base = *s_tmem;
   const long long deadline = clock64() + kIDeadlineCycles;
 
-  // epilogue state (warps 2..9): best and second-best (dot, index) of this row
+  // epilogue state (warps 2..17): best and second-best key of this row
   const int quarter = warp & 3;
-  const int colhalf = (warp >= 2) ? ((warp - 2) >> 2) : 0;
-  int d1 = 0, i1 = -1, d2 = 0, i2 = -1;
+  const int colgrp = (warp >= 2) ? ((warp - 2) >> 2) : 0;
+  uint32_t k1 = kNoKeyShared, k2 = kNoKeyShared;
 
   if (warp == 0) {
     if (lane == 0) {
@@ -311,7 +311,7 @@ __global__ void __launch_bounds__(kIThreads, 1)
       }
     }
   } else {
-    // epilogue: TMEM lanes 32*(warp&3).. (one query per lane), columns [128*colhalf, +128)
+    // epilogue: TMEM lanes 32*(warp&3).. (one query per lane), columns [64*colgrp, +64)
     bool ok = true;
     for (int i = 0; i < ntiles; i++) {
       const int acc = i & 1;
@@ -320,53 +320,50 @@ __global__ void __launch_bounds__(kIThreads, 1)
         break;
       }
       tc_fence_after();
-      const int gbase = (t_beg + i) * kIBN + colhalf * 128;
-      const uint32_t tbase =
-          tmem_base + ((uint32_t)(quarter * 32) << 16) + (uint32_t)(acc * kIBN + colhalf * 128);
-#pragma unroll 1
-      for (int c = 0; c < 4; c++) {
-        int v[32];
-        tmem_ld32(tbase + (uint32_t)(c * 32), v);
-        const int g0 = gbase + c * 32;
-        int m = v[0];
-#pragma unroll
-        for (int j = 1; j < 32; j++) m = max(m, v[j]);
-        // columns arrive in increasing index order, so only a strictly larger dot
-        // can enter the top two
-        if (__any_sync(0xffffffffu, i2 < 0 || m > d2)) {
-#pragma unroll
-          for (int j = 0; j < 32; j++) {
-            const int g = g0 + j;
-            const int dv = v[j];
-            if (g < ndb) {
-              if (i1 < 0 || dv > d1) {
-                d2 = d1;
-                i2 = i1;
-                d1 = dv;
-                i1 = g;
-              } else if (i2 < 0 || dv > d2) {
-                d2 = dv;
-                i2 = g;
-              }
-            }
-          }
-        }
-      }
+      const int g0 = (t_beg + i) * kIBN + colgrp * 64;
+      const uint32_t taddr = tmem_base + ((uint32_t)(quarter * 32) << 16) + (uint32_t)(acc * kIBN + colgrp * 64);
+      int v[64];
+      tmem_ld32(taddr, v);
+      tmem_ld32(taddr + 32u, v + 32);
+      tmem_wait_ld();
+      // the values are in registers: hand the accumulator back to the MMA warp now
       tc_fence_before();
       __syncwarp();
       if (lane == 0) mbar_arrive(BAR_ACCEMPTY(acc));
+      if (g0 + 64 > ndb) {
+#pragma unroll
+        for (int j = 0; j < 64; j++)
+          if (g0 + j >= ndb) v[j] = kMaskedDot;
+      }
+      int thr = (k2 == kNoKeyShared) ? kMaskedDot : 256 - 2 * (int)(k2 >> kIdxBitsShared);
+#pragma unroll
+      for (int c = 0; c < 2; c++) {
+        int m = v[32 * c];
+#pragma unroll
+        for (int j = 1; j < 32; j++) m = max(m, v[32 * c + j]);
+        // columns arrive in increasing index order, so only a strictly larger dot
+        // than the current second best can enter the top two
+        if (__any_sync(0xffffffffu, m > thr)) {
+          // top two of the chunk on local keys (dot << 5 | 31 - column): ties keep the lower column
+          int a1 = INT_MIN, a2 = INT_MIN;
+#pragma unroll
+          for (int j = 0; j < 32; j++) {
+            const int lk = (v[32 * c + j] << 5) | (31 - j);
+            a2 = max(a2, min(a1, lk));
+            a1 = max(a1, lk);
+          }
+          const int gc = g0 + 32 * c;
+          if ((a1 >> 5) > kMaskedDot) top2_push_shared(k1, k2, local_to_key(a1, gc));
+          if ((a2 >> 5) > kMaskedDot) top2_push_shared(k1, k2, local_to_key(a2, gc));
+          thr = (k2 == kNoKeyShared) ? kMaskedDot : 256 - 2 * (int)(k2 >> kIdxBitsShared);
+        }
+      }
     }
     if (!ok) {
       *s_abort = 1;
       if (lane == 0) atomicOr(err, kErrImmaTimeout);
     }
-    if (colhalf == 1) {
-      int* mrow = s_merge + 4 * (quarter * 32 + lane);
-      mrow[0] = d1;
-      mrow[1] = i1;
-      mrow[2] = d2;
-      mrow[3] = i2;
-    }
+    if (colgrp > 0) reinterpret_cast<uint2*>(s_merge)[(colgrp - 1) * kIBM + quarter * 32 + lane] = make_uint2(k1, k2);
   }
 #undef BAR_BFULL
 #undef BAR_BEMPTY
@@ -380,28 +377,16 @@ __global__ void __launch_bounds__(kIThreads, 1)
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem_base), "r"(kITmemCols)
                  : "memory");
   }
-  if (warp >= 2 && colhalf == 0) {
-    // merge the two column halves of each row: top two of four by (dot desc, index asc)
+  if (warp >= 2 && colgrp == 0) {
+    // merge the four column groups of each row
     const int row = quarter * 32 + lane;
-    const int* mrow = s_merge + 4 * row;
-    const int e1 = mrow[0], j1 = mrow[1], e2 = mrow[2], j2 = mrow[3];
-    int bd1, bi1, bd2, bi2;
-    if (dot_better(e1, j1, d1, i1)) {
-      bd1 = e1;
-      bi1 = j1;
-      const bool x = dot_better(d1, i1, e2, j2);
-      bd2 = x ? d1 : e2;
-      bi2 = x ? i1 : j2;
-    } else {
-      bd1 = d1;
-      bi1 = i1;
-      const bool x = dot_better(e1, j1, d2, i2);
-      bd2 = x ? e1 : d2;
-      bi2 = x ? j1 : i2;
+    for (int g = 0; g < 3; g++) {
+      const uint2 pk = reinterpret_cast<const uint2*>(s_merge)[g * kIBM + row];
+      top2_push_shared(k1, k2, pk.x);
+      top2_push_shared(k1, k2, pk.y);
     }
     const int q = qb * kIBM + row;
     if (q < nq) {
-      const uint32_t k1 = dot_key(bd1, bi1), k2 = dot_key(bd2, bi2);
       if (splits == 1)
         finish_query_shared(a, q, k1, k2);
       else
