@@ -1,0 +1,89 @@
+"""Host-side logic of bench.py without a GPU: the multi-rank plumbing on
+gloo (world size 2, 127.0.0.1), the per-kernel work model and the clock
+parser."""
+import os
+import socket
+
+import numpy as np
+import pytest
+import torch.multiprocessing as mp
+
+import bench
+
+
+def _free_port():
+    s = socket.socket()
+    s.bind(("127.0.0.1", 0))
+    port = s.getsockname()[1]
+    s.close()
+    return port
+
+
+def _rank_main(rank, world, port, out):
+    os.environ.update({"WORLD_SIZE": str(world), "RANK": str(rank), "LOCAL_RANK": str(rank),
+                       "MASTER_ADDR": "127.0.0.1", "MASTER_PORT": str(port)})
+    w, r, local = bench.dist_setup()
+    assert (w, r, local) == (world, rank, rank)
+    bench.barrier(w)
+    # per-rank step times differ; the job time is the slowest rank
+    t_max = bench.max_over_ranks(10.0 + 5.0 * rank, w)
+    t_sum = bench.sum_over_ranks(1.0, w)
+    out[rank] = (t_max, t_sum)
+    import torch.distributed as dist
+
+    dist.barrier()
+    dist.destroy_process_group()
+
+
+def test_replica_timing_gloo_world2():
+    ctx = mp.get_context("spawn")
+    mgr = ctx.Manager()
+    out = mgr.dict()
+    port = _free_port()
+    procs = [ctx.Process(target=_rank_main, args=(r, 2, port, out)) for r in range(2)]
+    for p in procs:
+        p.start()
+    for p in procs:
+        p.join(120)
+    assert all(p.exitcode == 0 for p in procs), [p.exitcode for p in procs]
+    assert out[0] == out[1] == (15.0, 2.0)
+
+
+def test_single_rank_helpers():
+    assert bench.max_over_ranks(3.5, 1) == 3.5
+    assert bench.sum_over_ranks(2.0, 1) == 2.0
+
+
+def test_stage_work_1080p():
+    import orbx
+
+    n, oszp = orbx.layout(1920, 1080, 8)
+    work = bench.stage_work(oszp, n, 1000, 1200)
+    assert work["pyramid_blur"] == 2 * (1080 * 1920 + 2 * 2799360)
+    assert work["detect"] == 2 * (2799360 + 8 * 1080 * 1920)
+    assert work["nms"] == 2 * 4 * 1080 * 1920 + 2200 * 28
+    assert work["describe"] == 2200 * (28 + 961 + 512 + 36)
+
+
+def test_clock_sampler_parses_reasons(monkeypatch):
+    class FakeProc:
+        def terminate(self):
+            pass
+
+        def communicate(self, timeout=None):
+            rows = ["0, 1965, 1965, 700.1, 0x0, Not Active, Not Active, Not Active, Not Active",
+                    "0, 1890, 1965, 990.0, 0x4, Not Active, Not Active, Not Active, Active",
+                    "0, 1900, 1965, 995.2, 0x4, Not Active, Not Active, Not Active, Active"]
+            return "\n".join(rows) + "\n", ""
+
+    s = bench.ClockSampler(0)
+    s.proc = FakeProc()
+    c = s.stop()
+    assert c["samples"] == 3 and c["sm_mhz"] == 1900.0 and c["sm_max_mhz"] == 1965.0
+    assert c["reasons"] == ["sw_power_cap"]
+
+
+def test_peaks_file_or_fallback():
+    pk, kind = bench.load_peaks()
+    assert kind in ("measured", "fallback")
+    assert pk["hbm_gbs"] > 1000
