@@ -41,7 +41,7 @@ POPC_PER_CLK_PER_SM = 16  # 32-bit population count results per clock per SM
 SMS = 148
 
 # DRAM bytes per launch measured by ncu (dram__bytes_read.sum + dram__bytes_write.sum)
-# for the same workload; see profiles/pair1080_kernels.md.  None until captured.
+# on the same workload; kernels without a capture report None.
 NCU_TRAFFIC = {}
 
 
@@ -53,6 +53,9 @@ def parse_args(argv=None):
     p.add_argument("--impl", choices=["orbx", "reference"], default="orbx")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-match-bench", action="store_true")
+    p.add_argument("--workload", choices=["pair1080", "match65536"], default="pair1080",
+                   help="pair1080: the 1920x1080 pair (default); match65536: k=2 matching only")
+    p.add_argument("--match-mode", choices=["imma", "popc"], default="imma")
     return p.parse_args(argv)
 
 
@@ -471,9 +474,65 @@ def run_reference(args, world, rank, local):
     }
 
 
+def run_match_workload(args, world, rank, local):
+    """k = 2 Hamming matching only: 65536 queries x 65536 database rows (uniform
+    256-bit rows, half the queries near-duplicates with p = 0.05 bit flips), L2
+    flushed before each step; metric match-pairs/s."""
+    import torch
+
+    import orbx
+    import synth
+
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    dbh, qh, _ = synth.match_workload(65536, 65536, seed=rank)
+    q = torch.from_numpy(qh).to(dev)
+    db = torch.from_numpy(dbh).to(dev)
+    stream = torch.cuda.Stream(device=dev)
+    ctx = orbx.Context(local, orbx.make_params(max_pts=1000), stream=stream)
+    mode = orbx.MATCH_IMMA if args.match_mode == "imma" else orbx.MATCH_POPC
+    flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device=dev)
+    steps = max(1, min(args.steps, 200))
+    with torch.cuda.stream(stream):
+        for _ in range(max(args.warmup, 3)):
+            orbx.knn2(ctx, q, db, mode)
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+        barrier(world)
+        torch.cuda.synchronize(dev)
+        for e0, e1 in ev:
+            flush.zero_()
+            e0.record(stream)
+            orbx.knn2(ctx, q, db, mode)
+            e1.record(stream)
+        torch.cuda.synchronize(dev)
+        barrier(world)
+    total_ms = max_over_ranks(sum(e0.elapsed_time(e1) for e0, e1 in ev), world)
+    ctx.close()
+    if rank != 0:
+        return None
+    pairs = 65536.0 * 65536.0 * world
+    return {"metric": "Hamming match-pairs/s (exact, k=2, 65536 x 65536)", "value": pairs * steps / (total_ms * 1e-3),
+            "unit": "pairs/s", "n_gpus": world, "steps": steps, "warmup": args.warmup,
+            "ms_per_step": total_ms / steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "int8" if mode == orbx.MATCH_IMMA else "u32", "data": "synthetic (cuda-orb_b200/synth.py)",
+            "config": {"workload": f"k=2 matching 65536 x 65536, {args.match_mode} form",
+                       "l2": "flushed before every step"},
+            "gpu_launches": 3 * steps if mode == orbx.MATCH_IMMA else steps}
+
+
 def main(argv=None):
     args = parse_args(argv)
     world, rank, local = dist_setup()
+    if args.workload == "match65536":
+        res = run_match_workload(args, world, rank, local)
+        if rank == 0 and res is not None:
+            print(json.dumps(res), flush=True)
+        if world > 1:
+            import torch.distributed as dist
+
+            dist.barrier()
+            dist.destroy_process_group()
+        return
     if args.impl == "reference":
         res = run_reference(args, world, rank, local)
     else:
