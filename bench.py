@@ -53,9 +53,11 @@ def parse_args(argv=None):
     p.add_argument("--impl", choices=["orbx", "reference"], default="orbx")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-match-bench", action="store_true")
-    p.add_argument("--workload", choices=["pair1080", "match65536"], default="pair1080",
-                   help="pair1080: the 1920x1080 pair (default); match65536: k=2 matching only")
+    p.add_argument("--workload", choices=["pair1080", "match65536", "batch64"], default="pair1080",
+                   help="pair1080: the 1920x1080 pair (default); match65536: k=2 matching only; "
+                        "batch64: 64 pairs of mixed resolution and caps in one batch")
     p.add_argument("--match-mode", choices=["imma", "popc"], default="imma")
+    p.add_argument("--no-autotune", action="store_true", help="batch64: keep the default launch shapes")
     return p.parse_args(argv)
 
 
@@ -520,11 +522,99 @@ def run_match_workload(args, world, rank, local):
             "gpu_launches": 3 * steps if mode == orbx.MATCH_IMMA else steps}
 
 
+BATCH_SIZES = [(320, 240), (640, 480), (1280, 720), (1920, 1080), (3840, 2160)]
+
+
+def batch64_layout(n_pairs=64, seed=0x0C3000):
+    """Resolutions uniform over BATCH_SIZES and keypoint caps uniform in [500, 10000]."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    sizes = [BATCH_SIZES[int(i)] for i in rng.integers(0, len(BATCH_SIZES), n_pairs)]
+    caps = [int(c) for c in rng.integers(500, 10001, n_pairs)]
+    return [(w, h, c) for (w, h), c in zip(sizes, caps)]
+
+
+def run_batch_workload(args, world, rank, local):
+    """64 frame pairs of mixed resolution and caps: detect + describe every image
+    and match every pair in shared launches (one CUDA graph), autotuned."""
+    import torch
+
+    import orbx
+    import synth
+
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    layout = batch64_layout()
+    pairs = []
+    for k, (w, h, cap) in enumerate(layout):
+        a, b, _ = synth.make_pair(w, h, seed=1000 * rank + k)
+        pairs.append((a, b, w, h, cap))
+    stream = torch.cuda.Stream(device=dev)
+    ctx = orbx.Context(local, orbx.make_params(max_pts=10000), stream=stream)
+    pb = orbx.PairBatch(pairs, dev)
+    flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device=dev)
+    with torch.cuda.stream(stream):
+        if args.no_autotune:
+            tuned, tuned_ms = ctx.get_tuning(), None
+        else:
+            tuned, tuned_ms = ctx.autotune_pairs(pb, reps=3)
+        for _ in range(max(args.warmup, 3)):
+            ctx.batch_pairs(pb)
+        steps = max(1, min(args.steps, 200))
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+        sampler = ClockSampler(local)
+        if rank == 0:
+            sampler.start()
+        barrier(world)
+        torch.cuda.synchronize(dev)
+        for e0, e1 in ev:
+            flush.zero_()
+            e0.record(stream)
+            ctx.batch_pairs(pb)
+            e1.record(stream)
+        torch.cuda.synchronize(dev)
+        barrier(world)
+        clocks = sampler.stop() if rank == 0 else None
+    total_ms = max_over_ranks(sum(e0.elapsed_time(e1) for e0, e1 in ev), world)
+    with torch.cuda.stream(stream):
+        acc = np.zeros(5)
+        for _ in range(10):
+            flush.zero_()
+            acc += ctx.profile_batch(pb)
+        stage_ms = acc / 10
+    nkp = 0
+    in_bytes = 0
+    for i, (a, b, w, h, cap) in enumerate(pairs):
+        A, B = pb.outs[i]
+        nkp += int(A.count.item()) + int(B.count.item())
+        in_bytes += 2 * w * h
+    ctx.close()
+    if rank != 0:
+        return None
+    ms = total_ms / steps
+    # algorithmic bytes per batch: every image read once, 28 + 32 bytes out per keypoint
+    alg = in_bytes + nkp * 60
+    peaks, peak_kind = load_peaks()
+    gbs = alg / (ms * 1e-3) / 1e9
+    return {"metric": "ms per batch of 64 frame pairs (detect+describe+match)", "value": ms, "unit": "ms",
+            "n_gpus": world, "steps": steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": False,
+            "scaling": "weak", "vs_baseline": None, "dtype": "u8", "data": "synthetic (cuda-orb_b200/synth.py)",
+            "config": {"workload": "64 pairs, resolutions uniform over 320x240..3840x2160, caps U[500,10000]",
+                       "pixels": in_bytes, "keypoints": nkp, "tuning": tuned.as_dict(), "autotune_ms": tuned_ms,
+                       "l2": "flushed before every step", "graph": "one CUDA graph per batch (5 kernels)"},
+            "pairs_per_s": 64 * 1000.0 / ms,
+            "roofline": {"kernel": "whole batch", "bound": "hbm", "achieved": gbs, "peak": peaks["hbm_gbs"],
+                         "unit": "GB/s", "frac": gbs / peaks["hbm_gbs"], "algorithmic_bytes": alg,
+                         "peak_kind": f"{peak_kind} hbm_gbs"},
+            "kernels": {k: {"ms": float(v)} for k, v in
+                        zip(["pyramid_blur", "detect", "nms", "describe", "match"], stage_ms)},
+            "gpu_launches": 5 * steps, "clocks": clocks}
+
+
 def main(argv=None):
     args = parse_args(argv)
     world, rank, local = dist_setup()
-    if args.workload == "match65536":
-        res = run_match_workload(args, world, rank, local)
+    if args.workload in ("match65536", "batch64"):
+        res = (run_match_workload if args.workload == "match65536" else run_batch_workload)(args, world, rank, local)
         if rank == 0 and res is not None:
             print(json.dumps(res), flush=True)
         if world > 1:

@@ -6,6 +6,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <algorithm>
 #include <vector>
 
 #include "orb_pattern31.h"
@@ -23,8 +24,9 @@ struct Workspace {
   size_t guard = 0;              // zeroed bytes before and after each pyramid
   uint8_t* pyr_alloc = nullptr;  // guard + obytes + guard
   uint8_t* blr_alloc = nullptr;
-  float* vmap = nullptr;
-  int* layer = nullptr;
+  float* vmap = nullptr;     // scores, valid where occ is set
+  uint8_t* oct8 = nullptr;   // octaves, valid where occ is set
+  uint32_t* occ = nullptr;   // occupancy bits
   unsigned long long* nms_status = nullptr;
   int* total = nullptr;
   int nms_strips = 0;
@@ -92,6 +94,21 @@ struct orbx_ctx {
   int* io_count_host = nullptr;  // pinned [2]
   int io_max_pts = 0;
   cudaEvent_t prof_ev[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
+  // launch shapes (orbx_tuning)
+  int nms_rows = kNmsRows;
+  int describe_bps = 8;
+  int match_bps = 8;
+  int match_blocks_per_pair = 0;
+  // batched pairs
+  std::vector<Workspace> bws;
+  BatchSlot batch;
+  MatchJob* d_jobs = nullptr;
+  int jobs_cap = 0;
+  uint32_t* batch_part = nullptr;
+  unsigned int* batch_tile_done = nullptr;
+  size_t batch_part_words = 0, batch_tile_words = 0;
+  std::vector<uint8_t> batch_key;
+  cudaGraphExec_t batch_exec = nullptr;
 };
 
 #define ORBX_CUDA(x)                   \
@@ -242,7 +259,8 @@ static void ws_free(Workspace& ws) {
   cudaFree(ws.pyr_alloc);
   cudaFree(ws.blr_alloc);
   cudaFree(ws.vmap);
-  cudaFree(ws.layer);
+  cudaFree(ws.oct8);
+  cudaFree(ws.occ);
   cudaFree(ws.nms_status);
   cudaFree(ws.total);
   ws = Workspace();
@@ -263,24 +281,38 @@ static int ws_ensure(orbx_ctx* c, Workspace& ws, int w, int h, int noct_req = -1
   const size_t alloc = ws.obytes + 2 * ws.guard;
   const size_t npx = (size_t)h * ws.oszp[3 * n];
   const int border = c->p.edge_threshold < 3 ? 3 : c->p.edge_threshold;
-  ws.nms_strips = (h - 2 * border > 0 && w - 2 * border > 0) ? div_up(h - 2 * border, kNmsRows) : 0;
+  ws.nms_strips = (h - 2 * border > 0 && w - 2 * border > 0) ? div_up(h - 2 * border, c->nms_rows) : 0;
   ORBX_CUDA(cudaMalloc(&ws.pyr_alloc, alloc));
   ORBX_CUDA(cudaMalloc(&ws.blr_alloc, alloc));
   ORBX_CUDA(cudaMalloc(&ws.vmap, npx * sizeof(float)));
-  ORBX_CUDA(cudaMalloc(&ws.layer, npx * sizeof(int)));
-  // look-back words for the smallest border (3), so any border fits
-  const int strips_max = (h - 6 > 0) ? div_up(h - 6, kNmsRows) : 1;
+  ORBX_CUDA(cudaMalloc(&ws.oct8, npx));
+  ORBX_CUDA(cudaMalloc(&ws.occ, npx / 8));
+  // look-back words for the smallest border (3) and one-row strips, so any fits
+  const int strips_max = (h - 6 > 0) ? h - 6 : 1;
   ORBX_CUDA(cudaMalloc(&ws.nms_status, sizeof(unsigned long long) * strips_max));
   ORBX_CUDA(cudaMalloc(&ws.total, sizeof(int)));
   ORBX_CUDA(cudaMemsetAsync(ws.pyr_alloc, 0, alloc, c->stream));
   ORBX_CUDA(cudaMemsetAsync(ws.blr_alloc, 0, alloc, c->stream));
   ORBX_CUDA(cudaMemsetAsync(ws.vmap, 0, npx * sizeof(float), c->stream));
-  ORBX_CUDA(cudaMemsetAsync(ws.layer, 0, npx * sizeof(int), c->stream));
+  ORBX_CUDA(cudaMemsetAsync(ws.oct8, 0, npx, c->stream));
+  // words past the detect tiles (row padding) are never written: they stay empty
+  ORBX_CUDA(cudaMemsetAsync(ws.occ, 0, npx / 8, c->stream));
   return ORBX_OK;
 }
 
+// NMS border, strip height (within the shared-memory budget of occupancy words
+// per strip) and strip count of a frame.
+static void set_nms_shape(Frame& F, int border, int rows_req) {
+  F.border = border < 3 ? 3 : border;
+  const int nw = (F.w - 2 * F.border > 0) ? ((F.w - F.border - 1) >> 5) - (F.border >> 5) + 1 : 1;
+  int rows = rows_req < 1 ? 1 : rows_req;
+  if (rows * nw > kNmsMaxWords) rows = kNmsMaxWords / nw > 0 ? kNmsMaxWords / nw : 1;
+  F.nms_rows = rows;
+  F.nms_strips = (F.h - 2 * F.border > 0 && F.w - 2 * F.border > 0) ? div_up(F.h - 2 * F.border, rows) : 0;
+}
+
 static void fill_frame(const orbx_ctx* c, const Workspace& ws, const uint8_t* img, int pitch_in, orbx_point* pts,
-                       uint8_t* desc, int* count, Frame& F) {
+                       uint8_t* desc, int* count, Frame& F, int max_pts = -1) {
   std::memset(&F, 0, sizeof(F));
   const int n = ws.n;
   F.img = img;
@@ -297,12 +329,14 @@ static void fill_frame(const orbx_ctx* c, const Workspace& ws, const uint8_t* im
   F.pyr = ws.pyr_alloc + ws.guard;
   F.blr = ws.blr_alloc + ws.guard;
   F.vmap = ws.vmap;
-  F.layer = ws.layer;
+  F.oct8 = ws.oct8;
+  F.occ = ws.occ;
+  F.layer = nullptr;
   F.pts = pts;
   F.desc = desc;
   F.count = count;
   F.total = ws.total;
-  F.max_pts = c->p.max_pts;
+  F.max_pts = max_pts > 0 ? max_pts : c->p.max_pts;
   F.border = c->p.edge_threshold < 3 ? 3 : c->p.edge_threshold;
   int acc = 0;
   for (int o = 0; o < n; o++) {
@@ -314,7 +348,7 @@ static void fill_frame(const orbx_ctx* c, const Workspace& ws, const uint8_t* im
   F.pyr_tile_base[n] = acc;
   F.det_tiles_x = div_up(F.w, kDetTW);
   F.det_tiles_y = div_up(F.h, kDetTH);
-  F.nms_strips = ws.nms_strips;
+  set_nms_shape(F, F.border, c->nms_rows);
   F.nms_status = ws.nms_status;
 }
 
@@ -396,7 +430,7 @@ static int launch_frames(orbx_ctx* c, const LaunchPlan& pl, bool compute_desc) {
   ORBX_CUDA(launch_pyramid_blur(pl.b, pl.pyr_tiles, c->stream));
   ORBX_CUDA(launch_detect(pl.b, pl.det_tiles, c->stream));
   ORBX_CUDA(launch_nms(pl.b, pl.nms_strips, c->stream));
-  if (compute_desc) ORBX_CUDA(launch_describe(pl.b, pl.total_max_pts, c->stream));
+  if (compute_desc) ORBX_CUDA(launch_describe(pl.b, pl.total_max_pts, c->stream, c->describe_bps));
   return ORBX_OK;
 }
 
@@ -475,17 +509,15 @@ int lower_detect(orbx_ctx* c, const uint8_t* image, uint8_t* octave_images, floa
   if (!image || !pts || !d_count) return ORBX_ERR_ARG;
   Frame F;
   fill_frame(c, *ws, image, ws->oszp[3 * noctaves], pts, nullptr, d_count, F);
-  F.border = border < 3 ? 3 : border;
-  F.nms_strips = (F.h - 2 * F.border > 0 && F.w - 2 * F.border > 0) ? div_up(F.h - 2 * F.border, kNmsRows) : 0;
+  set_nms_shape(F, border, c->nms_rows);
   rc = lower_run(c, *ws, F, 0, kDescribeBoth, threshold, harris ? 1 : 0, c->p.wta_k, c->half_k, 0);
   if (rc) return rc;
   const size_t npx = (size_t)ws->h * ws->oszp[3 * noctaves];
   if (octave_images)
     ORBX_CUDA(cudaMemcpyAsync(octave_images, ws->pyr_alloc + ws->guard, ws->obytes, cudaMemcpyDeviceToDevice, c->stream));
-  if (vmem) {
-    ORBX_CUDA(cudaMemcpyAsync(vmem, ws->vmap, npx * sizeof(float), cudaMemcpyDeviceToDevice, c->stream));
-    ORBX_CUDA(cudaMemcpyAsync(vmem + npx, ws->layer, npx * sizeof(int), cudaMemcpyDeviceToDevice, c->stream));
-  }
+  if (vmem)
+    ORBX_CUDA(launch_expand_score_map(c->single.d_frames, vmem, reinterpret_cast<int*>(vmem + npx), (long long)npx,
+                                      c->stream));
   return ORBX_OK;
 }
 
@@ -613,6 +645,16 @@ ORBX_API int orbx_destroy(orbx_ctx* c) {
     if (e) cudaEventDestroy(e);
   cudaFree(c->imma_q);
   cudaFree(c->imma_db);
+  for (auto& ws : c->bws) ws_free(ws);
+  cudaFree(c->batch.d_frames);
+  cudaFree(c->batch.d_bases);
+  cudaFree(c->batch.d_ticket);
+  cudaFreeHost(c->batch.h_stage);
+  if (c->batch.uploaded) cudaEventDestroy(c->batch.uploaded);
+  cudaFree(c->d_jobs);
+  cudaFree(c->batch_part);
+  cudaFree(c->batch_tile_done);
+  if (c->batch_exec) cudaGraphExecDestroy(c->batch_exec);
   cudaFree(c->d_pattern);
   cudaFree(c->d_umax);
   cudaFree(c->d_err);
@@ -756,7 +798,7 @@ static int launch_match(orbx_ctx* c, MatchWork& mw, const MatchArgs& a, int nq_c
   int rc = mw_ensure(mw, nq_cap);
   if (rc) return rc;
   if (mode == ORBX_MATCH_POPC) {
-    ORBX_CUDA(launch_match_popc(a, mw, c->stream));
+    ORBX_CUDA(launch_match_popc(a, mw, c->stream, c->match_bps));
     return ORBX_OK;
   }
   if ((rc = imma_ensure(c, nq_cap, ndb_cap)) != 0) return rc;
@@ -972,6 +1014,269 @@ ORBX_API int orbx_profile_pair(orbx_ctx* c, const uint8_t* d_img_a, const uint8_
   return ORBX_OK;
 }
 
+ORBX_API int orbx_get_tuning(orbx_ctx* c, orbx_tuning* t) {
+  if (!c || !t) return ORBX_ERR_ARG;
+  t->nms_rows = c->nms_rows;
+  t->describe_blocks_per_sm = c->describe_bps;
+  t->match_blocks_per_sm = c->match_bps;
+  t->match_blocks_per_pair = c->match_blocks_per_pair;
+  return ORBX_OK;
+}
+
+ORBX_API int orbx_set_tuning(orbx_ctx* c, const orbx_tuning* t) {
+  if (!c || !t) return ORBX_ERR_ARG;
+  if (t->nms_rows < 1 || t->nms_rows > kNmsMaxRows || t->describe_blocks_per_sm < 1 ||
+      t->describe_blocks_per_sm > 64 || t->match_blocks_per_sm < 1 || t->match_blocks_per_sm > 64 ||
+      t->match_blocks_per_pair < 0 || t->match_blocks_per_pair > 4096)
+    return ORBX_ERR_ARG;
+  c->nms_rows = t->nms_rows;
+  c->describe_bps = t->describe_blocks_per_sm;
+  c->match_bps = t->match_blocks_per_sm;
+  c->match_blocks_per_pair = t->match_blocks_per_pair;
+  // cached graphs baked in the old shapes
+  if (c->pg.exec) {
+    cudaGraphExecDestroy(c->pg.exec);
+    c->pg.exec = nullptr;
+  }
+  c->pg.valid = false;
+  c->single.last.clear();
+  c->pair.last.clear();
+  return ORBX_OK;
+}
+
+static constexpr int kBatchSplitsCap = 16;
+
+static int batch_pairs_impl(orbx_ctx* c, int n_pairs, const orbx_image* ia, const orbx_image* ib,
+                            const orbx_frame_out* oa, const orbx_frame_out* ob, int mode, float* stage_ms) {
+  if (!c || n_pairs < 0 || (n_pairs > 0 && (!ia || !ib || !oa || !ob))) return ORBX_ERR_ARG;
+  if (!c->inited) return ORBX_ERR_STATE;
+  if (n_pairs == 0) return ORBX_OK;
+  if (2 * n_pairs > kMaxFramesPerLaunch) return ORBX_ERR_SIZE;
+  if (mode != ORBX_MATCH_POPC && mode != ORBX_MATCH_AUTO) return ORBX_ERR_ARG;
+  int rc;
+  for (int i = 0; i < n_pairs; i++) {
+    for (const orbx_image* im : {&ia[i], &ib[i]}) {
+      if ((rc = check_image(c, im->data, im->w, im->h, im->pitch)) != 0) return rc;
+    }
+    for (const orbx_frame_out* o : {&oa[i], &ob[i]}) {
+      if (!o->points || !o->desc || !o->num_pts || o->max_pts < 1 || o->max_pts > (1 << 22) - 1) return ORBX_ERR_ARG;
+    }
+  }
+  DeviceGuard g(c->device);
+  if ((int)c->bws.size() < 2 * n_pairs) c->bws.resize(2 * n_pairs);
+  std::vector<Frame> frames(2 * n_pairs);
+  for (int i = 0; i < n_pairs; i++) {
+    for (int s = 0; s < 2; s++) {
+      const orbx_image& im = s ? ib[i] : ia[i];
+      const orbx_frame_out& o = s ? ob[i] : oa[i];
+      Workspace& ws = c->bws[2 * i + s];
+      if ((rc = ws_ensure(c, ws, im.w, im.h)) != 0) return rc;
+      fill_frame(c, ws, im.data, im.pitch, o.points, o.desc, o.num_pts, frames[2 * i + s], o.max_pts);
+    }
+  }
+  LaunchPlan pl;
+  if ((rc = upload_batch(c, c->batch, frames, &pl)) != 0) return rc;
+  // matching jobs, one per pair, with their own slices of the split scratch
+  int max_tiles = 1;
+  size_t part_words = 0, tile_words = 0;
+  std::vector<MatchJob> jobs(n_pairs);
+  for (int i = 0; i < n_pairs; i++) {
+    const int nq_cap = oa[i].max_pts;
+    max_tiles = std::max(max_tiles, div_up(nq_cap, 128));
+    part_words += (size_t)2 * kBatchSplitsCap * nq_cap;
+    tile_words += (size_t)div_up(nq_cap, 128);
+  }
+  if (c->batch_part_words < part_words || c->batch_tile_words < tile_words) {
+    cudaStreamSynchronize(c->stream);
+    cudaFree(c->batch_part);
+    cudaFree(c->batch_tile_done);
+    c->batch_part = nullptr;
+    c->batch_tile_done = nullptr;
+    c->batch_part_words = c->batch_tile_words = 0;
+    ORBX_CUDA(cudaMalloc(&c->batch_part, part_words * sizeof(uint32_t)));
+    ORBX_CUDA(cudaMalloc(&c->batch_tile_done, tile_words * sizeof(unsigned int)));
+    ORBX_CUDA(cudaMemset(c->batch_tile_done, 0, tile_words * sizeof(unsigned int)));
+    c->batch_part_words = part_words;
+    c->batch_tile_words = tile_words;
+    if (c->batch_exec) {
+      cudaGraphExecDestroy(c->batch_exec);
+      c->batch_exec = nullptr;
+    }
+    c->batch_key.clear();
+  }
+  {
+    size_t po = 0, to = 0;
+    for (int i = 0; i < n_pairs; i++) {
+      MatchJob& J = jobs[i];
+      std::memset(&J, 0, sizeof(J));
+      J.args.q = oa[i].desc;
+      J.args.db = ob[i].desc;
+      J.args.nq = oa[i].max_pts;
+      J.args.ndb = ob[i].max_pts;
+      J.args.d_nq = oa[i].num_pts;
+      J.args.d_ndb = ob[i].num_pts;
+      J.args.pts = oa[i].points;
+      J.work.part = c->batch_part + po;
+      J.work.tile_done = c->batch_tile_done + to;
+      J.work.nq_cap = oa[i].max_pts;
+      J.work.splits_cap = kBatchSplitsCap;
+      po += (size_t)2 * kBatchSplitsCap * oa[i].max_pts;
+      to += (size_t)div_up(oa[i].max_pts, 128);
+    }
+  }
+  int blocks_per_pair = c->match_blocks_per_pair;
+  if (blocks_per_pair <= 0) blocks_per_pair = std::max(max_tiles, div_up(8 * 148, n_pairs));
+  blocks_per_pair = std::max(blocks_per_pair, max_tiles);  // every query tile needs a block
+  // graph key: frames, jobs and launch shapes
+  std::vector<uint8_t> key(sizeof(MatchJob) * n_pairs + c->batch.last.size() + 4 * sizeof(int));
+  {
+    uint8_t* k = key.data();
+    std::memcpy(k, jobs.data(), sizeof(MatchJob) * n_pairs);
+    k += sizeof(MatchJob) * n_pairs;
+    std::memcpy(k, c->batch.last.data(), c->batch.last.size());
+    k += c->batch.last.size();
+    const int shapes[4] = {c->nms_rows, c->describe_bps, blocks_per_pair, mode};
+    std::memcpy(k, shapes, sizeof(shapes));
+  }
+  if (stage_ms) {
+    // profiling: the same launches, unrolled, with events between them
+    if (c->jobs_cap < n_pairs) {
+      cudaStreamSynchronize(c->stream);
+      cudaFree(c->d_jobs);
+      c->d_jobs = nullptr;
+      c->jobs_cap = 0;
+      ORBX_CUDA(cudaMalloc(&c->d_jobs, sizeof(MatchJob) * n_pairs));
+      c->jobs_cap = n_pairs;
+    }
+    ORBX_CUDA(cudaMemcpyAsync(c->d_jobs, jobs.data(), sizeof(MatchJob) * n_pairs, cudaMemcpyHostToDevice,
+                              c->stream));
+    ORBX_CUDA(cudaStreamSynchronize(c->stream));
+    c->batch_key.clear();  // the device job table may differ from the captured one now
+    for (auto& e : c->prof_ev)
+      if (!e) ORBX_CUDA(cudaEventCreate(&e));
+    ORBX_CUDA(cudaEventRecord(c->prof_ev[0], c->stream));
+    ORBX_CUDA(launch_pyramid_blur(pl.b, pl.pyr_tiles, c->stream));
+    ORBX_CUDA(cudaEventRecord(c->prof_ev[1], c->stream));
+    ORBX_CUDA(launch_detect(pl.b, pl.det_tiles, c->stream));
+    ORBX_CUDA(cudaEventRecord(c->prof_ev[2], c->stream));
+    ORBX_CUDA(launch_nms(pl.b, pl.nms_strips, c->stream));
+    ORBX_CUDA(cudaEventRecord(c->prof_ev[3], c->stream));
+    ORBX_CUDA(launch_describe(pl.b, pl.total_max_pts, c->stream, c->describe_bps));
+    ORBX_CUDA(cudaEventRecord(c->prof_ev[4], c->stream));
+    ORBX_CUDA(launch_match_popc_batch(c->d_jobs, n_pairs, blocks_per_pair, c->stream));
+    ORBX_CUDA(cudaEventRecord(c->prof_ev[5], c->stream));
+    ORBX_CUDA(cudaEventSynchronize(c->prof_ev[5]));
+    for (int i = 0; i < 5; i++) ORBX_CUDA(cudaEventElapsedTime(&stage_ms[i], c->prof_ev[i], c->prof_ev[i + 1]));
+    return ORBX_OK;
+  }
+  if (!(c->batch_exec && c->batch_key == key)) {
+    if (c->batch_exec) {
+      cudaGraphExecDestroy(c->batch_exec);
+      c->batch_exec = nullptr;
+    }
+    if (c->jobs_cap < n_pairs) {
+      cudaStreamSynchronize(c->stream);
+      cudaFree(c->d_jobs);
+      c->d_jobs = nullptr;
+      c->jobs_cap = 0;
+      ORBX_CUDA(cudaMalloc(&c->d_jobs, sizeof(MatchJob) * n_pairs));
+      c->jobs_cap = n_pairs;
+    }
+    ORBX_CUDA(cudaMemcpyAsync(c->d_jobs, jobs.data(), sizeof(MatchJob) * n_pairs, cudaMemcpyHostToDevice,
+                              c->stream));
+    ORBX_CUDA(cudaStreamSynchronize(c->stream));
+    cudaGraph_t graph = nullptr;
+    ORBX_CUDA(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+    int lrc = launch_frames(c, pl, true);
+    if (lrc == ORBX_OK)
+      lrc = launch_match_popc_batch(c->d_jobs, n_pairs, blocks_per_pair, c->stream) == cudaSuccess ? ORBX_OK
+                                                                                                     : ORBX_ERR_CUDA;
+    const cudaError_t ce = cudaStreamEndCapture(c->stream, &graph);
+    if (lrc != ORBX_OK) {
+      if (graph) cudaGraphDestroy(graph);
+      return lrc;
+    }
+    ORBX_CUDA(ce);
+    const cudaError_t ie = cudaGraphInstantiate(&c->batch_exec, graph, 0);
+    cudaGraphDestroy(graph);
+    ORBX_CUDA(ie);
+    c->batch_key.swap(key);
+  }
+  ORBX_CUDA(cudaGraphLaunch(c->batch_exec, c->stream));
+  return ORBX_OK;
+}
+
+ORBX_API int orbx_batch_pairs(orbx_ctx* c, int n_pairs, const orbx_image* ia, const orbx_image* ib,
+                              const orbx_frame_out* oa, const orbx_frame_out* ob, int mode) {
+  return batch_pairs_impl(c, n_pairs, ia, ib, oa, ob, mode, nullptr);
+}
+
+ORBX_API int orbx_profile_batch(orbx_ctx* c, int n_pairs, const orbx_image* ia, const orbx_image* ib,
+                                const orbx_frame_out* oa, const orbx_frame_out* ob, float* stage_ms) {
+  if (!stage_ms) return ORBX_ERR_ARG;
+  return batch_pairs_impl(c, n_pairs, ia, ib, oa, ob, ORBX_MATCH_POPC, stage_ms);
+}
+
+ORBX_API int orbx_autotune_pairs(orbx_ctx* c, int n_pairs, const orbx_image* ia, const orbx_image* ib,
+                                 const orbx_frame_out* oa, const orbx_frame_out* ob, int reps, orbx_tuning* best,
+                                 float* best_ms) {
+  if (!c || reps < 1) return ORBX_ERR_ARG;
+  DeviceGuard g(c->device);
+  orbx_tuning keep;
+  orbx_get_tuning(c, &keep);
+  cudaEvent_t e0, e1;
+  ORBX_CUDA(cudaEventCreate(&e0));
+  ORBX_CUDA(cudaEventCreate(&e1));
+  const int rows_c[] = {2, 4, 8, 16};
+  const int desc_c[] = {4, 8, 16};
+  const int match_c[] = {0, 64, 256};
+  orbx_tuning top = keep;
+  float top_ms = 1e30f;
+  int rc = ORBX_OK;
+  for (int r : rows_c) {
+    for (int d : desc_c) {
+      for (int m : match_c) {
+        orbx_tuning t = keep;
+        t.nms_rows = r;
+        t.describe_blocks_per_sm = d;
+        t.match_blocks_per_pair = m;
+        if ((rc = orbx_set_tuning(c, &t)) != 0) goto done;
+        if ((rc = orbx_batch_pairs(c, n_pairs, ia, ib, oa, ob, ORBX_MATCH_POPC)) != 0) goto done;  // capture
+        std::vector<float> ms;
+        for (int k = 0; k < reps; k++) {
+          cudaEventRecord(e0, c->stream);
+          if ((rc = orbx_batch_pairs(c, n_pairs, ia, ib, oa, ob, ORBX_MATCH_POPC)) != 0) goto done;
+          cudaEventRecord(e1, c->stream);
+          if (cudaEventSynchronize(e1) != cudaSuccess) {
+            rc = ORBX_ERR_CUDA;
+            goto done;
+          }
+          float v = 0.f;
+          cudaEventElapsedTime(&v, e0, e1);
+          ms.push_back(v);
+        }
+        std::sort(ms.begin(), ms.end());
+        const float med = ms[ms.size() / 2];
+        if (med < top_ms) {
+          top_ms = med;
+          top = t;
+        }
+      }
+    }
+  }
+done:
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (rc != ORBX_OK) {
+    orbx_set_tuning(c, &keep);
+    return rc;
+  }
+  orbx_set_tuning(c, &top);
+  if (best) *best = top;
+  if (best_ms) *best_ms = top_ms;
+  return orbx_sync(c);
+}
+
 ORBX_API int orbx_debug_buffers(orbx_ctx* c, uint8_t* h_pyr, uint8_t* h_blur, float* h_vmap, int* h_layer,
                                 int* h_total) {
   if (!c) return ORBX_ERR_ARG;
@@ -982,8 +1287,23 @@ ORBX_API int orbx_debug_buffers(orbx_ctx* c, uint8_t* h_pyr, uint8_t* h_blur, fl
   const size_t npx = (size_t)ws.h * ws.oszp[3 * ws.n];
   if (h_pyr) ORBX_CUDA(cudaMemcpy(h_pyr, ws.pyr_alloc + ws.guard, ws.obytes, cudaMemcpyDeviceToHost));
   if (h_blur) ORBX_CUDA(cudaMemcpy(h_blur, ws.blr_alloc + ws.guard, ws.obytes, cudaMemcpyDeviceToHost));
-  if (h_vmap) ORBX_CUDA(cudaMemcpy(h_vmap, ws.vmap, npx * sizeof(float), cudaMemcpyDeviceToHost));
-  if (h_layer) ORBX_CUDA(cudaMemcpy(h_layer, ws.layer, npx * sizeof(int), cudaMemcpyDeviceToHost));
+  if (h_vmap || h_layer) {
+    // the dense reference-layout maps of the last single-image call
+    float* dv = nullptr;
+    int* dl = nullptr;
+    ORBX_CUDA(cudaMalloc(&dv, npx * sizeof(float)));
+    if (cudaMalloc(&dl, npx * sizeof(int)) != cudaSuccess) {
+      cudaFree(dv);
+      return ORBX_ERR_NOMEM;
+    }
+    cudaError_t e = launch_expand_score_map(c->single.d_frames, dv, dl, (long long)npx, c->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    if (e == cudaSuccess && h_vmap) e = cudaMemcpy(h_vmap, dv, npx * sizeof(float), cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess && h_layer) e = cudaMemcpy(h_layer, dl, npx * sizeof(int), cudaMemcpyDeviceToHost);
+    cudaFree(dv);
+    cudaFree(dl);
+    ORBX_CUDA(e);
+  }
   if (h_total) ORBX_CUDA(cudaMemcpy(h_total, ws.total, sizeof(int), cudaMemcpyDeviceToHost));
   return ORBX_OK;
 }

@@ -147,11 +147,11 @@ __global__ void __launch_bounds__(kDescWarps * 32) k_describe(Batch b) {
   }
 }
 
-cudaError_t launch_describe(const Batch& b, int total_max_pts, cudaStream_t s) {
+cudaError_t launch_describe(const Batch& b, int total_max_pts, cudaStream_t s, int blocks_per_sm) {
   if (total_max_pts <= 0) return cudaSuccess;
   int warps_needed = total_max_pts;
   int blocks = (warps_needed + kDescWarps - 1) / kDescWarps;
-  const int cap = 148 * 8;
+  const int cap = 148 * (blocks_per_sm > 0 ? blocks_per_sm : 8);
   if (blocks > cap) blocks = cap;
   if (b.wta_k == 3)
     k_describe<3><<<blocks, kDescWarps * 32, 0, s>>>(b);

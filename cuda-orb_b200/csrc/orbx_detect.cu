@@ -147,8 +147,8 @@ __global__ void __launch_bounds__(256) k_pyramid_blur(Batch b) {
 // into it; it stages each octave's pixels with a 4-pixel halo (the Harris
 // window with its Sobel reach) in shared memory using the pyramid's linear
 // addressing, so reads past an octave edge return the same neighbouring bytes
-// as in the reference, merges the octaves in shared memory, and writes its
-// region of the score map densely (no clearing pass is needed).
+// as in the reference, merges the octaves in shared memory, and writes the
+// tile's occupancy bits densely and its scores sparsely (no clearing pass).
 // ---------------------------------------------------------------------------
 constexpr int kHalo = 4;
 __host__ __device__ constexpr int det_stage_bytes() {
@@ -303,12 +303,13 @@ __global__ void __launch_bounds__(256, 4) k_detect(Batch b) {
     if (threadIdx.x == 0) s_ncand = 0;
     __syncthreads();
     // phase A: segment test, corners appended to a shared list
+    const int tw_log = 6 - o;  // tw = kDetTW >> o = 1 << tw_log
     for (int i0 = 0; i0 < tw * th; i0 += blockDim.x) {
       const int i = i0 + threadIdx.x;
       bool corner = false;
       if (i < tw * th) {
-        const int ly = i / tw;
-        const int lx = i - ly * tw;
+        const int ly = i >> tw_log;
+        const int lx = i & (tw - 1);
         const int x = xb + lx, y = yb + ly;
         if (x >= 3 && x < ow - 3 && y >= 3 && y < oh - 3)
           corner = fast9(stage + (ly + kHalo) * sw + (lx + kHalo), sw, thr);
@@ -326,8 +327,8 @@ __global__ void __launch_bounds__(256, 4) k_detect(Batch b) {
     const int nc = s_ncand;
     for (int j = threadIdx.x; j < nc; j += blockDim.x) {
       const int i = s_cand[j];
-      const int ly = i / tw;
-      const int lx = i - ly * tw;
+      const int ly = i >> tw_log;
+      const int lx = i & (tw - 1);
       const uint8_t* c = stage + (ly + kHalo) * sw + (lx + kHalo);
       float score;
       if (b.harris) {
@@ -349,15 +350,25 @@ __global__ void __launch_bounds__(256, 4) k_detect(Batch b) {
     __syncthreads();
   }
 
+  // Output: occupancy bits for the whole tile (every word written, so no
+  // clearing pass), scores and octaves only where a score was stored.  The
+  // tile's 64 columns are two aligned 32-bit words of each row (pitch0 is a
+  // multiple of 128).
   const int p0 = F.op[0];
-  for (int i = threadIdx.x; i < kDetTH * kDetTW; i += blockDim.x) {
-    const int r = i / kDetTW;
-    const int c = i - r * kDetTW;
-    const int X = X0 + c, Y = Y0 + r;
-    if (X < F.w && Y < F.h) {
-      const size_t a = (size_t)Y * p0 + X;
-      F.vmap[a] = s_map[i];
-      F.layer[a] = s_oct[i];
+  const int warp = threadIdx.x >> 5;
+  for (int k = warp; k < kDetTH * (kDetTW / 32); k += blockDim.x >> 5) {
+    const int r = k >> 1;
+    const int c = ((k & 1) << 5) + lane;
+    const float v = s_map[r * kDetTW + c];
+    const uint32_t m = __ballot_sync(0xffffffffu, v > 0.f);
+    const int Y = Y0 + r;
+    if (Y < F.h) {
+      const size_t a = (size_t)Y * p0 + X0 + c;
+      if (lane == 0) F.occ[a >> 5] = m;
+      if (v > 0.f) {
+        F.vmap[a] = v;
+        F.oct8[a] = (uint8_t)s_oct[r * kDetTW + c];
+      }
     }
   }
 }
@@ -369,20 +380,14 @@ __global__ void __launch_bounds__(256, 4) k_detect(Batch b) {
 // octave o survives unless a neighbour in the square of radius 2^o has a larger
 // score, or an equal one at dx <= 0 && dy <= 0.  The reference appends
 // survivors with atomicInc (order and, past max_pts, the kept subset depend on
-// scheduling).  Here each block takes a full-width strip of kNmsRows rows in
+// scheduling).  Here each block takes a full-width strip of F.nms_rows rows in
 // ticket order, ranks its survivors with warp ballots, and chains strip totals
 // with a decoupled look-back, so keypoints come out in raster order and the cap
 // keeps the first max_pts of them.
 // ---------------------------------------------------------------------------
-constexpr int kNmsMaxChunks = 256;
 constexpr unsigned long long kFlagAgg = 1ull << 32;
 constexpr unsigned long long kFlagPre = 2ull << 32;
 constexpr int kLookbackSpinLimit = 1 << 22;
-
-// Neighbour rule (gNmsUnroll4, orbd.cu:938-956): positions are addressed
-// linearly like the reference (a column past the edge is the adjacent row's
-// entry); positions outside the map, reachable only with an edge threshold
-// below the window radius 2^o, read as 0.
 
 // Warp 0 of a strip's block resolves the strip's exclusive prefix: it reads the
 // look-back words of up to 32 predecessors per round with acquire loads, and
@@ -417,9 +422,48 @@ __device__ __forceinline__ int nms_lookback(unsigned long long* st, int s, int l
   return excl;
 }
 
+// Neighbour rule of gNmsUnroll4 (orbd.cu:938-956) for the centre at linear
+// index idx (score v, octave o), checked by the whole warp: lane i takes window
+// rows dy = i - r, i + 32 - r, ...; each row is at most two occupancy words, and
+// scores are read only where a bit is set.  Positions are linear like the
+// reference's (a column past the edge is the adjacent row's entry); positions
+// outside the map, reachable only with an edge threshold below 2^o, are empty.
+__device__ __forceinline__ bool nms_keep_warp(const Frame& F, long long idx, float v, int o, int p0, long long npx,
+                                              int lane) {
+  const int r = 1 << o;
+  bool sup = false;
+  for (int dyi = lane; dyi <= 2 * r; dyi += 32) {
+    const int dy = dyi - r;
+    const long long rc = idx + (long long)dy * p0;
+    long long lo = rc - r, hi = rc + r;
+    if (hi < 0 || lo >= npx) continue;
+    if (lo < 0) lo = 0;
+    if (hi >= npx) hi = npx - 1;
+    for (long long wi = lo >> 5; wi <= (hi >> 5) && !sup; wi++) {
+      const long long base = wi << 5;
+      uint32_t m = __ldg(F.occ + wi);
+      if (base < lo) m &= ~0u << (int)(lo - base);
+      if (hi - base < 31) m &= (2u << (int)(hi - base)) - 1u;
+      while (m) {
+        const int bb = __ffs(m) - 1;
+        m &= m - 1u;
+        const long long li = base + bb;
+        if (li == idx) continue;
+        const int dx = (int)(li - rc);
+        const float u = __ldg(F.vmap + li);
+        if (u > v || (u == v && dx <= 0 && dy <= 0)) {
+          sup = true;
+          break;
+        }
+      }
+    }
+  }
+  return !__any_sync(0xffffffffu, sup);
+}
+
 __global__ void __launch_bounds__(256) k_nms(Batch b) {
-  __shared__ uint32_t s_mask[kNmsMaxChunks * 8];
-  __shared__ int s_pref[kNmsMaxChunks * 8];
+  __shared__ uint32_t s_sur[kNmsMaxWords];
+  __shared__ int s_pref[kNmsMaxWords];
   __shared__ int s_warp_tot[8];
   __shared__ int s_ticket, s_base;
 
@@ -430,79 +474,57 @@ __global__ void __launch_bounds__(256) k_nms(Batch b) {
   const Frame& F = b.frames[f];
   const int s = ticket - b.nms_base[f];
   const int border = F.border;
-  const int row0 = border + s * kNmsRows;
-  const int row1 = min(row0 + kNmsRows, F.h - border);
-  const int ncols = F.w - 2 * border;
-  const int npx = (row1 - row0) * ncols;
-  const int nchunks = (npx + 255) >> 8;
+  const int row0 = border + s * F.nms_rows;
+  const int row1 = min(row0 + F.nms_rows, F.h - border);
+  const int xlo = border, xhi = F.w - border;  // columns [xlo, xhi)
+  const int wlo = xlo >> 5, whi = (xhi - 1) >> 5;
+  const int nw = whi - wlo + 1;
+  const int nwords = (row1 - row0) * nw;
   const int p0 = F.op[0];
-  const long long npx_map = (long long)F.h * p0;
-  const float* __restrict__ vmap = F.vmap;
+  const int wpr = p0 >> 5;  // occupancy words per row
+  const long long npx = (long long)F.h * p0;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 
-  // pass 1: survivor masks in raster order.  Four chunks' centre scores are
-  // loaded together; each centre with a score is then checked by the whole warp,
-  // 32 window positions per round, so even the 33x33 window of an octave-4
-  // keypoint costs a few dependent loads.
-  for (int k0 = 0; k0 < nchunks; k0 += 4) {
-    float v[4];
-    long long idx[4];
-#pragma unroll
-    for (int u = 0; u < 4; u++) {
-      const int p = ((k0 + u) << 8) + threadIdx.x;
-      v[u] = 0.f;
-      idx[u] = 0;
-      if (k0 + u < nchunks && p < npx) {
-        const int y = row0 + p / ncols;
-        const int x = border + p % ncols;
-        idx[u] = (long long)y * p0 + x;
-        v[u] = __ldg(vmap + idx[u]);
+  // pass 1: survivor bits of every occupancy word of the strip, in raster order
+  for (int k0 = 0; k0 < nwords; k0 += blockDim.x) {
+    const int k = k0 + threadIdx.x;
+    uint32_t m = 0;
+    int row = 0, cbase = 0;
+    if (k < nwords) {
+      row = row0 + k / nw;
+      const int wj = wlo + k % nw;
+      cbase = wj << 5;
+      m = __ldg(F.occ + (long long)row * wpr + wj);
+      if (cbase < xlo) m &= ~0u << (xlo - cbase);
+      if (xhi - cbase < 32) m &= (xhi - cbase <= 0) ? 0u : ((xhi - cbase == 32) ? ~0u : ((1u << (xhi - cbase)) - 1u));
+    }
+    uint32_t sur = 0;
+    uint32_t lanes = __ballot_sync(0xffffffffu, m != 0u);
+    while (lanes) {
+      const int l = __ffs(lanes) - 1;
+      lanes &= lanes - 1u;
+      uint32_t mm = __shfl_sync(0xffffffffu, m, l);
+      const int crow = __shfl_sync(0xffffffffu, row, l);
+      const int ccb = __shfl_sync(0xffffffffu, cbase, l);
+      while (mm) {
+        const int bit = __ffs(mm) - 1;
+        mm &= mm - 1u;
+        const long long idx = (long long)crow * p0 + ccb + bit;
+        const float v = __ldg(F.vmap + idx);
+        const int o = __ldg(F.oct8 + idx);
+        const bool keep = nms_keep_warp(F, idx, v, o, p0, npx, lane);
+        if (lane == l && keep) sur |= 1u << bit;
       }
     }
-#pragma unroll
-    for (int u = 0; u < 4; u++) {
-      if (k0 + u >= nchunks) break;
-      uint32_t cand = __ballot_sync(0xffffffffu, v[u] > 0.f);
-      uint32_t sur = 0;
-      while (cand) {
-        const int l = __ffs(cand) - 1;
-        cand &= cand - 1u;
-        const long long cidx = __shfl_sync(0xffffffffu, idx[u], l);
-        const float cv = __shfl_sync(0xffffffffu, v[u], l);
-        const int r = 1 << __ldg(F.layer + cidx);
-        const int side = 2 * r + 1;
-        const int npos = side * side;
-        bool sup = false;
-        for (int q0 = 0; q0 < npos; q0 += 32) {
-          const int q = q0 + lane;
-          bool s_ = false;
-          if (q < npos) {
-            const int dy = q / side - r;
-            const int dx = q - (q / side) * side - r;
-            if (dx != 0 || dy != 0) {
-              const long long li = cidx + (long long)dy * p0 + dx;
-              const float uu = (li >= 0 && li < npx_map) ? __ldg(vmap + li) : 0.f;
-              s_ = uu > 0.f && (uu > cv || (uu == cv && dx <= 0 && dy <= 0));
-            }
-          }
-          if (__any_sync(0xffffffffu, s_)) {
-            sup = true;
-            break;
-          }
-        }
-        if (!sup) sur |= 1u << l;
-      }
-      if (lane == 0) s_mask[(k0 + u) * 8 + warp] = sur;
-    }
+    if (k < nwords) s_sur[k] = sur;
   }
   __syncthreads();
 
-  // exclusive scan of the mask popcounts, in (chunk, warp) order
-  const int nent = nchunks * 8;
-  const int per = (nent + 255) >> 8;
-  const int beg = min((int)threadIdx.x * per, nent), end = min(beg + per, nent);
+  // exclusive scan of the survivor counts, in word order
+  const int per = (nwords + 255) >> 8;
+  const int beg = min((int)threadIdx.x * per, nwords), end = min(beg + per, nwords);
   int local = 0;
-  for (int i = beg; i < end; i++) local += __popc(s_mask[i]);
+  for (int i = beg; i < end; i++) local += __popc(s_sur[i]);
   int incl = local;
 #pragma unroll
   for (int d = 1; d < 32; d <<= 1) {
@@ -516,7 +538,7 @@ __global__ void __launch_bounds__(256) k_nms(Batch b) {
   int run = warp_off + incl - local;
   for (int i = beg; i < end; i++) {
     s_pref[i] = run;
-    run += __popc(s_mask[i]);
+    run += __popc(s_sur[i]);
   }
   int strip_total = 0;
   for (int w2 = 0; w2 < 8; w2++) strip_total += s_warp_tot[w2];
@@ -546,26 +568,49 @@ __global__ void __launch_bounds__(256) k_nms(Batch b) {
   const int base = s_base;
   if (base >= F.max_pts) return;
 
-  // pass 2: write survivors
-  for (int k = 0; k < nchunks; k++) {
-    const uint32_t m = s_mask[k * 8 + warp];
-    if (!((m >> lane) & 1u)) continue;
-    const int rank = base + s_pref[k * 8 + warp] + __popc(m & ((1u << lane) - 1u));
-    if (rank >= F.max_pts) continue;
-    const int p = (k << 8) + threadIdx.x;
-    const int y = row0 + p / ncols;
-    const int x = border + p % ncols;
-    const size_t idx = (size_t)y * p0 + x;
-    orbx_point q;
-    q.x = x;
-    q.y = y;
-    q.octave = F.layer[idx];
-    q.score = vmap[idx];
-    q.angle = 0.f;
-    q.match = 0;
-    q.distance = 0;
-    F.pts[rank] = q;
+  // pass 2: write the survivors
+  for (int k = threadIdx.x; k < nwords; k += blockDim.x) {
+    uint32_t m = s_sur[k];
+    if (!m) continue;
+    const int row = row0 + k / nw;
+    const int cbase = (wlo + k % nw) << 5;
+    int rank = base + s_pref[k];
+    while (m) {
+      const int bit = __ffs(m) - 1;
+      m &= m - 1u;
+      if (rank >= F.max_pts) break;
+      const long long idx = (long long)row * p0 + cbase + bit;
+      orbx_point q;
+      q.x = cbase + bit;
+      q.y = row;
+      q.octave = F.oct8[idx];
+      q.score = F.vmap[idx];
+      q.angle = 0.f;
+      q.match = 0;
+      q.distance = 0;
+      F.pts[rank] = q;
+      rank++;
+    }
   }
+}
+
+// Dense reference-layout maps (vmem: f32 scores then i32 octaves,
+// orbd.cu:1576-1577) from the sparse ones, for orbd.h callers and debugging.
+__global__ void k_expand_score_map(const Frame* __restrict__ fr, float* vmap_dense, int* layer_dense,
+                                   long long npx) {
+  const Frame& F = fr[0];
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < npx;
+       i += (long long)gridDim.x * blockDim.x) {
+    const bool on = (__ldg(F.occ + (i >> 5)) >> (i & 31)) & 1u;
+    vmap_dense[i] = on ? F.vmap[i] : 0.f;
+    layer_dense[i] = on ? (int)F.oct8[i] : 0;
+  }
+}
+
+cudaError_t launch_expand_score_map(const Frame* d_frame, float* vmap_dense, int* layer_dense, long long npx,
+                                    cudaStream_t s) {
+  k_expand_score_map<<<4 * 148, 256, 0, s>>>(d_frame, vmap_dense, layer_dense, npx);
+  return cudaGetLastError();
 }
 
 cudaError_t launch_pyramid_blur(const Batch& b, int total_tiles, cudaStream_t s) {

@@ -17,8 +17,10 @@ constexpr int kPyrTH = 32;
 // Detect tile (level-0 pixels); 32 keeps octave 4/5 tiles whole
 constexpr int kDetTW = 64;
 constexpr int kDetTH = 32;
-// NMS strip height (level-0 rows); strips span the full valid width
+// NMS strips span the full valid width; default and largest strip height
 constexpr int kNmsRows = 4;
+constexpr int kNmsMaxRows = 16;
+constexpr int kNmsMaxWords = 2048;  // occupancy words per NMS strip (rows x words per row)
 
 // Per-frame state, in device memory (one entry per frame of a launch).
 struct Frame {
@@ -30,8 +32,10 @@ struct Frame {
   long long ooff[kMaxOctaves + 1];  // octave offsets in the pyramid (orb.cpp:151-174)
   uint8_t* pyr;  // octave 0 of the raw pyramid (kGuard zeroed bytes on both sides)
   uint8_t* blr;  // octave 0 of the blurred pyramid (same layout and guards)
-  float* vmap;   // level-0 keyed score map, h * op[0] floats
-  int* layer;    // octave of each score map entry, h * op[0] ints
+  float* vmap;    // level-0 keyed scores, h * op[0] floats, valid where the occupancy bit is set
+  uint8_t* oct8;  // octave of each score, h * op[0] bytes, valid where the occupancy bit is set
+  uint32_t* occ;  // occupancy bits: bit (y * op[0] + x) set where score > 0, h * op[0] / 32 words
+  int* layer;     // dense octave map of the reference's vmem layout (debug and orbd.h only)
   orbx_point* pts;
   uint8_t* desc;
   int* count;    // min(survivors, max_pts)
@@ -42,6 +46,7 @@ struct Frame {
   int pyr_tiles_x[kMaxOctaves], pyr_tiles_y[kMaxOctaves];
   int pyr_tile_base[kMaxOctaves + 1];  // per-octave prefix within the frame
   int det_tiles_x, det_tiles_y;
+  int nms_rows;      // level-0 rows per NMS strip (tunable, <= kNmsMaxRows)
   int nms_strips;
   unsigned long long* nms_status;  // look-back words, one per strip
 };
@@ -81,7 +86,10 @@ namespace orbx {
 cudaError_t launch_pyramid_blur(const Batch& b, int total_tiles, cudaStream_t s);
 cudaError_t launch_detect(const Batch& b, int total_tiles, cudaStream_t s);
 cudaError_t launch_nms(const Batch& b, int total_strips, cudaStream_t s);
-cudaError_t launch_describe(const Batch& b, int total_max_pts, cudaStream_t s);
+// dense reference-layout score and octave maps from the sparse ones (frame 0 of b)
+cudaError_t launch_expand_score_map(const Frame* d_frame, float* vmap_dense, int* layer_dense, long long npx,
+                                    cudaStream_t s);
+cudaError_t launch_describe(const Batch& b, int total_max_pts, cudaStream_t s, int blocks_per_sm = 8);
 
 struct MatchArgs {
   const uint8_t* q;      // [nq][32]
@@ -99,7 +107,7 @@ struct MatchWork {          // scratch for split-train merging
   int nq_cap;               // query capacity the grid is sized for
   int splits_cap;           // most train splits per query tile
 };
-int match_popc_blocks(int nq_cap, int splits_cap);
+int match_popc_blocks(int nq_cap, int splits_cap, int blocks_per_sm = 8);
 
 // int8 tensor-core form (orbx_match_imma.cu)
 struct ImmaLaunch {
@@ -163,5 +171,12 @@ int lower_blur(orbx_ctx* c, uint8_t* octave_images, const int* oszp, int noctave
 int lower_last_layout(orbx_ctx* c, int* oszp, int noctaves);
 int lower_describe(orbx_ctx* c, const uint8_t* octave_images, orbx_point* pts, int n_pts, uint8_t* desc, int wta_k,
                    const int* oszp, int noctaves, int* d_tmp_count);
-cudaError_t launch_match_popc(const MatchArgs& a, const MatchWork& w, cudaStream_t s);
+cudaError_t launch_match_popc(const MatchArgs& a, const MatchWork& w, cudaStream_t s, int blocks_per_sm = 8);
+
+// one matching job of a batch (one frame pair)
+struct MatchJob {
+  MatchArgs args;
+  MatchWork work;
+};
+cudaError_t launch_match_popc_batch(const MatchJob* d_jobs, int n_jobs, int blocks_per_job, cudaStream_t s);
 }  // namespace orbx

@@ -23,9 +23,10 @@ __device__ __forceinline__ void finish_query(const MatchArgs& a, int q, uint32_t
   finish_query_shared(a, q, k1, k2);
 }
 
-__global__ void __launch_bounds__(kMQ) k_match_popc(MatchArgs a, MatchWork w) {
-  __shared__ uint4 s_db[kMChunk * 2];
-  __shared__ unsigned int s_last;
+// One block's share of a k = 2 search; bid / nblk replace blockIdx.x / gridDim.x
+// so that a batch launch can run one search per blockIdx.y.
+__device__ __forceinline__ void match_popc_block(const MatchArgs& a, const MatchWork& w, int bid, int nblk,
+                                                 uint4* s_db, unsigned int& s_last) {
 
   const int nq = min(a.d_nq ? *a.d_nq : a.nq, w.nq_cap);
   const int ndb = a.d_ndb ? *a.d_ndb : a.ndb;
@@ -33,12 +34,12 @@ __global__ void __launch_bounds__(kMQ) k_match_popc(MatchArgs a, MatchWork w) {
   // actual counts, which may be far below the capacities the grid was sized for.
   const int tiles = (nq + kMQ - 1) / kMQ;
   if (tiles == 0) return;
-  int splits = (int)gridDim.x / tiles;
+  int splits = nblk / tiles;
   splits = min(splits, w.splits_cap);
   splits = min(splits, max(1, (ndb + 63) / 64));
   splits = max(splits, 1);
-  const int tile = blockIdx.x / splits;
-  const int split = blockIdx.x - tile * splits;
+  const int tile = bid / splits;
+  const int split = bid - tile * splits;
   if (tile >= tiles) return;
   const int q = tile * kMQ + threadIdx.x;
   const bool active = q < nq;
@@ -96,18 +97,37 @@ __global__ void __launch_bounds__(kMQ) k_match_popc(MatchArgs a, MatchWork w) {
   finish_query(a, q, m1, m2);
 }
 
-int match_popc_blocks(int nq_cap, int splits_cap) {
+__global__ void __launch_bounds__(kMQ) k_match_popc(MatchArgs a, MatchWork w) {
+  __shared__ uint4 s_db[kMChunk * 2];
+  __shared__ unsigned int s_last;
+  match_popc_block(a, w, blockIdx.x, gridDim.x, s_db, s_last);
+}
+
+__global__ void __launch_bounds__(kMQ) k_match_popc_batch(const MatchJob* __restrict__ jobs) {
+  __shared__ uint4 s_db[kMChunk * 2];
+  __shared__ unsigned int s_last;
+  const MatchJob& J = jobs[blockIdx.y];
+  match_popc_block(J.args, J.work, blockIdx.x, gridDim.x, s_db, s_last);
+}
+
+int match_popc_blocks(int nq_cap, int splits_cap, int blocks_per_sm) {
   const int tiles = (nq_cap + kMQ - 1) / kMQ;
-  const long long target = 8 * 148;
+  const long long target = (long long)(blocks_per_sm > 0 ? blocks_per_sm : 8) * 148;
   long long blocks = (long long)tiles * splits_cap;
   if (blocks > target) blocks = target;
   if (blocks < tiles) blocks = tiles;
   return (int)blocks;
 }
 
-cudaError_t launch_match_popc(const MatchArgs& a, const MatchWork& w, cudaStream_t s) {
+cudaError_t launch_match_popc(const MatchArgs& a, const MatchWork& w, cudaStream_t s, int blocks_per_sm) {
   if (w.nq_cap <= 0) return cudaSuccess;
-  k_match_popc<<<match_popc_blocks(w.nq_cap, w.splits_cap), kMQ, 0, s>>>(a, w);
+  k_match_popc<<<match_popc_blocks(w.nq_cap, w.splits_cap, blocks_per_sm), kMQ, 0, s>>>(a, w);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_match_popc_batch(const MatchJob* d_jobs, int n_jobs, int blocks_per_job, cudaStream_t s) {
+  if (n_jobs <= 0 || blocks_per_job <= 0) return cudaSuccess;
+  k_match_popc_batch<<<dim3(blocks_per_job, n_jobs), kMQ, 0, s>>>(d_jobs);
   return cudaGetLastError();
 }
 

@@ -39,6 +39,23 @@ class Params(ctypes.Structure):
                 ("retain_topn", ctypes.c_int), ("max_pts", ctypes.c_int)]
 
 
+class Image(ctypes.Structure):
+    _fields_ = [("data", ctypes.c_void_p), ("w", ctypes.c_int), ("h", ctypes.c_int), ("pitch", ctypes.c_int)]
+
+
+class FrameOut(ctypes.Structure):
+    _fields_ = [("points", ctypes.c_void_p), ("desc", ctypes.c_void_p), ("num_pts", ctypes.c_void_p),
+                ("max_pts", ctypes.c_int)]
+
+
+class Tuning(ctypes.Structure):
+    _fields_ = [("nms_rows", ctypes.c_int), ("describe_blocks_per_sm", ctypes.c_int),
+                ("match_blocks_per_sm", ctypes.c_int), ("match_blocks_per_pair", ctypes.c_int)]
+
+    def as_dict(self):
+        return {f: int(getattr(self, f)) for f, _ in self._fields_}
+
+
 _lib = None
 
 
@@ -68,6 +85,15 @@ def lib():
         L.orbx_debug_buffers.argtypes = [vp, vp, vp, vp, vp, vp]
         L.orbx_pair_host.argtypes = [vp, vp, vp, i32, i32, i32, vp, vp, vp, vp, vp, vp, i32]
         L.orbx_profile_pair.argtypes = [vp, vp, vp, i32, i32, i32, vp, vp, vp, vp, vp, vp, i32, vp]
+        L.orbx_get_tuning.argtypes = [vp, ctypes.POINTER(Tuning)]
+        L.orbx_set_tuning.argtypes = [vp, ctypes.POINTER(Tuning)]
+        L.orbx_batch_pairs.argtypes = [vp, i32, ctypes.POINTER(Image), ctypes.POINTER(Image),
+                                       ctypes.POINTER(FrameOut), ctypes.POINTER(FrameOut), i32]
+        L.orbx_autotune_pairs.argtypes = [vp, i32, ctypes.POINTER(Image), ctypes.POINTER(Image),
+                                          ctypes.POINTER(FrameOut), ctypes.POINTER(FrameOut), i32,
+                                          ctypes.POINTER(Tuning), ctypes.POINTER(ctypes.c_float)]
+        L.orbx_profile_batch.argtypes = [vp, i32, ctypes.POINTER(Image), ctypes.POINTER(Image),
+                                         ctypes.POINTER(FrameOut), ctypes.POINTER(FrameOut), vp]
         L.orbx_selftest_pi_minus.argtypes = [ctypes.c_uint32, ctypes.c_uint32]
         L.orbx_selftest_pi_minus.restype = ctypes.c_longlong
         _lib = L
@@ -188,6 +214,32 @@ class Context:
                                        _ptr(pb), _ptr(db), _ptr(nb), mode, ms.ctypes.data), "orbx_profile_pair")
         return ms
 
+    def get_tuning(self):
+        t = Tuning()
+        _check(lib().orbx_get_tuning(self.h, ctypes.byref(t)), "orbx_get_tuning")
+        return t
+
+    def set_tuning(self, t):
+        _check(lib().orbx_set_tuning(self.h, ctypes.byref(t)), "orbx_set_tuning")
+
+    def batch_pairs(self, batch, mode=MATCH_POPC):
+        """batch: a PairBatch (device images and outputs).  Asynchronous."""
+        _check(lib().orbx_batch_pairs(self.h, batch.n, batch.ia, batch.ib, batch.oa, batch.ob, mode),
+               "orbx_batch_pairs")
+
+    def profile_batch(self, batch):
+        ms = np.zeros(5, dtype=np.float32)
+        _check(lib().orbx_profile_batch(self.h, batch.n, batch.ia, batch.ib, batch.oa, batch.ob, ms.ctypes.data),
+               "orbx_profile_batch")
+        return ms
+
+    def autotune_pairs(self, batch, reps=3):
+        t = Tuning()
+        ms = ctypes.c_float(0)
+        _check(lib().orbx_autotune_pairs(self.h, batch.n, batch.ia, batch.ib, batch.oa, batch.ob, reps,
+                                         ctypes.byref(t), ctypes.byref(ms)), "orbx_autotune_pairs")
+        return t, ms.value
+
     def debug_buffers(self, w, h):
         n, oszp = layout(w, h, self.params.noctaves)
         obytes = int(oszp[5 * n])
@@ -241,3 +293,36 @@ def knn2(ctx, q, db, mode=MATCH_POPC):
     idx = torch.empty((nq, 2), dtype=torch.int32, device=q.device)
     ctx.knn2_ptr(q, nq, db if ndb else None, ndb, dist, idx, mode)
     return dist, idx
+
+
+class PairBatch:
+    """Device images and output buffers for orbx_batch_pairs.
+
+    pairs: list of (img_a, img_b, w, h, max_pts) with uint8 host arrays of shape
+    (h, pitch); images are copied to the device once."""
+
+    def __init__(self, pairs, device="cuda"):
+        torch = _torch()
+        self.n = len(pairs)
+        self.ia = (Image * self.n)()
+        self.ib = (Image * self.n)()
+        self.oa = (FrameOut * self.n)()
+        self.ob = (FrameOut * self.n)()
+        self.imgs, self.outs, self.shapes = [], [], []
+        for i, (a, b, w, h, cap) in enumerate(pairs):
+            da = torch.from_numpy(np.ascontiguousarray(a)).to(device)
+            db = torch.from_numpy(np.ascontiguousarray(b)).to(device)
+            A, B = FrameBuffers(cap, device), FrameBuffers(cap, device)
+            self.imgs.append((da, db))
+            self.outs.append((A, B))
+            self.shapes.append((w, h, cap))
+            self.ia[i] = Image(da.data_ptr(), w, h, a.shape[1])
+            self.ib[i] = Image(db.data_ptr(), w, h, b.shape[1])
+            self.oa[i] = FrameOut(A.points.data_ptr(), A.desc.data_ptr(), A.count.data_ptr(), cap)
+            self.ob[i] = FrameOut(B.points.data_ptr(), B.desc.data_ptr(), B.count.data_ptr(), cap)
+
+    def results(self, i):
+        A, B = self.outs[i]
+        pa, da = A.to_host()
+        pb, db = B.to_host()
+        return pa, da, pb, db

@@ -137,6 +137,55 @@ ORBX_API int orbx_profile_pair(orbx_ctx* ctx, const uint8_t* d_img_a, const uint
                                orbx_point* d_pts_a, uint8_t* d_desc_a, int* d_n_a, orbx_point* d_pts_b,
                                uint8_t* d_desc_b, int* d_n_b, int mode, float* stage_ms);
 
+/* One image of a batch: device pointer, size and row pitch (>= w). */
+typedef struct orbx_image {
+  const uint8_t* data;
+  int w, h, pitch;
+} orbx_image;
+
+/* Device outputs of one image of a batch: max_pts keypoints, max_pts*32
+ * descriptor bytes, one int count; max_pts is this image's keypoint cap. */
+typedef struct orbx_frame_out {
+  orbx_point* points;
+  uint8_t* desc;
+  int* num_pts;
+  int max_pts;
+} orbx_frame_out;
+
+/* Launch shapes the autotuner chooses among. */
+typedef struct orbx_tuning {
+  int nms_rows;              /* level-0 rows per NMS strip, 1..16 */
+  int describe_blocks_per_sm; /* grid of the orientation + descriptor kernel */
+  int match_blocks_per_sm;    /* grid of the popcount matcher (single pairs) */
+  int match_blocks_per_pair;  /* grid per pair of the batched matcher, 0 = automatic */
+} orbx_tuning;
+
+ORBX_API int orbx_get_tuning(orbx_ctx* ctx, orbx_tuning* t);
+ORBX_API int orbx_set_tuning(orbx_ctx* ctx, const orbx_tuning* t);
+
+/* Many frame pairs of any sizes and keypoint caps: every stage of every image
+ * runs in shared launches (one per stage for the whole batch), then every pair
+ * is matched A -> B in one launch; replayed from a CUDA graph cached per
+ * (shapes, pointers, tuning).  Per pair the results are identical to
+ * orbx_pair on that pair with the same cap.  This batches what the reference
+ * does one Orbor::detectAndCompute / Orbor::match call at a time
+ * (orb.cpp:57-113).  Asynchronous. */
+ORBX_API int orbx_batch_pairs(orbx_ctx* ctx, int n_pairs, const orbx_image* imgs_a, const orbx_image* imgs_b,
+                              const orbx_frame_out* out_a, const orbx_frame_out* out_b, int mode);
+
+/* Project-written autotuner: times orbx_batch_pairs on these inputs for every
+ * candidate tuning (CUDA events, median of `reps` replays), keeps the fastest
+ * in the context and returns it with its time.  Synchronises. */
+ORBX_API int orbx_autotune_pairs(orbx_ctx* ctx, int n_pairs, const orbx_image* imgs_a, const orbx_image* imgs_b,
+                                 const orbx_frame_out* out_a, const orbx_frame_out* out_b, int reps,
+                                 orbx_tuning* best, float* best_ms);
+
+/* Profiling variant of orbx_batch_pairs: the same launches without the graph,
+ * with a CUDA event between consecutive kernels; stage_ms[0..4] as for
+ * orbx_profile_pair.  Synchronises. */
+ORBX_API int orbx_profile_batch(orbx_ctx* ctx, int n_pairs, const orbx_image* imgs_a, const orbx_image* imgs_b,
+                                const orbx_frame_out* out_a, const orbx_frame_out* out_b, float* stage_ms);
+
 /* Debug: copy the internal buffers of the last single-image call to the host:
  * raw pyramid, blurred pyramid (offsets[n] bytes each, reference layout),
  * score map and octave map (h * pitch0 each).  Synchronises the stream. */
