@@ -25,8 +25,18 @@ namespace orbx {
 constexpr int kPyrSW = kPyrTW + 8;  // 3-pixel halo each side, padded to a multiple of 4
 constexpr int kPyrSH = kPyrTH + 6;
 
+// Exact small-integer <-> float conversions on the full-rate pipes: a float
+// whose exponent field is 2^23 holds the integer in its mantissa.
+__device__ __forceinline__ float u8_to_float(uint32_t x) {  // 0 <= x < 2^23
+  return __fsub_rn(__uint_as_float(0x4B000000u | x), 8388608.0f);
+}
+__device__ __forceinline__ uint32_t float_to_u8_rne(float v) {  // 0 <= v < 2^22: round to nearest, ties to even
+  return (uint32_t)(__float_as_int(__fadd_rn(v, 12582912.0f)) - 0x4B400000);
+}
+
 __global__ void __launch_bounds__(256) k_pyramid_blur(Batch b) {
-  __shared__ __align__(16) uint8_t s_src[kPyrSH * kPyrSW];
+  __shared__ __align__(16) float s_src[kPyrSH * kPyrSW];
+  __shared__ __align__(16) uint8_t s_byte[kPyrSH * kPyrSW];
   __shared__ __align__(16) float s_row[kPyrSH * kPyrTW];
 
   const int t = blockIdx.x;
@@ -53,7 +63,8 @@ __global__ void __launch_bounds__(256) k_pyramid_blur(Batch b) {
   }
   if (t == 0 && threadIdx.x == 0) *b.nms_ticket = 0u;
 
-  // stage: source rows y0-3 .. y0+34, columns x0-3 .. x0+132, reflect-101 at the octave edges
+  // stage: source rows y0-3 .. y0+34, columns x0-3 .. x0+132, reflect-101 at
+  // the octave edges, as floats and as bytes
   const uint8_t* __restrict__ psrc = F.pyr_src ? F.pyr_src + F.ooff[o] : nullptr;
   constexpr int kGroups = kPyrSW / 4;
   for (int it = threadIdx.x; it < kPyrSH * kGroups; it += blockDim.x) {
@@ -62,74 +73,81 @@ __global__ void __launch_bounds__(256) k_pyramid_blur(Batch b) {
     const int y = reflect101(y0 - 3 + r, oh);
     const uint8_t* rowp = psrc ? psrc + (size_t)y * op : img + (size_t)(y << o) * pitch_in;
     const int sh = psrc ? 0 : o;
-    uint32_t word = 0;
+    uint32_t v[4];
 #pragma unroll
-    for (int j = 0; j < 4; j++) {
-      const int x = reflect101(x0 - 3 + 4 * g + j, ow);
-      word |= (uint32_t)__ldg(rowp + (x << sh)) << (8 * j);
-    }
-    reinterpret_cast<uint32_t*>(s_src)[it] = word;
+    for (int j = 0; j < 4; j++) v[j] = __ldg(rowp + (reflect101(x0 - 3 + 4 * g + j, ow) << sh));
+    reinterpret_cast<float4*>(s_src)[it] = make_float4(u8_to_float(v[0]), u8_to_float(v[1]), u8_to_float(v[2]),
+                                                       u8_to_float(v[3]));
+    reinterpret_cast<uint32_t*>(s_byte)[it] = v[0] | (v[1] << 8) | (v[2] << 16) | (v[3] << 24);
   }
   __syncthreads();
 
   const float* k = b.gauss;
-  // horizontal pass: 4 consecutive outputs per thread from 12 staged bytes
+  // horizontal pass: 4 consecutive outputs per thread; integer tap sums are
+  // exact in float, so they are summed as floats
   for (int it = threadIdx.x; it < kPyrSH * (kPyrTW / 4); it += blockDim.x) {
     const int r = it / (kPyrTW / 4);
     const int g = it - r * (kPyrTW / 4);
-    const uint32_t* w = reinterpret_cast<const uint32_t*>(s_src + r * kPyrSW) + g;
-    const uint32_t w0 = w[0], w1 = w[1], w2 = w[2];
-    int p[12];
-#pragma unroll
-    for (int j = 0; j < 4; j++) {
-      p[j] = (w0 >> (8 * j)) & 0xFF;
-      p[4 + j] = (w1 >> (8 * j)) & 0xFF;
-      p[8 + j] = (w2 >> (8 * j)) & 0xFF;
-    }
+    const float4* q = reinterpret_cast<const float4*>(s_src + r * kPyrSW) + g;
+    const float4 a0 = q[0], a1 = q[1], a2 = q[2];
+    const float p[12] = {a0.x, a0.y, a0.z, a0.w, a1.x, a1.y, a1.z, a1.w, a2.x, a2.y, a2.z, a2.w};
     float4 out;
     float* op4 = &out.x;
 #pragma unroll
     for (int j = 0; j < 4; j++) {
-      const float t0 = (float)p[j + 3];
-      const float t1 = (float)(p[j + 2] + p[j + 4]);
-      const float t2 = (float)(p[j + 1] + p[j + 5]);
-      const float t3 = (float)(p[j] + p[j + 6]);
-      op4[j] = gauss_dot4(k, t0, t1, t2, t3);
+      const float t1 = __fadd_rn(p[j + 2], p[j + 4]);
+      const float t2 = __fadd_rn(p[j + 1], p[j + 5]);
+      const float t3 = __fadd_rn(p[j], p[j + 6]);
+      op4[j] = gauss_dot4(k, p[j + 3], t1, t2, t3);
     }
     reinterpret_cast<float4*>(s_row + r * kPyrTW)[g] = out;
   }
   __syncthreads();
 
-  // vertical pass: 4 consecutive rows of one column per thread (10-row window)
+  // vertical pass and stores: 4 consecutive columns of one row per thread
   uint8_t* P = F.pyr + F.ooff[o];
   uint8_t* B = F.blr + F.ooff[o];
   const bool copy_pad = (o == 0) && (pitch_in == op);
-  for (int it = threadIdx.x; it < (kPyrTH / 4) * kPyrTW; it += blockDim.x) {
-    const int rg = it / kPyrTW;
-    const int c = it - rg * kPyrTW;
-    const int x = x0 + c;
-    if (x >= op) continue;
-    float hcol[10];
+  for (int it = threadIdx.x; it < kPyrTH * (kPyrTW / 4); it += blockDim.x) {
+    const int r = it / (kPyrTW / 4);
+    const int g = it - r * (kPyrTW / 4);
+    const int y = y0 + r;
+    const int x = x0 + 4 * g;
+    if (y >= oh || x >= op) continue;
+    float4 h[7];
 #pragma unroll
-    for (int j = 0; j < 10; j++) hcol[j] = s_row[(4 * rg + j) * kPyrTW + c];
+    for (int j = 0; j < 7; j++) h[j] = reinterpret_cast<const float4*>(s_row + (r + j) * kPyrTW)[g];
+    const float* hf = reinterpret_cast<const float*>(h);
+    uint32_t bw = 0;
 #pragma unroll
     for (int j = 0; j < 4; j++) {
-      const int y = y0 + 4 * rg + j;
-      if (y >= oh) break;
-      const size_t a = (size_t)y * op + x;
-      if (x < ow) {
-        const float t0 = hcol[j + 3];
-        const float t1 = __fadd_rn(hcol[j + 2], hcol[j + 4]);
-        const float t2 = __fadd_rn(hcol[j + 1], hcol[j + 5]);
-        const float t3 = __fadd_rn(hcol[j], hcol[j + 6]);
-        B[a] = (uint8_t)__float2int_rn(gauss_dot4(k, t0, t1, t2, t3));
-        P[a] = s_src[(4 * rg + j + 3) * kPyrSW + c + 3];
-      } else {
-        // Row padding: octave 0 carries the caller's padding bytes (the reference
-        // copies h * pitch0 bytes, orbd.cu:1584); other octaves hold zeros.
-        const uint8_t v = psrc ? __ldg(psrc + a) : (copy_pad ? __ldg(img + (size_t)y * pitch_in + x) : (uint8_t)0);
-        P[a] = v;
-        B[a] = v;
+      const float t1 = __fadd_rn(hf[8 + j], hf[16 + j]);
+      const float t2 = __fadd_rn(hf[4 + j], hf[20 + j]);
+      const float t3 = __fadd_rn(hf[j], hf[24 + j]);
+      bw |= (float_to_u8_rne(gauss_dot4(k, hf[12 + j], t1, t2, t3)) & 0xFFu) << (8 * j);
+    }
+    // raw bytes of the same 4 pixels: staged columns 4g+3 .. 4g+6 of row r+3
+    const uint32_t* sb = reinterpret_cast<const uint32_t*>(s_byte + (r + 3) * kPyrSW) + g;
+    const uint32_t pw = __byte_perm(sb[0], sb[1], 0x6543);
+    const size_t a = (size_t)y * op + x;
+    if (x + 4 <= ow) {
+      *reinterpret_cast<uint32_t*>(B + a) = bw;
+      *reinterpret_cast<uint32_t*>(P + a) = pw;
+    } else {
+      // the group reaches into the row padding: octave 0 carries the caller's
+      // padding bytes (the reference copies h * pitch0 bytes, orbd.cu:1584),
+      // other octaves hold zeros
+#pragma unroll
+      for (int j = 0; j < 4; j++) {
+        if (x + j < ow) {
+          B[a + j] = (uint8_t)(bw >> (8 * j));
+          P[a + j] = (uint8_t)(pw >> (8 * j));
+        } else {
+          const uint8_t v = psrc ? __ldg(psrc + a + j)
+                                 : (copy_pad ? __ldg(img + (size_t)y * pitch_in + x + j) : (uint8_t)0);
+          B[a + j] = v;
+          P[a + j] = v;
+        }
       }
     }
   }
@@ -151,11 +169,12 @@ __global__ void __launch_bounds__(256) k_pyramid_blur(Batch b) {
 // tile's occupancy bits densely and its scores sparsely (no clearing pass).
 // ---------------------------------------------------------------------------
 constexpr int kHalo = 4;
-__host__ __device__ constexpr int det_stage_bytes() {
+__host__ __device__ constexpr int det_stage_off(int octave) {
   int s = 0;
-  for (int o = 0; o < kMaxOctaves; o++) s += ((kDetTW >> o) + 2 * kHalo) * ((kDetTH >> o) + 2 * kHalo);
+  for (int o = 0; o < octave; o++) s += ((kDetTW >> o) + 2 * kHalo) * ((kDetTH >> o) + 2 * kHalo);
   return s;
 }
+__host__ __device__ constexpr int det_stage_bytes() { return det_stage_off(kMaxOctaves); }
 
 // FAST ring (makeOffsets, orbd.cu:463-496), as (dx, dy).
 __constant__ int8_t c_ring[16][2] = {{0, 3},  {1, 3},   {2, 2},   {3, 1},   {3, 0},  {3, -1}, {2, -2}, {1, -3},
@@ -168,6 +187,15 @@ __device__ __forceinline__ bool has_arc9(uint32_t m16) {
   a &= a >> 4;                     // runs of 8
   a &= m >> 8;                     // runs of 9
   return (a & 0xFFFFu) != 0u;
+}
+
+// Final step of dHarrisScore (orbd.cu:667-668) as the reference build evaluates it.
+__device__ __forceinline__ float harris_combine(int dxx, int dyy, int dxy, float scale4) {
+  const unsigned dsxy = (unsigned)dxx + (unsigned)dyy;
+  const int A = (int)((unsigned)dxx * (unsigned)dyy - (unsigned)dxy * (unsigned)dxy);
+  const unsigned Bq = dsxy * dsxy;
+  const float u = __fmaf_rn(-0.04f, __uint2float_rn(Bq), __int2float_rn(A));
+  return __fmul_rn(u, scale4);
 }
 
 // dHarrisScore (orbd.cu:651-669) on a shared-memory tile of row stride sw.
@@ -191,11 +219,7 @@ __device__ __forceinline__ float harris_score(const uint8_t* c, int sw, float sc
       dxy += dx * dy;
     }
   }
-  const unsigned dsxy = (unsigned)(dxx + dyy);
-  const int A = (int)((unsigned)dxx * (unsigned)dyy - (unsigned)dxy * (unsigned)dxy);
-  const unsigned Bq = dsxy * dsxy;
-  const float u = __fmaf_rn(-0.04f, __uint2float_rn(Bq), __int2float_rn(A));
-  return __fmul_rn(u, scale4);
+  return harris_combine(dxx, dyy, dxy, scale4);
 }
 
 // dFastScore (orbd.cu:538-586, FAST_PATTERN 16).
@@ -231,14 +255,22 @@ __device__ __forceinline__ float fast_score(const int* d, int threshold) {
   return (float)(-b0 - 1);
 }
 
-// FAST-9 segment test on a shared-memory tile of row stride sw.  The first
-// check is the reference's pre-test on ring pixels 0 and 8 (orbd.cu:700-702):
-// every run of 9 contains one of them, so most pixels stop there.
-__device__ __forceinline__ bool fast9(const uint8_t* c, int sw, int thr) {
-  const int v = c[0];
-  const int lo = v - thr, hi = v + thr;
-  const int p0 = c[3 * sw], p8 = c[-3 * sw];
-  if (!(p0 < lo || p0 > hi || p8 < lo || p8 > hi)) return false;
+// Necessary condition for FAST-9: every run of 9 ring pixels contains two
+// neighbouring cardinal points (ring positions k and k+4, k = 0, 4, 8, 12), so
+// both of some such pair must be darker than v - t, or both brighter than
+// v + t.  It rejects most pixels with four loads; it never changes a result.
+__device__ __forceinline__ bool fast9_pretest(const uint8_t* c, int sw, int lo, int hi) {
+  const int p0 = c[3 * sw], p4 = c[3], p8 = c[-3 * sw], p12 = c[-3];
+  const bool d0 = p0 < lo, d4 = p4 < lo, d8 = p8 < lo, d12 = p12 < lo;
+  const bool b0 = p0 > hi, b4 = p4 > hi, b8 = p8 > hi, b12 = p12 > hi;
+  return (d0 && d4) || (d4 && d8) || (d8 && d12) || (d12 && d0) || (b0 && b4) || (b4 && b8) || (b8 && b12) ||
+         (b12 && b0);
+}
+
+// FAST-9 segment test on a shared-memory tile of row stride sw: a run of 9
+// contiguous ring pixels all darker than v - t or all brighter than v + t (the
+// reference's LUT pre-test and arc loop, orbd.cu:683-740, decide exactly this).
+__device__ __forceinline__ bool fast9_full(const uint8_t* c, int sw, int lo, int hi) {
   uint32_t dark = 0, bright = 0;
 #pragma unroll
   for (int k = 0; k < 16; k++) {
@@ -249,12 +281,122 @@ __device__ __forceinline__ bool fast9(const uint8_t* c, int sw, int thr) {
   return has_arc9(dark) || has_arc9(bright);
 }
 
+__device__ __forceinline__ float corner_score(const Batch& b, const uint8_t* c, int sw) {
+  if (b.harris) return harris_score(c, sw, b.harris_scale4);
+  const int v = c[0];
+  int d[25];
+#pragma unroll
+  for (int k = 0; k < 25; k++) d[k] = (int)(short)(v - c[c_ring[k & 15][1] * sw + c_ring[k & 15][0]]);
+  return fast_score(d, b.fast_thr);
+}
+
+// Append this lane's item to a warp-private list when `take`; returns the new length.
+__device__ __forceinline__ int warp_append(int16_t* list, int len, bool take, int16_t item, int lane) {
+  const uint32_t m = __ballot_sync(0xffffffffu, take);
+  if (take) list[len + __popc(m & ((1u << lane) - 1u))] = item;
+  return len + __popc(m);
+}
+
+// One octave's pixels of a rectangle [lx0, lx0+nx) x [ly0, ly0+ny) of the
+// octave tile, processed by one warp: pre-test, compacted full test, compacted
+// scoring, merge into the level-0 map (strict >, so a lower octave keeps ties).
+__device__ __forceinline__ void detect_rect_warp(const Batch& b, const Frame& F, int o, const uint8_t* stage, int sw,
+                                                 int xb, int yb, int lx0, int ly0, int nx_log, int ny,
+                                                 int16_t* list_a, int16_t* list_b, float* s_map, int8_t* s_oct,
+                                                 int lane) {
+  const int ow = F.ow[o], oh = F.oh[o];
+  const int thr = b.fast_thr;
+  const int npx = ny << nx_log;
+  int na = 0;
+  for (int i0 = 0; i0 < npx; i0 += 32) {
+    const int i = i0 + lane;
+    bool take = false;
+    if (i < npx) {
+      const int lx = lx0 + (i & ((1 << nx_log) - 1));
+      const int ly = ly0 + (i >> nx_log);
+      const int x = xb + lx, y = yb + ly;
+      if (x >= 3 && x < ow - 3 && y >= 3 && y < oh - 3) {
+        const uint8_t* c = stage + (ly + kHalo) * sw + (lx + kHalo);
+        const int v = c[0];
+        take = fast9_pretest(c, sw, v - thr, v + thr);
+      }
+    }
+    na = warp_append(list_a, na, take, (int16_t)((ly0 + (i >> nx_log)) * 64 + lx0 + (i & ((1 << nx_log) - 1))),
+                     lane);
+  }
+  __syncwarp();
+  int nb = 0;
+  for (int j0 = 0; j0 < na; j0 += 32) {
+    const int j = j0 + lane;
+    bool take = false;
+    int16_t item = 0;
+    if (j < na) {
+      item = list_a[j];
+      const uint8_t* c = stage + ((item >> 6) + kHalo) * sw + ((item & 63) + kHalo);
+      const int v = c[0];
+      take = fast9_full(c, sw, v - thr, v + thr);
+    }
+    nb = warp_append(list_b, nb, take, item, lane);
+  }
+  __syncwarp();
+  if (b.harris) {
+    // one corner at a time, the whole warp: lane i takes window positions i and
+    // i + 32 of the 7x7 Harris window; the 32-bit sums wrap, so their order is free
+    for (int j = 0; j < nb; j++) {
+      const int item = list_b[j];
+      const int ly = item >> 6, lx = item & 63;
+      const uint8_t* c = stage + (ly + kHalo) * sw + (lx + kHalo);
+      int dxx = 0, dyy = 0, dxy = 0;
+#pragma unroll
+      for (int w2 = 0; w2 < 2; w2++) {
+        const int pos = lane + 32 * w2;
+        if (pos < 49) {
+          const int wy = pos / 7 - 3, wx = pos % 7 - 3;
+          const uint8_t* q = c + wy * sw + wx;
+          const int dx = ((int)q[1] - (int)q[-1]) * 2 + ((int)q[-sw + 1] - (int)q[-sw - 1]) +
+                         ((int)q[sw + 1] - (int)q[sw - 1]);
+          const int dy = ((int)q[sw] - (int)q[-sw]) * 2 + ((int)q[sw - 1] - (int)q[-sw - 1]) +
+                         ((int)q[sw + 1] - (int)q[-sw + 1]);
+          dxx += dx * dx;
+          dyy += dy * dy;
+          dxy += dx * dy;
+        }
+      }
+#pragma unroll
+      for (int d = 16; d >= 1; d >>= 1) {
+        dxx += __shfl_xor_sync(0xffffffffu, dxx, d);
+        dyy += __shfl_xor_sync(0xffffffffu, dyy, d);
+        dxy += __shfl_xor_sync(0xffffffffu, dxy, d);
+      }
+      if (lane == 0) {
+        const float score = harris_combine(dxx, dyy, dxy, b.harris_scale4);
+        const int m = (ly << o) * kDetTW + (lx << o);
+        if (s_map[m] < score) {
+          s_map[m] = score;
+          s_oct[m] = (int8_t)o;
+        }
+      }
+    }
+  } else {
+    for (int j = lane; j < nb; j += 32) {
+      const int item = list_b[j];
+      const int ly = item >> 6, lx = item & 63;
+      const float score = corner_score(b, stage + (ly + kHalo) * sw + (lx + kHalo), sw);
+      const int m = (ly << o) * kDetTW + (lx << o);
+      if (s_map[m] < score) {
+        s_map[m] = score;
+        s_oct[m] = (int8_t)o;
+      }
+    }
+  }
+  __syncwarp();
+}
+
 __global__ void __launch_bounds__(256, 4) k_detect(Batch b) {
   __shared__ __align__(16) uint8_t s_stage[det_stage_bytes()];
   __shared__ float s_map[kDetTH * kDetTW];
   __shared__ int8_t s_oct[kDetTH * kDetTW];
-  __shared__ int16_t s_cand[kDetTH * kDetTW];
-  __shared__ int s_ncand;
+  __shared__ int16_t s_list[8][2][256];
 
   const int t = blockIdx.x;
   const int f = find_frame(b.det_base, b.n_frames, t);
@@ -265,6 +407,7 @@ __global__ void __launch_bounds__(256, 4) k_detect(Batch b) {
   const int n_oct = F.n_oct;
   const uint8_t* __restrict__ pyr = F.pyr;
   const int lane = threadIdx.x & 31;
+  const int warp = threadIdx.x >> 5;
 
   for (int i = threadIdx.x; i < kDetTH * kDetTW; i += blockDim.x) {
     s_map[i] = 0.f;
@@ -272,90 +415,55 @@ __global__ void __launch_bounds__(256, 4) k_detect(Batch b) {
   }
   // Stage every octave's tile with its halo, 4 bytes per load: octave offsets
   // and pitches are multiples of 128 and (X0 >> o) - 4 is a multiple of 4.
-  {
-    int off = 0;
-    for (int o = 0; o < n_oct; o++) {
-      const int sw = (kDetTW >> o) + 2 * kHalo;
-      const int sh = (kDetTH >> o) + 2 * kHalo;
-      const int sw4 = sw >> 2;
-      const int op = F.op[o];
-      const long long base = F.ooff[o] + (long long)((Y0 >> o) - kHalo) * op + ((X0 >> o) - kHalo);
-      uint32_t* dst = reinterpret_cast<uint32_t*>(s_stage + off);
-      for (int i = threadIdx.x; i < sw4 * sh; i += blockDim.x) {
-        const int r = i / sw4;
-        const int c4 = i - r * sw4;
-        dst[i] = __ldg(reinterpret_cast<const uint32_t*>(pyr + base + (long long)r * op) + c4);
-      }
-      off += sw * sh;
+  for (int o = 0; o < n_oct; o++) {
+    const int sw = (kDetTW >> o) + 2 * kHalo;
+    const int sh = (kDetTH >> o) + 2 * kHalo;
+    const int sw4 = sw >> 2;
+    const int op = F.op[o];
+    const long long base = F.ooff[o] + (long long)((Y0 >> o) - kHalo) * op + ((X0 >> o) - kHalo);
+    uint32_t* dst = reinterpret_cast<uint32_t*>(s_stage + det_stage_off(o));
+    for (int i = threadIdx.x; i < sw4 * sh; i += blockDim.x) {
+      const int r = i / sw4;
+      const int c4 = i - r * sw4;
+      dst[i] = __ldg(reinterpret_cast<const uint32_t*>(pyr + base + (long long)r * op) + c4);
     }
   }
   __syncthreads();
 
-  const int thr = b.fast_thr;
-  int off = 0;
-  for (int o = 0; o < n_oct; o++) {
-    const int tw = kDetTW >> o;
-    const int th = kDetTH >> o;
-    const int sw = tw + 2 * kHalo;
-    const int ow = F.ow[o], oh = F.oh[o];
-    const int xb = X0 >> o, yb = Y0 >> o;
-    const uint8_t* stage = s_stage + off;
-    if (threadIdx.x == 0) s_ncand = 0;
-    __syncthreads();
-    // phase A: segment test, corners appended to a shared list
-    const int tw_log = 6 - o;  // tw = kDetTW >> o = 1 << tw_log
-    for (int i0 = 0; i0 < tw * th; i0 += blockDim.x) {
-      const int i = i0 + threadIdx.x;
-      bool corner = false;
-      if (i < tw * th) {
-        const int ly = i >> tw_log;
-        const int lx = i & (tw - 1);
-        const int x = xb + lx, y = yb + ly;
-        if (x >= 3 && x < ow - 3 && y >= 3 && y < oh - 3)
-          corner = fast9(stage + (ly + kHalo) * sw + (lx + kHalo), sw, thr);
-      }
-      const uint32_t m = __ballot_sync(0xffffffffu, corner);
-      if (m) {
-        int wbase = 0;
-        if (lane == 0) wbase = atomicAdd(&s_ncand, __popc(m));
-        wbase = __shfl_sync(0xffffffffu, wbase, 0);
-        if (corner) s_cand[wbase + __popc(m & ((1u << lane) - 1u))] = (int16_t)i;
-      }
+  // octaves 0..2: warp w owns level-0 rows [4w, 4w+4) of the tile, i.e. octave
+  // rows [4w >> o, (4w+4) >> o); no other warp touches those map positions
+  int16_t* la = s_list[warp][0];
+  int16_t* lb = s_list[warp][1];
+  for (int o = 0; o < n_oct && o < 3; o++) {
+    const int sw = (kDetTW >> o) + 2 * kHalo;
+    const int nx_log = 6 - o;
+    int ly0, ny;
+    if (o < 2) {
+      ly0 = (4 * warp) >> o;
+      ny = 4 >> o;
+    } else {
+      ly0 = warp;
+      ny = 1;
     }
-    __syncthreads();
-    // phase B: score every corner (each position once, so list order is irrelevant)
-    const int nc = s_ncand;
-    for (int j = threadIdx.x; j < nc; j += blockDim.x) {
-      const int i = s_cand[j];
-      const int ly = i >> tw_log;
-      const int lx = i & (tw - 1);
-      const uint8_t* c = stage + (ly + kHalo) * sw + (lx + kHalo);
-      float score;
-      if (b.harris) {
-        score = harris_score(c, sw, b.harris_scale4);
-      } else {
-        const int v = c[0];
-        int d[25];
-#pragma unroll
-        for (int k = 0; k < 25; k++) d[k] = (int)(short)(v - c[c_ring[k & 15][1] * sw + c_ring[k & 15][0]]);
-        score = fast_score(d, thr);
-      }
-      const int mpos = (ly << o) * kDetTW + (lx << o);
-      if (s_map[mpos] < score) {
-        s_map[mpos] = score;
-        s_oct[mpos] = (int8_t)o;
-      }
-    }
-    off += sw * ((kDetTH >> o) + 2 * kHalo);
-    __syncthreads();
+    detect_rect_warp(b, F, o, s_stage + det_stage_off(o), sw, X0 >> o, Y0 >> o, 0, ly0, nx_log, ny, la, lb, s_map,
+                     s_oct, lane);
   }
+  __syncthreads();
+  // octaves 3 and 4 (8x4 and 4x2 pixels per tile) by warp 0, in order
+  if (warp == 0) {
+    for (int o = 3; o < n_oct; o++) {
+      const int sw = (kDetTW >> o) + 2 * kHalo;
+      detect_rect_warp(b, F, o, s_stage + det_stage_off(o), sw, X0 >> o, Y0 >> o, 0, 0, 6 - o, kDetTH >> o, la, lb,
+                       s_map, s_oct, lane);
+    }
+  }
+  __syncthreads();
 
   // Output: occupancy bits for the whole tile (every word written, so no
   // clearing pass), scores and octaves only where a score was stored.  The
   // tile's 64 columns are two aligned 32-bit words of each row (pitch0 is a
   // multiple of 128).
   const int p0 = F.op[0];
-  const int warp = threadIdx.x >> 5;
   for (int k = warp; k < kDetTH * (kDetTW / 32); k += blockDim.x >> 5) {
     const int r = k >> 1;
     const int c = ((k & 1) << 5) + lane;
