@@ -81,6 +81,7 @@ def lib():
         L.orbx_detect_and_compute.argtypes = [vp, vp, i32, i32, i32, vp, vp, vp, i32]
         L.orbx_match.argtypes = [vp, vp, vp, vp, vp, vp, i32, i32, i32]
         L.orbx_match_knn2.argtypes = [vp, vp, i32, vp, i32, vp, vp, i32]
+        L.orbx_match_knn2_static.argtypes = [vp, i32, vp, i32, vp, vp, vp]
         L.orbx_pair.argtypes = [vp, vp, vp, i32, i32, i32, vp, vp, vp, vp, vp, vp, i32]
         L.orbx_debug_buffers.argtypes = [vp, vp, vp, vp, vp, vp]
         L.orbx_pair_host.argtypes = [vp, vp, vp, i32, i32, i32, vp, vp, vp, vp, vp, vp, i32]
@@ -293,6 +294,15 @@ def knn2(ctx, q, db, mode=MATCH_POPC):
     idx = torch.empty((nq, 2), dtype=torch.int32, device=q.device)
     ctx.knn2_ptr(q, nq, db if ndb else None, ndb, dist, idx, mode)
     return dist, idx
+
+
+STATIC_MAX_QUERIES = 16384  # ORBX_STATIC_MAX_QUERIES
+
+
+def knn2_static_ptr(d_q, nq, d_db, ndb, d_dist2, d_idx2, stream=None):
+    """orbx_match_knn2_static on the current device; stream is a raw cudaStream_t (int) or None."""
+    _check(lib().orbx_match_knn2_static(_ptr(d_q), nq, _ptr(d_db), ndb, _ptr(d_dist2), _ptr(d_idx2), stream),
+           "orbx_match_knn2_static")
 
 
 class PairBatch:

@@ -111,6 +111,18 @@ ORBX_API int orbx_match(orbx_ctx* ctx, orbx_point* d_points1, const int* d_n1, c
 ORBX_API int orbx_match_knn2(orbx_ctx* ctx, const uint8_t* d_q, int nq, const uint8_t* d_db, int ndb,
                              uint32_t* d_dist2, int32_t* d_idx2, int mode);
 
+/* No counterpart in the reference.  The orbx_match_knn2 popcount search with the
+ * same outputs, for callers that may not allocate device memory: it needs no
+ * context and allocates nothing.  Its scratch (about 4 MiB) is one fixed
+ * device array per device, whose address is looked up on the first call made
+ * with that device current; make that first call before any stream capture.
+ * Runs on the current device and on cuda_stream (0 = the legacy default stream).
+ * nq above ORBX_STATIC_MAX_QUERIES returns ORBX_ERR_SIZE.  Calls on one device
+ * share the scratch: calls whose work overlaps on the device race. */
+#define ORBX_STATIC_MAX_QUERIES 16384
+ORBX_API int orbx_match_knn2_static(const uint8_t* d_q, int nq, const uint8_t* d_db, int ndb,
+                                    uint32_t* d_dist2, int32_t* d_idx2, void* cuda_stream);
+
 /* A frame pair end to end: detect + describe A and B in shared launches, then
  * match A -> B (Orbor::detectAndCompute x2 + Orbor::match, main.cpp:233-243).
  * Replayed from a CUDA graph cached per (shape, pointers). */
