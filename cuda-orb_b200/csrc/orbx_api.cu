@@ -1326,3 +1326,9 @@ ORBX_API long long orbx_selftest_pi_minus(uint32_t lo_bits, uint32_t hi_bits) {
 }
 
 }  // extern "C"
+
+namespace orbx {
+int ctx_device(const orbx_ctx* c) { return c->device; }
+cudaStream_t ctx_stream(const orbx_ctx* c) { return c->stream; }
+int* ctx_err(orbx_ctx* c) { return c->d_err; }
+}  // namespace orbx

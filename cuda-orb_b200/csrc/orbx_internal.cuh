@@ -118,7 +118,11 @@ struct ImmaLaunch {
   int nq_cap, ndb_cap;
   int splits;         // database splits per query tile
   int* err;
+  bool q_ready;       // q_pm1 already holds the expanded queries (rows >= nq zero)
+  bool db_ready;      // db_pm1 already holds the expanded database (rows >= ndb zero)
 };
+// bits -> +-1 int8 rows (rows beyond the count are zero); 4 * 148 blocks of 256
+cudaError_t launch_expand_pm1(const uint8_t* bits, int n, const int* d_n, int rows, int8_t* out, cudaStream_t s);
 int imma_rows_q(int n);
 int imma_rows_db(int n);
 int imma_default_splits(int nq_cap);
@@ -179,4 +183,9 @@ struct MatchJob {
   MatchWork work;
 };
 cudaError_t launch_match_popc_batch(const MatchJob* d_jobs, int n_jobs, int blocks_per_job, cudaStream_t s);
+
+// context accessors for the entry points outside orbx_api.cu
+int ctx_device(const orbx_ctx* c);
+cudaStream_t ctx_stream(const orbx_ctx* c);
+int* ctx_err(orbx_ctx* c);
 }  // namespace orbx

@@ -1,0 +1,572 @@
+// Kernels of the learned matching proposal (no counterpart in the reference,
+// whose only matcher is exact brute force, orbd.cu:1471-1559):
+//  - bit rows -> +-1 bf16 rows (row-major and transposed) for the MLP GEMMs;
+//  - softmax cross-entropy forward + gradient, bf16 transposes, column sums
+//    and a fused split-sum + Adam update for training;
+//  - Hamming k-majority clustering of the database (assignment comes from the
+//    exact k = 2 matcher against the centroids);
+//  - search: top-8 cluster probes per query from the GEMM's top-8 keys, probe
+//    lists per cluster, exact Hamming rerank of each probed cluster, merge,
+//    and the plumbing that sends low-margin queries to exact brute force.
+#include "orbx_device.cuh"
+#include "orbx_internal.cuh"
+#include "orbx_learned.cuh"
+
+namespace orbx {
+
+namespace {
+__device__ __forceinline__ uint64_t splitmix64(uint64_t x) {
+  x += 0x9E3779B97F4A7C15ull;
+  x = (x ^ (x >> 30)) * 0xBF58476D1CE4E5B9ull;
+  x = (x ^ (x >> 27)) * 0x94D049BB133111EBull;
+  return x ^ (x >> 31);
+}
+__device__ __forceinline__ float u01(uint64_t h) {  // (0, 1]
+  return ((float)(h >> 40) + 1.0f) * (1.0f / 16777216.0f);
+}
+constexpr uint16_t kBfPlus1 = 0x3F80u, kBfMinus1 = 0xBF80u;
+}  // namespace
+
+// ---------------------------------------------------------------- expansion
+// out[r][k] = bit k of row r ? +1 : -1 (bit k = byte k / 8, bit k % 8), rows
+// n..rows-1 are zero.  One thread per (row, byte): one 16-byte store.
+__global__ void k_bits_pm1_bf16(const uint8_t* __restrict__ bits, int n, const int* d_n, int rows,
+                                __nv_bfloat16* __restrict__ out) {
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (long long)rows * 32) return;
+  const int r = (int)(t >> 5), j = (int)(t & 31);
+  const int nv = d_n ? min(*d_n, n) : n;
+  uint4 v = make_uint4(0, 0, 0, 0);
+  if (r < nv) {
+    const uint32_t b = bits[(size_t)r * 32 + j];
+    uint32_t w[4];
+#pragma unroll
+    for (int e = 0; e < 4; e++) {
+      const uint32_t lo = (b >> (2 * e)) & 1u ? kBfPlus1 : kBfMinus1;
+      const uint32_t hi = (b >> (2 * e + 1)) & 1u ? kBfPlus1 : kBfMinus1;
+      w[e] = lo | (hi << 16);
+    }
+    v = make_uint4(w[0], w[1], w[2], w[3]);
+  }
+  reinterpret_cast<uint4*>(out)[t] = v;
+}
+
+// Transposed: out[k][r] for r < rows (rows % 64 == 0).  A block takes 64 rows:
+// their bits go to shared memory, then thread k writes 64 values of row k.
+__global__ void __launch_bounds__(256) k_bits_pm1_bf16_t(const uint8_t* __restrict__ bits, int n, int rows,
+                                                         __nv_bfloat16* __restrict__ out) {
+  __shared__ uint8_t s[64 * 32];
+  const int r0 = blockIdx.x * 64;
+  for (int i = threadIdx.x; i < 64 * 32; i += 256) {
+    const int r = r0 + i / 32;
+    s[i] = r < n ? bits[(size_t)r * 32 + (i & 31)] : 0;
+  }
+  __syncthreads();
+  const int k = threadIdx.x;
+  uint4* dst = reinterpret_cast<uint4*>(out + (size_t)k * rows + r0);
+#pragma unroll
+  for (int q = 0; q < 8; q++) {
+    uint32_t w[4];
+#pragma unroll
+    for (int e = 0; e < 4; e++) {
+      const int ra = 8 * q + 2 * e, rb = ra + 1;
+      const uint32_t lo = (r0 + ra < n) ? (((s[ra * 32 + (k >> 3)] >> (k & 7)) & 1u) ? kBfPlus1 : kBfMinus1) : 0u;
+      const uint32_t hi = (r0 + rb < n) ? (((s[rb * 32 + (k >> 3)] >> (k & 7)) & 1u) ? kBfPlus1 : kBfMinus1) : 0u;
+      w[e] = lo | (hi << 16);
+    }
+    dst[q] = make_uint4(w[0], w[1], w[2], w[3]);
+  }
+}
+
+// ---------------------------------------------------------------- training
+// One warp per row of C logits (C % 128 == 0).  Rows r < n with label >= 0 get
+// dL = (softmax - onehot) * grad_scale, loss[r] = -log softmax[label] and
+// correct[r] = (argmax == label); other rows get dL = 0, loss 0, correct 0.
+__global__ void __launch_bounds__(256) k_softmax_xent(const float* __restrict__ logits, const int* __restrict__ labels,
+                                                      int n, int rows, int C, float grad_scale,
+                                                      __nv_bfloat16* __restrict__ dL, float* __restrict__ loss,
+                                                      int* __restrict__ correct) {
+  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (warp >= rows) return;
+  const int r = warp;
+  const int label = r < n ? labels[r] : -1;
+  uint2* drow = reinterpret_cast<uint2*>(dL + (size_t)r * C);
+  if (label < 0) {
+    for (int c = lane; c < C / 4; c += 32) drow[c] = make_uint2(0, 0);
+    if (lane == 0) {
+      loss[r] = 0.f;
+      correct[r] = 0;
+    }
+    return;
+  }
+  const float4* row = reinterpret_cast<const float4*>(logits + (size_t)r * C);
+  float mx = -3.0e38f;
+  int amax = 0;
+  for (int c = lane; c < C / 4; c += 32) {
+    const float4 v = row[c];
+    if (v.x > mx) { mx = v.x; amax = 4 * c; }
+    if (v.y > mx) { mx = v.y; amax = 4 * c + 1; }
+    if (v.z > mx) { mx = v.z; amax = 4 * c + 2; }
+    if (v.w > mx) { mx = v.w; amax = 4 * c + 3; }
+  }
+#pragma unroll
+  for (int o = 16; o; o >>= 1) {
+    const float om = __shfl_xor_sync(0xffffffffu, mx, o);
+    const int oa = __shfl_xor_sync(0xffffffffu, amax, o);
+    if (om > mx || (om == mx && oa < amax)) {
+      mx = om;
+      amax = oa;
+    }
+  }
+  float sum = 0.f;
+  for (int c = lane; c < C / 4; c += 32) {
+    const float4 v = row[c];
+    sum += __expf(v.x - mx) + __expf(v.y - mx) + __expf(v.z - mx) + __expf(v.w - mx);
+  }
+#pragma unroll
+  for (int o = 16; o; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
+  const float inv = 1.0f / sum;
+  for (int c = lane; c < C / 4; c += 32) {
+    const float4 v = row[c];
+    float p[4] = {__expf(v.x - mx) * inv, __expf(v.y - mx) * inv, __expf(v.z - mx) * inv, __expf(v.w - mx) * inv};
+#pragma unroll
+    for (int e = 0; e < 4; e++)
+      if (4 * c + e == label) p[e] -= 1.0f;
+    const __nv_bfloat162 a = __floats2bfloat162_rn(p[0] * grad_scale, p[1] * grad_scale);
+    const __nv_bfloat162 b = __floats2bfloat162_rn(p[2] * grad_scale, p[3] * grad_scale);
+    drow[c] = make_uint2(*reinterpret_cast<const uint32_t*>(&a), *reinterpret_cast<const uint32_t*>(&b));
+  }
+  if (lane == 0) {
+    loss[r] = logf(sum) + mx - logits[(size_t)r * C + label];
+    correct[r] = amax == label ? 1 : 0;
+  }
+}
+
+// out[c][r] = in[r][c]; R % 32 == 0, C % 32 == 0.  32 x 32 tiles, 32 x 8 threads.
+__global__ void __launch_bounds__(256) k_transpose_bf16(const __nv_bfloat16* __restrict__ in, int R, int C,
+                                                        __nv_bfloat16* __restrict__ out) {
+  __shared__ uint16_t t[32][33];
+  const uint16_t* src = reinterpret_cast<const uint16_t*>(in);
+  uint16_t* dst = reinterpret_cast<uint16_t*>(out);
+  const int c0 = blockIdx.x * 32, r0 = blockIdx.y * 32;
+  for (int i = threadIdx.y; i < 32; i += 8) t[i][threadIdx.x] = src[(size_t)(r0 + i) * C + c0 + threadIdx.x];
+  __syncthreads();
+  for (int i = threadIdx.y; i < 32; i += 8) dst[(size_t)(c0 + i) * R + r0 + threadIdx.x] = t[threadIdx.x][i];
+}
+
+// partial[chunk][c] = sum of in[r][c] over the chunk's rows (C % 64 == 0).
+// grid (C / 64, chunks); 8 warps split the rows, lane holds two columns.
+__global__ void __launch_bounds__(256) k_colsum_bf16(const __nv_bfloat16* __restrict__ in, int R, int C,
+                                                     int rows_per_chunk, float* __restrict__ partial) {
+  __shared__ float2 s[8][32];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int c = blockIdx.x * 64 + 2 * lane;
+  const int rb = blockIdx.y * rows_per_chunk, re = min(R, rb + rows_per_chunk);
+  float2 acc = make_float2(0.f, 0.f);
+  for (int r = rb + warp; r < re; r += 8) {
+    const __nv_bfloat162 v = *reinterpret_cast<const __nv_bfloat162*>(in + (size_t)r * C + c);
+    const float2 f = __bfloat1622float2(v);
+    acc.x += f.x;
+    acc.y += f.y;
+  }
+  s[warp][lane] = acc;
+  __syncthreads();
+  if (warp == 0) {
+    float2 t = s[0][lane];
+    for (int w = 1; w < 8; w++) {
+      t.x += s[w][lane].x;
+      t.y += s[w][lane].y;
+    }
+    partial[(size_t)blockIdx.y * C + c] = t.x;
+    partial[(size_t)blockIdx.y * C + c + 1] = t.y;
+  }
+}
+
+// g = sum of nsplit partial gradients; Adam step on the fp32 master weights;
+// bf16 copy for the GEMMs.
+__global__ void k_adam(float* __restrict__ w, float* __restrict__ m, float* __restrict__ v,
+                       const float* __restrict__ partial, int nsplit, long long n, __nv_bfloat16* __restrict__ w_bf16,
+                       AdamStep a) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  float g = 0.f;
+  for (int s = 0; s < nsplit; s++) g += partial[(size_t)s * n + i];
+  const float mi = a.b1 * m[i] + (1.f - a.b1) * g;
+  const float vi = a.b2 * v[i] + (1.f - a.b2) * g * g;
+  m[i] = mi;
+  v[i] = vi;
+  const float wi = w[i] - a.lr * (mi * a.c1) / (sqrtf(vi * a.c2) + a.eps);
+  w[i] = wi;
+  if (w_bf16) w_bf16[i] = __float2bfloat16_rn(wi);
+}
+
+// w[i] = std * N(0, 1) from a counter-based hash (Box-Muller), bf16 copy.
+__global__ void k_init_normal(float* __restrict__ w, long long n, float stddev, unsigned long long seed,
+                              __nv_bfloat16* __restrict__ w_bf16) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const uint64_t h1 = splitmix64(seed ^ (2ull * (uint64_t)i));
+  const uint64_t h2 = splitmix64(seed ^ (2ull * (uint64_t)i + 1ull));
+  const float z = sqrtf(-2.f * logf(u01(h1))) * cospif(2.f * u01(h2));
+  w[i] = stddev * z;
+  if (w_bf16) w_bf16[i] = __float2bfloat16_rn(w[i]);
+}
+
+// ---------------------------------------------------------------- k-majority
+// assign[i] = nearest centroid (the k = 2 matcher's first index); counts per
+// cluster; changed = number of rows whose cluster moved.
+__global__ void k_assign(const int32_t* __restrict__ idx2, int n, int* __restrict__ assign, int* __restrict__ counts,
+                         int* __restrict__ changed) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int c = idx2[2 * i];
+  if (assign[i] != c) atomicAdd(changed, 1);
+  assign[i] = c;
+  atomicAdd(&counts[c], 1);
+}
+
+// offsets[0..k] = exclusive scan of counts[0..k-1]; cursor = copy of offsets;
+// optional items[0..k] = exclusive scan of ceil(counts / per_item).  One block
+// of 1024 threads; k <= 1024 * 8.
+__global__ void __launch_bounds__(1024) k_scan_counts(const int* __restrict__ counts, int k, int* __restrict__ offsets,
+                                                      int* __restrict__ cursor, int per_item, int* __restrict__ items) {
+  __shared__ int s_sum[1024], s_items[1024];
+  const int t = threadIdx.x;
+  const int per = (k + 1023) / 1024;
+  int local = 0, local_items = 0;
+  for (int j = 0; j < per; j++) {
+    const int c = t * per + j;
+    if (c < k) {
+      local += counts[c];
+      if (per_item > 0) local_items += (counts[c] + per_item - 1) / per_item;
+    }
+  }
+  s_sum[t] = local;
+  s_items[t] = local_items;
+  __syncthreads();
+  for (int o = 1; o < 1024; o <<= 1) {
+    const int a = t >= o ? s_sum[t - o] : 0;
+    const int b = t >= o ? s_items[t - o] : 0;
+    __syncthreads();
+    s_sum[t] += a;
+    s_items[t] += b;
+    __syncthreads();
+  }
+  int run = s_sum[t] - local, run_items = s_items[t] - local_items;
+  for (int j = 0; j < per; j++) {
+    const int c = t * per + j;
+    if (c < k) {
+      offsets[c] = run;
+      if (cursor) cursor[c] = run;
+      if (per_item > 0) items[c] = run_items;
+      run += counts[c];
+      if (per_item > 0) run_items += (counts[c] + per_item - 1) / per_item;
+    }
+  }
+  if (t == 1023) {
+    offsets[k] = s_sum[1023];
+    if (per_item > 0) items[k] = s_items[1023];
+  }
+}
+
+__global__ void k_scatter_members(const int* __restrict__ assign, int n, int* __restrict__ cursor,
+                                  int* __restrict__ members) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  members[atomicAdd(&cursor[assign[i]], 1)] = i;
+}
+
+// Bitwise majority of each cluster's members (ties keep the old bit); an empty
+// cluster takes a database row chosen by a hash of (seed, iteration, cluster).
+// One block of 256 threads per cluster, thread t counts bit t.
+__global__ void __launch_bounds__(256) k_majority(const uint8_t* __restrict__ db, int n, const int* __restrict__ members,
+                                                  const int* __restrict__ offsets, uint8_t* __restrict__ centroids,
+                                                  unsigned long long seed, int iter) {
+  const int c = blockIdx.x;
+  const int t = threadIdx.x;
+  const int beg = offsets[c], end = offsets[c + 1];
+  __shared__ uint32_t s_bits[8];
+  if (t < 8) s_bits[t] = 0u;
+  __syncthreads();
+  uint32_t bit;
+  if (end == beg) {
+    const int src = (int)(splitmix64(seed ^ ((uint64_t)iter << 32) ^ (uint64_t)c) % (uint64_t)n);
+    bit = (db[(size_t)src * 32 + (t >> 3)] >> (t & 7)) & 1u;
+  } else {
+    int cnt = 0;
+    for (int j = beg; j < end; j++) cnt += (db[(size_t)members[j] * 32 + (t >> 3)] >> (t & 7)) & 1;
+    const int size = end - beg;
+    const uint32_t old = (centroids[(size_t)c * 32 + (t >> 3)] >> (t & 7)) & 1u;
+    bit = 2 * cnt > size ? 1u : (2 * cnt < size ? 0u : old);
+  }
+  if (bit) atomicOr(&s_bits[t >> 5], 1u << (t & 31));
+  __syncthreads();
+  if (t < 8) reinterpret_cast<uint32_t*>(centroids + (size_t)c * 32)[t] = s_bits[t];
+}
+
+// out[j] = db row members[j] (32 bytes), two threads per row.
+__global__ void k_gather_rows(const uint8_t* __restrict__ db, const int* __restrict__ members, int n,
+                              uint8_t* __restrict__ out) {
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= 2ll * n) return;
+  const int j = (int)(t >> 1), h = (int)(t & 1);
+  reinterpret_cast<uint4*>(out)[2 * (size_t)j + h] = reinterpret_cast<const uint4*>(db)[2 * (size_t)members[j] + h];
+}
+
+// out[j] = in[idx[j]]
+__global__ void k_gather_i32(const int* __restrict__ in, const int* __restrict__ idx, int n, int* __restrict__ out) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j < n) out[j] = in[idx[j]];
+}
+
+__global__ void k_count(const int* __restrict__ assign, int n, int* __restrict__ counts) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) atomicAdd(&counts[assign[i]], 1);
+}
+
+// acc[0] += sum of loss, acc[1] += sum of correct (one block of 256 per 256 * 8 rows)
+__global__ void __launch_bounds__(256) k_accum_stats(const float* __restrict__ loss, const int* __restrict__ correct,
+                                                     int n, float* __restrict__ acc) {
+  __shared__ float s_l[8], s_c[8];
+  float l = 0.f, c = 0.f;
+  for (int i = blockIdx.x * 256 * 8 + threadIdx.x; i < min(n, (blockIdx.x + 1) * 256 * 8); i += 256) {
+    l += loss[i];
+    c += (float)correct[i];
+  }
+#pragma unroll
+  for (int o = 16; o; o >>= 1) {
+    l += __shfl_xor_sync(0xffffffffu, l, o);
+    c += __shfl_xor_sync(0xffffffffu, c, o);
+  }
+  if ((threadIdx.x & 31) == 0) {
+    s_l[threadIdx.x >> 5] = l;
+    s_c[threadIdx.x >> 5] = c;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    float tl = 0.f, tc = 0.f;
+    for (int w = 0; w < 8; w++) {
+      tl += s_l[w];
+      tc += s_c[w];
+    }
+    atomicAdd(&acc[0], tl);
+    atomicAdd(&acc[1], tc);
+  }
+}
+
+// labels[i] = assign[nearest database row of training row i]
+__global__ void k_labels(const int32_t* __restrict__ idx2, int n, const int* __restrict__ assign,
+                         int* __restrict__ labels) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int nn = idx2[2 * i];
+  labels[i] = nn >= 0 ? assign[nn] : -1;
+}
+
+// ---------------------------------------------------------------- search
+// One warp per query: merge the GEMM's per-tile top-8 keys (tiles * 8 of them)
+// into the query's n_probe best clusters.  margin = logit1 - logit2.  A query
+// whose margin is below margin_thr goes to the fallback list; otherwise its
+// non-empty probed clusters are counted.  Every partial slot starts empty.
+__global__ void __launch_bounds__(256) k_select_probes(const uint32_t* __restrict__ keys, int nq, int tiles,
+                                                       int n_probe, float margin_thr, const int* __restrict__ ivf_offsets,
+                                                       int* __restrict__ probes, float* __restrict__ margin,
+                                                       int* __restrict__ probe_counts, int* __restrict__ fb_list,
+                                                       int* __restrict__ fb_count, uint2* __restrict__ partial) {
+  const int q = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (q >= nq) return;
+  const int nk = tiles * kTopK;  // <= 128
+  uint32_t mine[4];
+#pragma unroll
+  for (int i = 0; i < 4; i++) {
+    const int j = lane * 4 + i;
+    mine[i] = j < nk ? keys[(size_t)q * nk + j] : 0u;
+  }
+  // keep the lane's four keys in descending order
+#pragma unroll
+  for (int a = 0; a < 3; a++)
+#pragma unroll
+    for (int b = 0; b < 3 - a; b++) {
+      const uint32_t hi = max(mine[b], mine[b + 1]), lo = min(mine[b], mine[b + 1]);
+      mine[b] = hi;
+      mine[b + 1] = lo;
+    }
+  uint32_t best[kTopK];
+#pragma unroll
+  for (int i = 0; i < kTopK; i++) {
+    const uint32_t m = __reduce_max_sync(0xffffffffu, mine[0]);
+    best[i] = m;
+    if (mine[0] == m && m != 0u) {
+      mine[0] = mine[1];
+      mine[1] = mine[2];
+      mine[2] = mine[3];
+      mine[3] = 0u;
+    }
+  }
+  const float l1 = order_bits_float(best[0] & ~((1u << kTopColBits) - 1u));
+  const float l2 = order_bits_float(best[1] & ~((1u << kTopColBits) - 1u));
+  const float mg = l1 - l2;
+  const bool fb = mg < margin_thr;
+  if (lane < kTopK) partial[(size_t)q * kTopK + lane] = make_uint2(kNoKeyShared, kNoKeyShared);
+  if (lane == 0) {
+    margin[q] = mg;
+    if (fb) fb_list[atomicAdd(fb_count, 1)] = q;
+  }
+  if (lane < kTopK) {
+    int c = -1;
+#pragma unroll
+    for (int i = 0; i < kTopK; i++)
+      if (i == lane) c = best[i] ? top_key_col(best[i]) : -1;
+    if (lane >= n_probe || fb || c < 0 || ivf_offsets[c + 1] == ivf_offsets[c]) c = -1;
+    probes[(size_t)q * kTopK + lane] = c;
+    if (c >= 0) atomicAdd(&probe_counts[c], 1);
+  }
+}
+
+// list[cursor[c]++] = q * 8 + slot for every live probe (q, slot) of cluster c
+__global__ void k_fill_probe_lists(const int* __restrict__ probes, int nq, int* __restrict__ cursor,
+                                   int* __restrict__ list) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= nq * kTopK) return;
+  const int c = probes[t];
+  if (c >= 0) list[atomicAdd(&cursor[c], 1)] = t;
+}
+
+constexpr int kRerankChunk = 256;
+
+// One block per (cluster, up to 128 probing queries): each thread holds one
+// query; the cluster's rows stream through shared memory; the exact top-2 of
+// the cluster (keys = distance << 22 | database index) goes to the probe slot.
+__global__ void __launch_bounds__(kRerankQ) k_rerank(const uint8_t* __restrict__ q_desc, const int* __restrict__ list,
+                                                     const int* __restrict__ probe_offsets,
+                                                     const int* __restrict__ item_offsets, int n_clusters,
+                                                     const uint8_t* __restrict__ ivf_desc,
+                                                     const int* __restrict__ ivf_members,
+                                                     const int* __restrict__ ivf_offsets, uint2* __restrict__ partial) {
+  __shared__ uint4 s_db[kRerankChunk * 2];
+  __shared__ int s_id[kRerankChunk];
+  const int item = blockIdx.x;
+  if (item >= item_offsets[n_clusters]) return;
+  // cluster c with item_offsets[c] <= item < item_offsets[c + 1]
+  int lo = 0, hi = n_clusters;
+  while (hi - lo > 1) {
+    const int mid = (lo + hi) >> 1;
+    if (item_offsets[mid] <= item) lo = mid;
+    else hi = mid;
+  }
+  const int c = lo;
+  const int e0 = probe_offsets[c] + (item - item_offsets[c]) * kRerankQ;
+  const int e1 = min(e0 + kRerankQ, probe_offsets[c + 1]);
+  const int e = e0 + (int)threadIdx.x;
+  const bool active = e < e1;
+  const int slot = active ? list[e] : 0;
+  uint32_t qw[8];
+  {
+    const uint4* qp = reinterpret_cast<const uint4*>(q_desc) + 2 * (size_t)(slot >> 3);
+    const uint4 v0 = __ldg(qp), v1 = __ldg(qp + 1);
+    qw[0] = v0.x; qw[1] = v0.y; qw[2] = v0.z; qw[3] = v0.w;
+    qw[4] = v1.x; qw[5] = v1.y; qw[6] = v1.z; qw[7] = v1.w;
+  }
+  const int r_beg = ivf_offsets[c], r_end = ivf_offsets[c + 1];
+  uint32_t k1 = kNoKeyShared, k2 = kNoKeyShared;
+  const uint4* db4 = reinterpret_cast<const uint4*>(ivf_desc);
+  for (int r0 = r_beg; r0 < r_end; r0 += kRerankChunk) {
+    const int rows = min(kRerankChunk, r_end - r0);
+    __syncthreads();
+    for (int i = threadIdx.x; i < rows * 2; i += kRerankQ) s_db[i] = __ldg(db4 + 2 * (size_t)r0 + i);
+    for (int i = threadIdx.x; i < rows; i += kRerankQ) s_id[i] = __ldg(ivf_members + r0 + i);
+    __syncthreads();
+    for (int j = 0; j < rows; j++) {
+      const uint4 t0 = s_db[2 * j], t1 = s_db[2 * j + 1];
+      const uint32_t d = __popc(qw[0] ^ t0.x) + __popc(qw[1] ^ t0.y) + __popc(qw[2] ^ t0.z) +
+                         __popc(qw[3] ^ t0.w) + __popc(qw[4] ^ t1.x) + __popc(qw[5] ^ t1.y) +
+                         __popc(qw[6] ^ t1.z) + __popc(qw[7] ^ t1.w);
+      top2_push_shared(k1, k2, (d << kIdxBitsShared) | (uint32_t)s_id[j]);
+    }
+  }
+  if (active) partial[slot] = make_uint2(k1, k2);
+}
+
+// Per query not sent to the fallback: top-2 over its probe slots.
+__global__ void k_merge_probes(const uint2* __restrict__ partial, int nq, const float* __restrict__ margin,
+                               float margin_thr, uint32_t* __restrict__ dist2, int32_t* __restrict__ idx2) {
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= nq) return;
+  if (margin[q] < margin_thr) return;
+  uint32_t k1 = kNoKeyShared, k2 = kNoKeyShared;
+#pragma unroll
+  for (int s = 0; s < kTopK; s++) {
+    const uint2 p = partial[(size_t)q * kTopK + s];
+    top2_push_shared(k1, k2, p.x);
+    top2_push_shared(k1, k2, p.y);
+  }
+  MatchArgs a{};
+  a.dist2 = dist2;
+  a.idx2 = idx2;
+  finish_query_shared(a, q, k1, k2);
+}
+
+__global__ void k_gather_fallback(const uint8_t* __restrict__ q_desc, const int* __restrict__ fb_list,
+                                  const int* __restrict__ fb_count, uint8_t* __restrict__ out) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if ((t >> 1) >= *fb_count) return;
+  const int j = t >> 1, h = t & 1;
+  reinterpret_cast<uint4*>(out)[2 * (size_t)j + h] =
+      reinterpret_cast<const uint4*>(q_desc)[2 * (size_t)fb_list[j] + h];
+}
+
+__global__ void k_scatter_fallback(const int* __restrict__ fb_list, const int* __restrict__ fb_count,
+                                   const uint32_t* __restrict__ fd, const int32_t* __restrict__ fi,
+                                   uint32_t* __restrict__ dist2, int32_t* __restrict__ idx2) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= *fb_count) return;
+  const int q = fb_list[j];
+  dist2[2 * q] = fd[2 * j];
+  dist2[2 * q + 1] = fd[2 * j + 1];
+  idx2[2 * q] = fi[2 * j];
+  idx2[2 * q + 1] = fi[2 * j + 1];
+}
+
+// ---------------------------------------------------------------- LSH ablation
+// Random-projection buckets: bucket = sign bits of the first nbits projections.
+// Probes: the own bucket, then single-bit flips of the least confident bits
+// (smallest |projection|), in that order.
+__global__ void k_lsh_probes(const float* __restrict__ proj, int rows_stride, int n, int nbits, int n_probe,
+                             const int* __restrict__ ivf_offsets, int* __restrict__ probes, int* __restrict__ probe_counts,
+                             int* __restrict__ bucket_out, float* __restrict__ margin, uint2* __restrict__ partial) {
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= n) return;
+  const float* p = proj + (size_t)q * rows_stride;
+  int b = 0;
+  float conf[16];
+  int order[16];
+  for (int i = 0; i < nbits; i++) {
+    const float v = p[i];
+    if (v > 0.f) b |= 1 << i;
+    conf[i] = fabsf(v);
+    order[i] = i;
+  }
+  if (bucket_out) bucket_out[q] = b;
+  if (!probes) return;
+  // selection of the n_probe - 1 least confident bits
+  for (int i = 0; i < nbits; i++)
+    for (int j = i + 1; j < nbits; j++)
+      if (conf[order[j]] < conf[order[i]]) {
+        const int t = order[i];
+        order[i] = order[j];
+        order[j] = t;
+      }
+  margin[q] = 3.0e38f;
+  for (int s = 0; s < kTopK; s++) {
+    partial[(size_t)q * kTopK + s] = make_uint2(kNoKeyShared, kNoKeyShared);
+    int c = -1;
+    if (s < n_probe) c = s == 0 ? b : (b ^ (1 << order[s - 1]));
+    if (c >= 0 && ivf_offsets[c + 1] == ivf_offsets[c]) c = -1;
+    probes[(size_t)q * kTopK + s] = c;
+    if (c >= 0) atomicAdd(&probe_counts[c], 1);
+  }
+}
+
+}  // namespace orbx

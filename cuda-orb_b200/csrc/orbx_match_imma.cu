@@ -464,6 +464,12 @@ int imma_default_splits(int nq_cap) {
 }
 int imma_rows_db(int n) { return (n + kIBN - 1) / kIBN * kIBN; }
 
+cudaError_t launch_expand_pm1(const uint8_t* bits, int n, const int* d_n, int rows, int8_t* out, cudaStream_t s) {
+  if (rows <= 0) return cudaSuccess;
+  k_expand_pm1<<<4 * 148, 256, 0, s>>>(bits, n, d_n, rows, out);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_match_imma(const ImmaLaunch& L, cudaStream_t s) {
   if (L.nq_cap <= 0) return cudaSuccess;
   static bool attr_set = false;
@@ -476,8 +482,9 @@ cudaError_t launch_match_imma(const ImmaLaunch& L, cudaStream_t s) {
   const int dbrows = imma_rows_db(L.ndb_cap > 0 ? L.ndb_cap : 1);
   {
     const int blocks = 4 * 148;
-    k_expand_pm1<<<blocks, 256, 0, s>>>(L.args.q, L.args.nq, L.args.d_nq, qrows, L.q_pm1);
-    if (L.ndb_cap > 0) k_expand_pm1<<<blocks, 256, 0, s>>>(L.args.db, L.args.ndb, L.args.d_ndb, dbrows, L.db_pm1);
+    if (!L.q_ready) k_expand_pm1<<<blocks, 256, 0, s>>>(L.args.q, L.args.nq, L.args.d_nq, qrows, L.q_pm1);
+    if (L.ndb_cap > 0 && !L.db_ready)
+      k_expand_pm1<<<blocks, 256, 0, s>>>(L.args.db, L.args.ndb, L.args.d_ndb, dbrows, L.db_pm1);
   }
   CUtensorMap tq, td;
   if (!make_rows_map(&tq, L.q_pm1, (uint64_t)qrows, kIBM)) return cudaErrorInvalidValue;

@@ -95,10 +95,53 @@ def lib():
                                           ctypes.POINTER(Tuning), ctypes.POINTER(ctypes.c_float)]
         L.orbx_profile_batch.argtypes = [vp, i32, ctypes.POINTER(Image), ctypes.POINTER(Image),
                                          ctypes.POINTER(FrameOut), ctypes.POINTER(FrameOut), vp]
+        L.orbx_learned_default_params.argtypes = [ctypes.POINTER(LearnedParams)]
+        L.orbx_learned_build.argtypes = [vp, ctypes.POINTER(LearnedParams), vp, i32, vp, i32, ctypes.POINTER(vp)]
+        L.orbx_learned_search.argtypes = [vp, vp, vp, i32, vp, vp, vp, vp]
+        L.orbx_learned_set_margin.argtypes = [vp, ctypes.c_float]
+        L.orbx_learned_get_stats.argtypes = [vp, ctypes.POINTER(LearnedStats)]
+        L.orbx_learned_export.argtypes = [vp, vp, vp, vp, vp, vp, vp, vp]
+        L.orbx_learned_gradients.argtypes = [vp, vp, vp, vp, i32, vp, vp, vp, vp, vp]
+        L.orbx_learned_destroy.argtypes = [vp]
+        L.orbx_gemm_bf16.argtypes = [vp, vp, vp, i32, i32, i32, vp, i32, i32, vp, vp]
         L.orbx_selftest_pi_minus.argtypes = [ctypes.c_uint32, ctypes.c_uint32]
         L.orbx_selftest_pi_minus.restype = ctypes.c_longlong
         _lib = L
     return _lib
+
+
+PROPOSAL_MLP, PROPOSAL_LSH = 0, 1
+GEMM_F32, GEMM_BIAS_RELU_BF16, GEMM_MASK_BF16, GEMM_BF16, GEMM_TOP8 = 0, 1, 2, 3, 4
+
+
+class LearnedParams(ctypes.Structure):
+    _fields_ = [("proposal", ctypes.c_int), ("n_clusters", ctypes.c_int), ("hidden", ctypes.c_int),
+                ("n_probe", ctypes.c_int), ("kmeans_iters", ctypes.c_int), ("epochs", ctypes.c_int),
+                ("batch", ctypes.c_int), ("lr", ctypes.c_float), ("margin", ctypes.c_float),
+                ("lsh_bits", ctypes.c_int), ("seed", ctypes.c_ulonglong)]
+
+
+class LearnedStats(ctypes.Structure):
+    _fields_ = [("kmeans_iters_run", ctypes.c_int), ("kmeans_last_moved", ctypes.c_int),
+                ("largest_cluster", ctypes.c_int), ("epochs_run", ctypes.c_int),
+                ("loss", ctypes.c_float * 64), ("accuracy", ctypes.c_float * 64), ("build_ms", ctypes.c_float * 4)]
+
+    def to_dict(self):
+        e = self.epochs_run
+        return {"kmeans_iters": self.kmeans_iters_run, "kmeans_last_moved": self.kmeans_last_moved,
+                "largest_cluster": self.largest_cluster, "epochs": e,
+                "loss": [round(float(x), 4) for x in self.loss[:e]],
+                "accuracy": [round(float(x), 4) for x in self.accuracy[:e]],
+                "build_ms": {k: round(float(v), 2) for k, v in zip(("cluster", "labels", "train", "total"),
+                                                                    self.build_ms)}}
+
+
+def learned_params(**kw):
+    p = LearnedParams()
+    _check(lib().orbx_learned_default_params(ctypes.byref(p)), "orbx_learned_default_params")
+    for k, v in kw.items():
+        setattr(p, k, v)
+    return p
 
 
 def status_string(status):
@@ -303,6 +346,101 @@ def knn2_static_ptr(d_q, nq, d_db, ndb, d_dist2, d_idx2, stream=None):
     """orbx_match_knn2_static on the current device; stream is a raw cudaStream_t (int) or None."""
     _check(lib().orbx_match_knn2_static(_ptr(d_q), nq, _ptr(d_db), ndb, _ptr(d_dist2), _ptr(d_idx2), stream),
            "orbx_match_knn2_static")
+
+
+class LearnedIndex:
+    """orbx_learned_*: a trained proposal index over a device database.
+
+    db, train: uint8 CUDA tensors (n, 32); the index keeps its own copy of db."""
+
+    def __init__(self, ctx, db, train=None, params=None):
+        self.ctx = ctx
+        self.params = params if params is not None else learned_params()
+        h = ctypes.c_void_p()
+        ntrain = 0 if train is None else train.shape[0]
+        _check(lib().orbx_learned_build(ctx.h, ctypes.byref(self.params), _ptr(db), db.shape[0], _ptr(train), ntrain,
+                                        ctypes.byref(h)), "orbx_learned_build")
+        self.h = h
+        self.ndb = db.shape[0]
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().orbx_learned_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_margin(self, m):
+        self.params.margin = float(m)
+        _check(lib().orbx_learned_set_margin(self.h, float(m)), "orbx_learned_set_margin")
+
+    def stats(self):
+        st = LearnedStats()
+        _check(lib().orbx_learned_get_stats(self.h, ctypes.byref(st)), "orbx_learned_get_stats")
+        return st.to_dict()
+
+    def search_ptr(self, d_q, nq, d_dist2, d_idx2, d_margin=None, d_fb=None):
+        _check(lib().orbx_learned_search(self.ctx.h, self.h, _ptr(d_q), nq, _ptr(d_dist2), _ptr(d_idx2),
+                                         _ptr(d_margin), _ptr(d_fb)), "orbx_learned_search")
+
+    def search(self, q):
+        """Returns (dist2, idx2, margin, fallback_count tensor) as CUDA tensors."""
+        torch = _torch()
+        nq = q.shape[0]
+        dist = torch.empty((nq, 2), dtype=torch.int32, device=q.device)
+        idx = torch.empty((nq, 2), dtype=torch.int32, device=q.device)
+        margin = torch.empty(nq, dtype=torch.float32, device=q.device)
+        fb = torch.zeros(1, dtype=torch.int32, device=q.device)
+        self.search_ptr(q, nq, dist, idx, margin, fb)
+        return dist, idx, margin, fb
+
+    def export(self, weights=True):
+        p = self.params
+        assign = np.zeros(self.ndb, dtype=np.int32)
+        offsets = np.zeros(p.n_clusters + 1, dtype=np.int32)
+        out = {"assign": assign, "offsets": offsets}
+        args = [None] * 4
+        if weights and p.proposal == PROPOSAL_MLP:
+            out["w1"] = np.zeros((p.hidden, 256), dtype=np.float32)
+            out["b1"] = np.zeros(p.hidden, dtype=np.float32)
+            out["w2"] = np.zeros((p.n_clusters, p.hidden), dtype=np.float32)
+            out["b2"] = np.zeros(p.n_clusters, dtype=np.float32)
+            args = [out[k].ctypes.data for k in ("w1", "b1", "w2", "b2")]
+        _check(lib().orbx_learned_export(self.ctx.h, self.h, assign.ctypes.data, offsets.ctypes.data, *args),
+               "orbx_learned_export")
+        return out
+
+    def gradients(self, x, labels):
+        """x: uint8 CUDA (n, 32), labels: int32 CUDA (n,).  Returns loss and fp32 host gradients."""
+        p = self.params
+        n = x.shape[0]
+        g = {"w1": np.zeros((p.hidden, 256), dtype=np.float32), "b1": np.zeros(p.hidden, dtype=np.float32),
+             "w2": np.zeros((p.n_clusters, p.hidden), dtype=np.float32), "b2": np.zeros(p.n_clusters, dtype=np.float32)}
+        loss = ctypes.c_float()
+        _check(lib().orbx_learned_gradients(self.ctx.h, self.h, _ptr(x), _ptr(labels), n, ctypes.byref(loss),
+                                            *[g[k].ctypes.data for k in ("w1", "b1", "w2", "b2")]),
+               "orbx_learned_gradients")
+        return float(loss.value), g
+
+
+def gemm_bf16(ctx, a, b, mode=GEMM_F32, bias=None, splits=1, aux=None):
+    """C = a @ b.T on the tcgen05 BF16 GEMM; a (M, K), b (N, K) bf16 CUDA tensors."""
+    torch = _torch()
+    M, K = a.shape
+    N = b.shape[0]
+    if mode == GEMM_F32:
+        out = torch.empty((splits, M, N) if splits > 1 else (M, N), dtype=torch.float32, device=a.device)
+    elif mode == GEMM_TOP8:
+        out = torch.empty((M, N // 256, 8), dtype=torch.int32, device=a.device)
+    else:
+        out = torch.empty((M, N), dtype=torch.bfloat16, device=a.device)
+    _check(lib().orbx_gemm_bf16(ctx.h, _ptr(a), _ptr(b), M, N, K, _ptr(bias), mode, splits, _ptr(out), _ptr(aux)),
+           "orbx_gemm_bf16")
+    return out
 
 
 class PairBatch:

@@ -204,6 +204,78 @@ ORBX_API int orbx_profile_batch(orbx_ctx* ctx, int n_pairs, const orbx_image* im
 ORBX_API int orbx_debug_buffers(orbx_ctx* ctx, uint8_t* h_pyr, uint8_t* h_blur, float* h_vmap, int* h_layer,
                                 int* h_total);
 
+/* ---- Learned matching proposal.  No counterpart in the reference, whose only
+ * matcher is exact brute force (orbd.cu:1471-1559).
+ *
+ * An index over a database of descriptors for k = 2 search.  An MLP (256 +-1
+ * inputs -> hidden ReLU -> n_clusters logits, BF16 weights, FP32 accumulate,
+ * trained on the GPU by this library's own forward and backward kernels on the
+ * exact nearest neighbours of training descriptors) picks the n_probe most
+ * likely clusters of a Hamming k-majority clustering of the database; those
+ * clusters are searched exactly; a query whose top-2 logit margin is below
+ * `margin` is answered by exact brute force over the whole database instead.
+ * Outputs have the layout of orbx_match_knn2.  ORBX_PROPOSAL_LSH swaps the
+ * MLP and the clustering for random-projection buckets (for comparison). */
+enum { ORBX_PROPOSAL_MLP = 0, ORBX_PROPOSAL_LSH = 1 };
+
+typedef struct orbx_learned_params {
+  int proposal;     /* ORBX_PROPOSAL_* */
+  int n_clusters;   /* multiple of 256, <= 4096; LSH: 2^lsh_bits */
+  int hidden;       /* multiple of 256 */
+  int n_probe;      /* clusters searched per query, 1..8 */
+  int kmeans_iters; /* upper bound; stops when fewer than 0.1% of rows move */
+  int epochs;
+  int batch;        /* training rows per step, multiple of 128 */
+  float lr;         /* Adam step size, cosine-decayed over the run */
+  float margin;     /* exact fallback below this top-1 minus top-2 logit */
+  int lsh_bits;     /* LSH: log2 of the bucket count, 8..12 */
+  unsigned long long seed;
+} orbx_learned_params;
+
+typedef struct orbx_learned_stats {
+  int kmeans_iters_run;
+  int kmeans_last_moved; /* rows that changed cluster in the last iteration */
+  int largest_cluster;
+  int epochs_run;
+  float loss[64];        /* mean training cross-entropy per epoch */
+  float accuracy[64];    /* training top-1 cluster accuracy per epoch */
+  float build_ms[4];     /* clustering, labels, training, total */
+} orbx_learned_stats;
+
+typedef struct orbx_learned orbx_learned;
+
+ORBX_API int orbx_learned_default_params(orbx_learned_params* p);
+/* Clusters d_db (ndb rows of 32 bytes, kept as a copy), labels the d_train rows
+ * with the cluster of their exact nearest database row and trains the MLP.
+ * Runs on the context's stream and synchronises it. */
+ORBX_API int orbx_learned_build(orbx_ctx* ctx, const orbx_learned_params* p, const uint8_t* d_db, int ndb,
+                                const uint8_t* d_train, int ntrain, orbx_learned** out);
+/* k = 2 search of nq queries; optional d_margin [nq] (top-1 minus top-2 logit)
+ * and d_fallback_count (queries sent to exact search).  Asynchronous. */
+ORBX_API int orbx_learned_search(orbx_ctx* ctx, orbx_learned* index, const uint8_t* d_q, int nq,
+                                 uint32_t* d_dist2, int32_t* d_idx2, float* d_margin, int* d_fallback_count);
+ORBX_API int orbx_learned_set_margin(orbx_learned* index, float margin);
+ORBX_API int orbx_learned_get_stats(const orbx_learned* index, orbx_learned_stats* s);
+/* Host copies for checks: cluster of every database row, cluster offsets
+ * [n_clusters + 1] and the bf16 weights widened to float (any may be NULL). */
+ORBX_API int orbx_learned_export(orbx_ctx* ctx, const orbx_learned* index, int* h_assign, int* h_offsets,
+                                 float* h_w1, float* h_b1, float* h_w2, float* h_b2);
+/* Training loss and gradients of the current weights on n rows with labels
+ * (dW1 [hidden][256], db1, dW2 [n_clusters][hidden], db2), as one training
+ * step computes them, copied to the host.  n is a multiple of 128. */
+ORBX_API int orbx_learned_gradients(orbx_ctx* ctx, orbx_learned* index, const uint8_t* d_x, const int* d_labels, int n,
+                                    float* h_loss, float* h_dw1, float* h_db1, float* h_dw2, float* h_db2);
+ORBX_API int orbx_learned_destroy(orbx_learned* index);
+
+/* The BF16 tensor-core GEMM used by the MLP: C = A * B^T with A [M][K] and
+ * B [N][K] row-major bf16; M % 128 == 0, N % 256 == 0, K % (64 * splits) == 0.
+ * mode 0: fp32 C (+ bias; with splits > 1, splits partial sums [splits][M][N]
+ * and no bias); 1: bf16 relu(C + bias); 2: bf16 C where aux [M][N] > 0;
+ * 3: bf16 C + bias; 4: per row and 256-column tile the 8 largest C + bias as
+ * packed keys, uint32 [M][N / 256][8].  Asynchronous. */
+ORBX_API int orbx_gemm_bf16(orbx_ctx* ctx, const void* d_a, const void* d_b, int M, int N, int K, const float* d_bias,
+                            int mode, int splits, void* d_c, const void* d_aux);
+
 /* Host self-check of the float rounding of (double)pi - r used by the angle
  * kernel (orbd.cu:995), over every float r with bits in [lo_bits, hi_bits).
  * Returns the number of mismatches. */

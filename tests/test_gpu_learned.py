@@ -1,0 +1,219 @@
+"""The learned matching proposal (orbx_learned_*, orbx_gemm_bf16) on the GPU:
+the tcgen05 BF16 GEMM against a PyTorch fp32 reference, the MLP gradients
+against the CPU FP64 oracle (oracle/mlp_oracle.py), k-majority clustering
+layout, search exactness (all-fallback search equals exact brute force,
+probed results are consistent Hamming distances), recall, and the LSH
+ablation on clustered descriptors."""
+import numpy as np
+import pytest
+
+torch = pytest.importorskip("torch")
+pytestmark = pytest.mark.gpu
+
+import orbx  # noqa: E402
+from oracle import mlp_oracle as MO  # noqa: E402
+
+
+@pytest.fixture(scope="module")
+def ctx():
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    c = orbx.Context(0)
+    yield c
+    c.close()
+
+
+def clustered(n_db, n_q, n_centers=512, p_db=0.12, p_q=0.04, seed=0):
+    """Database rows = random centers with bits flipped at p_db; queries = random
+    database rows with bits flipped at p_q."""
+    rng = np.random.Generator(np.random.PCG64(0x0C4100 + seed))
+    centers = rng.integers(0, 2, size=(n_centers, 256), dtype=np.uint8)
+    cid = rng.integers(0, n_centers, size=n_db)
+    bits = centers[cid] ^ (rng.uniform(size=(n_db, 256)) < p_db).astype(np.uint8)
+    src = rng.integers(0, n_db, size=n_q)
+    qbits = bits[src] ^ (rng.uniform(size=(n_q, 256)) < p_q).astype(np.uint8)
+    return np.packbits(bits, axis=1), np.packbits(qbits, axis=1)
+
+
+def bf16_tensor(shape, gen, scale=1.0):
+    return (torch.randn(shape, generator=gen) * scale).to(torch.bfloat16).cuda()
+
+
+@pytest.mark.parametrize("M,N,K", [(128, 256, 64), (256, 512, 320), (512, 4096, 512)])
+def test_gemm_f32_vs_torch(ctx, M, N, K):
+    g = torch.Generator().manual_seed(M + N + K)
+    a, b = bf16_tensor((M, K), g), bf16_tensor((N, K), g)
+    bias = torch.randn(N, generator=g).cuda()
+    ref = a.float() @ b.float().T + bias
+    out = orbx.gemm_bf16(ctx, a, b, orbx.GEMM_F32, bias=bias)
+    ctx.sync()
+    # fp32 accumulation of exact bf16 products: only the summation order differs
+    assert torch.allclose(out, ref, rtol=1e-5, atol=1e-4 * K ** 0.5)
+
+
+def test_gemm_split_k(ctx):
+    g = torch.Generator().manual_seed(7)
+    a, b = bf16_tensor((256, 1024), g), bf16_tensor((512, 1024), g)
+    out = orbx.gemm_bf16(ctx, a, b, orbx.GEMM_F32, splits=4)
+    ctx.sync()
+    ref = a.float() @ b.float().T
+    assert out.shape == (4, 256, 512)
+    assert torch.allclose(out.sum(0), ref, rtol=1e-5, atol=1e-2)
+    # each split is the product over its quarter of K
+    q = 1024 // 4
+    for s in range(4):
+        part = a[:, s * q:(s + 1) * q].float() @ b[:, s * q:(s + 1) * q].float().T
+        assert torch.allclose(out[s], part, rtol=1e-5, atol=5e-3)
+
+
+def test_gemm_bf16_epilogues(ctx):
+    g = torch.Generator().manual_seed(11)
+    M, N, K = 256, 512, 256
+    a, b = bf16_tensor((M, K), g), bf16_tensor((N, K), g)
+    bias = torch.randn(N, generator=g).cuda()
+    ref = a.float() @ b.float().T
+    relu = orbx.gemm_bf16(ctx, a, b, orbx.GEMM_BIAS_RELU_BF16, bias=bias)
+    plain = orbx.gemm_bf16(ctx, a, b, orbx.GEMM_BF16, bias=bias)
+    aux = bf16_tensor((M, N), g)
+    aux[:, ::7] = 0
+    masked = orbx.gemm_bf16(ctx, a, b, orbx.GEMM_MASK_BF16, aux=aux)
+    ctx.sync()
+    tol = dict(rtol=2 ** -7, atol=1e-3)
+    assert torch.allclose(relu.float(), torch.relu(ref + bias), **tol)
+    assert torch.allclose(plain.float(), ref + bias, **tol)
+    assert torch.allclose(masked.float(), ref * (aux.float() > 0), **tol)
+    assert bool((masked[:, ::7] == 0).all())
+
+
+def test_gemm_top8(ctx):
+    g = torch.Generator().manual_seed(13)
+    M, N, K = 256, 1024, 512
+    a, b = bf16_tensor((M, K), g), bf16_tensor((N, K), g)
+    bias = torch.randn(N, generator=g).cuda()
+    keys = orbx.gemm_bf16(ctx, a, b, orbx.GEMM_TOP8, bias=bias)
+    ctx.sync()
+    ref = (a.float() @ b.float().T + bias).cpu().numpy()
+    k = keys.cpu().numpy().astype(np.uint32)  # (M, N / 256, 8)
+    cols = 4095 - (k & 0xFFF).astype(np.int64)
+    for t in range(N // 256):
+        tile = ref[:, t * 256:(t + 1) * 256]
+        kth = np.sort(tile, axis=1)[:, -8]
+        got = np.take_along_axis(ref, cols[:, t, :], axis=1)
+        assert np.all((cols[:, t, :] >= t * 256) & (cols[:, t, :] < (t + 1) * 256))
+        # every returned column is at least the tile's 8th largest (keys keep ~2^-11 of the logit)
+        assert np.all(got >= kth[:, None] - 1e-3 * np.abs(kth[:, None]) - 1e-3)
+        # descending, distinct
+        assert np.all(np.diff(k[:, t, :].astype(np.int64), axis=1) < 0)
+
+
+@pytest.fixture(scope="module")
+def small_index(ctx):
+    db, q = clustered(16384, 4096, seed=1)
+    train = clustered(16384, 8192, seed=1)[1][4096:]  # other noisy copies of the same database
+    p = orbx.learned_params(n_clusters=256, hidden=256, epochs=10, batch=512, kmeans_iters=12, lr=3e-3)
+    tdb, tq, ttr = (torch.from_numpy(x).cuda() for x in (db, q, train))
+    idx = orbx.LearnedIndex(ctx, tdb, ttr, p)
+    yield idx, db, q, tdb, tq
+    idx.close()
+
+
+def test_kmeans_layout(small_index):
+    idx, db, *_ = small_index
+    ex = idx.export(weights=False)
+    counts = np.bincount(ex["assign"], minlength=256)
+    assert ex["offsets"][0] == 0 and ex["offsets"][-1] == len(db)
+    assert np.array_equal(np.diff(ex["offsets"]), counts)
+    st = idx.stats()
+    assert st["kmeans_iters"] >= 1 and st["largest_cluster"] == counts.max()
+
+
+def test_training_reduces_loss(small_index):
+    st = small_index[0].stats()
+    assert st["epochs"] == 10
+    assert st["loss"][-1] < 0.5 * st["loss"][0]
+    assert st["accuracy"][-1] > 0.5
+
+
+def test_gradients_vs_fp64_oracle(ctx, small_index):
+    idx, db, q, tdb, tq = small_index
+    rng = np.random.Generator(np.random.PCG64(0x0C4200))
+    n = 256
+    x = q[:n]
+    labels = rng.integers(0, 256, size=n).astype(np.int32)
+    loss, g = idx.gradients(tq[:n].contiguous(), torch.from_numpy(labels).cuda())
+    w = idx.export()
+    ref_loss, ref = MO.forward_backward(x, labels, w["w1"], w["b1"], w["w2"], w["b2"], bf16=False)
+    _, ref16 = MO.forward_backward(x, labels, w["w1"], w["b1"], w["w2"], w["b2"], bf16=True)
+    assert abs(loss - ref_loss) < 1e-3 * max(1.0, abs(ref_loss))
+    for k in ("w1", "b1", "w2", "b2"):
+        err = np.linalg.norm(g[k] - ref[k]) / np.linalg.norm(ref[k])
+        err16 = np.linalg.norm(g[k] - ref16[k]) / np.linalg.norm(ref16[k])
+        assert err < 2e-2, (k, err)      # against exact FP64 arithmetic
+        assert err16 < 5e-3, (k, err16)  # against FP64 with the GPU's bf16 roundings
+
+
+def test_search_all_fallback_is_exact(ctx, small_index):
+    idx, db, q, tdb, tq = small_index
+    idx.set_margin(3.0e38)
+    try:
+        d, i, m, fb = idx.search(tq)
+        ed, ei = orbx.knn2(ctx, tq, tdb, orbx.MATCH_IMMA)
+        ctx.sync()
+        assert int(fb.item()) == len(q)
+        assert torch.equal(d, ed) and torch.equal(i, ei)
+    finally:
+        idx.set_margin(0.0)
+
+
+def _check_consistent(q, db, d, i):
+    d, i = d.cpu().numpy(), i.cpu().numpy()
+    ok = i[:, 0] >= 0
+    qb = np.unpackbits(q[ok], axis=1)
+    rb = np.unpackbits(db[i[ok, 0]], axis=1)
+    assert np.array_equal((qb != rb).sum(1), d[ok, 0])
+    return d, i
+
+
+def test_search_recall_and_margin(ctx, small_index):
+    idx, db, q, tdb, tq = small_index
+    d, i, m, fb = idx.search(tq)
+    ctx.sync()
+    assert int(fb.item()) == 0  # margin 0 never falls back
+    d, i = _check_consistent(q, db, d, i)
+    ed, ei = MO.knn1_bruteforce(q, db)
+    assert np.all(d[:, 0] >= ed)
+    recall = float(np.mean(d[:, 0] == ed))
+    assert recall > 0.9, recall
+    # queries below a margin threshold go to exact search: recall can only rise
+    mm = m.cpu().numpy()
+    thr = float(np.quantile(mm, 0.2))
+    idx.set_margin(thr)
+    try:
+        d2, i2, _, fb2 = idx.search(tq)
+        ctx.sync()
+        n_fb = int(fb2.item())
+        assert n_fb == int(np.sum(mm < thr))
+        d2, _ = _check_consistent(q, db, d2, i2)
+        assert np.all(d2[:, 0] >= ed)
+        assert np.all(d2[mm < thr, 0] == ed[mm < thr])
+        assert float(np.mean(d2[:, 0] == ed)) >= recall
+    finally:
+        idx.set_margin(0.0)
+
+
+def test_lsh_ablation(ctx, small_index):
+    idx, db, q, tdb, tq = small_index
+    d, i, _, _ = idx.search(tq)
+    p = orbx.learned_params(proposal=orbx.PROPOSAL_LSH, lsh_bits=8, n_clusters=256)
+    lsh = orbx.LearnedIndex(ctx, tdb, None, p)
+    try:
+        ld, li, _, lfb = lsh.search(tq)
+        ctx.sync()
+        assert int(lfb.item()) == 0
+        ld, _ = _check_consistent(q, db, ld, li)
+        ed, _ = MO.knn1_bruteforce(q, db)
+        r_mlp = float(np.mean(d.cpu().numpy()[:, 0] == ed))
+        r_lsh = float(np.mean(ld[:, 0] == ed))
+        assert r_mlp > r_lsh, (r_mlp, r_lsh)
+    finally:
+        lsh.close()
