@@ -213,6 +213,69 @@ __global__ void k_init_normal(float* __restrict__ w, long long n, float stddev, 
   if (w_bf16) w_bf16[i] = __float2bfloat16_rn(w[i]);
 }
 
+// MLP weights that compute nearest-centroid scores: hidden unit j < 256 is
+// relu(x_j), unit 256 + j is relu(-x_j) (the rest start at zero), so with
+// s_c = +-1 centroid bits, logit_c = scale * sum_j s_cj (relu(x_j) - relu(-x_j))
+// = scale * (256 - 2 * Hamming(x, centroid c)).
+__global__ void k_init_centroid_mlp(const uint8_t* __restrict__ centroids, int C, int Hd, float scale,
+                                    float* __restrict__ w1, float* __restrict__ b1, float* __restrict__ w2,
+                                    float* __restrict__ b2, __nv_bfloat16* __restrict__ w1b,
+                                    __nv_bfloat16* __restrict__ w2b) {
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long long n1 = (long long)Hd * 256, n2 = (long long)C * Hd;
+  if (t < n1) {
+    const int j = (int)(t / 256), k = (int)(t % 256);
+    const float v = (j < 256 && j == k) ? 1.f : ((j >= 256 && j < 512 && j - 256 == k) ? -1.f : 0.f);
+    w1[t] = v;
+    w1b[t] = __float2bfloat16_rn(v);
+  }
+  if (t < n2) {
+    const int c = (int)(t / Hd), j = (int)(t % Hd);
+    float v = 0.f;
+    if (j < 512) {
+      const int k = j & 255;
+      const float sbit = ((centroids[(size_t)c * 32 + (k >> 3)] >> (k & 7)) & 1u) ? 1.f : -1.f;
+      v = j < 256 ? scale * sbit : -scale * sbit;
+    }
+    w2[t] = v;
+    w2b[t] = __float2bfloat16_rn(v);
+  }
+  if (t < Hd) b1[t] = 0.f;
+  if (t < C) b2[t] = 0.f;
+}
+
+// out[r] = a random database row with each bit flipped with probability
+// p_r ~ U[flip_lo, flip_hi] (counter-based hash per row and bit).  One thread
+// per (row, 32-bit word).
+__global__ void k_perturb_rows(const uint8_t* __restrict__ db, int ndb, int n, unsigned long long seed, float flip_lo,
+                               float flip_hi, uint8_t* __restrict__ out) {
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= 8ll * n) return;
+  const int r = (int)(t >> 3), w = (int)(t & 7);
+  const uint64_t hr = splitmix64(seed ^ (0x9E37ull << 40) ^ (uint64_t)r);
+  const int src = (int)(hr % (uint64_t)ndb);
+  const float p = fminf(flip_lo + (flip_hi - flip_lo) * u01(splitmix64(hr ^ 0x5bd1e995ull)), 0.99999994f);
+  const uint32_t thr = (uint32_t)(fmaxf(p, 0.f) * 16777216.0f) << 8;  // p * 2^32, below 2^32
+  uint32_t v = reinterpret_cast<const uint32_t*>(db)[(size_t)src * 8 + w];
+  for (int b = 0; b < 32; b++) {
+    const uint32_t h = (uint32_t)splitmix64(hr ^ ((uint64_t)(w * 32 + b) << 32));
+    if (h < thr) v ^= 1u << b;
+  }
+  reinterpret_cast<uint32_t*>(out)[(size_t)r * 8 + w] = v;
+}
+
+// Spill lists: entry e < 2n is row e / 2 in cluster idx2[e] (its nearest, then
+// second-nearest centroid from the k = 2 matcher).
+__global__ void k_count_spill(const int32_t* __restrict__ idx2, int n, int* __restrict__ counts) {
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e < 2 * n && idx2[e] >= 0) atomicAdd(&counts[idx2[e]], 1);
+}
+__global__ void k_scatter_spill(const int32_t* __restrict__ idx2, int n, int* __restrict__ cursor,
+                                int* __restrict__ members) {
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e < 2 * n && idx2[e] >= 0) members[atomicAdd(&cursor[idx2[e]], 1)] = e >> 1;
+}
+
 // ---------------------------------------------------------------- k-majority
 // assign[i] = nearest centroid (the k = 2 matcher's first index); counts per
 // cluster; changed = number of rows whose cluster moved.
@@ -367,13 +430,13 @@ __global__ void k_labels(const int32_t* __restrict__ idx2, int n, const int* __r
 // ---------------------------------------------------------------- search
 // One warp per query: merge the GEMM's per-tile top-8 keys (tiles * 8 of them)
 // into the query's n_probe best clusters.  margin = logit1 - logit2.  A query
-// whose margin is below margin_thr goes to the fallback list; otherwise its
-// non-empty probed clusters are counted.  Every partial slot starts empty.
+// whose margin is below margin_thr probes nothing (the exact fallback answers
+// it); otherwise its non-empty probed clusters are counted.  Every partial slot
+// starts empty.
 __global__ void __launch_bounds__(256) k_select_probes(const uint32_t* __restrict__ keys, int nq, int tiles,
                                                        int n_probe, float margin_thr, const int* __restrict__ ivf_offsets,
                                                        int* __restrict__ probes, float* __restrict__ margin,
-                                                       int* __restrict__ probe_counts, int* __restrict__ fb_list,
-                                                       int* __restrict__ fb_count, uint2* __restrict__ partial) {
+                                                       int* __restrict__ probe_counts, uint2* __restrict__ partial) {
   const int q = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
   if (q >= nq) return;
@@ -408,12 +471,9 @@ __global__ void __launch_bounds__(256) k_select_probes(const uint32_t* __restric
   const float l1 = order_bits_float(best[0] & ~((1u << kTopColBits) - 1u));
   const float l2 = order_bits_float(best[1] & ~((1u << kTopColBits) - 1u));
   const float mg = l1 - l2;
-  const bool fb = mg < margin_thr;
+  const bool fb = mg < margin_thr;  // answered by the exact fallback: nothing to probe
   if (lane < kTopK) partial[(size_t)q * kTopK + lane] = make_uint2(kNoKeyShared, kNoKeyShared);
-  if (lane == 0) {
-    margin[q] = mg;
-    if (fb) fb_list[atomicAdd(fb_count, 1)] = q;
-  }
+  if (lane == 0) margin[q] = mg;
   if (lane < kTopK) {
     int c = -1;
 #pragma unroll
@@ -489,18 +549,27 @@ __global__ void __launch_bounds__(kRerankQ) k_rerank(const uint8_t* __restrict__
   if (active) partial[slot] = make_uint2(k1, k2);
 }
 
-// Per query not sent to the fallback: top-2 over its probe slots.
+// Per query: top-2 over its probe slots (a database row listed in two probed
+// clusters is counted once).  Queries with margin < margin_thr or a best
+// distance above max_dist go to the fallback list; the others get their result.
 __global__ void k_merge_probes(const uint2* __restrict__ partial, int nq, const float* __restrict__ margin,
-                               float margin_thr, uint32_t* __restrict__ dist2, int32_t* __restrict__ idx2) {
+                               float margin_thr, int max_dist, uint32_t* __restrict__ dist2,
+                               int32_t* __restrict__ idx2, int* __restrict__ fb_list, int* __restrict__ fb_count) {
   const int q = blockIdx.x * blockDim.x + threadIdx.x;
   if (q >= nq) return;
-  if (margin[q] < margin_thr) return;
   uint32_t k1 = kNoKeyShared, k2 = kNoKeyShared;
 #pragma unroll
   for (int s = 0; s < kTopK; s++) {
     const uint2 p = partial[(size_t)q * kTopK + s];
-    top2_push_shared(k1, k2, p.x);
-    top2_push_shared(k1, k2, p.y);
+    if (p.x != k1 && p.x != k2) top2_push_shared(k1, k2, p.x);
+    if (p.y != k1 && p.y != k2) top2_push_shared(k1, k2, p.y);
+  }
+  const bool far = k1 == kNoKeyShared || (int)(k1 >> kIdxBitsShared) > max_dist;
+  if (margin[q] < margin_thr || far) {
+    if (fb_list) {
+      fb_list[atomicAdd(fb_count, 1)] = q;
+      return;
+    }
   }
   MatchArgs a{};
   a.dist2 = dist2;

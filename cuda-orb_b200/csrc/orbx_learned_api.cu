@@ -166,6 +166,7 @@ struct orbx_learned {
   int device = 0;
   orbx_learned_params p{};
   int ndb = 0, C = 0, Hd = 0;
+  int n_entries = 0;  // cluster list entries (ndb, or up to 2 * ndb with spill)
   Arena keep;
   uint8_t* db = nullptr;
   int8_t* db_pm1 = nullptr;
@@ -259,6 +260,9 @@ int check_params(const orbx_learned_params* p) {
     if (p->n_clusters < 256 || p->n_clusters > 4096 || p->n_clusters % 256) return ORBX_ERR_ARG;
     if (p->hidden < 256 || p->hidden > 4096 || p->hidden % 256) return ORBX_ERR_ARG;
     if (p->batch < 128 || p->batch % 128 || p->epochs < 0 || p->epochs > 64 || p->kmeans_iters < 1) return ORBX_ERR_ARG;
+    if (p->spill < 1 || p->spill > 2 || (p->init != ORBX_INIT_CENTROIDS && p->init != ORBX_INIT_RANDOM)) return ORBX_ERR_ARG;
+    if (p->init == ORBX_INIT_CENTROIDS && p->hidden < 512) return ORBX_ERR_ARG;
+    if (p->synth_train < 0 || !(p->flip_lo >= 0.f && p->flip_lo <= p->flip_hi && p->flip_hi <= 0.5f)) return ORBX_ERR_ARG;
   }
   return ORBX_OK;
 }
@@ -309,10 +313,21 @@ int cluster_kmeans(orbx_learned* L, cudaStream_t s, int* err) {
     k_majority<<<C, 256, 0, s>>>(L->db, n, L->ivf_members, L->ivf_offsets, L->centroids, L->p.seed, it);
     LCHK(cudaGetLastError());
   }
+  if (L->p.spill == 2) {
+    // list every row in its nearest and second-nearest cluster (the last assignment's top-2)
+    LCHK(cudaMemsetAsync(counts, 0, sizeof(int) * C, s));
+    k_count_spill<<<grid1(2ll * n, 256), 256, 0, s>>>(idx2, n, counts);
+    k_scan_counts<<<1, 1024, 0, s>>>(counts, C, L->ivf_offsets, cursor, 0, nullptr);
+    k_scatter_spill<<<grid1(2ll * n, 256), 256, 0, s>>>(idx2, n, cursor, L->ivf_members);
+    LCHK(cudaGetLastError());
+  }
   std::vector<int> h_counts(C);
   LCHK(cudaMemcpyAsync(h_counts.data(), counts, sizeof(int) * C, cudaMemcpyDeviceToHost, s));
+  int total = 0;
+  LCHK(cudaMemcpyAsync(&total, L->ivf_offsets + C, sizeof(int), cudaMemcpyDeviceToHost, s));
   LCHK(cudaStreamSynchronize(s));
   L->stats.largest_cluster = *std::max_element(h_counts.begin(), h_counts.end());
+  L->n_entries = total;
   return ORBX_OK;
 }
 
@@ -347,6 +362,7 @@ int cluster_lsh(orbx_learned* L, cudaStream_t s, int* err) {
   LCHK(cudaMemcpyAsync(h_counts.data(), counts, sizeof(int) * C, cudaMemcpyDeviceToHost, s));
   LCHK(cudaStreamSynchronize(s));
   L->stats.largest_cluster = *std::max_element(h_counts.begin(), h_counts.end());
+  L->n_entries = n;
   return ORBX_OK;
 }
 
@@ -372,12 +388,18 @@ int train_mlp(orbx_learned* L, const uint8_t* d_train, int ntrain, const int* la
   float *m, *v;
   LRC(alloc_weights(L, a, &m, &v));
   const size_t n1 = (size_t)Hd * 256, n2 = (size_t)C * Hd;
-  k_init_normal<<<grid1((long long)n1, 256), 256, 0, s>>>(L->w1, (long long)n1, sqrtf(2.0f / 256.0f),
-                                                          L->p.seed ^ 0x77310000ull, L->w1b);
-  k_init_normal<<<grid1((long long)n2, 256), 256, 0, s>>>(L->w2, (long long)n2, sqrtf(1.0f / (float)Hd),
-                                                          L->p.seed ^ 0x77320000ull, L->w2b);
-  LCHK(cudaMemsetAsync(L->b1, 0, sizeof(float) * Hd, s));
-  LCHK(cudaMemsetAsync(L->b2, 0, sizeof(float) * C, s));
+  if (L->p.init == ORBX_INIT_CENTROIDS) {
+    // logit gap of 0.5 per Hamming bit between centroids
+    k_init_centroid_mlp<<<grid1((long long)std::max(n1, n2), 256), 256, 0, s>>>(L->centroids, C, Hd, 0.25f, L->w1,
+                                                                                L->b1, L->w2, L->b2, L->w1b, L->w2b);
+  } else {
+    k_init_normal<<<grid1((long long)n1, 256), 256, 0, s>>>(L->w1, (long long)n1, sqrtf(2.0f / 256.0f),
+                                                            L->p.seed ^ 0x77310000ull, L->w1b);
+    k_init_normal<<<grid1((long long)n2, 256), 256, 0, s>>>(L->w2, (long long)n2, sqrtf(1.0f / (float)Hd),
+                                                            L->p.seed ^ 0x77320000ull, L->w2b);
+    LCHK(cudaMemsetAsync(L->b1, 0, sizeof(float) * Hd, s));
+    LCHK(cudaMemsetAsync(L->b2, 0, sizeof(float) * C, s));
+  }
   LCHK(cudaMemsetAsync(m, 0, sizeof(float) * (n1 + Hd + n2 + C), s));
   LCHK(cudaMemsetAsync(v, 0, sizeof(float) * (n1 + Hd + n2 + C), s));
   k_transpose_bf16<<<dim3(Hd / 32, C / 32), dim3(32, 8), 0, s>>>(L->w2b, C, Hd, L->w2tb);
@@ -494,6 +516,12 @@ ORBX_API int orbx_learned_default_params(orbx_learned_params* p) {
   p->margin = 0.0f;
   p->lsh_bits = 12;
   p->seed = 0x0C4000ull;
+  p->max_distance = 256;
+  p->spill = 2;
+  p->init = ORBX_INIT_CENTROIDS;
+  p->synth_train = 0;
+  p->flip_lo = 0.05f;
+  p->flip_hi = 0.2f;
   return ORBX_OK;
 }
 
@@ -529,8 +557,8 @@ ORBX_API int orbx_learned_build(orbx_ctx* ctx, const orbx_learned_params* p, con
     const int dbrows = imma_rows_db(ndb);
     if (L->keep.alloc(&L->db, (size_t)ndb * 32) || L->keep.alloc(&L->db_pm1, (size_t)dbrows * 256) ||
         L->keep.alloc(&L->centroids, (size_t)L->C * 32) || L->keep.alloc(&L->assign, (size_t)ndb) ||
-        L->keep.alloc(&L->ivf_offsets, (size_t)L->C + 1) || L->keep.alloc(&L->ivf_members, (size_t)ndb) ||
-        L->keep.alloc(&L->ivf_desc, (size_t)ndb * 32) ||
+        L->keep.alloc(&L->ivf_offsets, (size_t)L->C + 1) || L->keep.alloc(&L->ivf_members, (size_t)ndb * 2) ||
+        L->keep.alloc(&L->ivf_desc, (size_t)ndb * 2 * 32) ||
         (p->proposal == ORBX_PROPOSAL_LSH && L->keep.alloc(&L->lsh, 256 * 256))) {
       rc = ORBX_ERR_NOMEM;
       break;
@@ -543,7 +571,7 @@ ORBX_API int orbx_learned_build(orbx_ctx* ctx, const orbx_learned_params* p, con
     }
     rc = p->proposal == ORBX_PROPOSAL_MLP ? cluster_kmeans(L, s, err) : cluster_lsh(L, s, err);
     if (rc) break;
-    k_gather_rows<<<grid1(2ll * ndb, 256), 256, 0, s>>>(L->db, L->ivf_members, ndb, L->ivf_desc);
+    k_gather_rows<<<grid1(2ll * L->n_entries, 256), 256, 0, s>>>(L->db, L->ivf_members, L->n_entries, L->ivf_desc);
     cudaEventRecord(ev[1], s);
     if (p->proposal == ORBX_PROPOSAL_MLP) {
       Arena t;
@@ -551,19 +579,30 @@ ORBX_API int orbx_learned_build(orbx_ctx* ctx, const orbx_learned_params* p, con
       int32_t* idx2;
       uint32_t* dist2;
       int8_t* tq;
-      if (t.alloc(&labels, (size_t)ntrain) || t.alloc(&idx2, 2 * (size_t)ntrain) ||
-          t.alloc(&dist2, 2 * (size_t)ntrain) || t.alloc(&tq, (size_t)imma_rows_q(ntrain) * 256)) {
+      uint8_t* rows;
+      const int nt = ntrain + p->synth_train;
+      if (t.alloc(&labels, (size_t)nt) || t.alloc(&idx2, 2 * (size_t)nt) || t.alloc(&dist2, 2 * (size_t)nt) ||
+          t.alloc(&tq, (size_t)imma_rows_q(nt) * 256) || t.alloc(&rows, (size_t)nt * 32)) {
         rc = ORBX_ERR_NOMEM;
         break;
       }
+      // training rows: the caller's, then database rows with random bit flips
+      if (cudaMemcpyAsync(rows, d_train, (size_t)ntrain * 32, cudaMemcpyDeviceToDevice, s) != cudaSuccess) {
+        rc = ORBX_ERR_CUDA;
+        break;
+      }
+      if (p->synth_train > 0)
+        k_perturb_rows<<<grid1(8ll * p->synth_train, 256), 256, 0, s>>>(L->db, ndb, p->synth_train,
+                                                                         p->seed ^ 0x73796e74ull, p->flip_lo,
+                                                                         p->flip_hi, rows + (size_t)ntrain * 32);
       ImmaWork iw;
-      rc = imma_work_alloc(t, iw, ntrain, ntrain, s);
+      rc = imma_work_alloc(t, iw, nt, nt, s);
       if (rc) break;
-      rc = imma_knn(s, err, iw, d_train, ntrain, nullptr, tq, false, L->db, ndb, L->db_pm1, true, dist2, idx2);
+      rc = imma_knn(s, err, iw, rows, nt, nullptr, tq, false, L->db, ndb, L->db_pm1, true, dist2, idx2);
       if (rc) break;
-      k_labels<<<grid1(ntrain, 256), 256, 0, s>>>(idx2, ntrain, L->assign, labels);
+      k_labels<<<grid1(nt, 256), 256, 0, s>>>(idx2, nt, L->assign, labels);
       cudaEventRecord(ev[2], s);
-      rc = train_mlp(L, d_train, ntrain, labels, s, err);
+      rc = train_mlp(L, rows, nt, labels, s, err);
       if (rc) break;
     } else {
       cudaEventRecord(ev[2], s);
@@ -594,8 +633,10 @@ ORBX_API int orbx_learned_build(orbx_ctx* ctx, const orbx_learned_params* p, con
   return ORBX_OK;
 }
 
-ORBX_API int orbx_learned_search(orbx_ctx* ctx, orbx_learned* L, const uint8_t* d_q, int nq, uint32_t* d_dist2,
-                                 int32_t* d_idx2, float* d_margin, int* d_fallback_count) {
+// The search; with ev non-null, events 0..5 bracket the phases proposal,
+// probe lists, rerank, merge and exact fallback.
+static int search_impl(orbx_ctx* ctx, orbx_learned* L, const uint8_t* d_q, int nq, uint32_t* d_dist2, int32_t* d_idx2,
+                       float* d_margin, int* d_fallback_count, cudaEvent_t* ev) {
   if (!ctx || !L || nq < 0 || (nq > 0 && (!d_q || !d_dist2 || !d_idx2))) return ORBX_ERR_ARG;
   if (ctx_device(ctx) != L->device) return ORBX_ERR_ARG;
   if (nq > (1 << 24)) return ORBX_ERR_SIZE;
@@ -607,6 +648,10 @@ ORBX_API int orbx_learned_search(orbx_ctx* ctx, orbx_learned* L, const uint8_t* 
   const int rows = round_up(nq, 128), C = L->C;
   const bool mlp = L->p.proposal == ORBX_PROPOSAL_MLP;
   const float thr = mlp ? L->p.margin : -3.0e38f;
+  auto mark = [&](int i) {
+    if (ev) cudaEventRecord(ev[i], s);
+  };
+  mark(0);
   LCHK(cudaMemsetAsync(L->counts, 0, sizeof(int) * C, s));
   LCHK(cudaMemsetAsync(L->fb_count, 0, sizeof(int), s));
   k_bits_pm1_bf16<<<grid1((long long)rows * 32, 256), 256, 0, s>>>(d_q, nq, nullptr, rows, L->xq);
@@ -615,18 +660,23 @@ ORBX_API int orbx_learned_search(orbx_ctx* ctx, orbx_learned* L, const uint8_t* 
     LCHK(gemm(s, err, L->hq, L->w2b, rows, C, L->Hd, L->b2, kTop8, 1, nullptr, nullptr, nullptr, L->keys));
     k_select_probes<<<grid1((long long)nq * 32, 256), 256, 0, s>>>(L->keys, nq, C / 256, L->p.n_probe, thr,
                                                                     L->ivf_offsets, L->probes, L->margin, L->counts,
-                                                                    L->fb_list, L->fb_count, L->partial);
+                                                                    L->partial);
   } else {
     LCHK(gemm(s, err, L->xq, L->lsh, rows, 256, 256, nullptr, kStoreF32, 1, L->proj, nullptr, nullptr, nullptr));
     k_lsh_probes<<<grid1(nq, 128), 128, 0, s>>>(L->proj, 256, nq, L->p.lsh_bits, L->p.n_probe, L->ivf_offsets,
                                                 L->probes, L->counts, nullptr, L->margin, L->partial);
   }
+  mark(1);
   k_scan_counts<<<1, 1024, 0, s>>>(L->counts, C, L->offsets, L->cursor, kRerankQ, L->items);
   k_fill_probe_lists<<<grid1((long long)nq * kTopK, 256), 256, 0, s>>>(L->probes, nq, L->cursor, L->list);
+  mark(2);
   const unsigned items_max = grid1((long long)nq * kTopK, kRerankQ) + (unsigned)C;
   k_rerank<<<items_max, kRerankQ, 0, s>>>(d_q, L->list, L->offsets, L->items, C, L->ivf_desc, L->ivf_members,
                                           L->ivf_offsets, L->partial);
-  k_merge_probes<<<grid1(nq, 256), 256, 0, s>>>(L->partial, nq, L->margin, thr, d_dist2, d_idx2);
+  mark(3);
+  k_merge_probes<<<grid1(nq, 256), 256, 0, s>>>(L->partial, nq, L->margin, thr, mlp ? L->p.max_distance : 1 << 20,
+                                                 d_dist2, d_idx2, mlp ? L->fb_list : nullptr, L->fb_count);
+  mark(4);
   LCHK(cudaGetLastError());
   if (mlp) {
     k_gather_fallback<<<grid1(2ll * nq, 256), 256, 0, s>>>(d_q, L->fb_list, L->fb_count, L->fb_q);
@@ -634,15 +684,48 @@ ORBX_API int orbx_learned_search(orbx_ctx* ctx, orbx_learned* L, const uint8_t* 
                  L->fb_d, L->fb_i));
     k_scatter_fallback<<<grid1(nq, 256), 256, 0, s>>>(L->fb_list, L->fb_count, L->fb_d, L->fb_i, d_dist2, d_idx2);
   }
+  mark(5);
   if (d_margin) LCHK(cudaMemcpyAsync(d_margin, L->margin, sizeof(float) * nq, cudaMemcpyDeviceToDevice, s));
   if (d_fallback_count) LCHK(cudaMemcpyAsync(d_fallback_count, L->fb_count, sizeof(int), cudaMemcpyDeviceToDevice, s));
   LCHK(cudaGetLastError());
   return ORBX_OK;
 }
 
+ORBX_API int orbx_learned_search(orbx_ctx* ctx, orbx_learned* L, const uint8_t* d_q, int nq, uint32_t* d_dist2,
+                                 int32_t* d_idx2, float* d_margin, int* d_fallback_count) {
+  return search_impl(ctx, L, d_q, nq, d_dist2, d_idx2, d_margin, d_fallback_count, nullptr);
+}
+
+ORBX_API int orbx_learned_profile_search(orbx_ctx* ctx, orbx_learned* L, const uint8_t* d_q, int nq,
+                                         uint32_t* d_dist2, int32_t* d_idx2, float* h_ms) {
+  if (!ctx || !L || !h_ms) return ORBX_ERR_ARG;
+  Guard g(L->device);
+  cudaEvent_t ev[6];
+  int made = 0;
+  int rc = ORBX_OK;
+  for (; made < 6; made++)
+    if (cudaEventCreate(&ev[made]) != cudaSuccess) {
+      rc = ORBX_ERR_CUDA;
+      break;
+    }
+  if (!rc) rc = search_impl(ctx, L, d_q, nq, d_dist2, d_idx2, nullptr, nullptr, ev);
+  if (!rc && cudaStreamSynchronize(ctx_stream(ctx)) != cudaSuccess) rc = ORBX_ERR_CUDA;
+  if (!rc)
+    for (int i = 0; i < 5; i++) cudaEventElapsedTime(&h_ms[i], ev[i], ev[i + 1]);
+  for (int i = 0; i < made; i++) cudaEventDestroy(ev[i]);
+  (void)cudaGetLastError();
+  return rc;
+}
+
 ORBX_API int orbx_learned_set_margin(orbx_learned* L, float margin) {
   if (!L) return ORBX_ERR_ARG;
   L->p.margin = margin;
+  return ORBX_OK;
+}
+
+ORBX_API int orbx_learned_set_max_distance(orbx_learned* L, int max_distance) {
+  if (!L) return ORBX_ERR_ARG;
+  L->p.max_distance = max_distance;
   return ORBX_OK;
 }
 

@@ -99,6 +99,8 @@ def lib():
         L.orbx_learned_build.argtypes = [vp, ctypes.POINTER(LearnedParams), vp, i32, vp, i32, ctypes.POINTER(vp)]
         L.orbx_learned_search.argtypes = [vp, vp, vp, i32, vp, vp, vp, vp]
         L.orbx_learned_set_margin.argtypes = [vp, ctypes.c_float]
+        L.orbx_learned_set_max_distance.argtypes = [vp, i32]
+        L.orbx_learned_profile_search.argtypes = [vp, vp, vp, i32, vp, vp, vp]
         L.orbx_learned_get_stats.argtypes = [vp, ctypes.POINTER(LearnedStats)]
         L.orbx_learned_export.argtypes = [vp, vp, vp, vp, vp, vp, vp, vp]
         L.orbx_learned_gradients.argtypes = [vp, vp, vp, vp, i32, vp, vp, vp, vp, vp]
@@ -111,6 +113,7 @@ def lib():
 
 
 PROPOSAL_MLP, PROPOSAL_LSH = 0, 1
+INIT_CENTROIDS, INIT_RANDOM = 0, 1
 GEMM_F32, GEMM_BIAS_RELU_BF16, GEMM_MASK_BF16, GEMM_BF16, GEMM_TOP8 = 0, 1, 2, 3, 4
 
 
@@ -118,7 +121,9 @@ class LearnedParams(ctypes.Structure):
     _fields_ = [("proposal", ctypes.c_int), ("n_clusters", ctypes.c_int), ("hidden", ctypes.c_int),
                 ("n_probe", ctypes.c_int), ("kmeans_iters", ctypes.c_int), ("epochs", ctypes.c_int),
                 ("batch", ctypes.c_int), ("lr", ctypes.c_float), ("margin", ctypes.c_float),
-                ("lsh_bits", ctypes.c_int), ("seed", ctypes.c_ulonglong)]
+                ("lsh_bits", ctypes.c_int), ("seed", ctypes.c_ulonglong), ("max_distance", ctypes.c_int),
+                ("spill", ctypes.c_int), ("init", ctypes.c_int), ("synth_train", ctypes.c_int),
+                ("flip_lo", ctypes.c_float), ("flip_hi", ctypes.c_float)]
 
 
 class LearnedStats(ctypes.Structure):
@@ -378,6 +383,10 @@ class LearnedIndex:
         self.params.margin = float(m)
         _check(lib().orbx_learned_set_margin(self.h, float(m)), "orbx_learned_set_margin")
 
+    def set_max_distance(self, d):
+        self.params.max_distance = int(d)
+        _check(lib().orbx_learned_set_max_distance(self.h, int(d)), "orbx_learned_set_max_distance")
+
     def stats(self):
         st = LearnedStats()
         _check(lib().orbx_learned_get_stats(self.h, ctypes.byref(st)), "orbx_learned_get_stats")
@@ -386,6 +395,13 @@ class LearnedIndex:
     def search_ptr(self, d_q, nq, d_dist2, d_idx2, d_margin=None, d_fb=None):
         _check(lib().orbx_learned_search(self.ctx.h, self.h, _ptr(d_q), nq, _ptr(d_dist2), _ptr(d_idx2),
                                          _ptr(d_margin), _ptr(d_fb)), "orbx_learned_search")
+
+    def profile_search(self, q, dist, idx):
+        """Per-phase device ms: proposal, lists, rerank, merge, fallback (synchronises)."""
+        ms = np.zeros(5, dtype=np.float32)
+        _check(lib().orbx_learned_profile_search(self.ctx.h, self.h, _ptr(q), q.shape[0], _ptr(dist), _ptr(idx),
+                                                 ms.ctypes.data), "orbx_learned_profile_search")
+        return ms
 
     def search(self, q):
         """Returns (dist2, idx2, margin, fallback_count tensor) as CUDA tensors."""

@@ -148,6 +148,41 @@ def make_image(w, h, seed=0):
     return _pad(_finish(r_noise_a, clean, 3.0))
 
 
+LEARNED_IMAGE_SEED = 0x100000  # images of the learned-proposal workload (disjoint from pair seeds)
+
+
+def make_views(w, h, seed, views, n_blobs=200, n_shapes=100, noise_sigma=3.0):
+    """Image A of make_pair(w, h, seed) and warped copies of its clean part, each
+    with its own homography and noise.  views: a count n (views 0..n-1) or a list
+    of view ids; view 0 is make_pair's B, view k >= 1 draws from its own pair of
+    random streams, so a view is the same whichever other views are asked for."""
+    ids = list(range(views)) if isinstance(views, int) else [int(v) for v in views]
+    rng = np.random.Generator(np.random.PCG64(PAIR_SEED_BASE + int(seed)))
+    ss = rng.bit_generator.seed_seq
+    r_img, r_noise_a, r_warp, r_noise_b = [np.random.Generator(np.random.PCG64(s)) for s in ss.spawn(4)]
+    top = max(ids) if ids else 0
+    extra = ss.spawn(2 * max(0, top))
+    clean = np.zeros((h, w), dtype=np.float64)
+    _blobs(r_img, clean, n_blobs)
+    _shapes(r_img, clean, n_shapes)
+    a = _pad(_finish(r_noise_a, clean, noise_sigma))
+    out = []
+    for k in ids:
+        if k == 0:
+            rw, rn = r_warp, r_noise_b
+        else:
+            rw, rn = (np.random.Generator(np.random.PCG64(s)) for s in extra[2 * k - 2:2 * k])
+        out.append(_pad(_finish(rn, _warp(clean, _homography(rw, w, h)), noise_sigma)))
+    return a, out
+
+
+def learned_image_set(args):
+    """(index, view ids) -> (A, views) of the learned-proposal image with that
+    index (1024 x 1024).  A top-level function so that a process pool can run it."""
+    i, views = args
+    return make_views(1024, 1024, LEARNED_IMAGE_SEED + int(i), list(views))
+
+
 def random_descriptors(n, seed):
     """n uniform random 256-bit descriptors as uint8 (n, 32)."""
     rng = np.random.Generator(np.random.PCG64(0x0C0000 + int(seed)))

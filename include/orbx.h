@@ -230,7 +230,17 @@ typedef struct orbx_learned_params {
   float margin;     /* exact fallback below this top-1 minus top-2 logit */
   int lsh_bits;     /* LSH: log2 of the bucket count, 8..12 */
   unsigned long long seed;
+  int max_distance; /* exact fallback also when the best reranked distance exceeds this (>= 256: off) */
+  int spill;        /* MLP: each database row is listed in its 1 or 2 nearest clusters */
+  int init;         /* ORBX_INIT_CENTROIDS or ORBX_INIT_RANDOM */
+  int synth_train;  /* extra training rows: database rows with random bit flips, exactly labelled */
+  float flip_lo;    /* per-row bit-flip probability of those rows, uniform in [flip_lo, flip_hi] */
+  float flip_hi;
 } orbx_learned_params;
+/* ORBX_INIT_CENTROIDS starts the MLP as nearest-centroid scoring (hidden units
+ * relu(x_k) and relu(-x_k), output c = scaled dot product with centroid c), so
+ * training refines the clustering's own proposal; needs hidden >= 512. */
+enum { ORBX_INIT_CENTROIDS = 0, ORBX_INIT_RANDOM = 1 };
 
 typedef struct orbx_learned_stats {
   int kmeans_iters_run;
@@ -251,10 +261,16 @@ ORBX_API int orbx_learned_default_params(orbx_learned_params* p);
 ORBX_API int orbx_learned_build(orbx_ctx* ctx, const orbx_learned_params* p, const uint8_t* d_db, int ndb,
                                 const uint8_t* d_train, int ntrain, orbx_learned** out);
 /* k = 2 search of nq queries; optional d_margin [nq] (top-1 minus top-2 logit)
- * and d_fallback_count (queries sent to exact search).  Asynchronous. */
+ * and d_fallback_count (queries sent to exact search: margin below `margin`, or
+ * best distance in the probed clusters above `max_distance`).  Asynchronous. */
 ORBX_API int orbx_learned_search(orbx_ctx* ctx, orbx_learned* index, const uint8_t* d_q, int nq,
                                  uint32_t* d_dist2, int32_t* d_idx2, float* d_margin, int* d_fallback_count);
+/* orbx_learned_search with per-phase device times in h_ms[5]: proposal (MLP or
+ * buckets), probe lists, exact rerank, merge, exact fallback.  Synchronises. */
+ORBX_API int orbx_learned_profile_search(orbx_ctx* ctx, orbx_learned* index, const uint8_t* d_q, int nq,
+                                         uint32_t* d_dist2, int32_t* d_idx2, float* h_ms);
 ORBX_API int orbx_learned_set_margin(orbx_learned* index, float margin);
+ORBX_API int orbx_learned_set_max_distance(orbx_learned* index, int max_distance);
 ORBX_API int orbx_learned_get_stats(const orbx_learned* index, orbx_learned_stats* s);
 /* Host copies for checks: cluster of every database row, cluster offsets
  * [n_clusters + 1] and the bf16 weights widened to float (any may be NULL). */

@@ -87,3 +87,41 @@ def test_peaks_file_or_fallback():
     pk, kind = bench.load_peaks()
     assert kind in ("measured", "fallback")
     assert pk["hbm_gbs"] > 1000
+
+
+def test_calibrate_margin():
+    # 10 queries; the proposal is wrong on the three with the smallest margins
+    margin = np.array([0.1, 5.0, 0.2, 3.0, 4.0, 0.3, 6.0, 7.0, 8.0, 9.0])
+    correct = np.array([0, 1, 0, 1, 1, 0, 1, 1, 1, 1], dtype=bool)
+    tau, frac = bench.calibrate_margin(margin, correct, 0.99)
+    assert tau == 3.0 and frac == 0.3      # the three wrong ones fall back
+    tau, frac = bench.calibrate_margin(margin, correct, 0.7)
+    assert tau == 0.1 and frac == 0.0      # already at 0.7
+    tau, frac = bench.calibrate_margin(margin, np.zeros(10, dtype=bool), 0.99)
+    assert tau == float("inf") and frac == 1.0
+
+
+def test_learned_view_ids():
+    short = {"db": True, "q": True, "train": True, "cal": True}
+    assert bench.learned_view_ids(1, short) == [0, 1]
+    assert bench.learned_view_ids(6, short) == [0]
+    assert bench.learned_view_ids(5, short) == [0, 2]
+    short["q"] = False
+    assert bench.learned_view_ids(4, short) == [1]
+
+
+def test_calibrate_fallback_uses_distance():
+    # wrong answers all have a large best distance but ordinary margins
+    rng = np.random.Generator(np.random.PCG64(3))
+    n = 1000
+    margin = rng.uniform(0, 10, n)
+    dstar = rng.integers(10, 40, n)
+    correct = np.ones(n, dtype=bool)
+    bad = rng.choice(n, 50, replace=False)
+    correct[bad] = False
+    dstar[bad] = rng.integers(60, 80, 50)
+    tm, td, frac = bench.calibrate_fallback(margin, dstar, correct, 0.99)
+    # only wrong answers need to fall back: at most the 5% that are wrong, all by distance
+    assert td >= 40 and frac <= 0.05 + 1e-9
+    fb = (margin < tm) | (dstar > td)
+    assert (fb.sum() + (correct & ~fb).sum()) / n >= 0.99
