@@ -1,12 +1,17 @@
 // BF16 GEMM on the 5th-generation tensor cores for the learned matching
 // proposal: C[M x N] = A[M x K] * B[N x K]^T with fp32 accumulation in TMEM.
 //
-// A and B are row-major bf16 with K contiguous (K-major).  One block computes a
-// 128 x 256 tile of C (for one K split): warp 0 streams 64-wide K blocks of A
-// and B through a 4-stage TMA ring (128-byte swizzle, no multicast), warp 1
-// issues tcgen05.mma.kind::f16 (four K = 16 steps per block) into a 256-column
-// TMEM accumulator, and warps 2-5 read the accumulator back (one row per
-// thread) and apply the epilogue chosen by GemmArgs::mode (orbx_learned.cuh).
+// A and B are row-major bf16 with K contiguous (K-major).  The kernel is
+// persistent: one block per SM walks the work items (128 x 256 output tile,
+// K split) blockIdx.x, blockIdx.x + gridDim.x, ...
+//   warp 0     TMA producer: 64-wide K blocks of A and B through a 4-stage
+//              shared-memory ring (128-byte swizzle, no multicast);
+//   warp 1     MMA issuer: tcgen05.mma.kind::f16, four K = 16 steps per K
+//              block, into one of two 256-column TMEM accumulators, so the
+//              next tile's MMAs run while the epilogue drains this one;
+//   warps 2-9  epilogue: warp w reads TMEM lanes 32 * (w % 4) (one output row
+//              per lane) and columns [128 * ((w - 2) / 4), +128) of the tile,
+//              then applies GemmArgs::mode (orbx_learned.cuh).
 // M must be a multiple of 128, N of 256, K of 64 * splits; callers pad.
 #include <cuda.h>
 #include <cuda_bf16.h>
@@ -22,14 +27,16 @@ constexpr int kGBM = 128;
 constexpr int kGBN = 256;
 constexpr int kGBK = 64;  // 128 bytes of bf16: one swizzle atom row
 constexpr int kGStages = 4;
-constexpr int kGThreads = 6 * 32;
+constexpr int kGEpiWarps = 8;
+constexpr int kGThreads = (2 + kGEpiWarps) * 32;
 constexpr uint32_t kGATile = kGBM * kGBK * 2;  // 16 KB
 constexpr uint32_t kGBTile = kGBN * kGBK * 2;  // 32 KB
 constexpr uint32_t kGStage = kGATile + kGBTile;
-constexpr uint32_t kGNumBars = 2 * kGStages + 1;
+constexpr uint32_t kGNumBars = 2 * kGStages + 4;  // full, empty per stage; acc full, acc empty per accumulator
 constexpr uint32_t kGSmemBytes = 1024 + kGStages * kGStage + 8 * kGNumBars + 16;
 static_assert(kGSmemBytes + 16 <= 232448, "exceeds the 227 KB shared-memory opt-in");
-constexpr long long kGDeadlineCycles = 4000000000ll;
+constexpr int kGTmemCols = 2 * kGBN;
+constexpr long long kGDeadlineCycles = 4000000000ll;  // per wait, about 2 s
 // instruction descriptor: F32 accumulate, BF16 x BF16, both K-major, N = 256, M = 128
 constexpr uint32_t kGDesc =
     (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(kGBN >> 3) << 17) | ((uint32_t)(kGBM >> 4) << 24);
@@ -59,13 +66,23 @@ __device__ __forceinline__ bool g_mbar_try(uint32_t bar, uint32_t parity) {
       : "memory");
   return ok != 0;
 }
-__device__ __forceinline__ bool g_mbar_wait(uint32_t bar, uint32_t parity, long long deadline,
-                                            volatile int* abort_flag) {
+// Bounded wait: gives up after kGDeadlineCycles or when another role aborted.
+__device__ __forceinline__ bool g_mbar_wait(uint32_t bar, uint32_t parity, volatile int* abort_flag) {
+  const long long deadline = clock64() + kGDeadlineCycles;
   while (!g_mbar_try(bar, parity)) {
     if (*abort_flag) return false;
     if (clock64() > deadline) return false;
   }
   return true;
+}
+__device__ __forceinline__ void g_mbar_arrive(uint32_t bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
+}
+// Warp-uniform bounded wait: lane 0 polls, the result is broadcast.
+__device__ __forceinline__ bool g_warp_wait(uint32_t bar, uint32_t parity, volatile int* abort_flag) {
+  int ok = 0;
+  if ((threadIdx.x & 31) == 0) ok = g_mbar_wait(bar, parity, abort_flag) ? 1 : 0;
+  return __shfl_sync(0xffffffffu, ok, 0) != 0;
 }
 __device__ __forceinline__ void g_tma_load_2d(uint32_t dst, const CUtensorMap* map, int x, int y, uint32_t bar) {
   asm volatile(
@@ -87,6 +104,7 @@ __device__ __forceinline__ void g_umma_bf16(uint32_t tmem_d, uint64_t da, uint64
 __device__ __forceinline__ void g_umma_commit(uint32_t bar) {
   asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar) : "memory");
 }
+// 32 consecutive accumulator columns of this lane's row (waits for the load)
 __device__ __forceinline__ void g_tmem_ld32(uint32_t taddr, float* v) {
   uint32_t r[32];
   asm volatile(
@@ -104,6 +122,68 @@ __device__ __forceinline__ void g_tmem_ld32(uint32_t taddr, float* v) {
 }
 }  // namespace
 
+// Epilogue of 32 columns [n0, n0 + 32) of row m (values in v).
+__device__ __forceinline__ void g_epilogue_chunk(const GemmArgs& g, int split, int m, int n0, float* v, uint32_t* top) {
+  if (g.bias && g.splits == 1) {
+#pragma unroll
+    for (int j = 0; j < 32; j++) v[j] = __fadd_rn(v[j], __ldg(g.bias + n0 + j));
+  }
+  const size_t off = (size_t)m * g.N + (size_t)n0;
+  if (g.mode == kStoreF32) {
+    float4* dst = reinterpret_cast<float4*>(g.c_f32 + (size_t)split * g.M * g.N + off);
+#pragma unroll
+    for (int j = 0; j < 8; j++) dst[j] = make_float4(v[4 * j], v[4 * j + 1], v[4 * j + 2], v[4 * j + 3]);
+    return;
+  }
+  if (g.mode == kTop8) {
+    float mx = v[0];
+#pragma unroll
+    for (int j = 1; j < 32; j++) mx = fmaxf(mx, v[j]);
+    if (top_key(mx, n0) <= top[kTopK - 1]) return;  // no column of this chunk can enter
+#pragma unroll
+    for (int j = 0; j < 32; j++) {
+      uint32_t key = top_key(v[j], n0 + j);
+      if (key > top[kTopK - 1]) {
+#pragma unroll
+        for (int i = 0; i < kTopK; i++) {
+          const uint32_t hi = max(top[i], key);
+          key = min(top[i], key);
+          top[i] = hi;
+        }
+      }
+    }
+    return;
+  }
+  if (g.mode == kBiasReluBF16) {
+#pragma unroll
+    for (int j = 0; j < 32; j++) v[j] = fmaxf(v[j], 0.f);
+  } else if (g.mode == kMaskBF16) {
+    const uint4* aux = reinterpret_cast<const uint4*>(g.aux + off);
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+      const uint4 w = __ldg(aux + j);
+      const uint32_t ws[4] = {w.x, w.y, w.z, w.w};
+#pragma unroll
+      for (int e = 0; e < 4; e++) {
+        // bf16 > 0: sign bit clear and not zero
+        if ((ws[e] & 0x8000u) || !(ws[e] & 0x7FFFu)) v[8 * j + 2 * e] = 0.f;
+        if ((ws[e] & 0x80000000u) || !(ws[e] & 0x7FFF0000u)) v[8 * j + 2 * e + 1] = 0.f;
+      }
+    }
+  }
+  uint4* dst = reinterpret_cast<uint4*>(g.c_bf16 + off);
+#pragma unroll
+  for (int j = 0; j < 4; j++) {
+    uint32_t w[4];
+#pragma unroll
+    for (int e = 0; e < 4; e++) {
+      const __nv_bfloat162 pr = __floats2bfloat162_rn(v[8 * j + 2 * e], v[8 * j + 2 * e + 1]);
+      w[e] = *reinterpret_cast<const uint32_t*>(&pr);
+    }
+    dst[j] = make_uint4(w[0], w[1], w[2], w[3]);
+  }
+}
+
 __global__ void __launch_bounds__(kGThreads, 1)
     k_gemm_bf16(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, GemmArgs g) {
   extern __shared__ uint8_t smem_raw[];
@@ -114,31 +194,32 @@ __global__ void __launch_bounds__(kGThreads, 1)
   volatile int* s_abort = reinterpret_cast<volatile int*>(s_tmem + 1);
 
   const int n_tiles = g.N / kGBN;
-  const int split = blockIdx.x % g.splits;
-  const int tile = blockIdx.x / g.splits;
-  const int tm = tile / n_tiles;
-  const int tn = tile - tm * n_tiles;
+  const int items = (g.M / kGBM) * n_tiles * g.splits;
   const int kblocks = g.K / kGBK / g.splits;
-  const int kb0 = split * kblocks;
+  const int my_items = blockIdx.x < items ? (items - 1 - (int)blockIdx.x) / (int)gridDim.x + 1 : 0;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const uint32_t bar0 = g_smem_u32(bars);
 #define GBAR_FULL(s) (bar0 + 8u * (s))
 #define GBAR_EMPTY(s) (bar0 + 8u * (kGStages + (s)))
-#define GBAR_ACC (bar0 + 8u * (2 * kGStages))
+#define GBAR_ACCFULL(a) (bar0 + 8u * (2 * kGStages + (a)))
+#define GBAR_ACCEMPTY(a) (bar0 + 8u * (2 * kGStages + 2 + (a)))
 
   if (threadIdx.x == 0) {
     for (int s = 0; s < kGStages; s++) {
       g_mbar_init(GBAR_FULL(s), 1);
       g_mbar_init(GBAR_EMPTY(s), 1);
     }
-    g_mbar_init(GBAR_ACC, 1);
+    for (int a = 0; a < 2; a++) {
+      g_mbar_init(GBAR_ACCFULL(a), 1);
+      g_mbar_init(GBAR_ACCEMPTY(a), kGEpiWarps);
+    }
     *s_abort = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
   }
   if (warp == 1) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(g_smem_u32(s_tmem)),
-                 "r"(256)
+                 "r"(kGTmemCols)
                  : "memory");
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
   }
@@ -146,25 +227,37 @@ __global__ void __launch_bounds__(kGThreads, 1)
   __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   const uint32_t tmem = *s_tmem;
-  const long long deadline = clock64() + kGDeadlineCycles;
 
   if (warp == 0) {
     if (lane == 0) {
+      // TMA producer over every K block of every item of this block
       int issued[kGStages];
       for (int s = 0; s < kGStages; s++) issued[s] = 0;
-      for (int kb = 0; kb < kblocks; kb++) {
-        const int s = kb % kGStages;
-        const int use = kb / kGStages;
-        if (use > 0 && !g_mbar_wait(GBAR_EMPTY(s), (use - 1) & 1, deadline, s_abort)) {
-          *s_abort = 1;
-          atomicOr(g.err, kErrImmaTimeout);
-          break;
+      long long gkb = 0;
+      bool ok = true;
+      for (int j = 0; ok && j < my_items; j++) {
+        const int item = (int)blockIdx.x + j * (int)gridDim.x;
+        const int split = item % g.splits;
+        const int tile = item / g.splits;
+        const int tm = tile / n_tiles, tn = tile - (tile / n_tiles) * n_tiles;
+        for (int kb = 0; kb < kblocks; kb++, gkb++) {
+          const int s = (int)(gkb % kGStages);
+          const long long use = gkb / kGStages;
+          if (use > 0 && !g_mbar_wait(GBAR_EMPTY(s), (uint32_t)((use - 1) & 1), s_abort)) {
+            ok = false;
+            break;
+          }
+          uint8_t* st = smem + s * kGStage;
+          const int kx = (split * kblocks + kb) * kGBK;
+          g_mbar_expect_tx(GBAR_FULL(s), kGStage);
+          g_tma_load_2d(g_smem_u32(st), &tmA, kx, tm * kGBM, GBAR_FULL(s));
+          g_tma_load_2d(g_smem_u32(st + kGATile), &tmB, kx, tn * kGBN, GBAR_FULL(s));
+          issued[s]++;
         }
-        uint8_t* st = smem + s * kGStage;
-        g_mbar_expect_tx(GBAR_FULL(s), kGStage);
-        g_tma_load_2d(g_smem_u32(st), &tmA, (kb0 + kb) * kGBK, tm * kGBM, GBAR_FULL(s));
-        g_tma_load_2d(g_smem_u32(st + kGATile), &tmB, (kb0 + kb) * kGBK, tn * kGBN, GBAR_FULL(s));
-        issued[s]++;
+      }
+      if (!ok) {
+        *s_abort = 1;
+        atomicOr(g.err, kErrImmaTimeout);
       }
       // drain before exit: copies landed and the MMAs that read them completed
       for (int s = 0; s < kGStages; s++) {
@@ -180,118 +273,90 @@ __global__ void __launch_bounds__(kGThreads, 1)
     }
   } else if (warp == 1) {
     if (lane == 0) {
+      long long gkb = 0;
       bool ok = true;
-      for (int kb = 0; kb < kblocks; kb++) {
-        const int s = kb % kGStages;
-        if (!g_mbar_wait(GBAR_FULL(s), (uint32_t)(kb / kGStages) & 1u, deadline, s_abort)) {
+      for (int j = 0; ok && j < my_items; j++) {
+        const int acc = j & 1;
+        if (j >= 2 && !g_mbar_wait(GBAR_ACCEMPTY(acc), (uint32_t)(((j >> 1) - 1) & 1), s_abort)) {
           ok = false;
           break;
         }
-        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-        const uint32_t a_lo = g_smem_u32(smem + s * kGStage);
-        const uint32_t b_lo = a_lo + kGATile;
+        const uint32_t d = tmem + (uint32_t)(acc * kGBN);
+        for (int kb = 0; kb < kblocks; kb++, gkb++) {
+          const int s = (int)(gkb % kGStages);
+          if (!g_mbar_wait(GBAR_FULL(s), (uint32_t)((gkb / kGStages) & 1), s_abort)) {
+            ok = false;
+            break;
+          }
+          asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+          const uint32_t a_lo = g_smem_u32(smem + s * kGStage);
+          const uint32_t b_lo = a_lo + kGATile;
 #pragma unroll
-        for (int k = 0; k < kGBK / 16; k++) {
-          g_umma_bf16(tmem, g_sw128_desc(a_lo) + (uint64_t)(2 * k), g_sw128_desc(b_lo) + (uint64_t)(2 * k), kGDesc,
-                      (kb > 0 || k > 0) ? 1u : 0u);
+          for (int k = 0; k < kGBK / 16; k++) {
+            g_umma_bf16(d, g_sw128_desc(a_lo) + (uint64_t)(2 * k), g_sw128_desc(b_lo) + (uint64_t)(2 * k), kGDesc,
+                        (kb > 0 || k > 0) ? 1u : 0u);
+          }
+          g_umma_commit(GBAR_EMPTY(s));
         }
-        g_umma_commit(GBAR_EMPTY(s));
+        if (ok) g_umma_commit(GBAR_ACCFULL(acc));
       }
-      if (ok) {
-        g_umma_commit(GBAR_ACC);
-      } else {
+      if (!ok) {
         *s_abort = 1;
         atomicOr(g.err, kErrImmaTimeout);
       }
     }
   } else {
-    // epilogue: warp w reads TMEM lanes 32*(w&3).., row m = tm*128 + lane quarter
     const int quarter = warp & 3;
-    int ok = 0;
-    if (lane == 0) ok = g_mbar_wait(GBAR_ACC, 0, deadline, s_abort) ? 1 : 0;
-    ok = __shfl_sync(0xffffffffu, ok, 0);
-    if (ok) {
+    const int half = (warp - 2) >> 2;
+    bool ok = true;
+    for (int j = 0; j < my_items; j++) {
+      const int acc = j & 1;
+      if (!g_warp_wait(GBAR_ACCFULL(acc), (uint32_t)((j >> 1) & 1), s_abort)) {
+        ok = false;
+        break;
+      }
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      const int item = (int)blockIdx.x + j * (int)gridDim.x;
+      const int split = item % g.splits;
+      const int tile = item / g.splits;
+      const int tm = tile / n_tiles, tn = tile - (tile / n_tiles) * n_tiles;
       const int m = tm * kGBM + quarter * 32 + lane;
-      const size_t crow = (size_t)m * g.N + (size_t)tn * kGBN;
-      const bool use_bias = g.bias && g.splits == 1;
       uint32_t top[kTopK];
 #pragma unroll
       for (int i = 0; i < kTopK; i++) top[i] = 0u;
+      const uint32_t tbase = tmem + ((uint32_t)(quarter * 32) << 16) + (uint32_t)(acc * kGBN + half * 128);
 #pragma unroll 1
-      for (int c = 0; c < kGBN / 32; c++) {
+      for (int c = 0; c < 4; c++) {
         float v[32];
-        g_tmem_ld32(tmem + ((uint32_t)(quarter * 32) << 16) + (uint32_t)(c * 32), v);
-        const int n0 = tn * kGBN + c * 32;
-        if (use_bias) {
-#pragma unroll
-          for (int j = 0; j < 32; j++) v[j] = __fadd_rn(v[j], __ldg(g.bias + n0 + j));
+        g_tmem_ld32(tbase + (uint32_t)(c * 32), v);
+        if (c == 3) {
+          // every column of this half is in registers: hand the accumulator back
+          asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+          __syncwarp();
+          if (lane == 0) g_mbar_arrive(GBAR_ACCEMPTY(acc));
         }
-        if (g.mode == kStoreF32) {
-          float4* dst = reinterpret_cast<float4*>(g.c_f32 + (size_t)split * g.M * g.N + crow + c * 32);
-#pragma unroll
-          for (int j = 0; j < 8; j++) dst[j] = make_float4(v[4 * j], v[4 * j + 1], v[4 * j + 2], v[4 * j + 3]);
-        } else if (g.mode == kTop8) {
-#pragma unroll
-          for (int j = 0; j < 32; j++) {
-            uint32_t key = top_key(v[j], n0 + j);
-            if (key > top[kTopK - 1]) {
-#pragma unroll
-              for (int i = 0; i < kTopK; i++) {
-                const uint32_t hi = max(top[i], key);
-                key = min(top[i], key);
-                top[i] = hi;
-              }
-            }
-          }
-        } else {
-          if (g.mode == kBiasReluBF16) {
-#pragma unroll
-            for (int j = 0; j < 32; j++) v[j] = fmaxf(v[j], 0.f);
-          } else if (g.mode == kMaskBF16) {
-            const uint4* aux = reinterpret_cast<const uint4*>(g.aux + crow + c * 32);
-#pragma unroll
-            for (int j = 0; j < 4; j++) {
-              const uint4 w = __ldg(aux + j);
-              const uint32_t ws[4] = {w.x, w.y, w.z, w.w};
-#pragma unroll
-              for (int e = 0; e < 4; e++) {
-                // bf16 > 0: sign bit clear and not zero
-                if ((ws[e] & 0x8000u) || !(ws[e] & 0x7FFFu)) v[8 * j + 2 * e] = 0.f;
-                if ((ws[e] & 0x80000000u) || !(ws[e] & 0x7FFF0000u)) v[8 * j + 2 * e + 1] = 0.f;
-              }
-            }
-          }
-          uint4* dst = reinterpret_cast<uint4*>(g.c_bf16 + crow + c * 32);
-#pragma unroll
-          for (int j = 0; j < 4; j++) {
-            uint32_t w[4];
-#pragma unroll
-            for (int e = 0; e < 4; e++) {
-              const __nv_bfloat162 pr = __floats2bfloat162_rn(v[8 * j + 2 * e], v[8 * j + 2 * e + 1]);
-              w[e] = *reinterpret_cast<const uint32_t*>(&pr);
-            }
-            dst[j] = make_uint4(w[0], w[1], w[2], w[3]);
-          }
-        }
+        g_epilogue_chunk(g, split, m, tn * kGBN + half * 128 + c * 32, v, top);
       }
       if (g.mode == kTop8) {
-        uint4* dst = reinterpret_cast<uint4*>(g.top_keys + ((size_t)m * n_tiles + tn) * kTopK);
+        uint4* dst = reinterpret_cast<uint4*>(g.top_keys + ((size_t)m * (2 * n_tiles) + 2 * tn + half) * kTopK);
         dst[0] = make_uint4(top[0], top[1], top[2], top[3]);
         dst[1] = make_uint4(top[4], top[5], top[6], top[7]);
       }
-    } else if (lane == 0) {
-      atomicOr(g.err, kErrImmaTimeout);
+    }
+    if (!ok) {
+      *s_abort = 1;
+      if (lane == 0) atomicOr(g.err, kErrImmaTimeout);
     }
   }
 #undef GBAR_FULL
 #undef GBAR_EMPTY
-#undef GBAR_ACC
+#undef GBAR_ACCFULL
+#undef GBAR_ACCEMPTY
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   if (warp == 1) {
-    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(256) : "memory");
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kGTmemCols) : "memory");
   }
 }
 
@@ -334,7 +399,11 @@ cudaError_t launch_gemm_bf16(const GemmArgs& g, cudaStream_t s) {
   CUtensorMap ta, tb;
   if (!make_bf16_map(&ta, g.a, (uint64_t)g.M, (uint64_t)g.K, kGBM)) return cudaErrorInvalidValue;
   if (!make_bf16_map(&tb, g.b, (uint64_t)g.N, (uint64_t)g.K, kGBN)) return cudaErrorInvalidValue;
-  const int blocks = (g.M / kGBM) * (g.N / kGBN) * g.splits;
+  int dev = 0, sms = 148;
+  if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
+    return cudaErrorInvalidValue;
+  const int items = (g.M / kGBM) * (g.N / kGBN) * g.splits;
+  const int blocks = items < sms ? items : sms;  // persistent: one block per SM
   k_gemm_bf16<<<blocks, kGThreads, kGSmemBytes, s>>>(ta, tb, g);
   return cudaGetLastError();
 }

@@ -428,30 +428,31 @@ __global__ void k_labels(const int32_t* __restrict__ idx2, int n, const int* __r
 }
 
 // ---------------------------------------------------------------- search
-// One warp per query: merge the GEMM's per-tile top-8 keys (tiles * 8 of them)
-// into the query's n_probe best clusters.  margin = logit1 - logit2.  A query
+// One warp per query: merge the GEMM's top-8 key lists (one per 128 columns,
+// lists * 8 keys) into the query's n_probe best clusters.  margin = logit1 - logit2.  A query
 // whose margin is below margin_thr probes nothing (the exact fallback answers
 // it); otherwise its non-empty probed clusters are counted.  Every partial slot
 // starts empty.
-__global__ void __launch_bounds__(256) k_select_probes(const uint32_t* __restrict__ keys, int nq, int tiles,
+__global__ void __launch_bounds__(256) k_select_probes(const uint32_t* __restrict__ keys, int nq, int lists,
                                                        int n_probe, float margin_thr, const int* __restrict__ ivf_offsets,
                                                        int* __restrict__ probes, float* __restrict__ margin,
                                                        int* __restrict__ probe_counts, uint2* __restrict__ partial) {
   const int q = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
   if (q >= nq) return;
-  const int nk = tiles * kTopK;  // <= 128
-  uint32_t mine[4];
+  const int nk = lists * kTopK;  // <= 256
+  const int kpl = (nk + 31) >> 5;
+  uint32_t mine[8];
 #pragma unroll
-  for (int i = 0; i < 4; i++) {
-    const int j = lane * 4 + i;
-    mine[i] = j < nk ? keys[(size_t)q * nk + j] : 0u;
+  for (int i = 0; i < 8; i++) {
+    const int j = lane * kpl + i;
+    mine[i] = (i < kpl && j < nk) ? keys[(size_t)q * nk + j] : 0u;
   }
-  // keep the lane's four keys in descending order
+  // the lane's keys in descending order
 #pragma unroll
-  for (int a = 0; a < 3; a++)
+  for (int a = 0; a < 7; a++)
 #pragma unroll
-    for (int b = 0; b < 3 - a; b++) {
+    for (int b = 0; b < 7 - a; b++) {
       const uint32_t hi = max(mine[b], mine[b + 1]), lo = min(mine[b], mine[b + 1]);
       mine[b] = hi;
       mine[b + 1] = lo;
@@ -462,10 +463,9 @@ __global__ void __launch_bounds__(256) k_select_probes(const uint32_t* __restric
     const uint32_t m = __reduce_max_sync(0xffffffffu, mine[0]);
     best[i] = m;
     if (mine[0] == m && m != 0u) {
-      mine[0] = mine[1];
-      mine[1] = mine[2];
-      mine[2] = mine[3];
-      mine[3] = 0u;
+#pragma unroll
+      for (int k = 0; k < 7; k++) mine[k] = mine[k + 1];
+      mine[7] = 0u;
     }
   }
   const float l1 = order_bits_float(best[0] & ~((1u << kTopColBits) - 1u));

@@ -15,7 +15,7 @@ enum GemmMode {
   kBiasReluBF16 = 1,  // bf16 max(acc + bias[n], 0)
   kMaskBF16 = 2,      // bf16 acc where aux[m][n] > 0 else 0 (ReLU backward)
   kStoreBF16 = 3,     // bf16 acc (+ bias[n])
-  kTop8 = 4,          // per row and 256-column tile: the 8 largest (acc + bias[n]) as packed keys
+  kTop8 = 4,          // per row and 128 columns: the 8 largest (acc + bias[n]) as packed keys
 };
 
 struct GemmArgs {
@@ -28,7 +28,7 @@ struct GemmArgs {
   float* c_f32;            // kStoreF32
   __nv_bfloat16* c_bf16;   // kBiasReluBF16, kMaskBF16, kStoreBF16
   const __nv_bfloat16* aux;  // kMaskBF16: [M][N]
-  uint32_t* top_keys;      // kTop8: [M][N / 256][8], descending
+  uint32_t* top_keys;      // kTop8: [M][N / 128][8], descending
   int* err;                // device error word
 };
 
@@ -90,7 +90,7 @@ __global__ void k_gather_i32(const int* in, const int* idx, int n, int* out);
 __global__ void k_count(const int* assign, int n, int* counts);
 __global__ void k_accum_stats(const float* loss, const int* correct, int n, float* acc);
 __global__ void k_labels(const int32_t* idx2, int n, const int* assign, int* labels);
-__global__ void k_select_probes(const uint32_t* keys, int nq, int tiles, int n_probe, float margin_thr,
+__global__ void k_select_probes(const uint32_t* keys, int nq, int lists, int n_probe, float margin_thr,
                                 const int* ivf_offsets, int* probes, float* margin, int* probe_counts,
                                 uint2* partial);
 __global__ void k_fill_probe_lists(const int* probes, int nq, int* cursor, int* list);

@@ -475,7 +475,7 @@ int ensure_search(orbx_learned* L, int nq) {
   LCHK(a.alloc(&L->xq, (size_t)rows * 256));
   if (L->p.proposal == ORBX_PROPOSAL_MLP) {
     LCHK(a.alloc(&L->hq, (size_t)rows * L->Hd));
-    LCHK(a.alloc(&L->keys, (size_t)rows * (C / 256) * kTopK));
+    LCHK(a.alloc(&L->keys, (size_t)rows * (C / 128) * kTopK));
   } else {
     LCHK(a.alloc(&L->proj, (size_t)rows * 256));
   }
@@ -658,7 +658,7 @@ static int search_impl(orbx_ctx* ctx, orbx_learned* L, const uint8_t* d_q, int n
   if (mlp) {
     LCHK(gemm(s, err, L->xq, L->w1b, rows, L->Hd, 256, L->b1, kBiasReluBF16, 1, nullptr, L->hq, nullptr, nullptr));
     LCHK(gemm(s, err, L->hq, L->w2b, rows, C, L->Hd, L->b2, kTop8, 1, nullptr, nullptr, nullptr, L->keys));
-    k_select_probes<<<grid1((long long)nq * 32, 256), 256, 0, s>>>(L->keys, nq, C / 256, L->p.n_probe, thr,
+    k_select_probes<<<grid1((long long)nq * 32, 256), 256, 0, s>>>(L->keys, nq, C / 128, L->p.n_probe, thr,
                                                                     L->ivf_offsets, L->probes, L->margin, L->counts,
                                                                     L->partial);
   } else {

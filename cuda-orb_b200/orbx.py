@@ -451,7 +451,7 @@ def gemm_bf16(ctx, a, b, mode=GEMM_F32, bias=None, splits=1, aux=None):
     if mode == GEMM_F32:
         out = torch.empty((splits, M, N) if splits > 1 else (M, N), dtype=torch.float32, device=a.device)
     elif mode == GEMM_TOP8:
-        out = torch.empty((M, N // 256, 8), dtype=torch.int32, device=a.device)
+        out = torch.empty((M, N // 128, 8), dtype=torch.int32, device=a.device)
     else:
         out = torch.empty((M, N), dtype=torch.bfloat16, device=a.device)
     _check(lib().orbx_gemm_bf16(ctx.h, _ptr(a), _ptr(b), M, N, K, _ptr(bias), mode, splits, _ptr(out), _ptr(aux)),

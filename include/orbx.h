@@ -287,8 +287,8 @@ ORBX_API int orbx_learned_destroy(orbx_learned* index);
  * B [N][K] row-major bf16; M % 128 == 0, N % 256 == 0, K % (64 * splits) == 0.
  * mode 0: fp32 C (+ bias; with splits > 1, splits partial sums [splits][M][N]
  * and no bias); 1: bf16 relu(C + bias); 2: bf16 C where aux [M][N] > 0;
- * 3: bf16 C + bias; 4: per row and 256-column tile the 8 largest C + bias as
- * packed keys, uint32 [M][N / 256][8].  Asynchronous. */
+ * 3: bf16 C + bias; 4: per row and 128 columns the 8 largest C + bias as
+ * packed keys, uint32 [M][N / 128][8].  Asynchronous. */
 ORBX_API int orbx_gemm_bf16(orbx_ctx* ctx, const void* d_a, const void* d_b, int M, int N, int K, const float* d_bias,
                             int mode, int splits, void* d_c, const void* d_aux);
 

@@ -93,13 +93,13 @@ def test_gemm_top8(ctx):
     keys = orbx.gemm_bf16(ctx, a, b, orbx.GEMM_TOP8, bias=bias)
     ctx.sync()
     ref = (a.float() @ b.float().T + bias).cpu().numpy()
-    k = keys.cpu().numpy().astype(np.uint32)  # (M, N / 256, 8)
+    k = keys.cpu().numpy().astype(np.uint32)  # (M, N / 128, 8)
     cols = 4095 - (k & 0xFFF).astype(np.int64)
-    for t in range(N // 256):
-        tile = ref[:, t * 256:(t + 1) * 256]
+    for t in range(N // 128):
+        tile = ref[:, t * 128:(t + 1) * 128]
         kth = np.sort(tile, axis=1)[:, -8]
         got = np.take_along_axis(ref, cols[:, t, :], axis=1)
-        assert np.all((cols[:, t, :] >= t * 256) & (cols[:, t, :] < (t + 1) * 256))
+        assert np.all((cols[:, t, :] >= t * 128) & (cols[:, t, :] < (t + 1) * 128))
         # every returned column is at least the tile's 8th largest (keys keep ~2^-11 of the logit)
         assert np.all(got >= kth[:, None] - 1e-3 * np.abs(kth[:, None]) - 1e-3)
         # descending, distinct
