@@ -77,10 +77,11 @@ void Orbor::detectAndCompute(unsigned char* image, OrbData& result, int3 whp0, v
     CHECK(cudaMalloc(desc_addr, (size_t)n * 32));
     CHECK(cudaMemcpy(*desc_addr, d_desc_work_, (size_t)n * 32, cudaMemcpyDeviceToDevice));
   }
-  if (result.h_data && n > 0) {
-    CHECK(cudaMemcpy2D(&result.h_data[0].x, sizeof(OrbPoint), &result.d_data[0].x, sizeof(OrbPoint),
-                       3 * sizeof(int) + 2 * sizeof(float), n, cudaMemcpyDeviceToHost));
-  }
+  // x, y, octave, score, angle of each host entry (orb.cpp:95-100), as one packed copy
+  if (result.h_data && n > 0)
+    orbx_check(orbx_download_points(ctx_, (const orbx_point*)result.d_data, n, (orbx_point*)result.h_data,
+                                    ORBX_FIELDS_KEYPOINT),
+               "Orbor::detectAndCompute");
 }
 
 // hMatch on a given context: the counts are host values (orbd.cu:1788-1790),
@@ -98,10 +99,11 @@ static void match_on(orbx_ctx* c, int* d_cnt, OrbData& result1, OrbData& result2
 void Orbor::match(OrbData& result1, OrbData& result2, unsigned char* desc1, unsigned char* desc2) {
   if (!ctx_) orbx_check(ORBX_ERR_STATE, "Orbor::match");
   match_on(ctx_, d_counts_ + 1, result1, result2, desc1, desc2, "Orbor::match");
-  if (result1.h_data && result1.num_pts > 0) {
-    CHECK(cudaMemcpy2D(&result1.h_data[0].match, sizeof(OrbPoint), &result1.d_data[0].match, sizeof(OrbPoint),
-                       2 * sizeof(int), result1.num_pts, cudaMemcpyDeviceToHost));
-  }
+  // match, distance of each host entry (orb.cpp:108-111), as one packed copy
+  if (result1.h_data && result1.num_pts > 0)
+    orbx_check(orbx_download_points(ctx_, (const orbx_point*)result1.d_data, result1.num_pts,
+                                    (orbx_point*)result1.h_data, ORBX_FIELDS_MATCH),
+               "Orbor::match");
 }
 
 void Orbor::initOrbData(OrbData& data, const int max_pts, const bool host, const bool dev) {

@@ -94,6 +94,7 @@ struct orbx_ctx {
   int* io_count_host = nullptr;  // pinned [2]
   int io_max_pts = 0;
   cudaEvent_t prof_ev[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
+  HostIO* hostio = nullptr;  // orbx_upload_image / orbx_download_points staging
   // launch shapes (orbx_tuning)
   int nms_rows = kNmsRows;
   int describe_bps = 8;
@@ -641,6 +642,7 @@ ORBX_API int orbx_destroy(orbx_ctx* c) {
   }
   cudaFree(c->io_count);
   cudaFreeHost(c->io_count_host);
+  hostio_free(c->hostio);
   for (auto& e : c->prof_ev)
     if (e) cudaEventDestroy(e);
   cudaFree(c->imma_q);
@@ -1331,4 +1333,5 @@ namespace orbx {
 int ctx_device(const orbx_ctx* c) { return c->device; }
 cudaStream_t ctx_stream(const orbx_ctx* c) { return c->stream; }
 int* ctx_err(orbx_ctx* c) { return c->d_err; }
+HostIO*& ctx_hostio(orbx_ctx* c) { return c->hostio; }
 }  // namespace orbx

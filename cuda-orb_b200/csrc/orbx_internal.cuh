@@ -188,4 +188,7 @@ cudaError_t launch_match_popc_batch(const MatchJob* d_jobs, int n_jobs, int bloc
 int ctx_device(const orbx_ctx* c);
 cudaStream_t ctx_stream(const orbx_ctx* c);
 int* ctx_err(orbx_ctx* c);
+struct HostIO;  // orbx_hostio.cu: pinned staging of the host I/O entry points
+HostIO*& ctx_hostio(orbx_ctx* c);
+void hostio_free(HostIO* io);
 }  // namespace orbx

@@ -106,12 +106,15 @@ def lib():
         L.orbx_learned_gradients.argtypes = [vp, vp, vp, vp, i32, vp, vp, vp, vp, vp]
         L.orbx_learned_destroy.argtypes = [vp]
         L.orbx_gemm_bf16.argtypes = [vp, vp, vp, i32, i32, i32, vp, i32, i32, vp, vp]
+        L.orbx_upload_image.argtypes = [vp, vp, i32, i32, i32, vp, i32]
+        L.orbx_download_points.argtypes = [vp, vp, i32, vp, i32]
         L.orbx_selftest_pi_minus.argtypes = [ctypes.c_uint32, ctypes.c_uint32]
         L.orbx_selftest_pi_minus.restype = ctypes.c_longlong
         _lib = L
     return _lib
 
 
+FIELDS_KEYPOINT, FIELDS_MATCH = 1, 2
 PROPOSAL_MLP, PROPOSAL_LSH = 0, 1
 INIT_CENTROIDS, INIT_RANDOM = 0, 1
 GEMM_F32, GEMM_BIAS_RELU_BF16, GEMM_MASK_BF16, GEMM_BF16, GEMM_TOP8 = 0, 1, 2, 3, 4
@@ -237,6 +240,15 @@ class Context:
     def match_ptr(self, d_points1, d_n1, d_desc1, d_n2, d_desc2, n1_cap, n2_cap, mode=MATCH_POPC):
         _check(lib().orbx_match(self.h, _ptr(d_points1), _ptr(d_n1), _ptr(d_desc1), _ptr(d_n2), _ptr(d_desc2),
                                 n1_cap, n2_cap, mode), "orbx_match")
+
+    def upload_image(self, h_img, w, h, h_pitch, d_img, d_pitch):
+        """h_img: numpy uint8 array or pinned torch tensor (h, h_pitch); d_img: CUDA tensor (h, d_pitch)."""
+        hp = h_img.ctypes.data if hasattr(h_img, "ctypes") else h_img.data_ptr()
+        _check(lib().orbx_upload_image(self.h, hp, w, h, h_pitch, _ptr(d_img), d_pitch), "orbx_upload_image")
+
+    def download_points(self, d_pts, n, h_pts, fields=3):
+        """h_pts: numpy array of ORB_POINT_DTYPE (updated in place, other fields kept)."""
+        _check(lib().orbx_download_points(self.h, _ptr(d_pts), n, h_pts.ctypes.data, fields), "orbx_download_points")
 
     def knn2_ptr(self, d_q, nq, d_db, ndb, d_dist2, d_idx2, mode=MATCH_POPC):
         _check(lib().orbx_match_knn2(self.h, _ptr(d_q), nq, _ptr(d_db), ndb, _ptr(d_dist2), _ptr(d_idx2), mode),

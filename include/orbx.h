@@ -141,6 +141,23 @@ ORBX_API int orbx_pair_host(orbx_ctx* ctx, const uint8_t* h_img_a, const uint8_t
                             orbx_point* h_pts_a, int* h_n_a, orbx_point* h_pts_b, int* h_n_b, uint8_t* h_desc_a,
                             uint8_t* h_desc_b, int mode);
 
+/* Host I/O.  orbx_upload_image copies a host image with any row pitch h_pitch
+ * >= w (pinned or pageable memory) into a device image with row pitch d_pitch
+ * >= w (the reference's layout is d_pitch = align_up(w, 128)), with zero
+ * padding.  Asynchronous for pinned sources; for pageable ones it returns once
+ * the rows are staged in the context's pinned buffers.  The reference leaves
+ * this to its callers (main.cpp). */
+ORBX_API int orbx_upload_image(orbx_ctx* ctx, const uint8_t* h_img, int w, int h, int h_pitch, uint8_t* d_img,
+                               int d_pitch);
+/* Copies fields of the first n device keypoints into the host OrbPoint array,
+ * leaving the other fields of each host entry as they were: ORBX_FIELDS_KEYPOINT
+ * (x, y, octave, score, angle: the copy at orb.cpp:95-100), ORBX_FIELDS_MATCH
+ * (match, distance: orb.cpp:108-111), or both.  One packing kernel and one
+ * contiguous DMA instead of the reference's strided cudaMemcpy2D.  Synchronous. */
+#define ORBX_FIELDS_KEYPOINT 1
+#define ORBX_FIELDS_MATCH 2
+ORBX_API int orbx_download_points(orbx_ctx* ctx, const orbx_point* d_points, int n, orbx_point* h_points, int fields);
+
 /* Profiling variant of orbx_pair: the same launches without the graph, with a
  * CUDA event between consecutive kernels; writes the milliseconds of the
  * pyramid/blur, detect, NMS, describe and match kernels to stage_ms[0..4].

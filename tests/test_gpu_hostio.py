@@ -1,0 +1,87 @@
+"""Host I/O boundary (orbx_upload_image, orbx_download_points): pitch
+conversion with zero padding from pageable and pinned host memory, detection
+on an uploaded image, and field-selective keypoint export that leaves the
+other fields of each host OrbPoint untouched (the reference's strided copies,
+orb.cpp:95-100 and 108-111)."""
+import numpy as np
+import pytest
+
+torch = pytest.importorskip("torch")
+pytestmark = pytest.mark.gpu
+
+import orbx  # noqa: E402
+import synth  # noqa: E402
+
+PT = orbx.ORB_POINT_DTYPE
+
+
+@pytest.fixture(scope="module")
+def ctx():
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    c = orbx.Context(0, orbx.make_params(max_pts=10000))
+    yield c
+    c.close()
+
+
+def _host_image(w, h, h_pitch, seed):
+    rng = np.random.Generator(np.random.PCG64(seed))
+    img = rng.integers(0, 256, size=(h, h_pitch), dtype=np.uint8)  # padding holds garbage
+    return img
+
+
+@pytest.mark.parametrize("pinned", [False, True])
+def test_upload_pitch_conversion(ctx, pinned):
+    w, h, hp, dp = 333, 257, 401, 384
+    imgs = [_host_image(w, h, hp, s) for s in (1, 2, 3)]
+    outs = [torch.full((h, dp), 0xAB, dtype=torch.uint8, device="cuda") for _ in imgs]
+    srcs = [torch.from_numpy(x).pin_memory() if pinned else x for x in imgs]
+    for src, out in zip(srcs, outs):  # three in a row: the staging buffers alternate
+        ctx.upload_image(src, w, h, hp, out, dp)
+    ctx.sync()
+    for img, out in zip(imgs, outs):
+        o = out.cpu().numpy()
+        assert np.array_equal(o[:, :w], img[:, :w])
+        assert not o[:, w:].any()
+
+
+def test_detect_on_uploaded_image(ctx):
+    a, _, _ = synth.make_pair(640, 480, seed=41)  # (480, 640) with the 128-aligned pitch
+    w, h = 640, 480
+    # the same picture with a wider, garbage-padded host pitch
+    hp = 700
+    host = np.full((h, hp), 0x5A, dtype=np.uint8)
+    host[:, :w] = a[:, :w]
+    d_up = torch.empty((h, a.shape[1]), dtype=torch.uint8, device="cuda")
+    ctx.upload_image(host, w, h, hp, d_up, a.shape[1])
+    ref = orbx.detect_and_compute(ctx, torch.from_numpy(a).cuda(), w, h)
+    ctx.sync()
+    rp, rd = ref.to_host()
+    got = orbx.detect_and_compute(ctx, d_up, w, h)
+    ctx.sync()
+    gp, gd = got.to_host()
+    assert len(rp) > 100
+    assert np.array_equal(rp, gp) and np.array_equal(rd, gd)
+
+
+@pytest.mark.parametrize("fields", [orbx.FIELDS_KEYPOINT, orbx.FIELDS_MATCH, 3])
+def test_download_fields(ctx, fields):
+    n = 9973
+    rng = np.random.Generator(np.random.PCG64(fields))
+    dev_np = np.zeros(n, dtype=PT)
+    for f in PT.names:
+        dev_np[f] = rng.integers(-1000, 1000, n).astype(PT[f])
+    d = torch.from_numpy(dev_np.view(np.int32).reshape(n, 7).copy()).cuda()
+    host = np.zeros(n + 5, dtype=PT)
+    for f in PT.names:
+        host[f] = 77
+    ctx.download_points(d, n, host, fields)
+    kp = ("x", "y", "octave", "score", "angle")
+    mt = ("match", "distance")
+    for f in PT.names:
+        copied = (f in kp and fields & 1) or (f in mt and fields & 2)
+        if copied:
+            assert np.array_equal(host[f][:n], dev_np[f]), f
+        else:
+            assert np.all(host[f][:n] == 77), f
+        assert np.all(host[f][n:] == 77)
