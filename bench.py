@@ -178,10 +178,11 @@ def stage_work(oszp, n, na, nb):
     return {
         # input read once, raw and blurred pyramids written
         "pyramid_blur": 2 * (npx + 2 * obytes),
-        # raw pyramid read, score + octave map written
-        "detect": 2 * (obytes + 8 * npx),
-        # score map read, keypoints written
-        "nms": 2 * 4 * npx + nk * 28,
+        # raw pyramid read, occupancy bits + sparse score/octave of the survivors written
+        # (corners that NMS removes are not counted: a lower bound)
+        "detect": 2 * (obytes + npx // 8) + nk * 5,
+        # occupancy bits and survivors' score/octave read, keypoints written
+        "nms": 2 * (npx // 8) + nk * (5 + 28),
         # per keypoint: point, 31x31 disc, 512 samples, angle + 32-byte descriptor
         "describe": nk * (28 + 961 + 512 + 4 + 32),
     }

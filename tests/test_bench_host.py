@@ -60,8 +60,8 @@ def test_stage_work_1080p():
     n, oszp = orbx.layout(1920, 1080, 8)
     work = bench.stage_work(oszp, n, 1000, 1200)
     assert work["pyramid_blur"] == 2 * (1080 * 1920 + 2 * 2799360)
-    assert work["detect"] == 2 * (2799360 + 8 * 1080 * 1920)
-    assert work["nms"] == 2 * 4 * 1080 * 1920 + 2200 * 28
+    assert work["detect"] == 2 * (2799360 + 1080 * 1920 // 8) + 2200 * 5
+    assert work["nms"] == 2 * (1080 * 1920 // 8) + 2200 * 33
     assert work["describe"] == 2200 * (28 + 961 + 512 + 36)
 
 
