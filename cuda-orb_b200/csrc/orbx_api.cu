@@ -507,7 +507,9 @@ int lower_detect(orbx_ctx* c, const uint8_t* image, uint8_t* octave_images, floa
   Workspace* ws = nullptr;
   int rc = lower_workspace(c, oszp, noctaves, &ws);
   if (rc) return rc;
-  if (!image || !pts || !d_count) return ORBX_ERR_ARG;
+  if (!image || !pts || !d_count || threshold < 0) return ORBX_ERR_ARG;
+  // above 255 no pixel can differ from its centre by more than the threshold
+  threshold = std::min(threshold, 255);
   Frame F;
   fill_frame(c, *ws, image, ws->oszp[3 * noctaves], pts, nullptr, d_count, F);
   set_nms_shape(F, border, c->nms_rows);

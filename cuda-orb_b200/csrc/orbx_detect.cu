@@ -258,13 +258,23 @@ __device__ __forceinline__ float fast_score(const int* d, int threshold) {
 // Necessary condition for FAST-9: every run of 9 ring pixels contains two
 // neighbouring cardinal points (ring positions k and k+4, k = 0, 4, 8, 12), so
 // both of some such pair must be darker than v - t, or both brighter than
-// v + t.  It rejects most pixels with four loads; it never changes a result.
-__device__ __forceinline__ bool fast9_pretest(const uint8_t* c, int sw, int lo, int hi) {
-  const int p0 = c[3 * sw], p4 = c[3], p8 = c[-3 * sw], p12 = c[-3];
-  const bool d0 = p0 < lo, d4 = p4 < lo, d8 = p8 < lo, d12 = p12 < lo;
-  const bool b0 = p0 > hi, b4 = p4 > hi, b8 = p8 > hi, b12 = p12 > hi;
-  return (d0 && d4) || (d4 && d8) || (d8 && d12) || (d12 && d0) || (b0 && b4) || (b4 && b8) || (b8 && b12) ||
-         (b12 && b0);
+// v + t.  It never changes a result.  Evaluated for four horizontally adjacent
+// centres at once on packed bytes: w points at the aligned word holding them
+// (row stride sw bytes, a multiple of 4); returns 0xFF in each byte whose
+// centre passes.  Saturating v - t and v + t (t <= 255) give the same answers
+// as the signed comparisons p < v - t and p > v + t.
+__device__ __forceinline__ uint32_t fast9_pretest4(const uint8_t* w, int sw, uint32_t t4) {
+  const uint32_t c = *reinterpret_cast<const uint32_t*>(w);
+  const uint32_t cl = *reinterpret_cast<const uint32_t*>(w - 4);
+  const uint32_t cr = *reinterpret_cast<const uint32_t*>(w + 4);
+  const uint32_t p0 = *reinterpret_cast<const uint32_t*>(w + 3 * sw);   // ring 0: (x, y + 3)
+  const uint32_t p8 = *reinterpret_cast<const uint32_t*>(w - 3 * sw);   // ring 8: (x, y - 3)
+  const uint32_t p4 = __byte_perm(c, cr, 0x6543);                       // ring 4: (x + 3, y)
+  const uint32_t p12 = __byte_perm(cl, c, 0x4321);                      // ring 12: (x - 3, y)
+  const uint32_t lo = __vsubus4(c, t4), hi = __vaddus4(c, t4);
+  const uint32_t d0 = __vcmpltu4(p0, lo), d4 = __vcmpltu4(p4, lo), d8 = __vcmpltu4(p8, lo), d12 = __vcmpltu4(p12, lo);
+  const uint32_t b0 = __vcmpgtu4(p0, hi), b4 = __vcmpgtu4(p4, hi), b8 = __vcmpgtu4(p8, hi), b12 = __vcmpgtu4(p12, hi);
+  return ((d0 | d8) & (d4 | d12)) | ((b0 | b8) & (b4 | b12));
 }
 
 // FAST-9 segment test on a shared-memory tile of row stride sw: a run of 9
@@ -297,32 +307,58 @@ __device__ __forceinline__ int warp_append(int16_t* list, int len, bool take, in
   return len + __popc(m);
 }
 
+// Merge a score into the tile's level-0 map: positions without their occupancy
+// bit count as 0, and only a strictly larger score replaces (so the first octave
+// to store a value keeps ties, and scores <= 0 are never stored).
+__device__ __forceinline__ void map_store(float* s_map, int8_t* s_oct, uint32_t* s_occ, int m, float score, int o) {
+  const uint32_t bit = 1u << (m & 31);
+  const bool has = (s_occ[m >> 5] & bit) != 0u;
+  const float cur = has ? s_map[m] : 0.f;
+  if (cur < score) {
+    s_map[m] = score;
+    s_oct[m] = (int8_t)o;
+    if (!has) atomicOr(&s_occ[m >> 5], bit);
+  }
+}
+
 // One octave's pixels of a rectangle [lx0, lx0+nx) x [ly0, ly0+ny) of the
-// octave tile, processed by one warp: pre-test, compacted full test, compacted
-// scoring, merge into the level-0 map (strict >, so a lower octave keeps ties).
+// octave tile, processed by one warp: pre-test four centres per lane, compacted
+// full test, compacted scoring, merge into the level-0 map.
 __device__ __forceinline__ void detect_rect_warp(const Batch& b, const Frame& F, int o, const uint8_t* stage, int sw,
                                                  int xb, int yb, int lx0, int ly0, int nx_log, int ny,
                                                  int16_t* list_a, int16_t* list_b, float* s_map, int8_t* s_oct,
-                                                 int lane) {
+                                                 uint32_t* s_occ, int lane) {
   const int ow = F.ow[o], oh = F.oh[o];
   const int thr = b.fast_thr;
-  const int npx = ny << nx_log;
+  const uint32_t t4 = (uint32_t)min(max(thr, 0), 255) * 0x01010101u;
+  const int nw_log = nx_log - 2;  // words of 4 pixels per row
+  const int nwords = ny << nw_log;
   int na = 0;
-  for (int i0 = 0; i0 < npx; i0 += 32) {
+  for (int i0 = 0; i0 < nwords; i0 += 32) {
     const int i = i0 + lane;
-    bool take = false;
-    if (i < npx) {
-      const int lx = lx0 + (i & ((1 << nx_log) - 1));
-      const int ly = ly0 + (i >> nx_log);
+    const int lx = lx0 + ((i & ((1 << nw_log) - 1)) << 2);
+    const int ly = ly0 + (i >> nw_log);
+    uint32_t m = 0u;
+    if (i < nwords) {
       const int x = xb + lx, y = yb + ly;
-      if (x >= 3 && x < ow - 3 && y >= 3 && y < oh - 3) {
-        const uint8_t* c = stage + (ly + kHalo) * sw + (lx + kHalo);
-        const int v = c[0];
-        take = fast9_pretest(c, sw, v - thr, v + thr);
+      if (y >= 3 && y < oh - 3 && x < ow - 3) {
+        m = fast9_pretest4(stage + (ly + kHalo) * sw + (lx + kHalo), sw, t4);
+        if (x < 3 || x + 3 >= ow - 3) {  // border word: keep the centres with 3 <= x + k < ow - 3
+          uint32_t vm = 0u;
+#pragma unroll
+          for (int k = 0; k < 4; k++)
+            if (x + k >= 3 && x + k < ow - 3) vm |= 0xFFu << (8 * k);
+          m &= vm;
+        }
       }
     }
-    na = warp_append(list_a, na, take, (int16_t)((ly0 + (i >> nx_log)) * 64 + lx0 + (i & ((1 << nx_log) - 1))),
-                     lane);
+    m &= 0x80808080u;  // one bit per passing centre
+    while (__any_sync(0xffffffffu, m != 0u)) {
+      const bool take = m != 0u;
+      const int k = take ? (__ffs(m) >> 3) - 1 : 0;
+      na = warp_append(list_a, na, take, (int16_t)(ly * 64 + lx + k), lane);
+      m &= m - 1u;
+    }
   }
   __syncwarp();
   int nb = 0;
@@ -368,25 +404,16 @@ __device__ __forceinline__ void detect_rect_warp(const Batch& b, const Frame& F,
         dyy += __shfl_xor_sync(0xffffffffu, dyy, d);
         dxy += __shfl_xor_sync(0xffffffffu, dxy, d);
       }
-      if (lane == 0) {
-        const float score = harris_combine(dxx, dyy, dxy, b.harris_scale4);
-        const int m = (ly << o) * kDetTW + (lx << o);
-        if (s_map[m] < score) {
-          s_map[m] = score;
-          s_oct[m] = (int8_t)o;
-        }
-      }
+      if (lane == 0)
+        map_store(s_map, s_oct, s_occ, (ly << o) * kDetTW + (lx << o), harris_combine(dxx, dyy, dxy, b.harris_scale4),
+                  o);
     }
   } else {
     for (int j = lane; j < nb; j += 32) {
       const int item = list_b[j];
       const int ly = item >> 6, lx = item & 63;
       const float score = corner_score(b, stage + (ly + kHalo) * sw + (lx + kHalo), sw);
-      const int m = (ly << o) * kDetTW + (lx << o);
-      if (s_map[m] < score) {
-        s_map[m] = score;
-        s_oct[m] = (int8_t)o;
-      }
+      map_store(s_map, s_oct, s_occ, (ly << o) * kDetTW + (lx << o), score, o);
     }
   }
   __syncwarp();
@@ -396,6 +423,7 @@ __global__ void __launch_bounds__(256, 4) k_detect(Batch b) {
   __shared__ __align__(16) uint8_t s_stage[det_stage_bytes()];
   __shared__ float s_map[kDetTH * kDetTW];
   __shared__ int8_t s_oct[kDetTH * kDetTW];
+  __shared__ uint32_t s_occ[kDetTH * kDetTW / 32];
   __shared__ int16_t s_list[8][2][256];
 
   const int t = blockIdx.x;
@@ -409,12 +437,10 @@ __global__ void __launch_bounds__(256, 4) k_detect(Batch b) {
   const int lane = threadIdx.x & 31;
   const int warp = threadIdx.x >> 5;
 
-  for (int i = threadIdx.x; i < kDetTH * kDetTW; i += blockDim.x) {
-    s_map[i] = 0.f;
-    s_oct[i] = 0;
-  }
-  // Stage every octave's tile with its halo, 4 bytes per load: octave offsets
-  // and pitches are multiples of 128 and (X0 >> o) - 4 is a multiple of 4.
+  if (threadIdx.x < kDetTH * kDetTW / 32) s_occ[threadIdx.x] = 0u;
+  // Stage every octave's tile with its halo, 4 bytes per load, one row per warp
+  // and step: octave offsets and pitches are multiples of 128 and (X0 >> o) - 4
+  // is a multiple of 4; a staged row is at most 18 words.
   for (int o = 0; o < n_oct; o++) {
     const int sw = (kDetTW >> o) + 2 * kHalo;
     const int sh = (kDetTH >> o) + 2 * kHalo;
@@ -422,11 +448,9 @@ __global__ void __launch_bounds__(256, 4) k_detect(Batch b) {
     const int op = F.op[o];
     const long long base = F.ooff[o] + (long long)((Y0 >> o) - kHalo) * op + ((X0 >> o) - kHalo);
     uint32_t* dst = reinterpret_cast<uint32_t*>(s_stage + det_stage_off(o));
-    for (int i = threadIdx.x; i < sw4 * sh; i += blockDim.x) {
-      const int r = i / sw4;
-      const int c4 = i - r * sw4;
-      dst[i] = __ldg(reinterpret_cast<const uint32_t*>(pyr + base + (long long)r * op) + c4);
-    }
+    if (lane < sw4)
+      for (int r = warp; r < sh; r += 8)
+        dst[r * sw4 + lane] = __ldg(reinterpret_cast<const uint32_t*>(pyr + base + (long long)r * op) + lane);
   }
   __syncthreads();
 
@@ -446,7 +470,7 @@ __global__ void __launch_bounds__(256, 4) k_detect(Batch b) {
       ny = 1;
     }
     detect_rect_warp(b, F, o, s_stage + det_stage_off(o), sw, X0 >> o, Y0 >> o, 0, ly0, nx_log, ny, la, lb, s_map,
-                     s_oct, lane);
+                     s_oct, s_occ, lane);
   }
   __syncthreads();
   // octaves 3 and 4 (8x4 and 4x2 pixels per tile) by warp 0, in order
@@ -454,28 +478,27 @@ __global__ void __launch_bounds__(256, 4) k_detect(Batch b) {
     for (int o = 3; o < n_oct; o++) {
       const int sw = (kDetTW >> o) + 2 * kHalo;
       detect_rect_warp(b, F, o, s_stage + det_stage_off(o), sw, X0 >> o, Y0 >> o, 0, 0, 6 - o, kDetTH >> o, la, lb,
-                       s_map, s_oct, lane);
+                       s_map, s_oct, s_occ, lane);
     }
   }
   __syncthreads();
 
-  // Output: occupancy bits for the whole tile (every word written, so no
-  // clearing pass), scores and octaves only where a score was stored.  The
-  // tile's 64 columns are two aligned 32-bit words of each row (pitch0 is a
-  // multiple of 128).
-  const int p0 = F.op[0];
-  for (int k = warp; k < kDetTH * (kDetTW / 32); k += blockDim.x >> 5) {
-    const int r = k >> 1;
-    const int c = ((k & 1) << 5) + lane;
-    const float v = s_map[r * kDetTW + c];
-    const uint32_t m = __ballot_sync(0xffffffffu, v > 0.f);
+  // Output: the tile's occupancy words (all of them, so no clearing pass is
+  // needed), then score and octave only where a bit is set.  The tile's 64
+  // columns are two aligned 32-bit words of each row (pitch0 is a multiple of 128).
+  if (threadIdx.x < kDetTH * kDetTW / 32) {
+    const int r = threadIdx.x >> 1, half = threadIdx.x & 1;
     const int Y = Y0 + r;
     if (Y < F.h) {
-      const size_t a = (size_t)Y * p0 + X0 + c;
-      if (lane == 0) F.occ[a >> 5] = m;
-      if (v > 0.f) {
-        F.vmap[a] = v;
-        F.oct8[a] = (uint8_t)s_oct[r * kDetTW + c];
+      uint32_t m = s_occ[threadIdx.x];
+      const size_t a0 = (size_t)Y * F.op[0] + X0 + 32 * half;
+      F.occ[a0 >> 5] = m;
+      while (m) {
+        const int k = __ffs(m) - 1;
+        m &= m - 1u;
+        const int idx = r * kDetTW + 32 * half + k;
+        F.vmap[a0 + k] = s_map[idx];
+        F.oct8[a0 + k] = (uint8_t)s_oct[idx];
       }
     }
   }
