@@ -554,23 +554,27 @@ __device__ __forceinline__ int nms_lookback(unsigned long long* st, int s, int l
 }
 
 // Neighbour rule of gNmsUnroll4 (orbd.cu:938-956) for the centre at linear
-// index idx (score v, octave o), checked by the whole warp: lane i takes window
-// rows dy = i - r, i + 32 - r, ...; each row is at most two occupancy words, and
-// scores are read only where a bit is set.  Positions are linear like the
-// reference's (a column past the edge is the adjacent row's entry); positions
-// outside the map, reachable only with an edge threshold below 2^o, are empty.
-__device__ __forceinline__ bool nms_keep_warp(const Frame& F, long long idx, float v, int o, int p0, long long npx,
-                                              int lane) {
+// index idx (score v, octave o), checked by a group of kNmsGroup lanes: lane
+// `sub` of the group takes window rows dy = sub - r, sub + kNmsGroup - r, ...;
+// each row is at most two occupancy words, and scores are read only where a
+// bit is set.  Returns whether this lane's rows hold a suppressing position.
+// Positions are linear like the reference's (a column past the edge is the
+// adjacent row's entry); positions outside the map, reachable only with an
+// edge threshold below 2^o, are empty.
+constexpr int kNmsGroup = 8;
+constexpr int kNmsChunkWords = 128;  // occupancy words compacted per round: at most 4096 centres
+
+__device__ __forceinline__ bool nms_suppressed_rows(const Frame& F, long long idx, float v, int o, int p0,
+                                                    long long npx, int sub) {
   const int r = 1 << o;
-  bool sup = false;
-  for (int dyi = lane; dyi <= 2 * r; dyi += 32) {
+  for (int dyi = sub; dyi <= 2 * r; dyi += kNmsGroup) {
     const int dy = dyi - r;
     const long long rc = idx + (long long)dy * p0;
     long long lo = rc - r, hi = rc + r;
     if (hi < 0 || lo >= npx) continue;
     if (lo < 0) lo = 0;
     if (hi >= npx) hi = npx - 1;
-    for (long long wi = lo >> 5; wi <= (hi >> 5) && !sup; wi++) {
+    for (long long wi = lo >> 5; wi <= (hi >> 5); wi++) {
       const long long base = wi << 5;
       uint32_t m = __ldg(F.occ + wi);
       if (base < lo) m &= ~0u << (int)(lo - base);
@@ -582,19 +586,20 @@ __device__ __forceinline__ bool nms_keep_warp(const Frame& F, long long idx, flo
         if (li == idx) continue;
         const int dx = (int)(li - rc);
         const float u = __ldg(F.vmap + li);
-        if (u > v || (u == v && dx <= 0 && dy <= 0)) {
-          sup = true;
-          break;
-        }
+        if (u > v || (u == v && dx <= 0 && dy <= 0)) return true;
       }
     }
   }
-  return !__any_sync(0xffffffffu, sup);
+  return false;
 }
 
 __global__ void __launch_bounds__(256) k_nms(Batch b) {
   __shared__ uint32_t s_sur[kNmsMaxWords];
   __shared__ int s_pref[kNmsMaxWords];
+  __shared__ uint16_t s_cand[kNmsChunkWords * 32];
+  __shared__ float s_cv[kNmsChunkWords * 32];
+  __shared__ uint8_t s_co[kNmsChunkWords * 32];
+  __shared__ int s_ncand[2];
   __shared__ int s_warp_tot[8];
   __shared__ int s_ticket, s_base;
 
@@ -616,38 +621,56 @@ __global__ void __launch_bounds__(256) k_nms(Batch b) {
   const long long npx = (long long)F.h * p0;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 
-  // pass 1: survivor bits of every occupancy word of the strip, in raster order
-  for (int k0 = 0; k0 < nwords; k0 += blockDim.x) {
-    const int k = k0 + threadIdx.x;
-    uint32_t m = 0;
-    int row = 0, cbase = 0;
-    if (k < nwords) {
-      row = row0 + k / nw;
+  // pass 1: survivor bits of every occupancy word of the strip.  In rounds of
+  // kNmsChunkWords words: the centres of the round (with their scores) are
+  // compacted into shared memory, then checked by 32 groups of 8 lanes, so a
+  // textured patch of the strip spreads over every warp.
+  for (int k = threadIdx.x; k < nwords; k += blockDim.x) s_sur[k] = 0u;
+  if (threadIdx.x == 0) s_ncand[0] = 0;
+  const int gid = warp * (32 / kNmsGroup) + (lane / kNmsGroup), sub = lane % kNmsGroup;
+  const uint32_t gmask = ((1u << kNmsGroup) - 1u) << (lane & ~(kNmsGroup - 1));
+  for (int c0 = 0, round = 0; c0 < nwords; c0 += kNmsChunkWords, round++) {
+    int* cnt = &s_ncand[round & 1];
+    __syncthreads();  // the previous round's checks are done; its counter is free
+    if (threadIdx.x == 0) s_ncand[(round + 1) & 1] = 0;
+    const int k = c0 + (int)threadIdx.x;
+    if (threadIdx.x < kNmsChunkWords && k < nwords) {
+      const int row = row0 + k / nw;
       const int wj = wlo + k % nw;
-      cbase = wj << 5;
-      m = __ldg(F.occ + (long long)row * wpr + wj);
+      const int cbase = wj << 5;
+      uint32_t m = __ldg(F.occ + (long long)row * wpr + wj);
       if (cbase < xlo) m &= ~0u << (xlo - cbase);
       if (xhi - cbase < 32) m &= (xhi - cbase <= 0) ? 0u : ((xhi - cbase == 32) ? ~0u : ((1u << (xhi - cbase)) - 1u));
-    }
-    uint32_t sur = 0;
-    uint32_t lanes = __ballot_sync(0xffffffffu, m != 0u);
-    while (lanes) {
-      const int l = __ffs(lanes) - 1;
-      lanes &= lanes - 1u;
-      uint32_t mm = __shfl_sync(0xffffffffu, m, l);
-      const int crow = __shfl_sync(0xffffffffu, row, l);
-      const int ccb = __shfl_sync(0xffffffffu, cbase, l);
-      while (mm) {
-        const int bit = __ffs(mm) - 1;
-        mm &= mm - 1u;
-        const long long idx = (long long)crow * p0 + ccb + bit;
-        const float v = __ldg(F.vmap + idx);
-        const int o = __ldg(F.oct8 + idx);
-        const bool keep = nms_keep_warp(F, idx, v, o, p0, npx, lane);
-        if (lane == l && keep) sur |= 1u << bit;
+      if (m) {
+        int pos = atomicAdd(cnt, __popc(m));
+        while (m) {
+          const int bit = __ffs(m) - 1;
+          m &= m - 1u;
+          const long long idx = (long long)row * p0 + cbase + bit;
+          s_cand[pos] = (uint16_t)(((k - c0) << 5) | bit);
+          s_cv[pos] = __ldg(F.vmap + idx);
+          s_co[pos] = __ldg(F.oct8 + idx);
+          pos++;
+        }
       }
     }
-    if (k < nwords) s_sur[k] = sur;
+    __syncthreads();
+    const int nc = *cnt;
+    for (int j0 = 0; j0 < nc; j0 += 32 * 8 / kNmsGroup) {
+      const int j = j0 + gid;
+      bool sup = false;
+      int kk = 0, bit = 0;
+      if (j < nc) {
+        const int e = s_cand[j];
+        kk = c0 + (e >> 5);
+        bit = e & 31;
+        const int row = row0 + kk / nw;
+        const int cbase = (wlo + kk % nw) << 5;
+        sup = nms_suppressed_rows(F, (long long)row * p0 + cbase + bit, s_cv[j], s_co[j], p0, npx, sub);
+      }
+      const uint32_t bal = __ballot_sync(0xffffffffu, sup);
+      if (j < nc && sub == 0 && !(bal & gmask)) atomicOr(&s_sur[kk], 1u << bit);
+    }
   }
   __syncthreads();
 

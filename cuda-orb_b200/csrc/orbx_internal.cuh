@@ -18,7 +18,7 @@ constexpr int kPyrTH = 32;
 constexpr int kDetTW = 64;
 constexpr int kDetTH = 32;
 // NMS strips span the full valid width; default and largest strip height
-constexpr int kNmsRows = 16;
+constexpr int kNmsRows = 4;
 constexpr int kNmsMaxRows = 16;
 constexpr int kNmsMaxWords = 2048;  // occupancy words per NMS strip (rows x words per row)
 
