@@ -300,131 +300,24 @@ __device__ __forceinline__ float corner_score(const Batch& b, const uint8_t* c, 
   return fast_score(d, b.fast_thr);
 }
 
-// Append this lane's item to a warp-private list when `take`; returns the new length.
-__device__ __forceinline__ int warp_append(int16_t* list, int len, bool take, int16_t item, int lane) {
-  const uint32_t m = __ballot_sync(0xffffffffu, take);
-  if (take) list[len + __popc(m & ((1u << lane) - 1u))] = item;
-  return len + __popc(m);
-}
+// Tile-level candidate lists hold (octave, row, column) of the octave tile as
+// o << 11 | ly << 6 | lx; a tile has at most 2048 + 512 + 128 + 32 + 8 pixels.
+constexpr int kDetMaxCand = 2728;
+__device__ __forceinline__ uint16_t det_item(int o, int ly, int lx) { return (uint16_t)((o << 11) | (ly << 6) | lx); }
 
-// Merge a score into the tile's level-0 map: positions without their occupancy
-// bit count as 0, and only a strictly larger score replaces (so the first octave
-// to store a value keeps ties, and scores <= 0 are never stored).
-__device__ __forceinline__ void map_store(float* s_map, int8_t* s_oct, uint32_t* s_occ, int m, float score, int o) {
-  const uint32_t bit = 1u << (m & 31);
-  const bool has = (s_occ[m >> 5] & bit) != 0u;
-  const float cur = has ? s_map[m] : 0.f;
-  if (cur < score) {
-    s_map[m] = score;
-    s_oct[m] = (int8_t)o;
-    if (!has) atomicOr(&s_occ[m >> 5], bit);
-  }
-}
-
-// One octave's pixels of a rectangle [lx0, lx0+nx) x [ly0, ly0+ny) of the
-// octave tile, processed by one warp: pre-test four centres per lane, compacted
-// full test, compacted scoring, merge into the level-0 map.
-__device__ __forceinline__ void detect_rect_warp(const Batch& b, const Frame& F, int o, const uint8_t* stage, int sw,
-                                                 int xb, int yb, int lx0, int ly0, int nx_log, int ny,
-                                                 int16_t* list_a, int16_t* list_b, float* s_map, int8_t* s_oct,
-                                                 uint32_t* s_occ, int lane) {
-  const int ow = F.ow[o], oh = F.oh[o];
-  const int thr = b.fast_thr;
-  const uint32_t t4 = (uint32_t)min(max(thr, 0), 255) * 0x01010101u;
-  const int nw_log = nx_log - 2;  // words of 4 pixels per row
-  const int nwords = ny << nw_log;
-  int na = 0;
-  for (int i0 = 0; i0 < nwords; i0 += 32) {
-    const int i = i0 + lane;
-    const int lx = lx0 + ((i & ((1 << nw_log) - 1)) << 2);
-    const int ly = ly0 + (i >> nw_log);
-    uint32_t m = 0u;
-    if (i < nwords) {
-      const int x = xb + lx, y = yb + ly;
-      if (y >= 3 && y < oh - 3 && x < ow - 3) {
-        m = fast9_pretest4(stage + (ly + kHalo) * sw + (lx + kHalo), sw, t4);
-        if (x < 3 || x + 3 >= ow - 3) {  // border word: keep the centres with 3 <= x + k < ow - 3
-          uint32_t vm = 0u;
-#pragma unroll
-          for (int k = 0; k < 4; k++)
-            if (x + k >= 3 && x + k < ow - 3) vm |= 0xFFu << (8 * k);
-          m &= vm;
-        }
-      }
-    }
-    m &= 0x80808080u;  // one bit per passing centre
-    while (__any_sync(0xffffffffu, m != 0u)) {
-      const bool take = m != 0u;
-      const int k = take ? (__ffs(m) >> 3) - 1 : 0;
-      na = warp_append(list_a, na, take, (int16_t)(ly * 64 + lx + k), lane);
-      m &= m - 1u;
-    }
-  }
-  __syncwarp();
-  int nb = 0;
-  for (int j0 = 0; j0 < na; j0 += 32) {
-    const int j = j0 + lane;
-    bool take = false;
-    int16_t item = 0;
-    if (j < na) {
-      item = list_a[j];
-      const uint8_t* c = stage + ((item >> 6) + kHalo) * sw + ((item & 63) + kHalo);
-      const int v = c[0];
-      take = fast9_full(c, sw, v - thr, v + thr);
-    }
-    nb = warp_append(list_b, nb, take, item, lane);
-  }
-  __syncwarp();
-  if (b.harris) {
-    // one corner at a time, the whole warp: lane i takes window positions i and
-    // i + 32 of the 7x7 Harris window; the 32-bit sums wrap, so their order is free
-    for (int j = 0; j < nb; j++) {
-      const int item = list_b[j];
-      const int ly = item >> 6, lx = item & 63;
-      const uint8_t* c = stage + (ly + kHalo) * sw + (lx + kHalo);
-      int dxx = 0, dyy = 0, dxy = 0;
-#pragma unroll
-      for (int w2 = 0; w2 < 2; w2++) {
-        const int pos = lane + 32 * w2;
-        if (pos < 49) {
-          const int wy = pos / 7 - 3, wx = pos % 7 - 3;
-          const uint8_t* q = c + wy * sw + wx;
-          const int dx = ((int)q[1] - (int)q[-1]) * 2 + ((int)q[-sw + 1] - (int)q[-sw - 1]) +
-                         ((int)q[sw + 1] - (int)q[sw - 1]);
-          const int dy = ((int)q[sw] - (int)q[-sw]) * 2 + ((int)q[sw - 1] - (int)q[-sw - 1]) +
-                         ((int)q[sw + 1] - (int)q[-sw + 1]);
-          dxx += dx * dx;
-          dyy += dy * dy;
-          dxy += dx * dy;
-        }
-      }
-#pragma unroll
-      for (int d = 16; d >= 1; d >>= 1) {
-        dxx += __shfl_xor_sync(0xffffffffu, dxx, d);
-        dyy += __shfl_xor_sync(0xffffffffu, dyy, d);
-        dxy += __shfl_xor_sync(0xffffffffu, dxy, d);
-      }
-      if (lane == 0)
-        map_store(s_map, s_oct, s_occ, (ly << o) * kDetTW + (lx << o), harris_combine(dxx, dyy, dxy, b.harris_scale4),
-                  o);
-    }
-  } else {
-    for (int j = lane; j < nb; j += 32) {
-      const int item = list_b[j];
-      const int ly = item >> 6, lx = item & 63;
-      const float score = corner_score(b, stage + (ly + kHalo) * sw + (lx + kHalo), sw);
-      map_store(s_map, s_oct, s_occ, (ly << o) * kDetTW + (lx << o), score, o);
-    }
-  }
-  __syncwarp();
+// Merge key of a level-0 position: the larger score wins and, between equal
+// scores, the lower octave (the reference visits octaves in increasing order
+// and replaces only on a strictly larger score).  Only scores > 0 are stored.
+__device__ __forceinline__ unsigned long long det_key(float score, int o) {
+  return ((unsigned long long)__float_as_uint(score) << 32) | (unsigned)(7 - o);
 }
 
 __global__ void __launch_bounds__(256, 4) k_detect(Batch b) {
   __shared__ __align__(16) uint8_t s_stage[det_stage_bytes()];
-  __shared__ float s_map[kDetTH * kDetTW];
-  __shared__ int8_t s_oct[kDetTH * kDetTW];
-  __shared__ uint32_t s_occ[kDetTH * kDetTW / 32];
-  __shared__ int16_t s_list[8][2][256];
+  __shared__ unsigned long long s_key[kDetTH * kDetTW];
+  __shared__ uint16_t s_cand[kDetMaxCand];
+  __shared__ uint16_t s_corner[kDetMaxCand];
+  __shared__ int s_n[2];
 
   const int t = blockIdx.x;
   const int f = find_frame(b.det_base, b.n_frames, t);
@@ -436,8 +329,10 @@ __global__ void __launch_bounds__(256, 4) k_detect(Batch b) {
   const uint8_t* __restrict__ pyr = F.pyr;
   const int lane = threadIdx.x & 31;
   const int warp = threadIdx.x >> 5;
+  const int thr = b.fast_thr;
 
-  if (threadIdx.x < kDetTH * kDetTW / 32) s_occ[threadIdx.x] = 0u;
+  for (int i = threadIdx.x; i < kDetTH * kDetTW; i += blockDim.x) s_key[i] = 0ull;
+  if (threadIdx.x < 2) s_n[threadIdx.x] = 0;
   // Stage every octave's tile with its halo, 4 bytes per load, one row per warp
   // and step: octave offsets and pitches are multiples of 128 and (X0 >> o) - 4
   // is a multiple of 4; a staged row is at most 18 words.
@@ -454,51 +349,131 @@ __global__ void __launch_bounds__(256, 4) k_detect(Batch b) {
   }
   __syncthreads();
 
-  // octaves 0..2: warp w owns level-0 rows [4w, 4w+4) of the tile, i.e. octave
-  // rows [4w >> o, (4w+4) >> o); no other warp touches those map positions
-  int16_t* la = s_list[warp][0];
-  int16_t* lb = s_list[warp][1];
-  for (int o = 0; o < n_oct && o < 3; o++) {
-    const int sw = (kDetTW >> o) + 2 * kHalo;
-    const int nx_log = 6 - o;
-    int ly0, ny;
-    if (o < 2) {
-      ly0 = (4 * warp) >> o;
-      ny = 4 >> o;
-    } else {
-      ly0 = warp;
-      ny = 1;
-    }
-    detect_rect_warp(b, F, o, s_stage + det_stage_off(o), sw, X0 >> o, Y0 >> o, 0, ly0, nx_log, ny, la, lb, s_map,
-                     s_oct, s_occ, lane);
-  }
-  __syncthreads();
-  // octaves 3 and 4 (8x4 and 4x2 pixels per tile) by warp 0, in order
-  if (warp == 0) {
-    for (int o = 3; o < n_oct; o++) {
-      const int sw = (kDetTW >> o) + 2 * kHalo;
-      detect_rect_warp(b, F, o, s_stage + det_stage_off(o), sw, X0 >> o, Y0 >> o, 0, 0, 6 - o, kDetTH >> o, la, lb,
-                       s_map, s_oct, s_occ, lane);
+  // 1. cardinal pre-test, four centres per word, words of every octave spread
+  //    over the whole block (octave o has (32 >> o) rows of (16 >> o) words)
+  {
+    const uint32_t t4 = (uint32_t)min(max(thr, 0), 255) * 0x01010101u;
+    int total = 0;
+    for (int o = 0; o < n_oct; o++) total += 512 >> (2 * o);
+    for (int i = threadIdx.x; i < total; i += blockDim.x) {
+      int o = 0, w = i;
+      while (w >= (512 >> (2 * o))) {
+        w -= 512 >> (2 * o);
+        o++;
+      }
+      const int nwl = 4 - o;  // log2 words per row
+      const int ly = w >> nwl, lx = (w & ((1 << nwl) - 1)) << 2;
+      const int x = (X0 >> o) + lx, y = (Y0 >> o) + ly;
+      const int ow = F.ow[o], oh = F.oh[o];
+      uint32_t m = 0u;
+      if (y >= 3 && y < oh - 3 && x < ow - 3) {
+        const int sw = (kDetTW >> o) + 2 * kHalo;
+        m = fast9_pretest4(s_stage + det_stage_off(o) + (ly + kHalo) * sw + (lx + kHalo), sw, t4);
+        if (x < 3 || x + 3 >= ow - 3) {  // border word: keep the centres with 3 <= x + k < ow - 3
+          uint32_t vm = 0u;
+#pragma unroll
+          for (int k = 0; k < 4; k++)
+            if (x + k >= 3 && x + k < ow - 3) vm |= 0xFFu << (8 * k);
+          m &= vm;
+        }
+      }
+      m &= 0x80808080u;
+      if (m) {
+        int pos = atomicAdd(&s_n[0], __popc(m));
+        while (m) {
+          const int k = (__ffs(m) >> 3) - 1;
+          m &= m - 1u;
+          s_cand[pos++] = det_item(o, ly, lx + k);
+        }
+      }
     }
   }
   __syncthreads();
 
-  // Output: the tile's occupancy words (all of them, so no clearing pass is
-  // needed), then score and octave only where a bit is set.  The tile's 64
-  // columns are two aligned 32-bit words of each row (pitch0 is a multiple of 128).
-  if (threadIdx.x < kDetTH * kDetTW / 32) {
-    const int r = threadIdx.x >> 1, half = threadIdx.x & 1;
+  // 2. full 9-arc segment test of the candidates
+  {
+    const int n1 = s_n[0];
+    for (int j = threadIdx.x; j < n1; j += blockDim.x) {
+      const int e = s_cand[j];
+      const int o = e >> 11, ly = (e >> 6) & 31, lx = e & 63;
+      const int sw = (kDetTW >> o) + 2 * kHalo;
+      const uint8_t* c = s_stage + det_stage_off(o) + (ly + kHalo) * sw + (lx + kHalo);
+      const int v = c[0];
+      if (fast9_full(c, sw, v - thr, v + thr)) s_corner[atomicAdd(&s_n[1], 1)] = (uint16_t)e;
+    }
+  }
+  __syncthreads();
+
+  // 3. scores of the corners, merged into the level-0 map
+  {
+    const int n2 = s_n[1];
+    if (b.harris) {
+      // 32 groups of 8 lanes, one corner per group; lane s of a group takes
+      // window positions s, s + 8, ... of the 7x7 Harris window (the 32-bit sums
+      // wrap, so their order is free)
+      const int gid = threadIdx.x >> 3, sub = threadIdx.x & 7;
+      for (int j0 = 0; j0 < n2; j0 += 32) {
+        const int j = j0 + gid;
+        int dxx = 0, dyy = 0, dxy = 0;
+        int e = 0;
+        if (j < n2) {
+          e = s_corner[j];
+          const int o = e >> 11, ly = (e >> 6) & 31, lx = e & 63;
+          const int sw = (kDetTW >> o) + 2 * kHalo;
+          const uint8_t* c = s_stage + det_stage_off(o) + (ly + kHalo) * sw + (lx + kHalo);
+          for (int pos = sub; pos < 49; pos += 8) {
+            const int wy = pos / 7 - 3, wx = pos % 7 - 3;
+            const uint8_t* q = c + wy * sw + wx;
+            const int dx = ((int)q[1] - (int)q[-1]) * 2 + ((int)q[-sw + 1] - (int)q[-sw - 1]) +
+                           ((int)q[sw + 1] - (int)q[sw - 1]);
+            const int dy = ((int)q[sw] - (int)q[-sw]) * 2 + ((int)q[sw - 1] - (int)q[-sw - 1]) +
+                           ((int)q[sw + 1] - (int)q[-sw + 1]);
+            dxx += dx * dx;
+            dyy += dy * dy;
+            dxy += dx * dy;
+          }
+        }
+#pragma unroll
+        for (int d = 4; d >= 1; d >>= 1) {
+          dxx += __shfl_xor_sync(0xffffffffu, dxx, d);
+          dyy += __shfl_xor_sync(0xffffffffu, dyy, d);
+          dxy += __shfl_xor_sync(0xffffffffu, dxy, d);
+        }
+        if (j < n2 && sub == 0) {
+          const int o = e >> 11, ly = (e >> 6) & 31, lx = e & 63;
+          const float score = harris_combine(dxx, dyy, dxy, b.harris_scale4);
+          if (score > 0.f) atomicMax(&s_key[(ly << o) * kDetTW + (lx << o)], det_key(score, o));
+        }
+      }
+    } else {
+      for (int j = threadIdx.x; j < n2; j += blockDim.x) {
+        const int e = s_corner[j];
+        const int o = e >> 11, ly = (e >> 6) & 31, lx = e & 63;
+        const int sw = (kDetTW >> o) + 2 * kHalo;
+        const float score = corner_score(b, s_stage + det_stage_off(o) + (ly + kHalo) * sw + (lx + kHalo), sw);
+        if (score > 0.f) atomicMax(&s_key[(ly << o) * kDetTW + (lx << o)], det_key(score, o));
+      }
+    }
+  }
+  __syncthreads();
+
+  // Output: occupancy bits for the whole tile (every word written, so no
+  // clearing pass), scores and octaves only where a score was stored.  The
+  // tile's 64 columns are two aligned 32-bit words of each row (pitch0 is a
+  // multiple of 128).
+  const int p0 = F.op[0];
+  for (int k = warp; k < kDetTH * (kDetTW / 32); k += blockDim.x >> 5) {
+    const int r = k >> 1;
+    const int c = ((k & 1) << 5) + lane;
+    const unsigned long long key = s_key[r * kDetTW + c];
+    const uint32_t m = __ballot_sync(0xffffffffu, key != 0ull);
     const int Y = Y0 + r;
     if (Y < F.h) {
-      uint32_t m = s_occ[threadIdx.x];
-      const size_t a0 = (size_t)Y * F.op[0] + X0 + 32 * half;
-      F.occ[a0 >> 5] = m;
-      while (m) {
-        const int k = __ffs(m) - 1;
-        m &= m - 1u;
-        const int idx = r * kDetTW + 32 * half + k;
-        F.vmap[a0 + k] = s_map[idx];
-        F.oct8[a0 + k] = (uint8_t)s_oct[idx];
+      const size_t a = (size_t)Y * p0 + X0 + c;
+      if (lane == 0) F.occ[a >> 5] = m;
+      if (key) {
+        F.vmap[a] = __uint_as_float((uint32_t)(key >> 32));
+        F.oct8[a] = (uint8_t)(7 - (int)(key & 0xFFu));
       }
     }
   }
