@@ -40,9 +40,11 @@ L2_FLUSH_BYTES = 256 << 20
 POPC_PER_CLK_PER_SM = 16  # 32-bit population count results per clock per SM
 SMS = 148
 
-# DRAM bytes per launch measured by ncu (dram__bytes_read.sum + dram__bytes_write.sum)
-# on the same workload; kernels without a capture report None.
-NCU_TRAFFIC = {}
+# DRAM bytes per launch measured by ncu (dram__bytes_read.sum + dram__bytes_write.sum,
+# cold cache) on the same workloads (profiles/pair1080_kernels.md,
+# profiles/knn2_65536_k_match_imma.md); kernels without a capture report None.
+NCU_TRAFFIC = {"k_pyramid_blur": 4159744, "k_detect": 5656832, "k_nms": 1499392, "k_describe<2>": 5611008,
+               "k_match_popc": 97792, "k_match_imma": 33602560}
 
 
 def parse_args(argv=None):
@@ -517,12 +519,29 @@ def run_match_workload(args, world, rank, local):
     if rank != 0:
         return None
     pairs = 65536.0 * 65536.0 * world
+    peaks, peak_kind = load_peaks()
+    ms1 = total_ms / steps
+    if mode == orbx.MATCH_IMMA:
+        # 512 int8 ops per pair (256 multiply-adds); the dense int8 rate is twice bf16
+        ach = 65536.0 * 65536.0 * 512 / (ms1 * 1e-3) / 1e12
+        roof = {"kernel": "k_match_imma", "bound": "tensor", "achieved": ach, "peak": 2 * peaks["bf16_tflops"],
+                "unit": "TOP/s (int8)", "frac": ach / (2 * peaks["bf16_tflops"]),
+                "traffic": NCU_TRAFFIC.get("k_match_imma"),
+                "peak_kind": f"{peak_kind}: 2 x bf16_tflops (int8 dense rate is twice bf16)"}
+    else:
+        peak_pairs = SMS * POPC_PER_CLK_PER_SM * peaks.get("sm_max_mhz", 1965.0) * 1e6 / 8
+        ach = 65536.0 * 65536.0 / (ms1 * 1e-3)
+        roof = {"kernel": "k_match_popc", "bound": "int", "achieved": ach / 1e12, "peak": peak_pairs / 1e12,
+                "unit": "Tpairs/s", "frac": ach / peak_pairs, "traffic": None,
+                "peak_kind": "derived: 148 SMs x 16 popc/clk x max SM clock / 8 popc per pair"}
+    cpu = cpu_baseline_knn2(qh, dbh, budget_s=8.0)
     return {"metric": "Hamming match-pairs/s (exact, k=2, 65536 x 65536)", "value": pairs * steps / (total_ms * 1e-3),
             "unit": "pairs/s", "n_gpus": world, "steps": steps, "warmup": args.warmup,
             "ms_per_step": total_ms / steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "int8" if mode == orbx.MATCH_IMMA else "u32", "data": "synthetic (cuda-orb_b200/synth.py)",
             "config": {"workload": f"k=2 matching 65536 x 65536, {args.match_mode} form",
                        "l2": "flushed before every step"},
+            "roofline": roof, "cpu_baseline": cpu,
             "gpu_launches": 3 * steps if mode == orbx.MATCH_IMMA else steps}
 
 
