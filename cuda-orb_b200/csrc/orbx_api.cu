@@ -962,16 +962,24 @@ ORBX_API int orbx_pair_host(orbx_ctx* c, const uint8_t* h_img_a, const uint8_t* 
   rc = orbx_pair(c, c->io_img[0], c->io_img[1], w, h, pitch, c->io_pts[0], c->io_desc[0], c->io_count,
                  c->io_pts[1], c->io_desc[1], c->io_count + 1, mode);
   if (rc) return rc;
-  ORBX_CUDA(cudaMemcpyAsync(c->io_count_host, c->io_count, 2 * sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+  // one export kernel writes counts, keypoints (and descriptors) into mapped
+  // pinned memory, so the host waits once and copies only what was found
+  const uint8_t* res = nullptr;
+  const bool with_desc = h_desc_a || h_desc_b;
+  if ((rc = hostio_export_pair(c, c->io_pts[0], c->io_pts[1], c->io_desc[0], c->io_desc[1], c->io_count,
+                               c->p.max_pts, with_desc, &res)) != 0)
+    return rc;
   ORBX_CUDA(cudaStreamSynchronize(c->stream));
-  const int na = c->io_count_host[0], nb = c->io_count_host[1];
+  const int na = reinterpret_cast<const int*>(res)[0], nb = reinterpret_cast<const int*>(res)[1];
   *h_n_a = na;
   *h_n_b = nb;
-  if (na > 0) ORBX_CUDA(cudaMemcpyAsync(h_pts_a, c->io_pts[0], sizeof(orbx_point) * na, cudaMemcpyDeviceToHost, c->stream));
-  if (nb > 0) ORBX_CUDA(cudaMemcpyAsync(h_pts_b, c->io_pts[1], sizeof(orbx_point) * nb, cudaMemcpyDeviceToHost, c->stream));
-  if (h_desc_a && na > 0) ORBX_CUDA(cudaMemcpyAsync(h_desc_a, c->io_desc[0], (size_t)32 * na, cudaMemcpyDeviceToHost, c->stream));
-  if (h_desc_b && nb > 0) ORBX_CUDA(cudaMemcpyAsync(h_desc_b, c->io_desc[1], (size_t)32 * nb, cudaMemcpyDeviceToHost, c->stream));
-  ORBX_CUDA(cudaStreamSynchronize(c->stream));
+  const size_t mp = (size_t)c->p.max_pts;
+  const uint8_t* pts = res + 16;
+  const uint8_t* desc = pts + 2 * mp * sizeof(orbx_point);
+  std::memcpy(h_pts_a, pts, sizeof(orbx_point) * (size_t)na);
+  std::memcpy(h_pts_b, pts + mp * sizeof(orbx_point), sizeof(orbx_point) * (size_t)nb);
+  if (h_desc_a) std::memcpy(h_desc_a, desc, (size_t)32 * na);
+  if (h_desc_b) std::memcpy(h_desc_b, desc + mp * 32, (size_t)32 * nb);
   return ORBX_OK;
 }
 

@@ -29,6 +29,9 @@ struct HostIO {
   int* pack = nullptr;  // device [n][k] packed fields
   int* pack_host = nullptr;  // pinned copy
   size_t pack_ints = 0;
+  uint8_t* map = nullptr;      // pinned, mapped: orbx_pair_host results written by the device
+  uint8_t* map_dev = nullptr;  // its device address
+  size_t map_bytes = 0;
 };
 
 void hostio_free(HostIO* io) {
@@ -40,7 +43,60 @@ void hostio_free(HostIO* io) {
   }
   cudaFree(io->pack);
   cudaFreeHost(io->pack_host);
+  cudaFreeHost(io->map);
   delete io;
+}
+
+// Result block of a pair in mapped host memory: counts (16 bytes), then the
+// keypoints of A and B (max_pts each), then optionally the descriptors.
+__global__ void k_export_pair(const orbx_point* __restrict__ pa, const orbx_point* __restrict__ pb,
+                              const uint8_t* __restrict__ da, const uint8_t* __restrict__ db,
+                              const int* __restrict__ count, int max_pts, int with_desc, uint8_t* __restrict__ out) {
+  const int na = min(count[0], max_pts), nb = min(count[1], max_pts);
+  if (blockIdx.x == 0 && threadIdx.x < 2) reinterpret_cast<int*>(out)[threadIdx.x] = threadIdx.x ? nb : na;
+  const size_t pts_words = (size_t)max_pts * 7;  // one image's keypoint block, in 32-bit words
+  int* o = reinterpret_cast<int*>(out + 16);
+  const long long wa = (long long)na * 7, wb = (long long)nb * 7;
+  const long long qa = with_desc ? (long long)na * 8 : 0, qb = with_desc ? (long long)nb * 8 : 0;
+  const long long total = wa + wb + qa + qb;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (long long)gridDim.x * blockDim.x) {
+    if (i < wa) {
+      o[i] = reinterpret_cast<const int*>(pa)[i];
+    } else if (i < wa + wb) {
+      o[pts_words + (i - wa)] = reinterpret_cast<const int*>(pb)[i - wa];
+    } else if (i < wa + wb + qa) {
+      o[2 * pts_words + (i - wa - wb)] = reinterpret_cast<const int*>(da)[i - wa - wb];
+    } else {
+      o[2 * pts_words + (size_t)max_pts * 8 + (i - wa - wb - qa)] = reinterpret_cast<const int*>(db)[i - wa - wb - qa];
+    }
+  }
+}
+
+// Queues k_export_pair on the context stream; *host points at the result block,
+// readable once the stream has been synchronised.
+int hostio_export_pair(orbx_ctx* c, const orbx_point* pa, const orbx_point* pb, const uint8_t* da, const uint8_t* db,
+                       const int* d_count, int max_pts, bool with_desc, const uint8_t** host) {
+  HostIO*& io = ctx_hostio(c);
+  if (!io) io = new HostIO();
+  const size_t bytes = 16 + (size_t)max_pts * (2 * sizeof(orbx_point) + 64);
+  if (io->map_bytes < bytes) {
+    cudaFreeHost(io->map);
+    io->map = nullptr;
+    io->map_dev = nullptr;
+    io->map_bytes = 0;
+    if (cudaHostAlloc(&io->map, bytes, cudaHostAllocMapped) != cudaSuccess ||
+        cudaHostGetDevicePointer(reinterpret_cast<void**>(&io->map_dev), io->map, 0) != cudaSuccess) {
+      (void)cudaGetLastError();
+      cudaFreeHost(io->map);
+      io->map = nullptr;
+      return ORBX_ERR_NOMEM;
+    }
+    io->map_bytes = bytes;
+  }
+  k_export_pair<<<2 * 148, 256, 0, ctx_stream(c)>>>(pa, pb, da, db, d_count, max_pts, with_desc ? 1 : 0, io->map_dev);
+  if (cudaGetLastError() != cudaSuccess) return ORBX_ERR_CUDA;
+  *host = io->map;
+  return ORBX_OK;
 }
 
 // fields: bit 0 = x, y, octave, score, angle (ints 0..4); bit 1 = match, distance (ints 5..6)

@@ -191,4 +191,6 @@ int* ctx_err(orbx_ctx* c);
 struct HostIO;  // orbx_hostio.cu: pinned staging of the host I/O entry points
 HostIO*& ctx_hostio(orbx_ctx* c);
 void hostio_free(HostIO* io);
+int hostio_export_pair(orbx_ctx* c, const orbx_point* pa, const orbx_point* pb, const uint8_t* da, const uint8_t* db,
+                       const int* d_count, int max_pts, bool with_desc, const uint8_t** host);
 }  // namespace orbx

@@ -85,3 +85,28 @@ def test_download_fields(ctx, fields):
         else:
             assert np.all(host[f][:n] == 77), f
         assert np.all(host[f][n:] == 77)
+
+
+@pytest.mark.parametrize("with_desc", [False, True])
+def test_pair_host_equals_device_pair(ctx, with_desc):
+    a, b, _ = synth.make_pair(1920, 1080, seed=43)
+    w, h, pitch = 1920, 1080, a.shape[1]
+    A, B = orbx.FrameBuffers(10000), orbx.FrameBuffers(10000)
+    ctx.pair_ptr(torch.from_numpy(a).cuda(), torch.from_numpy(b).cuda(), w, h, pitch, A.points, A.desc, A.count,
+                 B.points, B.desc, B.count)
+    ctx.sync()
+    pa, da = A.to_host()
+    pb, db = B.to_host()
+    for _ in range(2):  # twice: the mapped result block is reused
+        hpa = np.full((10000, 7), -7, dtype=np.int32)
+        hpb = np.full((10000, 7), -7, dtype=np.int32)
+        hna, hnb = np.zeros(1, np.int32), np.zeros(1, np.int32)
+        hda = np.zeros((10000, 32), np.uint8) if with_desc else None
+        hdb = np.zeros((10000, 32), np.uint8) if with_desc else None
+        ctx.pair_host(np.ascontiguousarray(a), np.ascontiguousarray(b), w, h, pitch, hpa, hna, hpb, hnb, hda, hdb)
+        assert int(hna[0]) == len(pa) and int(hnb[0]) == len(pb)
+        assert np.array_equal(hpa[:len(pa)].view(PT).reshape(-1), pa)
+        assert np.array_equal(hpb[:len(pb)].view(PT).reshape(-1), pb)
+        assert np.all(hpa[len(pa):] == -7)
+        if with_desc:
+            assert np.array_equal(hda[:len(pa)], da) and np.array_equal(hdb[:len(pb)], db)
