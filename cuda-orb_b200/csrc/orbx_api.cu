@@ -95,6 +95,7 @@ struct orbx_ctx {
   int io_max_pts = 0;
   cudaEvent_t prof_ev[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
   HostIO* hostio = nullptr;  // orbx_upload_image / orbx_download_points staging
+  OcvWork* ocv = nullptr;    // orbx_ocv_detect_and_compute workspace
   // launch shapes (orbx_tuning)
   int nms_rows = kNmsRows;
   int describe_bps = 8;
@@ -645,6 +646,7 @@ ORBX_API int orbx_destroy(orbx_ctx* c) {
   cudaFree(c->io_count);
   cudaFreeHost(c->io_count_host);
   hostio_free(c->hostio);
+  ocv_free(c->ocv);
   for (auto& e : c->prof_ev)
     if (e) cudaEventDestroy(e);
   cudaFree(c->imma_q);
@@ -1343,5 +1345,7 @@ namespace orbx {
 int ctx_device(const orbx_ctx* c) { return c->device; }
 cudaStream_t ctx_stream(const orbx_ctx* c) { return c->stream; }
 int* ctx_err(orbx_ctx* c) { return c->d_err; }
+void umax_table(int patch_size, int* umax) { make_umax(patch_size, umax); }
+OcvWork*& ctx_ocv(orbx_ctx* c) { return c->ocv; }
 HostIO*& ctx_hostio(orbx_ctx* c) { return c->hostio; }
 }  // namespace orbx

@@ -6,6 +6,7 @@
 // reads that leave an octave see the same bytes the reference sees.
 #include "orbx_device.cuh"
 #include "orbx_internal.cuh"
+#include "orbx_fast.cuh"
 
 namespace orbx {
 
@@ -176,28 +177,6 @@ __host__ __device__ constexpr int det_stage_off(int octave) {
 }
 __host__ __device__ constexpr int det_stage_bytes() { return det_stage_off(kMaxOctaves); }
 
-// FAST ring (makeOffsets, orbd.cu:463-496), as (dx, dy).
-__constant__ int8_t c_ring[16][2] = {{0, 3},  {1, 3},   {2, 2},   {3, 1},   {3, 0},  {3, -1}, {2, -2}, {1, -3},
-                                     {0, -3}, {-1, -3}, {-2, -2}, {-3, -1}, {-3, 0}, {-3, 1}, {-2, 2}, {-1, 3}};
-
-__device__ __forceinline__ bool has_arc9(uint32_t m16) {
-  uint32_t m = m16 | (m16 << 16);  // circular
-  uint32_t a = m & (m >> 1);       // runs of 2
-  a &= a >> 2;                     // runs of 4
-  a &= a >> 4;                     // runs of 8
-  a &= m >> 8;                     // runs of 9
-  return (a & 0xFFFFu) != 0u;
-}
-
-// Final step of dHarrisScore (orbd.cu:667-668) as the reference build evaluates it.
-__device__ __forceinline__ float harris_combine(int dxx, int dyy, int dxy, float scale4) {
-  const unsigned dsxy = (unsigned)dxx + (unsigned)dyy;
-  const int A = (int)((unsigned)dxx * (unsigned)dyy - (unsigned)dxy * (unsigned)dxy);
-  const unsigned Bq = dsxy * dsxy;
-  const float u = __fmaf_rn(-0.04f, __uint2float_rn(Bq), __int2float_rn(A));
-  return __fmul_rn(u, scale4);
-}
-
 // dHarrisScore (orbd.cu:651-669) on a shared-memory tile of row stride sw.
 // Integer sums wrap as 32-bit; the final combine is
 // fma(-0.04f, (float)(uint32)(dsxy*dsxy), (float)(int32)(dxx*dyy - dxy*dxy)) * scale^4,
@@ -222,39 +201,6 @@ __device__ __forceinline__ float harris_score(const uint8_t* c, int sw, float sc
   return harris_combine(dxx, dyy, dxy, scale4);
 }
 
-// dFastScore (orbd.cu:538-586, FAST_PATTERN 16).
-__device__ __forceinline__ float fast_score(const int* d, int threshold) {
-  int a0 = threshold;
-#pragma unroll
-  for (int k = 0; k < 16; k += 2) {
-    int a = min(d[k + 1], d[k + 2]);
-    a = min(a, d[k + 3]);
-    if (a <= a0) continue;
-    a = min(a, d[k + 4]);
-    a = min(a, d[k + 5]);
-    a = min(a, d[k + 6]);
-    a = min(a, d[k + 7]);
-    a = min(a, d[k + 8]);
-    a0 = max(a0, min(a, d[k]));
-    a0 = max(a0, min(a, d[k + 9]));
-  }
-  int b0 = -a0;
-#pragma unroll
-  for (int k = 0; k < 16; k += 2) {
-    int b = max(d[k + 1], d[k + 2]);
-    b = max(b, d[k + 3]);
-    b = max(b, d[k + 4]);
-    b = max(b, d[k + 5]);
-    if (b >= b0) continue;
-    b = max(b, d[k + 6]);
-    b = max(b, d[k + 7]);
-    b = max(b, d[k + 8]);
-    b0 = min(b0, max(b, d[k]));
-    b0 = min(b0, max(b, d[k + 9]));
-  }
-  return (float)(-b0 - 1);
-}
-
 // Necessary condition for FAST-9: every run of 9 ring pixels contains two
 // neighbouring cardinal points (ring positions k and k+4, k = 0, 4, 8, 12), so
 // both of some such pair must be darker than v - t, or both brighter than
@@ -275,20 +221,6 @@ __device__ __forceinline__ uint32_t fast9_pretest4(const uint8_t* w, int sw, uin
   const uint32_t d0 = __vcmpltu4(p0, lo), d4 = __vcmpltu4(p4, lo), d8 = __vcmpltu4(p8, lo), d12 = __vcmpltu4(p12, lo);
   const uint32_t b0 = __vcmpgtu4(p0, hi), b4 = __vcmpgtu4(p4, hi), b8 = __vcmpgtu4(p8, hi), b12 = __vcmpgtu4(p12, hi);
   return ((d0 | d8) & (d4 | d12)) | ((b0 | b8) & (b4 | b12));
-}
-
-// FAST-9 segment test on a shared-memory tile of row stride sw: a run of 9
-// contiguous ring pixels all darker than v - t or all brighter than v + t (the
-// reference's LUT pre-test and arc loop, orbd.cu:683-740, decide exactly this).
-__device__ __forceinline__ bool fast9_full(const uint8_t* c, int sw, int lo, int hi) {
-  uint32_t dark = 0, bright = 0;
-#pragma unroll
-  for (int k = 0; k < 16; k++) {
-    const int p = c[c_ring[k][1] * sw + c_ring[k][0]];
-    dark |= (uint32_t)(p < lo) << k;
-    bright |= (uint32_t)(p > hi) << k;
-  }
-  return has_arc9(dark) || has_arc9(bright);
 }
 
 __device__ __forceinline__ float corner_score(const Batch& b, const uint8_t* c, int sw) {

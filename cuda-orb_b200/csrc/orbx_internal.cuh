@@ -189,6 +189,10 @@ int ctx_device(const orbx_ctx* c);
 cudaStream_t ctx_stream(const orbx_ctx* c);
 int* ctx_err(orbx_ctx* c);
 struct HostIO;  // orbx_hostio.cu: pinned staging of the host I/O entry points
+struct OcvWork;  // orbx_ocv.cu: buffers of the OpenCV-style pipeline
+OcvWork*& ctx_ocv(orbx_ctx* c);
+void ocv_free(OcvWork* w);
+void umax_table(int patch_size, int* umax);  // setUmax (orbd.cu:66-92)
 HostIO*& ctx_hostio(orbx_ctx* c);
 void hostio_free(HostIO* io);
 int hostio_export_pair(orbx_ctx* c, const orbx_point* pa, const orbx_point* pb, const uint8_t* da, const uint8_t* db,

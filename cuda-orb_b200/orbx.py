@@ -107,6 +107,8 @@ def lib():
         L.orbx_learned_destroy.argtypes = [vp]
         L.orbx_gemm_bf16.argtypes = [vp, vp, vp, i32, i32, i32, vp, i32, i32, vp, vp]
         L.orbx_upload_image.argtypes = [vp, vp, i32, i32, i32, vp, i32]
+        L.orbx_ocv_default_params.argtypes = [ctypes.POINTER(OcvParams)]
+        L.orbx_ocv_detect_and_compute.argtypes = [vp, ctypes.POINTER(OcvParams), vp, i32, i32, i32, vp, vp, vp, i32]
         L.orbx_download_points.argtypes = [vp, vp, i32, vp, i32]
         L.orbx_selftest_pi_minus.argtypes = [ctypes.c_uint32, ctypes.c_uint32]
         L.orbx_selftest_pi_minus.restype = ctypes.c_longlong
@@ -115,6 +117,40 @@ def lib():
 
 
 FIELDS_KEYPOINT, FIELDS_MATCH = 1, 2
+class OcvParams(ctypes.Structure):
+    _fields_ = [("nfeatures", ctypes.c_int), ("scale_factor", ctypes.c_float), ("nlevels", ctypes.c_int),
+                ("edge_threshold", ctypes.c_int), ("score_type", ctypes.c_int), ("patch_size", ctypes.c_int),
+                ("fast_threshold", ctypes.c_int)]
+
+
+OCV_KEYPOINT_DTYPE = np.dtype([("x", "<f4"), ("y", "<f4"), ("size", "<f4"), ("angle", "<f4"),
+                               ("response", "<f4"), ("octave", "<i4")])
+
+
+def ocv_params(**kw):
+    p = OcvParams()
+    _check(lib().orbx_ocv_default_params(ctypes.byref(p)), "orbx_ocv_default_params")
+    for k, v in kw.items():
+        setattr(p, k, v)
+    return p
+
+
+def ocv_detect_and_compute(ctx, img, w, h, params=None, cap=None):
+    """OpenCV-compatible mode on a uint8 CUDA image (h, pitch).  Returns host
+    (keypoints as OCV_KEYPOINT_DTYPE, descriptors (n, 32) uint8)."""
+    torch = _torch()
+    params = params if params is not None else ocv_params()
+    cap = cap if cap is not None else params.nfeatures
+    kps = torch.zeros((cap, 6), dtype=torch.int32, device=img.device)
+    desc = torch.zeros((cap, 32), dtype=torch.uint8, device=img.device)
+    n = torch.zeros(1, dtype=torch.int32, device=img.device)
+    _check(lib().orbx_ocv_detect_and_compute(ctx.h, ctypes.byref(params), _ptr(img), w, h, img.shape[1], _ptr(kps),
+                                             _ptr(desc), _ptr(n), cap), "orbx_ocv_detect_and_compute")
+    ctx.sync()
+    k = int(n.item())
+    return kps[:k].cpu().numpy().copy().view(OCV_KEYPOINT_DTYPE).reshape(k), desc[:k].cpu().numpy().copy()
+
+
 PROPOSAL_MLP, PROPOSAL_LSH = 0, 1
 INIT_CENTROIDS, INIT_RANDOM = 0, 1
 GEMM_F32, GEMM_BIAS_RELU_BF16, GEMM_MASK_BF16, GEMM_BF16, GEMM_TOP8 = 0, 1, 2, 3, 4

@@ -158,6 +158,39 @@ ORBX_API int orbx_upload_image(orbx_ctx* ctx, const uint8_t* h_img, int w, int h
 #define ORBX_FIELDS_MATCH 2
 ORBX_API int orbx_download_points(orbx_ctx* ctx, const orbx_point* d_points, int n, orbx_point* h_points, int fields);
 
+/* OpenCV-compatible mode.  cv::ORB's algorithm rather than the reference's:
+ * a pyramid of `nlevels` levels, each resized from the previous one by
+ * 1 / scale_factor (bilinear); FAST-9 with 3x3 non-maximum suppression on each
+ * level, outside `edge_threshold`; a per-level feature budget (geometric in
+ * 1 / scale_factor) filled by FAST score (2x budget) then Harris score (budget),
+ * as orb.cpp's unused retain_topn hints at (orb.cpp:41); intensity-centroid
+ * angle; rBRIEF with the rotated pattern on each level blurred by a 7x7 sigma 2
+ * Gaussian.  Comparable with cv2.ORB statistically, not bit for bit.  Keypoints
+ * are sorted by level, then by decreasing score. */
+typedef struct orbx_ocv_params {
+  int nfeatures;       /* total budget, <= 16000 */
+  float scale_factor;  /* (1, 2] */
+  int nlevels;         /* 1..16 */
+  int edge_threshold;  /* >= 19: the angle disc and rotated pattern stay in the level */
+  int score_type;      /* 0 = HARRIS_SCORE, 1 = FAST_SCORE */
+  int patch_size;      /* 31 */
+  int fast_threshold;  /* 0..255 */
+} orbx_ocv_params;
+
+/* cv::KeyPoint fields: level-0 position, diameter, angle in degrees [0, 360),
+ * response (Harris or FAST score) and pyramid level. */
+typedef struct orbx_ocv_keypoint {
+  float x, y, size, angle, response;
+  int octave;
+} orbx_ocv_keypoint;
+
+ORBX_API int orbx_ocv_default_params(orbx_ocv_params* p);
+/* d_keypoints: cap entries; d_desc: cap * 32 bytes; *d_n (device) = keypoints
+ * written (min(found, cap)).  Asynchronous. */
+ORBX_API int orbx_ocv_detect_and_compute(orbx_ctx* ctx, const orbx_ocv_params* p, const uint8_t* d_image, int w, int h,
+                                         int pitch, orbx_ocv_keypoint* d_keypoints, uint8_t* d_desc, int* d_n,
+                                         int cap);
+
 /* Profiling variant of orbx_pair: the same launches without the graph, with a
  * CUDA event between consecutive kernels; writes the milliseconds of the
  * pyramid/blur, detect, NMS, describe and match kernels to stage_ms[0..4].
