@@ -201,12 +201,32 @@ __device__ __forceinline__ float harris_score(const uint8_t* c, int sw, float sc
   return harris_combine(dxx, dyy, dxy, scale4);
 }
 
+// Byte-wise arithmetic on packed words with plain integer operations (the
+// byte-SIMD intrinsics are several instructions each on this architecture).
+constexpr uint32_t kB7 = 0x80808080u, kLo7 = 0x7F7F7F7Fu;
+// bit 7 of each byte set where x < y (unsigned): the 7-bit differences cannot
+// borrow across bytes, and the top bits decide when they differ
+__device__ __forceinline__ uint32_t swar_lt(uint32_t x, uint32_t y) {
+  const uint32_t t = (x | kB7) - (y & kLo7);
+  return ((~x & y) | (~(x ^ y) & ~t)) & kB7;
+}
+// max(v - t, 0) and min(v + t, 255) per byte, t given in every byte
+__device__ __forceinline__ uint32_t swar_sub_sat(uint32_t v, uint32_t t4) {
+  const uint32_t d = ((v | kB7) - (t4 & kLo7)) ^ ((v ^ ~t4) & kB7);
+  return d & ~((swar_lt(v, t4) >> 7) * 0xFFu);
+}
+__device__ __forceinline__ uint32_t swar_add_sat(uint32_t v, uint32_t t4) {
+  const uint32_t s = ((v & kLo7) + (t4 & kLo7)) ^ ((v ^ t4) & kB7);
+  const uint32_t carry = ((v & t4) | ((v | t4) & ~s)) & kB7;
+  return s | ((carry >> 7) * 0xFFu);
+}
+
 // Necessary condition for FAST-9: every run of 9 ring pixels contains two
 // neighbouring cardinal points (ring positions k and k+4, k = 0, 4, 8, 12), so
 // both of some such pair must be darker than v - t, or both brighter than
 // v + t.  It never changes a result.  Evaluated for four horizontally adjacent
 // centres at once on packed bytes: w points at the aligned word holding them
-// (row stride sw bytes, a multiple of 4); returns 0xFF in each byte whose
+// (row stride sw bytes, a multiple of 4); returns bit 7 of each byte whose
 // centre passes.  Saturating v - t and v + t (t <= 255) give the same answers
 // as the signed comparisons p < v - t and p > v + t.
 __device__ __forceinline__ uint32_t fast9_pretest4(const uint8_t* w, int sw, uint32_t t4) {
@@ -217,9 +237,9 @@ __device__ __forceinline__ uint32_t fast9_pretest4(const uint8_t* w, int sw, uin
   const uint32_t p8 = *reinterpret_cast<const uint32_t*>(w - 3 * sw);   // ring 8: (x, y - 3)
   const uint32_t p4 = __byte_perm(c, cr, 0x6543);                       // ring 4: (x + 3, y)
   const uint32_t p12 = __byte_perm(cl, c, 0x4321);                      // ring 12: (x - 3, y)
-  const uint32_t lo = __vsubus4(c, t4), hi = __vaddus4(c, t4);
-  const uint32_t d0 = __vcmpltu4(p0, lo), d4 = __vcmpltu4(p4, lo), d8 = __vcmpltu4(p8, lo), d12 = __vcmpltu4(p12, lo);
-  const uint32_t b0 = __vcmpgtu4(p0, hi), b4 = __vcmpgtu4(p4, hi), b8 = __vcmpgtu4(p8, hi), b12 = __vcmpgtu4(p12, hi);
+  const uint32_t lo = swar_sub_sat(c, t4), hi = swar_add_sat(c, t4);
+  const uint32_t d0 = swar_lt(p0, lo), d4 = swar_lt(p4, lo), d8 = swar_lt(p8, lo), d12 = swar_lt(p12, lo);
+  const uint32_t b0 = swar_lt(hi, p0), b4 = swar_lt(hi, p4), b8 = swar_lt(hi, p8), b12 = swar_lt(hi, p12);
   return ((d0 | d8) & (d4 | d12)) | ((b0 | b8) & (b4 | b12));
 }
 
@@ -246,10 +266,12 @@ __device__ __forceinline__ unsigned long long det_key(float score, int o) {
 
 __global__ void __launch_bounds__(256, 4) k_detect(Batch b) {
   __shared__ __align__(16) uint8_t s_stage[det_stage_bytes()];
-  __shared__ unsigned long long s_key[kDetTH * kDetTW];
+  __shared__ __align__(16) unsigned long long s_key[kDetTH * kDetTW];
   __shared__ uint16_t s_cand[kDetMaxCand];
   __shared__ uint16_t s_corner[kDetMaxCand];
   __shared__ int s_n[2];
+  __shared__ uint32_t s_occ[kDetTH * kDetTW / 32];
+  __shared__ int s_ow[kMaxOctaves], s_oh[kMaxOctaves];
 
   const int t = blockIdx.x;
   const int f = find_frame(b.det_base, b.n_frames, t);
@@ -263,8 +285,14 @@ __global__ void __launch_bounds__(256, 4) k_detect(Batch b) {
   const int warp = threadIdx.x >> 5;
   const int thr = b.fast_thr;
 
-  for (int i = threadIdx.x; i < kDetTH * kDetTW; i += blockDim.x) s_key[i] = 0ull;
+  for (int i = threadIdx.x; i < kDetTH * kDetTW / 2; i += blockDim.x)
+    reinterpret_cast<ulonglong2*>(s_key)[i] = make_ulonglong2(0ull, 0ull);
+  if (threadIdx.x < kDetTH * kDetTW / 32) s_occ[threadIdx.x] = 0u;
   if (threadIdx.x < 2) s_n[threadIdx.x] = 0;
+  if (threadIdx.x < kMaxOctaves) {
+    s_ow[threadIdx.x] = threadIdx.x < n_oct ? F.ow[threadIdx.x] : 0;
+    s_oh[threadIdx.x] = threadIdx.x < n_oct ? F.oh[threadIdx.x] : 0;
+  }
   // Stage every octave's tile with its halo, 4 bytes per load, one row per warp
   // and step: octave offsets and pitches are multiples of 128 and (X0 >> o) - 4
   // is a multiple of 4; a staged row is at most 18 words.
@@ -296,7 +324,7 @@ __global__ void __launch_bounds__(256, 4) k_detect(Batch b) {
       const int nwl = 4 - o;  // log2 words per row
       const int ly = w >> nwl, lx = (w & ((1 << nwl) - 1)) << 2;
       const int x = (X0 >> o) + lx, y = (Y0 >> o) + ly;
-      const int ow = F.ow[o], oh = F.oh[o];
+      const int ow = s_ow[o], oh = s_oh[o];
       uint32_t m = 0u;
       if (y >= 3 && y < oh - 3 && x < ow - 3) {
         const int sw = (kDetTW >> o) + 2 * kHalo;
@@ -345,6 +373,7 @@ __global__ void __launch_bounds__(256, 4) k_detect(Batch b) {
       // wrap, so their order is free)
       const int gid = threadIdx.x >> 3, sub = threadIdx.x & 7;
       for (int j0 = 0; j0 < n2; j0 += 32) {
+        if (j0 + 4 * warp >= n2) break;  // this warp's four groups have no corner (warp-uniform)
         const int j = j0 + gid;
         int dxx = 0, dyy = 0, dxy = 0;
         int e = 0;
@@ -374,7 +403,10 @@ __global__ void __launch_bounds__(256, 4) k_detect(Batch b) {
         if (j < n2 && sub == 0) {
           const int o = e >> 11, ly = (e >> 6) & 31, lx = e & 63;
           const float score = harris_combine(dxx, dyy, dxy, b.harris_scale4);
-          if (score > 0.f) atomicMax(&s_key[(ly << o) * kDetTW + (lx << o)], det_key(score, o));
+          if (score > 0.f) {
+            const int m = (ly << o) * kDetTW + (lx << o);
+            if (atomicMax(&s_key[m], det_key(score, o)) == 0ull) atomicOr(&s_occ[m >> 5], 1u << (m & 31));
+          }
         }
       }
     } else {
@@ -383,29 +415,31 @@ __global__ void __launch_bounds__(256, 4) k_detect(Batch b) {
         const int o = e >> 11, ly = (e >> 6) & 31, lx = e & 63;
         const int sw = (kDetTW >> o) + 2 * kHalo;
         const float score = corner_score(b, s_stage + det_stage_off(o) + (ly + kHalo) * sw + (lx + kHalo), sw);
-        if (score > 0.f) atomicMax(&s_key[(ly << o) * kDetTW + (lx << o)], det_key(score, o));
+        if (score > 0.f) {
+          const int m = (ly << o) * kDetTW + (lx << o);
+          if (atomicMax(&s_key[m], det_key(score, o)) == 0ull) atomicOr(&s_occ[m >> 5], 1u << (m & 31));
+        }
       }
     }
   }
   __syncthreads();
 
-  // Output: occupancy bits for the whole tile (every word written, so no
-  // clearing pass), scores and octaves only where a score was stored.  The
-  // tile's 64 columns are two aligned 32-bit words of each row (pitch0 is a
-  // multiple of 128).
-  const int p0 = F.op[0];
-  for (int k = warp; k < kDetTH * (kDetTW / 32); k += blockDim.x >> 5) {
-    const int r = k >> 1;
-    const int c = ((k & 1) << 5) + lane;
-    const unsigned long long key = s_key[r * kDetTW + c];
-    const uint32_t m = __ballot_sync(0xffffffffu, key != 0ull);
+  // Output: the tile's occupancy words (every word written, so no clearing
+  // pass), then score and octave only where a bit is set.  The tile's 64
+  // columns are two aligned 32-bit words of each row (pitch0 is a multiple of 128).
+  if (threadIdx.x < kDetTH * kDetTW / 32) {
+    const int r = threadIdx.x >> 1, half = threadIdx.x & 1;
     const int Y = Y0 + r;
     if (Y < F.h) {
-      const size_t a = (size_t)Y * p0 + X0 + c;
-      if (lane == 0) F.occ[a >> 5] = m;
-      if (key) {
-        F.vmap[a] = __uint_as_float((uint32_t)(key >> 32));
-        F.oct8[a] = (uint8_t)(7 - (int)(key & 0xFFu));
+      uint32_t m = s_occ[threadIdx.x];
+      const size_t a0 = (size_t)Y * F.op[0] + X0 + 32 * half;
+      F.occ[a0 >> 5] = m;
+      while (m) {
+        const int k = __ffs(m) - 1;
+        m &= m - 1u;
+        const unsigned long long key = s_key[r * kDetTW + 32 * half + k];
+        F.vmap[a0 + k] = __uint_as_float((uint32_t)(key >> 32));
+        F.oct8[a0 + k] = (uint8_t)(7 - (int)(key & 0xFFu));
       }
     }
   }
