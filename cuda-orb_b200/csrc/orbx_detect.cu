@@ -67,6 +67,9 @@ __global__ void __launch_bounds__(256) k_pyramid_blur(Batch b) {
   // stage: source rows y0-3 .. y0+34, columns x0-3 .. x0+132, reflect-101 at
   // the octave edges, as floats and as bytes
   const uint8_t* __restrict__ psrc = F.pyr_src ? F.pyr_src + F.ooff[o] : nullptr;
+  // octave 0 read from a 4-byte aligned image: interior groups take two aligned
+  // words (the group starts one byte past a word boundary, x0 being a multiple of 4)
+  const bool words0 = (o == 0) && !psrc && ((reinterpret_cast<uintptr_t>(img) | (uintptr_t)pitch_in) & 3u) == 0;
   constexpr int kGroups = kPyrSW / 4;
   for (int it = threadIdx.x; it < kPyrSH * kGroups; it += blockDim.x) {
     const int r = it / kGroups;
@@ -74,9 +77,18 @@ __global__ void __launch_bounds__(256) k_pyramid_blur(Batch b) {
     const int y = reflect101(y0 - 3 + r, oh);
     const uint8_t* rowp = psrc ? psrc + (size_t)y * op : img + (size_t)(y << o) * pitch_in;
     const int sh = psrc ? 0 : o;
+    const int cx = x0 - 3 + 4 * g;
     uint32_t v[4];
+    if (words0 && cx >= 1 && cx + 3 < ow) {
+      // bytes cx-1 .. cx+6 lie in [0, pitch_in): cx + 3 < ow <= pitch_in and both words are aligned
+      const uint32_t* wp = reinterpret_cast<const uint32_t*>(rowp + (cx - 1));
+      const uint32_t word = __byte_perm(__ldg(wp), __ldg(wp + 1), 0x4321);
 #pragma unroll
-    for (int j = 0; j < 4; j++) v[j] = __ldg(rowp + (reflect101(x0 - 3 + 4 * g + j, ow) << sh));
+      for (int j = 0; j < 4; j++) v[j] = (word >> (8 * j)) & 0xFFu;
+    } else {
+#pragma unroll
+      for (int j = 0; j < 4; j++) v[j] = __ldg(rowp + (reflect101(cx + j, ow) << sh));
+    }
     reinterpret_cast<float4*>(s_src)[it] = make_float4(u8_to_float(v[0]), u8_to_float(v[1]), u8_to_float(v[2]),
                                                        u8_to_float(v[3]));
     reinterpret_cast<uint32_t*>(s_byte)[it] = v[0] | (v[1] << 8) | (v[2] << 16) | (v[3] << 24);
