@@ -267,6 +267,53 @@ int check_params(const orbx_learned_params* p) {
   return ORBX_OK;
 }
 
+// Largest list and the number of list entries, once the lists are built from
+// counts; synchronises the stream.
+int read_list_stats(orbx_learned* L, const int* counts, cudaStream_t s) {
+  const int C = L->C;
+  std::vector<int> h_counts(C);
+  int total = 0;
+  LCHK(cudaGetLastError());
+  LCHK(cudaMemcpyAsync(h_counts.data(), counts, sizeof(int) * C, cudaMemcpyDeviceToHost, s));
+  LCHK(cudaMemcpyAsync(&total, L->ivf_offsets + C, sizeof(int), cudaMemcpyDeviceToHost, s));
+  LCHK(cudaStreamSynchronize(s));
+  L->stats.largest_cluster = *std::max_element(h_counts.begin(), h_counts.end());
+  L->n_entries = total;
+  return ORBX_OK;
+}
+
+// Spill 2: every row listed in its nearest and second-nearest cluster, from the
+// matcher's top-2 against the centroids.
+int spill_lists(orbx_learned* L, const int32_t* idx2, int* counts, int* cursor, cudaStream_t s) {
+  const int n = L->ndb, C = L->C;
+  LCHK(cudaMemsetAsync(counts, 0, sizeof(int) * C, s));
+  k_count_spill<<<grid1(2ll * n, 256), 256, 0, s>>>(idx2, n, counts);
+  k_scan_counts<<<1, 1024, 0, s>>>(counts, C, L->ivf_offsets, cursor, 0, nullptr);
+  k_scatter_spill<<<grid1(2ll * n, 256), 256, 0, s>>>(idx2, n, cursor, L->ivf_members);
+  return read_list_stats(L, counts, s);
+}
+
+// Device buffers every index holds: the database (bits and the matcher's +-1
+// layout), centroids, assignment, the cluster lists and their rows; the LSH
+// projections.
+int alloc_core(orbx_learned* L) {
+  const int ndb = L->ndb;
+  if (L->keep.alloc(&L->db, (size_t)ndb * 32) || L->keep.alloc(&L->db_pm1, (size_t)imma_rows_db(ndb) * 256) ||
+      L->keep.alloc(&L->centroids, (size_t)L->C * 32) || L->keep.alloc(&L->assign, (size_t)ndb) ||
+      L->keep.alloc(&L->ivf_offsets, (size_t)L->C + 1) || L->keep.alloc(&L->ivf_members, (size_t)ndb * 2) ||
+      L->keep.alloc(&L->ivf_desc, (size_t)ndb * 2 * 32) ||
+      (L->p.proposal == ORBX_PROPOSAL_LSH && L->keep.alloc(&L->lsh, 256 * 256)))
+    return ORBX_ERR_NOMEM;
+  return ORBX_OK;
+}
+
+// The index's copy of the database and its +-1 layout for the int8 matcher.
+int upload_db(orbx_learned* L, const uint8_t* d_db, cudaStream_t s) {
+  LCHK(cudaMemcpyAsync(L->db, d_db, (size_t)L->ndb * 32, cudaMemcpyDeviceToDevice, s));
+  LCHK(launch_expand_pm1(L->db, L->ndb, nullptr, imma_rows_db(L->ndb), L->db_pm1, s));
+  return ORBX_OK;
+}
+
 int cluster_kmeans(orbx_learned* L, cudaStream_t s, int* err) {
   const int n = L->ndb, C = L->C;
   Arena t;
@@ -313,30 +360,49 @@ int cluster_kmeans(orbx_learned* L, cudaStream_t s, int* err) {
     k_majority<<<C, 256, 0, s>>>(L->db, n, L->ivf_members, L->ivf_offsets, L->centroids, L->p.seed, it);
     LCHK(cudaGetLastError());
   }
-  if (L->p.spill == 2) {
-    // list every row in its nearest and second-nearest cluster (the last assignment's top-2)
-    LCHK(cudaMemsetAsync(counts, 0, sizeof(int) * C, s));
-    k_count_spill<<<grid1(2ll * n, 256), 256, 0, s>>>(idx2, n, counts);
-    k_scan_counts<<<1, 1024, 0, s>>>(counts, C, L->ivf_offsets, cursor, 0, nullptr);
-    k_scatter_spill<<<grid1(2ll * n, 256), 256, 0, s>>>(idx2, n, cursor, L->ivf_members);
-    LCHK(cudaGetLastError());
-  }
-  std::vector<int> h_counts(C);
-  LCHK(cudaMemcpyAsync(h_counts.data(), counts, sizeof(int) * C, cudaMemcpyDeviceToHost, s));
-  int total = 0;
-  LCHK(cudaMemcpyAsync(&total, L->ivf_offsets + C, sizeof(int), cudaMemcpyDeviceToHost, s));
-  LCHK(cudaStreamSynchronize(s));
-  L->stats.largest_cluster = *std::max_element(h_counts.begin(), h_counts.end());
-  L->n_entries = total;
-  return ORBX_OK;
+  // spill 2: the last assignment's top-2
+  if (L->p.spill == 2) return spill_lists(L, idx2, counts, cursor, s);
+  return read_list_stats(L, counts, s);
 }
 
-int cluster_lsh(orbx_learned* L, cudaStream_t s, int* err) {
+// Lists over fixed centroids (a loaded index): every row's exact top-2
+// centroids by the int8 matcher, listed under the nearest (spill 1) or both
+// (spill 2).  The same assignment the last clustering iteration makes.
+int lists_from_centroids(orbx_learned* L, cudaStream_t s, int* err) {
   const int n = L->ndb, C = L->C;
   Arena t;
-  float* wtmp;
-  LCHK(t.alloc(&wtmp, 256 * 256));
-  k_init_normal<<<grid1(256 * 256, 256), 256, 0, s>>>(wtmp, 256 * 256, 1.0f, L->p.seed ^ 0x6c7368ull, L->lsh);
+  int *idx2, *counts, *cursor, *changed;
+  uint32_t* dist2;
+  int8_t* cent_pm1;
+  LCHK(t.alloc(&idx2, (size_t)2 * n));
+  LCHK(t.alloc(&dist2, (size_t)2 * n));
+  LCHK(t.alloc(&counts, C));
+  LCHK(t.alloc(&cursor, C));
+  LCHK(t.alloc(&changed, 1));
+  LCHK(t.alloc(&cent_pm1, (size_t)imma_rows_db(C) * 256));
+  ImmaWork iw;
+  LRC(imma_work_alloc(t, iw, n, n, s));
+  LRC(imma_knn(s, err, iw, L->db, n, nullptr, L->db_pm1, true, L->centroids, C, cent_pm1, false, dist2, idx2));
+  LCHK(cudaMemsetAsync(L->assign, 0xFF, sizeof(int) * (size_t)n, s));
+  LCHK(cudaMemsetAsync(counts, 0, sizeof(int) * C, s));
+  LCHK(cudaMemsetAsync(changed, 0, sizeof(int), s));
+  k_assign<<<grid1(n, 256), 256, 0, s>>>(idx2, n, L->assign, counts, changed);
+  if (L->p.spill == 2) return spill_lists(L, idx2, counts, cursor, s);
+  k_scan_counts<<<1, 1024, 0, s>>>(counts, C, L->ivf_offsets, cursor, 0, nullptr);
+  k_scatter_members<<<grid1(n, 256), 256, 0, s>>>(L->assign, n, cursor, L->ivf_members);
+  return read_list_stats(L, counts, s);
+}
+
+// Buckets of the database rows; make_proj draws the projections from the seed
+// (a loaded index brings its own).
+int cluster_lsh(orbx_learned* L, cudaStream_t s, int* err, bool make_proj) {
+  const int n = L->ndb, C = L->C;
+  Arena t;
+  if (make_proj) {
+    float* wtmp;
+    LCHK(t.alloc(&wtmp, 256 * 256));
+    k_init_normal<<<grid1(256 * 256, 256), 256, 0, s>>>(wtmp, 256 * 256, 1.0f, L->p.seed ^ 0x6c7368ull, L->lsh);
+  }
   const int chunk = 65536;
   bf16* x;
   float* proj;
@@ -358,12 +424,7 @@ int cluster_lsh(orbx_learned* L, cudaStream_t s, int* err) {
   k_count<<<grid1(n, 256), 256, 0, s>>>(L->assign, n, counts);
   k_scan_counts<<<1, 1024, 0, s>>>(counts, C, L->ivf_offsets, cursor, 0, nullptr);
   k_scatter_members<<<grid1(n, 256), 256, 0, s>>>(L->assign, n, cursor, L->ivf_members);
-  std::vector<int> h_counts(C);
-  LCHK(cudaMemcpyAsync(h_counts.data(), counts, sizeof(int) * C, cudaMemcpyDeviceToHost, s));
-  LCHK(cudaStreamSynchronize(s));
-  L->stats.largest_cluster = *std::max_element(h_counts.begin(), h_counts.end());
-  L->n_entries = n;
-  return ORBX_OK;
+  return read_list_stats(L, counts, s);
 }
 
 int alloc_weights(orbx_learned* L, Arena& a, float** m, float** v) {
@@ -554,22 +615,12 @@ ORBX_API int orbx_learned_build(orbx_ctx* ctx, const orbx_learned_params* p, con
   };
   int rc = ORBX_OK;
   do {
-    const int dbrows = imma_rows_db(ndb);
-    if (L->keep.alloc(&L->db, (size_t)ndb * 32) || L->keep.alloc(&L->db_pm1, (size_t)dbrows * 256) ||
-        L->keep.alloc(&L->centroids, (size_t)L->C * 32) || L->keep.alloc(&L->assign, (size_t)ndb) ||
-        L->keep.alloc(&L->ivf_offsets, (size_t)L->C + 1) || L->keep.alloc(&L->ivf_members, (size_t)ndb * 2) ||
-        L->keep.alloc(&L->ivf_desc, (size_t)ndb * 2 * 32) ||
-        (p->proposal == ORBX_PROPOSAL_LSH && L->keep.alloc(&L->lsh, 256 * 256))) {
-      rc = ORBX_ERR_NOMEM;
-      break;
-    }
+    rc = alloc_core(L);
+    if (rc) break;
     cudaEventRecord(ev[0], s);
-    if (cudaMemcpyAsync(L->db, d_db, (size_t)ndb * 32, cudaMemcpyDeviceToDevice, s) != cudaSuccess ||
-        launch_expand_pm1(L->db, ndb, nullptr, dbrows, L->db_pm1, s) != cudaSuccess) {
-      rc = ORBX_ERR_CUDA;
-      break;
-    }
-    rc = p->proposal == ORBX_PROPOSAL_MLP ? cluster_kmeans(L, s, err) : cluster_lsh(L, s, err);
+    rc = upload_db(L, d_db, s);
+    if (rc) break;
+    rc = p->proposal == ORBX_PROPOSAL_MLP ? cluster_kmeans(L, s, err) : cluster_lsh(L, s, err, true);
     if (rc) break;
     k_gather_rows<<<grid1(2ll * L->n_entries, 256), 256, 0, s>>>(L->db, L->ivf_members, L->n_entries, L->ivf_desc);
     cudaEventRecord(ev[1], s);
@@ -763,6 +814,243 @@ ORBX_API int orbx_learned_export(orbx_ctx* ctx, const orbx_learned* L, int* h_as
   }
   if (h_b1) LCHK(cudaMemcpy(h_b1, L->b1, sizeof(float) * L->Hd, cudaMemcpyDeviceToHost));
   if (h_b2) LCHK(cudaMemcpy(h_b2, L->b2, sizeof(float) * L->C, cudaMemcpyDeviceToHost));
+  return ORBX_OK;
+}
+
+// ---------------------------------------------------------------- save / load
+// A saved proposal, little-endian, every field 4-byte aligned:
+//   "ORBXLRN1", u32 version, u32 total bytes
+//   the orbx_learned_params fields in declaration order (seed as two u32, low
+//   word first), then the orbx_learned_stats words
+//   MLP: centroids [C][32] u8, W1 [Hd][256] bf16, b1 [Hd] f32, W2 [C][Hd] bf16,
+//        b2 [C] f32 (the weights search uses)
+//   LSH: projections [256][256] bf16
+//   u64 FNV-1a hash of every byte before it
+// The database and the cluster lists are not saved: loading lists a database
+// under the saved centroids (or buckets) again.
+namespace {
+
+constexpr char kSaveMagic[8] = {'O', 'R', 'B', 'X', 'L', 'R', 'N', '1'};
+constexpr uint32_t kSaveVersion = 1;
+constexpr size_t kSaveParamWords = 18;
+constexpr size_t kSaveStatsWords = sizeof(orbx_learned_stats) / 4;
+static_assert(sizeof(orbx_learned_stats) == 4 * (4 + 64 + 64 + 4), "stats are whole 4-byte words");
+
+size_t save_payload_bytes(const orbx_learned_params& p) {
+  const size_t C = (size_t)p.n_clusters, Hd = (size_t)p.hidden;
+  if (p.proposal == ORBX_PROPOSAL_LSH) return 256 * 256 * 2;
+  return C * 32 + Hd * 256 * 2 + Hd * 4 + C * Hd * 2 + C * 4;
+}
+
+size_t save_bytes(const orbx_learned_params& p) {
+  return 16 + 4 * (kSaveParamWords + kSaveStatsWords) + save_payload_bytes(p) + 8;
+}
+
+uint64_t fnv1a(const uint8_t* b, size_t n) {
+  uint64_t h = 0xcbf29ce484222325ull;
+  for (size_t i = 0; i < n; i++) h = (h ^ b[i]) * 0x100000001b3ull;
+  return h;
+}
+
+void put32(uint8_t*& w, uint32_t v) {
+  for (int i = 0; i < 4; i++) *w++ = (uint8_t)(v >> (8 * i));
+}
+uint32_t get32(const uint8_t*& r) {
+  uint32_t v = 0;
+  for (int i = 0; i < 4; i++) v |= (uint32_t)*r++ << (8 * i);
+  return v;
+}
+uint32_t fbits(float f) {
+  uint32_t u;
+  std::memcpy(&u, &f, 4);
+  return u;
+}
+float bitsf(uint32_t u) {
+  float f;
+  std::memcpy(&f, &u, 4);
+  return f;
+}
+
+void put_params(uint8_t*& w, const orbx_learned_params& p) {
+  const uint32_t v[kSaveParamWords] = {(uint32_t)p.proposal, (uint32_t)p.n_clusters, (uint32_t)p.hidden,
+                                       (uint32_t)p.n_probe, (uint32_t)p.kmeans_iters, (uint32_t)p.epochs,
+                                       (uint32_t)p.batch, fbits(p.lr), fbits(p.margin), (uint32_t)p.lsh_bits,
+                                       (uint32_t)p.seed, (uint32_t)(p.seed >> 32), (uint32_t)p.max_distance,
+                                       (uint32_t)p.spill, (uint32_t)p.init, (uint32_t)p.synth_train,
+                                       fbits(p.flip_lo), fbits(p.flip_hi)};
+  for (uint32_t x : v) put32(w, x);
+}
+orbx_learned_params get_params(const uint8_t*& r) {
+  uint32_t v[kSaveParamWords];
+  for (auto& x : v) x = get32(r);
+  orbx_learned_params p{};
+  p.proposal = (int)v[0];
+  p.n_clusters = (int)v[1];
+  p.hidden = (int)v[2];
+  p.n_probe = (int)v[3];
+  p.kmeans_iters = (int)v[4];
+  p.epochs = (int)v[5];
+  p.batch = (int)v[6];
+  p.lr = bitsf(v[7]);
+  p.margin = bitsf(v[8]);
+  p.lsh_bits = (int)v[9];
+  p.seed = (unsigned long long)v[10] | ((unsigned long long)v[11] << 32);
+  p.max_distance = (int)v[12];
+  p.spill = (int)v[13];
+  p.init = (int)v[14];
+  p.synth_train = (int)v[15];
+  p.flip_lo = bitsf(v[16]);
+  p.flip_hi = bitsf(v[17]);
+  return p;
+}
+
+// Device -> host copy of n bytes; the stream is already synchronised.
+int fetch(uint8_t*& w, const void* d, size_t n) {
+  LCHK(cudaMemcpy(w, d, n, cudaMemcpyDeviceToHost));
+  w += n;
+  return ORBX_OK;
+}
+// Host -> device copy of n bytes on the stream; the caller synchronises.
+int send(const uint8_t*& r, void* d, size_t n, cudaStream_t s) {
+  LCHK(cudaMemcpyAsync(d, r, n, cudaMemcpyHostToDevice, s));
+  r += n;
+  return ORBX_OK;
+}
+
+}  // namespace
+
+ORBX_API int orbx_learned_save(orbx_ctx* ctx, const orbx_learned* L, void* h_buf, size_t cap, size_t* h_need) {
+  if (!ctx || !L || !h_need) return ORBX_ERR_ARG;
+  const size_t need = save_bytes(L->p);
+  *h_need = need;
+  if (!h_buf) return ORBX_OK;
+  if (cap < need) return ORBX_ERR_SIZE;
+  if (need > 0xFFFFFFFFull) return ORBX_ERR_SIZE;
+  Guard g(L->device);
+  LCHK(cudaStreamSynchronize(ctx_stream(ctx)));
+  uint8_t* const b = static_cast<uint8_t*>(h_buf);
+  uint8_t* w = b;
+  std::memcpy(w, kSaveMagic, 8);
+  w += 8;
+  put32(w, kSaveVersion);
+  put32(w, (uint32_t)need);
+  put_params(w, L->p);
+  uint32_t st[kSaveStatsWords];
+  std::memcpy(st, &L->stats, sizeof(st));
+  for (uint32_t x : st) put32(w, x);
+  const size_t C = (size_t)L->C, Hd = (size_t)L->Hd;
+  if (L->p.proposal == ORBX_PROPOSAL_MLP) {
+    LRC(fetch(w, L->centroids, C * 32));
+    LRC(fetch(w, L->w1b, Hd * 256 * 2));
+    LRC(fetch(w, L->b1, Hd * 4));
+    LRC(fetch(w, L->w2b, C * Hd * 2));
+    LRC(fetch(w, L->b2, C * 4));
+  } else {
+    LRC(fetch(w, L->lsh, 256 * 256 * 2));
+  }
+  const uint64_t h = fnv1a(b, (size_t)(w - b));
+  put32(w, (uint32_t)h);
+  put32(w, (uint32_t)(h >> 32));
+  return (size_t)(w - b) == need ? ORBX_OK : ORBX_ERR_STATE;
+}
+
+ORBX_API int orbx_learned_load(orbx_ctx* ctx, const void* h_buf, size_t bytes, const uint8_t* d_db, int ndb,
+                               orbx_learned** out) {
+  if (!ctx || !h_buf || !out || !d_db || ndb < 1) return ORBX_ERR_ARG;
+  *out = nullptr;
+  if (ndb > (1 << 22) - 1) return ORBX_ERR_SIZE;
+  // header, parameters, size and hash before anything touches the device
+  const uint8_t* const b = static_cast<const uint8_t*>(h_buf);
+  if (bytes < 16 + 4 * kSaveParamWords + 8 || std::memcmp(b, kSaveMagic, 8) != 0) return ORBX_ERR_ARG;
+  const uint8_t* r = b + 8;
+  if (get32(r) != kSaveVersion || get32(r) != bytes) return ORBX_ERR_ARG;
+  const orbx_learned_params p = get_params(r);
+  LRC(check_params(&p));
+  if (save_bytes(p) != bytes) return ORBX_ERR_ARG;
+  {
+    const uint8_t* t = b + bytes - 8;
+    const uint64_t lo = get32(t), hi = get32(t);
+    if (fnv1a(b, bytes - 8) != (lo | (hi << 32))) return ORBX_ERR_ARG;
+  }
+  Guard g(ctx_device(ctx));
+  cudaStream_t s = ctx_stream(ctx);
+  int* err = ctx_err(ctx);
+  orbx_learned* L = new orbx_learned();
+  L->device = ctx_device(ctx);
+  L->p = p;
+  L->ndb = ndb;
+  L->C = p.n_clusters;
+  L->Hd = p.hidden;
+  uint32_t st[kSaveStatsWords];
+  for (auto& x : st) x = get32(r);
+  std::memcpy(&L->stats, st, sizeof(st));
+  cudaEvent_t ev[2];
+  int made = 0;
+  int rc = ORBX_OK;
+  for (; made < 2; made++)
+    if (cudaEventCreate(&ev[made]) != cudaSuccess) {
+      rc = ORBX_ERR_CUDA;
+      break;
+    }
+  const size_t C = (size_t)L->C, Hd = (size_t)L->Hd;
+  const bool mlp = p.proposal == ORBX_PROPOSAL_MLP;
+  do {
+    if (rc) break;
+    rc = alloc_core(L);
+    if (rc) break;
+    if (mlp && (L->keep.alloc(&L->w1b, Hd * 256) || L->keep.alloc(&L->b1, Hd) || L->keep.alloc(&L->w2b, C * Hd) ||
+                L->keep.alloc(&L->b2, C) || L->keep.alloc(&L->w2tb, C * Hd))) {
+      rc = ORBX_ERR_NOMEM;
+      break;
+    }
+    cudaEventRecord(ev[0], s);
+    rc = upload_db(L, d_db, s);
+    if (rc) break;
+    if (mlp) {
+      if ((rc = send(r, L->centroids, C * 32, s)) || (rc = send(r, L->w1b, Hd * 256 * 2, s)) ||
+          (rc = send(r, L->b1, Hd * 4, s)) || (rc = send(r, L->w2b, C * Hd * 2, s)) || (rc = send(r, L->b2, C * 4, s)))
+        break;
+      k_transpose_bf16<<<dim3(L->Hd / 32, L->C / 32), dim3(32, 8), 0, s>>>(L->w2b, L->C, L->Hd, L->w2tb);
+      rc = lists_from_centroids(L, s, err);
+    } else {
+      if ((rc = send(r, L->lsh, 256 * 256 * 2, s))) break;
+      rc = cluster_lsh(L, s, err, false);
+    }
+    if (rc) break;
+    k_gather_rows<<<grid1(2ll * L->n_entries, 256), 256, 0, s>>>(L->db, L->ivf_members, L->n_entries, L->ivf_desc);
+    cudaEventRecord(ev[1], s);
+    if (cudaStreamSynchronize(s) != cudaSuccess || cudaGetLastError() != cudaSuccess) {
+      rc = ORBX_ERR_CUDA;
+      break;
+    }
+    int h_err = 0;
+    cudaMemcpy(&h_err, err, sizeof(int), cudaMemcpyDeviceToHost);
+    if (h_err) {
+      cudaMemset(err, 0, sizeof(int));
+      rc = ORBX_ERR_TIMEOUT;
+      break;
+    }
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, ev[0], ev[1]);
+    L->stats.build_ms[0] = ms;
+    L->stats.build_ms[1] = 0.f;
+    L->stats.build_ms[2] = 0.f;
+    L->stats.build_ms[3] = ms;
+  } while (0);
+  for (int i = 0; i < made; i++) cudaEventDestroy(ev[i]);
+  if (rc) {
+    cudaStreamSynchronize(s);
+    (void)cudaGetLastError();
+    delete L;
+    return rc;
+  }
+  *out = L;
+  return ORBX_OK;
+}
+
+ORBX_API int orbx_learned_get_params(const orbx_learned* L, orbx_learned_params* p) {
+  if (!L || !p) return ORBX_ERR_ARG;
+  *p = L->p;
   return ORBX_OK;
 }
 

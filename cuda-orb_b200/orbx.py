@@ -16,6 +16,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "liborbx.so")
 
 ORBX_OK = 0
+ORBX_ERR_ARG, ORBX_ERR_CUDA, ORBX_ERR_SIZE, ORBX_ERR_STATE, ORBX_ERR_TIMEOUT, ORBX_ERR_NOMEM = 1, 2, 3, 4, 5, 6
 MATCH_POPC = 0
 MATCH_IMMA = 1
 MATCH_AUTO = 2
@@ -104,6 +105,9 @@ def lib():
         L.orbx_learned_get_stats.argtypes = [vp, ctypes.POINTER(LearnedStats)]
         L.orbx_learned_export.argtypes = [vp, vp, vp, vp, vp, vp, vp, vp]
         L.orbx_learned_gradients.argtypes = [vp, vp, vp, vp, i32, vp, vp, vp, vp, vp]
+        L.orbx_learned_save.argtypes = [vp, vp, vp, ctypes.c_size_t, ctypes.POINTER(ctypes.c_size_t)]
+        L.orbx_learned_load.argtypes = [vp, vp, ctypes.c_size_t, vp, i32, ctypes.POINTER(vp)]
+        L.orbx_learned_get_params.argtypes = [vp, ctypes.POINTER(LearnedParams)]
         L.orbx_learned_destroy.argtypes = [vp]
         L.orbx_gemm_bf16.argtypes = [vp, vp, vp, i32, i32, i32, vp, i32, i32, vp, vp]
         L.orbx_upload_image.argtypes = [vp, vp, i32, i32, i32, vp, i32]
@@ -415,6 +419,30 @@ class LearnedIndex:
                                         ctypes.byref(h)), "orbx_learned_build")
         self.h = h
         self.ndb = db.shape[0]
+
+    @classmethod
+    def load(cls, ctx, data, db):
+        """An index from save()'s bytes over the uint8 CUDA database db (n, 32),
+        listed again under the saved centroids or buckets; no training."""
+        self = cls.__new__(cls)
+        self.ctx = ctx
+        h = ctypes.c_void_p()
+        buf = ctypes.create_string_buffer(bytes(data), len(data))
+        _check(lib().orbx_learned_load(ctx.h, buf, len(data), _ptr(db), db.shape[0], ctypes.byref(h)),
+               "orbx_learned_load")
+        self.h = h
+        self.ndb = db.shape[0]
+        self.params = LearnedParams()
+        _check(lib().orbx_learned_get_params(self.h, ctypes.byref(self.params)), "orbx_learned_get_params")
+        return self
+
+    def save(self):
+        """The checkpoint as bytes (parameters, statistics, centroids, search weights)."""
+        need = ctypes.c_size_t()
+        _check(lib().orbx_learned_save(self.ctx.h, self.h, None, 0, ctypes.byref(need)), "orbx_learned_save")
+        buf = ctypes.create_string_buffer(need.value)
+        _check(lib().orbx_learned_save(self.ctx.h, self.h, buf, need.value, ctypes.byref(need)), "orbx_learned_save")
+        return buf.raw
 
     def close(self):
         if getattr(self, "h", None):

@@ -331,6 +331,23 @@ ORBX_API int orbx_learned_export(orbx_ctx* ctx, const orbx_learned* index, int* 
  * step computes them, copied to the host.  n is a multiple of 128. */
 ORBX_API int orbx_learned_gradients(orbx_ctx* ctx, orbx_learned* index, const uint8_t* d_x, const int* d_labels, int n,
                                     float* h_loss, float* h_dw1, float* h_db1, float* h_dw2, float* h_db2);
+/* Checkpoint of a built index: parameters, statistics, cluster centroids and
+ * the MLP's search weights (bf16 W1, W2; fp32 b1, b2), or the LSH projections,
+ * with a hash of the bytes.  Not the database and not the cluster lists.
+ * h_buf NULL: only *h_need is set.  cap < *h_need: ORBX_ERR_SIZE.
+ * Synchronises the context's stream. */
+ORBX_API int orbx_learned_save(orbx_ctx* ctx, const orbx_learned* index, void* h_buf, size_t cap, size_t* h_need);
+/* An index from a checkpoint over d_db (the database it was built on, or
+ * another one), without clustering or training: each row is listed under its
+ * nearest saved centroid (spill 2: its two nearest) by the exact int8 matcher,
+ * or under its LSH bucket.  Over the same database the loaded index searches
+ * exactly like the saved one.  A checkpoint with a wrong magic, version, size
+ * or hash, or invalid parameters, returns ORBX_ERR_ARG before any device work.
+ * The fp32 master weights stay behind, so orbx_learned_gradients works on a
+ * loaded index but no training continues from it.  Synchronises. */
+ORBX_API int orbx_learned_load(orbx_ctx* ctx, const void* h_buf, size_t bytes, const uint8_t* d_db, int ndb,
+                               orbx_learned** out);
+ORBX_API int orbx_learned_get_params(const orbx_learned* index, orbx_learned_params* p);
 ORBX_API int orbx_learned_destroy(orbx_learned* index);
 
 /* The BF16 tensor-core GEMM used by the MLP: C = A * B^T with A [M][K] and

@@ -271,3 +271,120 @@ def test_spill_and_synthetic_rows_and_distance_rule(ctx):
         finally:
             idx.close()
     assert rec[2] >= rec[1], rec
+
+
+# ---------------------------------------------------------------- checkpoints
+CKPT_HEAD = 16 + 4 * (18 + 136)  # magic, version, size; 18 parameter words; the statistics words
+
+
+def _ckpt_centroids(blob, C):
+    return np.frombuffer(blob, dtype=np.uint8, count=C * 32, offset=CKPT_HEAD).reshape(C, 32)
+
+
+def _hamming(a, b):
+    ab = np.unpackbits(a, axis=1).astype(np.int32)
+    bb = np.unpackbits(b, axis=1).astype(np.int32)
+    return ab.sum(1)[:, None] + bb.sum(1)[None, :] - 2 * (ab @ bb.T)
+
+
+def _same_search(ctx, a, b, tq):
+    ra, rb = a.search(tq), b.search(tq)
+    ctx.sync()
+    for x, y in zip(ra, rb):
+        assert torch.equal(x, y)
+
+
+def test_checkpoint_round_trip(ctx, small_index):
+    """save -> load over the same database: identical lists, weights and search."""
+    idx, db, q, tdb, tq = small_index
+    blob = idx.save()
+    p = orbx.LearnedParams.from_buffer_copy(idx.params)
+    assert len(blob) == CKPT_HEAD + 256 * 32 + 512 * 256 * 2 + 512 * 4 + 256 * 512 * 2 + 256 * 4 + 8
+    re = orbx.LearnedIndex.load(ctx, blob, tdb)
+    try:
+        for f in ("proposal", "n_clusters", "hidden", "n_probe", "spill", "seed", "max_distance", "lr", "margin"):
+            assert getattr(re.params, f) == getattr(p, f), f
+        st, rst = idx.stats(), re.stats()
+        assert rst["loss"] == st["loss"] and rst["largest_cluster"] == st["largest_cluster"]
+        a, b = idx.export(), re.export()
+        for k in a:
+            assert np.array_equal(a[k], b[k]), k
+        _same_search(ctx, idx, re, tq)
+        # with a margin threshold part of the queries go to exact search in both
+        for m in (1.0, 3.0e38):
+            idx.set_margin(m)
+            re.set_margin(m)
+            _same_search(ctx, idx, re, tq)
+        # saving the loaded index gives the same checkpoint apart from its build times
+        re.set_margin(p.margin)
+        blob2 = re.save()
+        bt = 16 + 4 * (18 + 4 + 64 + 64)
+        assert len(blob2) == len(blob) and blob2[:bt] == blob[:bt] and blob2[bt + 16:-8] == blob[bt + 16:-8]
+    finally:
+        idx.set_margin(0.0)
+        re.close()
+
+
+def test_checkpoint_over_new_database(ctx, small_index):
+    """load over another database lists each row under its two nearest saved
+    centroids (exact Hamming, ties to the smaller index) and searches it."""
+    idx, *_ = small_index
+    blob = idx.save()
+    cent = _ckpt_centroids(blob, 256)
+    db2, q2 = clustered(12000, 2048, seed=7)
+    tdb2, tq2 = torch.from_numpy(db2).cuda(), torch.from_numpy(q2).cuda()
+    re = orbx.LearnedIndex.load(ctx, blob, tdb2)
+    try:
+        ex = re.export(weights=False)
+        d = _hamming(db2, cent).astype(np.int64)
+        order = np.argsort(d * 256 + np.arange(256)[None, :], axis=1)
+        assert np.array_equal(ex["assign"], order[:, 0])
+        counts = np.bincount(order[:, 0], minlength=256) + np.bincount(order[:, 1], minlength=256)
+        assert np.array_equal(np.diff(ex["offsets"]), counts)
+        assert re.stats()["largest_cluster"] == counts.max()
+        dd, ii, _, fb = re.search(tq2)
+        ctx.sync()
+        assert int(fb.item()) == 0
+        _check_consistent(q2, db2, dd, ii)
+        re.set_margin(3.0e38)
+        dd, ii, _, fb = re.search(tq2)
+        ed, ei = orbx.knn2(ctx, tq2, tdb2, orbx.MATCH_IMMA)
+        ctx.sync()
+        assert int(fb.item()) == len(q2) and torch.equal(dd, ed) and torch.equal(ii, ei)
+    finally:
+        re.close()
+
+
+def test_checkpoint_lsh(ctx, small_index):
+    _, db, q, tdb, tq = small_index
+    p = orbx.learned_params(proposal=orbx.PROPOSAL_LSH, lsh_bits=8, n_clusters=256)
+    lsh = orbx.LearnedIndex(ctx, tdb, None, p)
+    try:
+        blob = lsh.save()
+        assert len(blob) == CKPT_HEAD + 256 * 256 * 2 + 8
+        re = orbx.LearnedIndex.load(ctx, blob, tdb)
+        try:
+            a, b = lsh.export(), re.export()
+            assert np.array_equal(a["assign"], b["assign"]) and np.array_equal(a["offsets"], b["offsets"])
+            _same_search(ctx, lsh, re, tq)
+        finally:
+            re.close()
+    finally:
+        lsh.close()
+
+
+def test_checkpoint_rejects_damaged_bytes(ctx, small_index):
+    idx, db, q, tdb, tq = small_index
+    blob = bytearray(idx.save())
+    cases = {"truncated": bytes(blob[:-1]), "empty": b"\0" * 8}
+    for name, off in (("magic", 0), ("version", 8), ("size", 12), ("params", 20), ("weights", CKPT_HEAD + 9000),
+                      ("hash", len(blob) - 1)):
+        bad = bytearray(blob)
+        bad[off] ^= 0x10
+        cases[name] = bytes(bad)
+    for name, bad in cases.items():
+        with pytest.raises(orbx.OrbxError) as e:
+            orbx.LearnedIndex.load(ctx, bad, tdb)
+        assert e.value.status == orbx.ORBX_ERR_ARG, name
+    with pytest.raises(orbx.OrbxError):
+        orbx.LearnedIndex.load(ctx, bytes(blob), tdb[:0])
