@@ -128,6 +128,26 @@ int imma_rows_db(int n);
 int imma_default_splits(int nq_cap);
 cudaError_t launch_match_imma(const ImmaLaunch& L, cudaStream_t s);
 
+// Probe rerank of the learned proposal on the int8 tensor cores
+// (orbx_match_imma.cu): per (cluster, up to 128 probing slots), the exact top-2
+// keys of each slot over the cluster's rows, one pair per 64-column group.
+constexpr int kRrGroups = 4;
+struct RerankImmaArgs {
+  const uint8_t* q_bits;     // [nq][32] queries
+  const int* list;           // probing slots grouped by cluster (slot = query * 8 + probe)
+  const int* probe_offsets;  // [C + 1] each cluster's first slot in list
+  const int* item_offsets;   // [C + 1] exclusive scan of ceil(slots / 128)
+  int n_clusters;
+  const int* ivf_offsets;    // [C + 1] list offsets: the cluster's row count
+  const int* pad_offsets;    // [C + 1] the cluster's first padded row (multiples of 256)
+  const int* pad_members;    // [pad_rows] database index of each padded row, -1 in the padding
+  uint2* partial;            // [slots][kRrGroups] top-2 keys
+  int* err;
+};
+// pad_pm1: [pad_rows][256] +-1 rows of the padded lists (padding rows zero)
+cudaError_t launch_rerank_imma(const RerankImmaArgs& a, const int8_t* pad_pm1, int pad_rows, int max_items,
+                               cudaStream_t s);
+
 // Top-2 keys shared by both matcher forms: key = distance << 22 | index, so
 // ordering keys orders by (distance, index); 0xFFFFFFFF means "none".
 constexpr int kIdxBitsShared = 22;

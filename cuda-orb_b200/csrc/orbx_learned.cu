@@ -431,12 +431,13 @@ __global__ void k_labels(const int32_t* __restrict__ idx2, int n, const int* __r
 // One warp per query: merge the GEMM's top-8 key lists (one per 128 columns,
 // lists * 8 keys) into the query's n_probe best clusters.  margin = logit1 - logit2.  A query
 // whose margin is below margin_thr probes nothing (the exact fallback answers
-// it); otherwise its non-empty probed clusters are counted.  Every partial slot
-// starts empty.
+// it); otherwise its non-empty probed clusters are counted.  Every partial entry
+// (per_slot per probe slot, per_slot <= 4) starts empty.
 __global__ void __launch_bounds__(256) k_select_probes(const uint32_t* __restrict__ keys, int nq, int lists,
                                                        int n_probe, float margin_thr, const int* __restrict__ ivf_offsets,
                                                        int* __restrict__ probes, float* __restrict__ margin,
-                                                       int* __restrict__ probe_counts, uint2* __restrict__ partial) {
+                                                       int* __restrict__ probe_counts, uint2* __restrict__ partial,
+                                                       int per_slot) {
   const int q = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
   if (q >= nq) return;
@@ -472,7 +473,7 @@ __global__ void __launch_bounds__(256) k_select_probes(const uint32_t* __restric
   const float l2 = order_bits_float(best[1] & ~((1u << kTopColBits) - 1u));
   const float mg = l1 - l2;
   const bool fb = mg < margin_thr;  // answered by the exact fallback: nothing to probe
-  if (lane < kTopK) partial[(size_t)q * kTopK + lane] = make_uint2(kNoKeyShared, kNoKeyShared);
+  if (lane < kTopK * per_slot) partial[(size_t)q * kTopK * per_slot + lane] = make_uint2(kNoKeyShared, kNoKeyShared);
   if (lane == 0) margin[q] = mg;
   if (lane < kTopK) {
     int c = -1;
@@ -549,18 +550,18 @@ __global__ void __launch_bounds__(kRerankQ) k_rerank(const uint8_t* __restrict__
   if (active) partial[slot] = make_uint2(k1, k2);
 }
 
-// Per query: top-2 over its probe slots (a database row listed in two probed
-// clusters is counted once).  Queries with margin < margin_thr or a best
+// Per query: top-2 over its probe slots' partial pairs (per_slot pairs per
+// slot; a database row listed in two probed clusters is counted once).  Queries with margin < margin_thr or a best
 // distance above max_dist go to the fallback list; the others get their result.
-__global__ void k_merge_probes(const uint2* __restrict__ partial, int nq, const float* __restrict__ margin,
+__global__ void k_merge_probes(const uint2* __restrict__ partial, int per_slot, int nq, const float* __restrict__ margin,
                                float margin_thr, int max_dist, uint32_t* __restrict__ dist2,
                                int32_t* __restrict__ idx2, int* __restrict__ fb_list, int* __restrict__ fb_count) {
   const int q = blockIdx.x * blockDim.x + threadIdx.x;
   if (q >= nq) return;
   uint32_t k1 = kNoKeyShared, k2 = kNoKeyShared;
-#pragma unroll
-  for (int s = 0; s < kTopK; s++) {
-    const uint2 p = partial[(size_t)q * kTopK + s];
+  const int n = kTopK * per_slot;
+  for (int s = 0; s < n; s++) {
+    const uint2 p = partial[(size_t)q * n + s];
     if (p.x != k1 && p.x != k2) top2_push_shared(k1, k2, p.x);
     if (p.y != k1 && p.y != k2) top2_push_shared(k1, k2, p.y);
   }
@@ -598,13 +599,47 @@ __global__ void k_scatter_fallback(const int* __restrict__ fb_list, const int* _
   idx2[2 * q + 1] = fi[2 * j + 1];
 }
 
+// ---------------------------------------------------------------- padded lists
+// Rows per cluster rounded up to the tensor-core rerank's 256-row tile.
+__global__ void k_pad_counts(const int* __restrict__ ivf_offsets, int C, int* __restrict__ pad_counts) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c < C) pad_counts[c] = (ivf_offsets[c + 1] - ivf_offsets[c] + 255) / 256 * 256;
+}
+
+// Cluster c's padded rows [pad_offsets[c], pad_offsets[c + 1]): its list's
+// database rows as +-1 bytes (bit j of packed byte i -> byte 8 i + j, as the
+// int8 matcher expands them) with their database index, then zero rows with
+// index -1.  One block per cluster.
+__global__ void __launch_bounds__(256) k_fill_pad(const uint8_t* __restrict__ db, const int* __restrict__ ivf_members,
+                                                  const int* __restrict__ ivf_offsets,
+                                                  const int* __restrict__ pad_offsets, int8_t* __restrict__ pad_pm1,
+                                                  int* __restrict__ pad_members) {
+  __shared__ unsigned long long lut[256];
+  for (int i = threadIdx.x; i < 256; i += blockDim.x) {
+    unsigned long long v = 0;
+    for (int j = 0; j < 8; j++) v |= (unsigned long long)(((i >> j) & 1) ? 0x01u : 0xFFu) << (8 * j);
+    lut[i] = v;
+  }
+  __syncthreads();
+  const int c = blockIdx.x;
+  const int m0 = ivf_offsets[c], n = ivf_offsets[c + 1] - m0;
+  const int p0 = pad_offsets[c], np = pad_offsets[c + 1] - p0;
+  unsigned long long* out = reinterpret_cast<unsigned long long*>(pad_pm1) + (size_t)p0 * 32;
+  for (long long i = threadIdx.x; i < (long long)np * 32; i += blockDim.x) {
+    const int r = (int)(i >> 5);
+    out[i] = r < n ? lut[db[(size_t)ivf_members[m0 + r] * 32 + (i & 31)]] : 0ull;
+  }
+  for (int r = threadIdx.x; r < np; r += blockDim.x) pad_members[p0 + r] = r < n ? ivf_members[m0 + r] : -1;
+}
+
 // ---------------------------------------------------------------- LSH ablation
 // Random-projection buckets: bucket = sign bits of the first nbits projections.
 // Probes: the own bucket, then single-bit flips of the least confident bits
 // (smallest |projection|), in that order.
 __global__ void k_lsh_probes(const float* __restrict__ proj, int rows_stride, int n, int nbits, int n_probe,
                              const int* __restrict__ ivf_offsets, int* __restrict__ probes, int* __restrict__ probe_counts,
-                             int* __restrict__ bucket_out, float* __restrict__ margin, uint2* __restrict__ partial) {
+                             int* __restrict__ bucket_out, float* __restrict__ margin, uint2* __restrict__ partial,
+                             int per_slot) {
   const int q = blockIdx.x * blockDim.x + threadIdx.x;
   if (q >= n) return;
   const float* p = proj + (size_t)q * rows_stride;
@@ -628,8 +663,8 @@ __global__ void k_lsh_probes(const float* __restrict__ proj, int rows_stride, in
         order[j] = t;
       }
   margin[q] = 3.0e38f;
+  for (int s = 0; s < kTopK * per_slot; s++) partial[(size_t)q * kTopK * per_slot + s] = make_uint2(kNoKeyShared, kNoKeyShared);
   for (int s = 0; s < kTopK; s++) {
-    partial[(size_t)q * kTopK + s] = make_uint2(kNoKeyShared, kNoKeyShared);
     int c = -1;
     if (s < n_probe) c = s == 0 ? b : (b ^ (1 << order[s - 1]));
     if (c >= 0 && ivf_offsets[c + 1] == ivf_offsets[c]) c = -1;

@@ -92,13 +92,16 @@ __global__ void k_accum_stats(const float* loss, const int* correct, int n, floa
 __global__ void k_labels(const int32_t* idx2, int n, const int* assign, int* labels);
 __global__ void k_select_probes(const uint32_t* keys, int nq, int lists, int n_probe, float margin_thr,
                                 const int* ivf_offsets, int* probes, float* margin, int* probe_counts,
-                                uint2* partial);
+                                uint2* partial, int per_slot);
 __global__ void k_fill_probe_lists(const int* probes, int nq, int* cursor, int* list);
 __global__ void k_rerank(const uint8_t* q_desc, const int* list, const int* probe_offsets, const int* item_offsets,
                          int n_clusters, const uint8_t* ivf_desc, const int* ivf_members, const int* ivf_offsets,
                          uint2* partial);
-__global__ void k_merge_probes(const uint2* partial, int nq, const float* margin, float margin_thr, int max_dist,
-                               uint32_t* dist2, int32_t* idx2, int* fb_list, int* fb_count);
+__global__ void k_merge_probes(const uint2* partial, int per_slot, int nq, const float* margin, float margin_thr,
+                               int max_dist, uint32_t* dist2, int32_t* idx2, int* fb_list, int* fb_count);
+__global__ void k_pad_counts(const int* ivf_offsets, int C, int* pad_counts);
+__global__ void k_fill_pad(const uint8_t* db, const int* ivf_members, const int* ivf_offsets, const int* pad_offsets,
+                           int8_t* pad_pm1, int* pad_members);
 __global__ void k_init_centroid_mlp(const uint8_t* centroids, int C, int Hd, float scale, float* w1, float* b1,
                                     float* w2, float* b2, __nv_bfloat16* w1b, __nv_bfloat16* w2b);
 __global__ void k_perturb_rows(const uint8_t* db, int ndb, int n, unsigned long long seed, float flip_lo,
@@ -109,7 +112,8 @@ __global__ void k_gather_fallback(const uint8_t* q_desc, const int* fb_list, con
 __global__ void k_scatter_fallback(const int* fb_list, const int* fb_count, const uint32_t* fd, const int32_t* fi,
                                    uint32_t* dist2, int32_t* idx2);
 __global__ void k_lsh_probes(const float* proj, int rows_stride, int n, int nbits, int n_probe, const int* ivf_offsets,
-                             int* probes, int* probe_counts, int* bucket_out, float* margin, uint2* partial);
+                             int* probes, int* probe_counts, int* bucket_out, float* margin, uint2* partial,
+                             int per_slot);
 constexpr int kRerankQ = 128;
 
 }  // namespace orbx

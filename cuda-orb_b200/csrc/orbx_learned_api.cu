@@ -24,6 +24,7 @@
 
 using namespace orbx;
 typedef __nv_bfloat16 bf16;
+static_assert(kRerankQ == 128, "the tensor-core rerank takes 128 probing slots per item");
 
 namespace {
 
@@ -175,6 +176,11 @@ struct orbx_learned {
   int* ivf_offsets = nullptr;
   int* ivf_members = nullptr;
   uint8_t* ivf_desc = nullptr;
+  // the lists padded per cluster to 256-row tiles, for the tensor-core rerank
+  int pad_rows = 0;
+  int* pad_offsets = nullptr;
+  int* pad_members = nullptr;
+  int8_t* pad_pm1 = nullptr;
   float *w1 = nullptr, *b1 = nullptr, *w2 = nullptr, *b2 = nullptr;
   bf16 *w1b = nullptr, *w2b = nullptr, *w2tb = nullptr;
   bf16* lsh = nullptr;  // [256][256] projections, rows >= lsh_bits unused
@@ -254,6 +260,7 @@ int check_params(const orbx_learned_params* p) {
   if (!p) return ORBX_ERR_ARG;
   if (p->proposal != ORBX_PROPOSAL_MLP && p->proposal != ORBX_PROPOSAL_LSH) return ORBX_ERR_ARG;
   if (p->n_probe < 1 || p->n_probe > kTopK) return ORBX_ERR_ARG;
+  if (p->rerank != ORBX_RERANK_TENSOR && p->rerank != ORBX_RERANK_POPC) return ORBX_ERR_ARG;
   if (p->proposal == ORBX_PROPOSAL_LSH) {
     if (p->lsh_bits < 8 || p->lsh_bits > 12 || p->n_clusters != (1 << p->lsh_bits)) return ORBX_ERR_ARG;
   } else {
@@ -311,6 +318,28 @@ int alloc_core(orbx_learned* L) {
 int upload_db(orbx_learned* L, const uint8_t* d_db, cudaStream_t s) {
   LCHK(cudaMemcpyAsync(L->db, d_db, (size_t)L->ndb * 32, cudaMemcpyDeviceToDevice, s));
   LCHK(launch_expand_pm1(L->db, L->ndb, nullptr, imma_rows_db(L->ndb), L->db_pm1, s));
+  return ORBX_OK;
+}
+
+// The padded lists of the tensor-core rerank, once the lists are built:
+// offsets, database indices and +-1 rows.  Synchronises the stream.
+int build_padded(orbx_learned* L, cudaStream_t s) {
+  const int C = L->C;
+  Arena t;
+  int *counts, *cursor;
+  LCHK(t.alloc(&counts, C));
+  LCHK(t.alloc(&cursor, C));
+  if (!L->pad_offsets) LCHK(L->keep.alloc(&L->pad_offsets, (size_t)C + 1));
+  k_pad_counts<<<grid1(C, 256), 256, 0, s>>>(L->ivf_offsets, C, counts);
+  k_scan_counts<<<1, 1024, 0, s>>>(counts, C, L->pad_offsets, cursor, 0, nullptr);
+  int rows = 0;
+  LCHK(cudaMemcpyAsync(&rows, L->pad_offsets + C, sizeof(int), cudaMemcpyDeviceToHost, s));
+  LCHK(cudaStreamSynchronize(s));
+  L->pad_rows = rows;
+  LCHK(L->keep.alloc(&L->pad_members, (size_t)std::max(rows, 1)));
+  LCHK(L->keep.alloc(&L->pad_pm1, (size_t)std::max(rows, 1) * 256));
+  k_fill_pad<<<C, 256, 0, s>>>(L->db, L->ivf_members, L->ivf_offsets, L->pad_offsets, L->pad_pm1, L->pad_members);
+  LCHK(cudaGetLastError());
   return ORBX_OK;
 }
 
@@ -418,7 +447,7 @@ int cluster_lsh(orbx_learned* L, cudaStream_t s, int* err, bool make_proj) {
     k_bits_pm1_bf16<<<grid1((long long)rows * 32, 256), 256, 0, s>>>(L->db + (size_t)off * 32, m, nullptr, rows, x);
     LCHK(gemm(s, err, x, L->lsh, rows, 256, 256, nullptr, kStoreF32, 1, proj, nullptr, nullptr, nullptr));
     k_lsh_probes<<<grid1(m, 128), 128, 0, s>>>(proj, 256, m, L->p.lsh_bits, 0, nullptr, nullptr, nullptr,
-                                               L->assign + off, nullptr, nullptr);
+                                               L->assign + off, nullptr, nullptr, 1);
   }
   LCHK(cudaMemsetAsync(counts, 0, sizeof(int) * C, s));
   k_count<<<grid1(n, 256), 256, 0, s>>>(L->assign, n, counts);
@@ -547,7 +576,7 @@ int ensure_search(orbx_learned* L, int nq) {
   LCHK(a.alloc(&L->cursor, (size_t)C));
   LCHK(a.alloc(&L->items, (size_t)C + 1));
   LCHK(a.alloc(&L->list, (size_t)nq * kTopK));
-  LCHK(a.alloc(&L->partial, (size_t)nq * kTopK));
+  LCHK(a.alloc(&L->partial, (size_t)nq * kTopK * kRrGroups));
   LCHK(a.alloc(&L->fb_list, (size_t)nq));
   LCHK(a.alloc(&L->fb_count, 1));
   LCHK(a.alloc(&L->fb_q, (size_t)nq * 32));
@@ -583,6 +612,7 @@ ORBX_API int orbx_learned_default_params(orbx_learned_params* p) {
   p->synth_train = 0;
   p->flip_lo = 0.05f;
   p->flip_hi = 0.2f;
+  p->rerank = ORBX_RERANK_TENSOR;
   return ORBX_OK;
 }
 
@@ -623,6 +653,8 @@ ORBX_API int orbx_learned_build(orbx_ctx* ctx, const orbx_learned_params* p, con
     rc = p->proposal == ORBX_PROPOSAL_MLP ? cluster_kmeans(L, s, err) : cluster_lsh(L, s, err, true);
     if (rc) break;
     k_gather_rows<<<grid1(2ll * L->n_entries, 256), 256, 0, s>>>(L->db, L->ivf_members, L->n_entries, L->ivf_desc);
+    rc = build_padded(L, s);
+    if (rc) break;
     cudaEventRecord(ev[1], s);
     if (p->proposal == ORBX_PROPOSAL_MLP) {
       Arena t;
@@ -699,6 +731,8 @@ static int search_impl(orbx_ctx* ctx, orbx_learned* L, const uint8_t* d_q, int n
   const int rows = round_up(nq, 128), C = L->C;
   const bool mlp = L->p.proposal == ORBX_PROPOSAL_MLP;
   const float thr = mlp ? L->p.margin : -3.0e38f;
+  const bool tensor = L->p.rerank == ORBX_RERANK_TENSOR && L->pad_rows > 0;
+  const int per_slot = tensor ? kRrGroups : 1;
   auto mark = [&](int i) {
     if (ev) cudaEventRecord(ev[i], s);
   };
@@ -711,21 +745,36 @@ static int search_impl(orbx_ctx* ctx, orbx_learned* L, const uint8_t* d_q, int n
     LCHK(gemm(s, err, L->hq, L->w2b, rows, C, L->Hd, L->b2, kTop8, 1, nullptr, nullptr, nullptr, L->keys));
     k_select_probes<<<grid1((long long)nq * 32, 256), 256, 0, s>>>(L->keys, nq, C / 128, L->p.n_probe, thr,
                                                                     L->ivf_offsets, L->probes, L->margin, L->counts,
-                                                                    L->partial);
+                                                                    L->partial, per_slot);
   } else {
     LCHK(gemm(s, err, L->xq, L->lsh, rows, 256, 256, nullptr, kStoreF32, 1, L->proj, nullptr, nullptr, nullptr));
     k_lsh_probes<<<grid1(nq, 128), 128, 0, s>>>(L->proj, 256, nq, L->p.lsh_bits, L->p.n_probe, L->ivf_offsets,
-                                                L->probes, L->counts, nullptr, L->margin, L->partial);
+                                                L->probes, L->counts, nullptr, L->margin, L->partial, per_slot);
   }
   mark(1);
   k_scan_counts<<<1, 1024, 0, s>>>(L->counts, C, L->offsets, L->cursor, kRerankQ, L->items);
   k_fill_probe_lists<<<grid1((long long)nq * kTopK, 256), 256, 0, s>>>(L->probes, nq, L->cursor, L->list);
   mark(2);
   const unsigned items_max = grid1((long long)nq * kTopK, kRerankQ) + (unsigned)C;
-  k_rerank<<<items_max, kRerankQ, 0, s>>>(d_q, L->list, L->offsets, L->items, C, L->ivf_desc, L->ivf_members,
-                                          L->ivf_offsets, L->partial);
+  if (tensor) {
+    RerankImmaArgs ra{};
+    ra.q_bits = d_q;
+    ra.list = L->list;
+    ra.probe_offsets = L->offsets;
+    ra.item_offsets = L->items;
+    ra.n_clusters = C;
+    ra.ivf_offsets = L->ivf_offsets;
+    ra.pad_offsets = L->pad_offsets;
+    ra.pad_members = L->pad_members;
+    ra.partial = L->partial;
+    ra.err = err;
+    LCHK(launch_rerank_imma(ra, L->pad_pm1, L->pad_rows, (int)items_max, s));
+  } else {
+    k_rerank<<<items_max, kRerankQ, 0, s>>>(d_q, L->list, L->offsets, L->items, C, L->ivf_desc, L->ivf_members,
+                                            L->ivf_offsets, L->partial);
+  }
   mark(3);
-  k_merge_probes<<<grid1(nq, 256), 256, 0, s>>>(L->partial, nq, L->margin, thr, mlp ? L->p.max_distance : 1 << 20,
+  k_merge_probes<<<grid1(nq, 256), 256, 0, s>>>(L->partial, per_slot, nq, L->margin, thr, mlp ? L->p.max_distance : 1 << 20,
                                                  d_dist2, d_idx2, mlp ? L->fb_list : nullptr, L->fb_count);
   mark(4);
   LCHK(cudaGetLastError());
@@ -771,6 +820,12 @@ ORBX_API int orbx_learned_profile_search(orbx_ctx* ctx, orbx_learned* L, const u
 ORBX_API int orbx_learned_set_margin(orbx_learned* L, float margin) {
   if (!L) return ORBX_ERR_ARG;
   L->p.margin = margin;
+  return ORBX_OK;
+}
+
+ORBX_API int orbx_learned_set_rerank(orbx_learned* L, int form) {
+  if (!L || (form != ORBX_RERANK_TENSOR && form != ORBX_RERANK_POPC)) return ORBX_ERR_ARG;
+  L->p.rerank = form;
   return ORBX_OK;
 }
 
@@ -821,7 +876,7 @@ ORBX_API int orbx_learned_export(orbx_ctx* ctx, const orbx_learned* L, int* h_as
 // A saved proposal, little-endian, every field 4-byte aligned:
 //   "ORBXLRN1", u32 version, u32 total bytes
 //   the orbx_learned_params fields in declaration order (seed as two u32, low
-//   word first), then the orbx_learned_stats words
+//   word first, rerank last), then the orbx_learned_stats words
 //   MLP: centroids [C][32] u8, W1 [Hd][256] bf16, b1 [Hd] f32, W2 [C][Hd] bf16,
 //        b2 [C] f32 (the weights search uses)
 //   LSH: projections [256][256] bf16
@@ -831,8 +886,8 @@ ORBX_API int orbx_learned_export(orbx_ctx* ctx, const orbx_learned* L, int* h_as
 namespace {
 
 constexpr char kSaveMagic[8] = {'O', 'R', 'B', 'X', 'L', 'R', 'N', '1'};
-constexpr uint32_t kSaveVersion = 1;
-constexpr size_t kSaveParamWords = 18;
+constexpr uint32_t kSaveVersion = 2;
+constexpr size_t kSaveParamWords = 19;
 constexpr size_t kSaveStatsWords = sizeof(orbx_learned_stats) / 4;
 static_assert(sizeof(orbx_learned_stats) == 4 * (4 + 64 + 64 + 4), "stats are whole 4-byte words");
 
@@ -877,7 +932,7 @@ void put_params(uint8_t*& w, const orbx_learned_params& p) {
                                        (uint32_t)p.batch, fbits(p.lr), fbits(p.margin), (uint32_t)p.lsh_bits,
                                        (uint32_t)p.seed, (uint32_t)(p.seed >> 32), (uint32_t)p.max_distance,
                                        (uint32_t)p.spill, (uint32_t)p.init, (uint32_t)p.synth_train,
-                                       fbits(p.flip_lo), fbits(p.flip_hi)};
+                                       fbits(p.flip_lo), fbits(p.flip_hi), (uint32_t)p.rerank};
   for (uint32_t x : v) put32(w, x);
 }
 orbx_learned_params get_params(const uint8_t*& r) {
@@ -901,6 +956,7 @@ orbx_learned_params get_params(const uint8_t*& r) {
   p.synth_train = (int)v[15];
   p.flip_lo = bitsf(v[16]);
   p.flip_hi = bitsf(v[17]);
+  p.rerank = (int)v[18];
   return p;
 }
 
@@ -1018,6 +1074,8 @@ ORBX_API int orbx_learned_load(orbx_ctx* ctx, const void* h_buf, size_t bytes, c
     }
     if (rc) break;
     k_gather_rows<<<grid1(2ll * L->n_entries, 256), 256, 0, s>>>(L->db, L->ivf_members, L->n_entries, L->ivf_desc);
+    rc = build_padded(L, s);
+    if (rc) break;
     cudaEventRecord(ev[1], s);
     if (cudaStreamSynchronize(s) != cudaSuccess || cudaGetLastError() != cudaSuccess) {
       rc = ORBX_ERR_CUDA;

@@ -416,6 +416,330 @@ __global__ void __launch_bounds__(kIThreads, 1)
 }
 
 // ---------------------------------------------------------------------------
+// Probe rerank of the learned proposal on the tensor cores
+//
+// A work item is one cluster c with up to 128 of the query slots that probe it
+// (list[probe_offsets[c] ..], grouped by cluster; slot = query * 8 + probe).
+// The block is persistent and walks items blockIdx.x, + gridDim.x, ...:
+//   warp 0      TMA producer: the cluster's +-1 rows, padded per cluster to
+//               256-row tiles, through a 2-stage ring;
+//   warp 1      MMA issuer, as in k_match_imma, into two 256-column
+//               accumulators; commits release the ring stage, the
+//               accumulator and, after an item's last tile, its query tile;
+//   warps 2-5   query gather: thread r expands slot r's 32 query bytes to a
+//               +-1 row in the 128-byte swizzled K-major layout the TMA writes,
+//               into one of two query tiles;
+//   warps 6-21  epilogue: warp w reads TMEM lanes 32 * (w % 4) and 64 columns,
+//               keeps the top-2 keys (distance << 22 | database index) of each
+//               slot over the item's tiles and writes them to
+//               partial[slot * 4 + column group].
+// Keys carry the database index itself, so ties resolve by index whatever the
+// order of a cluster's list.  Every wait is bounded (kIDeadlineCycles per
+// wait); on expiry the block records kErrImmaTimeout, drains its copies and
+// exits.
+// ---------------------------------------------------------------------------
+constexpr int kRrGatherWarps = 4;
+constexpr int kRrThreads = (2 + kRrGatherWarps + kIEpiWarps) * 32;
+constexpr uint32_t kRrBStages = 2;
+constexpr uint32_t kRrNumBars = 12;  // A full/empty, B full/empty, accumulator full/empty, two each
+constexpr uint32_t kRrSmemBytes = 1024 + 2 * kIATile + kRrBStages * kIBTile + 256 * 8 + 8 * kRrNumBars + 16;
+static_assert(kRrSmemBytes + 16 <= 232448, "exceeds the 227 KB shared-memory opt-in");
+
+struct RrItem {
+  int c;      // cluster
+  int e0;     // first slot in list
+  int rows;   // slots in this item (1..128)
+  int nrow;   // the cluster's database rows
+  int pbase;  // first padded row of the cluster
+  int tiles;  // 256-row tiles
+};
+
+__device__ __forceinline__ RrItem rr_item(const RerankImmaArgs& a, int it) {
+  int lo = 0, hi = a.n_clusters;
+  while (hi - lo > 1) {
+    const int mid = (lo + hi) >> 1;
+    if (__ldg(a.item_offsets + mid) <= it) lo = mid;
+    else hi = mid;
+  }
+  RrItem r;
+  r.c = lo;
+  r.e0 = __ldg(a.probe_offsets + lo) + (it - __ldg(a.item_offsets + lo)) * kIBM;
+  r.rows = min(kIBM, __ldg(a.probe_offsets + lo + 1) - r.e0);
+  r.nrow = __ldg(a.ivf_offsets + lo + 1) - __ldg(a.ivf_offsets + lo);
+  r.pbase = __ldg(a.pad_offsets + lo);
+  r.tiles = (r.nrow + kIBN - 1) / kIBN;
+  return r;
+}
+
+// Bounded wait with a fresh deadline: false on expiry or when another role aborted.
+__device__ __forceinline__ bool rr_wait(uint32_t bar, uint32_t parity, volatile int* abort_flag) {
+  return mbar_wait(bar, parity, clock64() + kIDeadlineCycles, abort_flag);
+}
+__device__ __forceinline__ bool rr_warp_wait(uint32_t bar, uint32_t parity, volatile int* abort_flag) {
+  int ok = 0;
+  if ((threadIdx.x & 31) == 0) ok = rr_wait(bar, parity, abort_flag) ? 1 : 0;
+  return __shfl_sync(0xffffffffu, ok, 0) != 0;
+}
+
+__global__ void __launch_bounds__(kRrThreads, 1)
+    k_rerank_imma(const __grid_constant__ CUtensorMap tmD, RerankImmaArgs a) {
+  extern __shared__ uint8_t smem_raw[];
+  const uint32_t raw = smem_u32(smem_raw);
+  uint8_t* smem = smem_raw + ((1024u - (raw & 1023u)) & 1023u);
+  uint8_t* sA = smem;                     // two query tiles
+  uint8_t* sB = sA + 2 * kIATile;         // ring of database tiles
+  unsigned long long* s_lut = reinterpret_cast<unsigned long long*>(sB + kRrBStages * kIBTile);
+  uint64_t* bars = reinterpret_cast<uint64_t*>(s_lut + 256);
+  uint32_t* s_tmem = reinterpret_cast<uint32_t*>(bars + kRrNumBars);
+  volatile int* s_abort = reinterpret_cast<volatile int*>(s_tmem + 1);
+
+  const int n_items = __ldg(a.item_offsets + a.n_clusters);
+  const int warp = threadIdx.x >> 5;
+  const int lane = threadIdx.x & 31;
+  const uint32_t bar0 = smem_u32(bars);
+#define RR_AFULL(b) (bar0 + 8u * (b))
+#define RR_AEMPTY(b) (bar0 + 8u * (2 + (b)))
+#define RR_BFULL(s) (bar0 + 8u * (4 + (s)))
+#define RR_BEMPTY(s) (bar0 + 8u * (6 + (s)))
+#define RR_ACCFULL(x) (bar0 + 8u * (8 + (x)))
+#define RR_ACCEMPTY(x) (bar0 + 8u * (10 + (x)))
+
+  for (int i = threadIdx.x; i < 256; i += blockDim.x) {
+    unsigned long long v = 0;
+    for (int j = 0; j < 8; j++) v |= (unsigned long long)(((i >> j) & 1) ? 0x01u : 0xFFu) << (8 * j);
+    s_lut[i] = v;
+  }
+  if (threadIdx.x == 0) {
+    for (int b = 0; b < 2; b++) {
+      mbar_init(RR_AFULL(b), kRrGatherWarps);
+      mbar_init(RR_AEMPTY(b), 1);
+      mbar_init(RR_BFULL(b), 1);
+      mbar_init(RR_BEMPTY(b), 1);
+      mbar_init(RR_ACCFULL(b), 1);
+      mbar_init(RR_ACCEMPTY(b), kIEpiWarps);
+    }
+    *s_abort = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  }
+  if (warp == 1) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(s_tmem)),
+                 "r"(kITmemCols)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem_base = *s_tmem;
+
+  if (warp == 0) {
+    if (lane == 0) {
+      // TMA producer: every tile of every item of this block, in order
+      uint32_t issued[kRrBStages] = {0u, 0u};
+      uint32_t g = 0;
+      bool ok = true;
+      for (int it = blockIdx.x; ok && it < n_items; it += gridDim.x) {
+        const RrItem r = rr_item(a, it);
+        for (int t = 0; t < r.tiles; t++, g++) {
+          const uint32_t s = g & 1u;
+          if (g >= 2 && !rr_wait(RR_BEMPTY(s), ((g >> 1) - 1) & 1u, s_abort)) {
+            ok = false;
+            break;
+          }
+          const int row = r.pbase + t * kIBN;
+          mbar_expect_tx(RR_BFULL(s), kIBTile);
+          tma_load_2d(smem_u32(sB + s * kIBTile), &tmD, 0, row, RR_BFULL(s));
+          tma_load_2d(smem_u32(sB + s * kIBTile + kIHalfB), &tmD, 128, row, RR_BFULL(s));
+          issued[s]++;
+        }
+      }
+      if (!ok) {
+        *s_abort = 1;
+        atomicOr(a.err, kErrImmaTimeout);
+      }
+      // drain: every issued copy landed and the MMAs that read it completed
+      for (uint32_t s = 0; s < kRrBStages; s++) {
+        if (issued[s] == 0) continue;
+        const uint32_t par = (issued[s] - 1) & 1u;
+        long long dl = clock64() + kIDeadlineCycles;
+        while (!mbar_try(RR_BFULL(s), par) && clock64() < dl) {
+        }
+        dl = clock64() + kIDeadlineCycles;
+        while (!mbar_try(RR_BEMPTY(s), par) && clock64() < dl) {
+        }
+      }
+    }
+  } else if (warp == 1) {
+    if (lane == 0) {
+      // MMA issuer
+      uint32_t g = 0, na = 0;
+      bool ok = true;
+      for (int it = blockIdx.x; ok && it < n_items; it += gridDim.x) {
+        const RrItem r = rr_item(a, it);
+        if (r.tiles == 0) continue;
+        const uint32_t b = na & 1u;
+        if (!rr_wait(RR_AFULL(b), (na >> 1) & 1u, s_abort)) {
+          ok = false;
+          break;
+        }
+        const uint32_t a_lo = smem_u32(sA + b * kIATile);
+        for (int t = 0; t < r.tiles; t++, g++) {
+          const uint32_t s = g & 1u, acc = g & 1u;
+          if (!rr_wait(RR_BFULL(s), (g >> 1) & 1u, s_abort) ||
+              (g >= 2 && !rr_wait(RR_ACCEMPTY(acc), ((g >> 1) - 1) & 1u, s_abort))) {
+            ok = false;
+            break;
+          }
+          tc_fence_after();
+          const uint32_t d = tmem_base + acc * (uint32_t)kIBN;
+          const uint32_t b_lo = smem_u32(sB + s * kIBTile);
+#pragma unroll
+          for (int k = 0; k < 8; k++) {
+            const int h = k >> 2, kk = k & 3;
+            const uint64_t da = sw128_desc(a_lo + h * kIHalfA) + (uint64_t)(2 * kk);
+            const uint64_t db = sw128_desc(b_lo + h * kIHalfB) + (uint64_t)(2 * kk);
+            umma_i8(d, da, db, kIDesc, k > 0 ? 1u : 0u);
+          }
+          umma_commit(RR_BEMPTY(s));
+          umma_commit(RR_ACCFULL(acc));
+        }
+        if (!ok) break;
+        umma_commit(RR_AEMPTY(b));
+        na++;
+      }
+      if (!ok) {
+        *s_abort = 1;
+        atomicOr(a.err, kErrImmaTimeout);
+      }
+    }
+  } else if (warp < 2 + kRrGatherWarps) {
+    // query gather: thread r fills row r of the item's query tile
+    const int r = threadIdx.x - 64;
+    uint32_t na = 0;
+    bool ok = true;
+    for (int it = blockIdx.x; it < n_items; it += gridDim.x) {
+      const RrItem ri = rr_item(a, it);
+      if (ri.tiles == 0) continue;
+      const uint32_t b = na & 1u;
+      if (na >= 2 && !rr_warp_wait(RR_AEMPTY(b), ((na >> 1) - 1) & 1u, s_abort)) {
+        ok = false;
+        break;
+      }
+      uint4 w0 = make_uint4(0u, 0u, 0u, 0u), w1 = w0;
+      if (r < ri.rows) {
+        const int q = __ldg(a.list + ri.e0 + r) >> 3;
+        const uint4* src = reinterpret_cast<const uint4*>(a.q_bits) + 2 * (size_t)q;
+        w0 = __ldg(src);
+        w1 = __ldg(src + 1);
+      }
+      const uint32_t wd[8] = {w0.x, w0.y, w0.z, w0.w, w1.x, w1.y, w1.z, w1.w};
+      uint8_t* row = sA + b * kIATile + r * 128;
+#pragma unroll
+      for (int cc = 0; cc < 16; cc++) {
+        // 16-byte chunk cc holds the expansions of packed bytes 2cc and 2cc + 1
+        const uint32_t word = wd[cc >> 1];
+        const int sh = (cc & 1) * 16;
+        uint4 v = make_uint4(0u, 0u, 0u, 0u);
+        if (r < ri.rows) {
+          const unsigned long long lo = s_lut[(word >> sh) & 0xFFu];
+          const unsigned long long hi = s_lut[(word >> (sh + 8)) & 0xFFu];
+          v = make_uint4((uint32_t)lo, (uint32_t)(lo >> 32), (uint32_t)hi, (uint32_t)(hi >> 32));
+        }
+        const int h = cc >> 3, j = cc & 7;
+        *reinterpret_cast<uint4*>(row + h * kIHalfA + ((j ^ (r & 7)) << 4)) = v;
+      }
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+      __syncwarp();
+      if (lane == 0) mbar_arrive(RR_AFULL(b));
+      na++;
+    }
+    if (!ok) {
+      *s_abort = 1;
+      if (lane == 0) atomicOr(a.err, kErrImmaTimeout);
+    }
+  } else {
+    // epilogue
+    const int ew = warp - 2 - kRrGatherWarps;
+    const int quarter = warp & 3;
+    const int colgrp = ew >> 2;
+    uint32_t g = 0;
+    bool ok = true;
+    for (int it = blockIdx.x; ok && it < n_items; it += gridDim.x) {
+      const RrItem ri = rr_item(a, it);
+      uint32_t k1 = kNoKeyShared, k2 = kNoKeyShared;
+      for (int t = 0; t < ri.tiles; t++, g++) {
+        const uint32_t acc = g & 1u;
+        if (!rr_warp_wait(RR_ACCFULL(acc), (g >> 1) & 1u, s_abort)) {
+          ok = false;
+          break;
+        }
+        tc_fence_after();
+        const uint32_t taddr = tmem_base + ((uint32_t)(quarter * 32) << 16) + acc * (uint32_t)kIBN + colgrp * 64;
+        int v[64];
+        tmem_ld32(taddr, v);
+        tmem_ld32(taddr + 32u, v + 32);
+        tmem_wait_ld();
+        tc_fence_before();
+        __syncwarp();
+        if (lane == 0) mbar_arrive(RR_ACCEMPTY(acc));
+        const int col0 = t * kIBN + colgrp * 64;  // first column's row within the cluster
+        const int valid = ri.nrow - col0;
+        if (valid < 64) {
+#pragma unroll
+          for (int j = 0; j < 64; j++)
+            if (j >= valid) v[j] = kMaskedDot;
+        }
+#pragma unroll
+        for (int c = 0; c < 2; c++) {
+          int m = v[32 * c];
+#pragma unroll
+          for (int j = 1; j < 32; j++) m = max(m, v[32 * c + j]);
+          // a column can enter the top two when its distance is at most the
+          // current second best's (an equal distance with a smaller index wins)
+          const int thr = (k2 == kNoKeyShared) ? kMaskedDot + 1 : 256 - 2 * (int)(k2 >> kIdxBitsShared);
+          if (__any_sync(0xffffffffu, m >= thr)) {
+            const int e = col0 + 32 * c + lane;
+            const int mine = __ldg(a.pad_members + ri.pbase + e);
+#pragma unroll
+            for (int j = 0; j < 32; j++) {
+              const int idx = __shfl_sync(0xffffffffu, mine, j);
+              const int dot = v[32 * c + j];
+              if (dot != kMaskedDot)
+                top2_push_shared(k1, k2, ((uint32_t)((256 - dot) >> 1) << kIdxBitsShared) | (uint32_t)idx);
+            }
+          }
+        }
+      }
+      if (!ok) break;
+      const int row = quarter * 32 + lane;
+      if (row < ri.rows) {
+        const int slot = __ldg(a.list + ri.e0 + row);
+        a.partial[(size_t)slot * kRrGroups + colgrp] = make_uint2(k1, k2);
+      }
+    }
+    if (!ok) {
+      *s_abort = 1;
+      if (lane == 0) atomicOr(a.err, kErrImmaTimeout);
+    }
+  }
+#undef RR_AFULL
+#undef RR_AEMPTY
+#undef RR_BFULL
+#undef RR_BEMPTY
+#undef RR_ACCFULL
+#undef RR_ACCEMPTY
+
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  if (warp == 1) {
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem_base), "r"(kITmemCols)
+                 : "memory");
+  }
+}
+
+// ---------------------------------------------------------------------------
 // host side
 // ---------------------------------------------------------------------------
 static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
@@ -491,6 +815,26 @@ cudaError_t launch_match_imma(const ImmaLaunch& L, cudaStream_t s) {
   if (!make_rows_map(&td, L.db_pm1, (uint64_t)dbrows, kIBN)) return cudaErrorInvalidValue;
   const int qtiles = qrows / kIBM;
   k_match_imma<<<qtiles * L.splits, kIThreads, kISmemBytes, s>>>(tq, td, L.args, L.work, L.splits, L.err);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_rerank_imma(const RerankImmaArgs& a, const int8_t* pad_pm1, int pad_rows, int max_items,
+                               cudaStream_t s) {
+  if (max_items <= 0 || pad_rows <= 0) return cudaSuccess;
+  if (pad_rows % kIBN) return cudaErrorInvalidValue;
+  static bool attr_set = false;
+  if (!attr_set) {
+    cudaError_t e = cudaFuncSetAttribute(k_rerank_imma, cudaFuncAttributeMaxDynamicSharedMemorySize, kRrSmemBytes);
+    if (e != cudaSuccess) return e;
+    attr_set = true;
+  }
+  CUtensorMap td;
+  if (!make_rows_map(&td, pad_pm1, (uint64_t)pad_rows, kIBN)) return cudaErrorInvalidValue;
+  int dev = 0, sms = 148;
+  if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
+    return cudaErrorInvalidValue;
+  const int blocks = max_items < sms ? max_items : sms;  // persistent: one block per SM
+  k_rerank_imma<<<blocks, kRrThreads, kRrSmemBytes, s>>>(td, a);
   return cudaGetLastError();
 }
 

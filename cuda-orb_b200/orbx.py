@@ -101,6 +101,7 @@ def lib():
         L.orbx_learned_search.argtypes = [vp, vp, vp, i32, vp, vp, vp, vp]
         L.orbx_learned_set_margin.argtypes = [vp, ctypes.c_float]
         L.orbx_learned_set_max_distance.argtypes = [vp, i32]
+        L.orbx_learned_set_rerank.argtypes = [vp, i32]
         L.orbx_learned_profile_search.argtypes = [vp, vp, vp, i32, vp, vp, vp]
         L.orbx_learned_get_stats.argtypes = [vp, ctypes.POINTER(LearnedStats)]
         L.orbx_learned_export.argtypes = [vp, vp, vp, vp, vp, vp, vp, vp]
@@ -156,6 +157,7 @@ def ocv_detect_and_compute(ctx, img, w, h, params=None, cap=None):
 
 
 PROPOSAL_MLP, PROPOSAL_LSH = 0, 1
+RERANK_TENSOR, RERANK_POPC = 0, 1
 INIT_CENTROIDS, INIT_RANDOM = 0, 1
 GEMM_F32, GEMM_BIAS_RELU_BF16, GEMM_MASK_BF16, GEMM_BF16, GEMM_TOP8 = 0, 1, 2, 3, 4
 
@@ -166,7 +168,7 @@ class LearnedParams(ctypes.Structure):
                 ("batch", ctypes.c_int), ("lr", ctypes.c_float), ("margin", ctypes.c_float),
                 ("lsh_bits", ctypes.c_int), ("seed", ctypes.c_ulonglong), ("max_distance", ctypes.c_int),
                 ("spill", ctypes.c_int), ("init", ctypes.c_int), ("synth_train", ctypes.c_int),
-                ("flip_lo", ctypes.c_float), ("flip_hi", ctypes.c_float)]
+                ("flip_lo", ctypes.c_float), ("flip_hi", ctypes.c_float), ("rerank", ctypes.c_int)]
 
 
 class LearnedStats(ctypes.Structure):
@@ -462,6 +464,10 @@ class LearnedIndex:
     def set_max_distance(self, d):
         self.params.max_distance = int(d)
         _check(lib().orbx_learned_set_max_distance(self.h, int(d)), "orbx_learned_set_max_distance")
+
+    def set_rerank(self, form):
+        self.params.rerank = int(form)
+        _check(lib().orbx_learned_set_rerank(self.h, int(form)), "orbx_learned_set_rerank")
 
     def stats(self):
         st = LearnedStats()

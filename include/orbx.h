@@ -286,7 +286,10 @@ typedef struct orbx_learned_params {
   int synth_train;  /* extra training rows: database rows with random bit flips, exactly labelled */
   float flip_lo;    /* per-row bit-flip probability of those rows, uniform in [flip_lo, flip_hi] */
   float flip_hi;
+  int rerank;       /* ORBX_RERANK_TENSOR (int8 tensor cores) or ORBX_RERANK_POPC (XOR-popc) */
 } orbx_learned_params;
+/* Exact rerank of the probed clusters: both forms give the same results. */
+enum { ORBX_RERANK_TENSOR = 0, ORBX_RERANK_POPC = 1 };
 /* ORBX_INIT_CENTROIDS starts the MLP as nearest-centroid scoring (hidden units
  * relu(x_k) and relu(-x_k), output c = scaled dot product with centroid c), so
  * training refines the clustering's own proposal; needs hidden >= 512. */
@@ -321,6 +324,7 @@ ORBX_API int orbx_learned_profile_search(orbx_ctx* ctx, orbx_learned* index, con
                                          uint32_t* d_dist2, int32_t* d_idx2, float* h_ms);
 ORBX_API int orbx_learned_set_margin(orbx_learned* index, float margin);
 ORBX_API int orbx_learned_set_max_distance(orbx_learned* index, int max_distance);
+ORBX_API int orbx_learned_set_rerank(orbx_learned* index, int form); /* ORBX_RERANK_* */
 ORBX_API int orbx_learned_get_stats(const orbx_learned* index, orbx_learned_stats* s);
 /* Host copies for checks: cluster of every database row, cluster offsets
  * [n_clusters + 1] and the bf16 weights widened to float (any may be NULL). */

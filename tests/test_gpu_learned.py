@@ -274,7 +274,7 @@ def test_spill_and_synthetic_rows_and_distance_rule(ctx):
 
 
 # ---------------------------------------------------------------- checkpoints
-CKPT_HEAD = 16 + 4 * (18 + 136)  # magic, version, size; 18 parameter words; the statistics words
+CKPT_HEAD = 16 + 4 * (19 + 136)  # magic, version, size; 19 parameter words; the statistics words
 
 
 def _ckpt_centroids(blob, C):
@@ -302,7 +302,8 @@ def test_checkpoint_round_trip(ctx, small_index):
     assert len(blob) == CKPT_HEAD + 256 * 32 + 512 * 256 * 2 + 512 * 4 + 256 * 512 * 2 + 256 * 4 + 8
     re = orbx.LearnedIndex.load(ctx, blob, tdb)
     try:
-        for f in ("proposal", "n_clusters", "hidden", "n_probe", "spill", "seed", "max_distance", "lr", "margin"):
+        for f in ("proposal", "n_clusters", "hidden", "n_probe", "spill", "seed", "max_distance", "lr", "margin",
+                  "rerank"):
             assert getattr(re.params, f) == getattr(p, f), f
         st, rst = idx.stats(), re.stats()
         assert rst["loss"] == st["loss"] and rst["largest_cluster"] == st["largest_cluster"]
@@ -318,7 +319,7 @@ def test_checkpoint_round_trip(ctx, small_index):
         # saving the loaded index gives the same checkpoint apart from its build times
         re.set_margin(p.margin)
         blob2 = re.save()
-        bt = 16 + 4 * (18 + 4 + 64 + 64)
+        bt = 16 + 4 * (19 + 4 + 64 + 64)
         assert len(blob2) == len(blob) and blob2[:bt] == blob[:bt] and blob2[bt + 16:-8] == blob[bt + 16:-8]
     finally:
         idx.set_margin(0.0)
@@ -388,3 +389,66 @@ def test_checkpoint_rejects_damaged_bytes(ctx, small_index):
         assert e.value.status == orbx.ORBX_ERR_ARG, name
     with pytest.raises(orbx.OrbxError):
         orbx.LearnedIndex.load(ctx, bytes(blob), tdb[:0])
+
+
+# ---------------------------------------------------------------- rerank forms
+def _both_forms(ctx, idx, tq):
+    out = {}
+    for form in (orbx.RERANK_TENSOR, orbx.RERANK_POPC):
+        idx.set_rerank(form)
+        out[form] = idx.search(tq)
+        ctx.sync()
+    idx.set_rerank(orbx.RERANK_TENSOR)
+    return out[orbx.RERANK_TENSOR], out[orbx.RERANK_POPC]
+
+
+def test_rerank_forms_agree(ctx, small_index):
+    """The int8 tensor-core rerank and the XOR-popc rerank give the same top-2
+    (distance, index) for every query, at margin 0 and with part of the queries
+    sent to exact search."""
+    idx, db, q, tdb, tq = small_index
+    for m in (0.0, 1.0):
+        idx.set_margin(m)
+        try:
+            t, p = _both_forms(ctx, idx, tq)
+        finally:
+            idx.set_margin(0.0)
+        for x, y in zip(t, p):
+            assert torch.equal(x, y)
+    d, i = _check_consistent(q, db, t[0], t[1])
+    # the second neighbour is a consistent distance too, ordered after the first
+    ok = i[:, 1] >= 0
+    qb = np.unpackbits(q[ok], axis=1)
+    rb = np.unpackbits(db[i[ok, 1]], axis=1)
+    assert np.array_equal((qb != rb).sum(1), d[ok, 1])
+    assert np.all((d[ok, 1] > d[ok, 0]) | ((d[ok, 1] == d[ok, 0]) & (i[ok, 1] > i[ok, 0])))
+
+
+def test_rerank_forms_ties_and_ragged_clusters(ctx):
+    """Many exact ties (rows duplicated in the database), clusters of every size
+    from empty to several 256-row tiles, queries that probe one cluster many
+    times over: both forms agree, and they find the exact nearest row whenever
+    it is listed in a probed cluster."""
+    rng = np.random.Generator(np.random.PCG64(0x0C4300))
+    base, _ = clustered(6000, 1, n_centers=96, p_db=0.1, seed=9)
+    # near-copies of one row make a cluster of several tiles; exact duplicates give equal distances
+    hub = np.unpackbits(np.repeat(base[:1], 1500, axis=0), axis=1) ^ (rng.uniform(size=(1500, 256)) < 0.005)
+    db = np.concatenate([base, np.packbits(hub.astype(np.uint8), axis=1), base[rng.integers(0, len(base), 1500)]])
+    db = db[rng.permutation(len(db))]
+    q = db[rng.integers(0, len(db), 3000)].copy()
+    flips = (rng.uniform(size=(len(q), 256)) < 0.03).astype(np.uint8)
+    q = np.packbits(np.unpackbits(q, axis=1) ^ flips, axis=1)
+    q = np.concatenate([q, q[:5]])  # a ragged query count
+    tdb, tq = torch.from_numpy(db).cuda(), torch.from_numpy(q).cuda()
+    for spill in (1, 2):
+        p = orbx.learned_params(n_clusters=256, hidden=512, epochs=1, batch=512, kmeans_iters=6, spill=spill)
+        idx = orbx.LearnedIndex(ctx, tdb, tq[:512].contiguous(), p)
+        try:
+            sizes = np.diff(idx.export(weights=False)["offsets"])
+            assert sizes.min() < 64 and sizes.max() > 512, (sizes.min(), sizes.max())
+            t, pp = _both_forms(ctx, idx, tq)
+            for x, y in zip(t, pp):
+                assert torch.equal(x, y)
+            _check_consistent(q, db, t[0], t[1])
+        finally:
+            idx.close()
