@@ -266,14 +266,50 @@ __global__ void k_perturb_rows(const uint8_t* __restrict__ db, int ndb, int n, u
 
 // Spill lists: entry e < 2n is row e / 2 in cluster idx2[e] (its nearest, then
 // second-nearest centroid from the k = 2 matcher).
-__global__ void k_count_spill(const int32_t* __restrict__ idx2, int n, int* __restrict__ counts) {
-  const int e = blockIdx.x * blockDim.x + threadIdx.x;
-  if (e < 2 * n && idx2[e] >= 0) atomicAdd(&counts[idx2[e]], 1);
+// Lists from per-row cluster choices idx[row * per_row + j] (negative: none).
+__global__ void k_count_spill(const int32_t* __restrict__ idx, int n, int per_row, int* __restrict__ counts) {
+  const long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e < (long long)n * per_row && idx[e] >= 0) atomicAdd(&counts[idx[e]], 1);
 }
-__global__ void k_scatter_spill(const int32_t* __restrict__ idx2, int n, int* __restrict__ cursor,
+__global__ void k_scatter_spill(const int32_t* __restrict__ idx, int n, int per_row, int* __restrict__ cursor,
                                 int* __restrict__ members) {
-  const int e = blockIdx.x * blockDim.x + threadIdx.x;
-  if (e < 2 * n && idx2[e] >= 0) members[atomicAdd(&cursor[idx2[e]], 1)] = e >> 1;
+  const long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e < (long long)n * per_row && idx[e] >= 0) members[atomicAdd(&cursor[idx[e]], 1)] = (int)(e / per_row);
+}
+
+// One warp per row: the row's s <= 16 best columns from the GEMM's top-8 key
+// lists (lists of 128 columns, 8 keys each, descending), written as column
+// indices out[row * s + j] in decreasing key order (-1 past the keys).
+__global__ void __launch_bounds__(256) k_select_topk(const uint32_t* __restrict__ keys, int n, int lists, int s,
+                                                     int* __restrict__ out) {
+  const int r = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (r >= n) return;
+  const int nk = lists * kTopK;  // <= 256
+  const int kpl = (nk + 31) >> 5;
+  uint32_t mine[8];
+#pragma unroll
+  for (int i = 0; i < 8; i++) {
+    const int j = lane * kpl + i;
+    mine[i] = (i < kpl && j < nk) ? keys[(size_t)r * nk + j] : 0u;
+  }
+#pragma unroll
+  for (int a = 0; a < 7; a++)
+#pragma unroll
+    for (int b = 0; b < 7 - a; b++) {
+      const uint32_t hi = max(mine[b], mine[b + 1]), lo = min(mine[b], mine[b + 1]);
+      mine[b] = hi;
+      mine[b + 1] = lo;
+    }
+  for (int i = 0; i < s; i++) {
+    const uint32_t m = __reduce_max_sync(0xffffffffu, mine[0]);
+    if (lane == 0) out[(size_t)r * s + i] = m ? top_key_col(m) : -1;
+    if (mine[0] == m && m != 0u) {
+#pragma unroll
+      for (int k = 0; k < 7; k++) mine[k] = mine[k + 1];
+      mine[7] = 0u;
+    }
+  }
 }
 
 // ---------------------------------------------------------------- k-majority

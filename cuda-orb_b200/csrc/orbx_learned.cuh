@@ -106,8 +106,9 @@ __global__ void k_init_centroid_mlp(const uint8_t* centroids, int C, int Hd, flo
                                     float* w2, float* b2, __nv_bfloat16* w1b, __nv_bfloat16* w2b);
 __global__ void k_perturb_rows(const uint8_t* db, int ndb, int n, unsigned long long seed, float flip_lo,
                                float flip_hi, uint8_t* out);
-__global__ void k_count_spill(const int32_t* idx2, int n, int* counts);
-__global__ void k_scatter_spill(const int32_t* idx2, int n, int* cursor, int* members);
+__global__ void k_count_spill(const int32_t* idx, int n, int per_row, int* counts);
+__global__ void k_scatter_spill(const int32_t* idx, int n, int per_row, int* cursor, int* members);
+__global__ void k_select_topk(const uint32_t* keys, int n, int lists, int s, int* out);
 __global__ void k_gather_fallback(const uint8_t* q_desc, const int* fb_list, const int* fb_count, uint8_t* out);
 __global__ void k_scatter_fallback(const int* fb_list, const int* fb_count, const uint32_t* fd, const int32_t* fi,
                                    uint32_t* dist2, int32_t* idx2);

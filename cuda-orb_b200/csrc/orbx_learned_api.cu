@@ -167,7 +167,7 @@ struct orbx_learned {
   int device = 0;
   orbx_learned_params p{};
   int ndb = 0, C = 0, Hd = 0;
-  int n_entries = 0;  // cluster list entries (ndb, or up to 2 * ndb with spill)
+  int n_entries = 0;  // cluster list entries (ndb, or up to spill * ndb)
   Arena keep;
   uint8_t* db = nullptr;
   int8_t* db_pm1 = nullptr;
@@ -267,7 +267,7 @@ int check_params(const orbx_learned_params* p) {
     if (p->n_clusters < 256 || p->n_clusters > 4096 || p->n_clusters % 256) return ORBX_ERR_ARG;
     if (p->hidden < 256 || p->hidden > 4096 || p->hidden % 256) return ORBX_ERR_ARG;
     if (p->batch < 128 || p->batch % 128 || p->epochs < 0 || p->epochs > 64 || p->kmeans_iters < 1) return ORBX_ERR_ARG;
-    if (p->spill < 1 || p->spill > 2 || (p->init != ORBX_INIT_CENTROIDS && p->init != ORBX_INIT_RANDOM)) return ORBX_ERR_ARG;
+    if (p->spill < 1 || p->spill > 16 || (p->init != ORBX_INIT_CENTROIDS && p->init != ORBX_INIT_RANDOM)) return ORBX_ERR_ARG;
     if (p->init == ORBX_INIT_CENTROIDS && p->hidden < 512) return ORBX_ERR_ARG;
     if (p->synth_train < 0 || !(p->flip_lo >= 0.f && p->flip_lo <= p->flip_hi && p->flip_hi <= 0.5f)) return ORBX_ERR_ARG;
   }
@@ -291,13 +291,40 @@ int read_list_stats(orbx_learned* L, const int* counts, cudaStream_t s) {
 
 // Spill 2: every row listed in its nearest and second-nearest cluster, from the
 // matcher's top-2 against the centroids.
-int spill_lists(orbx_learned* L, const int32_t* idx2, int* counts, int* cursor, cudaStream_t s) {
+int spill_lists(orbx_learned* L, const int32_t* idx, int per_row, int* counts, int* cursor, cudaStream_t s) {
   const int n = L->ndb, C = L->C;
   LCHK(cudaMemsetAsync(counts, 0, sizeof(int) * C, s));
-  k_count_spill<<<grid1(2ll * n, 256), 256, 0, s>>>(idx2, n, counts);
+  k_count_spill<<<grid1((long long)per_row * n, 256), 256, 0, s>>>(idx, n, per_row, counts);
   k_scan_counts<<<1, 1024, 0, s>>>(counts, C, L->ivf_offsets, cursor, 0, nullptr);
-  k_scatter_spill<<<grid1(2ll * n, 256), 256, 0, s>>>(idx2, n, cursor, L->ivf_members);
+  k_scatter_spill<<<grid1((long long)per_row * n, 256), 256, 0, s>>>(idx, n, per_row, cursor, L->ivf_members);
   return read_list_stats(L, counts, s);
+}
+
+// Spill 3 and up: every row listed in its `spill` nearest centroids.  The
+// Hamming distances to all centroids come from the BF16 tensor-core GEMM on +-1
+// rows (dot = 256 - 2 * Hamming, exact in fp32), whose epilogue keeps the 8
+// nearest of each 128 centroids by (distance, centroid index); the row's
+// clusters are the best `spill` of those (exactly the nearest for spill <= 8).
+int spill_lists_gemm(orbx_learned* L, int* counts, int* cursor, cudaStream_t s, int* err) {
+  const int n = L->ndb, C = L->C, S = L->p.spill;
+  const int chunk = 65536;
+  Arena t;
+  bf16 *cent, *x;
+  uint32_t* keys;
+  int* sel;
+  LCHK(t.alloc(&cent, (size_t)C * 256));
+  LCHK(t.alloc(&x, (size_t)chunk * 256));
+  LCHK(t.alloc(&keys, (size_t)chunk * (C / 128) * kTopK));
+  LCHK(t.alloc(&sel, (size_t)n * S));
+  k_bits_pm1_bf16<<<grid1((long long)C * 32, 256), 256, 0, s>>>(L->centroids, C, nullptr, C, cent);
+  for (int off = 0; off < n; off += chunk) {
+    const int m = std::min(chunk, n - off);
+    const int rows = round_up(m, 128);
+    k_bits_pm1_bf16<<<grid1((long long)rows * 32, 256), 256, 0, s>>>(L->db + (size_t)off * 32, m, nullptr, rows, x);
+    LCHK(gemm(s, err, x, cent, rows, C, 256, nullptr, kTop8, 1, nullptr, nullptr, nullptr, keys));
+    k_select_topk<<<grid1((long long)m * 32, 256), 256, 0, s>>>(keys, m, C / 128, S, sel + (size_t)off * S);
+  }
+  return spill_lists(L, sel, S, counts, cursor, s);
 }
 
 // Device buffers every index holds: the database (bits and the matcher's +-1
@@ -305,10 +332,11 @@ int spill_lists(orbx_learned* L, const int32_t* idx2, int* counts, int* cursor, 
 // projections.
 int alloc_core(orbx_learned* L) {
   const int ndb = L->ndb;
+  const size_t per = L->p.proposal == ORBX_PROPOSAL_MLP ? (size_t)std::max(1, L->p.spill) : 1;  // list entries per row
   if (L->keep.alloc(&L->db, (size_t)ndb * 32) || L->keep.alloc(&L->db_pm1, (size_t)imma_rows_db(ndb) * 256) ||
       L->keep.alloc(&L->centroids, (size_t)L->C * 32) || L->keep.alloc(&L->assign, (size_t)ndb) ||
-      L->keep.alloc(&L->ivf_offsets, (size_t)L->C + 1) || L->keep.alloc(&L->ivf_members, (size_t)ndb * 2) ||
-      L->keep.alloc(&L->ivf_desc, (size_t)ndb * 2 * 32) ||
+      L->keep.alloc(&L->ivf_offsets, (size_t)L->C + 1) || L->keep.alloc(&L->ivf_members, (size_t)ndb * per) ||
+      L->keep.alloc(&L->ivf_desc, (size_t)ndb * per * 32) ||
       (L->p.proposal == ORBX_PROPOSAL_LSH && L->keep.alloc(&L->lsh, 256 * 256)))
     return ORBX_ERR_NOMEM;
   return ORBX_OK;
@@ -390,13 +418,15 @@ int cluster_kmeans(orbx_learned* L, cudaStream_t s, int* err) {
     LCHK(cudaGetLastError());
   }
   // spill 2: the last assignment's top-2
-  if (L->p.spill == 2) return spill_lists(L, idx2, counts, cursor, s);
+  if (L->p.spill == 2) return spill_lists(L, idx2, 2, counts, cursor, s);
+  if (L->p.spill > 2) return spill_lists_gemm(L, counts, cursor, s, err);
   return read_list_stats(L, counts, s);
 }
 
 // Lists over fixed centroids (a loaded index): every row's exact top-2
-// centroids by the int8 matcher, listed under the nearest (spill 1) or both
-// (spill 2).  The same assignment the last clustering iteration makes.
+// centroids by the int8 matcher give its cluster and, for spill 1 and 2, its
+// lists; spill 3 and up go through the GEMM as in clustering.  The same
+// assignment the last clustering iteration makes.
 int lists_from_centroids(orbx_learned* L, cudaStream_t s, int* err) {
   const int n = L->ndb, C = L->C;
   Arena t;
@@ -416,7 +446,8 @@ int lists_from_centroids(orbx_learned* L, cudaStream_t s, int* err) {
   LCHK(cudaMemsetAsync(counts, 0, sizeof(int) * C, s));
   LCHK(cudaMemsetAsync(changed, 0, sizeof(int), s));
   k_assign<<<grid1(n, 256), 256, 0, s>>>(idx2, n, L->assign, counts, changed);
-  if (L->p.spill == 2) return spill_lists(L, idx2, counts, cursor, s);
+  if (L->p.spill == 2) return spill_lists(L, idx2, 2, counts, cursor, s);
+  if (L->p.spill > 2) return spill_lists_gemm(L, counts, cursor, s, err);
   k_scan_counts<<<1, 1024, 0, s>>>(counts, C, L->ivf_offsets, cursor, 0, nullptr);
   k_scatter_members<<<grid1(n, 256), 256, 0, s>>>(L->assign, n, cursor, L->ivf_members);
   return read_list_stats(L, counts, s);

@@ -281,7 +281,9 @@ typedef struct orbx_learned_params {
   int lsh_bits;     /* LSH: log2 of the bucket count, 8..12 */
   unsigned long long seed;
   int max_distance; /* exact fallback also when the best reranked distance exceeds this (>= 256: off) */
-  int spill;        /* MLP: each database row is listed in its 1 or 2 nearest clusters */
+  int spill;        /* MLP: each database row is listed in its `spill` nearest clusters, 1..16
+                       (1, 2: by the int8 matcher; 3..16: by the BF16 GEMM's per-128-centroid
+                       top 8, exactly the nearest up to 8) */
   int init;         /* ORBX_INIT_CENTROIDS or ORBX_INIT_RANDOM */
   int synth_train;  /* extra training rows: database rows with random bit flips, exactly labelled */
   float flip_lo;    /* per-row bit-flip probability of those rows, uniform in [flip_lo, flip_hi] */
@@ -343,7 +345,7 @@ ORBX_API int orbx_learned_gradients(orbx_ctx* ctx, orbx_learned* index, const ui
 ORBX_API int orbx_learned_save(orbx_ctx* ctx, const orbx_learned* index, void* h_buf, size_t cap, size_t* h_need);
 /* An index from a checkpoint over d_db (the database it was built on, or
  * another one), without clustering or training: each row is listed under its
- * nearest saved centroid (spill 2: its two nearest) by the exact int8 matcher,
+ * `spill` nearest saved centroids (chosen as orbx_learned_build chooses them),
  * or under its LSH bucket.  Over the same database the loaded index searches
  * exactly like the saved one.  A checkpoint with a wrong magic, version, size
  * or hash, or invalid parameters, returns ORBX_ERR_ARG before any device work.

@@ -452,3 +452,44 @@ def test_rerank_forms_ties_and_ragged_clusters(ctx):
             _check_consistent(q, db, t[0], t[1])
         finally:
             idx.close()
+
+
+def _cpu_spill_counts(db, cent, s):
+    """Each row's clusters as spill >= 3 chooses them: the 8 nearest of every 128
+    centroids by (distance, index), then the best s of those."""
+    key = _hamming(db, cent).astype(np.int64) * 4096 + np.arange(cent.shape[0])[None, :]
+    cand = np.concatenate([np.sort(key[:, t:t + 128], axis=1)[:, :8] for t in range(0, cent.shape[0], 128)], axis=1)
+    best = np.sort(cand, axis=1)[:, :s] % 4096
+    return np.bincount(best.reshape(-1), minlength=cent.shape[0])
+
+
+@pytest.mark.parametrize("spill", [3, 8, 12])
+def test_wide_spill_lists_and_recall(ctx, spill):
+    db, q = clustered(16384, 2048, seed=11)
+    tdb, tq = torch.from_numpy(db).cuda(), torch.from_numpy(q).cuda()
+    p = orbx.learned_params(n_clusters=256, hidden=512, epochs=1, batch=512, kmeans_iters=8, spill=spill)
+    idx = orbx.LearnedIndex(ctx, tdb, tq[:512].contiguous(), p)
+    try:
+        ex = idx.export(weights=False)
+        cent = _ckpt_centroids(idx.save(), 256)
+        counts = np.diff(ex["offsets"])
+        assert ex["offsets"][-1] == spill * len(db)
+        assert np.array_equal(counts, _cpu_spill_counts(db, cent, spill))
+        t, pp = _both_forms(ctx, idx, tq)
+        for x, y in zip(t, pp):
+            assert torch.equal(x, y)
+        d, _ = _check_consistent(q, db, t[0], t[1])
+        ed, _ = MO.knn1_bruteforce(q, db)
+        recall = float(np.mean(d[:, 0] == ed))
+        # spill 2 on the same data and clustering for comparison: wider lists find more
+        p2 = orbx.learned_params(n_clusters=256, hidden=512, epochs=1, batch=512, kmeans_iters=8, spill=2)
+        idx2 = orbx.LearnedIndex(ctx, tdb, tq[:512].contiguous(), p2)
+        try:
+            d2, i2, _, _ = idx2.search(tq)
+            ctx.sync()
+            r2 = float(np.mean(d2.cpu().numpy()[:, 0] == ed))
+        finally:
+            idx2.close()
+        assert recall >= r2, (recall, r2)
+    finally:
+        idx.close()
