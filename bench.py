@@ -59,6 +59,8 @@ def parse_args(argv=None):
                    help="pair1080: the 1920x1080 pair (default); match65536: k=2 matching only; "
                         "batch64: 64 pairs of mixed resolution and caps in one batch; "
                         "learned: learned-proposal k=2 search, 131072 queries x 1048576 database rows")
+    p.add_argument("--learned-spill", type=int, default=12,
+                   help="learned: clusters each database row is listed in (1..16)")
     p.add_argument("--learned-scale", type=float, default=1.0,
                    help="learned: fraction of the database / query / training sizes (tests use < 1)")
     p.add_argument("--match-mode", choices=["imma", "popc"], default="imma")
@@ -781,7 +783,7 @@ def run_learned_workload(args, world, rank, local):
         cal_d, _ = orbx.knn2(ctx, cal, db, orbx.MATCH_IMMA)
         cal_d1 = cal_d[:, 0].cpu().numpy()
         # build: clustering + labels + training on the GPU
-        lp = orbx.learned_params(synth_train=sizes["train"], flip_lo=0.08, flip_hi=0.2)
+        lp = orbx.learned_params(synth_train=sizes["train"], flip_lo=0.08, flip_hi=0.2, spill=args.learned_spill)
         tb = time.time()
         index = orbx.LearnedIndex(ctx, db, train, lp)
         build_wall_s = time.time() - tb
@@ -818,6 +820,15 @@ def run_learned_workload(args, world, rank, local):
             flush.zero_()
             prof += index.profile_search(q, dist, idx)
         prof /= 5
+        probe_pairs = index.probe_pairs()
+        # the same search with the XOR-popc rerank, for comparison
+        index.set_rerank(orbx.RERANK_POPC)
+        prof_popc = np.zeros(5)
+        for _ in range(3):
+            flush.zero_()
+            prof_popc += index.profile_search(q, dist, idx)
+        prof_popc /= 3
+        index.set_rerank(orbx.RERANK_TENSOR)
         # other operating points of the same index: (calibration target, recall, fallback, ms)
         curve = []
         for tgt in (0.9, 0.95, 0.98):
@@ -846,7 +857,7 @@ def run_learned_workload(args, world, rank, local):
         e2e_ms = timed(e2e, steps)
         index.close()
         # without training: the same clustering probed by nearest centroids
-        cen = orbx.LearnedIndex(ctx, db, train, orbx.learned_params(epochs=0))
+        cen = orbx.LearnedIndex(ctx, db, train, orbx.learned_params(epochs=0, spill=args.learned_spill))
         recall_centroid = float(np.mean(no_fallback(cen, q)[0] == ex_d1))
         cen.close()
         # non-learned proposal at the same probe budget: random-projection buckets
@@ -868,13 +879,22 @@ def run_learned_workload(args, world, rank, local):
     # (512 ops per pair, bound: twice the measured bf16 rate); the proposal is the MLP
     # (2 * (256 * 512 + 512 * 4096) FLOPs per query, bf16 tensor bound).
     mlp_flop = 2.0 * (256 * 512 + 512 * 4096) * nq
-    if phases["fallback"] >= phases["proposal"]:
+    top = max(("fallback", "proposal", "rerank"), key=lambda k: phases[k])
+    if top == "fallback":
         ops = float(n_fb) * ndb * 512.0
         achieved = ops / (phases["fallback"] * 1e-3) / 1e12
         roof = {"kernel": "k_match_imma (exact fallback)", "bound": "tensor", "achieved": achieved,
                 "peak": 2.0 * peaks["bf16_tflops"], "unit": "TOP/s (int8)",
                 "frac": achieved / (2.0 * peaks["bf16_tflops"]), "traffic": None,
                 "peak_kind": f"{peak_kind}: 2 x bf16_tflops (int8 dense rate is twice bf16)"}
+    elif top == "rerank":
+        ops = float(probe_pairs) * 512.0
+        achieved = ops / (phases["rerank"] * 1e-3) / 1e12
+        roof = {"kernel": "k_rerank_imma (probe rerank)", "bound": "tensor", "achieved": achieved,
+                "peak": 2.0 * peaks["bf16_tflops"], "unit": "TOP/s (int8)",
+                "frac": achieved / (2.0 * peaks["bf16_tflops"]), "traffic": None,
+                "peak_kind": f"{peak_kind}: 2 x bf16_tflops (int8 dense rate is twice bf16)",
+                "algorithmic": "512 int8 ops per scanned (query, row) pair"}
     else:
         achieved = mlp_flop / (phases["proposal"] * 1e-3) / 1e12
         roof = {"kernel": "k_gemm_bf16 (MLP proposal phase)", "bound": "tensor", "achieved": achieved,
@@ -888,7 +908,8 @@ def run_learned_workload(args, world, rank, local):
             "data": f"synthetic: pipeline descriptors of {n_images} generated 1024x1024 images",
             "config": {"workload": "learned-proposal k=2 search", "queries": nq, "database": ndb,
                        "train_rows": train.shape[0], "calibration_rows": cal.shape[0],
-                       "n_clusters": 4096, "hidden": 512, "n_probe": 8, "l2": "flushed before every step"},
+                       "n_clusters": 4096, "hidden": 512, "n_probe": 8, "spill": args.learned_spill,
+                       "rerank": "int8 tcgen05", "l2": "flushed before every step"},
             "recall_at_1": recall, "recall_target": LEARNED_RECALL,
             "fallback_rule": {"margin_below": tau_m, "distance_above": tau_d},
             "fallback_fraction": n_fb / nq, "calibration_fallback_fraction": cal_fb,
@@ -900,6 +921,10 @@ def run_learned_workload(args, world, rank, local):
                          "recall_lsh_no_fallback": recall_lsh,
                          "lsh_ms": statistics.median(lsh_ms), "lsh": "12 random-projection bits, 8 probes"},
             "phases_ms": phases, "proposal_tflops": proposal_tflops, "roofline": roof,
+            "rerank": {"pairs_scanned": probe_pairs, "pairs_per_query": probe_pairs / nq,
+                       "tensor_pairs_per_s": probe_pairs / (phases["rerank"] * 1e-3),
+                       "popc_ms": float(prof_popc[2]),
+                       "popc_pairs_per_s": probe_pairs / (float(prof_popc[2]) * 1e-3)},
             "build": build, "build_wall_s": build_wall_s, "generate_s": gen_s,
             "e2e": {"value": pairs / (statistics.median(e2e_ms) * 1e-3), "unit": "pairs/s",
                     "h2d_bytes_per_step": nq * 32, "d2h_bytes_per_step": nq * 16},

@@ -141,12 +141,12 @@ struct RerankImmaArgs {
   const int* ivf_offsets;    // [C + 1] list offsets: the cluster's row count
   const int* pad_offsets;    // [C + 1] the cluster's first padded row (multiples of 256)
   const int* pad_members;    // [pad_rows] database index of each padded row, -1 in the padding
+  const uint8_t* pad_desc;   // [pad_rows][32] packed rows of the padded lists (padding zero), 16-byte aligned
   uint2* partial;            // [slots][kRrGroups] top-2 keys
+  int* item_counter;         // zero at launch: the blocks claim items from it
   int* err;
 };
-// pad_pm1: [pad_rows][256] +-1 rows of the padded lists (padding rows zero)
-cudaError_t launch_rerank_imma(const RerankImmaArgs& a, const int8_t* pad_pm1, int pad_rows, int max_items,
-                               cudaStream_t s);
+cudaError_t launch_rerank_imma(const RerankImmaArgs& a, int max_items, cudaStream_t s);
 
 // Top-2 keys shared by both matcher forms: key = distance << 22 | index, so
 // ordering keys orders by (distance, index); 0xFFFFFFFF means "none".

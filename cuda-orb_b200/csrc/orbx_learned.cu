@@ -277,6 +277,59 @@ __global__ void k_scatter_spill(const int32_t* __restrict__ idx, int n, int per_
   if (e < (long long)n * per_row && idx[e] >= 0) members[atomicAdd(&cursor[idx[e]], 1)] = (int)(e / per_row);
 }
 
+// Stable list construction.  Entries e = row * per_row + j, in increasing e,
+// go to their cluster's list in that order: block b of the histogram and the
+// scatter owns entries [b * kStableEntries, + kStableEntries).
+__global__ void __launch_bounds__(256) k_stable_hist(const int32_t* __restrict__ idx, long long total, int C,
+                                                     int* __restrict__ hist) {
+  extern __shared__ int s_h[];
+  for (int c = threadIdx.x; c < C; c += blockDim.x) s_h[c] = 0;
+  __syncthreads();
+  const long long e0 = (long long)blockIdx.x * kStableEntries;
+  const long long e1 = min(total, e0 + kStableEntries);
+  for (long long e = e0 + threadIdx.x; e < e1; e += blockDim.x) {
+    const int c = idx[e];
+    if (c >= 0) atomicAdd(&s_h[c], 1);
+  }
+  __syncthreads();
+  for (int c = threadIdx.x; c < C; c += blockDim.x) hist[(size_t)blockIdx.x * C + c] = s_h[c];
+}
+
+// hist[b][c] <- offsets[c] + entries of cluster c in blocks before b.
+__global__ void k_stable_scan(int* __restrict__ hist, int nb, int C, const int* __restrict__ offsets) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= C) return;
+  int run = offsets[c];
+  for (int b = 0; b < nb; b++) {
+    const int v = hist[(size_t)b * C + c];
+    hist[(size_t)b * C + c] = run;
+    run += v;
+  }
+}
+
+// One warp per block of entries, 32 at a time in order: lanes with the same
+// cluster take consecutive positions in lane order.
+__global__ void __launch_bounds__(32) k_stable_scatter(const int32_t* __restrict__ idx, long long total, int per_row,
+                                                       int C, const int* __restrict__ hist,
+                                                       int* __restrict__ members) {
+  extern __shared__ int s_cur[];
+  const int lane = threadIdx.x;
+  for (int c = lane; c < C; c += 32) s_cur[c] = hist[(size_t)blockIdx.x * C + c];
+  __syncwarp();
+  const long long e0 = (long long)blockIdx.x * kStableEntries;
+  const long long e1 = min(total, e0 + kStableEntries);
+  for (long long base = e0; base < e1; base += 32) {
+    const long long e = base + lane;
+    const int c = e < e1 ? idx[e] : -1;
+    const unsigned peers = __match_any_sync(0xffffffffu, c);
+    const int rank = __popc(peers & ((1u << lane) - 1u));
+    if (c >= 0) members[s_cur[c] + rank] = (int)(e / per_row);
+    __syncwarp();
+    if (c >= 0 && rank == 0) s_cur[c] += __popc(peers);
+    __syncwarp();
+  }
+}
+
 // One warp per row: the row's s <= 16 best columns from the GEMM's top-8 key
 // lists (lists of 128 columns, 8 keys each, descending), written as column
 // indices out[row * s + j] in decreasing key order (-1 past the keys).
@@ -635,6 +688,25 @@ __global__ void k_scatter_fallback(const int* __restrict__ fb_list, const int* _
   idx2[2 * q + 1] = fi[2 * j + 1];
 }
 
+// (query, database row) pairs a rerank scans: sum over clusters of probing
+// slots x listed rows.  One block of 1024 threads.
+__global__ void __launch_bounds__(1024) k_probe_pairs(const int* __restrict__ probe_offsets,
+                                                      const int* __restrict__ ivf_offsets, int C,
+                                                      unsigned long long* __restrict__ out) {
+  __shared__ unsigned long long s_sum[32];
+  unsigned long long acc = 0;
+  for (int c = threadIdx.x; c < C; c += blockDim.x)
+    acc += (unsigned long long)(probe_offsets[c + 1] - probe_offsets[c]) * (unsigned)(ivf_offsets[c + 1] - ivf_offsets[c]);
+  for (int d = 16; d >= 1; d >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, d);
+  if ((threadIdx.x & 31) == 0) s_sum[threadIdx.x >> 5] = acc;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    acc = threadIdx.x < (blockDim.x >> 5) ? s_sum[threadIdx.x] : 0ull;
+    for (int d = 16; d >= 1; d >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, d);
+    if (threadIdx.x == 0) *out = acc;
+  }
+}
+
 // ---------------------------------------------------------------- padded lists
 // Rows per cluster rounded up to the tensor-core rerank's 256-row tile.
 __global__ void k_pad_counts(const int* __restrict__ ivf_offsets, int C, int* __restrict__ pad_counts) {
@@ -643,27 +715,20 @@ __global__ void k_pad_counts(const int* __restrict__ ivf_offsets, int C, int* __
 }
 
 // Cluster c's padded rows [pad_offsets[c], pad_offsets[c + 1]): its list's
-// database rows as +-1 bytes (bit j of packed byte i -> byte 8 i + j, as the
-// int8 matcher expands them) with their database index, then zero rows with
-// index -1.  One block per cluster.
+// packed database rows with their database index, then zero rows with index
+// -1.  One block per cluster, 16 bytes per thread and step.
 __global__ void __launch_bounds__(256) k_fill_pad(const uint8_t* __restrict__ db, const int* __restrict__ ivf_members,
                                                   const int* __restrict__ ivf_offsets,
-                                                  const int* __restrict__ pad_offsets, int8_t* __restrict__ pad_pm1,
+                                                  const int* __restrict__ pad_offsets, uint8_t* __restrict__ pad_desc,
                                                   int* __restrict__ pad_members) {
-  __shared__ unsigned long long lut[256];
-  for (int i = threadIdx.x; i < 256; i += blockDim.x) {
-    unsigned long long v = 0;
-    for (int j = 0; j < 8; j++) v |= (unsigned long long)(((i >> j) & 1) ? 0x01u : 0xFFu) << (8 * j);
-    lut[i] = v;
-  }
-  __syncthreads();
   const int c = blockIdx.x;
   const int m0 = ivf_offsets[c], n = ivf_offsets[c + 1] - m0;
   const int p0 = pad_offsets[c], np = pad_offsets[c + 1] - p0;
-  unsigned long long* out = reinterpret_cast<unsigned long long*>(pad_pm1) + (size_t)p0 * 32;
-  for (long long i = threadIdx.x; i < (long long)np * 32; i += blockDim.x) {
-    const int r = (int)(i >> 5);
-    out[i] = r < n ? lut[db[(size_t)ivf_members[m0 + r] * 32 + (i & 31)]] : 0ull;
+  uint4* out = reinterpret_cast<uint4*>(pad_desc) + (size_t)p0 * 2;
+  const uint4* src = reinterpret_cast<const uint4*>(db);
+  for (int i = threadIdx.x; i < np * 2; i += blockDim.x) {
+    const int r = i >> 1;
+    out[i] = r < n ? src[(size_t)ivf_members[m0 + r] * 2 + (i & 1)] : make_uint4(0u, 0u, 0u, 0u);
   }
   for (int r = threadIdx.x; r < np; r += blockDim.x) pad_members[p0 + r] = r < n ? ivf_members[m0 + r] : -1;
 }

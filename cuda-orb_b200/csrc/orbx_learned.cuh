@@ -100,8 +100,9 @@ __global__ void k_rerank(const uint8_t* q_desc, const int* list, const int* prob
 __global__ void k_merge_probes(const uint2* partial, int per_slot, int nq, const float* margin, float margin_thr,
                                int max_dist, uint32_t* dist2, int32_t* idx2, int* fb_list, int* fb_count);
 __global__ void k_pad_counts(const int* ivf_offsets, int C, int* pad_counts);
+__global__ void k_probe_pairs(const int* probe_offsets, const int* ivf_offsets, int C, unsigned long long* out);
 __global__ void k_fill_pad(const uint8_t* db, const int* ivf_members, const int* ivf_offsets, const int* pad_offsets,
-                           int8_t* pad_pm1, int* pad_members);
+                           uint8_t* pad_desc, int* pad_members);
 __global__ void k_init_centroid_mlp(const uint8_t* centroids, int C, int Hd, float scale, float* w1, float* b1,
                                     float* w2, float* b2, __nv_bfloat16* w1b, __nv_bfloat16* w2b);
 __global__ void k_perturb_rows(const uint8_t* db, int ndb, int n, unsigned long long seed, float flip_lo,
@@ -109,6 +110,11 @@ __global__ void k_perturb_rows(const uint8_t* db, int ndb, int n, unsigned long 
 __global__ void k_count_spill(const int32_t* idx, int n, int per_row, int* counts);
 __global__ void k_scatter_spill(const int32_t* idx, int n, int per_row, int* cursor, int* members);
 __global__ void k_select_topk(const uint32_t* keys, int n, int lists, int s, int* out);
+constexpr int kStableEntries = 4096;  // list entries per block of the stable list construction
+__global__ void k_stable_hist(const int32_t* idx, long long total, int C, int* hist);
+__global__ void k_stable_scan(int* hist, int nb, int C, const int* offsets);
+__global__ void k_stable_scatter(const int32_t* idx, long long total, int per_row, int C, const int* hist,
+                                 int* members);
 __global__ void k_gather_fallback(const uint8_t* q_desc, const int* fb_list, const int* fb_count, uint8_t* out);
 __global__ void k_scatter_fallback(const int* fb_list, const int* fb_count, const uint32_t* fd, const int32_t* fi,
                                    uint32_t* dist2, int32_t* idx2);

@@ -111,13 +111,13 @@ struct ImmaWork {
   MatchWork w{};
   int splits = 1;
 };
-int imma_work_alloc(Arena& a, ImmaWork& iw, int nq_cap, int splits_for, cudaStream_t s) {
+int imma_work_alloc(Arena& a, ImmaWork& iw, int nq_cap, int splits_for, cudaStream_t s, int splits_cap = 0) {
   iw.splits = imma_default_splits(std::max(1, splits_for));
   iw.w.nq_cap = nq_cap;
-  iw.w.splits_cap = iw.splits;
-  if (iw.splits > 1) {
+  iw.w.splits_cap = std::max(iw.splits, splits_cap);
+  if (iw.w.splits_cap > 1) {
     const int tiles = (nq_cap + 127) / 128;
-    LCHK(a.alloc(&iw.w.part, (size_t)2 * iw.splits * nq_cap));
+    LCHK(a.alloc(&iw.w.part, (size_t)2 * iw.w.splits_cap * nq_cap));
     LCHK(a.alloc(&iw.w.tile_done, (size_t)tiles));
     LCHK(cudaMemsetAsync(iw.w.tile_done, 0, sizeof(unsigned) * (size_t)tiles, s));
   }
@@ -176,11 +176,11 @@ struct orbx_learned {
   int* ivf_offsets = nullptr;
   int* ivf_members = nullptr;
   uint8_t* ivf_desc = nullptr;
-  // the lists padded per cluster to 256-row tiles, for the tensor-core rerank
+  // the lists padded per cluster to 256-row tiles (packed rows), for the tensor-core rerank
   int pad_rows = 0;
   int* pad_offsets = nullptr;
   int* pad_members = nullptr;
-  int8_t* pad_pm1 = nullptr;
+  uint8_t* pad_desc = nullptr;
   float *w1 = nullptr, *b1 = nullptr, *w2 = nullptr, *b2 = nullptr;
   bf16 *w1b = nullptr, *w2b = nullptr, *w2tb = nullptr;
   bf16* lsh = nullptr;  // [256][256] projections, rows >= lsh_bits unused
@@ -194,6 +194,7 @@ struct orbx_learned {
   float* margin = nullptr;
   uint2* partial = nullptr;
   int *fb_list = nullptr, *fb_count = nullptr;
+  int* rr_counter = nullptr;
   uint8_t* fb_q = nullptr;
   uint32_t* fb_d = nullptr;
   int32_t* fb_i = nullptr;
@@ -291,12 +292,22 @@ int read_list_stats(orbx_learned* L, const int* counts, cudaStream_t s) {
 
 // Spill 2: every row listed in its nearest and second-nearest cluster, from the
 // matcher's top-2 against the centroids.
+// The final lists from per-row cluster choices idx[row * per_row + j]: each
+// cluster's list holds its rows in increasing index order, the same on every
+// run (the tensor-core rerank relies on that order to resolve equal distances).
 int spill_lists(orbx_learned* L, const int32_t* idx, int per_row, int* counts, int* cursor, cudaStream_t s) {
   const int n = L->ndb, C = L->C;
+  const long long total = (long long)per_row * n;
+  const int nb = (int)((total + kStableEntries - 1) / kStableEntries);
+  Arena t;
+  int* hist;
+  LCHK(t.alloc(&hist, (size_t)nb * C));
   LCHK(cudaMemsetAsync(counts, 0, sizeof(int) * C, s));
-  k_count_spill<<<grid1((long long)per_row * n, 256), 256, 0, s>>>(idx, n, per_row, counts);
+  k_count_spill<<<grid1(total, 256), 256, 0, s>>>(idx, n, per_row, counts);
   k_scan_counts<<<1, 1024, 0, s>>>(counts, C, L->ivf_offsets, cursor, 0, nullptr);
-  k_scatter_spill<<<grid1((long long)per_row * n, 256), 256, 0, s>>>(idx, n, per_row, cursor, L->ivf_members);
+  k_stable_hist<<<nb, 256, sizeof(int) * C, s>>>(idx, total, C, hist);
+  k_stable_scan<<<grid1(C, 256), 256, 0, s>>>(hist, nb, C, L->ivf_offsets);
+  k_stable_scatter<<<nb, 32, sizeof(int) * C, s>>>(idx, total, per_row, C, hist, L->ivf_members);
   return read_list_stats(L, counts, s);
 }
 
@@ -350,7 +361,7 @@ int upload_db(orbx_learned* L, const uint8_t* d_db, cudaStream_t s) {
 }
 
 // The padded lists of the tensor-core rerank, once the lists are built:
-// offsets, database indices and +-1 rows.  Synchronises the stream.
+// offsets, database indices and packed rows.  Synchronises the stream.
 int build_padded(orbx_learned* L, cudaStream_t s) {
   const int C = L->C;
   Arena t;
@@ -365,8 +376,8 @@ int build_padded(orbx_learned* L, cudaStream_t s) {
   LCHK(cudaStreamSynchronize(s));
   L->pad_rows = rows;
   LCHK(L->keep.alloc(&L->pad_members, (size_t)std::max(rows, 1)));
-  LCHK(L->keep.alloc(&L->pad_pm1, (size_t)std::max(rows, 1) * 256));
-  k_fill_pad<<<C, 256, 0, s>>>(L->db, L->ivf_members, L->ivf_offsets, L->pad_offsets, L->pad_pm1, L->pad_members);
+  LCHK(L->keep.alloc(&L->pad_desc, (size_t)std::max(rows, 1) * 32));
+  k_fill_pad<<<C, 256, 0, s>>>(L->db, L->ivf_members, L->ivf_offsets, L->pad_offsets, L->pad_desc, L->pad_members);
   LCHK(cudaGetLastError());
   return ORBX_OK;
 }
@@ -420,7 +431,7 @@ int cluster_kmeans(orbx_learned* L, cudaStream_t s, int* err) {
   // spill 2: the last assignment's top-2
   if (L->p.spill == 2) return spill_lists(L, idx2, 2, counts, cursor, s);
   if (L->p.spill > 2) return spill_lists_gemm(L, counts, cursor, s, err);
-  return read_list_stats(L, counts, s);
+  return spill_lists(L, L->assign, 1, counts, cursor, s);
 }
 
 // Lists over fixed centroids (a loaded index): every row's exact top-2
@@ -448,9 +459,7 @@ int lists_from_centroids(orbx_learned* L, cudaStream_t s, int* err) {
   k_assign<<<grid1(n, 256), 256, 0, s>>>(idx2, n, L->assign, counts, changed);
   if (L->p.spill == 2) return spill_lists(L, idx2, 2, counts, cursor, s);
   if (L->p.spill > 2) return spill_lists_gemm(L, counts, cursor, s, err);
-  k_scan_counts<<<1, 1024, 0, s>>>(counts, C, L->ivf_offsets, cursor, 0, nullptr);
-  k_scatter_members<<<grid1(n, 256), 256, 0, s>>>(L->assign, n, cursor, L->ivf_members);
-  return read_list_stats(L, counts, s);
+  return spill_lists(L, L->assign, 1, counts, cursor, s);
 }
 
 // Buckets of the database rows; make_proj draws the projections from the seed
@@ -480,11 +489,7 @@ int cluster_lsh(orbx_learned* L, cudaStream_t s, int* err, bool make_proj) {
     k_lsh_probes<<<grid1(m, 128), 128, 0, s>>>(proj, 256, m, L->p.lsh_bits, 0, nullptr, nullptr, nullptr,
                                                L->assign + off, nullptr, nullptr, 1);
   }
-  LCHK(cudaMemsetAsync(counts, 0, sizeof(int) * C, s));
-  k_count<<<grid1(n, 256), 256, 0, s>>>(L->assign, n, counts);
-  k_scan_counts<<<1, 1024, 0, s>>>(counts, C, L->ivf_offsets, cursor, 0, nullptr);
-  k_scatter_members<<<grid1(n, 256), 256, 0, s>>>(L->assign, n, cursor, L->ivf_members);
-  return read_list_stats(L, counts, s);
+  return spill_lists(L, L->assign, 1, counts, cursor, s);
 }
 
 int alloc_weights(orbx_learned* L, Arena& a, float** m, float** v) {
@@ -610,13 +615,15 @@ int ensure_search(orbx_learned* L, int nq) {
   LCHK(a.alloc(&L->partial, (size_t)nq * kTopK * kRrGroups));
   LCHK(a.alloc(&L->fb_list, (size_t)nq));
   LCHK(a.alloc(&L->fb_count, 1));
+  LCHK(a.alloc(&L->rr_counter, 1));
   LCHK(a.alloc(&L->fb_q, (size_t)nq * 32));
   LCHK(a.alloc(&L->fb_d, (size_t)nq * 2));
   LCHK(a.alloc(&L->fb_i, (size_t)nq * 2));
   LCHK(a.alloc(&L->fb_pm1, (size_t)imma_rows_q(nq) * 256));
-  // fallback splits sized for about one query in eight
+  // fallback splits sized for about one query in eight; fewer fallback queries
+  // split the database scan further, up to 32 ways
   L->fb_work = ImmaWork();
-  LRC(imma_work_alloc(a, L->fb_work, nq, std::max(128, nq / 8), 0));
+  LRC(imma_work_alloc(a, L->fb_work, nq, std::max(128, nq / 8), 0, 32));
   LCHK(cudaDeviceSynchronize());
   L->nq_cap = nq;
   return ORBX_OK;
@@ -797,9 +804,12 @@ static int search_impl(orbx_ctx* ctx, orbx_learned* L, const uint8_t* d_q, int n
     ra.ivf_offsets = L->ivf_offsets;
     ra.pad_offsets = L->pad_offsets;
     ra.pad_members = L->pad_members;
+    ra.pad_desc = L->pad_desc;
     ra.partial = L->partial;
+    ra.item_counter = L->rr_counter;
     ra.err = err;
-    LCHK(launch_rerank_imma(ra, L->pad_pm1, L->pad_rows, (int)items_max, s));
+    LCHK(cudaMemsetAsync(L->rr_counter, 0, sizeof(int), s));
+    LCHK(launch_rerank_imma(ra, (int)items_max, s));
   } else {
     k_rerank<<<items_max, kRerankQ, 0, s>>>(d_q, L->list, L->offsets, L->items, C, L->ivf_desc, L->ivf_members,
                                             L->ivf_offsets, L->partial);
@@ -851,6 +861,21 @@ ORBX_API int orbx_learned_profile_search(orbx_ctx* ctx, orbx_learned* L, const u
 ORBX_API int orbx_learned_set_margin(orbx_learned* L, float margin) {
   if (!L) return ORBX_ERR_ARG;
   L->p.margin = margin;
+  return ORBX_OK;
+}
+
+ORBX_API int orbx_learned_probe_pairs(orbx_ctx* ctx, const orbx_learned* L, unsigned long long* h_pairs) {
+  if (!ctx || !L || !h_pairs) return ORBX_ERR_ARG;
+  if (L->nq_cap == 0) return ORBX_ERR_STATE;
+  Guard g(L->device);
+  cudaStream_t s = ctx_stream(ctx);
+  Arena t;
+  unsigned long long* d;
+  LCHK(t.alloc(&d, 1));
+  k_probe_pairs<<<1, 1024, 0, s>>>(L->offsets, L->ivf_offsets, L->C, d);
+  LCHK(cudaGetLastError());
+  LCHK(cudaMemcpyAsync(h_pairs, d, sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
+  LCHK(cudaStreamSynchronize(s));
   return ORBX_OK;
 }
 

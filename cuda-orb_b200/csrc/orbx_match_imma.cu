@@ -186,6 +186,10 @@ __global__ void __launch_bounds__(kIThreads, 1)
   const int nq = min(a.d_nq ? *a.d_nq : a.nq, w.nq_cap);
   const int ndb = a.d_ndb ? *a.d_ndb : a.ndb;
   const int qtiles = (nq + kIBM - 1) / kIBM;
+  // With the query count on the device, the grid is sized for the capacity;
+  // when fewer query tiles are live, their database scans are split further
+  // (up to the merge scratch's splits_cap) so that the whole grid works.
+  if (a.d_nq && w.splits_cap > splits && qtiles > 0) splits = max(splits, min(w.splits_cap, (int)gridDim.x / qtiles));
   const int qb = blockIdx.x / splits;
   const int sp = blockIdx.x - qb * splits;
   if (qb >= qtiles) return;  // uniform over the block: before any barrier or TMEM use
@@ -420,30 +424,42 @@ __global__ void __launch_bounds__(kIThreads, 1)
 //
 // A work item is one cluster c with up to 128 of the query slots that probe it
 // (list[probe_offsets[c] ..], grouped by cluster; slot = query * 8 + probe).
-// The block is persistent and walks items blockIdx.x, + gridDim.x, ...:
-//   warp 0      TMA producer: the cluster's +-1 rows, padded per cluster to
-//               256-row tiles, through a 2-stage ring;
+// The cluster's rows are kept packed (32 bytes each, padded per cluster to
+// 256-row tiles) and expanded in shared memory, so HBM carries an eighth of
+// the bytes expanded rows would.  The blocks are persistent and claim items
+// from a global counter (items differ widely in size); the producer thread
+// claims them and passes them to the other roles through a small queue:
+//   warp 0      producer: each tile's 8 KB of packed rows by cp.async.bulk
+//               into a 4-stage ring;
 //   warp 1      MMA issuer, as in k_match_imma, into two 256-column
-//               accumulators; commits release the ring stage, the
+//               accumulators; commits release the expanded stage, the
 //               accumulator and, after an item's last tile, its query tile;
-//   warps 2-5   query gather: thread r expands slot r's 32 query bytes to a
-//               +-1 row in the 128-byte swizzled K-major layout the TMA writes,
-//               into one of two query tiles;
-//   warps 6-21  epilogue: warp w reads TMEM lanes 32 * (w % 4) and 64 columns,
+//   warps 2-9   expanders: at an item's start they gather its slots' queries
+//               as +-1 rows (two threads per row) into one of two query tiles,
+//               then expand each packed tile to 0 / 1 rows into one of two
+//               database tiles, one row per thread, in the 128-byte swizzled
+//               K-major layout the TMA writes;
+//   warps 10-25 epilogue: warp w reads TMEM lanes 32 * (w % 4) and 64 columns,
 //               keeps the top-2 keys (distance << 22 | database index) of each
-//               slot over the item's tiles and writes them to
-//               partial[slot * 4 + column group].
-// Keys carry the database index itself, so ties resolve by index whatever the
-// order of a cluster's list.  Every wait is bounded (kIDeadlineCycles per
+//               slot over the item's tiles (distance = popcount(query) - dot')
+//               and writes them to partial[slot * 4 + column group].
+// Each cluster's list is in increasing database index, so column order is
+// index order and ties resolve as in the other matchers.  Every wait is bounded (kIDeadlineCycles per
 // wait); on expiry the block records kErrImmaTimeout, drains its copies and
 // exits.
 // ---------------------------------------------------------------------------
-constexpr int kRrGatherWarps = 4;
-constexpr int kRrThreads = (2 + kRrGatherWarps + kIEpiWarps) * 32;
-constexpr uint32_t kRrBStages = 2;
-constexpr uint32_t kRrNumBars = 12;  // A full/empty, B full/empty, accumulator full/empty, two each
-constexpr uint32_t kRrSmemBytes = 1024 + 2 * kIATile + kRrBStages * kIBTile + 256 * 8 + 8 * kRrNumBars + 16;
+constexpr int kRrExpWarps = 8;
+constexpr int kRrThreads = (2 + kRrExpWarps + kIEpiWarps) * 32;
+constexpr uint32_t kRrPStages = 4;
+constexpr uint32_t kRrPTile = kIBN * 32;  // packed rows of one tile
+constexpr uint32_t kRrQueue = 8;  // claimed items in flight between the producer and the other roles
+constexpr uint32_t kRrNumBars = 2 + 2 + 2 * kRrPStages + 2 + 2 + 2 + 2 + 2 * kRrQueue;
+// the item queue's consumers: the MMA thread, the expander and the epilogue warps
+constexpr uint32_t kRrQueueReaders = 1 + kRrExpWarps + kIEpiWarps;
+constexpr uint32_t kRrSmemBytes =
+    1024 + 2 * kIATile + 2 * kIBTile + kRrPStages * kRrPTile + 8 * kRrNumBars + 4 * kRrQueue + 16;
 static_assert(kRrSmemBytes + 16 <= 232448, "exceeds the 227 KB shared-memory opt-in");
+static_assert(kRrExpWarps * 32 == kIBN && kRrExpWarps * 32 == 2 * kIBM, "one expander thread per row, two per query");
 
 struct RrItem {
   int c;      // cluster
@@ -481,16 +497,64 @@ __device__ __forceinline__ bool rr_warp_wait(uint32_t bar, uint32_t parity, vola
   return __shfl_sync(0xffffffffu, ok, 0) != 0;
 }
 
-__global__ void __launch_bounds__(kRrThreads, 1)
-    k_rerank_imma(const __grid_constant__ CUtensorMap tmD, RerankImmaArgs a) {
+// Four +-1 bytes from four bits: byte j is +1 where bit j of n is set, else -1
+// (the expansion k_expand_pm1 makes).  The multiply spreads bit j to bit 8j
+// without carries (bit positions j + 7i are distinct for j, i < 4).
+__device__ __forceinline__ uint32_t pm1_nibble(uint32_t n) {
+  return 0xFFFFFFFFu ^ (((n * 0x00204081u) & 0x01010101u) * 0xFEu);
+}
+
+// 16-byte chunk cc (K bytes 16 cc .. 16 cc + 15) of a +-1 row from its packed
+// 32-bit word w = words[cc >> 1]: bits 16 (cc & 1) .. + 15.
+__device__ __forceinline__ uint4 pm1_chunk(uint32_t w, int cc) {
+  const uint32_t h = w >> ((cc & 1) * 16);
+  return make_uint4(pm1_nibble(h & 0xFu), pm1_nibble((h >> 4) & 0xFu), pm1_nibble((h >> 8) & 0xFu),
+                    pm1_nibble((h >> 12) & 0xFu));
+}
+
+// The same chunk as 0 / 1 bytes (byte j = bit j): a database row in this form
+// gives dot' = sum of the query's +-1 values where the row has a one, and
+// Hamming(q, row) = popcount(q) - dot'.
+__device__ __forceinline__ uint32_t b01_nibble(uint32_t n) { return (n * 0x00204081u) & 0x01010101u; }
+__device__ __forceinline__ uint4 b01_chunk(uint32_t w, int cc) {
+  const uint32_t h = w >> ((cc & 1) * 16);
+  return make_uint4(b01_nibble(h & 0xFu), b01_nibble((h >> 4) & 0xFu), b01_nibble((h >> 8) & 0xFu),
+                    b01_nibble((h >> 12) & 0xFu));
+}
+
+// Swizzled address of chunk cc of row r in a K-major tile of `rows` rows
+// (two 128-byte K halves, each rows x 128 bytes).
+__device__ __forceinline__ uint8_t* sw128_chunk(uint8_t* tile, uint32_t half_bytes, int r, int cc) {
+  return tile + (cc >> 3) * half_bytes + r * 128 + (((cc & 7) ^ (r & 7)) << 4);
+}
+
+__device__ __forceinline__ void bulk_load(uint32_t dst, const void* src, uint32_t bytes, uint32_t bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
+               "l"(src), "r"(bytes), "r"(bar)
+               : "memory");
+}
+
+// The next claimed item of the queue (-1 when none is left), for a whole warp;
+// one arrival per warp frees the entry.  False on a timeout.
+__device__ __forceinline__ bool rr_next_item(uint32_t qfull, uint32_t qempty, volatile int* s_queue, uint32_t qs,
+                                             uint32_t parity, volatile int* abort_flag, int* it) {
+  if (!rr_warp_wait(qfull, parity, abort_flag)) return false;
+  *it = s_queue[qs];
+  __syncwarp();
+  if ((threadIdx.x & 31) == 0) mbar_arrive(qempty);
+  return true;
+}
+
+__global__ void __launch_bounds__(kRrThreads, 1) k_rerank_imma(RerankImmaArgs a) {
   extern __shared__ uint8_t smem_raw[];
   const uint32_t raw = smem_u32(smem_raw);
   uint8_t* smem = smem_raw + ((1024u - (raw & 1023u)) & 1023u);
-  uint8_t* sA = smem;                     // two query tiles
-  uint8_t* sB = sA + 2 * kIATile;         // ring of database tiles
-  unsigned long long* s_lut = reinterpret_cast<unsigned long long*>(sB + kRrBStages * kIBTile);
-  uint64_t* bars = reinterpret_cast<uint64_t*>(s_lut + 256);
-  uint32_t* s_tmem = reinterpret_cast<uint32_t*>(bars + kRrNumBars);
+  uint8_t* sA = smem;               // two query tiles
+  uint8_t* sX = sA + 2 * kIATile;   // two expanded database tiles
+  uint8_t* sP = sX + 2 * kIBTile;   // ring of packed database tiles
+  uint64_t* bars = reinterpret_cast<uint64_t*>(sP + kRrPStages * kRrPTile);
+  volatile int* s_queue = reinterpret_cast<volatile int*>(bars + kRrNumBars);
+  uint32_t* s_tmem = reinterpret_cast<uint32_t*>(const_cast<int*>(s_queue) + kRrQueue);
   volatile int* s_abort = reinterpret_cast<volatile int*>(s_tmem + 1);
 
   const int n_items = __ldg(a.item_offsets + a.n_clusters);
@@ -499,24 +563,31 @@ __global__ void __launch_bounds__(kRrThreads, 1)
   const uint32_t bar0 = smem_u32(bars);
 #define RR_AFULL(b) (bar0 + 8u * (b))
 #define RR_AEMPTY(b) (bar0 + 8u * (2 + (b)))
-#define RR_BFULL(s) (bar0 + 8u * (4 + (s)))
-#define RR_BEMPTY(s) (bar0 + 8u * (6 + (s)))
-#define RR_ACCFULL(x) (bar0 + 8u * (8 + (x)))
-#define RR_ACCEMPTY(x) (bar0 + 8u * (10 + (x)))
+#define RR_PFULL(s) (bar0 + 8u * (4 + (s)))
+#define RR_PEMPTY(s) (bar0 + 8u * (4 + kRrPStages + (s)))
+#define RR_XFULL(x) (bar0 + 8u * (4 + 2 * kRrPStages + (x)))
+#define RR_XEMPTY(x) (bar0 + 8u * (6 + 2 * kRrPStages + (x)))
+#define RR_ACCFULL(x) (bar0 + 8u * (8 + 2 * kRrPStages + (x)))
+#define RR_ACCEMPTY(x) (bar0 + 8u * (10 + 2 * kRrPStages + (x)))
+#define RR_QFULL(k) (bar0 + 8u * (12 + 2 * kRrPStages + (k)))
+#define RR_QEMPTY(k) (bar0 + 8u * (12 + 2 * kRrPStages + kRrQueue + (k)))
 
-  for (int i = threadIdx.x; i < 256; i += blockDim.x) {
-    unsigned long long v = 0;
-    for (int j = 0; j < 8; j++) v |= (unsigned long long)(((i >> j) & 1) ? 0x01u : 0xFFu) << (8 * j);
-    s_lut[i] = v;
-  }
   if (threadIdx.x == 0) {
     for (int b = 0; b < 2; b++) {
-      mbar_init(RR_AFULL(b), kRrGatherWarps);
+      mbar_init(RR_AFULL(b), kRrExpWarps);
       mbar_init(RR_AEMPTY(b), 1);
-      mbar_init(RR_BFULL(b), 1);
-      mbar_init(RR_BEMPTY(b), 1);
+      mbar_init(RR_XFULL(b), kRrExpWarps);
+      mbar_init(RR_XEMPTY(b), 1);
       mbar_init(RR_ACCFULL(b), 1);
       mbar_init(RR_ACCEMPTY(b), kIEpiWarps);
+    }
+    for (uint32_t st = 0; st < kRrPStages; st++) {
+      mbar_init(RR_PFULL(st), 1);
+      mbar_init(RR_PEMPTY(st), kRrExpWarps);
+    }
+    for (uint32_t k = 0; k < kRrQueue; k++) {
+      mbar_init(RR_QFULL(k), 1);
+      mbar_init(RR_QEMPTY(k), kRrQueueReaders);
     }
     *s_abort = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -535,47 +606,68 @@ __global__ void __launch_bounds__(kRrThreads, 1)
 
   if (warp == 0) {
     if (lane == 0) {
-      // TMA producer: every tile of every item of this block, in order
-      uint32_t issued[kRrBStages] = {0u, 0u};
-      uint32_t g = 0;
+      // producer: the packed rows of every tile of every item of this block, in order
+      uint32_t issued[kRrPStages];
+      for (uint32_t st = 0; st < kRrPStages; st++) issued[st] = 0u;
+      uint32_t g = 0, k = 0;
       bool ok = true;
-      for (int it = blockIdx.x; ok && it < n_items; it += gridDim.x) {
+      while (ok) {
+        // claim the next item and hand it to the other roles (-1: none left)
+        const uint32_t qs = k % kRrQueue;
+        if (k >= kRrQueue && !rr_wait(RR_QEMPTY(qs), ((k / kRrQueue) - 1) & 1u, s_abort)) {
+          ok = false;
+          break;
+        }
+        int it = atomicAdd(a.item_counter, 1);
+        if (it >= n_items) it = -1;
+        s_queue[qs] = it;
+        mbar_arrive(RR_QFULL(qs));
+        k++;
+        if (it < 0) break;
         const RrItem r = rr_item(a, it);
         for (int t = 0; t < r.tiles; t++, g++) {
-          const uint32_t s = g & 1u;
-          if (g >= 2 && !rr_wait(RR_BEMPTY(s), ((g >> 1) - 1) & 1u, s_abort)) {
+          const uint32_t st = g % kRrPStages;
+          if (g >= kRrPStages && !rr_wait(RR_PEMPTY(st), ((g / kRrPStages) - 1) & 1u, s_abort)) {
             ok = false;
             break;
           }
-          const int row = r.pbase + t * kIBN;
-          mbar_expect_tx(RR_BFULL(s), kIBTile);
-          tma_load_2d(smem_u32(sB + s * kIBTile), &tmD, 0, row, RR_BFULL(s));
-          tma_load_2d(smem_u32(sB + s * kIBTile + kIHalfB), &tmD, 128, row, RR_BFULL(s));
-          issued[s]++;
+          mbar_expect_tx(RR_PFULL(st), kRrPTile);
+          bulk_load(smem_u32(sP + st * kRrPTile), a.pad_desc + (size_t)(r.pbase + t * kIBN) * 32, kRrPTile,
+                    RR_PFULL(st));
+          issued[st]++;
         }
       }
       if (!ok) {
         *s_abort = 1;
         atomicOr(a.err, kErrImmaTimeout);
       }
-      // drain: every issued copy landed and the MMAs that read it completed
-      for (uint32_t s = 0; s < kRrBStages; s++) {
-        if (issued[s] == 0) continue;
-        const uint32_t par = (issued[s] - 1) & 1u;
+      // drain: every issued copy has landed and been read
+      for (uint32_t st = 0; st < kRrPStages; st++) {
+        if (issued[st] == 0) continue;
+        const uint32_t par = (issued[st] - 1) & 1u;
         long long dl = clock64() + kIDeadlineCycles;
-        while (!mbar_try(RR_BFULL(s), par) && clock64() < dl) {
+        while (!mbar_try(RR_PFULL(st), par) && clock64() < dl) {
         }
         dl = clock64() + kIDeadlineCycles;
-        while (!mbar_try(RR_BEMPTY(s), par) && clock64() < dl) {
+        while (!mbar_try(RR_PEMPTY(st), par) && clock64() < dl && !*s_abort) {
         }
       }
     }
   } else if (warp == 1) {
     if (lane == 0) {
       // MMA issuer
-      uint32_t g = 0, na = 0;
+      uint32_t g = 0, na = 0, k = 0;
       bool ok = true;
-      for (int it = blockIdx.x; ok && it < n_items; it += gridDim.x) {
+      while (ok) {
+        const uint32_t qs = k % kRrQueue;
+        if (!rr_wait(RR_QFULL(qs), (k / kRrQueue) & 1u, s_abort)) {
+          ok = false;
+          break;
+        }
+        const int it = s_queue[qs];
+        mbar_arrive(RR_QEMPTY(qs));
+        k++;
+        if (it < 0) break;
         const RrItem r = rr_item(a, it);
         if (r.tiles == 0) continue;
         const uint32_t b = na & 1u;
@@ -585,15 +677,15 @@ __global__ void __launch_bounds__(kRrThreads, 1)
         }
         const uint32_t a_lo = smem_u32(sA + b * kIATile);
         for (int t = 0; t < r.tiles; t++, g++) {
-          const uint32_t s = g & 1u, acc = g & 1u;
-          if (!rr_wait(RR_BFULL(s), (g >> 1) & 1u, s_abort) ||
-              (g >= 2 && !rr_wait(RR_ACCEMPTY(acc), ((g >> 1) - 1) & 1u, s_abort))) {
+          const uint32_t x = g & 1u;
+          if (!rr_wait(RR_XFULL(x), (g >> 1) & 1u, s_abort) ||
+              (g >= 2 && !rr_wait(RR_ACCEMPTY(x), ((g >> 1) - 1) & 1u, s_abort))) {
             ok = false;
             break;
           }
           tc_fence_after();
-          const uint32_t d = tmem_base + acc * (uint32_t)kIBN;
-          const uint32_t b_lo = smem_u32(sB + s * kIBTile);
+          const uint32_t d = tmem_base + x * (uint32_t)kIBN;
+          const uint32_t b_lo = smem_u32(sX + x * kIBTile);
 #pragma unroll
           for (int k = 0; k < 8; k++) {
             const int h = k >> 2, kk = k & 3;
@@ -601,8 +693,8 @@ __global__ void __launch_bounds__(kRrThreads, 1)
             const uint64_t db = sw128_desc(b_lo + h * kIHalfB) + (uint64_t)(2 * kk);
             umma_i8(d, da, db, kIDesc, k > 0 ? 1u : 0u);
           }
-          umma_commit(RR_BEMPTY(s));
-          umma_commit(RR_ACCFULL(acc));
+          umma_commit(RR_XEMPTY(x));
+          umma_commit(RR_ACCFULL(x));
         }
         if (!ok) break;
         umma_commit(RR_AEMPTY(b));
@@ -613,46 +705,69 @@ __global__ void __launch_bounds__(kRrThreads, 1)
         atomicOr(a.err, kErrImmaTimeout);
       }
     }
-  } else if (warp < 2 + kRrGatherWarps) {
-    // query gather: thread r fills row r of the item's query tile
-    const int r = threadIdx.x - 64;
-    uint32_t na = 0;
+  } else if (warp < 2 + kRrExpWarps) {
+    // expanders: thread e (0..255)
+    const int e = threadIdx.x - 64;
+    uint32_t na = 0, g = 0, k = 0;
     bool ok = true;
-    for (int it = blockIdx.x; it < n_items; it += gridDim.x) {
+    while (ok) {
+      int it;
+      const uint32_t qs = k % kRrQueue;
+      if (!rr_next_item(RR_QFULL(qs), RR_QEMPTY(qs), s_queue, qs, (k / kRrQueue) & 1u, s_abort, &it)) {
+        ok = false;
+        break;
+      }
+      k++;
+      if (it < 0) break;
       const RrItem ri = rr_item(a, it);
       if (ri.tiles == 0) continue;
+      // the item's queries: row e >> 1, K half e & 1
       const uint32_t b = na & 1u;
       if (na >= 2 && !rr_warp_wait(RR_AEMPTY(b), ((na >> 1) - 1) & 1u, s_abort)) {
         ok = false;
         break;
       }
-      uint4 w0 = make_uint4(0u, 0u, 0u, 0u), w1 = w0;
-      if (r < ri.rows) {
-        const int q = __ldg(a.list + ri.e0 + r) >> 3;
-        const uint4* src = reinterpret_cast<const uint4*>(a.q_bits) + 2 * (size_t)q;
-        w0 = __ldg(src);
-        w1 = __ldg(src + 1);
-      }
-      const uint32_t wd[8] = {w0.x, w0.y, w0.z, w0.w, w1.x, w1.y, w1.z, w1.w};
-      uint8_t* row = sA + b * kIATile + r * 128;
-#pragma unroll
-      for (int cc = 0; cc < 16; cc++) {
-        // 16-byte chunk cc holds the expansions of packed bytes 2cc and 2cc + 1
-        const uint32_t word = wd[cc >> 1];
-        const int sh = (cc & 1) * 16;
-        uint4 v = make_uint4(0u, 0u, 0u, 0u);
+      {
+        const int r = e >> 1, half = e & 1;
+        uint4 w = make_uint4(0u, 0u, 0u, 0u);
         if (r < ri.rows) {
-          const unsigned long long lo = s_lut[(word >> sh) & 0xFFu];
-          const unsigned long long hi = s_lut[(word >> (sh + 8)) & 0xFFu];
-          v = make_uint4((uint32_t)lo, (uint32_t)(lo >> 32), (uint32_t)hi, (uint32_t)(hi >> 32));
+          const int q = __ldg(a.list + ri.e0 + r) >> 3;
+          w = __ldg(reinterpret_cast<const uint4*>(a.q_bits) + 2 * (size_t)q + half);
         }
-        const int h = cc >> 3, j = cc & 7;
-        *reinterpret_cast<uint4*>(row + h * kIHalfA + ((j ^ (r & 7)) << 4)) = v;
+        const uint32_t wd[4] = {w.x, w.y, w.z, w.w};
+        uint8_t* tile = sA + b * kIATile;
+#pragma unroll
+        for (int j = 0; j < 8; j++) {
+          const int cc = 8 * half + j;
+          const uint4 v = (r < ri.rows) ? pm1_chunk(wd[j >> 1], cc) : make_uint4(0u, 0u, 0u, 0u);
+          *reinterpret_cast<uint4*>(sw128_chunk(tile, kIHalfA, r, cc)) = v;
+        }
       }
       asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
       __syncwarp();
       if (lane == 0) mbar_arrive(RR_AFULL(b));
       na++;
+      // the item's database tiles: row e of each
+      for (int t = 0; t < ri.tiles; t++, g++) {
+        const uint32_t st = g % kRrPStages, x = g & 1u;
+        if (!rr_warp_wait(RR_PFULL(st), (g / kRrPStages) & 1u, s_abort) ||
+            (g >= 2 && !rr_warp_wait(RR_XEMPTY(x), ((g >> 1) - 1) & 1u, s_abort))) {
+          ok = false;
+          break;
+        }
+        const uint4* src = reinterpret_cast<const uint4*>(sP + st * kRrPTile) + 2 * e;
+        const uint4 w0 = src[0], w1 = src[1];
+        const uint32_t wd[8] = {w0.x, w0.y, w0.z, w0.w, w1.x, w1.y, w1.z, w1.w};
+        __syncwarp();
+        if (lane == 0) mbar_arrive(RR_PEMPTY(st));
+        uint8_t* tile = sX + x * kIBTile;
+#pragma unroll
+        for (int cc = 0; cc < 16; cc++)
+          *reinterpret_cast<uint4*>(sw128_chunk(tile, kIHalfB, e, cc)) = b01_chunk(wd[cc >> 1], cc);
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        __syncwarp();
+        if (lane == 0) mbar_arrive(RR_XFULL(x));
+      }
     }
     if (!ok) {
       *s_abort = 1;
@@ -660,13 +775,31 @@ __global__ void __launch_bounds__(kRrThreads, 1)
     }
   } else {
     // epilogue
-    const int ew = warp - 2 - kRrGatherWarps;
+    const int ew = warp - 2 - kRrExpWarps;
     const int quarter = warp & 3;
     const int colgrp = ew >> 2;
-    uint32_t g = 0;
+    const int row = quarter * 32 + lane;
+    uint32_t g = 0, k = 0;
     bool ok = true;
-    for (int it = blockIdx.x; ok && it < n_items; it += gridDim.x) {
+    while (ok) {
+      int it;
+      const uint32_t qs = k % kRrQueue;
+      if (!rr_next_item(RR_QFULL(qs), RR_QEMPTY(qs), s_queue, qs, (k / kRrQueue) & 1u, s_abort, &it)) {
+        ok = false;
+        break;
+      }
+      k++;
+      if (it < 0) break;
       const RrItem ri = rr_item(a, it);
+      // this lane's slot and its query's popcount
+      int slot = -1, pc = 0;
+      if (row < ri.rows) {
+        slot = __ldg(a.list + ri.e0 + row);
+        const uint4* qp = reinterpret_cast<const uint4*>(a.q_bits) + 2 * (size_t)(slot >> 3);
+        const uint4 w0 = __ldg(qp), w1 = __ldg(qp + 1);
+        pc = __popc(w0.x) + __popc(w0.y) + __popc(w0.z) + __popc(w0.w) + __popc(w1.x) + __popc(w1.y) +
+             __popc(w1.z) + __popc(w1.w);
+      }
       uint32_t k1 = kNoKeyShared, k2 = kNoKeyShared;
       for (int t = 0; t < ri.tiles; t++, g++) {
         const uint32_t acc = g & 1u;
@@ -676,47 +809,53 @@ __global__ void __launch_bounds__(kRrThreads, 1)
         }
         tc_fence_after();
         const uint32_t taddr = tmem_base + ((uint32_t)(quarter * 32) << 16) + acc * (uint32_t)kIBN + colgrp * 64;
-        int v[64];
-        tmem_ld32(taddr, v);
-        tmem_ld32(taddr + 32u, v + 32);
-        tmem_wait_ld();
-        tc_fence_before();
-        __syncwarp();
-        if (lane == 0) mbar_arrive(RR_ACCEMPTY(acc));
-        const int col0 = t * kIBN + colgrp * 64;  // first column's row within the cluster
-        const int valid = ri.nrow - col0;
-        if (valid < 64) {
-#pragma unroll
-          for (int j = 0; j < 64; j++)
-            if (j >= valid) v[j] = kMaskedDot;
-        }
-#pragma unroll
+#pragma unroll 1
         for (int c = 0; c < 2; c++) {
-          int m = v[32 * c];
+          int v[32];
+          tmem_ld32(taddr + 32u * c, v);
+          tmem_wait_ld();
+          if (c == 1) {
+            // every column of this group is in registers: hand the accumulator back
+            tc_fence_before();
+            __syncwarp();
+            if (lane == 0) mbar_arrive(RR_ACCEMPTY(acc));
+          }
+          const int col0 = t * kIBN + colgrp * 64 + 32 * c;  // first column's row within the cluster
+          const int valid = ri.nrow - col0;
+          if (valid < 32) {
 #pragma unroll
-          for (int j = 1; j < 32; j++) m = max(m, v[32 * c + j]);
-          // a column can enter the top two when its distance is at most the
-          // current second best's (an equal distance with a smaller index wins)
-          const int thr = (k2 == kNoKeyShared) ? kMaskedDot + 1 : 256 - 2 * (int)(k2 >> kIdxBitsShared);
-          if (__any_sync(0xffffffffu, m >= thr)) {
-            const int e = col0 + 32 * c + lane;
-            const int mine = __ldg(a.pad_members + ri.pbase + e);
+            for (int j = 0; j < 32; j++)
+              if (j >= valid) v[j] = kMaskedDot;
+          }
+          int m = v[0];
+#pragma unroll
+          for (int j = 1; j < 32; j++) m = max(m, v[j]);
+          // The cluster's list is in increasing database index and the columns
+          // arrive in list order, so only a strictly larger dot' (a strictly
+          // smaller distance) than the current second best's can enter.
+          const int thr = (k2 == kNoKeyShared) ? kMaskedDot : pc - (int)(k2 >> kIdxBitsShared);
+          if (__any_sync(0xffffffffu, m > thr)) {
+            // the chunk's best two on local keys (dot' << 5 | 31 - column): ties keep the lower column
+            int a1 = INT_MIN, a2 = INT_MIN;
 #pragma unroll
             for (int j = 0; j < 32; j++) {
-              const int idx = __shfl_sync(0xffffffffu, mine, j);
-              const int dot = v[32 * c + j];
-              if (dot != kMaskedDot)
-                top2_push_shared(k1, k2, ((uint32_t)((256 - dot) >> 1) << kIdxBitsShared) | (uint32_t)idx);
+              const int lk = (v[j] << 5) | (31 - j);
+              a2 = max(a2, min(a1, lk));
+              a1 = max(a1, lk);
+            }
+            if ((a1 >> 5) > thr) {
+              const int m1 = __ldg(a.pad_members + ri.pbase + col0 + 31 - (a1 & 31));
+              top2_push_shared(k1, k2, ((uint32_t)(pc - (a1 >> 5)) << kIdxBitsShared) | (uint32_t)m1);
+              if ((a2 >> 5) > thr) {
+                const int m2 = __ldg(a.pad_members + ri.pbase + col0 + 31 - (a2 & 31));
+                top2_push_shared(k1, k2, ((uint32_t)(pc - (a2 >> 5)) << kIdxBitsShared) | (uint32_t)m2);
+              }
             }
           }
         }
       }
       if (!ok) break;
-      const int row = quarter * 32 + lane;
-      if (row < ri.rows) {
-        const int slot = __ldg(a.list + ri.e0 + row);
-        a.partial[(size_t)slot * kRrGroups + colgrp] = make_uint2(k1, k2);
-      }
+      if (slot >= 0) a.partial[(size_t)slot * kRrGroups + colgrp] = make_uint2(k1, k2);
     }
     if (!ok) {
       *s_abort = 1;
@@ -725,10 +864,14 @@ __global__ void __launch_bounds__(kRrThreads, 1)
   }
 #undef RR_AFULL
 #undef RR_AEMPTY
-#undef RR_BFULL
-#undef RR_BEMPTY
+#undef RR_PFULL
+#undef RR_PEMPTY
+#undef RR_XFULL
+#undef RR_XEMPTY
 #undef RR_ACCFULL
 #undef RR_ACCEMPTY
+#undef RR_QFULL
+#undef RR_QEMPTY
 
   tc_fence_before();
   __syncthreads();
@@ -818,23 +961,20 @@ cudaError_t launch_match_imma(const ImmaLaunch& L, cudaStream_t s) {
   return cudaGetLastError();
 }
 
-cudaError_t launch_rerank_imma(const RerankImmaArgs& a, const int8_t* pad_pm1, int pad_rows, int max_items,
-                               cudaStream_t s) {
-  if (max_items <= 0 || pad_rows <= 0) return cudaSuccess;
-  if (pad_rows % kIBN) return cudaErrorInvalidValue;
+cudaError_t launch_rerank_imma(const RerankImmaArgs& a, int max_items, cudaStream_t s) {
+  if (max_items <= 0) return cudaSuccess;
+  if (!a.pad_desc || (reinterpret_cast<uintptr_t>(a.pad_desc) & 15u)) return cudaErrorInvalidValue;
   static bool attr_set = false;
   if (!attr_set) {
     cudaError_t e = cudaFuncSetAttribute(k_rerank_imma, cudaFuncAttributeMaxDynamicSharedMemorySize, kRrSmemBytes);
     if (e != cudaSuccess) return e;
     attr_set = true;
   }
-  CUtensorMap td;
-  if (!make_rows_map(&td, pad_pm1, (uint64_t)pad_rows, kIBN)) return cudaErrorInvalidValue;
   int dev = 0, sms = 148;
   if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
     return cudaErrorInvalidValue;
   const int blocks = max_items < sms ? max_items : sms;  // persistent: one block per SM
-  k_rerank_imma<<<blocks, kRrThreads, kRrSmemBytes, s>>>(td, a);
+  k_rerank_imma<<<blocks, kRrThreads, kRrSmemBytes, s>>>(a);
   return cudaGetLastError();
 }
 

@@ -102,6 +102,7 @@ def lib():
         L.orbx_learned_set_margin.argtypes = [vp, ctypes.c_float]
         L.orbx_learned_set_max_distance.argtypes = [vp, i32]
         L.orbx_learned_set_rerank.argtypes = [vp, i32]
+        L.orbx_learned_probe_pairs.argtypes = [vp, vp, ctypes.POINTER(ctypes.c_ulonglong)]
         L.orbx_learned_profile_search.argtypes = [vp, vp, vp, i32, vp, vp, vp]
         L.orbx_learned_get_stats.argtypes = [vp, ctypes.POINTER(LearnedStats)]
         L.orbx_learned_export.argtypes = [vp, vp, vp, vp, vp, vp, vp, vp]
@@ -468,6 +469,12 @@ class LearnedIndex:
     def set_rerank(self, form):
         self.params.rerank = int(form)
         _check(lib().orbx_learned_set_rerank(self.h, int(form)), "orbx_learned_set_rerank")
+
+    def probe_pairs(self):
+        """(query, row) pairs the last search's rerank scanned (synchronises)."""
+        v = ctypes.c_ulonglong()
+        _check(lib().orbx_learned_probe_pairs(self.ctx.h, self.h, ctypes.byref(v)), "orbx_learned_probe_pairs")
+        return int(v.value)
 
     def stats(self):
         st = LearnedStats()

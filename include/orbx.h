@@ -327,6 +327,9 @@ ORBX_API int orbx_learned_profile_search(orbx_ctx* ctx, orbx_learned* index, con
 ORBX_API int orbx_learned_set_margin(orbx_learned* index, float margin);
 ORBX_API int orbx_learned_set_max_distance(orbx_learned* index, int max_distance);
 ORBX_API int orbx_learned_set_rerank(orbx_learned* index, int form); /* ORBX_RERANK_* */
+/* (query, database row) pairs the last search's rerank scanned (its probing
+ * slots times the rows of their clusters).  Synchronises. */
+ORBX_API int orbx_learned_probe_pairs(orbx_ctx* ctx, const orbx_learned* index, unsigned long long* h_pairs);
 ORBX_API int orbx_learned_get_stats(const orbx_learned* index, orbx_learned_stats* s);
 /* Host copies for checks: cluster of every database row, cluster offsets
  * [n_clusters + 1] and the bf16 weights widened to float (any may be NULL). */
