@@ -12,6 +12,8 @@
 //   warps 2-9  epilogue: warp w reads TMEM lanes 32 * (w % 4) (one output row
 //              per lane) and columns [128 * ((w - 2) / 4), +128) of the tile,
 //              then applies GemmArgs::mode (orbx_learned.cuh).
+// A work item is one output tile, or for kTop8Row an M tile with a run of N
+// tiles, whose rows keep running top-8 lists across the run.
 // M must be a multiple of 128, N of 256, K of 64 * splits; callers pad.
 #include <cuda.h>
 #include <cuda_bf16.h>
@@ -135,20 +137,25 @@ __device__ __forceinline__ void g_epilogue_chunk(const GemmArgs& g, int split, i
     for (int j = 0; j < 8; j++) dst[j] = make_float4(v[4 * j], v[4 * j + 1], v[4 * j + 2], v[4 * j + 3]);
     return;
   }
-  if (g.mode == kTop8) {
+  if (g.mode == kTop8 || g.mode == kTop8Row) {
     float mx = v[0];
 #pragma unroll
     for (int j = 1; j < 32; j++) mx = fmaxf(mx, v[j]);
-    if (top_key(mx, n0) <= top[kTopK - 1]) return;  // no column of this chunk can enter
+    if (!__any_sync(0xffffffffu, top_key(mx, n0) > top[kTopK - 1])) return;  // no column of this chunk can enter
+    // a key above the 8th needs a logit at least the 8th's (truncated) value
+    float f8 = top[kTopK - 1] ? order_bits_float(top[kTopK - 1] & ~((1u << kTopColBits) - 1u)) : -INFINITY;
 #pragma unroll
     for (int j = 0; j < 32; j++) {
-      uint32_t key = top_key(v[j], n0 + j);
-      if (key > top[kTopK - 1]) {
+      if (v[j] >= f8) {
+        uint32_t key = top_key(v[j], n0 + j);
+        if (key > top[kTopK - 1]) {
 #pragma unroll
-        for (int i = 0; i < kTopK; i++) {
-          const uint32_t hi = max(top[i], key);
-          key = min(top[i], key);
-          top[i] = hi;
+          for (int i = 0; i < kTopK; i++) {
+            const uint32_t hi = max(top[i], key);
+            key = min(top[i], key);
+            top[i] = hi;
+          }
+          if (top[kTopK - 1]) f8 = order_bits_float(top[kTopK - 1] & ~((1u << kTopColBits) - 1u));
         }
       }
     }
@@ -184,6 +191,28 @@ __device__ __forceinline__ void g_epilogue_chunk(const GemmArgs& g, int split, i
   }
 }
 
+// Work item -> (M tile, first N tile, K split, part): one tile per item, or
+// kTop8Row's M tile with `tpi` consecutive N tiles.
+struct GItem {
+  int tm, tn0, split, part;
+};
+__device__ __forceinline__ GItem g_item(const GemmArgs& g, int item, int n_tiles, int parts, int tpi) {
+  GItem r;
+  if (g.mode == kTop8Row) {
+    r.tm = item / parts;
+    r.part = item - r.tm * parts;
+    r.tn0 = r.part * tpi;
+    r.split = 0;
+  } else {
+    r.split = item % g.splits;
+    const int tile = item / g.splits;
+    r.tm = tile / n_tiles;
+    r.tn0 = tile - r.tm * n_tiles;
+    r.part = 0;
+  }
+  return r;
+}
+
 __global__ void __launch_bounds__(kGThreads, 1)
     k_gemm_bf16(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, GemmArgs g) {
   extern __shared__ uint8_t smem_raw[];
@@ -194,7 +223,10 @@ __global__ void __launch_bounds__(kGThreads, 1)
   volatile int* s_abort = reinterpret_cast<volatile int*>(s_tmem + 1);
 
   const int n_tiles = g.N / kGBN;
-  const int items = (g.M / kGBM) * n_tiles * g.splits;
+  const bool row_top = g.mode == kTop8Row;
+  const int parts = row_top ? gemm_top_parts(n_tiles) : 1;
+  const int tpi = row_top ? n_tiles / parts : 1;  // N tiles per work item
+  const int items = row_top ? (g.M / kGBM) * parts : (g.M / kGBM) * n_tiles * g.splits;
   const int kblocks = g.K / kGBK / g.splits;
   const int my_items = blockIdx.x < items ? (items - 1 - (int)blockIdx.x) / (int)gridDim.x + 1 : 0;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -236,23 +268,23 @@ __global__ void __launch_bounds__(kGThreads, 1)
       long long gkb = 0;
       bool ok = true;
       for (int j = 0; ok && j < my_items; j++) {
-        const int item = (int)blockIdx.x + j * (int)gridDim.x;
-        const int split = item % g.splits;
-        const int tile = item / g.splits;
-        const int tm = tile / n_tiles, tn = tile - (tile / n_tiles) * n_tiles;
-        for (int kb = 0; kb < kblocks; kb++, gkb++) {
-          const int s = (int)(gkb % kGStages);
-          const long long use = gkb / kGStages;
-          if (use > 0 && !g_mbar_wait(GBAR_EMPTY(s), (uint32_t)((use - 1) & 1), s_abort)) {
-            ok = false;
-            break;
+        const GItem it = g_item(g, (int)blockIdx.x + j * (int)gridDim.x, n_tiles, parts, tpi);
+        for (int t = 0; ok && t < tpi; t++) {
+          const int tn = it.tn0 + t;
+          for (int kb = 0; kb < kblocks; kb++, gkb++) {
+            const int s = (int)(gkb % kGStages);
+            const long long use = gkb / kGStages;
+            if (use > 0 && !g_mbar_wait(GBAR_EMPTY(s), (uint32_t)((use - 1) & 1), s_abort)) {
+              ok = false;
+              break;
+            }
+            uint8_t* st = smem + s * kGStage;
+            const int kx = (it.split * kblocks + kb) * kGBK;
+            g_mbar_expect_tx(GBAR_FULL(s), kGStage);
+            g_tma_load_2d(g_smem_u32(st), &tmA, kx, it.tm * kGBM, GBAR_FULL(s));
+            g_tma_load_2d(g_smem_u32(st + kGATile), &tmB, kx, tn * kGBN, GBAR_FULL(s));
+            issued[s]++;
           }
-          uint8_t* st = smem + s * kGStage;
-          const int kx = (split * kblocks + kb) * kGBK;
-          g_mbar_expect_tx(GBAR_FULL(s), kGStage);
-          g_tma_load_2d(g_smem_u32(st), &tmA, kx, tm * kGBM, GBAR_FULL(s));
-          g_tma_load_2d(g_smem_u32(st + kGATile), &tmB, kx, tn * kGBN, GBAR_FULL(s));
-          issued[s]++;
         }
       }
       if (!ok) {
@@ -275,7 +307,8 @@ __global__ void __launch_bounds__(kGThreads, 1)
     if (lane == 0) {
       long long gkb = 0;
       bool ok = true;
-      for (int j = 0; ok && j < my_items; j++) {
+      const int my_tiles = my_items * tpi;
+      for (int j = 0; ok && j < my_tiles; j++) {
         const int acc = j & 1;
         if (j >= 2 && !g_mbar_wait(GBAR_ACCEMPTY(acc), (uint32_t)(((j >> 1) - 1) & 1), s_abort)) {
           ok = false;
@@ -309,36 +342,46 @@ __global__ void __launch_bounds__(kGThreads, 1)
     const int quarter = warp & 3;
     const int half = (warp - 2) >> 2;
     bool ok = true;
-    for (int j = 0; j < my_items; j++) {
-      const int acc = j & 1;
-      if (!g_warp_wait(GBAR_ACCFULL(acc), (uint32_t)((j >> 1) & 1), s_abort)) {
-        ok = false;
-        break;
-      }
-      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-      const int item = (int)blockIdx.x + j * (int)gridDim.x;
-      const int split = item % g.splits;
-      const int tile = item / g.splits;
-      const int tm = tile / n_tiles, tn = tile - (tile / n_tiles) * n_tiles;
-      const int m = tm * kGBM + quarter * 32 + lane;
+    int gt = 0;  // tiles of this block so far: accumulator gt & 1
+    for (int j = 0; ok && j < my_items; j++) {
+      const GItem it = g_item(g, (int)blockIdx.x + j * (int)gridDim.x, n_tiles, parts, tpi);
+      const int m = it.tm * kGBM + quarter * 32 + lane;
       uint32_t top[kTopK];
 #pragma unroll
       for (int i = 0; i < kTopK; i++) top[i] = 0u;
-      const uint32_t tbase = tmem + ((uint32_t)(quarter * 32) << 16) + (uint32_t)(acc * kGBN + half * 128);
-#pragma unroll 1
-      for (int c = 0; c < 4; c++) {
-        float v[32];
-        g_tmem_ld32(tbase + (uint32_t)(c * 32), v);
-        if (c == 3) {
-          // every column of this half is in registers: hand the accumulator back
-          asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-          __syncwarp();
-          if (lane == 0) g_mbar_arrive(GBAR_ACCEMPTY(acc));
+      for (int t = 0; t < tpi; t++, gt++) {
+        const int acc = gt & 1;
+        const int tn = it.tn0 + t;
+        if (!g_warp_wait(GBAR_ACCFULL(acc), (uint32_t)((gt >> 1) & 1), s_abort)) {
+          ok = false;
+          break;
         }
-        g_epilogue_chunk(g, split, m, tn * kGBN + half * 128 + c * 32, v, top);
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        if (g.mode == kTop8) {
+#pragma unroll
+          for (int i = 0; i < kTopK; i++) top[i] = 0u;
+        }
+        const uint32_t tbase = tmem + ((uint32_t)(quarter * 32) << 16) + (uint32_t)(acc * kGBN + half * 128);
+#pragma unroll 1
+        for (int c = 0; c < 4; c++) {
+          float v[32];
+          g_tmem_ld32(tbase + (uint32_t)(c * 32), v);
+          if (c == 3) {
+            // every column of this half is in registers: hand the accumulator back
+            asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+            __syncwarp();
+            if (lane == 0) g_mbar_arrive(GBAR_ACCEMPTY(acc));
+          }
+          g_epilogue_chunk(g, it.split, m, tn * kGBN + half * 128 + c * 32, v, top);
+        }
+        if (g.mode == kTop8) {
+          uint4* dst = reinterpret_cast<uint4*>(g.top_keys + ((size_t)m * (2 * n_tiles) + 2 * tn + half) * kTopK);
+          dst[0] = make_uint4(top[0], top[1], top[2], top[3]);
+          dst[1] = make_uint4(top[4], top[5], top[6], top[7]);
+        }
       }
-      if (g.mode == kTop8) {
-        uint4* dst = reinterpret_cast<uint4*>(g.top_keys + ((size_t)m * (2 * n_tiles) + 2 * tn + half) * kTopK);
+      if (ok && row_top) {
+        uint4* dst = reinterpret_cast<uint4*>(g.top_keys + ((size_t)m * (2 * parts) + 2 * it.part + half) * kTopK);
         dst[0] = make_uint4(top[0], top[1], top[2], top[3]);
         dst[1] = make_uint4(top[4], top[5], top[6], top[7]);
       }
@@ -388,7 +431,7 @@ cudaError_t launch_gemm_bf16(const GemmArgs& g, cudaStream_t s) {
   if (g.M <= 0 || g.N <= 0 || g.K <= 0) return cudaSuccess;
   if (g.splits < 1 || (g.splits > 1 && g.mode != kStoreF32)) return cudaErrorInvalidValue;
   if (g.M % kGBM || g.N % kGBN || g.K % (kGBK * g.splits)) return cudaErrorInvalidValue;
-  if (g.mode == kTop8 && g.N > (1 << kTopColBits)) return cudaErrorInvalidValue;
+  if ((g.mode == kTop8 || g.mode == kTop8Row) && g.N > (1 << kTopColBits)) return cudaErrorInvalidValue;
   if (!g.err) return cudaErrorInvalidValue;
   static bool attr_set = false;
   if (!attr_set) {
@@ -402,7 +445,7 @@ cudaError_t launch_gemm_bf16(const GemmArgs& g, cudaStream_t s) {
   int dev = 0, sms = 148;
   if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
     return cudaErrorInvalidValue;
-  const int items = (g.M / kGBM) * (g.N / kGBN) * g.splits;
+  const int items = g.mode == kTop8Row ? (g.M / kGBM) * gemm_top_parts(g.N / kGBN) : (g.M / kGBM) * (g.N / kGBN) * g.splits;
   const int blocks = items < sms ? items : sms;  // persistent: one block per SM
   k_gemm_bf16<<<blocks, kGThreads, kGSmemBytes, s>>>(ta, tb, g);
   return cudaGetLastError();

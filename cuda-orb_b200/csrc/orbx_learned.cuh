@@ -16,7 +16,15 @@ enum GemmMode {
   kMaskBF16 = 2,      // bf16 acc where aux[m][n] > 0 else 0 (ReLU backward)
   kStoreBF16 = 3,     // bf16 acc (+ bias[n])
   kTop8 = 4,          // per row and 128 columns: the 8 largest (acc + bias[n]) as packed keys
+  kTop8Row = 5,       // per row, the 8 largest over each of gemm_top_lists(N) column sets (see below)
 };
+
+// kTop8Row: a block takes an M tile with half of the 256-column N tiles (all
+// of them when N / 256 is odd) and each row keeps one running top-8 per
+// 128-column half of those tiles, so list l = 2 * part + half covers columns
+// {256 t + 128 half + c : t in part's tiles, c < 128}.  Lists per row:
+__host__ __device__ __forceinline__ int gemm_top_parts(int n_tiles) { return (n_tiles % 2 == 0) ? 2 : 1; }
+__host__ __device__ __forceinline__ int gemm_top_lists(int N) { return 2 * gemm_top_parts(N / 256); }
 
 struct GemmArgs {
   const __nv_bfloat16* a;  // [M][K]
@@ -28,7 +36,7 @@ struct GemmArgs {
   float* c_f32;            // kStoreF32
   __nv_bfloat16* c_bf16;   // kBiasReluBF16, kMaskBF16, kStoreBF16
   const __nv_bfloat16* aux;  // kMaskBF16: [M][N]
-  uint32_t* top_keys;      // kTop8: [M][N / 128][8], descending
+  uint32_t* top_keys;      // kTop8: [M][N / 128][8]; kTop8Row: [M][gemm_top_lists(N)][8]; descending
   int* err;                // device error word
 };
 

@@ -780,8 +780,8 @@ static int search_impl(orbx_ctx* ctx, orbx_learned* L, const uint8_t* d_q, int n
   k_bits_pm1_bf16<<<grid1((long long)rows * 32, 256), 256, 0, s>>>(d_q, nq, nullptr, rows, L->xq);
   if (mlp) {
     LCHK(gemm(s, err, L->xq, L->w1b, rows, L->Hd, 256, L->b1, kBiasReluBF16, 1, nullptr, L->hq, nullptr, nullptr));
-    LCHK(gemm(s, err, L->hq, L->w2b, rows, C, L->Hd, L->b2, kTop8, 1, nullptr, nullptr, nullptr, L->keys));
-    k_select_probes<<<grid1((long long)nq * 32, 256), 256, 0, s>>>(L->keys, nq, C / 128, L->p.n_probe, thr,
+    LCHK(gemm(s, err, L->hq, L->w2b, rows, C, L->Hd, L->b2, kTop8Row, 1, nullptr, nullptr, nullptr, L->keys));
+    k_select_probes<<<grid1((long long)nq * 32, 256), 256, 0, s>>>(L->keys, nq, gemm_top_lists(C), L->p.n_probe, thr,
                                                                     L->ivf_offsets, L->probes, L->margin, L->counts,
                                                                     L->partial, per_slot);
   } else {
@@ -1221,10 +1221,11 @@ ORBX_API int orbx_learned_destroy(orbx_learned* L) {
 
 ORBX_API int orbx_gemm_bf16(orbx_ctx* ctx, const void* d_a, const void* d_b, int M, int N, int K, const float* d_bias,
                             int mode, int splits, void* d_c, const void* d_aux) {
-  if (!ctx || !d_a || !d_b || !d_c || M < 0 || N < 0 || K < 0 || mode < kStoreF32 || mode > kTop8 || splits < 1)
+  if (!ctx || !d_a || !d_b || !d_c || M < 0 || N < 0 || K < 0 || mode < kStoreF32 || mode > kTop8Row || splits < 1)
     return ORBX_ERR_ARG;
   if (mode == kMaskBF16 && !d_aux) return ORBX_ERR_ARG;
-  if (M % 128 || N % 256 || (K % (64 * splits)) || (splits > 1 && mode != kStoreF32) || (mode == kTop8 && N > 4096))
+  if (M % 128 || N % 256 || (K % (64 * splits)) || (splits > 1 && mode != kStoreF32) ||
+      ((mode == kTop8 || mode == kTop8Row) && N > 4096))
     return ORBX_ERR_SIZE;
   Guard g(ctx_device(ctx));
   LCHK(gemm(ctx_stream(ctx), ctx_err(ctx), static_cast<const bf16*>(d_a), static_cast<const bf16*>(d_b), M, N, K,

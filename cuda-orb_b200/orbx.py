@@ -160,7 +160,12 @@ def ocv_detect_and_compute(ctx, img, w, h, params=None, cap=None):
 PROPOSAL_MLP, PROPOSAL_LSH = 0, 1
 RERANK_TENSOR, RERANK_POPC = 0, 1
 INIT_CENTROIDS, INIT_RANDOM = 0, 1
-GEMM_F32, GEMM_BIAS_RELU_BF16, GEMM_MASK_BF16, GEMM_BF16, GEMM_TOP8 = 0, 1, 2, 3, 4
+GEMM_F32, GEMM_BIAS_RELU_BF16, GEMM_MASK_BF16, GEMM_BF16, GEMM_TOP8, GEMM_TOP8_ROW = 0, 1, 2, 3, 4, 5
+
+
+def gemm_top_lists(n):
+    """Key lists per row of GEMM_TOP8_ROW for n columns."""
+    return 4 if (n // 256) % 2 == 0 else 2
 
 
 class LearnedParams(ctypes.Structure):
@@ -541,6 +546,8 @@ def gemm_bf16(ctx, a, b, mode=GEMM_F32, bias=None, splits=1, aux=None):
         out = torch.empty((splits, M, N) if splits > 1 else (M, N), dtype=torch.float32, device=a.device)
     elif mode == GEMM_TOP8:
         out = torch.empty((M, N // 128, 8), dtype=torch.int32, device=a.device)
+    elif mode == GEMM_TOP8_ROW:
+        out = torch.empty((M, gemm_top_lists(N), 8), dtype=torch.int32, device=a.device)
     else:
         out = torch.empty((M, N), dtype=torch.bfloat16, device=a.device)
     _check(lib().orbx_gemm_bf16(ctx.h, _ptr(a), _ptr(b), M, N, K, _ptr(bias), mode, splits, _ptr(out), _ptr(aux)),

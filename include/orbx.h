@@ -364,7 +364,12 @@ ORBX_API int orbx_learned_destroy(orbx_learned* index);
  * mode 0: fp32 C (+ bias; with splits > 1, splits partial sums [splits][M][N]
  * and no bias); 1: bf16 relu(C + bias); 2: bf16 C where aux [M][N] > 0;
  * 3: bf16 C + bias; 4: per row and 128 columns the 8 largest C + bias as
- * packed keys, uint32 [M][N / 128][8].  Asynchronous. */
+ * packed keys, uint32 [M][N / 128][8]; 5: per row the 8 largest C + bias of
+ * each of L column sets, uint32 [M][L][8] with L = 4 when N / 256 is even, else
+ * 2 (set 2p + h: columns 256 t + 128 h + c, c < 128, for the tiles t of the
+ * p-th half of the N / 256 tiles, or of all of them when L = 2).  Keys are the
+ * logit's order-preserving bits with the low 12 replaced by 4095 - column, in
+ * descending order; N <= 4096 for modes 4 and 5.  Asynchronous. */
 ORBX_API int orbx_gemm_bf16(orbx_ctx* ctx, const void* d_a, const void* d_b, int M, int N, int K, const float* d_bias,
                             int mode, int splits, void* d_c, const void* d_aux);
 

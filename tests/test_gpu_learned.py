@@ -106,6 +106,41 @@ def test_gemm_top8(ctx):
         assert np.all(np.diff(k[:, t, :].astype(np.int64), axis=1) < 0)
 
 
+def _top8_row_sets(N):
+    """Column sets of GEMM_TOP8_ROW's lists for N columns."""
+    tiles = N // 256
+    parts = 2 if tiles % 2 == 0 else 1
+    tpi = tiles // parts
+    return [np.concatenate([np.arange(256 * t + 128 * h, 256 * t + 128 * h + 128) for t in range(p * tpi, (p + 1) * tpi)])
+            for p in range(parts) for h in range(2)]
+
+
+@pytest.mark.parametrize("N", [1024, 768, 4096])
+def test_gemm_top8_row(ctx, N):
+    g = torch.Generator().manual_seed(17)
+    M, K = 384, 512
+    a, b = bf16_tensor((M, K), g), bf16_tensor((N, K), g)
+    bias = torch.randn(N, generator=g).cuda()
+    keys = orbx.gemm_bf16(ctx, a, b, orbx.GEMM_TOP8_ROW, bias=bias)
+    ctx.sync()
+    ref = (a.float() @ b.float().T + bias).cpu().numpy()
+    k = keys.cpu().numpy().astype(np.uint32)  # (M, lists, 8)
+    sets = _top8_row_sets(N)
+    assert k.shape == (M, len(sets), 8) == (M, orbx.gemm_top_lists(N), 8)
+    cols = 4095 - (k & 0xFFF).astype(np.int64)
+    for l, cs in enumerate(sets):
+        assert np.all(np.isin(cols[:, l, :], cs))
+        kth = np.sort(ref[:, cs], axis=1)[:, -8]
+        got = np.take_along_axis(ref, cols[:, l, :], axis=1)
+        assert np.all(got >= kth[:, None] - 1e-3 * np.abs(kth[:, None]) - 1e-3)
+        assert np.all(np.diff(k[:, l, :].astype(np.int64), axis=1) < 0)
+    # the best 8 keys over all lists are the row's 8 largest logits
+    allk = np.sort(k.reshape(M, -1).astype(np.int64), axis=1)[:, ::-1][:, :8]
+    top_cols = 4095 - (allk & 0xFFF)
+    kth = np.sort(ref, axis=1)[:, -8]
+    assert np.all(np.take_along_axis(ref, top_cols, axis=1) >= kth[:, None] - 1e-3 * np.abs(kth[:, None]) - 1e-3)
+
+
 @pytest.fixture(scope="module")
 def small_index(ctx):
     db, q = clustered(16384, 4096, seed=1)
