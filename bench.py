@@ -55,6 +55,8 @@ def parse_args(argv=None):
     p.add_argument("--impl", choices=["orbx", "reference"], default="orbx")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-match-bench", action="store_true")
+    p.add_argument("--no-learned-bench", action="store_true",
+                   help="pair workload: skip the learned-proposal summary (about 20 s on rank 0)")
     p.add_argument("--workload", choices=["pair1080", "match65536", "batch64", "learned"], default="pair1080",
                    help="pair1080: the 1920x1080 pair (default); match65536: k=2 matching only; "
                         "batch64: 64 pairs of mixed resolution and caps in one batch; "
@@ -737,7 +739,7 @@ def calibrate_fallback(margin, dstar, correct, target, max_dists=None):
     return best
 
 
-def run_learned_workload(args, world, rank, local):
+def run_learned_workload(args, world, rank, local, with_cpu=True):
     """Learned-proposal k = 2 search: 131072 queries against 1048576 database
     rows, all pipeline descriptors of synthetic 1024 x 1024 images (queries from
     warped copies).  The MLP index is built and trained on the GPU, its fallback
@@ -873,7 +875,7 @@ def run_learned_workload(args, world, rank, local):
     t_exact = statistics.median(exact_ms)
     t_learned = sum(learned_ms) / len(learned_ms)
     pairs = float(nq) * float(ndb)
-    cpu = cpu_baseline_knn2(q.cpu().numpy(), db.cpu().numpy())
+    cpu = cpu_baseline_knn2(q.cpu().numpy(), db.cpu().numpy()) if with_cpu else None
     phases = dict(zip(["proposal", "probe_lists", "rerank", "merge", "fallback"], prof.tolist()))
     # Roofline of the dominant phase.  The fallback is exact int8 tensor-core matching
     # (512 ops per pair, bound: twice the measured bf16 rate); the proposal is the MLP
@@ -932,6 +934,16 @@ def run_learned_workload(args, world, rank, local):
             "gpu_launches": 12 * steps, "clocks": clocks}
 
 
+def learned_summary(args, world, rank, local):
+    """The learned-proposal workload (131072 x 1048576 k = 2 search at recall@1
+    >= 0.99) reduced to its headline figures, for the default bench line."""
+    la = parse_args(["--workload", "learned", "--steps", str(min(args.steps, 20)), "--warmup", "3"])
+    r = run_learned_workload(la, world, rank, local, with_cpu=False)
+    keep = ("metric", "value", "unit", "ms_per_step", "recall_at_1", "recall_target", "fallback_fraction",
+            "speedup_vs_exact", "exact", "phases_ms", "rerank", "roofline", "ablation", "config", "clocks")
+    return {k: r[k] for k in keep if k in r}
+
+
 def cpu_baseline_knn2(q, db, budget_s=10.0):
     """Exact k = 2 brute force of the oracle's C port (one thread) on a sample of queries."""
     from oracle import oracle as O
@@ -975,6 +987,8 @@ def main(argv=None):
         res = run_reference(args, world, rank, local)
     else:
         res, imgs = run_orbx(args, world, rank, local)
+        if rank == 0 and not args.no_learned_bench:
+            res["learned_proposal"] = learned_summary(args, world, rank, local)
         if rank == 0 and not args.no_cpu_baseline:
             res["cpu_baseline"] = cpu_baseline_port(*imgs)
             res["cpu_opencv"] = cpu_baseline_opencv(*imgs)
