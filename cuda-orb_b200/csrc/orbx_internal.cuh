@@ -144,6 +144,7 @@ struct RerankImmaArgs {
   const uint8_t* pad_desc;   // [pad_rows][32] packed rows of the padded lists (padding zero), 16-byte aligned
   uint2* partial;            // [slots][kRrGroups] top-2 keys
   int* item_counter;         // zero at launch: the blocks claim items from it
+  uint32_t* q_bound;         // [nq] 0xFFFFFFFF at launch: per query the least second-best key any item has found
   int* err;
 };
 cudaError_t launch_rerank_imma(const RerankImmaArgs& a, int max_items, cudaStream_t s);

@@ -195,6 +195,7 @@ struct orbx_learned {
   uint2* partial = nullptr;
   int *fb_list = nullptr, *fb_count = nullptr;
   int* rr_counter = nullptr;
+  uint32_t* rr_bound = nullptr;
   uint8_t* fb_q = nullptr;
   uint32_t* fb_d = nullptr;
   int32_t* fb_i = nullptr;
@@ -616,6 +617,7 @@ int ensure_search(orbx_learned* L, int nq) {
   LCHK(a.alloc(&L->fb_list, (size_t)nq));
   LCHK(a.alloc(&L->fb_count, 1));
   LCHK(a.alloc(&L->rr_counter, 1));
+  LCHK(a.alloc(&L->rr_bound, (size_t)nq));
   LCHK(a.alloc(&L->fb_q, (size_t)nq * 32));
   LCHK(a.alloc(&L->fb_d, (size_t)nq * 2));
   LCHK(a.alloc(&L->fb_i, (size_t)nq * 2));
@@ -807,8 +809,10 @@ static int search_impl(orbx_ctx* ctx, orbx_learned* L, const uint8_t* d_q, int n
     ra.pad_desc = L->pad_desc;
     ra.partial = L->partial;
     ra.item_counter = L->rr_counter;
+    ra.q_bound = L->rr_bound;
     ra.err = err;
     LCHK(cudaMemsetAsync(L->rr_counter, 0, sizeof(int), s));
+    LCHK(cudaMemsetAsync(L->rr_bound, 0xFF, sizeof(uint32_t) * (size_t)nq, s));
     LCHK(launch_rerank_imma(ra, (int)items_max, s));
   } else {
     k_rerank<<<items_max, kRerankQ, 0, s>>>(d_q, L->list, L->offsets, L->items, C, L->ivf_desc, L->ivf_members,

@@ -808,6 +808,8 @@ __global__ void __launch_bounds__(kRrThreads, 1) k_rerank_imma(RerankImmaArgs a)
           break;
         }
         tc_fence_after();
+        // the query's bound from its other items so far (any stale value is a valid, looser bound)
+        const uint32_t gb = slot >= 0 ? __ldcg(a.q_bound + (slot >> 3)) : kNoKeyShared;
         const uint32_t taddr = tmem_base + ((uint32_t)(quarter * 32) << 16) + acc * (uint32_t)kIBN + colgrp * 64;
 #pragma unroll 1
         for (int c = 0; c < 2; c++) {
@@ -833,7 +835,11 @@ __global__ void __launch_bounds__(kRrThreads, 1) k_rerank_imma(RerankImmaArgs a)
           // The cluster's list is in increasing database index and the columns
           // arrive in list order, so only a strictly larger dot' (a strictly
           // smaller distance) than the current second best's can enter.
-          const int thr = (k2 == kNoKeyShared) ? kMaskedDot : pc - (int)(k2 >> kIdxBitsShared);
+          int thr = (k2 == kNoKeyShared) ? kMaskedDot : pc - (int)(k2 >> kIdxBitsShared);
+          // another item of the same query may already hold a closer second best:
+          // columns farther than it cannot reach the query's top two (equal
+          // distances stay, their index decides)
+          if (gb != kNoKeyShared) thr = max(thr, pc - (int)(gb >> kIdxBitsShared) - 1);
           if (__any_sync(0xffffffffu, m > thr)) {
             // the chunk's best two on local keys (dot' << 5 | 31 - column): ties keep the lower column
             int a1 = INT_MIN, a2 = INT_MIN;
@@ -855,7 +861,11 @@ __global__ void __launch_bounds__(kRrThreads, 1) k_rerank_imma(RerankImmaArgs a)
         }
       }
       if (!ok) break;
-      if (slot >= 0) a.partial[(size_t)slot * kRrGroups + colgrp] = make_uint2(k1, k2);
+      if (slot >= 0) {
+        a.partial[(size_t)slot * kRrGroups + colgrp] = make_uint2(k1, k2);
+        // two distinct rows at or below k2: the query's final second best is no worse
+        if (k2 != kNoKeyShared) atomicMin(a.q_bound + (slot >> 3), k2);
+      }
     }
     if (!ok) {
       *s_abort = 1;
