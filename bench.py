@@ -63,6 +63,9 @@ def parse_args(argv=None):
                         "learned: learned-proposal k=2 search, 131072 queries x 1048576 database rows")
     p.add_argument("--learned-spill", type=int, default=12,
                    help="learned: clusters each database row is listed in (1..16)")
+    p.add_argument("--learned-epochs", type=int, default=3, help="learned: training epochs")
+    p.add_argument("--learned-labels", choices=["nearest", "listed"], default="listed",
+                   help="learned: training target, the nearest row's cluster or all clusters it is listed in")
     p.add_argument("--learned-scale", type=float, default=1.0,
                    help="learned: fraction of the database / query / training sizes (tests use < 1)")
     p.add_argument("--match-mode", choices=["imma", "popc"], default="imma")
@@ -785,7 +788,9 @@ def run_learned_workload(args, world, rank, local, with_cpu=True):
         cal_d, _ = orbx.knn2(ctx, cal, db, orbx.MATCH_IMMA)
         cal_d1 = cal_d[:, 0].cpu().numpy()
         # build: clustering + labels + training on the GPU
-        lp = orbx.learned_params(synth_train=sizes["train"], flip_lo=0.08, flip_hi=0.2, spill=args.learned_spill)
+        label_mode = orbx.LABEL_LISTED if args.learned_labels == "listed" else orbx.LABEL_NEAREST
+        lp = orbx.learned_params(synth_train=sizes["train"], flip_lo=0.08, flip_hi=0.2, spill=args.learned_spill,
+                                 label_mode=label_mode, epochs=args.learned_epochs)
         tb = time.time()
         index = orbx.LearnedIndex(ctx, db, train, lp)
         build_wall_s = time.time() - tb
@@ -862,6 +867,13 @@ def run_learned_workload(args, world, rank, local, with_cpu=True):
         cen = orbx.LearnedIndex(ctx, db, train, orbx.learned_params(epochs=0, spill=args.learned_spill))
         recall_centroid = float(np.mean(no_fallback(cen, q)[0] == ex_d1))
         cen.close()
+        # the other training target, same data and schedule
+        other = orbx.LABEL_NEAREST if label_mode == orbx.LABEL_LISTED else orbx.LABEL_LISTED
+        alt = orbx.LearnedIndex(ctx, db, train, orbx.learned_params(synth_train=sizes["train"], flip_lo=0.08,
+                                                                    flip_hi=0.2, spill=args.learned_spill,
+                                                                    label_mode=other, epochs=args.learned_epochs))
+        recall_other_labels = float(np.mean(no_fallback(alt, q)[0] == ex_d1))
+        alt.close()
         # non-learned proposal at the same probe budget: random-projection buckets
         lsh = orbx.LearnedIndex(ctx, db, None, orbx.learned_params(proposal=orbx.PROPOSAL_LSH, lsh_bits=12,
                                                                     n_clusters=4096))
@@ -911,6 +923,7 @@ def run_learned_workload(args, world, rank, local, with_cpu=True):
             "config": {"workload": "learned-proposal k=2 search", "queries": nq, "database": ndb,
                        "train_rows": train.shape[0], "calibration_rows": cal.shape[0],
                        "n_clusters": 4096, "hidden": 512, "n_probe": 8, "spill": args.learned_spill,
+                       "labels": args.learned_labels, "epochs": args.learned_epochs,
                        "rerank": "int8 tcgen05", "l2": "flushed before every step"},
             "recall_at_1": recall, "recall_target": LEARNED_RECALL,
             "fallback_rule": {"margin_below": tau_m, "distance_above": tau_d},
@@ -919,6 +932,8 @@ def run_learned_workload(args, world, rank, local, with_cpu=True):
             "speedup_vs_exact": t_exact / t_learned,
             "operating_points": [dict(c, speedup_vs_exact=t_exact / c["ms"]) for c in curve],
             "ablation": {"recall_mlp_no_fallback": recall_mlp_only,
+                         "labels": args.learned_labels, "epochs": args.learned_epochs,
+                         "recall_mlp_other_labels_no_fallback": recall_other_labels,
                          "recall_nearest_centroid_no_fallback": recall_centroid,
                          "recall_lsh_no_fallback": recall_lsh,
                          "lsh_ms": statistics.median(lsh_ms), "lsh": "12 random-projection bits, 8 probes"},

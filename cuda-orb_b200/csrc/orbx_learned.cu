@@ -79,20 +79,23 @@ __global__ void __launch_bounds__(256) k_bits_pm1_bf16_t(const uint8_t* __restri
 }
 
 // ---------------------------------------------------------------- training
-// One warp per row of C logits (C % 128 == 0).  Rows r < n with label >= 0 get
-// dL = (softmax - onehot) * grad_scale, loss[r] = -log softmax[label] and
-// correct[r] = (argmax == label); other rows get dL = 0, loss 0, correct 0.
+// One warp per row of C logits (C % 128 == 0) with a set of S labels
+// labels[r * S ..] (-1 entries unused; S = 1 is the usual one-hot target).
+// With P = the softmax mass on the set, rows r < n with a label get
+// loss[r] = -log P, dL = (softmax - softmax * [c in set] / P) * grad_scale and
+// correct[r] = (argmax in the set); other rows get dL = 0, loss 0, correct 0.
 __global__ void __launch_bounds__(256) k_softmax_xent(const float* __restrict__ logits, const int* __restrict__ labels,
-                                                      int n, int rows, int C, float grad_scale,
+                                                      int S, int n, int rows, int C, float grad_scale,
                                                       __nv_bfloat16* __restrict__ dL, float* __restrict__ loss,
                                                       int* __restrict__ correct) {
   const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
   if (warp >= rows) return;
   const int r = warp;
-  const int label = r < n ? labels[r] : -1;
+  const int mine = (r < n && lane < S) ? labels[(size_t)r * S + lane] : -1;
+  const bool any = __any_sync(0xffffffffu, mine >= 0);
   uint2* drow = reinterpret_cast<uint2*>(dL + (size_t)r * C);
-  if (label < 0) {
+  if (!any) {
     for (int c = lane; c < C / 4; c += 32) drow[c] = make_uint2(0, 0);
     if (lane == 0) {
       loss[r] = 0.f;
@@ -127,19 +130,26 @@ __global__ void __launch_bounds__(256) k_softmax_xent(const float* __restrict__ 
 #pragma unroll
   for (int o = 16; o; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
   const float inv = 1.0f / sum;
+  // the set's unnormalised mass
+  const float em = mine >= 0 ? __expf(logits[(size_t)r * C + mine] - mx) : 0.f;
+  float es = em;
+#pragma unroll
+  for (int o = 16; o; o >>= 1) es += __shfl_xor_sync(0xffffffffu, es, o);
   for (int c = lane; c < C / 4; c += 32) {
     const float4 v = row[c];
-    float p[4] = {__expf(v.x - mx) * inv, __expf(v.y - mx) * inv, __expf(v.z - mx) * inv, __expf(v.w - mx) * inv};
-#pragma unroll
-    for (int e = 0; e < 4; e++)
-      if (4 * c + e == label) p[e] -= 1.0f;
+    const float p[4] = {__expf(v.x - mx) * inv, __expf(v.y - mx) * inv, __expf(v.z - mx) * inv,
+                        __expf(v.w - mx) * inv};
     const __nv_bfloat162 a = __floats2bfloat162_rn(p[0] * grad_scale, p[1] * grad_scale);
     const __nv_bfloat162 b = __floats2bfloat162_rn(p[2] * grad_scale, p[3] * grad_scale);
     drow[c] = make_uint2(*reinterpret_cast<const uint32_t*>(&a), *reinterpret_cast<const uint32_t*>(&b));
   }
+  __syncwarp();
+  // label columns: p - p / P = p - e / es
+  if (mine >= 0) dL[(size_t)r * C + mine] = __float2bfloat16_rn((em * inv - em / es) * grad_scale);
+  const unsigned hit = __ballot_sync(0xffffffffu, mine == amax);
   if (lane == 0) {
-    loss[r] = logf(sum) + mx - logits[(size_t)r * C + label];
-    correct[r] = amax == label ? 1 : 0;
+    loss[r] = logf(sum) - logf(es);
+    correct[r] = hit ? 1 : 0;
   }
 }
 
@@ -467,9 +477,12 @@ __global__ void k_gather_rows(const uint8_t* __restrict__ db, const int* __restr
 }
 
 // out[j] = in[idx[j]]
-__global__ void k_gather_i32(const int* __restrict__ in, const int* __restrict__ idx, int n, int* __restrict__ out) {
-  const int j = blockIdx.x * blockDim.x + threadIdx.x;
-  if (j < n) out[j] = in[idx[j]];
+__global__ void k_gather_i32(const int* __restrict__ in, const int* __restrict__ idx, int n, int width,
+                             int* __restrict__ out) {
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (long long)n * width) return;
+  const int i = (int)(t / width), j = (int)(t - (long long)i * width);
+  out[t] = in[(size_t)idx[i] * width + j];
 }
 
 __global__ void k_count(const int* __restrict__ assign, int n, int* __restrict__ counts) {
@@ -508,12 +521,15 @@ __global__ void __launch_bounds__(256) k_accum_stats(const float* __restrict__ l
 }
 
 // labels[i] = assign[nearest database row of training row i]
-__global__ void k_labels(const int32_t* __restrict__ idx2, int n, const int* __restrict__ assign,
-                         int* __restrict__ labels) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
+// Training labels: row i's S labels are the first S clusters row_sets lists
+// for its exact nearest database row (its nearest cluster when S = 1).
+__global__ void k_labels(const int32_t* __restrict__ idx2, int n, const int* __restrict__ row_sets, int set_width,
+                         int S, int* __restrict__ labels) {
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (long long)n * S) return;
+  const int i = (int)(t / S), j = (int)(t - (long long)i * S);
   const int nn = idx2[2 * i];
-  labels[i] = nn >= 0 ? assign[nn] : -1;
+  labels[t] = nn >= 0 ? row_sets[(size_t)nn * set_width + j] : -1;
 }
 
 // ---------------------------------------------------------------- search

@@ -81,8 +81,8 @@ struct AdamStep {
 // orbx_learned.cu
 __global__ void k_bits_pm1_bf16(const uint8_t* bits, int n, const int* d_n, int rows, __nv_bfloat16* out);
 __global__ void k_bits_pm1_bf16_t(const uint8_t* bits, int n, int rows, __nv_bfloat16* out);
-__global__ void k_softmax_xent(const float* logits, const int* labels, int n, int rows, int C, float grad_scale,
-                               __nv_bfloat16* dL, float* loss, int* correct);
+__global__ void k_softmax_xent(const float* logits, const int* labels, int S, int n, int rows, int C,
+                               float grad_scale, __nv_bfloat16* dL, float* loss, int* correct);
 __global__ void k_transpose_bf16(const __nv_bfloat16* in, int R, int C, __nv_bfloat16* out);
 __global__ void k_colsum_bf16(const __nv_bfloat16* in, int R, int C, int rows_per_chunk, float* partial);
 __global__ void k_adam(float* w, float* m, float* v, const float* partial, int nsplit, long long n,
@@ -94,10 +94,10 @@ __global__ void k_scatter_members(const int* assign, int n, int* cursor, int* me
 __global__ void k_majority(const uint8_t* db, int n, const int* members, const int* offsets, uint8_t* centroids,
                            unsigned long long seed, int iter);
 __global__ void k_gather_rows(const uint8_t* db, const int* members, int n, uint8_t* out);
-__global__ void k_gather_i32(const int* in, const int* idx, int n, int* out);
+__global__ void k_gather_i32(const int* in, const int* idx, int n, int width, int* out);
 __global__ void k_count(const int* assign, int n, int* counts);
 __global__ void k_accum_stats(const float* loss, const int* correct, int n, float* acc);
-__global__ void k_labels(const int32_t* idx2, int n, const int* assign, int* labels);
+__global__ void k_labels(const int32_t* idx2, int n, const int* row_sets, int set_width, int S, int* labels);
 __global__ void k_select_probes(const uint32_t* keys, int nq, int lists, int n_probe, float margin_thr,
                                 const int* ivf_offsets, int* probes, float* margin, int* probe_counts,
                                 uint2* partial, int per_slot);

@@ -168,6 +168,9 @@ struct orbx_learned {
   orbx_learned_params p{};
   int ndb = 0, C = 0, Hd = 0;
   int n_entries = 0;  // cluster list entries (ndb, or up to spill * ndb)
+  // during a build only: each database row's listed clusters, nearest first
+  int* row_sets = nullptr;
+  int set_width = 1;
   Arena keep;
   uint8_t* db = nullptr;
   int8_t* db_pm1 = nullptr;
@@ -206,14 +209,14 @@ struct orbx_learned {
 
 namespace {
 
-int train_alloc(orbx_learned* L, TrainBufs& T, int B) {
+int train_alloc(orbx_learned* L, TrainBufs& T, int B, int S = 1) {
   const int C = L->C, Hd = L->Hd;
   T.B = B;
   T.s2 = pick_splits((C / 128) * (Hd / 256), B / 64);
   T.s1 = pick_splits((Hd / 128) * (256 / 256), B / 64);
   T.chunks = B / 128;
   LCHK(T.a.alloc(&T.xbits, (size_t)B * 32));
-  LCHK(T.a.alloc(&T.lbl, (size_t)B));
+  LCHK(T.a.alloc(&T.lbl, (size_t)B * S));
   LCHK(T.a.alloc(&T.X, (size_t)B * 256));
   LCHK(T.a.alloc(&T.XT, (size_t)B * 256));
   LCHK(T.a.alloc(&T.H, (size_t)B * Hd));
@@ -235,13 +238,14 @@ int train_alloc(orbx_learned* L, TrainBufs& T, int B) {
 // Forward and backward over the B rows of xbits / lbl: leaves the loss per row
 // and the gradients as split partial sums (P1 [s1][Hd][256], Pb1 [chunks][Hd],
 // P2 [s2][C][Hd], Pb2 [chunks][C]).
-int forward_backward(orbx_learned* L, TrainBufs& T, const uint8_t* xbits, const int* lbl, cudaStream_t s, int* err) {
+int forward_backward(orbx_learned* L, TrainBufs& T, const uint8_t* xbits, const int* lbl, int S, cudaStream_t s,
+                     int* err) {
   const int B = T.B, C = L->C, Hd = L->Hd;
   k_bits_pm1_bf16<<<grid1((long long)B * 32, 256), 256, 0, s>>>(xbits, B, nullptr, B, T.X);
   k_bits_pm1_bf16_t<<<B / 64, 256, 0, s>>>(xbits, B, B, T.XT);
   LCHK(gemm(s, err, T.X, L->w1b, B, Hd, 256, L->b1, kBiasReluBF16, 1, nullptr, T.H, nullptr, nullptr));
   LCHK(gemm(s, err, T.H, L->w2b, B, C, Hd, L->b2, kStoreF32, 1, T.logits, nullptr, nullptr, nullptr));
-  k_softmax_xent<<<grid1((long long)B * 32, 256), 256, 0, s>>>(T.logits, lbl, B, B, C, 1.0f / (float)B, T.dL, T.loss,
+  k_softmax_xent<<<grid1((long long)B * 32, 256), 256, 0, s>>>(T.logits, lbl, S, B, B, C, 1.0f / (float)B, T.dL, T.loss,
                                                                 T.correct);
   k_transpose_bf16<<<dim3(C / 32, B / 32), dim3(32, 8), 0, s>>>(T.dL, B, C, T.dLT);
   k_transpose_bf16<<<dim3(Hd / 32, B / 32), dim3(32, 8), 0, s>>>(T.H, B, Hd, T.HT);
@@ -263,6 +267,7 @@ int check_params(const orbx_learned_params* p) {
   if (p->proposal != ORBX_PROPOSAL_MLP && p->proposal != ORBX_PROPOSAL_LSH) return ORBX_ERR_ARG;
   if (p->n_probe < 1 || p->n_probe > kTopK) return ORBX_ERR_ARG;
   if (p->rerank != ORBX_RERANK_TENSOR && p->rerank != ORBX_RERANK_POPC) return ORBX_ERR_ARG;
+  if (p->label_mode != ORBX_LABEL_NEAREST && p->label_mode != ORBX_LABEL_LISTED) return ORBX_ERR_ARG;
   if (p->proposal == ORBX_PROPOSAL_LSH) {
     if (p->lsh_bits < 8 || p->lsh_bits > 12 || p->n_clusters != (1 << p->lsh_bits)) return ORBX_ERR_ARG;
   } else {
@@ -309,6 +314,11 @@ int spill_lists(orbx_learned* L, const int32_t* idx, int per_row, int* counts, i
   k_stable_hist<<<nb, 256, sizeof(int) * C, s>>>(idx, total, C, hist);
   k_stable_scan<<<grid1(C, 256), 256, 0, s>>>(hist, nb, C, L->ivf_offsets);
   k_stable_scatter<<<nb, 32, sizeof(int) * C, s>>>(idx, total, per_row, C, hist, L->ivf_members);
+  if (L->row_sets) {
+    // a build keeps each row's clusters for the training labels
+    LCHK(cudaMemcpyAsync(L->row_sets, idx, sizeof(int) * (size_t)total, cudaMemcpyDeviceToDevice, s));
+    L->set_width = per_row;
+  }
   return read_list_stats(L, counts, s);
 }
 
@@ -509,7 +519,8 @@ int alloc_weights(orbx_learned* L, Arena& a, float** m, float** v) {
   return ORBX_OK;
 }
 
-int train_mlp(orbx_learned* L, const uint8_t* d_train, int ntrain, const int* labels, cudaStream_t s, int* err) {
+int train_mlp(orbx_learned* L, const uint8_t* d_train, int ntrain, const int* labels, int S, cudaStream_t s,
+              int* err) {
   const int Hd = L->Hd, C = L->C, B = L->p.batch;
   Arena a;
   float *m, *v;
@@ -535,7 +546,7 @@ int train_mlp(orbx_learned* L, const uint8_t* d_train, int ntrain, const int* la
   const int epochs = steps > 0 ? L->p.epochs : 0;
   if (epochs == 0) return ORBX_OK;
   TrainBufs T;
-  LRC(train_alloc(L, T, B));
+  LRC(train_alloc(L, T, B, S));
   int* d_perm;
   float* acc;
   LCHK(a.alloc(&d_perm, ntrain));
@@ -555,8 +566,8 @@ int train_mlp(orbx_learned* L, const uint8_t* d_train, int ntrain, const int* la
     for (int st = 0; st < steps; st++) {
       const int* idx = d_perm + (size_t)st * B;
       k_gather_rows<<<grid1(2ll * B, 256), 256, 0, s>>>(d_train, idx, B, T.xbits);
-      k_gather_i32<<<grid1(B, 256), 256, 0, s>>>(labels, idx, B, T.lbl);
-      LRC(forward_backward(L, T, T.xbits, T.lbl, s, err));
+      k_gather_i32<<<grid1((long long)B * S, 256), 256, 0, s>>>(labels, idx, B, S, T.lbl);
+      LRC(forward_backward(L, T, T.xbits, T.lbl, S, s, err));
       t++;
       AdamStep as{};
       as.lr = (float)(L->p.lr * 0.5 * (1.0 + cos(M_PI * (double)(t - 1) / (double)total)));
@@ -653,6 +664,7 @@ ORBX_API int orbx_learned_default_params(orbx_learned_params* p) {
   p->flip_lo = 0.05f;
   p->flip_hi = 0.2f;
   p->rerank = ORBX_RERANK_TENSOR;
+  p->label_mode = ORBX_LABEL_LISTED;
   return ORBX_OK;
 }
 
@@ -683,6 +695,7 @@ ORBX_API int orbx_learned_build(orbx_ctx* ctx, const orbx_learned_params* p, con
   auto events_free = [&]() {
     for (auto& e : ev) cudaEventDestroy(e);
   };
+  Arena build_tmp;  // buffers that live for the build only
   int rc = ORBX_OK;
   do {
     rc = alloc_core(L);
@@ -690,6 +703,10 @@ ORBX_API int orbx_learned_build(orbx_ctx* ctx, const orbx_learned_params* p, con
     cudaEventRecord(ev[0], s);
     rc = upload_db(L, d_db, s);
     if (rc) break;
+    if (build_tmp.alloc(&L->row_sets, (size_t)ndb * (p->proposal == ORBX_PROPOSAL_MLP ? std::max(1, p->spill) : 1))) {
+      rc = ORBX_ERR_NOMEM;
+      break;
+    }
     rc = p->proposal == ORBX_PROPOSAL_MLP ? cluster_kmeans(L, s, err) : cluster_lsh(L, s, err, true);
     if (rc) break;
     k_gather_rows<<<grid1(2ll * L->n_entries, 256), 256, 0, s>>>(L->db, L->ivf_members, L->n_entries, L->ivf_desc);
@@ -704,7 +721,8 @@ ORBX_API int orbx_learned_build(orbx_ctx* ctx, const orbx_learned_params* p, con
       int8_t* tq;
       uint8_t* rows;
       const int nt = ntrain + p->synth_train;
-      if (t.alloc(&labels, (size_t)nt) || t.alloc(&idx2, 2 * (size_t)nt) || t.alloc(&dist2, 2 * (size_t)nt) ||
+      const int S = p->label_mode == ORBX_LABEL_LISTED ? L->set_width : 1;
+      if (t.alloc(&labels, (size_t)nt * S) || t.alloc(&idx2, 2 * (size_t)nt) || t.alloc(&dist2, 2 * (size_t)nt) ||
           t.alloc(&tq, (size_t)imma_rows_q(nt) * 256) || t.alloc(&rows, (size_t)nt * 32)) {
         rc = ORBX_ERR_NOMEM;
         break;
@@ -723,9 +741,9 @@ ORBX_API int orbx_learned_build(orbx_ctx* ctx, const orbx_learned_params* p, con
       if (rc) break;
       rc = imma_knn(s, err, iw, rows, nt, nullptr, tq, false, L->db, ndb, L->db_pm1, true, dist2, idx2);
       if (rc) break;
-      k_labels<<<grid1(nt, 256), 256, 0, s>>>(idx2, nt, L->assign, labels);
+      k_labels<<<grid1((long long)nt * S, 256), 256, 0, s>>>(idx2, nt, L->row_sets, L->set_width, S, labels);
       cudaEventRecord(ev[2], s);
-      rc = train_mlp(L, rows, nt, labels, s, err);
+      rc = train_mlp(L, rows, nt, labels, S, s, err);
       if (rc) break;
     } else {
       cudaEventRecord(ev[2], s);
@@ -747,6 +765,8 @@ ORBX_API int orbx_learned_build(orbx_ctx* ctx, const orbx_learned_params* p, con
     cudaEventElapsedTime(&L->stats.build_ms[2], ev[2], ev[3]);
     cudaEventElapsedTime(&L->stats.build_ms[3], ev[0], ev[3]);
   } while (0);
+  cudaStreamSynchronize(s);
+  L->row_sets = nullptr;
   events_free();
   if (rc) {
     (void)cudaGetLastError();
@@ -936,7 +956,7 @@ ORBX_API int orbx_learned_export(orbx_ctx* ctx, const orbx_learned* L, int* h_as
 // A saved proposal, little-endian, every field 4-byte aligned:
 //   "ORBXLRN1", u32 version, u32 total bytes
 //   the orbx_learned_params fields in declaration order (seed as two u32, low
-//   word first, rerank last), then the orbx_learned_stats words
+//   word first, then rerank and label_mode), then the orbx_learned_stats words
 //   MLP: centroids [C][32] u8, W1 [Hd][256] bf16, b1 [Hd] f32, W2 [C][Hd] bf16,
 //        b2 [C] f32 (the weights search uses)
 //   LSH: projections [256][256] bf16
@@ -946,8 +966,8 @@ ORBX_API int orbx_learned_export(orbx_ctx* ctx, const orbx_learned* L, int* h_as
 namespace {
 
 constexpr char kSaveMagic[8] = {'O', 'R', 'B', 'X', 'L', 'R', 'N', '1'};
-constexpr uint32_t kSaveVersion = 2;
-constexpr size_t kSaveParamWords = 19;
+constexpr uint32_t kSaveVersion = 3;
+constexpr size_t kSaveParamWords = 20;
 constexpr size_t kSaveStatsWords = sizeof(orbx_learned_stats) / 4;
 static_assert(sizeof(orbx_learned_stats) == 4 * (4 + 64 + 64 + 4), "stats are whole 4-byte words");
 
@@ -992,7 +1012,8 @@ void put_params(uint8_t*& w, const orbx_learned_params& p) {
                                        (uint32_t)p.batch, fbits(p.lr), fbits(p.margin), (uint32_t)p.lsh_bits,
                                        (uint32_t)p.seed, (uint32_t)(p.seed >> 32), (uint32_t)p.max_distance,
                                        (uint32_t)p.spill, (uint32_t)p.init, (uint32_t)p.synth_train,
-                                       fbits(p.flip_lo), fbits(p.flip_hi), (uint32_t)p.rerank};
+                                       fbits(p.flip_lo), fbits(p.flip_hi), (uint32_t)p.rerank,
+                                       (uint32_t)p.label_mode};
   for (uint32_t x : v) put32(w, x);
 }
 orbx_learned_params get_params(const uint8_t*& r) {
@@ -1017,6 +1038,7 @@ orbx_learned_params get_params(const uint8_t*& r) {
   p.flip_lo = bitsf(v[16]);
   p.flip_hi = bitsf(v[17]);
   p.rerank = (int)v[18];
+  p.label_mode = (int)v[19];
   return p;
 }
 
@@ -1181,7 +1203,7 @@ ORBX_API int orbx_learned_gradients(orbx_ctx* ctx, orbx_learned* L, const uint8_
   int* err = ctx_err(ctx);
   TrainBufs T;
   LRC(train_alloc(L, T, n));
-  LRC(forward_backward(L, T, d_x, d_labels, s, err));
+  LRC(forward_backward(L, T, d_x, d_labels, 1, s, err));
   LCHK(cudaStreamSynchronize(s));
   const int Hd = L->Hd, C = L->C;
   auto reduce = [&](const float* d, int splits, size_t count, float* out) -> int {

@@ -159,6 +159,7 @@ def ocv_detect_and_compute(ctx, img, w, h, params=None, cap=None):
 
 PROPOSAL_MLP, PROPOSAL_LSH = 0, 1
 RERANK_TENSOR, RERANK_POPC = 0, 1
+LABEL_NEAREST, LABEL_LISTED = 0, 1
 INIT_CENTROIDS, INIT_RANDOM = 0, 1
 GEMM_F32, GEMM_BIAS_RELU_BF16, GEMM_MASK_BF16, GEMM_BF16, GEMM_TOP8, GEMM_TOP8_ROW = 0, 1, 2, 3, 4, 5
 
@@ -174,7 +175,8 @@ class LearnedParams(ctypes.Structure):
                 ("batch", ctypes.c_int), ("lr", ctypes.c_float), ("margin", ctypes.c_float),
                 ("lsh_bits", ctypes.c_int), ("seed", ctypes.c_ulonglong), ("max_distance", ctypes.c_int),
                 ("spill", ctypes.c_int), ("init", ctypes.c_int), ("synth_train", ctypes.c_int),
-                ("flip_lo", ctypes.c_float), ("flip_hi", ctypes.c_float), ("rerank", ctypes.c_int)]
+                ("flip_lo", ctypes.c_float), ("flip_hi", ctypes.c_float), ("rerank", ctypes.c_int),
+                ("label_mode", ctypes.c_int)]
 
 
 class LearnedStats(ctypes.Structure):

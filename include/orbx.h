@@ -289,7 +289,13 @@ typedef struct orbx_learned_params {
   float flip_lo;    /* per-row bit-flip probability of those rows, uniform in [flip_lo, flip_hi] */
   float flip_hi;
   int rerank;       /* ORBX_RERANK_TENSOR (int8 tensor cores) or ORBX_RERANK_POPC (XOR-popc) */
+  int label_mode;   /* training target: ORBX_LABEL_NEAREST or ORBX_LABEL_LISTED */
 } orbx_learned_params;
+/* ORBX_LABEL_NEAREST trains on the cluster of each training row's exact nearest
+ * database row (cross-entropy); ORBX_LABEL_LISTED on all `spill` clusters that
+ * row is listed in, maximising the softmax mass on that set, which is what a
+ * probe needs to find it. */
+enum { ORBX_LABEL_NEAREST = 0, ORBX_LABEL_LISTED = 1 };
 /* Exact rerank of the probed clusters: both forms give the same results. */
 enum { ORBX_RERANK_TENSOR = 0, ORBX_RERANK_POPC = 1 };
 /* ORBX_INIT_CENTROIDS starts the MLP as nearest-centroid scoring (hidden units

@@ -309,7 +309,7 @@ def test_spill_and_synthetic_rows_and_distance_rule(ctx):
 
 
 # ---------------------------------------------------------------- checkpoints
-CKPT_HEAD = 16 + 4 * (19 + 136)  # magic, version, size; 19 parameter words; the statistics words
+CKPT_HEAD = 16 + 4 * (20 + 136)  # magic, version, size; 20 parameter words; the statistics words
 
 
 def _ckpt_centroids(blob, C):
@@ -338,7 +338,7 @@ def test_checkpoint_round_trip(ctx, small_index):
     re = orbx.LearnedIndex.load(ctx, blob, tdb)
     try:
         for f in ("proposal", "n_clusters", "hidden", "n_probe", "spill", "seed", "max_distance", "lr", "margin",
-                  "rerank"):
+                  "rerank", "label_mode"):
             assert getattr(re.params, f) == getattr(p, f), f
         st, rst = idx.stats(), re.stats()
         assert rst["loss"] == st["loss"] and rst["largest_cluster"] == st["largest_cluster"]
@@ -354,7 +354,7 @@ def test_checkpoint_round_trip(ctx, small_index):
         # saving the loaded index gives the same checkpoint apart from its build times
         re.set_margin(p.margin)
         blob2 = re.save()
-        bt = 16 + 4 * (19 + 4 + 64 + 64)
+        bt = 16 + 4 * (20 + 4 + 64 + 64)
         assert len(blob2) == len(blob) and blob2[:bt] == blob[:bt] and blob2[bt + 16:-8] == blob[bt + 16:-8]
     finally:
         idx.set_margin(0.0)
@@ -526,5 +526,35 @@ def test_wide_spill_lists_and_recall(ctx, spill):
         finally:
             idx2.close()
         assert recall >= r2, (recall, r2)
+    finally:
+        idx.close()
+
+
+# ---------------------------------------------------------------- label sets
+def test_listed_labels(ctx):
+    """ORBX_LABEL_LISTED trains on the softmax mass of the nearest row's listed
+    clusters.  With spill 1 that set is the nearest cluster alone, so training
+    equals ORBX_LABEL_NEAREST weight for weight; with spill 4 the set loss
+    falls over the epochs and the search stays exact in the rows it scans."""
+    db, q = clustered(16384, 2048, seed=21)
+    tdb, tq = torch.from_numpy(db).cuda(), torch.from_numpy(q).cuda()
+    train = tq[:1024].contiguous()
+    base = dict(n_clusters=256, hidden=512, epochs=3, batch=512, kmeans_iters=6)
+    w = {}
+    for mode in (orbx.LABEL_NEAREST, orbx.LABEL_LISTED):
+        idx = orbx.LearnedIndex(ctx, tdb, train, orbx.learned_params(spill=1, label_mode=mode, **base))
+        try:
+            w[mode] = idx.export()
+        finally:
+            idx.close()
+    for k in ("w1", "b1", "w2", "b2"):
+        assert np.array_equal(w[orbx.LABEL_NEAREST][k], w[orbx.LABEL_LISTED][k]), k
+    idx = orbx.LearnedIndex(ctx, tdb, train, orbx.learned_params(spill=4, label_mode=orbx.LABEL_LISTED, **base))
+    try:
+        st = idx.stats()
+        assert st["loss"][-1] < st["loss"][0], st["loss"]
+        d, i, _, _ = idx.search(tq)
+        ctx.sync()
+        _check_consistent(q, db, d, i)
     finally:
         idx.close()
