@@ -41,8 +41,8 @@ POPC_PER_CLK_PER_SM = 16  # 32-bit population count results per clock per SM
 SMS = 148
 
 # DRAM bytes per launch measured by ncu (dram__bytes_read.sum + dram__bytes_write.sum,
-# cold cache) on the same workloads (profiles/pair1080_kernels.md,
-# profiles/knn2_65536_k_match_imma.md); kernels without a capture report None.
+# cold cache) on the same workloads (the committed ncu summaries of the 1080p
+# pair and of 65536 x 65536 matching); kernels without a capture report None.
 NCU_TRAFFIC = {"k_pyramid_blur": 4159744, "k_detect": 5656832, "k_nms": 1499392, "k_describe<2>": 5611008,
                "k_match_popc": 97792, "k_match_imma": 33602560}
 
