@@ -11,6 +11,9 @@ there; this module states the mathematics directly:
     logits  = H W2^T + b2
     loss    = mean_r ( logsumexp(logits_r) - logits_r[label_r] )
     dL      = (softmax(logits) - onehot(label)) / n
+    (label sets, labels of shape (n, S) with -1 unused, as ORBX_LABEL_LISTED:
+     loss = mean_r -log P_r with P_r the softmax mass on the set, and
+     dL   = (softmax - softmax * [c in set] / P_r) / n; S = 1 is the line above)
     dW2     = dL^T H,        db2 = sum_r dL
     dH      = (dL W2) * [H > 0]
     dW1     = dH^T X,        db1 = sum_r dH
@@ -52,9 +55,15 @@ def forward_backward(bits, labels, w1, b1, w2, b2, bf16=False):
     e = np.exp(logits - m)
     s = e.sum(axis=1, keepdims=True)
     lab = np.asarray(labels, dtype=np.int64)
-    loss = float(np.mean(np.log(s[:, 0]) + m[:, 0] - logits[np.arange(n), lab]))
-    dL = e / s
-    dL[np.arange(n), lab] -= 1.0
+    if lab.ndim == 1:
+        lab = lab[:, None]
+    member = np.zeros_like(logits, dtype=bool)
+    rows, cols = np.nonzero(lab >= 0)
+    member[rows, lab[rows, cols]] = True
+    p = e / s
+    mass = (p * member).sum(axis=1)
+    loss = float(np.mean(-np.log(mass)))
+    dL = p - p * member / mass[:, None]
     dL /= n
     if bf16:
         dL = bf16_round(dL)

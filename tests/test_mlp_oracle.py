@@ -59,3 +59,31 @@ def test_knn1_bruteforce_ties_smallest_index():
     q = np.zeros((1, 32), dtype=np.uint8)
     d, i = MO.knn1_bruteforce(q, np.vstack([db[1:2], db[0:1], db[0:1]]))
     assert d[0] == 0 and i[0] == 1
+
+
+def test_label_set_gradients_match_finite_differences():
+    """The listed-cluster target: loss -log(softmax mass on the set), sets of
+    up to 3 distinct clusters with unused (-1) entries."""
+    bits, labels, w = _setup()
+    rng = np.random.Generator(np.random.PCG64(2))
+    C = w["b2"].shape[0]
+    sets = np.full((len(labels), 3), -1, dtype=np.int64)
+    for r, l in enumerate(labels):
+        k = int(rng.integers(1, 4))
+        others = rng.permutation([c for c in range(C) if c != l])[: k - 1]
+        sets[r, :k] = [l] + list(others)
+    loss, g = MO.forward_backward(bits, sets, w["w1"], w["b1"], w["w2"], w["b2"])
+    loss1, _ = MO.forward_backward(bits, labels, w["w1"], w["b1"], w["w2"], w["b2"])
+    assert loss <= loss1 + 1e-12  # a superset of the label has at least its mass
+    eps = 1e-6
+    for name in ("w1", "b1", "w2", "b2"):
+        for _ in range(8):
+            idx = tuple(int(rng.integers(0, s)) for s in w[name].shape)
+            wp = {k: v.copy() for k, v in w.items()}
+            wm = {k: v.copy() for k, v in w.items()}
+            wp[name][idx] += eps
+            wm[name][idx] -= eps
+            lp, _ = MO.forward_backward(bits, sets, wp["w1"], wp["b1"], wp["w2"], wp["b2"])
+            lm, _ = MO.forward_backward(bits, sets, wm["w1"], wm["b1"], wm["w2"], wm["b2"])
+            num = (lp - lm) / (2 * eps)
+            assert abs(num - g[name][idx]) < 1e-6 + 1e-5 * abs(num), (name, idx, num, g[name][idx])
