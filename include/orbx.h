@@ -317,8 +317,9 @@ typedef struct orbx_learned orbx_learned;
 
 ORBX_API int orbx_learned_default_params(orbx_learned_params* p);
 /* Clusters d_db (ndb rows of 32 bytes, kept as a copy), labels the d_train rows
- * with the cluster of their exact nearest database row and trains the MLP.
- * Runs on the context's stream and synchronises it. */
+ * with the clusters their exact nearest database row is listed in (or only its
+ * nearest cluster, per label_mode) and trains the MLP.  Runs on the context's
+ * stream and synchronises it. */
 ORBX_API int orbx_learned_build(orbx_ctx* ctx, const orbx_learned_params* p, const uint8_t* d_db, int ndb,
                                 const uint8_t* d_train, int ntrain, orbx_learned** out);
 /* k = 2 search of nq queries; optional d_margin [nq] (top-1 minus top-2 logit)
