@@ -199,3 +199,101 @@ def detect_and_compute(img, w, h, noctaves=8, edge=31, wta_k=2, harris=True, pat
     pat = pattern(patch, wta_k)
     desc = describe(bstore, n, oszp, pts, s, c, pat, wta_k)
     return {"points": pts, "desc": desc, "total": total, "n": n, "oszp": oszp, "sin": s, "cos": c}
+
+
+# ---------------------------------------------------------------------------
+# FP64 side-oracle and the exception counts of the parity report.
+# ---------------------------------------------------------------------------
+
+# Tolerances of the FP64 comparison.  Harris: 1e-5 relative, plus an absolute
+# floor for the cancellation of A - 0.04 B.  The float path rounds A and B to
+# 24 bits before they cancel, so its absolute error is below
+# 2^-22 * (|A| + 0.04 B) * scale^4 (four times the rounding of the two terms);
+# over every possible int32 term pair that is at most HARRIS_ABS_FLOOR.
+# Angle: 1e-5 relative with an absolute floor of 2^-20 rad (four float ulps of
+# pi); the folds pi/2 - r and pi - r never cancel (r <= pi/4 and r <= pi/2).
+FP64_REL_TOL = 1e-5
+HARRIS_TERM_FLOOR = 2.0 ** -22
+HARRIS_ABS_FLOOR = 2.0 ** -22 * (2.0 ** 31 + 0.04 * 2.0 ** 32) * (1.0 / (4 * 7 * 255.0)) ** 4
+ANGLE_ABS_FLOOR = 2.0 ** -20
+TIE_EPS = 1e-4
+TIE, STRADDLE_ANGLE, STRADDLE_DESC = 1, 2, 4
+
+
+def harris_f64(pyr_store, n, oszp, pts):
+    """FP64 Harris at each keypoint; returns (score, |A| scale^4, 0.04 B scale^4)."""
+    pts = np.ascontiguousarray(pts)
+    score = np.zeros(max(len(pts), 1), dtype=np.float64)
+    terms = np.zeros((max(len(pts), 1), 2), dtype=np.float64)
+    lib().oo_harris_f64(_gp(pyr_store), _p(oszp), n, _p(pts), len(pts), _p(score), _p(terms))
+    return score[:len(pts)], terms[:len(pts), 0], terms[:len(pts), 1]
+
+
+def angle_f64(pyr_store, n, oszp, pts, patch_size=31):
+    pts = np.ascontiguousarray(pts)
+    ang = np.zeros(max(len(pts), 1), dtype=np.float64)
+    lib().oo_angle_f64(_gp(pyr_store), _p(oszp), n, _p(pts), len(pts), patch_size, _p(ang))
+    return ang[:len(pts)]
+
+
+def exception_flags(n, oszp, pts, sinv, cosv, pat, patch_size=31, tie_eps=TIE_EPS):
+    pts = np.ascontiguousarray(pts)
+    pat = np.ascontiguousarray(pat, dtype=np.int32)
+    s = np.ascontiguousarray(sinv, dtype=np.float32)
+    c = np.ascontiguousarray(cosv, dtype=np.float32)
+    flags = np.zeros(max(len(pts), 1), dtype=np.int32)
+    lib().oo_exception_flags(_p(oszp), n, _p(pts), len(pts), _p(s), _p(c), _p(pat), len(pat), patch_size,
+                             ctypes.c_double(tie_eps), _p(flags))
+    return flags[:len(pts)]
+
+
+def fp64_check(img, w, h, pts, sinv, cosv, noctaves=8, patch=31, wta_k=2, harris=True):
+    """Compare GPU keypoint scores and angles (float32) with the FP64 side-oracle
+    and count the keypoints the parity report lists.  Returns a dict of counts and
+    the largest relative errors; 'harris_fail' and 'angle_fail' count keypoints
+    outside tolerance (rel 1e-5 or the absolute floor)."""
+    n, oszp = layout(w, h, noctaves)
+    pyr_store, _ = pyramid(img, w, h, n, oszp)
+    pts = np.ascontiguousarray(pts)
+    out = {"keypoints": int(len(pts))}
+    if harris:
+        s64, ta, tb = harris_f64(pyr_store, n, oszp, pts)
+        g = pts["score"].astype(np.float64)
+        err = np.abs(g - s64)
+        rel_ok = err <= FP64_REL_TOL * np.abs(s64)
+        ok = err <= FP64_REL_TOL * np.abs(s64) + HARRIS_ABS_FLOOR
+        # the per-keypoint bound the fixed floor comes from, checked too
+        term_ok = err <= FP64_REL_TOL * np.abs(s64) + HARRIS_TERM_FLOOR * (ta + tb)
+        rel = np.where(s64 != 0, err / np.maximum(np.abs(s64), 1e-300), 0.0)
+        out.update(harris_fail=int((~ok).sum()), harris_needs_floor=int((ok & ~rel_ok).sum()),
+                   harris_term_bound_fail=int((~term_ok).sum()),
+                   harris_max_rel=float(rel[rel_ok].max()) if rel_ok.any() else 0.0,
+                   harris_max_abs=float(err.max()) if len(err) else 0.0)
+    a64 = angle_f64(pyr_store, n, oszp, pts, patch)
+    ga = pts["angle"].astype(np.float64)
+    both_nan = np.isnan(ga) & np.isnan(a64)
+    aerr = np.where(both_nan, 0.0, np.abs(ga - a64))
+    arel_ok = both_nan | (aerr <= FP64_REL_TOL * np.abs(a64))
+    aok = both_nan | (aerr <= FP64_REL_TOL * np.abs(a64) + ANGLE_ABS_FLOOR)
+    arel = np.where(np.abs(a64) > 0, aerr / np.maximum(np.abs(a64), 1e-300), 0.0)
+    out.update(angle_fail=int((~aok).sum()), angle_needs_floor=int((aok & ~arel_ok).sum()),
+               angle_max_rel=float(np.nanmax(arel[arel_ok])) if arel_ok.any() else 0.0,
+               angle_max_abs=float(np.nanmax(aerr)) if len(aerr) else 0.0, angle_nan=int(both_nan.sum()))
+    flags = exception_flags(n, oszp, pts, sinv, cosv, pattern(patch, wta_k), patch)
+    out.update(rounding_tie=int(((flags & TIE) != 0).sum()),
+               straddle_angle=int(((flags & STRADDLE_ANGLE) != 0).sum()),
+               straddle_desc=int(((flags & STRADDLE_DESC) != 0).sum()),
+               straddle_any=int(((flags & (STRADDLE_ANGLE | STRADDLE_DESC)) != 0).sum()))
+    out["flags"] = flags
+    return out
+
+
+def blur_race_rows(desc_race_free, desc_stock):
+    """Descriptor rows (same keypoint order) that differ between the race-free
+    build and the stock reference, whose in-place blur (orbd.cu:1756) lets
+    neighbouring blocks overwrite halo pixels before they are read."""
+    a = np.asarray(desc_race_free)
+    b = np.asarray(desc_stock)
+    if len(a) == 0:
+        return 0
+    return int(np.any(a != b, axis=1).sum())

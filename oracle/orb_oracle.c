@@ -587,3 +587,150 @@ void oo_knn2(const uint8_t* q, int nq, const uint8_t* db, int ndb, uint32_t* dis
     idx2[2 * i + 1] = i2;
   }
 }
+
+/* ------------------------------------------------------------------------ */
+/* FP64 side-oracle and per-keypoint exception flags.                        */
+/* ------------------------------------------------------------------------ */
+
+/* The wrapped integer Harris sums of dHarrisScore (orbd.cu:651-669) at one
+ * octave pixel: A = int32(dxx*dyy - dxy*dxy), B = uint32((dxx+dyy)^2), both
+ * with the GPU's 32-bit wrap. */
+static void harris_terms(const uint8_t* ptr, int p, int32_t* A, uint32_t* B) {
+  int dxx = 0, dyy = 0, dxy = 0;
+  for (int i = 0; i < 7; i++) {
+    for (int j = 0; j < 7; j++) {
+      const uint8_t* c = ptr + (i - 3) * p + (j - 3);
+      int dx = ((int)c[1] - (int)c[-1]) * 2 + ((int)c[-p + 1] - (int)c[-p - 1]) + ((int)c[p + 1] - (int)c[p - 1]);
+      int dy = ((int)c[p] - (int)c[-p]) * 2 + ((int)c[p - 1] - (int)c[-p - 1]) + ((int)c[p + 1] - (int)c[-p + 1]);
+      dxx += dx * dx;
+      dyy += dy * dy;
+      dxy += dx * dy;
+    }
+  }
+  int dsxy = dxx + dyy;
+  *A = (int32_t)((uint32_t)dxx * (uint32_t)dyy - (uint32_t)dxy * (uint32_t)dxy);
+  *B = (uint32_t)dsxy * (uint32_t)dsxy;
+}
+
+/* FP64 restatement of the Harris combine (orbd.cu:651-669) at each keypoint's
+ * own octave pixel (x >> o, y >> o): the same wrapped integer terms, combined
+ * as (A - 0.04 B) * (1 / (4*7*255))^4 in double with exact decimal constants.
+ * terms[2i] = |A| and terms[2i+1] = 0.04 B (the magnitudes that cancel), so a
+ * caller can scale an absolute floor by them. */
+void oo_harris_f64(const uint8_t* pyr, const int* oszp, int n, const oo_point* pts, int npts, double* score,
+                   double* terms) {
+  const int* widths = oszp + n;
+  const int* heights = widths + n;
+  const int* pitchs = heights + n;
+  const int* offsets = pitchs + n;
+  const double s = 1.0 / (4.0 * 7.0 * 255.0);
+  const double scale4 = s * s * s * s;
+  (void)widths;
+  (void)heights;
+#pragma omp parallel for schedule(static)
+  for (int i = 0; i < npts; i++) {
+    const int o = pts[i].octave;
+    const int p = pitchs[o];
+    const uint8_t* ptr = pyr + offsets[o] + (ptrdiff_t)(pts[i].y >> o) * p + (pts[i].x >> o);
+    int32_t A;
+    uint32_t B;
+    harris_terms(ptr, p, &A, &B);
+    score[i] = ((double)A - 0.04 * (double)B) * scale4;
+    if (terms) {
+      terms[2 * i] = fabs((double)A) * scale4;
+      terms[2 * i + 1] = 0.04 * (double)B * scale4;
+    }
+  }
+}
+
+/* FP64 restatement of angleIC + dFastAtan2 (orbd.cu:1001-1036, 986-998): the
+ * same integer moments, then the same 3-term polynomial and quadrant folds in
+ * double (not libm atan2: the polynomial itself is about 1e-5 rad from atan2).
+ * Zero moments give NaN, as 0/0 does in the reference. */
+void oo_angle_f64(const uint8_t* pyr, const int* oszp, int n, const oo_point* pts, int npts, int patch_size,
+                  double* angle) {
+  const int* widths = oszp + n;
+  const int* heights = widths + n;
+  const int* pitchs = heights + n;
+  const int* offsets = pitchs + n;
+  int umax[32];
+  oo_umax(patch_size, umax);
+  const int half_k = patch_size / 2;
+  (void)widths;
+  (void)heights;
+#pragma omp parallel for schedule(static)
+  for (int i = 0; i < npts; i++) {
+    const int o = pts[i].octave;
+    const int pitch = pitchs[o];
+    const uint8_t* center = pyr + offsets[o] + (ptrdiff_t)(pts[i].y >> o) * pitch + (pts[i].x >> o);
+    int m01 = 0, m10 = 0;
+    for (int u = -half_k; u <= half_k; ++u) m10 += u * center[u];
+    for (int v = 1; v <= half_k; ++v) {
+      int v_sum = 0;
+      const int pofs = v * pitch;
+      for (int u = -umax[v]; u <= umax[v]; ++u) {
+        int vp = center[u + pofs], vm = center[u - pofs];
+        v_sum += vp - vm;
+        m10 += u * (vp + vm);
+      }
+      m01 += v * v_sum;
+    }
+    const double x = (double)m10, y = (double)m01;
+    const double ax = fabs(x), ay = fabs(y);
+    const double a = fmin(ax, ay) / fmax(ax, ay);
+    const double q = a * a;
+    double r = ((-0.0464964749 * q + 0.15931422) * q - 0.327622764) * q * a + a;
+    if (ay > ax) r = 1.5707963267948966 - r;
+    if (x < 0) r = 3.14159265358979323846 - r;
+    if (y < 0) r = -r;
+    angle[i] = r;
+  }
+}
+
+/* Per-keypoint exception flags for the parity report:
+ *  bit 0 (ORACLE_TIE): a rotated pattern coordinate x*c - y*s or x*s + y*c,
+ *        evaluated in double from the float sin/cos the descriptor used, lies
+ *        within tie_eps of a .5 rounding tie (getValue, orbd.cu:1341-1348), so
+ *        the sampled pixel depends on the last bits of sin/cos and on FMA
+ *        contraction;
+ *  bit 1 (ORACLE_STRADDLE_ANGLE): the umax disc of angleIC (orbd.cu:1001-1036)
+ *        reaches outside its octave's w x h rectangle;
+ *  bit 2 (ORACLE_STRADDLE_DESC): a rotated, rounded pattern point of the
+ *        descriptor (orbd.cu:1437-1468, rounding as the reference build)
+ *        lands outside its octave's w x h rectangle.
+ * Pixels outside the rectangle are pitch padding, a neighbouring octave or the
+ * zero guard after the last one: the reference's result there depends on its
+ * memory layout. */
+void oo_exception_flags(const int* oszp, int n, const oo_point* pts, int npts, const float* sinv, const float* cosv,
+                        const int* pat, int npat, int patch_size, double tie_eps, int* flags) {
+  const int* widths = oszp + n;
+  const int* heights = widths + n;
+  int umax[32];
+  oo_umax(patch_size, umax);
+  const int half_k = patch_size / 2;
+#pragma omp parallel for schedule(static)
+  for (int i = 0; i < npts; i++) {
+    const int o = pts[i].octave;
+    const int w = widths[o], h = heights[o];
+    const int cx = pts[i].x >> o, cy = pts[i].y >> o;
+    int f = 0;
+    /* the disc: rows cy-half_k..cy+half_k; row v spans +-umax[|v|] (row 0 spans +-half_k) */
+    for (int v = -half_k; v <= half_k && !(f & 2); v++) {
+      const int u = v == 0 ? half_k : umax[v < 0 ? -v : v];
+      if (cy + v < 0 || cy + v >= h || cx - u < 0 || cx + u >= w) f |= 2;
+    }
+    const float s = sinv[i], c = cosv[i];
+    for (int k = 0; k < npat; k++) {
+      const double px = (double)pat[2 * k], py = (double)pat[2 * k + 1];
+      const double fx = px * (double)c - py * (double)s;
+      const double fy = px * (double)s + py * (double)c;
+      const double tx = fx - floor(fx), ty = fy - floor(fy);
+      if (fabs(tx - 0.5) < tie_eps || fabs(ty - 0.5) < tie_eps) f |= 1;
+      const float gx = fmaf((float)pat[2 * k], c, -((float)pat[2 * k + 1] * s));
+      const float gy = fmaf((float)pat[2 * k], s, (float)pat[2 * k + 1] * c);
+      const int ix = cx + rint_i(gx), iy = cy + rint_i(gy);
+      if (ix < 0 || ix >= w || iy < 0 || iy >= h) f |= 4;
+    }
+    flags[i] = f;
+  }
+}

@@ -44,4 +44,16 @@ void oo_describe(const uint8_t* blurred, const int* oszp, int n, const oo_point*
 void oo_match(const uint8_t* d1, int n1, const uint8_t* d2, int n2, int* match, int* dist);
 void oo_knn2(const uint8_t* q, int nq, const uint8_t* db, int ndb, uint32_t* dist2, int32_t* idx2);
 int oo_threads(void);
+
+/* FP64 side-oracle (Harris combine and angle polynomial in double) and the
+ * per-keypoint exception flags of the parity report. */
+#define ORACLE_TIE 1
+#define ORACLE_STRADDLE_ANGLE 2
+#define ORACLE_STRADDLE_DESC 4
+void oo_harris_f64(const uint8_t* pyr, const int* oszp, int n, const oo_point* pts, int npts, double* score,
+                   double* terms);
+void oo_angle_f64(const uint8_t* pyr, const int* oszp, int n, const oo_point* pts, int npts, int patch_size,
+                  double* angle);
+void oo_exception_flags(const int* oszp, int n, const oo_point* pts, int npts, const float* sinv, const float* cosv,
+                        const int* pattern_xy, int npat, int patch_size, double tie_eps, int* flags);
 #endif

@@ -147,6 +147,11 @@ def hmatch(d1, d2):
     return m[:n1], d[:n1]
 
 
+def set_zero_fill(on):
+    """Zero-fill of the reference's allocations (on for parity runs, off for timing)."""
+    lib().ref_set_zero_fill(int(bool(on)))
+
+
 def time_pair(a, b, w, h, warmup, iters):
     ms = ctypes.c_float(0)
     na = ctypes.c_int(0)
