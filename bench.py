@@ -197,6 +197,14 @@ def stage_work(oszp, n, na, nb):
     }
 
 
+def pair_config(n, na, nb):
+    """The pair workload's config, printed identically by both arms."""
+    return {"workload": "1920x1080 uint8 pair: detect+describe A and B, match A->B",
+            "levels": n, "noctaves_requested": 8, "fast_threshold": 20, "edge": 31, "wta_k": 2,
+            "score": "harris", "patch": 31, "max_pts": MAX_PTS, "keypoints": [na, nb],
+            "l2": "flushed (256 MiB write) before every timed step", "parallelism": "replicas"}
+
+
 def load_peaks():
     path = os.path.join(ROOT, "MEASURED_PEAKS.json")
     try:
@@ -225,6 +233,103 @@ def cpu_baseline_port(a, b, budget_s=12.0, max_reps=20):
     return {"value": 1000.0 * statistics.median(times), "unit": "ms", "cores": O.threads(), "kind": "port",
             "sample": f"{len(times)} runs of the full 1920x1080 pair (detect+describe A and B, match A->B) "
                       f"by the oracle restatement, median"}
+
+
+def parity_report(a, b, pa, da, pb, db):
+    """Check of the timed pair's output (outside every timed region), run with
+    the CPU baseline: bit-exactness with the oracle (given the reference build's
+    __sinf/__cosf when present) and with the live reference build, Harris
+    scores and angles against the FP64 side-oracle (1e-5 relative, absolute
+    floors in oracle/oracle.py), and the counted exceptions: rotation rounding
+    ties, patches that leave their octave, and descriptors the stock
+    reference's in-place blur race changes."""
+    from oracle import oracle as O
+    from oracle import refharness as R
+
+    have_ref = R.available()
+    sincos = None
+    if have_ref:
+        R.lib()
+        sincos = R.sincos
+    rep = {"sin_cos": "reference build __sinf/__cosf" if have_ref else "libm (reference build absent)",
+           "fp64_rel_tol": O.FP64_REL_TOL, "harris_abs_floor": O.HARRIS_ABS_FLOOR,
+           "angle_abs_floor": O.ANGLE_ABS_FLOOR, "tie_eps": O.TIE_EPS, "frames": {}}
+    for name, img, pts, desc in (("A", a, pa, da), ("B", b, pb, db)):
+        ref = O.detect_and_compute(img, W, H, max_pts=MAX_PTS, sincos=sincos)
+        fr = {"keypoints": int(len(pts)),
+              "points_bit_exact_vs_oracle": bool(len(pts) == len(ref["points"]) and
+                                                 np.array_equal(pts[["x", "y", "octave"]],
+                                                                ref["points"][["x", "y", "octave"]]) and
+                                                 np.array_equal(pts["score"].view(np.uint32),
+                                                                ref["points"]["score"].view(np.uint32)) and
+                                                 np.array_equal(pts["angle"].view(np.uint32),
+                                                                ref["points"]["angle"].view(np.uint32))),
+              "desc_rows_differing_vs_oracle": int(np.any(desc != ref["desc"], axis=1).sum())
+              if desc.shape == ref["desc"].shape else -1}
+        chk = O.fp64_check(img, W, H, pts, ref["sin"], ref["cos"])
+        flags = chk.pop("flags")
+        fr.update({k: v for k, v in chk.items() if k != "keypoints"})
+        if have_ref:
+            # rows whose bits change when libm sin/cos replace __sinf/__cosf: these
+            # are the rotation-sensitive keypoints, and should carry the tie flag
+            alt = O.detect_and_compute(img, W, H, max_pts=MAX_PTS)
+            if alt["desc"].shape == ref["desc"].shape:
+                sens = np.any(alt["desc"] != ref["desc"], axis=1)
+                fr["desc_rows_sensitive_to_sincos"] = int(sens.sum())
+                fr["of_which_flagged_tie"] = int((sens & ((flags & O.TIE) != 0)).sum())
+        if have_ref:
+            # the reference build live on the same image: race-free form (A') and stock form (A)
+            R.init(noctaves=8, edge=31, wta_k=2, score_type=0, patch=31, fast_thr=20, retain_topn=-1,
+                   max_pts=MAX_PTS)
+            rf = R.stages(img, W, H, MAX_PTS, race_free=True)
+            st = R.stages(img, W, H, MAX_PTS, race_free=False)
+            o1 = np.lexsort((rf["points"]["x"], rf["points"]["y"]))
+            o2 = np.lexsort((st["points"]["x"], st["points"]["y"]))
+            rpts = rf["points"][o1]
+            fr["bit_exact_vs_reference_build"] = bool(
+                len(rpts) == len(pts) and np.array_equal(pts[["x", "y", "octave"]], rpts[["x", "y", "octave"]])
+                and np.array_equal(pts["score"].view(np.uint32), rpts["score"].view(np.uint32))
+                and np.array_equal(pts["angle"].view(np.uint32), rpts["angle"].view(np.uint32))
+                and np.array_equal(desc, rf["desc"][o1]))
+            fr["blur_race_desc_rows"] = O.blur_race_rows(rf["desc"][o1], st["desc"][o2])
+        rep["frames"][name] = fr
+    m, d = O.match(da, db)
+    rep["matches_bit_exact_vs_oracle"] = bool(np.array_equal(pa["match"], m) and np.array_equal(pa["distance"], d))
+    return rep
+
+
+def cpu_baseline_opencv_c0(budget_s=6.0):
+    """OpenCV's own ORB + BFMatcher on the 640x480 pair (5000 keypoints, 8
+    levels, scale 1.2), on all host cores and on one thread: the comparison the
+    reference's demo makes on the host (main.cpp:274-336)."""
+    try:
+        import cv2
+    except ImportError:
+        return {"unavailable": "cv2 not importable on this host"}
+    import synth
+
+    a, b, _ = synth.make_pair(640, 480, seed=0)
+    ia, ib = np.ascontiguousarray(a[:, :640]), np.ascontiguousarray(b[:, :640])
+    out = {"workload": "640x480 uint8 pair, cv2.ORB(5000, 1.2, 8 levels, FAST 20) + BFMatcher knn k=2"}
+    all_cores = len(os.sched_getaffinity(0))
+    for key, cores in (("all_cores", all_cores), ("one_thread", 1)):
+        cv2.setNumThreads(cores)
+        orb = cv2.ORB_create(nfeatures=5000, scaleFactor=1.2, nlevels=8, edgeThreshold=31, patchSize=31,
+                             fastThreshold=20, WTA_K=2)
+        bf = cv2.BFMatcher(cv2.NORM_HAMMING)
+        times = []
+        t_end = time.time() + budget_s
+        while len(times) < 50 and (not times or time.time() < t_end):
+            t0 = time.perf_counter()
+            ka, da = orb.detectAndCompute(ia, None)
+            kb, db = orb.detectAndCompute(ib, None)
+            if da is not None and db is not None:
+                bf.knnMatch(da, db, k=2)
+            times.append(time.perf_counter() - t0)
+        out[key] = {"value": 1000.0 * statistics.median(times), "unit": "ms", "cores": cores,
+                    "runs": len(times), "keypoints": [len(ka), len(kb)]}
+    cv2.setNumThreads(all_cores)
+    return out
 
 
 def cpu_baseline_opencv(a, b, budget_s=8.0):
@@ -303,6 +408,28 @@ def run_orbx(args, world, rank, local):
     total_ms = max_over_ranks(local_total, world)
     na, nb = int(A.count.item()), int(B.count.item())
     matched = int((A.points[:na, 5] >= 0).sum().item())
+    host_pa, host_da = A.to_host()
+    host_pb, host_db = B.to_host()
+
+    # the same pair with the int8 tcgen05 matcher (the other exact form)
+    imma_ms = []
+    with torch.cuda.stream(stream):
+        for _ in range(3):
+            ctx.pair_ptr(da, db, W, H, pitch, A.points, A.desc, A.count, B.points, B.desc, B.count,
+                         orbx.MATCH_IMMA)
+        for _ in range(min(args.steps, 100)):
+            flush.zero_()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            ctx.pair_ptr(da, db, W, H, pitch, A.points, A.desc, A.count, B.points, B.desc, B.count,
+                         orbx.MATCH_IMMA)
+            e1.record(stream)
+            e1.synchronize()
+            imma_ms.append(e0.elapsed_time(e1))
+    imma_pa, _ = A.to_host()
+    pair_imma = {"ms": statistics.median(imma_ms), "steps": len(imma_ms),
+                 "matches_equal_popc": bool(np.array_equal(imma_pa["match"], host_pa["match"]) and
+                                            np.array_equal(imma_pa["distance"], host_pa["distance"]))}
 
     # end to end through the host-buffer C ABI call, pinned host images
     ha = torch.from_numpy(a).pin_memory()
@@ -380,23 +507,22 @@ def run_orbx(args, world, rank, local):
             "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": False,
             "scaling": "weak", "vs_baseline": None, "dtype": "u8",
             "data": "synthetic (seeded blobs + polygons + noise, homography-warped partner; cuda-orb_b200/synth.py)",
-            "config": {"workload": "1920x1080 uint8 pair: detect+describe A and B, match A->B (XOR-popc)",
-                       "levels": n, "noctaves_requested": 8, "fast_threshold": 20, "edge": 31, "wta_k": 2,
-                       "max_pts": MAX_PTS, "keypoints": [na, nb], "matches": matched,
-                       "l2": "flushed (256 MiB write) before every timed step", "parallelism": "replicas",
-                       "graph": "one CUDA graph per pair (5 kernels)"},
+            "config": pair_config(n, na, nb),
+            "impl_detail": {"matcher": "XOR-popc", "graph": "one CUDA graph per pair (5 kernels)",
+                            "matches": matched},
             "e2e": {"value": e2e_total / (e2e_steps * world), "unit": "ms", "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h,
                     "how": "orbx_pair_host: pinned host images in, host keypoints/matches out, CUDA events"},
             "gpu_launches": 5 * args.steps,
             "roofline": roofline,
             "kernels": kernels,
+            "pair_int8_tcgen05_matcher": pair_imma,
             "clocks": clocks,
         }
         if match_bench:
             result["match_65536"] = match_bench
     ctx.close()
-    return result, (a, b)
+    return result, (a, b), (host_pa, host_da, host_pb, host_db)
 
 
 def bench_knn2(ctx, stream, dev, peaks):
@@ -460,26 +586,40 @@ def run_reference(args, world, rank, local):
     dev = torch.device("cuda", local)
     a, b, _ = synth.make_pair(W, H, seed=rank)
     R.init(noctaves=8, edge=31, wta_k=2, score_type=0, patch=31, fast_thr=20, retain_topn=-1, max_pts=MAX_PTS)
-    R.time_pair(a, b, W, H, max(args.warmup, 3), 1)
     flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device=dev)
     steps = min(args.steps, 300)
-    ms = []
+
+    def timed(zero_fill):
+        # zero_fill off: the reference's own per-call descriptor cudaMalloc
+        # without the harness's parity-run memset of the block and its guards
+        R.set_zero_fill(zero_fill)
+        R.time_pair(a, b, W, H, max(args.warmup, 3), 1)
+        out = []
+        for _ in range(steps):
+            flush.zero_()
+            torch.cuda.synchronize(dev)
+            t, na_, nb_ = R.time_pair(a, b, W, H, 0, 1)
+            out.append(t)
+        return out, na_, nb_
+
     sampler = ClockSampler(local)
     sampler.start()
-    for _ in range(steps):
-        flush.zero_()
-        torch.cuda.synchronize(dev)
-        t, na, nb = R.time_pair(a, b, W, H, 0, 1)
-        ms.append(t)
+    ms, na, nb = timed(False)
     clocks = sampler.stop()
+    ms_fill, _, _ = timed(True)
+    R.set_zero_fill(True)
     value = sum(ms) / len(ms)
+    lay = R.layout_for(W, H, 8)
     return {
         "metric": METRIC, "value": value, "unit": "ms", "n_gpus": 1, "steps": steps, "warmup": args.warmup,
         "ms_per_step": value, "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "u8",
         "impl": "reference",
         "data": "synthetic (same generator and seed as the library arm)",
-        "config": {"workload": "1920x1080 uint8 pair: Orbor::detectAndCompute A and B, Orbor::match A->B",
-                   "max_pts": MAX_PTS, "keypoints": [na, nb], "l2": "flushed before every step"},
+        "config": pair_config(int(lay["n"]), na, nb),
+        "impl_detail": {"api": "Orbor::detectAndCompute A and B, Orbor::match A->B (orb.cpp:57-113)",
+                        "with_parity_zero_fill_ms": sum(ms_fill) / len(ms_fill),
+                        "note": "value is timed without the harness's zero-fill of each allocation; "
+                                "with_parity_zero_fill_ms is the same run with it"},
         "e2e": {"value": value, "unit": "ms", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "cpu_baseline": {"value": value, "unit": "ms", "cores": 1, "kind": "reference",
                          "sample": f"{steps} pairs through the reference CUDA build (its orbd.cu/orb.cpp compiled "
@@ -1001,12 +1141,14 @@ def main(argv=None):
     if args.impl == "reference":
         res = run_reference(args, world, rank, local)
     else:
-        res, imgs = run_orbx(args, world, rank, local)
+        res, imgs, outs = run_orbx(args, world, rank, local)
         if rank == 0 and not args.no_learned_bench:
             res["learned_proposal"] = learned_summary(args, world, rank, local)
         if rank == 0 and not args.no_cpu_baseline:
             res["cpu_baseline"] = cpu_baseline_port(*imgs)
+            res["parity_report"] = parity_report(imgs[0], imgs[1], *outs)
             res["cpu_opencv"] = cpu_baseline_opencv(*imgs)
+            res["cpu_opencv_640x480"] = cpu_baseline_opencv_c0()
     if rank == 0 and res is not None:
         print(json.dumps(res), flush=True)
     if world > 1:

@@ -6,14 +6,14 @@ orbd.cu:95-375).  Bit-exact descriptors need the identical table, so it is read
 out of the reference source instead of being retyped, and written in this
 project's own compact layout (int8 point pairs, no comments).
 
-Usage:  python gen_pattern31.py [path/to/orbd.cu]
+Usage:  python gen_pattern31.py path/to/orbd.cu
+        (or set ORB_REFERENCE_SRC to the reference's orbd.cu)
 """
 import os
 import re
 import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-DEFAULT_SRC = "/root/reference/orbd.cu"
 
 
 def read_pattern(src_path):
@@ -45,7 +45,9 @@ def render(vals):
 
 
 def main():
-    src = sys.argv[1] if len(sys.argv) > 1 else DEFAULT_SRC
+    src = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("ORB_REFERENCE_SRC")
+    if not src:
+        sys.exit("usage: gen_pattern31.py path/to/orbd.cu (or set ORB_REFERENCE_SRC)")
     vals = read_pattern(src)
     out = os.path.join(HERE, "orb_pattern31.h")
     with open(out, "w") as f:

@@ -4,12 +4,14 @@
 //
 // The scratch holds, for at most kStaticMaxQueries queries and kStaticSplits
 // train splits, the partial top-2 keys of every split (8 bytes per query and
-// split) and one arrival counter per 128-query tile.  Its address is looked up
-// once per device with cudaGetSymbolAddress, on the first call made with that
-// device current; the counters are cleared on the caller's stream before every
-// search.  All calls on one device share the array, so two calls whose work
-// overlaps on the device (different streams, or different host threads) race.
-#include <mutex>
+// split) and one arrival counter per 128-query tile.  Its device address is
+// looked up with cudaGetSymbolAddress on every call, with the caller's device
+// current.  The first call on a device loads this module there, which commits
+// the array; later calls only look the address up, and a cudaDeviceReset (which
+// unloads the module) between calls cannot leave a stale address behind.  The
+// counters are cleared on the caller's stream before every search.  All calls
+// on one device share the array, so two calls whose work overlaps on the
+// device (different streams, or different host threads) race.
 
 #include "../../include/orbx.h"
 #include "orbx_internal.cuh"
@@ -29,23 +31,16 @@ static_assert(sizeof(StaticScratch) <= (5u << 20), "static matcher scratch shoul
 
 static __device__ __align__(256) StaticScratch g_static_scratch;
 
-constexpr int kStaticMaxDevices = 64;
-static StaticScratch* g_static_ptr[kStaticMaxDevices];
-static std::mutex g_static_mu;
-
-// Address of g_static_scratch on the current device; looked up on first use.
-static int static_scratch(int dev, StaticScratch** out) {
-  std::lock_guard<std::mutex> lk(g_static_mu);
-  if (!g_static_ptr[dev]) {
-    void* p = nullptr;
-    const cudaError_t e = cudaGetSymbolAddress(&p, g_static_scratch);
-    if (e != cudaSuccess || !p) {
-      (void)cudaGetLastError();
-      return ORBX_ERR_CUDA;
-    }
-    g_static_ptr[dev] = static_cast<StaticScratch*>(p);
+// Address of g_static_scratch on the current device.  In host code the symbol
+// is a host-side stand-in, never a device address, so kernels get this value.
+static int static_scratch(StaticScratch** out) {
+  void* p = nullptr;
+  const cudaError_t e = cudaGetSymbolAddress(&p, g_static_scratch);
+  if (e != cudaSuccess || !p) {
+    (void)cudaGetLastError();
+    return ORBX_ERR_CUDA;
   }
-  *out = g_static_ptr[dev];
+  *out = static_cast<StaticScratch*>(p);
   return ORBX_OK;
 }
 
@@ -58,14 +53,8 @@ ORBX_API int orbx_match_knn2_static(const uint8_t* d_q, int nq, const uint8_t* d
   if (nq < 0 || ndb < 0 || (nq > 0 && (!d_q || !d_dist2 || !d_idx2)) || (ndb > 0 && !d_db)) return ORBX_ERR_ARG;
   if (nq > kStaticMaxQueries || ndb > (1 << 22) - 1) return ORBX_ERR_SIZE;
   if (nq == 0) return ORBX_OK;
-  int dev = 0;
-  if (cudaGetDevice(&dev) != cudaSuccess) {
-    (void)cudaGetLastError();
-    return ORBX_ERR_CUDA;
-  }
-  if (dev < 0 || dev >= kStaticMaxDevices) return ORBX_ERR_ARG;
   StaticScratch* s = nullptr;
-  int rc = static_scratch(dev, &s);
+  int rc = static_scratch(&s);
   if (rc) return rc;
   cudaStream_t stream = static_cast<cudaStream_t>(cuda_stream);
   const int tiles = (nq + 127) / 128;

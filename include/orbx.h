@@ -114,8 +114,11 @@ ORBX_API int orbx_match_knn2(orbx_ctx* ctx, const uint8_t* d_q, int nq, const ui
 /* No counterpart in the reference.  The orbx_match_knn2 popcount search with the
  * same outputs, for callers that may not allocate device memory: it needs no
  * context and allocates nothing.  Its scratch (about 4 MiB) is one fixed
- * device array per device, whose address is looked up on the first call made
- * with that device current; make that first call before any stream capture.
+ * device array per device, whose address is looked up on every call with that
+ * device current.  The first call on a device loads the library's module
+ * there and so commits the 4 MiB (a failure then, e.g. with no device memory
+ * left, returns ORBX_ERR_CUDA): make that first call at start-up, before any
+ * stream capture.  Later calls only look the address up.
  * Runs on the current device and on cuda_stream (0 = the legacy default stream).
  * nq above ORBX_STATIC_MAX_QUERIES returns ORBX_ERR_SIZE.  Calls on one device
  * share the scratch: calls whose work overlaps on the device race. */

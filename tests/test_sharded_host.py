@@ -54,8 +54,24 @@ def test_merge_knn2_orders_by_distance_then_index():
     i = torch.tensor([[[10, 11], [0, 1], [-1, -1]],
                       [[4, 20], [30, 31], [-1, -1]]])
     md, mi = sharded.merge_knn2(d, i)
-    assert md.tolist() == [[5, 5], [2, 3], [sharded.NO_DIST, sharded.NO_DIST]]
+    # the types and sentinels of orbx.knn2: int32, missing distance 0xFFFFFFFF (-1 as int32)
+    assert md.dtype == torch.int32 and mi.dtype == torch.int32
+    assert md.tolist() == [[5, 5], [2, 3], [-1, -1]]
     assert mi.tolist() == [[4, 10], [30, 0], [-1, -1]]
+    assert md.numpy().view(np.uint32)[2].tolist() == [sharded.NO_DIST, sharded.NO_DIST]
+
+
+def test_merge_knn2_one_missing_second():
+    # a query with one candidate in one shard and none in the other
+    d = torch.tensor([[[7, -1]], [[-1, -1]]], dtype=torch.int32)
+    i = torch.tensor([[[3, -1]], [[-1, -1]]], dtype=torch.int32)
+    md, mi = sharded.merge_knn2(d, i)
+    assert md.tolist() == [[7, -1]] and mi.tolist() == [[3, -1]]
+
+
+def test_packed_key_is_16_bytes_per_query():
+    keys = sharded.pack_keys(torch.zeros((10, 2), dtype=torch.int32), torch.zeros((10, 2), dtype=torch.int32))
+    assert keys.dtype == torch.int64 and keys.numel() * keys.element_size() == 16 * 10
 
 
 def _rank_main(rank, world, port, n_db, n_q, seed, out):
@@ -67,14 +83,19 @@ def _rank_main(rank, world, port, n_db, n_q, seed, out):
         b, e = sharded.shard_rows(n_db, world, rank)
         ld, li = O.knn2(q, db[b:e])
         gi = np.where(li >= 0, li.astype(np.int64) + b, -1)
-        md, mi = sharded.gather_merge_knn2(torch.from_numpy(ld.astype(np.int64)), torch.from_numpy(gi))
-        out[rank] = (md.numpy().astype(np.int64).tolist(), mi.numpy().astype(np.int64).tolist())
+        # the local search's own types: uint32 bits in int32 distances, int32 indices
+        md, mi = sharded.gather_merge_knn2(torch.from_numpy(ld.view(np.int32)), torch.from_numpy(gi))
+        assert md.dtype == torch.int32 and mi.dtype == torch.int32
+        out[rank] = (md.numpy().view(np.uint32).tolist(), mi.numpy().tolist())
         dist.barrier()
     finally:
         dist.destroy_process_group()
 
 
-@pytest.mark.parametrize("world,n_db,n_q,seed", [(2, 1000, 64, 1), (3, 1001, 50, 2), (2, 1, 5, 3), (3, 2, 4, 4)])
+# (2, 3, ...) and (3, 2, ...): fewer database rows than world_size x 2, so some
+# queries have a missing second neighbour and some shards are empty
+@pytest.mark.parametrize("world,n_db,n_q,seed", [(2, 1000, 64, 1), (3, 1001, 50, 2), (2, 1, 5, 3), (3, 2, 4, 4),
+                                                 (2, 3, 6, 5)])
 def test_sharded_knn2_gloo_equals_whole_database(world, n_db, n_q, seed):
     ctx = mp.get_context("spawn")
     mgr = ctx.Manager()
@@ -90,5 +111,5 @@ def test_sharded_knn2_gloo_equals_whole_database(world, n_db, n_q, seed):
     ed, ei = O.knn2(q, db)
     for r in range(world):
         d, i = out[r]
-        assert np.array_equal(np.array(d, dtype=np.int64), ed.astype(np.int64)), r
-        assert np.array_equal(np.array(i, dtype=np.int64), ei.astype(np.int64)), r
+        assert np.array_equal(np.array(d, dtype=np.uint32), ed), r
+        assert np.array_equal(np.array(i, dtype=np.int32), ei), r
