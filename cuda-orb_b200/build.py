@@ -15,7 +15,7 @@ CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "liborbx.so")
 SOURCES = ["orbx_api.cu", "orbx_detect.cu", "orbx_describe.cu", "orbx_match.cu", "orbx_match_imma.cu",
            "orb_compat.cu", "orbx_static.cu", "orbx_gemm.cu", "orbx_learned.cu", "orbx_learned_api.cu",
-           "orbx_hostio.cu", "orbx_ocv.cu"]
+           "orbx_hostio.cu", "orbx_ocv.cu", "orbx_persist.cu"]
 NVCC = os.environ.get("NVCC", "nvcc")
 FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "-std=c++17",
          "-Xcompiler", "-fPIC", "-Xcompiler", "-O2"]

@@ -12,6 +12,7 @@
 #include "orb_pattern31.h"
 #include "orbx_device.cuh"
 #include "orbx_internal.cuh"
+#include "orbx_persist.cuh"
 
 using namespace orbx;
 
@@ -111,6 +112,19 @@ struct orbx_ctx {
   size_t batch_part_words = 0, batch_tile_words = 0;
   std::vector<uint8_t> batch_key;
   cudaGraphExec_t batch_exec = nullptr;
+  // persistent batch form: run table, describe slices, completion counters
+  int batch_form = 0;
+  int persist_group = 0;
+  int persist_bps = 0;
+  PersistRun* d_runs = nullptr;
+  int* d_run_base = nullptr;  // [runs + 1]
+  int* d_desc_base = nullptr;  // [frames + 1]
+  int* d_done = nullptr;       // [4 * frames + 1]: stage counters, then the item counter
+  size_t runs_cap = 0, frames_cap = 0;
+  // device-side waits
+  int wait_us = 1000000;
+  long long wait_cycles = 0;
+  int clock_khz = 2000000;
 };
 
 #define ORBX_CUDA(x)                   \
@@ -413,6 +427,7 @@ static int upload_batch(orbx_ctx* c, BatchSlot& bs, const std::vector<Frame>& fr
   b.nms_base = bs.d_bases + 2 * (nf + 1);
   b.nms_ticket = bs.d_ticket;
   b.err = c->d_err;
+  b.wait_cycles = c->wait_cycles;
   b.fast_thr = c->p.fast_threshold;
   b.harris = c->p.score_type == 0 ? 1 : 0;
   b.wta_k = c->p.wta_k;
@@ -617,6 +632,13 @@ ORBX_API int orbx_create(orbx_ctx** out, int device) {
     return ORBX_ERR_CUDA;
   }
   c->own_stream = true;
+  int khz = 0;
+  if (cudaDeviceGetAttribute(&khz, cudaDevAttrClockRate, device) != cudaSuccess || khz <= 0) {
+    (void)cudaGetLastError();
+    khz = 2000000;
+  }
+  c->clock_khz = khz;
+  c->wait_cycles = (long long)c->wait_us * khz / 1000;
   *out = c;
   return ORBX_OK;
 }
@@ -661,6 +683,10 @@ ORBX_API int orbx_destroy(orbx_ctx* c) {
   cudaFree(c->batch_part);
   cudaFree(c->batch_tile_done);
   if (c->batch_exec) cudaGraphExecDestroy(c->batch_exec);
+  cudaFree(c->d_runs);
+  cudaFree(c->d_run_base);
+  cudaFree(c->d_desc_base);
+  cudaFree(c->d_done);
   cudaFree(c->d_pattern);
   cudaFree(c->d_umax);
   cudaFree(c->d_err);
@@ -1034,6 +1060,10 @@ ORBX_API int orbx_get_tuning(orbx_ctx* c, orbx_tuning* t) {
   t->describe_blocks_per_sm = c->describe_bps;
   t->match_blocks_per_sm = c->match_bps;
   t->match_blocks_per_pair = c->match_blocks_per_pair;
+  t->batch_form = c->batch_form;
+  t->persist_group = c->persist_group;
+  t->persist_blocks_per_sm = c->persist_bps;
+  t->wait_timeout_us = c->wait_us;
   return ORBX_OK;
 }
 
@@ -1041,12 +1071,24 @@ ORBX_API int orbx_set_tuning(orbx_ctx* c, const orbx_tuning* t) {
   if (!c || !t) return ORBX_ERR_ARG;
   if (t->nms_rows < 1 || t->nms_rows > kNmsMaxRows || t->describe_blocks_per_sm < 1 ||
       t->describe_blocks_per_sm > 64 || t->match_blocks_per_sm < 1 || t->match_blocks_per_sm > 64 ||
-      t->match_blocks_per_pair < 0 || t->match_blocks_per_pair > 4096)
+      t->match_blocks_per_pair < 0 || t->match_blocks_per_pair > 4096 || t->batch_form < 0 || t->batch_form > 1 ||
+      t->persist_group < 0 || t->persist_group > kMaxFramesPerLaunch || t->persist_blocks_per_sm < 0 ||
+      t->persist_blocks_per_sm > 32 || t->wait_timeout_us < 1 || t->wait_timeout_us > 10000000)
     return ORBX_ERR_ARG;
   c->nms_rows = t->nms_rows;
   c->describe_bps = t->describe_blocks_per_sm;
   c->match_bps = t->match_blocks_per_sm;
   c->match_blocks_per_pair = t->match_blocks_per_pair;
+  c->batch_form = t->batch_form;
+  c->persist_group = t->persist_group;
+  c->persist_bps = t->persist_blocks_per_sm;
+  c->wait_us = t->wait_timeout_us;
+  c->wait_cycles = (long long)c->wait_us * c->clock_khz / 1000;
+  if (c->batch_exec) {
+    cudaGraphExecDestroy(c->batch_exec);
+    c->batch_exec = nullptr;
+  }
+  c->batch_key.clear();
   // cached graphs baked in the old shapes
   if (c->pg.exec) {
     cudaGraphExecDestroy(c->pg.exec);
@@ -1059,6 +1101,107 @@ ORBX_API int orbx_set_tuning(orbx_ctx* c, const orbx_tuning* t) {
 }
 
 static constexpr int kBatchSplitsCap = 16;
+
+// The persistent form of orbx_batch_pairs (orbx_persist.cu): run table,
+// describe slices and counters uploaded when the batch layout changes, then a
+// graph of one counter reset and one persistent launch.
+static int batch_persistent(orbx_ctx* c, const LaunchPlan& pl, const std::vector<Frame>& frames,
+                            const std::vector<MatchJob>& jobs, int blocks_per_pair, std::vector<uint8_t>& key) {
+  const int nf = (int)frames.size();
+  const int n_pairs = (int)jobs.size();
+  std::vector<int> pyr_n(nf), det_n(nf), nms_n(nf), desc_n(nf), desc_base(nf + 1, 0);
+  for (int f = 0; f < nf; f++) {
+    const Frame& F = frames[f];
+    pyr_n[f] = F.pyr_tile_base[F.n_oct];
+    det_n[f] = F.det_tiles_x * F.det_tiles_y;
+    nms_n[f] = F.nms_strips;
+    desc_n[f] = std::max(1, div_up(F.w * F.h, kDescSlicePixels));
+    desc_base[f + 1] = desc_base[f] + desc_n[f];
+  }
+  const int group = c->persist_group > 0 ? c->persist_group : nf;
+  std::vector<PersistRun> runs;
+  std::vector<int> run_base;
+  build_persist_runs(nf, group, pyr_n.data(), det_n.data(), nms_n.data(), desc_n.data(), blocks_per_pair, &runs,
+                     &run_base);
+  const int bps_max = persist_blocks_per_sm(c->p.wta_k);
+  if (bps_max <= 0) return ORBX_ERR_CUDA;
+  const int bps = c->persist_bps > 0 ? std::min(c->persist_bps, bps_max) : bps_max;
+  int nsm = 0;
+  ORBX_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, c->device));
+  const int grid = bps * nsm;
+  {
+    const int extra[4] = {1, group, grid, (int)runs.size()};
+    const size_t k0 = key.size();
+    key.resize(k0 + sizeof(extra));
+    std::memcpy(key.data() + k0, extra, sizeof(extra));
+  }
+  if (!(c->batch_exec && c->batch_key == key)) {
+    if (c->batch_exec) {
+      cudaGraphExecDestroy(c->batch_exec);
+      c->batch_exec = nullptr;
+    }
+    ORBX_CUDA(cudaStreamSynchronize(c->stream));
+    if (c->jobs_cap < n_pairs) {
+      cudaFree(c->d_jobs);
+      c->d_jobs = nullptr;
+      c->jobs_cap = 0;
+      ORBX_CUDA(cudaMalloc(&c->d_jobs, sizeof(MatchJob) * n_pairs));
+      c->jobs_cap = n_pairs;
+    }
+    if (c->runs_cap < runs.size()) {
+      cudaFree(c->d_runs);
+      cudaFree(c->d_run_base);
+      c->d_runs = nullptr;
+      c->d_run_base = nullptr;
+      c->runs_cap = 0;
+      ORBX_CUDA(cudaMalloc(&c->d_runs, sizeof(PersistRun) * runs.size()));
+      ORBX_CUDA(cudaMalloc(&c->d_run_base, sizeof(int) * (runs.size() + 1)));
+      c->runs_cap = runs.size();
+    }
+    if (c->frames_cap < (size_t)nf) {
+      cudaFree(c->d_desc_base);
+      cudaFree(c->d_done);
+      c->d_desc_base = nullptr;
+      c->d_done = nullptr;
+      c->frames_cap = 0;
+      ORBX_CUDA(cudaMalloc(&c->d_desc_base, sizeof(int) * (nf + 1)));
+      ORBX_CUDA(cudaMalloc(&c->d_done, sizeof(int) * (4 * (size_t)nf + 1)));
+      c->frames_cap = nf;
+    }
+    ORBX_CUDA(cudaMemcpy(c->d_jobs, jobs.data(), sizeof(MatchJob) * n_pairs, cudaMemcpyHostToDevice));
+    ORBX_CUDA(cudaMemcpy(c->d_runs, runs.data(), sizeof(PersistRun) * runs.size(), cudaMemcpyHostToDevice));
+    ORBX_CUDA(cudaMemcpy(c->d_run_base, run_base.data(), sizeof(int) * run_base.size(), cudaMemcpyHostToDevice));
+    ORBX_CUDA(cudaMemcpy(c->d_desc_base, desc_base.data(), sizeof(int) * (nf + 1), cudaMemcpyHostToDevice));
+    PersistArgs a{};
+    a.b = pl.b;
+    a.runs = c->d_runs;
+    a.run_base = c->d_run_base;
+    a.n_runs = (int)runs.size();
+    a.run_base_host_total = run_base.back();
+    a.desc_base = c->d_desc_base;
+    a.done = c->d_done;
+    a.item_counter = reinterpret_cast<unsigned int*>(c->d_done + 4 * (size_t)nf);
+    a.jobs = c->d_jobs;
+    a.blocks_per_job = blocks_per_pair;
+    cudaGraph_t graph = nullptr;
+    ORBX_CUDA(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+    cudaError_t le = cudaMemsetAsync(c->d_done, 0, sizeof(int) * (4 * (size_t)nf + 1), c->stream);
+    if (le == cudaSuccess) le = launch_batch_persistent(a, grid, c->stream);
+    const cudaError_t ce = cudaStreamEndCapture(c->stream, &graph);
+    if (le != cudaSuccess) {
+      if (graph) cudaGraphDestroy(graph);
+      (void)cudaGetLastError();
+      return ORBX_ERR_CUDA;
+    }
+    ORBX_CUDA(ce);
+    const cudaError_t ie = cudaGraphInstantiate(&c->batch_exec, graph, 0);
+    cudaGraphDestroy(graph);
+    ORBX_CUDA(ie);
+    c->batch_key.swap(key);
+  }
+  ORBX_CUDA(cudaGraphLaunch(c->batch_exec, c->stream));
+  return ORBX_OK;
+}
 
 static int batch_pairs_impl(orbx_ctx* c, int n_pairs, const orbx_image* ia, const orbx_image* ib,
                             const orbx_frame_out* oa, const orbx_frame_out* ob, int mode, float* stage_ms) {
@@ -1152,6 +1295,7 @@ static int batch_pairs_impl(orbx_ctx* c, int n_pairs, const orbx_image* ia, cons
     const int shapes[4] = {c->nms_rows, c->describe_bps, blocks_per_pair, mode};
     std::memcpy(k, shapes, sizeof(shapes));
   }
+  if (c->batch_form == 1 && !stage_ms) return batch_persistent(c, pl, frames, jobs, blocks_per_pair, key);
   if (stage_ms) {
     // profiling: the same launches, unrolled, with events between them
     if (c->jobs_cap < n_pairs) {
@@ -1234,26 +1378,53 @@ ORBX_API int orbx_profile_batch(orbx_ctx* c, int n_pairs, const orbx_image* ia, 
 ORBX_API int orbx_autotune_pairs(orbx_ctx* c, int n_pairs, const orbx_image* ia, const orbx_image* ib,
                                  const orbx_frame_out* oa, const orbx_frame_out* ob, int reps, orbx_tuning* best,
                                  float* best_ms) {
-  if (!c || reps < 1) return ORBX_ERR_ARG;
+  return orbx_autotune_pairs_forms(c, n_pairs, ia, ib, oa, ob, reps, 3, best, best_ms);
+}
+
+ORBX_API int orbx_autotune_pairs_forms(orbx_ctx* c, int n_pairs, const orbx_image* ia, const orbx_image* ib,
+                                       const orbx_frame_out* oa, const orbx_frame_out* ob, int reps, int forms,
+                                       orbx_tuning* best, float* best_ms) {
+  if (!c || reps < 1 || forms < 1 || forms > 3) return ORBX_ERR_ARG;
   DeviceGuard g(c->device);
   orbx_tuning keep;
   orbx_get_tuning(c, &keep);
   cudaEvent_t e0, e1;
   ORBX_CUDA(cudaEventCreate(&e0));
   ORBX_CUDA(cudaEventCreate(&e1));
-  const int rows_c[] = {2, 4, 8, 16};
-  const int desc_c[] = {4, 8, 16};
-  const int match_c[] = {0, 64, 256};
-  orbx_tuning top = keep;
-  float top_ms = 1e30f;
-  int rc = ORBX_OK;
-  for (int r : rows_c) {
-    for (int d : desc_c) {
-      for (int m : match_c) {
+  // candidates: the five-launch form over NMS strip height, describe grid and
+  // match blocks per pair; the persistent form over NMS strip height, match
+  // blocks per pair, frames per wave and resident blocks per SM
+  std::vector<orbx_tuning> cands;
+  if (forms & 1)
+  for (int r : {2, 4, 8, 16})
+    for (int d : {4, 8, 16})
+      for (int m : {0, 64, 256}) {
         orbx_tuning t = keep;
+        t.batch_form = 0;
         t.nms_rows = r;
         t.describe_blocks_per_sm = d;
         t.match_blocks_per_pair = m;
+        cands.push_back(t);
+      }
+  if (forms & 2)
+  for (int r : {4, 16})
+    for (int m : {0, 64})
+      for (int gsz : {0, 4, 16, 48})
+        for (int bps : {0, 2}) {
+          orbx_tuning t = keep;
+          t.batch_form = 1;
+          t.nms_rows = r;
+          t.match_blocks_per_pair = m;
+          t.persist_group = gsz;
+          t.persist_blocks_per_sm = bps;
+          cands.push_back(t);
+        }
+  orbx_tuning top = keep;
+  float top_ms = 1e30f;
+  int rc = ORBX_OK;
+  for (const orbx_tuning& t : cands) {
+    {
+      {
         if ((rc = orbx_set_tuning(c, &t)) != 0) goto done;
         if ((rc = orbx_batch_pairs(c, n_pairs, ia, ib, oa, ob, ORBX_MATCH_POPC)) != 0) goto done;  // capture
         std::vector<float> ms;
@@ -1320,6 +1491,19 @@ ORBX_API int orbx_debug_buffers(orbx_ctx* c, uint8_t* h_pyr, uint8_t* h_blur, fl
   }
   if (h_total) ORBX_CUDA(cudaMemcpy(h_total, ws.total, sizeof(int), cudaMemcpyDeviceToHost));
   return ORBX_OK;
+}
+
+ORBX_API int orbx_selftest_wait_timeout(orbx_ctx* c, int timeout_us) {
+  if (!c || timeout_us < 1 || timeout_us > 10000000) return ORBX_ERR_ARG;
+  DeviceGuard g(c->device);
+  int* ctr = nullptr;
+  ORBX_CUDA(cudaMallocAsync(&ctr, sizeof(int), c->stream));
+  cudaError_t e = cudaMemsetAsync(ctr, 0, sizeof(int), c->stream);
+  if (e == cudaSuccess)
+    e = launch_wait_selftest(ctr, 1, c->d_err, (long long)timeout_us * c->clock_khz / 1000, c->stream);
+  cudaFreeAsync(ctr, c->stream);
+  ORBX_CUDA(e);
+  return orbx_sync(c);
 }
 
 ORBX_API long long orbx_selftest_pi_minus(uint32_t lo_bits, uint32_t hi_bits) {

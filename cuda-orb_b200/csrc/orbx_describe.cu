@@ -5,51 +5,9 @@
 // one coalesced 31-byte read), reduces the integer moments with shuffles, and
 // every lane then evaluates the angle; lane t builds descriptor byte t from its
 // pattern points, which it keeps in registers for all keypoints it visits.
-#include "orbx_device.cuh"
-#include "orbx_internal.cuh"
+#include "orbx_stages.cuh"
 
 namespace orbx {
-
-constexpr int kDescWarps = 8;
-
-// getValue (orbd.cu:1341-1348): the rotated point is
-// (rint(x*c - y*s), rint(x*s + y*c)), evaluated by the reference build as
-// fma(x, c, -(y*s)) and fma(x, s, y*c).
-__device__ __forceinline__ int sample_at(const uint8_t* center, int pitch, float x, float y, float s, float c) {
-  const int ix = __float2int_rn(__fmaf_rn(x, c, -__fmul_rn(y, s)));
-  const int iy = __float2int_rn(__fmaf_rn(x, s, __fmul_rn(y, c)));
-  return center[(ptrdiff_t)iy * pitch + ix];
-}
-
-template <int WTA>
-__device__ __forceinline__ uint8_t describe_byte(const uint8_t* center, int pitch, const float* px, const float* py,
-                                                 float s, float c) {
-#define G(j) sample_at(center, pitch, px[j], py[j], s, c)
-  uint8_t val = 0;
-  if (WTA == 2) {  // feature2 (orbd.cu:1351-1361)
-#pragma unroll
-    for (int j = 0; j < 8; j++) val |= (uint8_t)((G(2 * j) < G(2 * j + 1)) << j);
-  } else if (WTA == 3) {  // feature3 (orbd.cu:1364-1388), including its index reuse of 8 and skip of 10
-    const int idx[4][3] = {{0, 1, 2}, {3, 4, 5}, {6, 7, 8}, {8, 9, 11}};
-#pragma unroll
-    for (int g = 0; g < 4; g++) {
-      const int t0 = G(idx[g][0]), t1 = G(idx[g][1]), t2 = G(idx[g][2]);
-      const int v = t2 > t1 ? (t2 > t0 ? 2 : 0) : (t1 > t0);
-      val |= (uint8_t)(v << (2 * g));
-    }
-  } else {  // feature4 (orbd.cu:1391-1434)
-#pragma unroll
-    for (int g = 0; g < 4; g++) {
-      int t0 = G(4 * g), t1 = G(4 * g + 1), t2 = G(4 * g + 2), t3 = G(4 * g + 3);
-      int u = 0, v = 2;
-      if (t1 > t0) t0 = t1, u = 1;
-      if (t3 > t2) t2 = t3, v = 3;
-      val |= (uint8_t)((t0 > t2 ? u : v) << (2 * g));
-    }
-  }
-#undef G
-  return val;
-}
 
 template <int WTA>
 __global__ void __launch_bounds__(kDescWarps * 32) k_describe(Batch b) {
@@ -89,13 +47,8 @@ __global__ void __launch_bounds__(kDescWarps * 32) k_describe(Batch b) {
 
   constexpr int PSTEP = (WTA == 3) ? 12 : 16;
   float px[PSTEP], py[PSTEP];
-#pragma unroll
-  for (int j = 0; j < PSTEP; j++) {
-    px[j] = (float)b.pattern[2 * (PSTEP * lane + j)];
-    py[j] = (float)b.pattern[2 * (PSTEP * lane + j) + 1];
-  }
+  load_pattern<WTA>(b, lane, px, py);
 
-  const int u = lane - 15;
   const int gw = blockIdx.x * kDescWarps + (threadIdx.x >> 5);
   const int nw = gridDim.x * kDescWarps;
   for (int i = gw; i < total; i += nw) {
@@ -107,43 +60,7 @@ __global__ void __launch_bounds__(kDescWarps * 32) k_describe(Batch b) {
       else
         hi = mid - 1;
     }
-    const Frame& F = b.frames[lo];
-    const int k = i - s_pref[lo];
-    orbx_point* P = F.pts + k;
-    const int x = P->x, y = P->y, o = P->octave;
-    const int pitch = F.op[o];
-    const long long coff = F.ooff[o] + (long long)(y >> o) * pitch + (x >> o);
-
-    float angle;
-    if (b.describe_mode != kDescribeDescOnly) {
-      // intensity centroid on the raw octave
-      const uint8_t* center = F.pyr + coff;
-      int m10 = 0, m01 = 0;
-      for (int v = -half_k; v <= half_k; v++) {
-        const int um = s_umax[v < 0 ? -v : v];
-        if (lane < 31 && u >= -um && u <= um) {
-          const int val = center[(ptrdiff_t)v * pitch + u];
-          m10 += u * val;
-          m01 += v * val;
-        }
-      }
-#pragma unroll
-      for (int d = 16; d >= 1; d >>= 1) {
-        m10 += __shfl_xor_sync(0xffffffffu, m10, d);
-        m01 += __shfl_xor_sync(0xffffffffu, m01, d);
-      }
-      angle = fast_atan2(__int2float_rn(m01), __int2float_rn(m10));
-      if (lane == 0) P->angle = angle;
-      if (b.describe_mode == kDescribeAngleOnly) continue;
-    } else {
-      angle = P->angle;
-    }
-
-    // rBRIEF on the blurred octave
-    const float sn = __sinf(angle);
-    const float cs = __cosf(angle);
-    const uint8_t byte = describe_byte<WTA>(F.blr + coff, pitch, px, py, sn, cs);
-    F.desc[(size_t)k * 32 + lane] = byte;
+    describe_keypoint<WTA, false>(b, b.frames[lo], i - s_pref[lo], px, py, s_umax, lane);
   }
 }
 

@@ -60,6 +60,7 @@ struct Batch {
   const int* nms_base;   // [n_frames + 1] for k_nms
   unsigned int* nms_ticket;  // dynamic strip ticket (reset by k_pyramid_blur)
   int* err;              // sticky error word (bounded waits that gave up)
+  long long wait_cycles; // bound of every device-side wait, in SM clock cycles
   int describe_mode;     // 0: angle + descriptor, 1: angle only, 2: descriptor only
   // parameters (Orbor::init, orb.h:18-19)
   int fast_thr;
@@ -75,6 +76,7 @@ struct Batch {
 enum : int {
   kErrLookbackTimeout = 1,
   kErrImmaTimeout = 2,
+  kErrStageTimeout = 4,  // persistent batch kernel: a stage dependency never completed
 };
 enum : int { kDescribeBoth = 0, kDescribeAngleOnly = 1, kDescribeDescOnly = 2 };
 

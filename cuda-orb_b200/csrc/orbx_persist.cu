@@ -1,0 +1,230 @@
+// Batched frame pairs in one persistent launch with a device work queue.
+//
+// The reference runs one Orbor::detectAndCompute / Orbor::match call at a time
+// (orb.cpp:57-113).  Here every stage of every frame of a batch is a list of
+// work items: pyramid + blur tiles, detect tiles, NMS strips, describe slices
+// (a share of one frame's keypoints) and match blocks (a share of one pair's
+// k = 2 search).  A host-built run table orders the items; resident blocks
+// claim items from a global counter in that order and run the same stage
+// bodies as the five-launch form (orbx_stages.cuh), so results are identical.
+//
+// Dependencies are per frame: an item of stage k for frame f waits until every
+// item of stage k - 1 for f has finished (a completion counter per stage and
+// frame, released with a fence and read with an acquire).  The run table puts
+// every item after all items it depends on, so the item with the smallest
+// unfinished ticket never waits: progress needs only one resident block, and
+// blocks that are not resident hold no ticket.  Each wait is bounded by
+// wait_cycles of clock64(); on expiry it sets kErrStageTimeout, later waits
+// stop waiting, and the kernel finishes (the host reports ORBX_ERR_TIMEOUT).
+//
+// The run table is built in "waves" of G frames: wave w holds the pyramid
+// tiles of frame group w, the detect tiles of group w - 1, the NMS strips of
+// group w - 2, the describe slices of group w - 3 and the match blocks of the
+// pairs of group w - 4.  G = all frames gives stage-major order; smaller G
+// overlaps the memory-bound pyramid of later frames with the ALU-bound detect
+// of earlier ones.  G and the grid are chosen by the autotuner.
+#include <algorithm>
+
+#include "orbx_stages.cuh"
+#include "orbx_persist.cuh"
+
+namespace orbx {
+
+union PersistSmem {
+  PyrSmem pyr;
+  DetSmem det;
+  NmsSmem nms;
+  struct {
+    int umax[32];
+  } desc;
+  struct {
+    uint4 db[kMChunk * 2];
+    unsigned int last;
+  } match;
+};
+
+constexpr int kPersistThreads = 256;
+
+// Thread 0 waits until *ctr >= need (acquire), bounded by wait_cycles; the
+// block then proceeds together.  After one wait has given up, later waits
+// return at once so the launch drains.
+__device__ __forceinline__ void stage_wait(const int* ctr, int need, int* err, long long wait_cycles) {
+  if (threadIdx.x == 0) {
+    const long long t0 = clock64();
+    for (;;) {
+      int v;
+      asm volatile("ld.acquire.gpu.global.s32 %0, [%1];" : "=r"(v) : "l"(ctr) : "memory");
+      if (v >= need) break;
+      if (*(volatile int*)err & kErrStageTimeout) break;
+      if (clock64() - t0 > wait_cycles) {
+        atomicOr(err, kErrStageTimeout);
+        break;
+      }
+      __nanosleep(64);
+    }
+  }
+  __syncthreads();
+}
+
+__device__ __forceinline__ void stage_done(int* ctr) {
+  __syncthreads();  // every thread's stores of this item precede the release
+  if (threadIdx.x == 0) {
+    __threadfence();
+    atomicAdd(ctr, 1);
+  }
+}
+
+// Run r covers tickets [run_base[r], run_base[r + 1]).
+__device__ __forceinline__ int find_run(const int* run_base, int n_runs, int t) {
+  int lo = 0, hi = n_runs - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (__ldg(run_base + mid) <= t)
+      lo = mid;
+    else
+      hi = mid - 1;
+  }
+  return lo;
+}
+
+template <int WTA>
+__global__ void __launch_bounds__(kPersistThreads, 3) k_batch_persistent(PersistArgs p) {
+  __shared__ PersistSmem sm;
+  __shared__ int s_item;
+  const Batch& b = p.b;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int total = p.run_base_host_total;
+  for (;;) {
+    __syncthreads();  // the previous item is done with shared memory and s_item
+    if (threadIdx.x == 0) s_item = (int)atomicAdd(p.item_counter, 1u);
+    __syncthreads();
+    const int t = s_item;
+    if (t >= total) break;
+    const int r = find_run(p.run_base, p.n_runs, t);
+    const PersistRun run = p.runs[r];
+    const int local = t - __ldg(p.run_base + r);
+    const int f = run.frame;
+    int* done = p.done;
+    const int nf = b.n_frames;
+    switch (run.stage) {
+      case kStagePyr:
+        pyr_tile(b, __ldg(b.pyr_base + f) + local, sm.pyr);
+        stage_done(done + 0 * nf + f);
+        break;
+      case kStageDet:
+        stage_wait(done + 0 * nf + f, __ldg(b.pyr_base + f + 1) - __ldg(b.pyr_base + f), b.err, b.wait_cycles);
+        det_tile<true>(b, __ldg(b.det_base + f) + local, sm.det);
+        stage_done(done + 1 * nf + f);
+        break;
+      case kStageNms:
+        stage_wait(done + 1 * nf + f, __ldg(b.det_base + f + 1) - __ldg(b.det_base + f), b.err, b.wait_cycles);
+        nms_strip<true>(b, __ldg(b.nms_base + f) + local, sm.nms);
+        stage_done(done + 2 * nf + f);
+        break;
+      case kStageDesc: {
+        stage_wait(done + 2 * nf + f, __ldg(b.nms_base + f + 1) - __ldg(b.nms_base + f), b.err, b.wait_cycles);
+        if (threadIdx.x < b.half_k + 1) sm.desc.umax[threadIdx.x] = __ldg(b.umax + threadIdx.x);
+        __syncthreads();
+        const Frame& F = b.frames[f];
+        const int n = __ldcg(F.count);
+        const int slices = __ldg(p.desc_base + f + 1) - __ldg(p.desc_base + f);
+        const int k0 = (int)((long long)n * local / slices);
+        const int k1 = (int)((long long)n * (local + 1) / slices);
+        constexpr int PSTEP = (WTA == 3) ? 12 : 16;
+        float px[PSTEP], py[PSTEP];
+        load_pattern<WTA>(b, lane, px, py);
+        for (int k = k0 + warp; k < k1; k += kPersistThreads / 32)
+          describe_keypoint<WTA, true>(b, F, k, px, py, sm.desc.umax, lane);
+        stage_done(done + 3 * nf + f);
+        break;
+      }
+      default: {  // kStageMatch: run.frame is frame A of pair f / 2
+        const int fa = f, fb = f + 1;
+        stage_wait(done + 3 * nf + fa, __ldg(p.desc_base + fa + 1) - __ldg(p.desc_base + fa), b.err,
+                   b.wait_cycles);
+        stage_wait(done + 3 * nf + fb, __ldg(p.desc_base + fb + 1) - __ldg(p.desc_base + fb), b.err,
+                   b.wait_cycles);
+        const MatchJob& J = p.jobs[f >> 1];
+        match_popc_block<kPersistThreads, true>(J.args, J.work, local, p.blocks_per_job, sm.match.db,
+                                                sm.match.last);
+        break;
+      }
+    }
+  }
+}
+
+int persist_blocks_per_sm(int wta_k) {
+  int n = 0;
+  cudaError_t e;
+  if (wta_k == 3)
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_batch_persistent<3>, kPersistThreads, 0);
+  else if (wta_k == 4)
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_batch_persistent<4>, kPersistThreads, 0);
+  else
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_batch_persistent<2>, kPersistThreads, 0);
+  if (e != cudaSuccess) {
+    (void)cudaGetLastError();
+    return 0;
+  }
+  return n;
+}
+
+cudaError_t launch_batch_persistent(const PersistArgs& p, int blocks, cudaStream_t s) {
+  if (blocks <= 0 || p.run_base_host_total <= 0) return cudaSuccess;
+  if (p.b.wta_k == 3)
+    k_batch_persistent<3><<<blocks, kPersistThreads, 0, s>>>(p);
+  else if (p.b.wta_k == 4)
+    k_batch_persistent<4><<<blocks, kPersistThreads, 0, s>>>(p);
+  else
+    k_batch_persistent<2><<<blocks, kPersistThreads, 0, s>>>(p);
+  return cudaGetLastError();
+}
+
+// A wait on a counter that nothing increments: the bounded-wait path of the
+// persistent kernel, run on its own so that a test can make it expire.
+__global__ void k_wait_selftest(const int* ctr, int need, int* err, long long wait_cycles) {
+  stage_wait(ctr, need, err, wait_cycles);
+}
+
+cudaError_t launch_wait_selftest(const int* ctr, int need, int* err, long long wait_cycles, cudaStream_t s) {
+  k_wait_selftest<<<1, 32, 0, s>>>(ctr, need, err, wait_cycles);
+  return cudaGetLastError();
+}
+
+// Host side: the run table in waves of `group` frames (pairs kept whole).
+void build_persist_runs(int nf, int group, const int* pyr_n, const int* det_n, const int* nms_n,
+                        const int* desc_n, int match_per_pair, std::vector<PersistRun>* runs,
+                        std::vector<int>* run_base) {
+  runs->clear();
+  run_base->clear();
+  if (group < 2) group = 2;
+  group += group & 1;
+  const int groups = (nf + group - 1) / group;
+  int acc = 0;
+  auto add = [&](int stage, int frame, int count) {
+    if (count <= 0) return;
+    runs->push_back(PersistRun{stage, frame});
+    run_base->push_back(acc);
+    acc += count;
+  };
+  for (int w = 0; w < groups + kNumStages - 1; w++) {
+    for (int k = 0; k < kNumStages; k++) {
+      const int g = w - k;
+      if (g < 0 || g >= groups) continue;
+      const int f0 = g * group, f1 = std::min(nf, f0 + group);
+      for (int f = f0; f < f1; f++) {
+        switch (k) {
+          case kStagePyr: add(k, f, pyr_n[f]); break;
+          case kStageDet: add(k, f, det_n[f]); break;
+          case kStageNms: add(k, f, nms_n[f]); break;
+          case kStageDesc: add(k, f, desc_n[f]); break;
+          default:
+            if ((f & 1) == 0) add(k, f, match_per_pair);
+        }
+      }
+    }
+  }
+  run_base->push_back(acc);
+}
+
+}  // namespace orbx

@@ -1,0 +1,41 @@
+// Persistent batch kernel (orbx_persist.cu): work-item run table and launch arguments.
+#pragma once
+#include <vector>
+
+#include "orbx_internal.cuh"
+
+namespace orbx {
+
+enum : int { kStagePyr = 0, kStageDet = 1, kStageNms = 2, kStageDesc = 3, kStageMatch = 4, kNumStages = 5 };
+
+// A run of consecutive tickets: every item of one stage of one frame (for the
+// match stage, frame = frame A of the pair).
+struct PersistRun {
+  int stage;
+  int frame;
+};
+
+struct PersistArgs {
+  Batch b;
+  const PersistRun* runs;
+  const int* run_base;       // [n_runs + 1] first ticket of each run
+  int n_runs;
+  int run_base_host_total;   // total tickets
+  const int* desc_base;      // [n_frames + 1] prefix of describe slices per frame
+  int* done;                 // [4][n_frames] completed items per (stage, frame); zero at launch
+  unsigned int* item_counter;  // zero at launch
+  const MatchJob* jobs;      // one per pair
+  int blocks_per_job;        // match items per pair
+};
+
+// Level-0 pixels per describe slice: a frame's keypoints are split into
+// ceil(w * h / kDescSlicePixels) slices.
+constexpr int kDescSlicePixels = 65536;
+
+int persist_blocks_per_sm(int wta_k);
+cudaError_t launch_batch_persistent(const PersistArgs& p, int blocks, cudaStream_t s);
+cudaError_t launch_wait_selftest(const int* ctr, int need, int* err, long long wait_cycles, cudaStream_t s);
+void build_persist_runs(int nf, int group, const int* pyr_n, const int* det_n, const int* nms_n, const int* desc_n,
+                        int match_per_pair, std::vector<PersistRun>* runs, std::vector<int>* run_base);
+
+}  // namespace orbx

@@ -1,0 +1,947 @@
+// Stage bodies of the sm_100a ORB pipeline as device functions: pyramid +
+// blur tiles, FAST-9 + score tiles and NMS strips.  Each kernel of the
+// five-launch form (orbx_detect.cu) runs one of them per block, and the
+// persistent batch kernel (orbx_persist.cu) runs them per claimed work item.
+#pragma once
+#include "orbx_device.cuh"
+#include "orbx_internal.cuh"
+#include "orbx_fast.cuh"
+
+namespace orbx {
+
+// Loads of data a stage reads.  Standalone kernels read their inputs through
+// the read-only path; in the persistent kernel a stage reads what an earlier
+// stage wrote in the same launch, after an acquire, so it uses plain
+// (coherent) cached loads instead.
+template <bool P, class T>
+__device__ __forceinline__ T ldx(const T* p) {
+  if constexpr (P)
+    return __ldca(p);
+  else
+    return __ldg(p);
+}
+
+
+// ---------------------------------------------------------------------------
+// Pyramid + blur
+//
+// Octave o is the nearest-neighbour decimation img[y<<o][x<<o] of level 0
+// (gDownSampleUnroll4, orbd.cu:514-535; octave 0 is a copy, orbd.cu:1584).
+// The blurred pyramid is the separable 7-tap sigma-2 filter of each octave with
+// reflect-101 borders (gConv2dUnroll, orbd.cu:1273-1338), computed here out of
+// place, so it has no dependence on block scheduling.  One block owns a
+// kPyrTW x kPyrTH octave tile: it stages the tile plus a 3-pixel reflected
+// halo in shared memory, writes the raw tile, and blurs it.  With pyr_src set
+// the octaves are read from an existing pyramid instead (hGassianBlur on a
+// caller's buffer, orbd.cu:1732-1773).
+// ---------------------------------------------------------------------------
+constexpr int kPyrSW = kPyrTW + 8;  // 3-pixel halo each side, padded to a multiple of 4
+constexpr int kPyrSH = kPyrTH + 6;
+
+// Exact small-integer <-> float conversions on the full-rate pipes: a float
+// whose exponent field is 2^23 holds the integer in its mantissa.
+__device__ __forceinline__ float u8_to_float(uint32_t x) {  // 0 <= x < 2^23
+  return __fsub_rn(__uint_as_float(0x4B000000u | x), 8388608.0f);
+}
+__device__ __forceinline__ uint32_t float_to_u8_rne(float v) {  // 0 <= v < 2^22: round to nearest, ties to even
+  return (uint32_t)(__float_as_int(__fadd_rn(v, 12582912.0f)) - 0x4B400000);
+}
+
+struct PyrSmem {
+  __align__(16) float src[kPyrSH * kPyrSW];
+  __align__(16) uint8_t byte[kPyrSH * kPyrSW];
+  __align__(16) float row[kPyrSH * kPyrTW];
+};
+
+// One pyramid tile (tile index t over the batch).  It reads only the caller's
+// images, so it needs no load policy.
+__device__ __forceinline__ void pyr_tile(const Batch& b, int t, PyrSmem& sm) {
+  float* s_src = sm.src;
+  uint8_t* s_byte = sm.byte;
+  float* s_row = sm.row;
+  const int f = find_frame(b.pyr_base, b.n_frames, t);
+  const Frame& F = b.frames[f];
+  int lt = t - b.pyr_base[f];
+  int o = 0;
+  while (o + 1 < F.n_oct && lt >= F.pyr_tile_base[o + 1]) o++;
+  lt -= F.pyr_tile_base[o];
+  const int tiles_x = F.pyr_tiles_x[o];
+  const int x0 = (lt % tiles_x) * kPyrTW;
+  const int y0 = (lt / tiles_x) * kPyrTH;
+  const int ow = F.ow[o], oh = F.oh[o], op = F.op[o];
+  const uint8_t* __restrict__ img = F.img;
+  const int pitch_in = F.pitch_in;
+
+  // Per-frame housekeeping for the later stages of the same batch.
+  if (o == 0 && lt == 0) {
+    for (int i = threadIdx.x; i < F.nms_strips; i += blockDim.x) F.nms_status[i] = 0ull;
+    if (threadIdx.x == 0) {
+      *F.count = 0;
+      if (F.total) *F.total = 0;
+    }
+  }
+  if (t == 0 && threadIdx.x == 0) *b.nms_ticket = 0u;
+
+  // stage: source rows y0-3 .. y0+34, columns x0-3 .. x0+132, reflect-101 at
+  // the octave edges, as floats and as bytes
+  const uint8_t* __restrict__ psrc = F.pyr_src ? F.pyr_src + F.ooff[o] : nullptr;
+  // octave 0 read from a 4-byte aligned image: interior groups take two aligned
+  // words (the group starts one byte past a word boundary, x0 being a multiple of 4)
+  const bool words0 = (o == 0) && !psrc && ((reinterpret_cast<uintptr_t>(img) | (uintptr_t)pitch_in) & 3u) == 0;
+  constexpr int kGroups = kPyrSW / 4;
+  for (int it = threadIdx.x; it < kPyrSH * kGroups; it += blockDim.x) {
+    const int r = it / kGroups;
+    const int g = it - r * kGroups;
+    const int y = reflect101(y0 - 3 + r, oh);
+    const uint8_t* rowp = psrc ? psrc + (size_t)y * op : img + (size_t)(y << o) * pitch_in;
+    const int sh = psrc ? 0 : o;
+    const int cx = x0 - 3 + 4 * g;
+    uint32_t v[4];
+    if (words0 && cx >= 1 && cx + 3 < ow) {
+      // bytes cx-1 .. cx+6 lie in [0, pitch_in): cx + 3 < ow <= pitch_in and both words are aligned
+      const uint32_t* wp = reinterpret_cast<const uint32_t*>(rowp + (cx - 1));
+      const uint32_t word = __byte_perm(__ldg(wp), __ldg(wp + 1), 0x4321);
+#pragma unroll
+      for (int j = 0; j < 4; j++) v[j] = (word >> (8 * j)) & 0xFFu;
+    } else {
+#pragma unroll
+      for (int j = 0; j < 4; j++) v[j] = __ldg(rowp + (reflect101(cx + j, ow) << sh));
+    }
+    reinterpret_cast<float4*>(s_src)[it] = make_float4(u8_to_float(v[0]), u8_to_float(v[1]), u8_to_float(v[2]),
+                                                       u8_to_float(v[3]));
+    reinterpret_cast<uint32_t*>(s_byte)[it] = v[0] | (v[1] << 8) | (v[2] << 16) | (v[3] << 24);
+  }
+  __syncthreads();
+
+  const float* k = b.gauss;
+  // horizontal pass: 4 consecutive outputs per thread; integer tap sums are
+  // exact in float, so they are summed as floats
+  for (int it = threadIdx.x; it < kPyrSH * (kPyrTW / 4); it += blockDim.x) {
+    const int r = it / (kPyrTW / 4);
+    const int g = it - r * (kPyrTW / 4);
+    const float4* q = reinterpret_cast<const float4*>(s_src + r * kPyrSW) + g;
+    const float4 a0 = q[0], a1 = q[1], a2 = q[2];
+    const float p[12] = {a0.x, a0.y, a0.z, a0.w, a1.x, a1.y, a1.z, a1.w, a2.x, a2.y, a2.z, a2.w};
+    float4 out;
+    float* op4 = &out.x;
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+      const float t1 = __fadd_rn(p[j + 2], p[j + 4]);
+      const float t2 = __fadd_rn(p[j + 1], p[j + 5]);
+      const float t3 = __fadd_rn(p[j], p[j + 6]);
+      op4[j] = gauss_dot4(k, p[j + 3], t1, t2, t3);
+    }
+    reinterpret_cast<float4*>(s_row + r * kPyrTW)[g] = out;
+  }
+  __syncthreads();
+
+  // vertical pass and stores: 4 consecutive columns of one row per thread
+  uint8_t* P = F.pyr + F.ooff[o];
+  uint8_t* B = F.blr + F.ooff[o];
+  const bool copy_pad = (o == 0) && (pitch_in == op);
+  for (int it = threadIdx.x; it < kPyrTH * (kPyrTW / 4); it += blockDim.x) {
+    const int r = it / (kPyrTW / 4);
+    const int g = it - r * (kPyrTW / 4);
+    const int y = y0 + r;
+    const int x = x0 + 4 * g;
+    if (y >= oh || x >= op) continue;
+    float4 h[7];
+#pragma unroll
+    for (int j = 0; j < 7; j++) h[j] = reinterpret_cast<const float4*>(s_row + (r + j) * kPyrTW)[g];
+    const float* hf = reinterpret_cast<const float*>(h);
+    uint32_t bw = 0;
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+      const float t1 = __fadd_rn(hf[8 + j], hf[16 + j]);
+      const float t2 = __fadd_rn(hf[4 + j], hf[20 + j]);
+      const float t3 = __fadd_rn(hf[j], hf[24 + j]);
+      bw |= (float_to_u8_rne(gauss_dot4(k, hf[12 + j], t1, t2, t3)) & 0xFFu) << (8 * j);
+    }
+    // raw bytes of the same 4 pixels: staged columns 4g+3 .. 4g+6 of row r+3
+    const uint32_t* sb = reinterpret_cast<const uint32_t*>(s_byte + (r + 3) * kPyrSW) + g;
+    const uint32_t pw = __byte_perm(sb[0], sb[1], 0x6543);
+    const size_t a = (size_t)y * op + x;
+    if (x + 4 <= ow) {
+      *reinterpret_cast<uint32_t*>(B + a) = bw;
+      *reinterpret_cast<uint32_t*>(P + a) = pw;
+    } else {
+      // the group reaches into the row padding: octave 0 carries the caller's
+      // padding bytes (the reference copies h * pitch0 bytes, orbd.cu:1584),
+      // other octaves hold zeros
+#pragma unroll
+      for (int j = 0; j < 4; j++) {
+        if (x + j < ow) {
+          B[a + j] = (uint8_t)(bw >> (8 * j));
+          P[a + j] = (uint8_t)(pw >> (8 * j));
+        } else {
+          const uint8_t v = psrc ? __ldg(psrc + a + j)
+                                 : (copy_pad ? __ldg(img + (size_t)y * pitch_in + x + j) : (uint8_t)0);
+          B[a + j] = v;
+          P[a + j] = v;
+        }
+      }
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// FAST-9 + score -> level-0 keyed score map
+//
+// gCalcExtramaMap (orbd.cu:672-756) run for octaves 0..n-1 in order
+// (orbd.cu:1616-1634): a pixel is a corner when 9 contiguous ring pixels are
+// all darker than v - t or all brighter than v + t (the reference's LUT pre-test
+// and arc loop decide exactly this).  Its score lands at level-0 position
+// (x << o, y << o) if strictly greater than what a lower octave put there.
+// One block owns a kDetTW x kDetTH level-0 tile and all octave pixels that map
+// into it; it stages each octave's pixels with a 4-pixel halo (the Harris
+// window with its Sobel reach) in shared memory using the pyramid's linear
+// addressing, so reads past an octave edge return the same neighbouring bytes
+// as in the reference, merges the octaves in shared memory, and writes the
+// tile's occupancy bits densely and its scores sparsely (no clearing pass).
+// ---------------------------------------------------------------------------
+constexpr int kHalo = 4;
+__host__ __device__ constexpr int det_stage_off(int octave) {
+  int s = 0;
+  for (int o = 0; o < octave; o++) s += ((kDetTW >> o) + 2 * kHalo) * ((kDetTH >> o) + 2 * kHalo);
+  return s;
+}
+__host__ __device__ constexpr int det_stage_bytes() { return det_stage_off(kMaxOctaves); }
+
+// dHarrisScore (orbd.cu:651-669) on a shared-memory tile of row stride sw.
+// Integer sums wrap as 32-bit; the final combine is
+// fma(-0.04f, (float)(uint32)(dsxy*dsxy), (float)(int32)(dxx*dyy - dxy*dxy)) * scale^4,
+// which is how the reference build evaluates
+// (dxx*dyy - dxy*dxy - HARRIS_K*(dsxy*dsxy)) * d_scale_sq_sq.
+__device__ __forceinline__ float harris_score(const uint8_t* c, int sw, float scale4) {
+  int dxx = 0, dyy = 0, dxy = 0;
+#pragma unroll 1
+  for (int i = -3; i <= 3; i++) {
+#pragma unroll
+    for (int j = -3; j <= 3; j++) {
+      const uint8_t* q = c + i * sw + j;
+      const int dx = ((int)q[1] - (int)q[-1]) * 2 + ((int)q[-sw + 1] - (int)q[-sw - 1]) +
+                     ((int)q[sw + 1] - (int)q[sw - 1]);
+      const int dy = ((int)q[sw] - (int)q[-sw]) * 2 + ((int)q[sw - 1] - (int)q[-sw - 1]) +
+                     ((int)q[sw + 1] - (int)q[-sw + 1]);
+      dxx += dx * dx;
+      dyy += dy * dy;
+      dxy += dx * dy;
+    }
+  }
+  return harris_combine(dxx, dyy, dxy, scale4);
+}
+
+// Byte-wise arithmetic on packed words with plain integer operations (the
+// byte-SIMD intrinsics are several instructions each on this architecture).
+constexpr uint32_t kB7 = 0x80808080u, kLo7 = 0x7F7F7F7Fu;
+// bit 7 of each byte set where x < y (unsigned): the 7-bit differences cannot
+// borrow across bytes, and the top bits decide when they differ
+__device__ __forceinline__ uint32_t swar_lt(uint32_t x, uint32_t y) {
+  const uint32_t t = (x | kB7) - (y & kLo7);
+  return ((~x & y) | (~(x ^ y) & ~t)) & kB7;
+}
+// max(v - t, 0) and min(v + t, 255) per byte, t given in every byte
+__device__ __forceinline__ uint32_t swar_sub_sat(uint32_t v, uint32_t t4) {
+  const uint32_t d = ((v | kB7) - (t4 & kLo7)) ^ ((v ^ ~t4) & kB7);
+  return d & ~((swar_lt(v, t4) >> 7) * 0xFFu);
+}
+__device__ __forceinline__ uint32_t swar_add_sat(uint32_t v, uint32_t t4) {
+  const uint32_t s = ((v & kLo7) + (t4 & kLo7)) ^ ((v ^ t4) & kB7);
+  const uint32_t carry = ((v & t4) | ((v | t4) & ~s)) & kB7;
+  return s | ((carry >> 7) * 0xFFu);
+}
+
+// Necessary condition for FAST-9: every run of 9 ring pixels contains two
+// neighbouring cardinal points (ring positions k and k+4, k = 0, 4, 8, 12), so
+// both of some such pair must be darker than v - t, or both brighter than
+// v + t.  It never changes a result.  Evaluated for four horizontally adjacent
+// centres at once on packed bytes: w points at the aligned word holding them
+// (row stride sw bytes, a multiple of 4); returns bit 7 of each byte whose
+// centre passes.  Saturating v - t and v + t (t <= 255) give the same answers
+// as the signed comparisons p < v - t and p > v + t.
+__device__ __forceinline__ uint32_t fast9_pretest4(const uint8_t* w, int sw, uint32_t t4) {
+  const uint32_t c = *reinterpret_cast<const uint32_t*>(w);
+  const uint32_t cl = *reinterpret_cast<const uint32_t*>(w - 4);
+  const uint32_t cr = *reinterpret_cast<const uint32_t*>(w + 4);
+  const uint32_t p0 = *reinterpret_cast<const uint32_t*>(w + 3 * sw);   // ring 0: (x, y + 3)
+  const uint32_t p8 = *reinterpret_cast<const uint32_t*>(w - 3 * sw);   // ring 8: (x, y - 3)
+  const uint32_t p4 = __byte_perm(c, cr, 0x6543);                       // ring 4: (x + 3, y)
+  const uint32_t p12 = __byte_perm(cl, c, 0x4321);                      // ring 12: (x - 3, y)
+  const uint32_t lo = swar_sub_sat(c, t4), hi = swar_add_sat(c, t4);
+  const uint32_t d0 = swar_lt(p0, lo), d4 = swar_lt(p4, lo), d8 = swar_lt(p8, lo), d12 = swar_lt(p12, lo);
+  const uint32_t b0 = swar_lt(hi, p0), b4 = swar_lt(hi, p4), b8 = swar_lt(hi, p8), b12 = swar_lt(hi, p12);
+  return ((d0 | d8) & (d4 | d12)) | ((b0 | b8) & (b4 | b12));
+}
+
+__device__ __forceinline__ float corner_score(const Batch& b, const uint8_t* c, int sw) {
+  if (b.harris) return harris_score(c, sw, b.harris_scale4);
+  const int v = c[0];
+  int d[25];
+#pragma unroll
+  for (int k = 0; k < 25; k++) d[k] = (int)(short)(v - c[c_ring[k & 15][1] * sw + c_ring[k & 15][0]]);
+  return fast_score(d, b.fast_thr);
+}
+
+// Tile-level candidate lists hold (octave, row, column) of the octave tile as
+// o << 11 | ly << 6 | lx; a tile has at most 2048 + 512 + 128 + 32 + 8 pixels.
+constexpr int kDetMaxCand = 2728;
+__device__ __forceinline__ uint16_t det_item(int o, int ly, int lx) { return (uint16_t)((o << 11) | (ly << 6) | lx); }
+
+// Merge key of a level-0 position: the larger score wins and, between equal
+// scores, the lower octave (the reference visits octaves in increasing order
+// and replaces only on a strictly larger score).  Only scores > 0 are stored.
+__device__ __forceinline__ unsigned long long det_key(float score, int o) {
+  return ((unsigned long long)__float_as_uint(score) << 32) | (unsigned)(7 - o);
+}
+
+struct DetSmem {
+  __align__(16) uint8_t stage[det_stage_bytes()];
+  __align__(16) unsigned long long key[kDetTH * kDetTW];
+  uint16_t cand[kDetMaxCand];
+  uint16_t corner[kDetMaxCand];
+  int n[2];
+  uint32_t occ[kDetTH * kDetTW / 32];
+  int ow[kMaxOctaves], oh[kMaxOctaves];
+};
+
+// One detect tile (tile index t over the batch).  P: the raw pyramid was
+// written earlier in the same launch (coherent loads instead of the read-only path).
+template <bool P>
+__device__ __forceinline__ void det_tile(const Batch& b, int t, DetSmem& sm) {
+  uint8_t* s_stage = sm.stage;
+  unsigned long long* s_key = sm.key;
+  uint16_t* s_cand = sm.cand;
+  uint16_t* s_corner = sm.corner;
+  int* s_n = sm.n;
+  uint32_t* s_occ = sm.occ;
+  int* s_ow = sm.ow;
+  int* s_oh = sm.oh;
+  const int f = find_frame(b.det_base, b.n_frames, t);
+  const Frame& F = b.frames[f];
+  const int lt = t - b.det_base[f];
+  const int X0 = (lt % F.det_tiles_x) * kDetTW;
+  const int Y0 = (lt / F.det_tiles_x) * kDetTH;
+  const int n_oct = F.n_oct;
+  const uint8_t* __restrict__ pyr = F.pyr;
+  const int lane = threadIdx.x & 31;
+  const int warp = threadIdx.x >> 5;
+  const int thr = b.fast_thr;
+
+  for (int i = threadIdx.x; i < kDetTH * kDetTW / 2; i += blockDim.x)
+    reinterpret_cast<ulonglong2*>(s_key)[i] = make_ulonglong2(0ull, 0ull);
+  if (threadIdx.x < kDetTH * kDetTW / 32) s_occ[threadIdx.x] = 0u;
+  if (threadIdx.x < 2) s_n[threadIdx.x] = 0;
+  if (threadIdx.x < kMaxOctaves) {
+    s_ow[threadIdx.x] = threadIdx.x < n_oct ? F.ow[threadIdx.x] : 0;
+    s_oh[threadIdx.x] = threadIdx.x < n_oct ? F.oh[threadIdx.x] : 0;
+  }
+  // Stage every octave's tile with its halo, 4 bytes per load, one row per warp
+  // and step: octave offsets and pitches are multiples of 128 and (X0 >> o) - 4
+  // is a multiple of 4; a staged row is at most 18 words.
+  for (int o = 0; o < n_oct; o++) {
+    const int sw = (kDetTW >> o) + 2 * kHalo;
+    const int sh = (kDetTH >> o) + 2 * kHalo;
+    const int sw4 = sw >> 2;
+    const int op = F.op[o];
+    const long long base = F.ooff[o] + (long long)((Y0 >> o) - kHalo) * op + ((X0 >> o) - kHalo);
+    uint32_t* dst = reinterpret_cast<uint32_t*>(s_stage + det_stage_off(o));
+    if (lane < sw4)
+      for (int r = warp; r < sh; r += 8)
+        dst[r * sw4 + lane] = ldx<P>(reinterpret_cast<const uint32_t*>(pyr + base + (long long)r * op) + lane);
+  }
+  __syncthreads();
+
+  // 1. cardinal pre-test, four centres per word, words of every octave spread
+  //    over the whole block (octave o has (32 >> o) rows of (16 >> o) words)
+  {
+    const uint32_t t4 = (uint32_t)min(max(thr, 0), 255) * 0x01010101u;
+    int total = 0;
+    for (int o = 0; o < n_oct; o++) total += 512 >> (2 * o);
+    for (int i = threadIdx.x; i < total; i += blockDim.x) {
+      int o = 0, w = i;
+      while (w >= (512 >> (2 * o))) {
+        w -= 512 >> (2 * o);
+        o++;
+      }
+      const int nwl = 4 - o;  // log2 words per row
+      const int ly = w >> nwl, lx = (w & ((1 << nwl) - 1)) << 2;
+      const int x = (X0 >> o) + lx, y = (Y0 >> o) + ly;
+      const int ow = s_ow[o], oh = s_oh[o];
+      uint32_t m = 0u;
+      if (y >= 3 && y < oh - 3 && x < ow - 3) {
+        const int sw = (kDetTW >> o) + 2 * kHalo;
+        m = fast9_pretest4(s_stage + det_stage_off(o) + (ly + kHalo) * sw + (lx + kHalo), sw, t4);
+        if (x < 3 || x + 3 >= ow - 3) {  // border word: keep the centres with 3 <= x + k < ow - 3
+          uint32_t vm = 0u;
+#pragma unroll
+          for (int k = 0; k < 4; k++)
+            if (x + k >= 3 && x + k < ow - 3) vm |= 0xFFu << (8 * k);
+          m &= vm;
+        }
+      }
+      m &= 0x80808080u;
+      if (m) {
+        int pos = atomicAdd(&s_n[0], __popc(m));
+        while (m) {
+          const int k = (__ffs(m) >> 3) - 1;
+          m &= m - 1u;
+          s_cand[pos++] = det_item(o, ly, lx + k);
+        }
+      }
+    }
+  }
+  __syncthreads();
+
+  // 2. full 9-arc segment test of the candidates
+  {
+    const int n1 = s_n[0];
+    for (int j = threadIdx.x; j < n1; j += blockDim.x) {
+      const int e = s_cand[j];
+      const int o = e >> 11, ly = (e >> 6) & 31, lx = e & 63;
+      const int sw = (kDetTW >> o) + 2 * kHalo;
+      const uint8_t* c = s_stage + det_stage_off(o) + (ly + kHalo) * sw + (lx + kHalo);
+      const int v = c[0];
+      if (fast9_full(c, sw, v - thr, v + thr)) s_corner[atomicAdd(&s_n[1], 1)] = (uint16_t)e;
+    }
+  }
+  __syncthreads();
+
+  // 3. scores of the corners, merged into the level-0 map
+  {
+    const int n2 = s_n[1];
+    if (b.harris) {
+      // 32 groups of 8 lanes, one corner per group; lane s of a group takes
+      // window positions s, s + 8, ... of the 7x7 Harris window (the 32-bit sums
+      // wrap, so their order is free)
+      const int gid = threadIdx.x >> 3, sub = threadIdx.x & 7;
+      for (int j0 = 0; j0 < n2; j0 += 32) {
+        if (j0 + 4 * warp >= n2) break;  // this warp's four groups have no corner (warp-uniform)
+        const int j = j0 + gid;
+        int dxx = 0, dyy = 0, dxy = 0;
+        int e = 0;
+        if (j < n2) {
+          e = s_corner[j];
+          const int o = e >> 11, ly = (e >> 6) & 31, lx = e & 63;
+          const int sw = (kDetTW >> o) + 2 * kHalo;
+          const uint8_t* c = s_stage + det_stage_off(o) + (ly + kHalo) * sw + (lx + kHalo);
+          for (int pos = sub; pos < 49; pos += 8) {
+            const int wy = pos / 7 - 3, wx = pos % 7 - 3;
+            const uint8_t* q = c + wy * sw + wx;
+            const int dx = ((int)q[1] - (int)q[-1]) * 2 + ((int)q[-sw + 1] - (int)q[-sw - 1]) +
+                           ((int)q[sw + 1] - (int)q[sw - 1]);
+            const int dy = ((int)q[sw] - (int)q[-sw]) * 2 + ((int)q[sw - 1] - (int)q[-sw - 1]) +
+                           ((int)q[sw + 1] - (int)q[-sw + 1]);
+            dxx += dx * dx;
+            dyy += dy * dy;
+            dxy += dx * dy;
+          }
+        }
+#pragma unroll
+        for (int d = 4; d >= 1; d >>= 1) {
+          dxx += __shfl_xor_sync(0xffffffffu, dxx, d);
+          dyy += __shfl_xor_sync(0xffffffffu, dyy, d);
+          dxy += __shfl_xor_sync(0xffffffffu, dxy, d);
+        }
+        if (j < n2 && sub == 0) {
+          const int o = e >> 11, ly = (e >> 6) & 31, lx = e & 63;
+          const float score = harris_combine(dxx, dyy, dxy, b.harris_scale4);
+          if (score > 0.f) {
+            const int m = (ly << o) * kDetTW + (lx << o);
+            if (atomicMax(&s_key[m], det_key(score, o)) == 0ull) atomicOr(&s_occ[m >> 5], 1u << (m & 31));
+          }
+        }
+      }
+    } else {
+      for (int j = threadIdx.x; j < n2; j += blockDim.x) {
+        const int e = s_corner[j];
+        const int o = e >> 11, ly = (e >> 6) & 31, lx = e & 63;
+        const int sw = (kDetTW >> o) + 2 * kHalo;
+        const float score = corner_score(b, s_stage + det_stage_off(o) + (ly + kHalo) * sw + (lx + kHalo), sw);
+        if (score > 0.f) {
+          const int m = (ly << o) * kDetTW + (lx << o);
+          if (atomicMax(&s_key[m], det_key(score, o)) == 0ull) atomicOr(&s_occ[m >> 5], 1u << (m & 31));
+        }
+      }
+    }
+  }
+  __syncthreads();
+
+  // Output: the tile's occupancy words (every word written, so no clearing
+  // pass), then score and octave only where a bit is set.  The tile's 64
+  // columns are two aligned 32-bit words of each row (pitch0 is a multiple of 128).
+  if (threadIdx.x < kDetTH * kDetTW / 32) {
+    const int r = threadIdx.x >> 1, half = threadIdx.x & 1;
+    const int Y = Y0 + r;
+    if (Y < F.h) {
+      uint32_t m = s_occ[threadIdx.x];
+      const size_t a0 = (size_t)Y * F.op[0] + X0 + 32 * half;
+      F.occ[a0 >> 5] = m;
+      while (m) {
+        const int k = __ffs(m) - 1;
+        m &= m - 1u;
+        const unsigned long long key = s_key[r * kDetTW + 32 * half + k];
+        F.vmap[a0 + k] = __uint_as_float((uint32_t)(key >> 32));
+        F.oct8[a0 + k] = (uint8_t)(7 - (int)(key & 0xFFu));
+      }
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// NMS + ordered compaction
+//
+// gNmsUnroll4 (orbd.cu:919-983): a level-0 position with score v > 0 from
+// octave o survives unless a neighbour in the square of radius 2^o has a larger
+// score, or an equal one at dx <= 0 && dy <= 0.  The reference appends
+// survivors with atomicInc (order and, past max_pts, the kept subset depend on
+// scheduling).  Here each block takes a full-width strip of F.nms_rows rows in
+// ticket order, ranks its survivors with warp ballots, and chains strip totals
+// with a decoupled look-back, so keypoints come out in raster order and the cap
+// keeps the first max_pts of them.
+// ---------------------------------------------------------------------------
+constexpr unsigned long long kFlagAgg = 1ull << 32;
+constexpr unsigned long long kFlagPre = 2ull << 32;
+
+// Warp 0 of a strip's block resolves the strip's exclusive prefix: it reads the
+// look-back words of up to 32 predecessors per round with acquire loads, and
+// stops at the nearest one that already carries an inclusive prefix.  The wait
+// for a predecessor is bounded by wait_cycles of clock64(); on expiry it sets
+// kErrLookbackTimeout and returns the prefix found so far.
+__device__ __forceinline__ int nms_lookback(unsigned long long* st, int s, int lane, int* err,
+                                            long long wait_cycles) {
+  int excl = 0;
+  int j = s - 1;
+  const long long t0 = clock64();
+  while (j >= 0) {
+    const int idx = j - lane;
+    const unsigned long long wv = (idx >= 0) ? ld_acquire_u64(&st[idx]) : kFlagPre;
+    const unsigned long long flag = wv & (3ull << 32);
+    const unsigned pre = __ballot_sync(0xffffffffu, flag == kFlagPre);
+    const unsigned notready = __ballot_sync(0xffffffffu, flag == 0ull);
+    const int first_pre = pre ? (__ffs(pre) - 1) : 32;
+    const unsigned need = (first_pre >= 31) ? 0xffffffffu : ((2u << first_pre) - 1u);
+    if (notready & need) {
+      if (clock64() - t0 > wait_cycles) {
+        if (lane == 0) atomicOr(err, kErrLookbackTimeout);
+        break;
+      }
+      __nanosleep(20);
+      continue;
+    }
+    int v = ((need >> lane) & 1u) ? (int)(unsigned)wv : 0;
+#pragma unroll
+    for (int d = 16; d >= 1; d >>= 1) v += __shfl_xor_sync(0xffffffffu, v, d);
+    excl += v;
+    if (first_pre < 32) break;
+    j -= 32;
+  }
+  return excl;
+}
+
+// Neighbour rule of gNmsUnroll4 (orbd.cu:938-956) for the centre at linear
+// index idx (score v, octave o), checked by a group of kNmsGroup lanes: lane
+// `sub` of the group takes window rows dy = sub - r, sub + kNmsGroup - r, ...;
+// each row is at most two occupancy words, and scores are read only where a
+// bit is set.  Returns whether this lane's rows hold a suppressing position.
+// Positions are linear like the reference's (a column past the edge is the
+// adjacent row's entry); positions outside the map, reachable only with an
+// edge threshold below 2^o, are empty.
+constexpr int kNmsGroup = 8;
+constexpr int kNmsChunkWords = 128;  // occupancy words compacted per round: at most 4096 centres
+
+template <bool P>
+__device__ __forceinline__ bool nms_suppressed_rows(const Frame& F, long long idx, float v, int o, int p0,
+                                                    long long npx, int sub) {
+  const int r = 1 << o;
+  for (int dyi = sub; dyi <= 2 * r; dyi += kNmsGroup) {
+    const int dy = dyi - r;
+    const long long rc = idx + (long long)dy * p0;
+    long long lo = rc - r, hi = rc + r;
+    if (hi < 0 || lo >= npx) continue;
+    if (lo < 0) lo = 0;
+    if (hi >= npx) hi = npx - 1;
+    for (long long wi = lo >> 5; wi <= (hi >> 5); wi++) {
+      const long long base = wi << 5;
+      uint32_t m = ldx<P>(F.occ + wi);
+      if (base < lo) m &= ~0u << (int)(lo - base);
+      if (hi - base < 31) m &= (2u << (int)(hi - base)) - 1u;
+      while (m) {
+        const int bb = __ffs(m) - 1;
+        m &= m - 1u;
+        const long long li = base + bb;
+        if (li == idx) continue;
+        const int dx = (int)(li - rc);
+        const float u = ldx<P>(F.vmap + li);
+        if (u > v || (u == v && dx <= 0 && dy <= 0)) return true;
+      }
+    }
+  }
+  return false;
+}
+
+struct NmsSmem {
+  uint32_t sur[kNmsMaxWords];
+  int pref[kNmsMaxWords];
+  uint16_t cand[kNmsChunkWords * 32];
+  float cv[kNmsChunkWords * 32];
+  uint8_t co[kNmsChunkWords * 32];
+  int ncand[2];
+  int warp_tot[8];
+  int base;
+};
+
+// One NMS strip; `ticket` is the strip's index over the batch, and strips must
+// start in ticket order (the look-back waits only on smaller tickets).  P: the
+// score map was written earlier in the same launch.
+template <bool P>
+__device__ __forceinline__ void nms_strip(const Batch& b, int ticket, NmsSmem& sm) {
+  uint32_t* s_sur = sm.sur;
+  int* s_pref = sm.pref;
+  uint16_t* s_cand = sm.cand;
+  float* s_cv = sm.cv;
+  uint8_t* s_co = sm.co;
+  int* s_ncand = sm.ncand;
+  int* s_warp_tot = sm.warp_tot;
+  int& s_base = sm.base;
+  const int f = find_frame(b.nms_base, b.n_frames, ticket);
+  const Frame& F = b.frames[f];
+  const int s = ticket - b.nms_base[f];
+  const int border = F.border;
+  const int row0 = border + s * F.nms_rows;
+  const int row1 = min(row0 + F.nms_rows, F.h - border);
+  const int xlo = border, xhi = F.w - border;  // columns [xlo, xhi)
+  const int wlo = xlo >> 5, whi = (xhi - 1) >> 5;
+  const int nw = whi - wlo + 1;
+  const int nwords = (row1 - row0) * nw;
+  const int p0 = F.op[0];
+  const int wpr = p0 >> 5;  // occupancy words per row
+  const long long npx = (long long)F.h * p0;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+
+  // pass 1: survivor bits of every occupancy word of the strip.  In rounds of
+  // kNmsChunkWords words: the centres of the round (with their scores) are
+  // compacted into shared memory, then checked by 32 groups of 8 lanes, so a
+  // textured patch of the strip spreads over every warp.
+  for (int k = threadIdx.x; k < nwords; k += blockDim.x) s_sur[k] = 0u;
+  if (threadIdx.x == 0) s_ncand[0] = 0;
+  const int gid = warp * (32 / kNmsGroup) + (lane / kNmsGroup), sub = lane % kNmsGroup;
+  const uint32_t gmask = ((1u << kNmsGroup) - 1u) << (lane & ~(kNmsGroup - 1));
+  for (int c0 = 0, round = 0; c0 < nwords; c0 += kNmsChunkWords, round++) {
+    int* cnt = &s_ncand[round & 1];
+    __syncthreads();  // the previous round's checks are done; its counter is free
+    if (threadIdx.x == 0) s_ncand[(round + 1) & 1] = 0;
+    const int k = c0 + (int)threadIdx.x;
+    if (threadIdx.x < kNmsChunkWords && k < nwords) {
+      const int row = row0 + k / nw;
+      const int wj = wlo + k % nw;
+      const int cbase = wj << 5;
+      uint32_t m = ldx<P>(F.occ + (long long)row * wpr + wj);
+      if (cbase < xlo) m &= ~0u << (xlo - cbase);
+      if (xhi - cbase < 32) m &= (xhi - cbase <= 0) ? 0u : ((xhi - cbase == 32) ? ~0u : ((1u << (xhi - cbase)) - 1u));
+      if (m) {
+        int pos = atomicAdd(cnt, __popc(m));
+        while (m) {
+          const int bit = __ffs(m) - 1;
+          m &= m - 1u;
+          const long long idx = (long long)row * p0 + cbase + bit;
+          s_cand[pos] = (uint16_t)(((k - c0) << 5) | bit);
+          s_cv[pos] = ldx<P>(F.vmap + idx);
+          s_co[pos] = ldx<P>(F.oct8 + idx);
+          pos++;
+        }
+      }
+    }
+    __syncthreads();
+    const int nc = *cnt;
+    for (int j0 = 0; j0 < nc; j0 += 32 * 8 / kNmsGroup) {
+      const int j = j0 + gid;
+      bool sup = false;
+      int kk = 0, bit = 0;
+      if (j < nc) {
+        const int e = s_cand[j];
+        kk = c0 + (e >> 5);
+        bit = e & 31;
+        const int row = row0 + kk / nw;
+        const int cbase = (wlo + kk % nw) << 5;
+        sup = nms_suppressed_rows<P>(F, (long long)row * p0 + cbase + bit, s_cv[j], s_co[j], p0, npx, sub);
+      }
+      const uint32_t bal = __ballot_sync(0xffffffffu, sup);
+      if (j < nc && sub == 0 && !(bal & gmask)) atomicOr(&s_sur[kk], 1u << bit);
+    }
+  }
+  __syncthreads();
+
+  // exclusive scan of the survivor counts, in word order
+  const int per = (nwords + 255) >> 8;
+  const int beg = min((int)threadIdx.x * per, nwords), end = min(beg + per, nwords);
+  int local = 0;
+  for (int i = beg; i < end; i++) local += __popc(s_sur[i]);
+  int incl = local;
+#pragma unroll
+  for (int d = 1; d < 32; d <<= 1) {
+    const int n = __shfl_up_sync(0xffffffffu, incl, d);
+    if (lane >= d) incl += n;
+  }
+  if (lane == 31) s_warp_tot[warp] = incl;
+  __syncthreads();
+  int warp_off = 0;
+  for (int w2 = 0; w2 < warp; w2++) warp_off += s_warp_tot[w2];
+  int run = warp_off + incl - local;
+  for (int i = beg; i < end; i++) {
+    s_pref[i] = run;
+    run += __popc(s_sur[i]);
+  }
+  int strip_total = 0;
+  for (int w2 = 0; w2 < 8; w2++) strip_total += s_warp_tot[w2];
+
+  // decoupled look-back over the frame's strips (warp 0)
+  if (warp == 0) {
+    unsigned long long* st = F.nms_status;
+    int excl = 0;
+    if (s == 0) {
+      if (lane == 0) st_release_u64(&st[0], kFlagPre | (unsigned)strip_total);
+    } else {
+      if (lane == 0) st_release_u64(&st[s], kFlagAgg | (unsigned)strip_total);
+      __syncwarp();
+      excl = nms_lookback(st, s, lane, b.err, b.wait_cycles);
+      if (lane == 0) st_release_u64(&st[s], kFlagPre | (unsigned)(excl + strip_total));
+    }
+    if (lane == 0) {
+      s_base = excl;
+      if (s == F.nms_strips - 1) {
+        const int tot = excl + strip_total;
+        *F.count = min(tot, F.max_pts);
+        if (F.total) *F.total = tot;
+      }
+    }
+  }
+  __syncthreads();
+  const int base = s_base;
+  if (base >= F.max_pts) return;
+
+  // pass 2: write the survivors
+  for (int k = threadIdx.x; k < nwords; k += blockDim.x) {
+    uint32_t m = s_sur[k];
+    if (!m) continue;
+    const int row = row0 + k / nw;
+    const int cbase = (wlo + k % nw) << 5;
+    int rank = base + s_pref[k];
+    while (m) {
+      const int bit = __ffs(m) - 1;
+      m &= m - 1u;
+      if (rank >= F.max_pts) break;
+      const long long idx = (long long)row * p0 + cbase + bit;
+      orbx_point q;
+      q.x = cbase + bit;
+      q.y = row;
+      q.octave = F.oct8[idx];
+      q.score = F.vmap[idx];
+      q.angle = 0.f;
+      q.match = 0;
+      q.distance = 0;
+      F.pts[rank] = q;
+      rank++;
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Orientation and rBRIEF (orbx_describe.cu and the persistent kernel)
+// ---------------------------------------------------------------------------
+// Plain loads of data written earlier in the same launch (PL) or by earlier
+// launches; PL uses the coherent cached path explicitly.
+template <bool PL, class T>
+__device__ __forceinline__ T ldc(const T* p) {
+  if constexpr (PL)
+    return __ldca(p);
+  else
+    return *p;
+}
+
+constexpr int kDescWarps = 8;
+
+// getValue (orbd.cu:1341-1348): the rotated point is
+// (rint(x*c - y*s), rint(x*s + y*c)), evaluated by the reference build as
+// fma(x, c, -(y*s)) and fma(x, s, y*c).
+template <bool PL>
+__device__ __forceinline__ int sample_at(const uint8_t* center, int pitch, float x, float y, float s, float c) {
+  const int ix = __float2int_rn(__fmaf_rn(x, c, -__fmul_rn(y, s)));
+  const int iy = __float2int_rn(__fmaf_rn(x, s, __fmul_rn(y, c)));
+  return ldc<PL>(center + (ptrdiff_t)iy * pitch + ix);
+}
+
+template <int WTA, bool PL>
+__device__ __forceinline__ uint8_t describe_byte(const uint8_t* center, int pitch, const float* px, const float* py,
+                                                 float s, float c) {
+#define G(j) sample_at<PL>(center, pitch, px[j], py[j], s, c)
+  uint8_t val = 0;
+  if (WTA == 2) {  // feature2 (orbd.cu:1351-1361)
+#pragma unroll
+    for (int j = 0; j < 8; j++) val |= (uint8_t)((G(2 * j) < G(2 * j + 1)) << j);
+  } else if (WTA == 3) {  // feature3 (orbd.cu:1364-1388), including its index reuse of 8 and skip of 10
+    const int idx[4][3] = {{0, 1, 2}, {3, 4, 5}, {6, 7, 8}, {8, 9, 11}};
+#pragma unroll
+    for (int g = 0; g < 4; g++) {
+      const int t0 = G(idx[g][0]), t1 = G(idx[g][1]), t2 = G(idx[g][2]);
+      const int v = t2 > t1 ? (t2 > t0 ? 2 : 0) : (t1 > t0);
+      val |= (uint8_t)(v << (2 * g));
+    }
+  } else {  // feature4 (orbd.cu:1391-1434)
+#pragma unroll
+    for (int g = 0; g < 4; g++) {
+      int t0 = G(4 * g), t1 = G(4 * g + 1), t2 = G(4 * g + 2), t3 = G(4 * g + 3);
+      int u = 0, v = 2;
+      if (t1 > t0) t0 = t1, u = 1;
+      if (t3 > t2) t2 = t3, v = 3;
+      val |= (uint8_t)((t0 > t2 ? u : v) << (2 * g));
+    }
+  }
+#undef G
+  return val;
+}
+
+// This lane's pattern points of descriptor byte `lane` (setPattern, orbd.cu:95-410).
+template <int WTA>
+__device__ __forceinline__ void load_pattern(const Batch& b, int lane, float* px, float* py) {
+  constexpr int PSTEP = (WTA == 3) ? 12 : 16;
+#pragma unroll
+  for (int j = 0; j < PSTEP; j++) {
+    px[j] = (float)b.pattern[2 * (PSTEP * lane + j)];
+    py[j] = (float)b.pattern[2 * (PSTEP * lane + j) + 1];
+  }
+}
+
+// angleIC + gDescrible for keypoint k of frame F, by one warp.
+template <int WTA, bool PL>
+__device__ __forceinline__ void describe_keypoint(const Batch& b, const Frame& F, int k, const float* px,
+                                                  const float* py, const int* s_umax, int lane) {
+  const int half_k = b.half_k;
+  const int u = lane - 15;
+  orbx_point* P = F.pts + k;
+  const int x = ldc<PL>(&P->x), y = ldc<PL>(&P->y), o = ldc<PL>(&P->octave);
+  const int pitch = F.op[o];
+  const long long coff = F.ooff[o] + (long long)(y >> o) * pitch + (x >> o);
+
+  float angle;
+  if (b.describe_mode != kDescribeDescOnly) {
+    // intensity centroid on the raw octave
+    const uint8_t* center = F.pyr + coff;
+    int m10 = 0, m01 = 0;
+    for (int v = -half_k; v <= half_k; v++) {
+      const int um = s_umax[v < 0 ? -v : v];
+      if (lane < 31 && u >= -um && u <= um) {
+        const int val = ldc<PL>(center + (ptrdiff_t)v * pitch + u);
+        m10 += u * val;
+        m01 += v * val;
+      }
+    }
+#pragma unroll
+    for (int d = 16; d >= 1; d >>= 1) {
+      m10 += __shfl_xor_sync(0xffffffffu, m10, d);
+      m01 += __shfl_xor_sync(0xffffffffu, m01, d);
+    }
+    angle = fast_atan2(__int2float_rn(m01), __int2float_rn(m10));
+    if (lane == 0) P->angle = angle;
+    if (b.describe_mode == kDescribeAngleOnly) return;
+  } else {
+    angle = ldc<PL>(&P->angle);
+  }
+
+  // rBRIEF on the blurred octave
+  const float sn = __sinf(angle);
+  const float cs = __cosf(angle);
+  const uint8_t byte = describe_byte<WTA, PL>(F.blr + coff, pitch, px, py, sn, cs);
+  F.desc[(size_t)k * 32 + lane] = byte;
+}
+
+// ---------------------------------------------------------------------------
+// k = 2 XOR-popcount matching (orbx_match.cu and the persistent kernel)
+// ---------------------------------------------------------------------------
+constexpr int kMQ = 128;      // queries per block
+constexpr int kMChunk = 512;  // train rows per shared-memory chunk (16 KB)
+constexpr int kIdxBits = kIdxBitsShared;
+constexpr uint32_t kNoKey = kNoKeyShared;
+
+__device__ __forceinline__ void top2_push(uint32_t& k1, uint32_t& k2, uint32_t key) { top2_push_shared(k1, k2, key); }
+__device__ __forceinline__ void finish_query(const MatchArgs& a, int q, uint32_t k1, uint32_t k2) {
+  finish_query_shared(a, q, k1, k2);
+}
+
+// One block's share of a k = 2 search with QPB queries per block (QPB =
+// blockDim.x); bid / nblk replace blockIdx.x / gridDim.x so that a batch launch
+// or a work item of the persistent kernel can run one search each.  P: the
+// descriptors and counts were written earlier in the same launch.
+template <int QPB, bool P>
+__device__ __forceinline__ void match_popc_block(const MatchArgs& a, const MatchWork& w, int bid, int nblk,
+                                                 uint4* s_db, unsigned int& s_last) {
+
+  const int nq = min(a.d_nq ? ldx<P>(a.d_nq) : a.nq, w.nq_cap);
+  const int ndb = a.d_ndb ? ldx<P>(a.d_ndb) : a.ndb;
+  // Spread (query tile, train split) pairs over the launched blocks using the
+  // actual counts, which may be far below the capacities the grid was sized for.
+  const int tiles = (nq + QPB - 1) / QPB;
+  if (tiles == 0) return;
+  int splits = nblk / tiles;
+  splits = min(splits, w.splits_cap);
+  splits = min(splits, max(1, (ndb + 63) / 64));
+  splits = max(splits, 1);
+  const int tile = bid / splits;
+  const int split = bid - tile * splits;
+  if (tile >= tiles) return;
+  const int q = tile * QPB + threadIdx.x;
+  const bool active = q < nq;
+
+  uint32_t qw[8];
+  {
+    const uint4* qp = reinterpret_cast<const uint4*>(a.q) + 2 * (size_t)(active ? q : 0);
+    const uint4 v0 = ldx<P>(qp), v1 = ldx<P>(qp + 1);
+    qw[0] = v0.x; qw[1] = v0.y; qw[2] = v0.z; qw[3] = v0.w;
+    qw[4] = v1.x; qw[5] = v1.y; qw[6] = v1.z; qw[7] = v1.w;
+  }
+
+  const int r_beg = (int)((long long)ndb * split / splits);
+  const int r_end = (int)((long long)ndb * (split + 1) / splits);
+  uint32_t k1 = kNoKey, k2 = kNoKey;
+  const uint4* db4 = reinterpret_cast<const uint4*>(a.db);
+  for (int r0 = r_beg; r0 < r_end; r0 += kMChunk) {
+    const int rows = min(kMChunk, r_end - r0);
+    __syncthreads();
+    for (int i = threadIdx.x; i < rows * 2; i += QPB) s_db[i] = ldx<P>(db4 + 2 * (size_t)r0 + i);
+    __syncthreads();
+    for (int j = 0; j < rows; j++) {
+      const uint4 t0 = s_db[2 * j], t1 = s_db[2 * j + 1];
+      const uint32_t d = __popc(qw[0] ^ t0.x) + __popc(qw[1] ^ t0.y) + __popc(qw[2] ^ t0.z) +
+                         __popc(qw[3] ^ t0.w) + __popc(qw[4] ^ t1.x) + __popc(qw[5] ^ t1.y) +
+                         __popc(qw[6] ^ t1.z) + __popc(qw[7] ^ t1.w);
+      top2_push(k1, k2, (d << kIdxBits) | (uint32_t)(r0 + j));
+    }
+  }
+
+  if (splits == 1) {
+    if (active) finish_query(a, q, k1, k2);
+    return;
+  }
+  // publish this split's partial top-2; the last split to finish the tile merges
+  if (active) {
+    uint2* part = reinterpret_cast<uint2*>(w.part);
+    part[(size_t)split * w.nq_cap + q] = make_uint2(k1, k2);
+  }
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) s_last = (atomicAdd(&w.tile_done[tile], 1u) == (unsigned)(splits - 1)) ? 1u : 0u;
+  __syncthreads();
+  if (!s_last) return;
+  __threadfence();
+  if (threadIdx.x == 0) w.tile_done[tile] = 0u;  // ready for the next launch
+  if (!active) return;
+  const uint2* part = reinterpret_cast<const uint2*>(w.part);
+  uint32_t m1 = kNoKey, m2 = kNoKey;
+  for (int sp = 0; sp < splits; sp++) {
+    const uint2 pk = __ldcg(part + (size_t)sp * w.nq_cap + q);
+    top2_push(m1, m2, pk.x);
+    top2_push(m1, m2, pk.y);
+  }
+  finish_query(a, q, m1, m2);
+}
+
+}  // namespace orbx

@@ -51,7 +51,9 @@ class FrameOut(ctypes.Structure):
 
 class Tuning(ctypes.Structure):
     _fields_ = [("nms_rows", ctypes.c_int), ("describe_blocks_per_sm", ctypes.c_int),
-                ("match_blocks_per_sm", ctypes.c_int), ("match_blocks_per_pair", ctypes.c_int)]
+                ("match_blocks_per_sm", ctypes.c_int), ("match_blocks_per_pair", ctypes.c_int),
+                ("batch_form", ctypes.c_int), ("persist_group", ctypes.c_int),
+                ("persist_blocks_per_sm", ctypes.c_int), ("wait_timeout_us", ctypes.c_int)]
 
     def as_dict(self):
         return {f: int(getattr(self, f)) for f, _ in self._fields_}
@@ -94,6 +96,10 @@ def lib():
         L.orbx_autotune_pairs.argtypes = [vp, i32, ctypes.POINTER(Image), ctypes.POINTER(Image),
                                           ctypes.POINTER(FrameOut), ctypes.POINTER(FrameOut), i32,
                                           ctypes.POINTER(Tuning), ctypes.POINTER(ctypes.c_float)]
+        L.orbx_autotune_pairs_forms.argtypes = [vp, i32, ctypes.POINTER(Image), ctypes.POINTER(Image),
+                                                ctypes.POINTER(FrameOut), ctypes.POINTER(FrameOut), i32, i32,
+                                                ctypes.POINTER(Tuning), ctypes.POINTER(ctypes.c_float)]
+        L.orbx_selftest_wait_timeout.argtypes = [vp, i32]
         L.orbx_profile_batch.argtypes = [vp, i32, ctypes.POINTER(Image), ctypes.POINTER(Image),
                                          ctypes.POINTER(FrameOut), ctypes.POINTER(FrameOut), vp]
         L.orbx_learned_default_params.argtypes = [ctypes.POINTER(LearnedParams)]
@@ -350,6 +356,18 @@ class Context:
         _check(lib().orbx_autotune_pairs(self.h, batch.n, batch.ia, batch.ib, batch.oa, batch.ob, reps,
                                          ctypes.byref(t), ctypes.byref(ms)), "orbx_autotune_pairs")
         return t, ms.value
+
+    def autotune_pairs_forms(self, batch, forms, reps=3):
+        """forms: 1 = five launches, 2 = persistent, 3 = both."""
+        t = Tuning()
+        ms = ctypes.c_float(0)
+        _check(lib().orbx_autotune_pairs_forms(self.h, batch.n, batch.ia, batch.ib, batch.oa, batch.ob, reps, forms,
+                                               ctypes.byref(t), ctypes.byref(ms)), "orbx_autotune_pairs_forms")
+        return t, ms.value
+
+    def selftest_wait_timeout(self, timeout_us):
+        """Returns the status of a device wait on a counter nothing sets (ORBX_ERR_TIMEOUT expected)."""
+        return int(lib().orbx_selftest_wait_timeout(self.h, int(timeout_us)))
 
     def debug_buffers(self, w, h):
         n, oszp = layout(w, h, self.params.noctaves)

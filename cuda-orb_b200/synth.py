@@ -201,3 +201,16 @@ def match_workload(n_db, n_q, seed=0, flip_p=0.05):
     flips = (rng.uniform(size=bits.shape) < flip_p).astype(np.uint8)
     q[:half] = np.packbits(bits ^ flips, axis=1)
     return db, q, src
+
+
+# Resolutions of the batched workload (64 pairs of mixed size and keypoint cap).
+BATCH_SIZES = [(320, 240), (640, 480), (1280, 720), (1920, 1080), (3840, 2160)]
+
+
+def batch_layout(n_pairs=64, seed=0x0C3000):
+    """(w, h, cap) per pair: resolutions uniform over BATCH_SIZES and keypoint
+    caps uniform in [500, 10000]."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    sizes = [BATCH_SIZES[int(i)] for i in rng.integers(0, len(BATCH_SIZES), n_pairs)]
+    caps = [int(c) for c in rng.integers(500, 10001, n_pairs)]
+    return [(w, h, c) for (w, h), c in zip(sizes, caps)]

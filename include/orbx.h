@@ -217,21 +217,35 @@ typedef struct orbx_frame_out {
   int max_pts;
 } orbx_frame_out;
 
-/* Launch shapes the autotuner chooses among. */
+/* Launch shapes the autotuner chooses among, and the bound of device-side waits. */
 typedef struct orbx_tuning {
   int nms_rows;              /* level-0 rows per NMS strip, 1..16 */
   int describe_blocks_per_sm; /* grid of the orientation + descriptor kernel */
   int match_blocks_per_sm;    /* grid of the popcount matcher (single pairs) */
   int match_blocks_per_pair;  /* grid per pair of the batched matcher, 0 = automatic */
+  int batch_form;             /* orbx_batch_pairs: 0 = five graph-replayed launches, 1 = one persistent launch */
+  int persist_group;          /* persistent form: frames per wave of the work order (even), 0 = all frames */
+  int persist_blocks_per_sm;  /* persistent form: resident blocks per SM, 0 = the occupancy limit */
+  int wait_timeout_us;        /* bound of every device-side wait, 1 .. 10,000,000 us (default 1,000,000) */
 } orbx_tuning;
 
 ORBX_API int orbx_get_tuning(orbx_ctx* ctx, orbx_tuning* t);
 ORBX_API int orbx_set_tuning(orbx_ctx* ctx, const orbx_tuning* t);
 
+/* No counterpart in the reference (its CUDA errors exit the process,
+ * cuda_utils.h:18-38).  Runs the device-side bounded wait of the persistent
+ * batch kernel on a counter that nothing increments, bounded by timeout_us:
+ * the wait gives up, the call returns ORBX_ERR_TIMEOUT through the context's
+ * error word (as any call that timed out does at orbx_sync), and the context
+ * stays usable.  For tests of the failure path. */
+ORBX_API int orbx_selftest_wait_timeout(orbx_ctx* ctx, int timeout_us);
+
 /* Many frame pairs of any sizes and keypoint caps: every stage of every image
  * runs in shared launches (one per stage for the whole batch), then every pair
- * is matched A -> B in one launch; replayed from a CUDA graph cached per
- * (shapes, pointers, tuning).  Per pair the results are identical to
+ * is matched A -> B in one launch; or, with tuning batch_form = 1, all of it
+ * runs in one persistent launch whose blocks claim (stage, frame, tile) work
+ * items from a device queue, waiting per frame on the stage before.  Replayed
+ * from a CUDA graph cached per (shapes, pointers, tuning).  Per pair the results are identical to
  * orbx_pair on that pair with the same cap.  This batches what the reference
  * does one Orbor::detectAndCompute / Orbor::match call at a time
  * (orb.cpp:57-113).  Asynchronous. */
@@ -244,6 +258,13 @@ ORBX_API int orbx_batch_pairs(orbx_ctx* ctx, int n_pairs, const orbx_image* imgs
 ORBX_API int orbx_autotune_pairs(orbx_ctx* ctx, int n_pairs, const orbx_image* imgs_a, const orbx_image* imgs_b,
                                  const orbx_frame_out* out_a, const orbx_frame_out* out_b, int reps,
                                  orbx_tuning* best, float* best_ms);
+
+/* orbx_autotune_pairs over the batch forms in `forms`: bit 0 the five-launch
+ * form, bit 1 the persistent form (3 = both, as orbx_autotune_pairs). */
+ORBX_API int orbx_autotune_pairs_forms(orbx_ctx* ctx, int n_pairs, const orbx_image* imgs_a,
+                                       const orbx_image* imgs_b, const orbx_frame_out* out_a,
+                                       const orbx_frame_out* out_b, int reps, int forms, orbx_tuning* best,
+                                       float* best_ms);
 
 /* Profiling variant of orbx_batch_pairs: the same launches without the graph,
  * with a CUDA event between consecutive kernels; stage_ms[0..4] as for
