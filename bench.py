@@ -439,21 +439,43 @@ def run_orbx(args, world, rank, local):
     hna = np.zeros(1, dtype=np.int32)
     hnb = np.zeros(1, dtype=np.int32)
     e2e_steps = min(args.steps, 300)
-    with torch.cuda.stream(stream):
-        for _ in range(3):
-            ctx.pair_host(ha.data_ptr(), hb.data_ptr(), W, H, pitch, hpa, hna, hpb, hnb)
-        e_ms = []
-        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        barrier(world)
-        for _ in range(e2e_steps):
-            flush.zero_()
-            ev0.record(stream)
-            ctx.pair_host(ha.data_ptr(), hb.data_ptr(), W, H, pitch, hpa, hna, hpb, hnb)
-            ev1.record(stream)
-            ev1.synchronize()
-            e_ms.append(ev0.elapsed_time(ev1))
-        barrier(world)
+
+    def e2e_run(bands, steps):
+        """CUDA-event and host wall times of orbx_pair_host with the given upload banding."""
+        t = ctx.get_tuning()
+        keep = t.upload_bands
+        if bands is not None:
+            t.upload_bands = bands
+            ctx.set_tuning(t)
+        with torch.cuda.stream(stream):
+            for _ in range(3):
+                ctx.pair_host(ha.data_ptr(), hb.data_ptr(), W, H, pitch, hpa, hna, hpb, hnb)
+            ev_ms, wall_ms = [], []
+            ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            barrier(world)
+            for _ in range(steps):
+                flush.zero_()
+                stream.synchronize()
+                t0 = time.perf_counter()
+                ev0.record(stream)
+                ctx.pair_host(ha.data_ptr(), hb.data_ptr(), W, H, pitch, hpa, hna, hpb, hnb)
+                ev1.record(stream)
+                wall_ms.append(1000.0 * (time.perf_counter() - t0))
+                ev1.synchronize()
+                ev_ms.append(ev0.elapsed_time(ev1))
+            barrier(world)
+        if bands is not None:
+            t.upload_bands = keep
+            ctx.set_tuning(t)
+        return ev_ms, wall_ms
+
+    ctx_tuning_bands = int(ctx.get_tuning().upload_bands)
+    e_ms, e_wall = e2e_run(None, e2e_steps)
     e2e_total = max_over_ranks(sum(e_ms), world)
+    e2e_variants = {}
+    for bands in (0, 2, 4, 8):
+        v_ev, v_wall = e2e_run(bands, min(e2e_steps, 50))
+        e2e_variants[str(bands)] = {"ms": statistics.median(v_ev), "host_wall_ms": statistics.median(v_wall)}
     h2d = 2 * H * pitch
     d2h = 8 + (int(hna[0]) + int(hnb[0])) * 28
 
@@ -511,8 +533,10 @@ def run_orbx(args, world, rank, local):
             "impl_detail": {"matcher": "XOR-popc", "graph": "one CUDA graph per pair (5 kernels)",
                             "matches": matched},
             "e2e": {"value": e2e_total / (e2e_steps * world), "unit": "ms", "h2d_bytes_per_step": h2d,
-                    "d2h_bytes_per_step": d2h,
-                    "how": "orbx_pair_host: pinned host images in, host keypoints/matches out, CUDA events"},
+                    "d2h_bytes_per_step": d2h, "host_wall_ms_median": statistics.median(e_wall),
+                    "upload_bands": ctx_tuning_bands,
+                    "how": "orbx_pair_host: pinned host images in, host keypoints/matches out, CUDA events",
+                    "by_upload_bands": e2e_variants},
             "gpu_launches": 5 * args.steps,
             "roofline": roofline,
             "kernels": kernels,

@@ -1,5 +1,7 @@
 // C ABI of the sm_100a ORB library: contexts, constant tables, workspaces,
 // batch descriptors and the per-call launch sequences.
+#include <cuda.h>
+#include <mutex>
 #include <cuda_runtime.h>
 
 #include <cmath>
@@ -49,6 +51,27 @@ struct PairGraph {
   cudaGraphExec_t exec = nullptr;
   MatchWork mw{};
 };
+
+// Device tables of one persistent launch (orbx_persist.cu), reused while
+// their content is unchanged.
+struct PersistBufs {
+  PersistRun* runs = nullptr;
+  int* run_base = nullptr;   // [runs + 1]
+  int* desc_base = nullptr;  // [frames + 1]
+  int* done = nullptr;       // [4 * frames + 1 + frames]: stage counters, item counter, upload flags
+  MatchJob* jobs = nullptr;
+  size_t runs_cap = 0, frames_cap = 0, jobs_cap = 0;
+  std::vector<uint8_t> last;  // content of the last upload
+};
+
+static void persist_free(PersistBufs& pb) {
+  cudaFree(pb.runs);
+  cudaFree(pb.run_base);
+  cudaFree(pb.desc_base);
+  cudaFree(pb.done);
+  cudaFree(pb.jobs);
+  pb = PersistBufs();
+}
 
 struct DeviceGuard {
   int prev = -1;
@@ -116,11 +139,13 @@ struct orbx_ctx {
   int batch_form = 0;
   int persist_group = 0;
   int persist_bps = 0;
-  PersistRun* d_runs = nullptr;
-  int* d_run_base = nullptr;  // [runs + 1]
-  int* d_desc_base = nullptr;  // [frames + 1]
-  int* d_done = nullptr;       // [4 * frames + 1]: stage counters, then the item counter
-  size_t runs_cap = 0, frames_cap = 0;
+  PersistBufs pbatch;  // orbx_batch_pairs, persistent form
+  PersistBufs ppair;   // orbx_pair_host with overlapped uploads
+  PairGraph pho;       // its graph: persistent launch + export
+  cudaStream_t copy_stream = nullptr;
+  cudaEvent_t ev_reset = nullptr;
+  int upload_bands = 0;  // orbx_pair_host: 0 = copy then run; 1..16 = bands overlapped with the persistent launch
+  int memops = -1;       // stream write-value support: -1 unknown, 0 no, 1 yes
   // device-side waits
   int wait_us = 1000000;
   long long wait_cycles = 0;
@@ -683,10 +708,13 @@ ORBX_API int orbx_destroy(orbx_ctx* c) {
   cudaFree(c->batch_part);
   cudaFree(c->batch_tile_done);
   if (c->batch_exec) cudaGraphExecDestroy(c->batch_exec);
-  cudaFree(c->d_runs);
-  cudaFree(c->d_run_base);
-  cudaFree(c->d_desc_base);
-  cudaFree(c->d_done);
+  persist_free(c->pbatch);
+  persist_free(c->ppair);
+  if (c->pho.exec) cudaGraphExecDestroy(c->pho.exec);
+  cudaFree(c->pho.mw.part);
+  cudaFree(c->pho.mw.tile_done);
+  if (c->copy_stream) cudaStreamDestroy(c->copy_stream);
+  if (c->ev_reset) cudaEventDestroy(c->ev_reset);
   cudaFree(c->d_pattern);
   cudaFree(c->d_umax);
   cudaFree(c->d_err);
@@ -952,6 +980,140 @@ ORBX_API int orbx_pair(orbx_ctx* c, const uint8_t* d_img_a, const uint8_t* d_img
   return ORBX_OK;
 }
 
+static int persist_prepare(orbx_ctx* c, PersistBufs& pb, const LaunchPlan& pl, const std::vector<Frame>& frames,
+                           const std::vector<MatchJob>& jobs, int blocks_per_pair, int group, PersistArgs* out,
+                           int* grid_out);
+
+// cuStreamWriteValue32 through the runtime's driver entry point (no link-time
+// dependency on the driver library): a copy stream publishes each uploaded band.
+typedef CUresult (*WriteValue32Fn)(CUstream, CUdeviceptr, cuuint32_t, unsigned int);
+static WriteValue32Fn write_value32() {
+  static WriteValue32Fn fn = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuStreamWriteValue32", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<WriteValue32Fn>(p);
+    (void)cudaGetLastError();
+  });
+  return fn;
+}
+
+// Whether stream write-value operations work on this context's device: one
+// write to device memory, checked after a synchronisation.
+static bool memops_ok(orbx_ctx* c) {
+  if (c->memops >= 0) return c->memops == 1;
+  c->memops = 0;
+  WriteValue32Fn wv = write_value32();
+  if (!wv) return false;
+  int* d = nullptr;
+  if (cudaMalloc(&d, sizeof(int)) != cudaSuccess) {
+    (void)cudaGetLastError();
+    return false;
+  }
+  int h = 0;
+  if (cudaMemsetAsync(d, 0, sizeof(int), c->stream) == cudaSuccess &&
+      wv((CUstream)c->stream, (CUdeviceptr)d, 7u, 0) == CUDA_SUCCESS &&
+      cudaMemcpyAsync(&h, d, sizeof(int), cudaMemcpyDeviceToHost, c->stream) == cudaSuccess &&
+      cudaStreamSynchronize(c->stream) == cudaSuccess && h == 7)
+    c->memops = 1;
+  (void)cudaGetLastError();
+  cudaFree(d);
+  return c->memops == 1;
+}
+
+// orbx_pair_host with the uploads overlapped: the two images go up in
+// `bands` row bands on a copy stream, each followed by a write of its band
+// count to a device flag, while one persistent launch (orbx_persist.cu) is
+// already running: a pyramid tile starts as soon as the rows it reads have
+// arrived, so frame A is processed while frame B is still being copied.  The
+// export kernel follows in the same graph.  Returns the mapped result block.
+static int pair_host_overlap(orbx_ctx* c, const uint8_t* h_a, const uint8_t* h_b, int w, int h, int pitch,
+                             bool with_desc, const uint8_t** res) {
+  int rc;
+  if ((rc = ws_ensure(c, c->ws[0], w, h)) != 0) return rc;
+  if ((rc = ws_ensure(c, c->ws[1], w, h)) != 0) return rc;
+  if (!c->copy_stream) ORBX_CUDA(cudaStreamCreateWithFlags(&c->copy_stream, cudaStreamNonBlocking));
+  if (!c->ev_reset) ORBX_CUDA(cudaEventCreateWithFlags(&c->ev_reset, cudaEventDisableTiming));
+  std::vector<Frame> frames(2);
+  fill_frame(c, c->ws[0], c->io_img[0], pitch, c->io_pts[0], c->io_desc[0], c->io_count, frames[0]);
+  fill_frame(c, c->ws[1], c->io_img[1], pitch, c->io_pts[1], c->io_desc[1], c->io_count + 1, frames[1]);
+  LaunchPlan pl;
+  if ((rc = upload_batch(c, c->pair, frames, &pl)) != 0) return rc;
+  PairGraph& pg = c->pho;
+  if ((rc = mw_ensure(pg.mw, c->p.max_pts)) != 0) return rc;
+  std::vector<MatchJob> jobs(1);
+  std::memset(jobs.data(), 0, sizeof(MatchJob));
+  jobs[0].args.q = c->io_desc[0];
+  jobs[0].args.db = c->io_desc[1];
+  jobs[0].args.nq = c->p.max_pts;
+  jobs[0].args.ndb = c->p.max_pts;
+  jobs[0].args.d_nq = c->io_count;
+  jobs[0].args.d_ndb = c->io_count + 1;
+  jobs[0].args.pts = c->io_pts[0];
+  jobs[0].work = pg.mw;
+  const int match_items = 2 * 148;
+  PersistArgs a;
+  int grid = 0;
+  if ((rc = persist_prepare(c, c->ppair, pl, frames, jobs, match_items, 0, &a, &grid)) != 0) return rc;
+  const int bands = c->upload_bands;
+  const int band_rows = div_up(h, bands);
+  a.upload_flags = a.done + 4 * 2 + 1;
+  a.band_rows = band_rows;
+  const uint8_t* map_dev = nullptr;
+  if ((rc = hostio_map(c, c->p.max_pts, res, &map_dev)) != 0) return rc;
+  std::vector<uint8_t> key(sizeof(PersistArgs) + 3 * sizeof(int) + sizeof(void*));
+  std::memcpy(key.data(), &a, sizeof(PersistArgs));
+  const int extra[3] = {grid, c->p.max_pts, with_desc ? 1 : 0};
+  std::memcpy(key.data() + sizeof(PersistArgs), extra, sizeof(extra));
+  std::memcpy(key.data() + sizeof(PersistArgs) + sizeof(extra), &map_dev, sizeof(void*));
+  if (!(pg.valid && pg.key == key)) {
+    if (pg.exec) {
+      cudaGraphExecDestroy(pg.exec);
+      pg.exec = nullptr;
+    }
+    pg.valid = false;
+    cudaGraph_t graph = nullptr;
+    ORBX_CUDA(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+    int lrc = launch_batch_persistent(a, grid, c->stream) == cudaSuccess ? ORBX_OK : ORBX_ERR_CUDA;
+    if (lrc == ORBX_OK)
+      lrc = hostio_export_pair(c, c->io_pts[0], c->io_pts[1], c->io_desc[0], c->io_desc[1], c->io_count,
+                               c->p.max_pts, with_desc, res);
+    const cudaError_t ce = cudaStreamEndCapture(c->stream, &graph);
+    if (lrc != ORBX_OK) {
+      if (graph) cudaGraphDestroy(graph);
+      (void)cudaGetLastError();
+      return lrc;
+    }
+    ORBX_CUDA(ce);
+    const cudaError_t ie = cudaGraphInstantiate(&pg.exec, graph, 0);
+    cudaGraphDestroy(graph);
+    ORBX_CUDA(ie);
+    pg.key.swap(key);
+    pg.valid = true;
+  }
+  // reset the counters and flags, start the launch, then feed it the bands
+  ORBX_CUDA(cudaMemsetAsync(a.done, 0, sizeof(int) * (5 * 2 + 1), c->stream));
+  ORBX_CUDA(cudaEventRecord(c->ev_reset, c->stream));
+  ORBX_CUDA(cudaGraphLaunch(pg.exec, c->stream));
+  ORBX_CUDA(cudaStreamWaitEvent(c->copy_stream, c->ev_reset, 0));
+  WriteValue32Fn wv = write_value32();
+  const uint8_t* src[2] = {h_a, h_b};
+  for (int f = 0; f < 2; f++) {
+    for (int k = 0; k < bands; k++) {
+      const int r0 = k * band_rows, r1 = std::min(h, r0 + band_rows);
+      if (r1 > r0)
+        ORBX_CUDA(cudaMemcpyAsync(c->io_img[f] + (size_t)r0 * pitch, src[f] + (size_t)r0 * pitch,
+                                  (size_t)(r1 - r0) * pitch, cudaMemcpyHostToDevice, c->copy_stream));
+      if (wv((CUstream)c->copy_stream, (CUdeviceptr)(a.upload_flags + f), (cuuint32_t)(k + 1), 0) != CUDA_SUCCESS)
+        return ORBX_ERR_CUDA;
+    }
+  }
+  return ORBX_OK;
+}
+
 ORBX_API int orbx_pair_host(orbx_ctx* c, const uint8_t* h_img_a, const uint8_t* h_img_b, int w, int h, int pitch,
                             orbx_point* h_pts_a, int* h_n_a, orbx_point* h_pts_b, int* h_n_b, uint8_t* h_desc_a,
                             uint8_t* h_desc_b, int mode) {
@@ -985,19 +1147,38 @@ ORBX_API int orbx_pair_host(orbx_ctx* c, const uint8_t* h_img_a, const uint8_t* 
     if (!c->io_count_host) ORBX_CUDA(cudaMallocHost(&c->io_count_host, 2 * sizeof(int)));
     c->io_max_pts = c->p.max_pts;
   }
-  ORBX_CUDA(cudaMemcpyAsync(c->io_img[0], h_img_a, ibytes, cudaMemcpyHostToDevice, c->stream));
-  ORBX_CUDA(cudaMemcpyAsync(c->io_img[1], h_img_b, ibytes, cudaMemcpyHostToDevice, c->stream));
-  rc = orbx_pair(c, c->io_img[0], c->io_img[1], w, h, pitch, c->io_pts[0], c->io_desc[0], c->io_count,
-                 c->io_pts[1], c->io_desc[1], c->io_count + 1, mode);
-  if (rc) return rc;
-  // one export kernel writes counts, keypoints (and descriptors) into mapped
-  // pinned memory, so the host waits once and copies only what was found
   const uint8_t* res = nullptr;
   const bool with_desc = h_desc_a || h_desc_b;
-  if ((rc = hostio_export_pair(c, c->io_pts[0], c->io_pts[1], c->io_desc[0], c->io_desc[1], c->io_count,
-                               c->p.max_pts, with_desc, &res)) != 0)
-    return rc;
-  ORBX_CUDA(cudaStreamSynchronize(c->stream));
+  if (c->upload_bands > 0 && mode != ORBX_MATCH_IMMA && memops_ok(c)) {
+    rc = pair_host_overlap(c, h_img_a, h_img_b, w, h, pitch, with_desc, &res);
+    if (rc) {
+      cudaStreamSynchronize(c->copy_stream);
+      cudaStreamSynchronize(c->stream);
+      return rc;
+    }
+    ORBX_CUDA(cudaStreamSynchronize(c->stream));
+    ORBX_CUDA(cudaStreamSynchronize(c->copy_stream));
+  } else {
+    ORBX_CUDA(cudaMemcpyAsync(c->io_img[0], h_img_a, ibytes, cudaMemcpyHostToDevice, c->stream));
+    ORBX_CUDA(cudaMemcpyAsync(c->io_img[1], h_img_b, ibytes, cudaMemcpyHostToDevice, c->stream));
+    rc = orbx_pair(c, c->io_img[0], c->io_img[1], w, h, pitch, c->io_pts[0], c->io_desc[0], c->io_count,
+                   c->io_pts[1], c->io_desc[1], c->io_count + 1, mode);
+    if (rc) return rc;
+    // one export kernel writes counts, keypoints (and descriptors) into mapped
+    // pinned memory, so the host waits once and copies only what was found
+    if ((rc = hostio_export_pair(c, c->io_pts[0], c->io_pts[1], c->io_desc[0], c->io_desc[1], c->io_count,
+                                 c->p.max_pts, with_desc, &res)) != 0)
+      return rc;
+    ORBX_CUDA(cudaStreamSynchronize(c->stream));
+  }
+  {
+    int err = 0;
+    ORBX_CUDA(cudaMemcpy(&err, c->d_err, sizeof(int), cudaMemcpyDeviceToHost));
+    if (err) {
+      ORBX_CUDA(cudaMemset(c->d_err, 0, sizeof(int)));
+      return ORBX_ERR_TIMEOUT;
+    }
+  }
   const int na = reinterpret_cast<const int*>(res)[0], nb = reinterpret_cast<const int*>(res)[1];
   *h_n_a = na;
   *h_n_b = nb;
@@ -1064,6 +1245,7 @@ ORBX_API int orbx_get_tuning(orbx_ctx* c, orbx_tuning* t) {
   t->persist_group = c->persist_group;
   t->persist_blocks_per_sm = c->persist_bps;
   t->wait_timeout_us = c->wait_us;
+  t->upload_bands = c->upload_bands;
   return ORBX_OK;
 }
 
@@ -1073,7 +1255,8 @@ ORBX_API int orbx_set_tuning(orbx_ctx* c, const orbx_tuning* t) {
       t->describe_blocks_per_sm > 64 || t->match_blocks_per_sm < 1 || t->match_blocks_per_sm > 64 ||
       t->match_blocks_per_pair < 0 || t->match_blocks_per_pair > 4096 || t->batch_form < 0 || t->batch_form > 1 ||
       t->persist_group < 0 || t->persist_group > kMaxFramesPerLaunch || t->persist_blocks_per_sm < 0 ||
-      t->persist_blocks_per_sm > 32 || t->wait_timeout_us < 1 || t->wait_timeout_us > 10000000)
+      t->persist_blocks_per_sm > 32 || t->wait_timeout_us < 1 || t->wait_timeout_us > 10000000 ||
+      t->upload_bands < 0 || t->upload_bands > 16)
     return ORBX_ERR_ARG;
   c->nms_rows = t->nms_rows;
   c->describe_bps = t->describe_blocks_per_sm;
@@ -1083,6 +1266,7 @@ ORBX_API int orbx_set_tuning(orbx_ctx* c, const orbx_tuning* t) {
   c->persist_group = t->persist_group;
   c->persist_bps = t->persist_blocks_per_sm;
   c->wait_us = t->wait_timeout_us;
+  c->upload_bands = t->upload_bands;
   c->wait_cycles = (long long)c->wait_us * c->clock_khz / 1000;
   if (c->batch_exec) {
     cudaGraphExecDestroy(c->batch_exec);
@@ -1102,11 +1286,13 @@ ORBX_API int orbx_set_tuning(orbx_ctx* c, const orbx_tuning* t) {
 
 static constexpr int kBatchSplitsCap = 16;
 
-// The persistent form of orbx_batch_pairs (orbx_persist.cu): run table,
-// describe slices and counters uploaded when the batch layout changes, then a
-// graph of one counter reset and one persistent launch.
-static int batch_persistent(orbx_ctx* c, const LaunchPlan& pl, const std::vector<Frame>& frames,
-                            const std::vector<MatchJob>& jobs, int blocks_per_pair, std::vector<uint8_t>& key) {
+// Builds the run table of a persistent launch over `frames` (orbx_persist.cu),
+// uploads the tables to `pb` when their content changed, and fills the launch
+// arguments and grid.  Uploads are synchronous (they happen only when a batch
+// layout is new).
+static int persist_prepare(orbx_ctx* c, PersistBufs& pb, const LaunchPlan& pl, const std::vector<Frame>& frames,
+                           const std::vector<MatchJob>& jobs, int blocks_per_pair, int group, PersistArgs* out,
+                           int* grid_out) {
   const int nf = (int)frames.size();
   const int n_pairs = (int)jobs.size();
   std::vector<int> pyr_n(nf), det_n(nf), nms_n(nf), desc_n(nf), desc_base(nf + 1, 0);
@@ -1118,74 +1304,102 @@ static int batch_persistent(orbx_ctx* c, const LaunchPlan& pl, const std::vector
     desc_n[f] = std::max(1, div_up(F.w * F.h, kDescSlicePixels));
     desc_base[f + 1] = desc_base[f] + desc_n[f];
   }
-  const int group = c->persist_group > 0 ? c->persist_group : nf;
   std::vector<PersistRun> runs;
   std::vector<int> run_base;
-  build_persist_runs(nf, group, pyr_n.data(), det_n.data(), nms_n.data(), desc_n.data(), blocks_per_pair, &runs,
-                     &run_base);
+  build_persist_runs(nf, group > 0 ? group : nf, pyr_n.data(), det_n.data(), nms_n.data(), desc_n.data(),
+                     blocks_per_pair, &runs, &run_base);
   const int bps_max = persist_blocks_per_sm(c->p.wta_k);
   if (bps_max <= 0) return ORBX_ERR_CUDA;
   const int bps = c->persist_bps > 0 ? std::min(c->persist_bps, bps_max) : bps_max;
   int nsm = 0;
   ORBX_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, c->device));
-  const int grid = bps * nsm;
+  *grid_out = bps * nsm;
+  std::vector<uint8_t> blob(sizeof(PersistRun) * runs.size() + sizeof(int) * (run_base.size() + nf + 1) +
+                            sizeof(MatchJob) * n_pairs);
   {
-    const int extra[4] = {1, group, grid, (int)runs.size()};
+    uint8_t* q = blob.data();
+    std::memcpy(q, runs.data(), sizeof(PersistRun) * runs.size());
+    q += sizeof(PersistRun) * runs.size();
+    std::memcpy(q, run_base.data(), sizeof(int) * run_base.size());
+    q += sizeof(int) * run_base.size();
+    std::memcpy(q, desc_base.data(), sizeof(int) * (nf + 1));
+    q += sizeof(int) * (nf + 1);
+    std::memcpy(q, jobs.data(), sizeof(MatchJob) * n_pairs);
+  }
+  if (pb.last != blob) {
+    ORBX_CUDA(cudaStreamSynchronize(c->stream));
+    if (pb.runs_cap < runs.size()) {
+      cudaFree(pb.runs);
+      cudaFree(pb.run_base);
+      pb.runs = nullptr;
+      pb.run_base = nullptr;
+      pb.runs_cap = 0;
+      ORBX_CUDA(cudaMalloc(&pb.runs, sizeof(PersistRun) * runs.size()));
+      ORBX_CUDA(cudaMalloc(&pb.run_base, sizeof(int) * (runs.size() + 1)));
+      pb.runs_cap = runs.size();
+    }
+    if (pb.frames_cap < (size_t)nf) {
+      cudaFree(pb.desc_base);
+      cudaFree(pb.done);
+      pb.desc_base = nullptr;
+      pb.done = nullptr;
+      pb.frames_cap = 0;
+      ORBX_CUDA(cudaMalloc(&pb.desc_base, sizeof(int) * (nf + 1)));
+      ORBX_CUDA(cudaMalloc(&pb.done, sizeof(int) * (5 * (size_t)nf + 1)));
+      pb.frames_cap = nf;
+    }
+    if (pb.jobs_cap < (size_t)n_pairs) {
+      cudaFree(pb.jobs);
+      pb.jobs = nullptr;
+      pb.jobs_cap = 0;
+      ORBX_CUDA(cudaMalloc(&pb.jobs, sizeof(MatchJob) * n_pairs));
+      pb.jobs_cap = n_pairs;
+    }
+    ORBX_CUDA(cudaMemcpy(pb.runs, runs.data(), sizeof(PersistRun) * runs.size(), cudaMemcpyHostToDevice));
+    ORBX_CUDA(cudaMemcpy(pb.run_base, run_base.data(), sizeof(int) * run_base.size(), cudaMemcpyHostToDevice));
+    ORBX_CUDA(cudaMemcpy(pb.desc_base, desc_base.data(), sizeof(int) * (nf + 1), cudaMemcpyHostToDevice));
+    ORBX_CUDA(cudaMemcpy(pb.jobs, jobs.data(), sizeof(MatchJob) * n_pairs, cudaMemcpyHostToDevice));
+    pb.last.swap(blob);
+  }
+  PersistArgs& a = *out;
+  a = PersistArgs{};
+  a.b = pl.b;
+  a.runs = pb.runs;
+  a.run_base = pb.run_base;
+  a.n_runs = (int)runs.size();
+  a.run_base_host_total = run_base.back();
+  a.desc_base = pb.desc_base;
+  a.done = pb.done;
+  a.item_counter = reinterpret_cast<unsigned int*>(pb.done + 4 * (size_t)nf);
+  a.jobs = pb.jobs;
+  a.blocks_per_job = blocks_per_pair;
+  return ORBX_OK;
+}
+
+// The persistent form of orbx_batch_pairs: a graph of one counter reset and
+// one persistent launch.
+static int batch_persistent(orbx_ctx* c, const LaunchPlan& pl, const std::vector<Frame>& frames,
+                            const std::vector<MatchJob>& jobs, int blocks_per_pair, std::vector<uint8_t>& key) {
+  const int nf = (int)frames.size();
+  PersistArgs a;
+  int grid = 0;
+  int rc = persist_prepare(c, c->pbatch, pl, frames, jobs, blocks_per_pair, c->persist_group, &a, &grid);
+  if (rc) return rc;
+  {
+    const int extra[4] = {1, c->persist_group, grid, a.n_runs};
     const size_t k0 = key.size();
-    key.resize(k0 + sizeof(extra));
+    key.resize(k0 + sizeof(extra) + sizeof(void*));
     std::memcpy(key.data() + k0, extra, sizeof(extra));
+    std::memcpy(key.data() + k0 + sizeof(extra), &a.done, sizeof(void*));
   }
   if (!(c->batch_exec && c->batch_key == key)) {
     if (c->batch_exec) {
       cudaGraphExecDestroy(c->batch_exec);
       c->batch_exec = nullptr;
     }
-    ORBX_CUDA(cudaStreamSynchronize(c->stream));
-    if (c->jobs_cap < n_pairs) {
-      cudaFree(c->d_jobs);
-      c->d_jobs = nullptr;
-      c->jobs_cap = 0;
-      ORBX_CUDA(cudaMalloc(&c->d_jobs, sizeof(MatchJob) * n_pairs));
-      c->jobs_cap = n_pairs;
-    }
-    if (c->runs_cap < runs.size()) {
-      cudaFree(c->d_runs);
-      cudaFree(c->d_run_base);
-      c->d_runs = nullptr;
-      c->d_run_base = nullptr;
-      c->runs_cap = 0;
-      ORBX_CUDA(cudaMalloc(&c->d_runs, sizeof(PersistRun) * runs.size()));
-      ORBX_CUDA(cudaMalloc(&c->d_run_base, sizeof(int) * (runs.size() + 1)));
-      c->runs_cap = runs.size();
-    }
-    if (c->frames_cap < (size_t)nf) {
-      cudaFree(c->d_desc_base);
-      cudaFree(c->d_done);
-      c->d_desc_base = nullptr;
-      c->d_done = nullptr;
-      c->frames_cap = 0;
-      ORBX_CUDA(cudaMalloc(&c->d_desc_base, sizeof(int) * (nf + 1)));
-      ORBX_CUDA(cudaMalloc(&c->d_done, sizeof(int) * (4 * (size_t)nf + 1)));
-      c->frames_cap = nf;
-    }
-    ORBX_CUDA(cudaMemcpy(c->d_jobs, jobs.data(), sizeof(MatchJob) * n_pairs, cudaMemcpyHostToDevice));
-    ORBX_CUDA(cudaMemcpy(c->d_runs, runs.data(), sizeof(PersistRun) * runs.size(), cudaMemcpyHostToDevice));
-    ORBX_CUDA(cudaMemcpy(c->d_run_base, run_base.data(), sizeof(int) * run_base.size(), cudaMemcpyHostToDevice));
-    ORBX_CUDA(cudaMemcpy(c->d_desc_base, desc_base.data(), sizeof(int) * (nf + 1), cudaMemcpyHostToDevice));
-    PersistArgs a{};
-    a.b = pl.b;
-    a.runs = c->d_runs;
-    a.run_base = c->d_run_base;
-    a.n_runs = (int)runs.size();
-    a.run_base_host_total = run_base.back();
-    a.desc_base = c->d_desc_base;
-    a.done = c->d_done;
-    a.item_counter = reinterpret_cast<unsigned int*>(c->d_done + 4 * (size_t)nf);
-    a.jobs = c->d_jobs;
-    a.blocks_per_job = blocks_per_pair;
     cudaGraph_t graph = nullptr;
     ORBX_CUDA(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
-    cudaError_t le = cudaMemsetAsync(c->d_done, 0, sizeof(int) * (4 * (size_t)nf + 1), c->stream);
+    cudaError_t le = cudaMemsetAsync(a.done, 0, sizeof(int) * (4 * (size_t)nf + 1), c->stream);
     if (le == cudaSuccess) le = launch_batch_persistent(a, grid, c->stream);
     const cudaError_t ce = cudaStreamEndCapture(c->stream, &graph);
     if (le != cudaSuccess) {

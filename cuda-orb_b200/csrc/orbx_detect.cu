@@ -10,7 +10,7 @@ namespace orbx {
 
 __global__ void __launch_bounds__(256) k_pyramid_blur(Batch b) {
   __shared__ PyrSmem sm;
-  pyr_tile(b, blockIdx.x, sm);
+  pyr_tile<false>(b, blockIdx.x, sm);
 }
 
 __global__ void __launch_bounds__(256, 4) k_detect(Batch b) {

@@ -74,8 +74,7 @@ __global__ void k_export_pair(const orbx_point* __restrict__ pa, const orbx_poin
 
 // Queues k_export_pair on the context stream; *host points at the result block,
 // readable once the stream has been synchronised.
-int hostio_export_pair(orbx_ctx* c, const orbx_point* pa, const orbx_point* pb, const uint8_t* da, const uint8_t* db,
-                       const int* d_count, int max_pts, bool with_desc, const uint8_t** host) {
+int hostio_map(orbx_ctx* c, int max_pts, const uint8_t** host, const uint8_t** dev) {
   HostIO*& io = ctx_hostio(c);
   if (!io) io = new HostIO();
   const size_t bytes = 16 + (size_t)max_pts * (2 * sizeof(orbx_point) + 64);
@@ -93,9 +92,19 @@ int hostio_export_pair(orbx_ctx* c, const orbx_point* pa, const orbx_point* pb, 
     }
     io->map_bytes = bytes;
   }
-  k_export_pair<<<2 * 148, 256, 0, ctx_stream(c)>>>(pa, pb, da, db, d_count, max_pts, with_desc ? 1 : 0, io->map_dev);
-  if (cudaGetLastError() != cudaSuccess) return ORBX_ERR_CUDA;
   *host = io->map;
+  if (dev) *dev = io->map_dev;
+  return ORBX_OK;
+}
+
+int hostio_export_pair(orbx_ctx* c, const orbx_point* pa, const orbx_point* pb, const uint8_t* da, const uint8_t* db,
+                       const int* d_count, int max_pts, bool with_desc, const uint8_t** host) {
+  const uint8_t* dev = nullptr;
+  const int rc = hostio_map(c, max_pts, host, &dev);
+  if (rc) return rc;
+  k_export_pair<<<2 * 148, 256, 0, ctx_stream(c)>>>(pa, pb, da, db, d_count, max_pts, with_desc ? 1 : 0,
+                                                     const_cast<uint8_t*>(dev));
+  if (cudaGetLastError() != cudaSuccess) return ORBX_ERR_CUDA;
   return ORBX_OK;
 }
 

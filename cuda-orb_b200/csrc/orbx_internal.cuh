@@ -218,6 +218,8 @@ void ocv_free(OcvWork* w);
 void umax_table(int patch_size, int* umax);  // setUmax (orbd.cu:66-92)
 HostIO*& ctx_hostio(orbx_ctx* c);
 void hostio_free(HostIO* io);
+// The pinned, mapped result block of orbx_pair_host (allocated or grown here).
+int hostio_map(orbx_ctx* c, int max_pts, const uint8_t** host, const uint8_t** dev);
 int hostio_export_pair(orbx_ctx* c, const orbx_point* pa, const orbx_point* pb, const uint8_t* da, const uint8_t* db,
                        const int* d_count, int max_pts, bool with_desc, const uint8_t** host);
 }  // namespace orbx

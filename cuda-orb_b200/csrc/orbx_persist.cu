@@ -74,6 +74,17 @@ __device__ __forceinline__ void stage_done(int* ctr) {
   }
 }
 
+// Level-0 rows [0, n) that pyramid tile `local` of frame F reads: octave o
+// samples row y << o for the tile's rows and its 3-row reflected halo.
+__device__ __forceinline__ int pyr_tile_rows(const Frame& F, int local) {
+  int o = 0;
+  while (o + 1 < F.n_oct && local >= F.pyr_tile_base[o + 1]) o++;
+  const int lt = local - F.pyr_tile_base[o];
+  const int y0 = (lt / F.pyr_tiles_x[o]) * kPyrTH;
+  const int ylast = min(y0 + kPyrTH - 1 + 3, F.oh[o] - 1);
+  return (ylast << o) + 1;
+}
+
 // Run r covers tickets [run_base[r], run_base[r + 1]).
 __device__ __forceinline__ int find_run(const int* run_base, int n_runs, int t) {
   int lo = 0, hi = n_runs - 1;
@@ -108,7 +119,13 @@ __global__ void __launch_bounds__(kPersistThreads, 3) k_batch_persistent(Persist
     const int nf = b.n_frames;
     switch (run.stage) {
       case kStagePyr:
-        pyr_tile(b, __ldg(b.pyr_base + f) + local, sm.pyr);
+        if (p.upload_flags) {
+          const int rows = pyr_tile_rows(b.frames[f], local);
+          stage_wait(p.upload_flags + f, (rows + p.band_rows - 1) / p.band_rows, b.err, b.wait_cycles);
+          pyr_tile<true>(b, __ldg(b.pyr_base + f) + local, sm.pyr);
+        } else {
+          pyr_tile<false>(b, __ldg(b.pyr_base + f) + local, sm.pyr);
+        }
         stage_done(done + 0 * nf + f);
         break;
       case kStageDet:

@@ -26,6 +26,11 @@ struct PersistArgs {
   unsigned int* item_counter;  // zero at launch
   const MatchJob* jobs;      // one per pair
   int blocks_per_job;        // match items per pair
+  // optional: level-0 images arrive during the launch in bands of band_rows
+  // rows; upload_flags[f] = bands of frame f already copied (written by the
+  // copy stream after each band), and pyramid tiles wait for the rows they read
+  const int* upload_flags;
+  int band_rows;
 };
 
 // Level-0 pixels per describe slice: a frame's keypoints are split into

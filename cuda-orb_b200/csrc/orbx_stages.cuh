@@ -53,8 +53,9 @@ struct PyrSmem {
   __align__(16) float row[kPyrSH * kPyrTW];
 };
 
-// One pyramid tile (tile index t over the batch).  It reads only the caller's
-// images, so it needs no load policy.
+// One pyramid tile (tile index t over the batch).  PL: the level-0 image is
+// copied in during the same launch (coherent loads instead of the read-only path).
+template <bool PL>
 __device__ __forceinline__ void pyr_tile(const Batch& b, int t, PyrSmem& sm) {
   float* s_src = sm.src;
   uint8_t* s_byte = sm.byte;
@@ -100,12 +101,12 @@ __device__ __forceinline__ void pyr_tile(const Batch& b, int t, PyrSmem& sm) {
     if (words0 && cx >= 1 && cx + 3 < ow) {
       // bytes cx-1 .. cx+6 lie in [0, pitch_in): cx + 3 < ow <= pitch_in and both words are aligned
       const uint32_t* wp = reinterpret_cast<const uint32_t*>(rowp + (cx - 1));
-      const uint32_t word = __byte_perm(__ldg(wp), __ldg(wp + 1), 0x4321);
+      const uint32_t word = __byte_perm(ldx<PL>(wp), ldx<PL>(wp + 1), 0x4321);
 #pragma unroll
       for (int j = 0; j < 4; j++) v[j] = (word >> (8 * j)) & 0xFFu;
     } else {
 #pragma unroll
-      for (int j = 0; j < 4; j++) v[j] = __ldg(rowp + (reflect101(cx + j, ow) << sh));
+      for (int j = 0; j < 4; j++) v[j] = ldx<PL>(rowp + (reflect101(cx + j, ow) << sh));
     }
     reinterpret_cast<float4*>(s_src)[it] = make_float4(u8_to_float(v[0]), u8_to_float(v[1]), u8_to_float(v[2]),
                                                        u8_to_float(v[3]));
@@ -174,8 +175,8 @@ __device__ __forceinline__ void pyr_tile(const Batch& b, int t, PyrSmem& sm) {
           B[a + j] = (uint8_t)(bw >> (8 * j));
           P[a + j] = (uint8_t)(pw >> (8 * j));
         } else {
-          const uint8_t v = psrc ? __ldg(psrc + a + j)
-                                 : (copy_pad ? __ldg(img + (size_t)y * pitch_in + x + j) : (uint8_t)0);
+          const uint8_t v = psrc ? ldx<PL>(psrc + a + j)
+                                 : (copy_pad ? ldx<PL>(img + (size_t)y * pitch_in + x + j) : (uint8_t)0);
           B[a + j] = v;
           P[a + j] = v;
         }

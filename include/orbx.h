@@ -227,6 +227,9 @@ typedef struct orbx_tuning {
   int persist_group;          /* persistent form: frames per wave of the work order (even), 0 = all frames */
   int persist_blocks_per_sm;  /* persistent form: resident blocks per SM, 0 = the occupancy limit */
   int wait_timeout_us;        /* bound of every device-side wait, 1 .. 10,000,000 us (default 1,000,000) */
+  int upload_bands;           /* orbx_pair_host: 0 = copy both images, then run the pair; 1..16 = copy them in
+                                 this many row bands per image on a second stream while one persistent launch
+                                 already processes the bands that have arrived (popcount matching) */
 } orbx_tuning;
 
 ORBX_API int orbx_get_tuning(orbx_ctx* ctx, orbx_tuning* t);

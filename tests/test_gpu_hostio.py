@@ -110,3 +110,38 @@ def test_pair_host_equals_device_pair(ctx, with_desc):
         assert np.all(hpa[len(pa):] == -7)
         if with_desc:
             assert np.array_equal(hda[:len(pa)], da) and np.array_equal(hdb[:len(pb)], db)
+
+
+@pytest.mark.parametrize("bands", [1, 4, 7, 16])
+@pytest.mark.parametrize("w,h,seed", [(1920, 1080, 44), (333, 257, 45)])
+def test_pair_host_overlapped_upload_equals_device_pair(w, h, seed, bands):
+    """orbx_pair_host with the images copied in row bands on a second stream,
+    while one persistent launch processes the bands that have arrived: the same
+    results as orbx_pair on device-resident images, on repeated calls."""
+    a, b, _ = synth.make_pair(w, h, seed=seed)
+    pitch = a.shape[1]
+    ref = orbx.Context(0, orbx.make_params(max_pts=10000))
+    A, B = orbx.FrameBuffers(10000), orbx.FrameBuffers(10000)
+    ref.pair_ptr(torch.from_numpy(a).cuda(), torch.from_numpy(b).cuda(), w, h, pitch, A.points, A.desc, A.count,
+                 B.points, B.desc, B.count)
+    ref.sync()
+    pa, da = A.to_host()
+    pb, db = B.to_host()
+    ctx = orbx.Context(0, orbx.make_params(max_pts=10000))
+    t = ctx.get_tuning()
+    t.upload_bands = bands
+    ctx.set_tuning(t)
+    ha, hb = torch.from_numpy(a).pin_memory(), torch.from_numpy(b).pin_memory()
+    for _ in range(3):
+        hpa = np.full((10000, 7), -7, dtype=np.int32)
+        hpb = np.full((10000, 7), -7, dtype=np.int32)
+        hna, hnb = np.zeros(1, np.int32), np.zeros(1, np.int32)
+        hda = np.zeros((10000, 32), np.uint8)
+        hdb = np.zeros((10000, 32), np.uint8)
+        ctx.pair_host(ha.data_ptr(), hb.data_ptr(), w, h, pitch, hpa, hna, hpb, hnb, hda, hdb)
+        assert int(hna[0]) == len(pa) and int(hnb[0]) == len(pb)
+        assert np.array_equal(hpa[:len(pa)].view(PT).reshape(-1), pa)
+        assert np.array_equal(hpb[:len(pb)].view(PT).reshape(-1), pb)
+        assert np.array_equal(hda[:len(pa)], da) and np.array_equal(hdb[:len(pb)], db)
+    ctx.close()
+    ref.close()
