@@ -134,6 +134,38 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, int* v) {
 // Dot value given to database columns past the end of the set (never selected).
 constexpr int kMaskedDot = -65536;
 
+// Three-input max of float bit patterns, without flushing denormals.
+__device__ __forceinline__ float fmax3_bits(float a, float b, float c) {
+  float r;
+  asm("max.f32 %0, %1, %2, %3;" : "=f"(r) : "f"(a), "f"(b), "f"(c));
+  return r;
+}
+
+// Whether any of 32 dot products exceeds thr.  With thr >= 0 the values are
+// reduced as float bit patterns by three-input max: a non-negative int32 is a
+// zero or denormal float and keeps its order, a negative one is a NaN, which
+// max ignores (it cannot exceed a non-negative thr anyway); 16 instructions
+// instead of the 31 of an integer max.  A negative thr takes the integer max.
+__device__ __forceinline__ bool any_exceeds32(const int* v, int thr) {
+  if (thr >= 0) {
+    float m[12];
+#pragma unroll
+    for (int i = 0; i < 10; i++)
+      m[i] = fmax3_bits(__int_as_float(v[3 * i]), __int_as_float(v[3 * i + 1]), __int_as_float(v[3 * i + 2]));
+    m[10] = __int_as_float(v[30]);
+    m[11] = __int_as_float(v[31]);
+    const float r0 = fmax3_bits(m[0], m[1], m[2]), r1 = fmax3_bits(m[3], m[4], m[5]);
+    const float r2 = fmax3_bits(m[6], m[7], m[8]), r3 = fmax3_bits(m[9], m[10], m[11]);
+    const float r = fmax3_bits(r0, r1, fmax3_bits(r2, r3, r3));
+    const int rb = __float_as_int(r);
+    return rb > thr && rb < 0x7F800000;  // all 32 negative: the result is a NaN
+  }
+  int m = v[0];
+#pragma unroll
+  for (int j = 1; j < 32; j++) m = max(m, v[j]);
+  return m > thr;
+}
+
 // Global key (distance << 22 | index) of a chunk-local key (dot << 5 | 31 - column).
 __device__ __forceinline__ uint32_t local_to_key(int lk, int g_chunk) {
   const int dot = lk >> 5;
@@ -342,12 +374,9 @@ __global__ void __launch_bounds__(kIThreads, 1)
       int thr = (k2 == kNoKeyShared) ? kMaskedDot : 256 - 2 * (int)(k2 >> kIdxBitsShared);
 #pragma unroll
       for (int c = 0; c < 2; c++) {
-        int m = v[32 * c];
-#pragma unroll
-        for (int j = 1; j < 32; j++) m = max(m, v[32 * c + j]);
         // columns arrive in increasing index order, so only a strictly larger dot
         // than the current second best can enter the top two
-        if (__any_sync(0xffffffffu, m > thr)) {
+        if (__any_sync(0xffffffffu, any_exceeds32(v + 32 * c, thr))) {
           // top two of the chunk on local keys (dot << 5 | 31 - column): ties keep the lower column
           int a1 = INT_MIN, a2 = INT_MIN;
 #pragma unroll
@@ -829,9 +858,6 @@ __global__ void __launch_bounds__(kRrThreads, 1) k_rerank_imma(RerankImmaArgs a)
             for (int j = 0; j < 32; j++)
               if (j >= valid) v[j] = kMaskedDot;
           }
-          int m = v[0];
-#pragma unroll
-          for (int j = 1; j < 32; j++) m = max(m, v[j]);
           // The cluster's list is in increasing database index and the columns
           // arrive in list order, so only a strictly larger dot' (a strictly
           // smaller distance) than the current second best's can enter.
@@ -840,7 +866,7 @@ __global__ void __launch_bounds__(kRrThreads, 1) k_rerank_imma(RerankImmaArgs a)
           // columns farther than it cannot reach the query's top two (equal
           // distances stay, their index decides)
           if (gb != kNoKeyShared) thr = max(thr, pc - (int)(gb >> kIdxBitsShared) - 1);
-          if (__any_sync(0xffffffffu, m > thr)) {
+          if (__any_sync(0xffffffffu, any_exceeds32(v, thr))) {
             // the chunk's best two on local keys (dot' << 5 | 31 - column): ties keep the lower column
             int a1 = INT_MIN, a2 = INT_MIN;
 #pragma unroll
