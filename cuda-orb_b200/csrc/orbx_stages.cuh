@@ -305,6 +305,40 @@ struct DetSmem {
   int ow[kMaxOctaves], oh[kMaxOctaves];
 };
 
+// Pre-test of word w (four centres) of octave O of a detect tile: octave O
+// has (32 >> O) rows of (16 >> O) words.  Centres that pass are appended to
+// the tile's candidate list.
+template <int O>
+__device__ __forceinline__ void pretest_word(int w, int X0, int Y0, const uint8_t* s_stage, int ow, int oh,
+                                             uint32_t t4, int* s_n, uint16_t* s_cand) {
+  static_assert(kDetTW == 64 && kDetTH == 32, "word layout assumes 64 x 32 detect tiles");
+  constexpr int nwl = 4 - O;  // log2 words per row
+  constexpr int sw = (kDetTW >> O) + 2 * kHalo;
+  constexpr int off = det_stage_off(O);
+  const int ly = w >> nwl, lx = (w & ((1 << nwl) - 1)) << 2;
+  const int x = (X0 >> O) + lx, y = (Y0 >> O) + ly;
+  uint32_t m = 0u;
+  if (y >= 3 && y < oh - 3 && x < ow - 3) {
+    m = fast9_pretest4(s_stage + off + (ly + kHalo) * sw + (lx + kHalo), sw, t4);
+    if (x < 3 || x + 3 >= ow - 3) {  // border word: keep the centres with 3 <= x + k < ow - 3
+      uint32_t vm = 0u;
+#pragma unroll
+      for (int k = 0; k < 4; k++)
+        if (x + k >= 3 && x + k < ow - 3) vm |= 0xFFu << (8 * k);
+      m &= vm;
+    }
+  }
+  m &= 0x80808080u;
+  if (m) {
+    int pos = atomicAdd(&s_n[0], __popc(m));
+    while (m) {
+      const int k = (__ffs(m) >> 3) - 1;
+      m &= m - 1u;
+      s_cand[pos++] = det_item(O, ly, lx + k);
+    }
+  }
+}
+
 // One detect tile (tile index t over the batch).  P: the raw pyramid was
 // written earlier in the same launch (coherent loads instead of the read-only path).
 template <bool P>
@@ -352,43 +386,21 @@ __device__ __forceinline__ void det_tile(const Batch& b, int t, DetSmem& sm) {
   }
   __syncthreads();
 
-  // 1. cardinal pre-test, four centres per word, words of every octave spread
-  //    over the whole block (octave o has (32 >> o) rows of (16 >> o) words)
+  // 1. cardinal pre-test, four centres per word: the 512 words of octave 0 take
+  //    two passes of the block, the 128 + 32 + 8 + 2 words of octaves 1..4 one
   {
     const uint32_t t4 = (uint32_t)min(max(thr, 0), 255) * 0x01010101u;
-    int total = 0;
-    for (int o = 0; o < n_oct; o++) total += 512 >> (2 * o);
-    for (int i = threadIdx.x; i < total; i += blockDim.x) {
-      int o = 0, w = i;
-      while (w >= (512 >> (2 * o))) {
-        w -= 512 >> (2 * o);
-        o++;
-      }
-      const int nwl = 4 - o;  // log2 words per row
-      const int ly = w >> nwl, lx = (w & ((1 << nwl) - 1)) << 2;
-      const int x = (X0 >> o) + lx, y = (Y0 >> o) + ly;
-      const int ow = s_ow[o], oh = s_oh[o];
-      uint32_t m = 0u;
-      if (y >= 3 && y < oh - 3 && x < ow - 3) {
-        const int sw = (kDetTW >> o) + 2 * kHalo;
-        m = fast9_pretest4(s_stage + det_stage_off(o) + (ly + kHalo) * sw + (lx + kHalo), sw, t4);
-        if (x < 3 || x + 3 >= ow - 3) {  // border word: keep the centres with 3 <= x + k < ow - 3
-          uint32_t vm = 0u;
-#pragma unroll
-          for (int k = 0; k < 4; k++)
-            if (x + k >= 3 && x + k < ow - 3) vm |= 0xFFu << (8 * k);
-          m &= vm;
-        }
-      }
-      m &= 0x80808080u;
-      if (m) {
-        int pos = atomicAdd(&s_n[0], __popc(m));
-        while (m) {
-          const int k = (__ffs(m) >> 3) - 1;
-          m &= m - 1u;
-          s_cand[pos++] = det_item(o, ly, lx + k);
-        }
-      }
+    const int t = threadIdx.x;
+    pretest_word<0>(t, X0, Y0, s_stage, s_ow[0], s_oh[0], t4, s_n, s_cand);
+    pretest_word<0>(t + 256, X0, Y0, s_stage, s_ow[0], s_oh[0], t4, s_n, s_cand);
+    if (t < 128) {
+      if (n_oct > 1) pretest_word<1>(t, X0, Y0, s_stage, s_ow[1], s_oh[1], t4, s_n, s_cand);
+    } else if (t < 160) {
+      if (n_oct > 2) pretest_word<2>(t - 128, X0, Y0, s_stage, s_ow[2], s_oh[2], t4, s_n, s_cand);
+    } else if (t < 168) {
+      if (n_oct > 3) pretest_word<3>(t - 160, X0, Y0, s_stage, s_ow[3], s_oh[3], t4, s_n, s_cand);
+    } else if (t < 170) {
+      if (n_oct > 4) pretest_word<4>(t - 168, X0, Y0, s_stage, s_ow[4], s_oh[4], t4, s_n, s_cand);
     }
   }
   __syncthreads();
