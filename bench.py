@@ -427,6 +427,31 @@ def run_orbx(args, world, rank, local):
             e1.synchronize()
             imma_ms.append(e0.elapsed_time(e1))
     imma_pa, _ = A.to_host()
+
+    # both forms of the device-resident pair: five graph-replayed launches and
+    # one persistent launch with a device work queue
+    pair_forms = {}
+    keep_t = ctx.get_tuning()
+    for name, form in (("five_launch", 0), ("persistent", 1)):
+        t = ctx.get_tuning()
+        t.pair_form = form
+        ctx.set_tuning(t)
+        f_ms = []
+        with torch.cuda.stream(stream):
+            for _ in range(3):
+                step()
+            for _ in range(min(args.steps, 100)):
+                flush.zero_()
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                step()
+                e1.record(stream)
+                e1.synchronize()
+                f_ms.append(e0.elapsed_time(e1))
+        fa, fda = A.to_host()
+        pair_forms[name] = {"ms": statistics.median(f_ms),
+                            "equal_to_timed_run": bool(np.array_equal(fa, host_pa) and np.array_equal(fda, host_da))}
+    ctx.set_tuning(keep_t)
     pair_imma = {"ms": statistics.median(imma_ms), "steps": len(imma_ms),
                  "matches_equal_popc": bool(np.array_equal(imma_pa["match"], host_pa["match"]) and
                                             np.array_equal(imma_pa["distance"], host_pa["distance"]))}
@@ -541,6 +566,7 @@ def run_orbx(args, world, rank, local):
             "roofline": roofline,
             "kernels": kernels,
             "pair_int8_tcgen05_matcher": pair_imma,
+            "pair_forms": pair_forms,
             "clocks": clocks,
         }
         if match_bench:

@@ -145,6 +145,8 @@ struct orbx_ctx {
   cudaStream_t copy_stream = nullptr;
   cudaEvent_t ev_reset = nullptr;
   int upload_bands = 0;  // orbx_pair_host: 0 = copy then run; 1..16 = bands overlapped with the persistent launch
+  int pair_form = 0;     // orbx_pair: 0 = five graph-replayed launches, 1 = one persistent launch
+  PairGraph ppg;         // orbx_pair's persistent graph
   int memops = -1;       // stream write-value support: -1 unknown, 0 no, 1 yes
   // device-side waits
   int wait_us = 1000000;
@@ -711,6 +713,7 @@ ORBX_API int orbx_destroy(orbx_ctx* c) {
   persist_free(c->pbatch);
   persist_free(c->ppair);
   if (c->pho.exec) cudaGraphExecDestroy(c->pho.exec);
+  if (c->ppg.exec) cudaGraphExecDestroy(c->ppg.exec);
   cudaFree(c->pho.mw.part);
   cudaFree(c->pho.mw.tile_done);
   if (c->copy_stream) cudaStreamDestroy(c->copy_stream);
@@ -788,11 +791,13 @@ ORBX_API int orbx_init(orbx_ctx* c, const orbx_params* p) {
   ORBX_CUDA(cudaMemcpy(c->d_umax, umax, sizeof(umax), cudaMemcpyHostToDevice));
   if (shape_change)
     for (auto& ws : c->ws) ws_free(ws);
-  if (c->pg.exec) {
-    cudaGraphExecDestroy(c->pg.exec);
-    c->pg.exec = nullptr;
+  for (PairGraph* g : {&c->pg, &c->ppg, &c->pho}) {
+    if (g->exec) {
+      cudaGraphExecDestroy(g->exec);
+      g->exec = nullptr;
+    }
+    g->valid = false;
   }
-  c->pg.valid = false;
   c->single.last.clear();
   c->pair.last.clear();
   c->inited = true;
@@ -915,6 +920,54 @@ ORBX_API int orbx_match_knn2(orbx_ctx* c, const uint8_t* d_q, int nq, const uint
   return match_common(c, c->mw, a, nq, ndb, mode);
 }
 
+static int persist_prepare(orbx_ctx* c, PersistBufs& pb, const LaunchPlan& pl, const std::vector<Frame>& frames,
+                           const std::vector<MatchJob>& jobs, int blocks_per_pair, int group, PersistArgs* out,
+                           int* grid_out);
+
+// orbx_pair as one persistent launch (orbx_persist.cu) over the pair's two
+// frames: a graph of a counter reset and the launch.
+static int pair_persistent(orbx_ctx* c, const LaunchPlan& pl, const std::vector<Frame>& frames,
+                           const MatchArgs& m) {
+  PairGraph& pg = c->ppg;
+  int rc;
+  if ((rc = mw_ensure(pg.mw, c->p.max_pts)) != 0) return rc;
+  std::vector<MatchJob> jobs(1);
+  std::memset(jobs.data(), 0, sizeof(MatchJob));
+  jobs[0].args = m;
+  jobs[0].work = pg.mw;
+  PersistArgs a;
+  int grid = 0;
+  if ((rc = persist_prepare(c, c->ppair, pl, frames, jobs, 2 * 148, 0, &a, &grid)) != 0) return rc;
+  std::vector<uint8_t> key(sizeof(PersistArgs) + sizeof(int));
+  std::memcpy(key.data(), &a, sizeof(PersistArgs));
+  std::memcpy(key.data() + sizeof(PersistArgs), &grid, sizeof(int));
+  if (!(pg.valid && pg.key == key)) {
+    if (pg.exec) {
+      cudaGraphExecDestroy(pg.exec);
+      pg.exec = nullptr;
+    }
+    pg.valid = false;
+    cudaGraph_t graph = nullptr;
+    ORBX_CUDA(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+    cudaError_t le = cudaMemsetAsync(a.done, 0, sizeof(int) * (4 * 2 + 1), c->stream);
+    if (le == cudaSuccess) le = launch_batch_persistent(a, grid, c->stream);
+    const cudaError_t ce = cudaStreamEndCapture(c->stream, &graph);
+    if (le != cudaSuccess) {
+      if (graph) cudaGraphDestroy(graph);
+      (void)cudaGetLastError();
+      return ORBX_ERR_CUDA;
+    }
+    ORBX_CUDA(ce);
+    const cudaError_t ie = cudaGraphInstantiate(&pg.exec, graph, 0);
+    cudaGraphDestroy(graph);
+    ORBX_CUDA(ie);
+    pg.key.swap(key);
+    pg.valid = true;
+  }
+  ORBX_CUDA(cudaGraphLaunch(pg.exec, c->stream));
+  return ORBX_OK;
+}
+
 ORBX_API int orbx_pair(orbx_ctx* c, const uint8_t* d_img_a, const uint8_t* d_img_b, int w, int h, int pitch,
                        orbx_point* d_pts_a, uint8_t* d_desc_a, int* d_n_a, orbx_point* d_pts_b, uint8_t* d_desc_b,
                        int* d_n_b, int mode) {
@@ -941,6 +994,7 @@ ORBX_API int orbx_pair(orbx_ctx* c, const uint8_t* d_img_a, const uint8_t* d_img
   a.d_nq = d_n_a;
   a.d_ndb = d_n_b;
   a.pts = d_pts_a;
+  if (c->pair_form == 1 && mode == ORBX_MATCH_POPC) return pair_persistent(c, pl, frames, a);
   // graph key: launch shapes and every pointer baked into the captured launches
   std::vector<uint8_t> key(sizeof(Batch) + sizeof(MatchArgs) + sizeof(LaunchPlan) + sizeof(int));
   {
@@ -979,10 +1033,6 @@ ORBX_API int orbx_pair(orbx_ctx* c, const uint8_t* d_img_a, const uint8_t* d_img
   ORBX_CUDA(cudaGraphLaunch(pg.exec, c->stream));
   return ORBX_OK;
 }
-
-static int persist_prepare(orbx_ctx* c, PersistBufs& pb, const LaunchPlan& pl, const std::vector<Frame>& frames,
-                           const std::vector<MatchJob>& jobs, int blocks_per_pair, int group, PersistArgs* out,
-                           int* grid_out);
 
 // cuStreamWriteValue32 through the runtime's driver entry point (no link-time
 // dependency on the driver library): a copy stream publishes each uploaded band.
@@ -1246,6 +1296,7 @@ ORBX_API int orbx_get_tuning(orbx_ctx* c, orbx_tuning* t) {
   t->persist_blocks_per_sm = c->persist_bps;
   t->wait_timeout_us = c->wait_us;
   t->upload_bands = c->upload_bands;
+  t->pair_form = c->pair_form;
   return ORBX_OK;
 }
 
@@ -1256,7 +1307,7 @@ ORBX_API int orbx_set_tuning(orbx_ctx* c, const orbx_tuning* t) {
       t->match_blocks_per_pair < 0 || t->match_blocks_per_pair > 4096 || t->batch_form < 0 || t->batch_form > 1 ||
       t->persist_group < 0 || t->persist_group > kMaxFramesPerLaunch || t->persist_blocks_per_sm < 0 ||
       t->persist_blocks_per_sm > 32 || t->wait_timeout_us < 1 || t->wait_timeout_us > 10000000 ||
-      t->upload_bands < 0 || t->upload_bands > 16)
+      t->upload_bands < 0 || t->upload_bands > 16 || t->pair_form < 0 || t->pair_form > 1)
     return ORBX_ERR_ARG;
   c->nms_rows = t->nms_rows;
   c->describe_bps = t->describe_blocks_per_sm;
@@ -1267,6 +1318,7 @@ ORBX_API int orbx_set_tuning(orbx_ctx* c, const orbx_tuning* t) {
   c->persist_bps = t->persist_blocks_per_sm;
   c->wait_us = t->wait_timeout_us;
   c->upload_bands = t->upload_bands;
+  c->pair_form = t->pair_form;
   c->wait_cycles = (long long)c->wait_us * c->clock_khz / 1000;
   if (c->batch_exec) {
     cudaGraphExecDestroy(c->batch_exec);
@@ -1274,11 +1326,13 @@ ORBX_API int orbx_set_tuning(orbx_ctx* c, const orbx_tuning* t) {
   }
   c->batch_key.clear();
   // cached graphs baked in the old shapes
-  if (c->pg.exec) {
-    cudaGraphExecDestroy(c->pg.exec);
-    c->pg.exec = nullptr;
+  for (PairGraph* g : {&c->pg, &c->ppg, &c->pho}) {
+    if (g->exec) {
+      cudaGraphExecDestroy(g->exec);
+      g->exec = nullptr;
+    }
+    g->valid = false;
   }
-  c->pg.valid = false;
   c->single.last.clear();
   c->pair.last.clear();
   return ORBX_OK;

@@ -230,6 +230,8 @@ typedef struct orbx_tuning {
   int upload_bands;           /* orbx_pair_host: 0 = copy both images, then run the pair; 1..16 = copy them in
                                  this many row bands per image on a second stream while one persistent launch
                                  already processes the bands that have arrived (popcount matching) */
+  int pair_form;              /* orbx_pair: 0 = five graph-replayed launches, 1 = one persistent launch
+                                 (popcount matching) */
 } orbx_tuning;
 
 ORBX_API int orbx_get_tuning(orbx_ctx* ctx, orbx_tuning* t);

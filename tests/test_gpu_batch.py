@@ -212,3 +212,21 @@ def test_wait_timeout_tuning_is_validated():
     with pytest.raises(orbx.OrbxError):
         ctx.set_tuning(t)
     ctx.close()
+
+
+@pytest.mark.parametrize("w,h,seed,cap", [(1920, 1080, 7, 10000), (333, 257, 8, 200), (3840, 2160, 9, 10000)])
+def test_pair_persistent_form_equals_five_launches(w, h, seed, cap):
+    """orbx_pair as one persistent launch gives exactly the five-launch results."""
+    a, b, _ = synth.make_pair(w, h, seed=seed)
+    five = orbx.Context(0, orbx.make_params(max_pts=cap))
+    pers = orbx.Context(0, orbx.make_params(max_pts=cap))
+    t = pers.get_tuning()
+    t.pair_form = 1
+    pers.set_tuning(t)
+    want = _single(five, a, b, w, h, cap)
+    for _ in range(3):
+        got = _single(pers, a, b, w, h, cap)
+        for g, e in zip(got, want):
+            assert np.array_equal(g, e)
+    five.close()
+    pers.close()
