@@ -146,6 +146,7 @@ struct orbx_ctx {
   cudaEvent_t ev_reset = nullptr;
   int upload_bands = 0;  // orbx_pair_host: 0 = copy then run; 1..16 = bands overlapped with the persistent launch
   int pair_form = 0;     // orbx_pair: 0 = five graph-replayed launches, 1 = one persistent launch
+  int pyr_shape = 0;     // pyramid tile shape of the five-launch forms (kPyrShapeTW/TH)
   PairGraph ppg;         // orbx_pair's persistent graph
   int memops = -1;       // stream write-value support: -1 unknown, 0 no, 1 yes
   // device-side waits
@@ -355,7 +356,7 @@ static void set_nms_shape(Frame& F, int border, int rows_req) {
 }
 
 static void fill_frame(const orbx_ctx* c, const Workspace& ws, const uint8_t* img, int pitch_in, orbx_point* pts,
-                       uint8_t* desc, int* count, Frame& F, int max_pts = -1) {
+                       uint8_t* desc, int* count, Frame& F, int max_pts = -1, int pyr_shape = 0) {
   std::memset(&F, 0, sizeof(F));
   const int n = ws.n;
   F.img = img;
@@ -383,12 +384,13 @@ static void fill_frame(const orbx_ctx* c, const Workspace& ws, const uint8_t* im
   F.border = c->p.edge_threshold < 3 ? 3 : c->p.edge_threshold;
   int acc = 0;
   for (int o = 0; o < n; o++) {
-    F.pyr_tiles_x[o] = div_up(F.ow[o], kPyrTW);
-    F.pyr_tiles_y[o] = div_up(F.oh[o], kPyrTH);
+    F.pyr_tiles_x[o] = div_up(F.ow[o], kPyrShapeTW[pyr_shape]);
+    F.pyr_tiles_y[o] = div_up(F.oh[o], kPyrShapeTH[pyr_shape]);
     F.pyr_tile_base[o] = acc;
     acc += F.pyr_tiles_x[o] * F.pyr_tiles_y[o];
   }
   F.pyr_tile_base[n] = acc;
+  F.pyr_shape = pyr_shape;
   F.det_tiles_x = div_up(F.w, kDetTW);
   F.det_tiles_y = div_up(F.h, kDetTH);
   set_nms_shape(F, F.border, c->nms_rows);
@@ -455,6 +457,7 @@ static int upload_batch(orbx_ctx* c, BatchSlot& bs, const std::vector<Frame>& fr
   b.nms_ticket = bs.d_ticket;
   b.err = c->d_err;
   b.wait_cycles = c->wait_cycles;
+  b.pyr_shape = frames[0].pyr_shape;
   b.fast_thr = c->p.fast_threshold;
   b.harris = c->p.score_type == 0 ? 1 : 0;
   b.wta_k = c->p.wta_k;
@@ -823,7 +826,7 @@ ORBX_API int orbx_detect_and_compute(orbx_ctx* c, const uint8_t* d_image, int w,
   rc = ws_ensure(c, c->ws[0], w, h);
   if (rc) return rc;
   std::vector<Frame> frames(1);
-  fill_frame(c, c->ws[0], d_image, pitch, d_points, d_desc, d_num_pts, frames[0]);
+  fill_frame(c, c->ws[0], d_image, pitch, d_points, d_desc, d_num_pts, frames[0], -1, c->pyr_shape);
   LaunchPlan pl;
   rc = upload_batch(c, c->single, frames, &pl);
   if (rc) return rc;
@@ -982,8 +985,9 @@ ORBX_API int orbx_pair(orbx_ctx* c, const uint8_t* d_img_a, const uint8_t* d_img
   if ((rc = ws_ensure(c, c->ws[1], w, h)) != 0) return rc;
   if (mode == ORBX_MATCH_IMMA && (rc = imma_ensure(c, c->p.max_pts, c->p.max_pts)) != 0) return rc;
   std::vector<Frame> frames(2);
-  fill_frame(c, c->ws[0], d_img_a, pitch, d_pts_a, d_desc_a, d_n_a, frames[0]);
-  fill_frame(c, c->ws[1], d_img_b, pitch, d_pts_b, d_desc_b, d_n_b, frames[1]);
+  const int shape = (c->pair_form == 1 && mode == ORBX_MATCH_POPC) ? 0 : c->pyr_shape;
+  fill_frame(c, c->ws[0], d_img_a, pitch, d_pts_a, d_desc_a, d_n_a, frames[0], -1, shape);
+  fill_frame(c, c->ws[1], d_img_b, pitch, d_pts_b, d_desc_b, d_n_b, frames[1], -1, shape);
   LaunchPlan pl;
   if ((rc = upload_batch(c, c->pair, frames, &pl)) != 0) return rc;
   MatchArgs a{};
@@ -1254,8 +1258,8 @@ ORBX_API int orbx_profile_pair(orbx_ctx* c, const uint8_t* d_img_a, const uint8_
   if ((rc = ws_ensure(c, c->ws[0], w, h)) != 0) return rc;
   if ((rc = ws_ensure(c, c->ws[1], w, h)) != 0) return rc;
   std::vector<Frame> frames(2);
-  fill_frame(c, c->ws[0], d_img_a, pitch, d_pts_a, d_desc_a, d_n_a, frames[0]);
-  fill_frame(c, c->ws[1], d_img_b, pitch, d_pts_b, d_desc_b, d_n_b, frames[1]);
+  fill_frame(c, c->ws[0], d_img_a, pitch, d_pts_a, d_desc_a, d_n_a, frames[0], -1, c->pyr_shape);
+  fill_frame(c, c->ws[1], d_img_b, pitch, d_pts_b, d_desc_b, d_n_b, frames[1], -1, c->pyr_shape);
   LaunchPlan pl;
   if ((rc = upload_batch(c, c->pair, frames, &pl)) != 0) return rc;
   if ((rc = mw_ensure(c->mw, c->p.max_pts)) != 0) return rc;
@@ -1297,6 +1301,7 @@ ORBX_API int orbx_get_tuning(orbx_ctx* c, orbx_tuning* t) {
   t->wait_timeout_us = c->wait_us;
   t->upload_bands = c->upload_bands;
   t->pair_form = c->pair_form;
+  t->pyr_tile = c->pyr_shape;
   return ORBX_OK;
 }
 
@@ -1307,7 +1312,8 @@ ORBX_API int orbx_set_tuning(orbx_ctx* c, const orbx_tuning* t) {
       t->match_blocks_per_pair < 0 || t->match_blocks_per_pair > 4096 || t->batch_form < 0 || t->batch_form > 1 ||
       t->persist_group < 0 || t->persist_group > kMaxFramesPerLaunch || t->persist_blocks_per_sm < 0 ||
       t->persist_blocks_per_sm > 32 || t->wait_timeout_us < 1 || t->wait_timeout_us > 10000000 ||
-      t->upload_bands < 0 || t->upload_bands > 16 || t->pair_form < 0 || t->pair_form > 1)
+      t->upload_bands < 0 || t->upload_bands > 16 || t->pair_form < 0 || t->pair_form > 1 ||
+      t->pyr_tile < 0 || t->pyr_tile >= kPyrShapes)
     return ORBX_ERR_ARG;
   c->nms_rows = t->nms_rows;
   c->describe_bps = t->describe_blocks_per_sm;
@@ -1319,6 +1325,7 @@ ORBX_API int orbx_set_tuning(orbx_ctx* c, const orbx_tuning* t) {
   c->wait_us = t->wait_timeout_us;
   c->upload_bands = t->upload_bands;
   c->pair_form = t->pair_form;
+  c->pyr_shape = t->pyr_tile;
   c->wait_cycles = (long long)c->wait_us * c->clock_khz / 1000;
   if (c->batch_exec) {
     cudaGraphExecDestroy(c->batch_exec);
@@ -1496,7 +1503,8 @@ static int batch_pairs_impl(orbx_ctx* c, int n_pairs, const orbx_image* ia, cons
       const orbx_frame_out& o = s ? ob[i] : oa[i];
       Workspace& ws = c->bws[2 * i + s];
       if ((rc = ws_ensure(c, ws, im.w, im.h)) != 0) return rc;
-      fill_frame(c, ws, im.data, im.pitch, o.points, o.desc, o.num_pts, frames[2 * i + s], o.max_pts);
+      fill_frame(c, ws, im.data, im.pitch, o.points, o.desc, o.num_pts, frames[2 * i + s], o.max_pts,
+                 (c->batch_form == 1 && !stage_ms) ? 0 : c->pyr_shape);
     }
   }
   LaunchPlan pl;
@@ -1689,31 +1697,51 @@ ORBX_API int orbx_autotune_pairs_forms(orbx_ctx* c, int n_pairs, const orbx_imag
         }
   orbx_tuning top = keep;
   float top_ms = 1e30f;
+  orbx_tuning top5 = keep;  // best of the five-launch form, for the tile-shape pass
+  float top5_ms = 1e30f;
   int rc = ORBX_OK;
+  // median of `reps` replays of one candidate (the first call captures its graph)
+  auto measure = [&](const orbx_tuning& t, float* out) -> int {
+    int r;
+    if ((r = orbx_set_tuning(c, &t)) != 0) return r;
+    if ((r = orbx_batch_pairs(c, n_pairs, ia, ib, oa, ob, ORBX_MATCH_POPC)) != 0) return r;
+    std::vector<float> ms;
+    for (int k = 0; k < reps; k++) {
+      cudaEventRecord(e0, c->stream);
+      if ((r = orbx_batch_pairs(c, n_pairs, ia, ib, oa, ob, ORBX_MATCH_POPC)) != 0) return r;
+      cudaEventRecord(e1, c->stream);
+      if (cudaEventSynchronize(e1) != cudaSuccess) return ORBX_ERR_CUDA;
+      float v = 0.f;
+      cudaEventElapsedTime(&v, e0, e1);
+      ms.push_back(v);
+    }
+    std::sort(ms.begin(), ms.end());
+    *out = ms[ms.size() / 2];
+    return ORBX_OK;
+  };
   for (const orbx_tuning& t : cands) {
-    {
-      {
-        if ((rc = orbx_set_tuning(c, &t)) != 0) goto done;
-        if ((rc = orbx_batch_pairs(c, n_pairs, ia, ib, oa, ob, ORBX_MATCH_POPC)) != 0) goto done;  // capture
-        std::vector<float> ms;
-        for (int k = 0; k < reps; k++) {
-          cudaEventRecord(e0, c->stream);
-          if ((rc = orbx_batch_pairs(c, n_pairs, ia, ib, oa, ob, ORBX_MATCH_POPC)) != 0) goto done;
-          cudaEventRecord(e1, c->stream);
-          if (cudaEventSynchronize(e1) != cudaSuccess) {
-            rc = ORBX_ERR_CUDA;
-            goto done;
-          }
-          float v = 0.f;
-          cudaEventElapsedTime(&v, e0, e1);
-          ms.push_back(v);
-        }
-        std::sort(ms.begin(), ms.end());
-        const float med = ms[ms.size() / 2];
-        if (med < top_ms) {
-          top_ms = med;
-          top = t;
-        }
+    float med = 0.f;
+    if ((rc = measure(t, &med)) != 0) goto done;
+    if (med < top_ms) {
+      top_ms = med;
+      top = t;
+    }
+    if (t.batch_form == 0 && med < top5_ms) {
+      top5_ms = med;
+      top5 = t;
+    }
+  }
+  // second pass: the pyramid tile shapes on the best five-launch candidate
+  if (forms & 1) {
+    for (int shape = 0; shape < kPyrShapes; shape++) {
+      if (shape == top5.pyr_tile) continue;
+      orbx_tuning t = top5;
+      t.pyr_tile = shape;
+      float med = 0.f;
+      if ((rc = measure(t, &med)) != 0) goto done;
+      if (med < top_ms) {
+        top_ms = med;
+        top = t;
       }
     }
   }

@@ -11,9 +11,14 @@ constexpr int kMaxOctaves = 5;        // MAX_OCTAVE, orbd.cu:18
 constexpr int kMaxFramesPerLaunch = 1024;
 constexpr size_t kGuard = 256 * 1024; // zeroed bytes before/after each pyramid
 
-// Pyramid-and-blur tile (octave pixels)
+// Pyramid-and-blur tile (octave pixels): the default shape, which the
+// persistent kernel uses; the five-launch kernel also has the other shapes of
+// kPyrShapeTW/TH (tuning pyr_tile), one instantiation each
 constexpr int kPyrTW = 128;
 constexpr int kPyrTH = 32;
+constexpr int kPyrShapes = 4;
+constexpr int kPyrShapeTW[kPyrShapes] = {128, 64, 128, 64};
+constexpr int kPyrShapeTH[kPyrShapes] = {32, 32, 16, 64};
 // Detect tile (level-0 pixels); 32 keeps octave 4/5 tiles whole
 constexpr int kDetTW = 64;
 constexpr int kDetTH = 32;
@@ -43,6 +48,7 @@ struct Frame {
   int max_pts;
   int border;    // max(edge_threshold, 3)
   // tiling
+  int pyr_shape;  // index into kPyrShapeTW/TH of the pyramid tile tables below
   int pyr_tiles_x[kMaxOctaves], pyr_tiles_y[kMaxOctaves];
   int pyr_tile_base[kMaxOctaves + 1];  // per-octave prefix within the frame
   int det_tiles_x, det_tiles_y;
@@ -61,6 +67,7 @@ struct Batch {
   unsigned int* nms_ticket;  // dynamic strip ticket (reset by k_pyramid_blur)
   int* err;              // sticky error word (bounded waits that gave up)
   long long wait_cycles; // bound of every device-side wait, in SM clock cycles
+  int pyr_shape;         // pyramid tile shape of every frame of the launch
   int describe_mode;     // 0: angle + descriptor, 1: angle only, 2: descriptor only
   // parameters (Orbor::init, orb.h:18-19)
   int fast_thr;

@@ -31,7 +31,7 @@
 namespace orbx {
 
 union PersistSmem {
-  PyrSmem pyr;
+  PyrSmem<kPyrTW, kPyrTH> pyr;
   DetSmem det;
   NmsSmem nms;
   struct {

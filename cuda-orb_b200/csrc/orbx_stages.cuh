@@ -35,8 +35,6 @@ __device__ __forceinline__ T ldx(const T* p) {
 // the octaves are read from an existing pyramid instead (hGassianBlur on a
 // caller's buffer, orbd.cu:1732-1773).
 // ---------------------------------------------------------------------------
-constexpr int kPyrSW = kPyrTW + 8;  // 3-pixel halo each side, padded to a multiple of 4
-constexpr int kPyrSH = kPyrTH + 6;
 
 // Exact small-integer <-> float conversions on the full-rate pipes: a float
 // whose exponent field is 2^23 holds the integer in its mantissa.
@@ -47,16 +45,24 @@ __device__ __forceinline__ uint32_t float_to_u8_rne(float v) {  // 0 <= v < 2^22
   return (uint32_t)(__float_as_int(__fadd_rn(v, 12582912.0f)) - 0x4B400000);
 }
 
+// Staged source of a TW x TH tile: a 3-pixel halo on each side, the width
+// padded to a multiple of 4.
+template <int TW, int TH>
 struct PyrSmem {
-  __align__(16) float src[kPyrSH * kPyrSW];
-  __align__(16) uint8_t byte[kPyrSH * kPyrSW];
-  __align__(16) float row[kPyrSH * kPyrTW];
+  static constexpr int SW = TW + 8;
+  static constexpr int SH = TH + 6;
+  __align__(16) float src[SH * SW];
+  __align__(16) uint8_t byte[SH * SW];
+  __align__(16) float row[SH * TW];
 };
 
-// One pyramid tile (tile index t over the batch).  PL: the level-0 image is
-// copied in during the same launch (coherent loads instead of the read-only path).
-template <bool PL>
-__device__ __forceinline__ void pyr_tile(const Batch& b, int t, PyrSmem& sm) {
+// One pyramid tile (tile index t over the batch) of shape TW x TH.  PL: the
+// level-0 image is copied in during the same launch (coherent loads instead of
+// the read-only path).
+template <bool PL, int TW = kPyrTW, int TH = kPyrTH>
+__device__ __forceinline__ void pyr_tile(const Batch& b, int t, PyrSmem<TW, TH>& sm) {
+  constexpr int kPyrTW = TW, kPyrTH = TH;
+  constexpr int kPyrSW = PyrSmem<TW, TH>::SW, kPyrSH = PyrSmem<TW, TH>::SH;
   float* s_src = sm.src;
   uint8_t* s_byte = sm.byte;
   float* s_row = sm.row;

@@ -232,6 +232,8 @@ typedef struct orbx_tuning {
                                  already processes the bands that have arrived (popcount matching) */
   int pair_form;              /* orbx_pair: 0 = five graph-replayed launches, 1 = one persistent launch
                                  (popcount matching) */
+  int pyr_tile;               /* pyramid + blur tile of the five-launch forms: 0 = 128 x 32, 1 = 64 x 32,
+                                 2 = 128 x 16, 3 = 64 x 64 octave pixels (the persistent forms use 128 x 32) */
 } orbx_tuning;
 
 ORBX_API int orbx_get_tuning(orbx_ctx* ctx, orbx_tuning* t);

@@ -230,3 +230,20 @@ def test_pair_persistent_form_equals_five_launches(w, h, seed, cap):
             assert np.array_equal(g, e)
     five.close()
     pers.close()
+
+
+@pytest.mark.parametrize("shape", [1, 2, 3])
+def test_pyramid_tile_shapes_agree(batch, shape):
+    """Every pyramid + blur tile shape of the five-launch form gives the same
+    batch results (pair by pair equal to orbx_pair with the default shape)."""
+    ctx = orbx.Context(0, orbx.make_params(max_pts=10000))
+    single = orbx.Context(0, orbx.make_params(max_pts=10000))
+    t = ctx.get_tuning()
+    t.pyr_tile = shape
+    ctx.set_tuning(t)
+    pb = orbx.PairBatch(batch)
+    ctx.batch_pairs(pb)
+    ctx.sync()
+    _check_against_single(single, pb, batch)
+    ctx.close()
+    single.close()
