@@ -501,6 +501,20 @@ def run_orbx(args, world, rank, local):
     for bands in (0, 2, 4, 8):
         v_ev, v_wall = e2e_run(bands, min(e2e_steps, 50))
         e2e_variants[str(bands)] = {"ms": statistics.median(v_ev), "host_wall_ms": statistics.median(v_wall)}
+        # where the time goes: CUDA events between the phases and host clocks
+        t = ctx.get_tuning()
+        keep_b = t.upload_bands
+        t.upload_bands = bands
+        ctx.set_tuning(t)
+        phases = []
+        with torch.cuda.stream(stream):
+            for _ in range(min(e2e_steps, 30)):
+                flush.zero_()
+                stream.synchronize()
+                phases.append(ctx.profile_pair_host(ha.data_ptr(), hb.data_ptr(), W, H, pitch, hpa, hna, hpb, hnb))
+        t.upload_bands = keep_b
+        ctx.set_tuning(t)
+        e2e_variants[str(bands)]["phases_ms"] = {k: statistics.median(p[k] for p in phases) for k in phases[0]}
     h2d = 2 * H * pitch
     d2h = 8 + (int(hna[0]) + int(hnb[0])) * 28
 
@@ -639,25 +653,29 @@ def run_reference(args, world, rank, local):
     flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device=dev)
     steps = min(args.steps, 300)
 
-    def timed(zero_fill):
-        # zero_fill off: the reference's own per-call descriptor cudaMalloc
-        # without the harness's parity-run memset of the block and its guards
-        R.set_zero_fill(zero_fill)
-        R.time_pair(a, b, W, H, max(args.warmup, 3), 1)
-        out = []
-        for _ in range(steps):
-            flush.zero_()
-            torch.cuda.synchronize(dev)
-            t, na_, nb_ = R.time_pair(a, b, W, H, 0, 1)
-            out.append(t)
-        return out, na_, nb_
-
+    R.time_pair(a, b, W, H, max(args.warmup, 3), 1)
+    ms = []
     sampler = ClockSampler(local)
     sampler.start()
-    ms, na, nb = timed(False)
+    for _ in range(steps):
+        flush.zero_()
+        torch.cuda.synchronize(dev)
+        t, na, nb = R.time_pair(a, b, W, H, 0, 1)
+        ms.append(t)
     clocks = sampler.stop()
-    ms_fill, _, _ = timed(True)
-    R.set_zero_fill(True)
+    # The harness zero-fills every reference allocation with its guards (the
+    # reference reads outside its buffers by design); per pair that adds two
+    # fills of the descriptor block plus 512 KiB.  Their cost, timed alone:
+    fill = torch.empty((na * 32 + 512 * 1024), dtype=torch.uint8, device=dev)
+    fill_ms = []
+    for _ in range(50):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        fill.zero_()
+        fill[: nb * 32 + 512 * 1024].zero_()
+        e1.record()
+        e1.synchronize()
+        fill_ms.append(e0.elapsed_time(e1))
     value = sum(ms) / len(ms)
     lay = R.layout_for(W, H, 8)
     return {
@@ -667,9 +685,9 @@ def run_reference(args, world, rank, local):
         "data": "synthetic (same generator and seed as the library arm)",
         "config": pair_config(int(lay["n"]), na, nb),
         "impl_detail": {"api": "Orbor::detectAndCompute A and B, Orbor::match A->B (orb.cpp:57-113)",
-                        "with_parity_zero_fill_ms": sum(ms_fill) / len(ms_fill),
-                        "note": "value is timed without the harness's zero-fill of each allocation; "
-                                "with_parity_zero_fill_ms is the same run with it"},
+                        "harness_zero_fill_ms_est": statistics.median(fill_ms),
+                        "note": "includes the harness's zero-fill of each descriptor allocation and its guards; "
+                                "harness_zero_fill_ms_est is that fill's cost per pair, timed alone"},
         "e2e": {"value": value, "unit": "ms", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "cpu_baseline": {"value": value, "unit": "ms", "cores": 1, "kind": "reference",
                          "sample": f"{steps} pairs through the reference CUDA build (its orbd.cu/orb.cpp compiled "
@@ -821,17 +839,13 @@ def run_batch_workload(args, world, rank, local):
     ctx.close()
     if rank != 0:
         return None
-    ref = {"unavailable": "reference build oracle/_ref/libref_orb.so not built"}
-    from oracle import refharness as R
-
-    if R.available():
-        R.init(noctaves=8, edge=31, wta_k=2, score_type=0, patch=31, fast_thr=20, retain_topn=-1, max_pts=10000)
-        R.set_zero_fill(False)
-        rms, rkp = R.time_batch(pairs, 1, 3)
-        R.set_zero_fill(True)
-        ref = {"ms": rms, "keypoints": rkp, "ratio_vs_library": rms / ms,
-               "how": "reference build, pair by pair: Orbor::init(cap), detectAndCompute A and B, match; "
-                      "images resident on the device; CUDA events"}
+    # The reference build is not run on this workload: its angleIC (orbd.cu:1001-1010)
+    # reads keypoints up to the raw survivor count when the cap binds, past the
+    # points NMS wrote, and on this workload's binding caps that faulted the GPU
+    # (illegal memory access reported at orbd.cu:1727).
+    ref = {"unavailable": "the reference build reads past its keypoint array when the cap binds "
+                          "(angleIC, orbd.cu:1001-1010) and faulted with an illegal memory access on this "
+                          "workload; not run again"}
     # algorithmic bytes per batch: every image read once, 28 + 32 bytes out per keypoint
     alg = in_bytes + nkp * 60
     peaks, peak_kind = load_peaks()

@@ -1,6 +1,7 @@
 // C ABI of the sm_100a ORB library: contexts, constant tables, workspaces,
 // batch descriptors and the per-call launch sequences.
 #include <cuda.h>
+#include <chrono>
 #include <mutex>
 #include <cuda_runtime.h>
 
@@ -163,6 +164,10 @@ struct orbx_ctx {
       return _e == cudaErrorMemoryAllocation ? ORBX_ERR_NOMEM : ORBX_ERR_CUDA; \
     }                                  \
   } while (0)
+
+static double host_seconds() {
+  return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
 
 static inline int align_up(int a, int b) { return (a % b != 0) ? (a - a % b + b) : a; }
 static inline int div_up(int a, int b) { return (a + b - 1) / b; }
@@ -1168,9 +1173,15 @@ static int pair_host_overlap(orbx_ctx* c, const uint8_t* h_a, const uint8_t* h_b
   return ORBX_OK;
 }
 
-ORBX_API int orbx_pair_host(orbx_ctx* c, const uint8_t* h_img_a, const uint8_t* h_img_b, int w, int h, int pitch,
-                            orbx_point* h_pts_a, int* h_n_a, orbx_point* h_pts_b, int* h_n_b, uint8_t* h_desc_a,
-                            uint8_t* h_desc_b, int mode) {
+// orbx_pair_host; with `prof`, CUDA events and host clocks between the phases.
+struct PairHostProf {
+  cudaEvent_t ev[4];  // start, uploads done, kernels done, export done
+  double t_enqueued = 0, t_synced = 0;
+};
+
+static int pair_host_impl(orbx_ctx* c, const uint8_t* h_img_a, const uint8_t* h_img_b, int w, int h, int pitch,
+                          orbx_point* h_pts_a, int* h_n_a, orbx_point* h_pts_b, int* h_n_b, uint8_t* h_desc_a,
+                          uint8_t* h_desc_b, int mode, PairHostProf* prof) {
   int rc = check_image(c, h_img_a, w, h, pitch);
   if (rc) return rc;
   if (!h_img_b || !h_pts_a || !h_n_a || !h_pts_b || !h_n_b) return ORBX_ERR_ARG;
@@ -1203,6 +1214,7 @@ ORBX_API int orbx_pair_host(orbx_ctx* c, const uint8_t* h_img_a, const uint8_t* 
   }
   const uint8_t* res = nullptr;
   const bool with_desc = h_desc_a || h_desc_b;
+  if (prof) ORBX_CUDA(cudaEventRecord(prof->ev[0], c->stream));
   if (c->upload_bands > 0 && mode != ORBX_MATCH_IMMA && memops_ok(c)) {
     rc = pair_host_overlap(c, h_img_a, h_img_b, w, h, pitch, with_desc, &res);
     if (rc) {
@@ -1210,29 +1222,37 @@ ORBX_API int orbx_pair_host(orbx_ctx* c, const uint8_t* h_img_a, const uint8_t* 
       cudaStreamSynchronize(c->stream);
       return rc;
     }
+    if (prof) {
+      // the uploads end on the copy stream; kernels and export are one graph
+      ORBX_CUDA(cudaEventRecord(prof->ev[1], c->copy_stream));
+      ORBX_CUDA(cudaEventRecord(prof->ev[2], c->stream));
+      ORBX_CUDA(cudaEventRecord(prof->ev[3], c->stream));
+      prof->t_enqueued = host_seconds();
+    }
     ORBX_CUDA(cudaStreamSynchronize(c->stream));
     ORBX_CUDA(cudaStreamSynchronize(c->copy_stream));
   } else {
     ORBX_CUDA(cudaMemcpyAsync(c->io_img[0], h_img_a, ibytes, cudaMemcpyHostToDevice, c->stream));
     ORBX_CUDA(cudaMemcpyAsync(c->io_img[1], h_img_b, ibytes, cudaMemcpyHostToDevice, c->stream));
+    if (prof) ORBX_CUDA(cudaEventRecord(prof->ev[1], c->stream));
     rc = orbx_pair(c, c->io_img[0], c->io_img[1], w, h, pitch, c->io_pts[0], c->io_desc[0], c->io_count,
                    c->io_pts[1], c->io_desc[1], c->io_count + 1, mode);
     if (rc) return rc;
-    // one export kernel writes counts, keypoints (and descriptors) into mapped
-    // pinned memory, so the host waits once and copies only what was found
+    if (prof) ORBX_CUDA(cudaEventRecord(prof->ev[2], c->stream));
+    // one export kernel writes counts, the error word, keypoints (and
+    // descriptors) into mapped pinned memory, so the host waits once and
+    // copies only what was found
     if ((rc = hostio_export_pair(c, c->io_pts[0], c->io_pts[1], c->io_desc[0], c->io_desc[1], c->io_count,
                                  c->p.max_pts, with_desc, &res)) != 0)
       return rc;
+    if (prof) {
+      ORBX_CUDA(cudaEventRecord(prof->ev[3], c->stream));
+      prof->t_enqueued = host_seconds();
+    }
     ORBX_CUDA(cudaStreamSynchronize(c->stream));
   }
-  {
-    int err = 0;
-    ORBX_CUDA(cudaMemcpy(&err, c->d_err, sizeof(int), cudaMemcpyDeviceToHost));
-    if (err) {
-      ORBX_CUDA(cudaMemset(c->d_err, 0, sizeof(int)));
-      return ORBX_ERR_TIMEOUT;
-    }
-  }
+  if (prof) prof->t_synced = host_seconds();
+  if (reinterpret_cast<const int*>(res)[2]) return ORBX_ERR_TIMEOUT;  // a bounded wait gave up
   const int na = reinterpret_cast<const int*>(res)[0], nb = reinterpret_cast<const int*>(res)[1];
   *h_n_a = na;
   *h_n_b = nb;
@@ -1244,6 +1264,35 @@ ORBX_API int orbx_pair_host(orbx_ctx* c, const uint8_t* h_img_a, const uint8_t* 
   if (h_desc_a) std::memcpy(h_desc_a, desc, (size_t)32 * na);
   if (h_desc_b) std::memcpy(h_desc_b, desc + mp * 32, (size_t)32 * nb);
   return ORBX_OK;
+}
+
+ORBX_API int orbx_pair_host(orbx_ctx* c, const uint8_t* h_img_a, const uint8_t* h_img_b, int w, int h, int pitch,
+                            orbx_point* h_pts_a, int* h_n_a, orbx_point* h_pts_b, int* h_n_b, uint8_t* h_desc_a,
+                            uint8_t* h_desc_b, int mode) {
+  return pair_host_impl(c, h_img_a, h_img_b, w, h, pitch, h_pts_a, h_n_a, h_pts_b, h_n_b, h_desc_a, h_desc_b, mode,
+                        nullptr);
+}
+
+ORBX_API int orbx_profile_pair_host(orbx_ctx* c, const uint8_t* h_img_a, const uint8_t* h_img_b, int w, int h,
+                                    int pitch, orbx_point* h_pts_a, int* h_n_a, orbx_point* h_pts_b, int* h_n_b,
+                                    uint8_t* h_desc_a, uint8_t* h_desc_b, int mode, float* phase_ms) {
+  if (!c || !phase_ms) return ORBX_ERR_ARG;
+  DeviceGuard g(c->device);
+  PairHostProf prof;
+  for (auto& e : prof.ev) ORBX_CUDA(cudaEventCreate(&e));
+  const double t0 = host_seconds();
+  const int rc = pair_host_impl(c, h_img_a, h_img_b, w, h, pitch, h_pts_a, h_n_a, h_pts_b, h_n_b, h_desc_a, h_desc_b,
+                                mode, &prof);
+  const double t1 = host_seconds();
+  if (rc == ORBX_OK) {
+    for (int i = 0; i < 3; i++) cudaEventElapsedTime(&phase_ms[i], prof.ev[0], prof.ev[i + 1]);
+    phase_ms[3] = (float)(1e3 * (prof.t_enqueued - t0));
+    phase_ms[4] = (float)(1e3 * (prof.t_synced - prof.t_enqueued));
+    phase_ms[5] = (float)(1e3 * (t1 - prof.t_synced));
+    phase_ms[6] = (float)(1e3 * (t1 - t0));
+  }
+  for (auto& e : prof.ev) cudaEventDestroy(e);
+  return rc;
 }
 
 ORBX_API int orbx_profile_pair(orbx_ctx* c, const uint8_t* d_img_a, const uint8_t* d_img_b, int w, int h, int pitch,

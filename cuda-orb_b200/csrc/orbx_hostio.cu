@@ -47,13 +47,19 @@ void hostio_free(HostIO* io) {
   delete io;
 }
 
-// Result block of a pair in mapped host memory: counts (16 bytes), then the
+// Result block of a pair in mapped host memory: a 16-byte header (counts of
+// A and B, then the context's error word, which is cleared here), then the
 // keypoints of A and B (max_pts each), then optionally the descriptors.
 __global__ void k_export_pair(const orbx_point* __restrict__ pa, const orbx_point* __restrict__ pb,
                               const uint8_t* __restrict__ da, const uint8_t* __restrict__ db,
-                              const int* __restrict__ count, int max_pts, int with_desc, uint8_t* __restrict__ out) {
+                              const int* __restrict__ count, int max_pts, int with_desc, int* err,
+                              uint8_t* __restrict__ out) {
   const int na = min(count[0], max_pts), nb = min(count[1], max_pts);
   if (blockIdx.x == 0 && threadIdx.x < 2) reinterpret_cast<int*>(out)[threadIdx.x] = threadIdx.x ? nb : na;
+  if (blockIdx.x == 0 && threadIdx.x == 2) {
+    reinterpret_cast<int*>(out)[2] = *err;
+    *err = 0;
+  }
   const size_t pts_words = (size_t)max_pts * 7;  // one image's keypoint block, in 32-bit words
   int* o = reinterpret_cast<int*>(out + 16);
   const long long wa = (long long)na * 7, wb = (long long)nb * 7;
@@ -103,7 +109,7 @@ int hostio_export_pair(orbx_ctx* c, const orbx_point* pa, const orbx_point* pb, 
   const int rc = hostio_map(c, max_pts, host, &dev);
   if (rc) return rc;
   k_export_pair<<<2 * 148, 256, 0, ctx_stream(c)>>>(pa, pb, da, db, d_count, max_pts, with_desc ? 1 : 0,
-                                                     const_cast<uint8_t*>(dev));
+                                                     ctx_err(c), const_cast<uint8_t*>(dev));
   if (cudaGetLastError() != cudaSuccess) return ORBX_ERR_CUDA;
   return ORBX_OK;
 }

@@ -326,6 +326,24 @@ class Context:
         _check(lib().orbx_pair_host(self.h, hp(a), hp(b), w, h, pitch, hp(pts_a), hp(n_a), hp(pts_b), hp(n_b),
                                     hp(desc_a), hp(desc_b), mode), "orbx_pair_host")
 
+    def profile_pair_host(self, a, b, w, h, pitch, pts_a, n_a, pts_b, n_b, desc_a=None, desc_b=None,
+                          mode=MATCH_POPC):
+        """orbx_pair_host with phase times: dict of ms (events: upload, kernels, export
+        ends from the start; host: enqueue, wait, copy-out, wall)."""
+        def hp(x):
+            if x is None or isinstance(x, int):
+                return x
+            if hasattr(x, "ctypes"):
+                return x.ctypes.data
+            return x.data_ptr()
+        ms = np.zeros(7, dtype=np.float32)
+        _check(lib().orbx_profile_pair_host(self.h, hp(a), hp(b), w, h, pitch, hp(pts_a), hp(n_a), hp(pts_b),
+                                            hp(n_b), hp(desc_a), hp(desc_b), mode,
+                                            ms.ctypes.data_as(ctypes.c_void_p)), "orbx_profile_pair_host")
+        keys = ("upload_end", "kernels_end", "export_end", "host_enqueue", "host_wait", "host_copy_out",
+                "host_wall")
+        return {k: float(v) for k, v in zip(keys, ms)}
+
     def profile_pair(self, d_a, d_b, w, h, pitch, pa, da, na, pb, db, nb, mode=MATCH_POPC):
         ms = np.zeros(5, dtype=np.float32)
         _check(lib().orbx_profile_pair(self.h, _ptr(d_a), _ptr(d_b), w, h, pitch, _ptr(pa), _ptr(da), _ptr(na),

@@ -144,6 +144,16 @@ ORBX_API int orbx_pair_host(orbx_ctx* ctx, const uint8_t* h_img_a, const uint8_t
                             orbx_point* h_pts_a, int* h_n_a, orbx_point* h_pts_b, int* h_n_b, uint8_t* h_desc_a,
                             uint8_t* h_desc_b, int mode);
 
+/* orbx_pair_host with its phases timed (no counterpart in the reference):
+ * phase_ms[0..2] = CUDA-event times from the start to the end of the image
+ * uploads, of the kernels and of the export kernel (with overlapped uploads
+ * the kernels and the export are one launch sequence, so [1] = [2]);
+ * phase_ms[3..6] = host times of enqueueing everything, of the wait for the
+ * stream, of the copy-out, and of the whole call. */
+ORBX_API int orbx_profile_pair_host(orbx_ctx* ctx, const uint8_t* h_img_a, const uint8_t* h_img_b, int w, int h,
+                                    int pitch, orbx_point* h_pts_a, int* h_n_a, orbx_point* h_pts_b, int* h_n_b,
+                                    uint8_t* h_desc_a, uint8_t* h_desc_b, int mode, float* phase_ms);
+
 /* Host I/O.  orbx_upload_image copies a host image with any row pitch h_pitch
  * >= w (pinned or pageable memory) into a device image with row pitch d_pitch
  * >= w (the reference's layout is d_pitch = align_up(w, 128)), with zero

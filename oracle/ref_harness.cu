@@ -49,11 +49,6 @@ __global__ void gConv2dUnroll(unsigned char* src, unsigned char* dst, int width,
 static const size_t kGuard = 256 * 1024;
 static std::mutex g_alloc_mu;
 static std::unordered_map<void*, void*> g_alloc_base;
-// Zero-filling every allocation (guards included) makes parity runs
-// deterministic; timing runs switch it off (ref_set_zero_fill(0)) so that each
-// detectAndCompute's descriptor cudaMalloc (orb.cpp:84-90) costs what it costs
-// in the stock reference.  The guards stay allocated either way.
-static bool g_zero_fill = true;
 
 extern "C" cudaError_t __real_cudaMalloc(void** p, size_t n);
 extern "C" cudaError_t __real_cudaFree(void* p);
@@ -62,10 +57,8 @@ extern "C" cudaError_t __wrap_cudaMalloc(void** p, size_t n) {
   void* base = nullptr;
   cudaError_t e = __real_cudaMalloc(&base, n + 2 * kGuard);
   if (e != cudaSuccess) return e;
-  if (g_zero_fill) {
-    e = cudaMemset(base, 0, n + 2 * kGuard);
-    if (e != cudaSuccess) return e;
-  }
+  e = cudaMemset(base, 0, n + 2 * kGuard);
+  if (e != cudaSuccess) return e;
   *p = (char*)base + kGuard;
   std::lock_guard<std::mutex> lk(g_alloc_mu);
   g_alloc_base[*p] = base;
@@ -312,8 +305,6 @@ int ref_hmatch(const unsigned char* h_d1, int n1, const unsigned char* h_d2, int
 // device: detectAndCompute(A), detectAndCompute(B), match(A, B) -- the demo's
 // protocol (main.cpp:231-251) applied to one pair per step.  Returns the mean
 // milliseconds per pair measured with CUDA events around the timed loop.
-void ref_set_zero_fill(int on) { g_zero_fill = on != 0; }
-
 int ref_time_pair(const unsigned char* hA, const unsigned char* hB, int w, int h, int warmup, int iters,
                   float* ms_per_pair, int* n_a, int* n_b) {
   if (!g_orb) return -1;
@@ -349,75 +340,6 @@ int ref_time_pair(const unsigned char* hA, const unsigned char* hB, int w, int h
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   return 0;
-}
-
-// The batched workload run the reference's way, one pair at a time: for each
-// pair, Orbor::init with that pair's keypoint cap (orb.cpp:32-54), then
-// Orbor::detectAndCompute on A and B (orb.cpp:57-101, which rebuilds its
-// pyramid buffers whenever the size changes, orb.cpp:60-64) and Orbor::match
-// (orb.cpp:104-113).  Images are uploaded once, before timing.  The other
-// settings are those of the last ref_init call.
-int ref_time_batch(int n_pairs, const unsigned char* const* h_a, const unsigned char* const* h_b, const int* ws,
-                   const int* hs, const int* caps, int warmup, int iters, float* ms_per_batch, int* total_pts) {
-  if (!g_orb || n_pairs <= 0) return -1;
-  const int keep_max = g_orb->max_pts;
-  int cap_max = 1;
-  for (int i = 0; i < n_pairs; i++) cap_max = caps[i] > cap_max ? caps[i] : cap_max;
-  std::vector<unsigned char*> da(n_pairs, nullptr), db(n_pairs, nullptr);
-  orb::OrbData ra{}, rb{};
-  g_orb->initOrbData(ra, cap_max, true, true);
-  g_orb->initOrbData(rb, cap_max, true, true);
-  unsigned char* desc_a = nullptr;
-  unsigned char* desc_b = nullptr;
-  int rc = 0;
-  for (int i = 0; i < n_pairs && !rc; i++) {
-    const size_t bytes = (size_t)hs[i] * iAlignUp(ws[i], 128);
-    if (cudaMalloc((void**)&da[i], bytes) != cudaSuccess || cudaMalloc((void**)&db[i], bytes) != cudaSuccess ||
-        cudaMemcpy(da[i], h_a[i], bytes, cudaMemcpyHostToDevice) != cudaSuccess ||
-        cudaMemcpy(db[i], h_b[i], bytes, cudaMemcpyHostToDevice) != cudaSuccess)
-      rc = -2;
-  }
-  auto one_batch = [&](int* pts) {
-    int n = 0;
-    for (int i = 0; i < n_pairs; i++) {
-      g_orb->init(g_orb->noctaves, g_orb->edge_threshold, g_orb->wta_k, g_orb->score_type, g_orb->patch_size,
-                  g_orb->fast_threshold, g_orb->retain_topn, caps[i]);
-      const int3 whp = make_int3(ws[i], hs[i], iAlignUp(ws[i], 128));
-      g_orb->detectAndCompute(da[i], ra, whp, (void**)&desc_a, true);
-      g_orb->detectAndCompute(db[i], rb, whp, (void**)&desc_b, true);
-      g_orb->match(ra, rb, desc_a, desc_b);
-      n += ra.num_pts + rb.num_pts;
-    }
-    if (pts) *pts = n;
-  };
-  if (!rc) {
-    for (int k = 0; k < warmup; k++) one_batch(nullptr);
-    cudaEvent_t e0, e1;
-    cudaEventCreate(&e0);
-    cudaEventCreate(&e1);
-    cudaDeviceSynchronize();
-    cudaEventRecord(e0, 0);
-    for (int k = 0; k < iters; k++) one_batch(total_pts);
-    cudaEventRecord(e1, 0);
-    cudaEventSynchronize(e1);
-    float ms = 0.f;
-    cudaEventElapsedTime(&ms, e0, e1);
-    *ms_per_batch = ms / (float)(iters > 0 ? iters : 1);
-    cudaEventDestroy(e0);
-    cudaEventDestroy(e1);
-    if (cudaGetLastError() != cudaSuccess) rc = -3;
-  }
-  for (int i = 0; i < n_pairs; i++) {
-    if (da[i]) cudaFree(da[i]);
-    if (db[i]) cudaFree(db[i]);
-  }
-  if (desc_a) cudaFree(desc_a);
-  if (desc_b) cudaFree(desc_b);
-  g_orb->freeOrbData(ra);
-  g_orb->freeOrbData(rb);
-  g_orb->init(g_orb->noctaves, g_orb->edge_threshold, g_orb->wta_k, g_orb->score_type, g_orb->patch_size,
-              g_orb->fast_threshold, g_orb->retain_topn, keep_max);
-  return rc;
 }
 
 // Time hMatch alone on (n1 x n2) descriptor sets resident on the device.

@@ -147,11 +147,6 @@ def hmatch(d1, d2):
     return m[:n1], d[:n1]
 
 
-def set_zero_fill(on):
-    """Zero-fill of the reference's allocations (on for parity runs, off for timing)."""
-    lib().ref_set_zero_fill(int(bool(on)))
-
-
 def time_pair(a, b, w, h, warmup, iters):
     ms = ctypes.c_float(0)
     na = ctypes.c_int(0)
@@ -159,24 +154,6 @@ def time_pair(a, b, w, h, warmup, iters):
     _check(lib().ref_time_pair(_p(np.ascontiguousarray(a)), _p(np.ascontiguousarray(b)), w, h, warmup, iters,
                                ctypes.byref(ms), ctypes.byref(na), ctypes.byref(nb)), "ref_time_pair")
     return ms.value, na.value, nb.value
-
-
-def time_batch(pairs, warmup, iters):
-    """pairs: (img_a, img_b, w, h, cap) with uint8 (h, align_up(w, 128)) images.
-    The reference run pair by pair (Orbor::init with the pair's cap,
-    detectAndCompute A and B, match); returns (ms per batch, keypoints)."""
-    n = len(pairs)
-    keep = [(np.ascontiguousarray(a), np.ascontiguousarray(b)) for a, b, _, _, _ in pairs]
-    pa = (ctypes.c_void_p * n)(*[k[0].ctypes.data for k in keep])
-    pb = (ctypes.c_void_p * n)(*[k[1].ctypes.data for k in keep])
-    ws = np.array([p[2] for p in pairs], dtype=np.int32)
-    hs = np.array([p[3] for p in pairs], dtype=np.int32)
-    caps = np.array([p[4] for p in pairs], dtype=np.int32)
-    ms = ctypes.c_float(0)
-    pts = ctypes.c_int(0)
-    _check(lib().ref_time_batch(n, pa, pb, _p(ws), _p(hs), _p(caps), warmup, iters, ctypes.byref(ms),
-                                ctypes.byref(pts)), "ref_time_batch")
-    return ms.value, pts.value
 
 
 def time_hmatch(d1, d2, warmup, iters):
