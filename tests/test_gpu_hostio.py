@@ -145,3 +145,29 @@ def test_pair_host_overlapped_upload_equals_device_pair(w, h, seed, bands):
         assert np.array_equal(hda[:len(pa)], da) and np.array_equal(hdb[:len(pb)], db)
     ctx.close()
     ref.close()
+
+
+@pytest.mark.parametrize("bands", [0, 4])
+def test_profile_pair_host_phases(bands):
+    """orbx_profile_pair_host returns the same results as orbx_pair_host and
+    phase times in order: uploads end before the kernels, the kernels before
+    the export, and the host wall time covers the device span."""
+    w, h = 1920, 1080
+    a, b, _ = synth.make_pair(w, h, seed=46)
+    pitch = a.shape[1]
+    ctx = orbx.Context(0, orbx.make_params(max_pts=10000))
+    t = ctx.get_tuning()
+    t.upload_bands = bands
+    ctx.set_tuning(t)
+    ha, hb = torch.from_numpy(a).pin_memory(), torch.from_numpy(b).pin_memory()
+    hpa, hpb = np.zeros((10000, 7), np.int32), np.zeros((10000, 7), np.int32)
+    hna, hnb = np.zeros(1, np.int32), np.zeros(1, np.int32)
+    ctx.pair_host(ha.data_ptr(), hb.data_ptr(), w, h, pitch, hpa, hna, hpb, hnb)
+    want = (hpa[:int(hna[0])].copy(), hpb[:int(hnb[0])].copy())
+    for _ in range(3):
+        ph = ctx.profile_pair_host(ha.data_ptr(), hb.data_ptr(), w, h, pitch, hpa, hna, hpb, hnb)
+        assert np.array_equal(hpa[:int(hna[0])], want[0]) and np.array_equal(hpb[:int(hnb[0])], want[1])
+        assert 0 < ph["upload_end"] <= ph["kernels_end"] + 1e-3 <= ph["export_end"] + 2e-3
+        assert ph["host_wall"] >= ph["export_end"] * 0.9
+        assert min(ph[k] for k in ("host_enqueue", "host_wait", "host_copy_out")) >= 0
+    ctx.close()
