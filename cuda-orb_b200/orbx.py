@@ -89,6 +89,7 @@ def lib():
         L.orbx_pair.argtypes = [vp, vp, vp, i32, i32, i32, vp, vp, vp, vp, vp, vp, i32]
         L.orbx_debug_buffers.argtypes = [vp, vp, vp, vp, vp, vp]
         L.orbx_pair_host.argtypes = [vp, vp, vp, i32, i32, i32, vp, vp, vp, vp, vp, vp, i32]
+        L.orbx_profile_pair_host.argtypes = [vp, vp, vp, i32, i32, i32, vp, vp, vp, vp, vp, vp, i32, vp]
         L.orbx_profile_pair.argtypes = [vp, vp, vp, i32, i32, i32, vp, vp, vp, vp, vp, vp, i32, vp]
         L.orbx_get_tuning.argtypes = [vp, ctypes.POINTER(Tuning)]
         L.orbx_set_tuning.argtypes = [vp, ctypes.POINTER(Tuning)]

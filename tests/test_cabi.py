@@ -93,3 +93,13 @@ def test_create_without_gpu_fails_cleanly():
     with pytest.raises(orbx.OrbxError) as e:
         orbx.Context(0)
     assert e.value.status == 2
+
+
+def test_every_binding_call_has_argtypes():
+    """Each C entry point the Python binding calls declares its argument types:
+    without them ctypes passes Python ints as 32-bit C ints, truncating pointers."""
+    src = open(os.path.join(os.path.dirname(__file__), "..", "cuda-orb_b200", "orbx.py")).read()
+    called = set(re.findall(r"lib\(\)\.(orbx_\w+)\(", src)) | set(re.findall(r"\bL\.(orbx_\w+)\(", src))
+    typed = set(re.findall(r"L\.(orbx_\w+)\.argtypes", src))
+    no_args = {"orbx_version"}  # takes no arguments
+    assert called - typed - no_args == set()
