@@ -432,9 +432,10 @@ def run_orbx(args, world, rank, local):
     # one persistent launch with a device work queue
     pair_forms = {}
     keep_t = ctx.get_tuning()
-    for name, form in (("five_launch", 0), ("persistent", 1)):
+    for name, form, rows in (("five_launch", 0, 0), ("persistent", 1, 0), ("persistent_row_deps", 1, 1)):
         t = ctx.get_tuning()
         t.pair_form = form
+        t.persist_row_deps = rows
         ctx.set_tuning(t)
         f_ms = []
         with torch.cuda.stream(stream):
@@ -465,12 +466,13 @@ def run_orbx(args, world, rank, local):
     hnb = np.zeros(1, dtype=np.int32)
     e2e_steps = min(args.steps, 300)
 
-    def e2e_run(bands, steps):
+    def e2e_run(bands, steps, rows=0):
         """CUDA-event and host wall times of orbx_pair_host with the given upload banding."""
         t = ctx.get_tuning()
-        keep = t.upload_bands
+        keep = (t.upload_bands, t.persist_row_deps)
         if bands is not None:
             t.upload_bands = bands
+            t.persist_row_deps = rows
             ctx.set_tuning(t)
         with torch.cuda.stream(stream):
             for _ in range(3):
@@ -490,7 +492,7 @@ def run_orbx(args, world, rank, local):
                 ev_ms.append(ev0.elapsed_time(ev1))
             barrier(world)
         if bands is not None:
-            t.upload_bands = keep
+            t.upload_bands, t.persist_row_deps = keep
             ctx.set_tuning(t)
         return ev_ms, wall_ms
 
@@ -498,13 +500,15 @@ def run_orbx(args, world, rank, local):
     e_ms, e_wall = e2e_run(None, e2e_steps)
     e2e_total = max_over_ranks(sum(e_ms), world)
     e2e_variants = {}
-    for bands in (0, 2, 4, 8):
-        v_ev, v_wall = e2e_run(bands, min(e2e_steps, 50))
-        e2e_variants[str(bands)] = {"ms": statistics.median(v_ev), "host_wall_ms": statistics.median(v_wall)}
+    for bands, rows in ((0, 0), (2, 0), (4, 0), (8, 0), (2, 1), (4, 1)):
+        name = f"{bands}" + ("_row_deps" if rows else "")
+        v_ev, v_wall = e2e_run(bands, min(e2e_steps, 50), rows)
+        e2e_variants[name] = {"ms": statistics.median(v_ev), "host_wall_ms": statistics.median(v_wall)}
         # where the time goes: CUDA events between the phases and host clocks
         t = ctx.get_tuning()
-        keep_b = t.upload_bands
+        keep_b = (t.upload_bands, t.persist_row_deps)
         t.upload_bands = bands
+        t.persist_row_deps = rows
         ctx.set_tuning(t)
         phases = []
         with torch.cuda.stream(stream):
@@ -512,9 +516,9 @@ def run_orbx(args, world, rank, local):
                 flush.zero_()
                 stream.synchronize()
                 phases.append(ctx.profile_pair_host(ha.data_ptr(), hb.data_ptr(), W, H, pitch, hpa, hna, hpb, hnb))
-        t.upload_bands = keep_b
+        t.upload_bands, t.persist_row_deps = keep_b
         ctx.set_tuning(t)
-        e2e_variants[str(bands)]["phases_ms"] = {k: statistics.median(p[k] for p in phases) for k in phases[0]}
+        e2e_variants[name]["phases_ms"] = {k: statistics.median(p[k] for p in phases) for k in phases[0]}
     h2d = 2 * H * pitch
     d2h = 8 + (int(hna[0]) + int(hnb[0])) * 28
 

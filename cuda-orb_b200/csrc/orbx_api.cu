@@ -61,7 +61,9 @@ struct PersistBufs {
   int* desc_base = nullptr;  // [frames + 1]
   int* done = nullptr;       // [4 * frames + 1 + frames]: stage counters, item counter, upload flags
   MatchJob* jobs = nullptr;
-  size_t runs_cap = 0, frames_cap = 0, jobs_cap = 0;
+  PersistRows* rows = nullptr;  // [frames] row-counter offsets (row-level dependencies)
+  size_t runs_cap = 0, frames_cap = 0, jobs_cap = 0, done_cap = 0;
+  size_t done_ints = 0;       // counters to clear before each launch
   std::vector<uint8_t> last;  // content of the last upload
 };
 
@@ -71,6 +73,7 @@ static void persist_free(PersistBufs& pb) {
   cudaFree(pb.desc_base);
   cudaFree(pb.done);
   cudaFree(pb.jobs);
+  cudaFree(pb.rows);
   pb = PersistBufs();
 }
 
@@ -148,6 +151,7 @@ struct orbx_ctx {
   int upload_bands = 0;  // orbx_pair_host: 0 = copy then run; 1..16 = bands overlapped with the persistent launch
   int pair_form = 0;     // orbx_pair: 0 = five graph-replayed launches, 1 = one persistent launch
   int pyr_shape = 0;     // pyramid tile shape of the five-launch forms (kPyrShapeTW/TH)
+  int row_deps = 0;      // persistent launches: detect waits per pyramid tile row, not per frame
   PairGraph ppg;         // orbx_pair's persistent graph
   int memops = -1;       // stream write-value support: -1 unknown, 0 no, 1 yes
   // device-side waits
@@ -946,9 +950,10 @@ static int pair_persistent(orbx_ctx* c, const LaunchPlan& pl, const std::vector<
   PersistArgs a;
   int grid = 0;
   if ((rc = persist_prepare(c, c->ppair, pl, frames, jobs, 2 * 148, 0, &a, &grid)) != 0) return rc;
-  std::vector<uint8_t> key(sizeof(PersistArgs) + sizeof(int));
+  std::vector<uint8_t> key(sizeof(PersistArgs) + sizeof(int) + sizeof(size_t));
   std::memcpy(key.data(), &a, sizeof(PersistArgs));
   std::memcpy(key.data() + sizeof(PersistArgs), &grid, sizeof(int));
+  std::memcpy(key.data() + sizeof(PersistArgs) + sizeof(int), &c->ppair.done_ints, sizeof(size_t));
   if (!(pg.valid && pg.key == key)) {
     if (pg.exec) {
       cudaGraphExecDestroy(pg.exec);
@@ -957,7 +962,7 @@ static int pair_persistent(orbx_ctx* c, const LaunchPlan& pl, const std::vector<
     pg.valid = false;
     cudaGraph_t graph = nullptr;
     ORBX_CUDA(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
-    cudaError_t le = cudaMemsetAsync(a.done, 0, sizeof(int) * (4 * 2 + 1), c->stream);
+    cudaError_t le = cudaMemsetAsync(a.done, 0, sizeof(int) * c->ppair.done_ints, c->stream);
     if (le == cudaSuccess) le = launch_batch_persistent(a, grid, c->stream);
     const cudaError_t ce = cudaStreamEndCapture(c->stream, &graph);
     if (le != cudaSuccess) {
@@ -1123,9 +1128,9 @@ static int pair_host_overlap(orbx_ctx* c, const uint8_t* h_a, const uint8_t* h_b
   a.band_rows = band_rows;
   const uint8_t* map_dev = nullptr;
   if ((rc = hostio_map(c, c->p.max_pts, res, &map_dev)) != 0) return rc;
-  std::vector<uint8_t> key(sizeof(PersistArgs) + 3 * sizeof(int) + sizeof(void*));
+  std::vector<uint8_t> key(sizeof(PersistArgs) + 4 * sizeof(int) + sizeof(void*));
   std::memcpy(key.data(), &a, sizeof(PersistArgs));
-  const int extra[3] = {grid, c->p.max_pts, with_desc ? 1 : 0};
+  const int extra[4] = {grid, c->p.max_pts, with_desc ? 1 : 0, (int)c->ppair.done_ints};
   std::memcpy(key.data() + sizeof(PersistArgs), extra, sizeof(extra));
   std::memcpy(key.data() + sizeof(PersistArgs) + sizeof(extra), &map_dev, sizeof(void*));
   if (!(pg.valid && pg.key == key)) {
@@ -1154,7 +1159,7 @@ static int pair_host_overlap(orbx_ctx* c, const uint8_t* h_a, const uint8_t* h_b
     pg.valid = true;
   }
   // reset the counters and flags, start the launch, then feed it the bands
-  ORBX_CUDA(cudaMemsetAsync(a.done, 0, sizeof(int) * (5 * 2 + 1), c->stream));
+  ORBX_CUDA(cudaMemsetAsync(a.done, 0, sizeof(int) * c->ppair.done_ints, c->stream));
   ORBX_CUDA(cudaEventRecord(c->ev_reset, c->stream));
   ORBX_CUDA(cudaGraphLaunch(pg.exec, c->stream));
   ORBX_CUDA(cudaStreamWaitEvent(c->copy_stream, c->ev_reset, 0));
@@ -1351,6 +1356,7 @@ ORBX_API int orbx_get_tuning(orbx_ctx* c, orbx_tuning* t) {
   t->upload_bands = c->upload_bands;
   t->pair_form = c->pair_form;
   t->pyr_tile = c->pyr_shape;
+  t->persist_row_deps = c->row_deps;
   return ORBX_OK;
 }
 
@@ -1362,7 +1368,7 @@ ORBX_API int orbx_set_tuning(orbx_ctx* c, const orbx_tuning* t) {
       t->persist_group < 0 || t->persist_group > kMaxFramesPerLaunch || t->persist_blocks_per_sm < 0 ||
       t->persist_blocks_per_sm > 32 || t->wait_timeout_us < 1 || t->wait_timeout_us > 10000000 ||
       t->upload_bands < 0 || t->upload_bands > 16 || t->pair_form < 0 || t->pair_form > 1 ||
-      t->pyr_tile < 0 || t->pyr_tile >= kPyrShapes)
+      t->pyr_tile < 0 || t->pyr_tile >= kPyrShapes || t->persist_row_deps < 0 || t->persist_row_deps > 1)
     return ORBX_ERR_ARG;
   c->nms_rows = t->nms_rows;
   c->describe_bps = t->describe_blocks_per_sm;
@@ -1375,6 +1381,7 @@ ORBX_API int orbx_set_tuning(orbx_ctx* c, const orbx_tuning* t) {
   c->upload_bands = t->upload_bands;
   c->pair_form = t->pair_form;
   c->pyr_shape = t->pyr_tile;
+  c->row_deps = t->persist_row_deps;
   c->wait_cycles = (long long)c->wait_us * c->clock_khz / 1000;
   if (c->batch_exec) {
     cudaGraphExecDestroy(c->batch_exec);
@@ -1416,8 +1423,15 @@ static int persist_prepare(orbx_ctx* c, PersistBufs& pb, const LaunchPlan& pl, c
   }
   std::vector<PersistRun> runs;
   std::vector<int> run_base;
-  build_persist_runs(nf, group > 0 ? group : nf, pyr_n.data(), det_n.data(), nms_n.data(), desc_n.data(),
-                     blocks_per_pair, &runs, &run_base);
+  std::vector<PersistRows> rows;
+  int n_rows = 0;
+  if (c->row_deps)
+    n_rows = build_persist_runs_rows(frames, desc_n.data(), blocks_per_pair, &runs, &run_base, &rows);
+  else
+    build_persist_runs(nf, group > 0 ? group : nf, pyr_n.data(), det_n.data(), nms_n.data(), desc_n.data(),
+                       blocks_per_pair, &runs, &run_base);
+  // counters: [4 x frames] stage counters, the item counter, [frames] upload flags, row counters
+  const size_t done_ints = 5 * (size_t)nf + 1 + (size_t)n_rows;
   const int bps_max = persist_blocks_per_sm(c->p.wta_k);
   if (bps_max <= 0) return ORBX_ERR_CUDA;
   const int bps = c->persist_bps > 0 ? std::min(c->persist_bps, bps_max) : bps_max;
@@ -1425,9 +1439,13 @@ static int persist_prepare(orbx_ctx* c, PersistBufs& pb, const LaunchPlan& pl, c
   ORBX_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, c->device));
   *grid_out = bps * nsm;
   std::vector<uint8_t> blob(sizeof(PersistRun) * runs.size() + sizeof(int) * (run_base.size() + nf + 1) +
-                            sizeof(MatchJob) * n_pairs);
+                            sizeof(MatchJob) * n_pairs + sizeof(PersistRows) * rows.size() + sizeof(size_t));
   {
     uint8_t* q = blob.data();
+    std::memcpy(q, &done_ints, sizeof(size_t));
+    q += sizeof(size_t);
+    if (!rows.empty()) std::memcpy(q, rows.data(), sizeof(PersistRows) * rows.size());
+    q += sizeof(PersistRows) * rows.size();
     std::memcpy(q, runs.data(), sizeof(PersistRun) * runs.size());
     q += sizeof(PersistRun) * runs.size();
     std::memcpy(q, run_base.data(), sizeof(int) * run_base.size());
@@ -1450,14 +1468,23 @@ static int persist_prepare(orbx_ctx* c, PersistBufs& pb, const LaunchPlan& pl, c
     }
     if (pb.frames_cap < (size_t)nf) {
       cudaFree(pb.desc_base);
-      cudaFree(pb.done);
+      cudaFree(pb.rows);
       pb.desc_base = nullptr;
-      pb.done = nullptr;
+      pb.rows = nullptr;
       pb.frames_cap = 0;
       ORBX_CUDA(cudaMalloc(&pb.desc_base, sizeof(int) * (nf + 1)));
-      ORBX_CUDA(cudaMalloc(&pb.done, sizeof(int) * (5 * (size_t)nf + 1)));
+      ORBX_CUDA(cudaMalloc(&pb.rows, sizeof(PersistRows) * nf));
       pb.frames_cap = nf;
     }
+    if (pb.done_cap < done_ints) {
+      cudaFree(pb.done);
+      pb.done = nullptr;
+      pb.done_cap = 0;
+      ORBX_CUDA(cudaMalloc(&pb.done, sizeof(int) * done_ints));
+      pb.done_cap = done_ints;
+    }
+    if (!rows.empty())
+      ORBX_CUDA(cudaMemcpy(pb.rows, rows.data(), sizeof(PersistRows) * nf, cudaMemcpyHostToDevice));
     if (pb.jobs_cap < (size_t)n_pairs) {
       cudaFree(pb.jobs);
       pb.jobs = nullptr;
@@ -1483,6 +1510,11 @@ static int persist_prepare(orbx_ctx* c, PersistBufs& pb, const LaunchPlan& pl, c
   a.item_counter = reinterpret_cast<unsigned int*>(pb.done + 4 * (size_t)nf);
   a.jobs = pb.jobs;
   a.blocks_per_job = blocks_per_pair;
+  if (n_rows > 0) {
+    a.rows = pb.rows;
+    a.rows_done = pb.done + 5 * (size_t)nf + 1;
+  }
+  pb.done_ints = done_ints;
   return ORBX_OK;
 }
 
@@ -1496,7 +1528,7 @@ static int batch_persistent(orbx_ctx* c, const LaunchPlan& pl, const std::vector
   int rc = persist_prepare(c, c->pbatch, pl, frames, jobs, blocks_per_pair, c->persist_group, &a, &grid);
   if (rc) return rc;
   {
-    const int extra[4] = {1, c->persist_group, grid, a.n_runs};
+    const int extra[4] = {1, c->persist_group, grid, (int)c->pbatch.done_ints};
     const size_t k0 = key.size();
     key.resize(k0 + sizeof(extra) + sizeof(void*));
     std::memcpy(key.data() + k0, extra, sizeof(extra));
@@ -1509,7 +1541,7 @@ static int batch_persistent(orbx_ctx* c, const LaunchPlan& pl, const std::vector
     }
     cudaGraph_t graph = nullptr;
     ORBX_CUDA(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
-    cudaError_t le = cudaMemsetAsync(a.done, 0, sizeof(int) * (4 * (size_t)nf + 1), c->stream);
+    cudaError_t le = cudaMemsetAsync(a.done, 0, sizeof(int) * c->pbatch.done_ints, c->stream);
     if (le == cudaSuccess) le = launch_batch_persistent(a, grid, c->stream);
     const cudaError_t ce = cudaStreamEndCapture(c->stream, &graph);
     if (le != cudaSuccess) {
@@ -1742,7 +1774,12 @@ ORBX_API int orbx_autotune_pairs_forms(orbx_ctx* c, int n_pairs, const orbx_imag
           t.match_blocks_per_pair = m;
           t.persist_group = gsz;
           t.persist_blocks_per_sm = bps;
+          t.persist_row_deps = 0;
           cands.push_back(t);
+          if (gsz == 0) {  // row-level dependencies order items by row, not in waves
+            t.persist_row_deps = 1;
+            cands.push_back(t);
+          }
         }
   orbx_tuning top = keep;
   float top_ms = 1e30f;

@@ -45,32 +45,66 @@ union PersistSmem {
 
 constexpr int kPersistThreads = 256;
 
-// Thread 0 waits until *ctr >= need (acquire), bounded by wait_cycles; the
-// block then proceeds together.  After one wait has given up, later waits
-// return at once so the launch drains.
-__device__ __forceinline__ void stage_wait(const int* ctr, int need, int* err, long long wait_cycles) {
-  if (threadIdx.x == 0) {
-    const long long t0 = clock64();
-    for (;;) {
-      int v;
-      asm volatile("ld.acquire.gpu.global.s32 %0, [%1];" : "=r"(v) : "l"(ctr) : "memory");
-      if (v >= need) break;
-      if (*(volatile int*)err & kErrStageTimeout) break;
-      if (clock64() - t0 > wait_cycles) {
-        atomicOr(err, kErrStageTimeout);
-        break;
-      }
-      __nanosleep(64);
+// One thread waits until *ctr >= need (acquire), bounded by wait_cycles.
+// After one wait has given up, later waits return at once so the launch drains.
+__device__ __forceinline__ void wait_counter(const int* ctr, int need, int* err, long long wait_cycles) {
+  const long long t0 = clock64();
+  for (;;) {
+    int v;
+    asm volatile("ld.acquire.gpu.global.s32 %0, [%1];" : "=r"(v) : "l"(ctr) : "memory");
+    if (v >= need) break;
+    if (*(volatile int*)err & kErrStageTimeout) break;
+    if (clock64() - t0 > wait_cycles) {
+      atomicOr(err, kErrStageTimeout);
+      break;
     }
+    __nanosleep(64);
   }
+}
+
+// Thread 0 waits; the block then proceeds together.
+__device__ __forceinline__ void stage_wait(const int* ctr, int need, int* err, long long wait_cycles) {
+  if (threadIdx.x == 0) wait_counter(ctr, need, err, wait_cycles);
   __syncthreads();
 }
 
-__device__ __forceinline__ void stage_done(int* ctr) {
+__device__ __forceinline__ void stage_done(int* ctr, int* ctr2 = nullptr) {
   __syncthreads();  // every thread's stores of this item precede the release
   if (threadIdx.x == 0) {
     __threadfence();
     atomicAdd(ctr, 1);
+    if (ctr2) atomicAdd(ctr2, 1);
+  }
+}
+
+// Octave and tile row of pyramid tile `local` of frame F.
+__device__ __forceinline__ void pyr_tile_pos(const Frame& F, int local, int* o_out, int* row_out) {
+  int o = 0;
+  while (o + 1 < F.n_oct && local >= F.pyr_tile_base[o + 1]) o++;
+  *o_out = o;
+  *row_out = (local - F.pyr_tile_base[o]) / F.pyr_tiles_x[o];
+}
+
+// Thread 0: waits for every pyramid tile row that detect tile row `ty` reads.
+// At octave o the tile stages rows (32 ty >> o) - 4 .. ((32 ty + 31) >> o) + 4
+// with the linear addressing of the pyramid, so one more row on each side (a
+// column past the edge is the neighbouring row), and rows outside the octave
+// are the last rows of octave o - 1 or the first rows of octave o + 1 (the
+// guard before octave 0 and after the last octave needs nothing).
+__device__ __forceinline__ void wait_detect_row_deps(const Frame& F, const PersistRows& R, const int* rows_done,
+                                                     int ty, int* err, long long wait_cycles) {
+  for (int o = 0; o < F.n_oct; o++) {
+    const int r_lo = ((kDetTH * ty) >> o) - 4 - 1;
+    const int r_hi = ((kDetTH * ty + kDetTH - 1) >> o) + 4 + 1;
+    const int lo = max(r_lo, 0), hi = min(r_hi, F.oh[o] - 1);
+    for (int t = lo / kPyrTH; lo <= hi && t <= hi / kPyrTH; t++)
+      wait_counter(rows_done + R.pyr[o] + t, F.pyr_tiles_x[o], err, wait_cycles);
+    if (r_lo < 0 && o > 0)
+      for (int t = max(0, F.pyr_tiles_y[o - 1] - 2); t < F.pyr_tiles_y[o - 1]; t++)
+        wait_counter(rows_done + R.pyr[o - 1] + t, F.pyr_tiles_x[o - 1], err, wait_cycles);
+    if (r_hi >= F.oh[o] && o + 1 < F.n_oct)
+      for (int t = 0; t < min(2, F.pyr_tiles_y[o + 1]); t++)
+        wait_counter(rows_done + R.pyr[o + 1] + t, F.pyr_tiles_x[o + 1], err, wait_cycles);
   }
 }
 
@@ -113,12 +147,12 @@ __global__ void __launch_bounds__(kPersistThreads, 3) k_batch_persistent(Persist
     if (t >= total) break;
     const int r = find_run(p.run_base, p.n_runs, t);
     const PersistRun run = p.runs[r];
-    const int local = t - __ldg(p.run_base + r);
+    const int local = run.first + (t - __ldg(p.run_base + r));
     const int f = run.frame;
     int* done = p.done;
     const int nf = b.n_frames;
     switch (run.stage) {
-      case kStagePyr:
+      case kStagePyr: {
         if (p.upload_flags) {
           const int rows = pyr_tile_rows(b.frames[f], local);
           stage_wait(p.upload_flags + f, (rows + p.band_rows - 1) / p.band_rows, b.err, b.wait_cycles);
@@ -126,19 +160,41 @@ __global__ void __launch_bounds__(kPersistThreads, 3) k_batch_persistent(Persist
         } else {
           pyr_tile<false>(b, __ldg(b.pyr_base + f) + local, sm.pyr);
         }
-        stage_done(done + 0 * nf + f);
+        int* row_ctr = nullptr;
+        if (p.rows) {
+          int o, tr;
+          pyr_tile_pos(b.frames[f], local, &o, &tr);
+          row_ctr = p.rows_done + p.rows[f].pyr[o] + tr;
+        }
+        stage_done(done + 0 * nf + f, row_ctr);
         break;
-      case kStageDet:
-        stage_wait(done + 0 * nf + f, __ldg(b.pyr_base + f + 1) - __ldg(b.pyr_base + f), b.err, b.wait_cycles);
+      }
+      case kStageDet: {
+        const Frame& F = b.frames[f];
+        const int ty = local / F.det_tiles_x;
+        if (p.rows) {
+          if (threadIdx.x == 0) wait_detect_row_deps(F, p.rows[f], p.rows_done, ty, b.err, b.wait_cycles);
+          __syncthreads();
+        } else {
+          stage_wait(done + 0 * nf + f, __ldg(b.pyr_base + f + 1) - __ldg(b.pyr_base + f), b.err, b.wait_cycles);
+        }
         det_tile<true>(b, __ldg(b.det_base + f) + local, sm.det);
-        stage_done(done + 1 * nf + f);
+        stage_done(done + 1 * nf + f, p.rows ? p.rows_done + p.rows[f].det + ty : nullptr);
         break;
+      }
       case kStageNms:
+        // per frame in both modes: the strips' look-back needs them to start in
+        // order, and the top strips read detect rows that wait for the bottom
+        // of the octave before (the window's row -1 is that octave's last row)
         stage_wait(done + 1 * nf + f, __ldg(b.det_base + f + 1) - __ldg(b.det_base + f), b.err, b.wait_cycles);
         nms_strip<true>(b, __ldg(b.nms_base + f) + local, sm.nms);
         stage_done(done + 2 * nf + f);
         break;
       case kStageDesc: {
+        // with row-level dependencies, NMS completion does not imply every
+        // pyramid tile: the patches may read rows no NMS strip waited for
+        if (p.rows && threadIdx.x == 0)
+          wait_counter(done + 0 * nf + f, __ldg(b.pyr_base + f + 1) - __ldg(b.pyr_base + f), b.err, b.wait_cycles);
         stage_wait(done + 2 * nf + f, __ldg(b.nms_base + f + 1) - __ldg(b.nms_base + f), b.err, b.wait_cycles);
         if (threadIdx.x < b.half_k + 1) sm.desc.umax[threadIdx.x] = __ldg(b.umax + threadIdx.x);
         __syncthreads();
@@ -220,7 +276,7 @@ void build_persist_runs(int nf, int group, const int* pyr_n, const int* det_n, c
   int acc = 0;
   auto add = [&](int stage, int frame, int count) {
     if (count <= 0) return;
-    runs->push_back(PersistRun{stage, frame});
+    runs->push_back(PersistRun{stage, frame, 0});
     run_base->push_back(acc);
     acc += count;
   };
@@ -242,6 +298,83 @@ void build_persist_runs(int nf, int group, const int* pyr_n, const int* det_n, c
     }
   }
   run_base->push_back(acc);
+}
+
+// Host side: the run table with row-level dependencies.  Each item gets the
+// level-0 row from which it can run (a pyramid tile row its start row, a
+// detect tile row the largest of its pyramid dependencies' keys, the NMS
+// strips of a frame the largest key of its detect rows); items sort by (key,
+// stage, frame, index), which puts every item after its dependencies and the
+// NMS strips of a frame in order.  Consecutive items of one stage and frame
+// form a run.
+int build_persist_runs_rows(const std::vector<Frame>& frames, const int* desc_n, int match_per_pair,
+                            std::vector<PersistRun>* runs, std::vector<int>* run_base,
+                            std::vector<PersistRows>* rows) {
+  struct Item {
+    long long key;
+    int stage, frame, local;
+  };
+  const int nf = (int)frames.size();
+  std::vector<Item> items;
+  rows->assign(nf, PersistRows{});
+  int n_rows = 0;
+  const long long kEnd = 1ll << 40;
+  for (int f = 0; f < nf; f++) {
+    const Frame& F = frames[f];
+    PersistRows& R = (*rows)[f];
+    std::vector<std::vector<long long>> pkey(F.n_oct);
+    for (int o = 0; o < F.n_oct; o++) {
+      R.pyr[o] = n_rows;
+      n_rows += F.pyr_tiles_y[o];
+      pkey[o].resize(F.pyr_tiles_y[o]);
+      for (int t = 0; t < F.pyr_tiles_y[o]; t++) {
+        pkey[o][t] = (long long)(kPyrTH * t) << o;
+        for (int x = 0; x < F.pyr_tiles_x[o]; x++)
+          items.push_back({pkey[o][t], kStagePyr, f, F.pyr_tile_base[o] + t * F.pyr_tiles_x[o] + x});
+      }
+    }
+    R.det = n_rows;
+    n_rows += F.det_tiles_y;
+    std::vector<long long> dkey(F.det_tiles_y, 0);
+    for (int ty = 0; ty < F.det_tiles_y; ty++) {
+      long long k = 0;
+      for (int o = 0; o < F.n_oct; o++) {  // the same rows as wait_detect_row_deps
+        const int r_lo = ((kDetTH * ty) >> o) - 4 - 1;
+        const int r_hi = ((kDetTH * ty + kDetTH - 1) >> o) + 4 + 1;
+        const int lo = std::max(r_lo, 0), hi = std::min(r_hi, F.oh[o] - 1);
+        for (int t = lo / kPyrTH; lo <= hi && t <= hi / kPyrTH; t++) k = std::max(k, pkey[o][t]);
+        if (r_lo < 0 && o > 0) k = std::max(k, pkey[o - 1][F.pyr_tiles_y[o - 1] - 1]);
+        if (r_hi >= F.oh[o] && o + 1 < F.n_oct) k = std::max(k, pkey[o + 1][std::min(1, F.pyr_tiles_y[o + 1] - 1)]);
+      }
+      dkey[ty] = k;
+      for (int x = 0; x < F.det_tiles_x; x++) items.push_back({k, kStageDet, f, ty * F.det_tiles_x + x});
+    }
+    long long nkey = 0;  // NMS strips wait for every detect tile of the frame
+    for (long long k : dkey) nkey = std::max(nkey, k);
+    for (int st = 0; st < F.nms_strips; st++) items.push_back({nkey, kStageNms, f, st});
+    for (int d = 0; d < desc_n[f]; d++) items.push_back({kEnd, kStageDesc, f, d});
+    if ((f & 1) == 0)
+      for (int m = 0; m < match_per_pair; m++) items.push_back({kEnd, kStageMatch, f, m});
+  }
+  std::stable_sort(items.begin(), items.end(), [](const Item& a, const Item& b) {
+    if (a.key != b.key) return a.key < b.key;
+    if (a.stage != b.stage) return a.stage < b.stage;
+    if (a.frame != b.frame) return a.frame < b.frame;
+    return a.local < b.local;
+  });
+  runs->clear();
+  run_base->clear();
+  for (size_t i = 0; i < items.size(); i++) {
+    const Item& it = items[i];
+    const bool extend = !runs->empty() && runs->back().stage == it.stage && runs->back().frame == it.frame &&
+                        runs->back().first + (int)(i - (size_t)run_base->back()) == it.local;
+    if (!extend) {
+      runs->push_back(PersistRun{it.stage, it.frame, it.local});
+      run_base->push_back((int)i);
+    }
+  }
+  run_base->push_back((int)items.size());
+  return n_rows;
 }
 
 }  // namespace orbx

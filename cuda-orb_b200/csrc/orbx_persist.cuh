@@ -13,6 +13,15 @@ enum : int { kStagePyr = 0, kStageDet = 1, kStageNms = 2, kStageDesc = 3, kStage
 struct PersistRun {
   int stage;
   int frame;
+  int first;  // local index (within the stage and frame) of the run's first ticket
+};
+
+// Row-level dependencies (optional): per frame, the offsets in rows_done of
+// its counters of finished pyramid tiles per (octave, tile row) and of
+// finished detect tiles per tile row.
+struct PersistRows {
+  int pyr[kMaxOctaves];
+  int det;
 };
 
 struct PersistArgs {
@@ -31,6 +40,11 @@ struct PersistArgs {
   // copy stream after each band), and pyramid tiles wait for the rows they read
   const int* upload_flags;
   int band_rows;
+  // optional: row-level dependencies.  A detect tile row then waits only for
+  // the pyramid tile rows it reads, so a frame's detection overlaps its
+  // pyramid row by row (NMS strips still wait for the whole frame).
+  const PersistRows* rows;  // [n_frames], null: per-frame dependencies only
+  int* rows_done;           // counters, zero at launch
 };
 
 // Level-0 pixels per describe slice: a frame's keypoints are split into
@@ -42,5 +56,11 @@ cudaError_t launch_batch_persistent(const PersistArgs& p, int blocks, cudaStream
 cudaError_t launch_wait_selftest(const int* ctr, int need, int* err, long long wait_cycles, cudaStream_t s);
 void build_persist_runs(int nf, int group, const int* pyr_n, const int* det_n, const int* nms_n, const int* desc_n,
                         int match_per_pair, std::vector<PersistRun>* runs, std::vector<int>* run_base);
+// The run table with row-level dependencies: items ordered by the level-0 row
+// from which they can run, stage and frame.  Fills the per-frame counter
+// offsets and returns the number of row counters.
+int build_persist_runs_rows(const std::vector<Frame>& frames, const int* desc_n, int match_per_pair,
+                            std::vector<PersistRun>* runs, std::vector<int>* run_base,
+                            std::vector<PersistRows>* rows);
 
 }  // namespace orbx

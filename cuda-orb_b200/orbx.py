@@ -54,7 +54,8 @@ class Tuning(ctypes.Structure):
                 ("match_blocks_per_sm", ctypes.c_int), ("match_blocks_per_pair", ctypes.c_int),
                 ("batch_form", ctypes.c_int), ("persist_group", ctypes.c_int),
                 ("persist_blocks_per_sm", ctypes.c_int), ("wait_timeout_us", ctypes.c_int),
-                ("upload_bands", ctypes.c_int), ("pair_form", ctypes.c_int), ("pyr_tile", ctypes.c_int)]
+                ("upload_bands", ctypes.c_int), ("pair_form", ctypes.c_int), ("pyr_tile", ctypes.c_int),
+                ("persist_row_deps", ctypes.c_int)]
 
     def as_dict(self):
         return {f: int(getattr(self, f)) for f, _ in self._fields_}

@@ -244,6 +244,8 @@ typedef struct orbx_tuning {
                                  (popcount matching) */
   int pyr_tile;               /* pyramid + blur tile of the five-launch forms: 0 = 128 x 32, 1 = 64 x 32,
                                  2 = 128 x 16, 3 = 64 x 64 octave pixels (the persistent forms use 128 x 32) */
+  int persist_row_deps;       /* persistent launches: 1 = a detect tile row waits only for the pyramid tile rows
+                                 it reads (a frame's stages overlap row by row), 0 = for the whole frame */
 } orbx_tuning;
 
 ORBX_API int orbx_get_tuning(orbx_ctx* ctx, orbx_tuning* t);

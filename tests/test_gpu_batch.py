@@ -92,19 +92,20 @@ def test_nms_strip_heights_agree(batch, rows):
     ctx.close()
 
 
-def _set_form(ctx, form, group=0, bps=0):
+def _set_form(ctx, form, group=0, bps=0, rows=0):
     t = ctx.get_tuning()
     t.batch_form = form
     t.persist_group = group
     t.persist_blocks_per_sm = bps
+    t.persist_row_deps = rows
     ctx.set_tuning(t)
 
 
-@pytest.mark.parametrize("group,bps", [(0, 0), (2, 1), (4, 0)])
-def test_persistent_batch_equals_single_pairs(batch, group, bps):
+@pytest.mark.parametrize("group,bps,rows", [(0, 0, 0), (2, 1, 0), (4, 0, 0), (0, 0, 1), (0, 1, 1)])
+def test_persistent_batch_equals_single_pairs(batch, group, bps, rows):
     ctx = orbx.Context(0, orbx.make_params(max_pts=10000))
     single = orbx.Context(0, orbx.make_params(max_pts=10000))
-    _set_form(ctx, 1, group, bps)
+    _set_form(ctx, 1, group, bps, rows)
     pb = orbx.PairBatch(batch)
     for _ in range(3):  # capture, then replays (counters and strip words reset each time)
         ctx.batch_pairs(pb)
@@ -214,14 +215,17 @@ def test_wait_timeout_tuning_is_validated():
     ctx.close()
 
 
+@pytest.mark.parametrize("rows", [0, 1])
 @pytest.mark.parametrize("w,h,seed,cap", [(1920, 1080, 7, 10000), (333, 257, 8, 200), (3840, 2160, 9, 10000)])
-def test_pair_persistent_form_equals_five_launches(w, h, seed, cap):
-    """orbx_pair as one persistent launch gives exactly the five-launch results."""
+def test_pair_persistent_form_equals_five_launches(w, h, seed, cap, rows):
+    """orbx_pair as one persistent launch (per-frame or row-level stage
+    dependencies) gives exactly the five-launch results."""
     a, b, _ = synth.make_pair(w, h, seed=seed)
     five = orbx.Context(0, orbx.make_params(max_pts=cap))
     pers = orbx.Context(0, orbx.make_params(max_pts=cap))
     t = pers.get_tuning()
     t.pair_form = 1
+    t.persist_row_deps = rows
     pers.set_tuning(t)
     want = _single(five, a, b, w, h, cap)
     for _ in range(3):

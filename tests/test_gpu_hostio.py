@@ -112,9 +112,9 @@ def test_pair_host_equals_device_pair(ctx, with_desc):
             assert np.array_equal(hda[:len(pa)], da) and np.array_equal(hdb[:len(pb)], db)
 
 
-@pytest.mark.parametrize("bands", [1, 4, 7, 16])
+@pytest.mark.parametrize("bands,rows", [(1, 0), (4, 0), (7, 0), (16, 0), (4, 1), (16, 1)])
 @pytest.mark.parametrize("w,h,seed", [(1920, 1080, 44), (333, 257, 45)])
-def test_pair_host_overlapped_upload_equals_device_pair(w, h, seed, bands):
+def test_pair_host_overlapped_upload_equals_device_pair(w, h, seed, bands, rows):
     """orbx_pair_host with the images copied in row bands on a second stream,
     while one persistent launch processes the bands that have arrived: the same
     results as orbx_pair on device-resident images, on repeated calls."""
@@ -130,6 +130,7 @@ def test_pair_host_overlapped_upload_equals_device_pair(w, h, seed, bands):
     ctx = orbx.Context(0, orbx.make_params(max_pts=10000))
     t = ctx.get_tuning()
     t.upload_bands = bands
+    t.persist_row_deps = rows
     ctx.set_tuning(t)
     ha, hb = torch.from_numpy(a).pin_memory(), torch.from_numpy(b).pin_memory()
     for _ in range(3):
