@@ -56,20 +56,18 @@ struct PairGraph {
 // Device tables of one persistent launch (orbx_persist.cu), reused while
 // their content is unchanged.
 struct PersistBufs {
-  PersistRun* runs = nullptr;
-  int* run_base = nullptr;   // [runs + 1]
+  unsigned long long* items = nullptr;  // [tickets] packed work items in claim order
   int* desc_base = nullptr;  // [frames + 1]
   int* done = nullptr;       // [4 * frames + 1 + frames]: stage counters, item counter, upload flags
   MatchJob* jobs = nullptr;
   PersistRows* rows = nullptr;  // [frames] row-counter offsets (row-level dependencies)
-  size_t runs_cap = 0, frames_cap = 0, jobs_cap = 0, done_cap = 0;
+  size_t items_cap = 0, frames_cap = 0, jobs_cap = 0, done_cap = 0;
   size_t done_ints = 0;       // counters to clear before each launch
   std::vector<uint8_t> last;  // content of the last upload
 };
 
 static void persist_free(PersistBufs& pb) {
-  cudaFree(pb.runs);
-  cudaFree(pb.run_base);
+  cudaFree(pb.items);
   cudaFree(pb.desc_base);
   cudaFree(pb.done);
   cudaFree(pb.jobs);
@@ -1432,13 +1430,18 @@ static int persist_prepare(orbx_ctx* c, PersistBufs& pb, const LaunchPlan& pl, c
                        blocks_per_pair, &runs, &run_base);
   // counters: [4 x frames] stage counters, the item counter, [frames] upload flags, row counters
   const size_t done_ints = 5 * (size_t)nf + 1 + (size_t)n_rows;
+  // one packed item per ticket: a claim decodes its item with one load
+  std::vector<unsigned long long> items((size_t)run_base.back());
+  for (size_t r = 0; r < runs.size(); r++)
+    for (int t = run_base[r]; t < run_base[r + 1]; t++)
+      items[t] = persist_item(runs[r].stage, runs[r].frame, runs[r].first + (t - run_base[r]));
   const int bps_max = persist_blocks_per_sm(c->p.wta_k);
   if (bps_max <= 0) return ORBX_ERR_CUDA;
   const int bps = c->persist_bps > 0 ? std::min(c->persist_bps, bps_max) : bps_max;
   int nsm = 0;
   ORBX_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, c->device));
   *grid_out = bps * nsm;
-  std::vector<uint8_t> blob(sizeof(PersistRun) * runs.size() + sizeof(int) * (run_base.size() + nf + 1) +
+  std::vector<uint8_t> blob(sizeof(unsigned long long) * items.size() + sizeof(int) * (nf + 1) +
                             sizeof(MatchJob) * n_pairs + sizeof(PersistRows) * rows.size() + sizeof(size_t));
   {
     uint8_t* q = blob.data();
@@ -1446,25 +1449,20 @@ static int persist_prepare(orbx_ctx* c, PersistBufs& pb, const LaunchPlan& pl, c
     q += sizeof(size_t);
     if (!rows.empty()) std::memcpy(q, rows.data(), sizeof(PersistRows) * rows.size());
     q += sizeof(PersistRows) * rows.size();
-    std::memcpy(q, runs.data(), sizeof(PersistRun) * runs.size());
-    q += sizeof(PersistRun) * runs.size();
-    std::memcpy(q, run_base.data(), sizeof(int) * run_base.size());
-    q += sizeof(int) * run_base.size();
+    std::memcpy(q, items.data(), sizeof(unsigned long long) * items.size());
+    q += sizeof(unsigned long long) * items.size();
     std::memcpy(q, desc_base.data(), sizeof(int) * (nf + 1));
     q += sizeof(int) * (nf + 1);
     std::memcpy(q, jobs.data(), sizeof(MatchJob) * n_pairs);
   }
   if (pb.last != blob) {
     ORBX_CUDA(cudaStreamSynchronize(c->stream));
-    if (pb.runs_cap < runs.size()) {
-      cudaFree(pb.runs);
-      cudaFree(pb.run_base);
-      pb.runs = nullptr;
-      pb.run_base = nullptr;
-      pb.runs_cap = 0;
-      ORBX_CUDA(cudaMalloc(&pb.runs, sizeof(PersistRun) * runs.size()));
-      ORBX_CUDA(cudaMalloc(&pb.run_base, sizeof(int) * (runs.size() + 1)));
-      pb.runs_cap = runs.size();
+    if (pb.items_cap < items.size()) {
+      cudaFree(pb.items);
+      pb.items = nullptr;
+      pb.items_cap = 0;
+      ORBX_CUDA(cudaMalloc(&pb.items, sizeof(unsigned long long) * items.size()));
+      pb.items_cap = items.size();
     }
     if (pb.frames_cap < (size_t)nf) {
       cudaFree(pb.desc_base);
@@ -1492,8 +1490,8 @@ static int persist_prepare(orbx_ctx* c, PersistBufs& pb, const LaunchPlan& pl, c
       ORBX_CUDA(cudaMalloc(&pb.jobs, sizeof(MatchJob) * n_pairs));
       pb.jobs_cap = n_pairs;
     }
-    ORBX_CUDA(cudaMemcpy(pb.runs, runs.data(), sizeof(PersistRun) * runs.size(), cudaMemcpyHostToDevice));
-    ORBX_CUDA(cudaMemcpy(pb.run_base, run_base.data(), sizeof(int) * run_base.size(), cudaMemcpyHostToDevice));
+    ORBX_CUDA(cudaMemcpy(pb.items, items.data(), sizeof(unsigned long long) * items.size(),
+                         cudaMemcpyHostToDevice));
     ORBX_CUDA(cudaMemcpy(pb.desc_base, desc_base.data(), sizeof(int) * (nf + 1), cudaMemcpyHostToDevice));
     ORBX_CUDA(cudaMemcpy(pb.jobs, jobs.data(), sizeof(MatchJob) * n_pairs, cudaMemcpyHostToDevice));
     pb.last.swap(blob);
@@ -1501,9 +1499,7 @@ static int persist_prepare(orbx_ctx* c, PersistBufs& pb, const LaunchPlan& pl, c
   PersistArgs& a = *out;
   a = PersistArgs{};
   a.b = pl.b;
-  a.runs = pb.runs;
-  a.run_base = pb.run_base;
-  a.n_runs = (int)runs.size();
+  a.items = pb.items;
   a.run_base_host_total = run_base.back();
   a.desc_base = pb.desc_base;
   a.done = pb.done;

@@ -119,18 +119,6 @@ __device__ __forceinline__ int pyr_tile_rows(const Frame& F, int local) {
   return (ylast << o) + 1;
 }
 
-// Run r covers tickets [run_base[r], run_base[r + 1]).
-__device__ __forceinline__ int find_run(const int* run_base, int n_runs, int t) {
-  int lo = 0, hi = n_runs - 1;
-  while (lo < hi) {
-    const int mid = (lo + hi + 1) >> 1;
-    if (__ldg(run_base + mid) <= t)
-      lo = mid;
-    else
-      hi = mid - 1;
-  }
-  return lo;
-}
 
 template <int WTA>
 __global__ void __launch_bounds__(kPersistThreads, 3) k_batch_persistent(PersistArgs p) {
@@ -139,19 +127,26 @@ __global__ void __launch_bounds__(kPersistThreads, 3) k_batch_persistent(Persist
   const Batch& b = p.b;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int total = p.run_base_host_total;
+  // Thread 0 claims the next ticket while the block works on the current one
+  // (its result is only stored at the end of the item), so the claim's
+  // latency overlaps the work.  A claimed ticket waits only for its own
+  // block's current item, which has a smaller ticket, so the smallest
+  // unfinished ticket still always runs.
+  if (threadIdx.x == 0) s_item = (int)atomicAdd(p.item_counter, 1u);
   for (;;) {
-    __syncthreads();  // the previous item is done with shared memory and s_item
-    if (threadIdx.x == 0) s_item = (int)atomicAdd(p.item_counter, 1u);
-    __syncthreads();
+    __syncthreads();  // the previous item is done with shared memory; s_item holds the ticket
     const int t = s_item;
+    __syncthreads();  // every thread has read it before thread 0 may overwrite it
     if (t >= total) break;
-    const int r = find_run(p.run_base, p.n_runs, t);
-    const PersistRun run = p.runs[r];
-    const int local = run.first + (t - __ldg(p.run_base + r));
-    const int f = run.frame;
+    int next = 0;
+    if (threadIdx.x == 0) next = (int)atomicAdd(p.item_counter, 1u);
+    const unsigned long long it = __ldg(p.items + t);
+    const int stage = (int)(it >> 56);
+    const int f = (int)((it >> 32) & 0xFFFFFFu);
+    const int local = (int)(unsigned)it;
     int* done = p.done;
     const int nf = b.n_frames;
-    switch (run.stage) {
+    switch (stage) {
       case kStagePyr: {
         if (p.upload_flags) {
           const int rows = pyr_tile_rows(b.frames[f], local);
@@ -223,6 +218,7 @@ __global__ void __launch_bounds__(kPersistThreads, 3) k_batch_persistent(Persist
         break;
       }
     }
+    if (threadIdx.x == 0) s_item = next;  // published to the block by the barrier at the loop's top
   }
 }
 

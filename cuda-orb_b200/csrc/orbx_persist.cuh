@@ -24,11 +24,14 @@ struct PersistRows {
   int det;
 };
 
+// One work item, packed: stage << 56 | frame << 32 | index within the stage and frame.
+__host__ __device__ inline unsigned long long persist_item(int stage, int frame, int local) {
+  return ((unsigned long long)stage << 56) | ((unsigned long long)frame << 32) | (unsigned)local;
+}
+
 struct PersistArgs {
   Batch b;
-  const PersistRun* runs;
-  const int* run_base;       // [n_runs + 1] first ticket of each run
-  int n_runs;
+  const unsigned long long* items;  // [total tickets] packed items in claim order
   int run_base_host_total;   // total tickets
   const int* desc_base;      // [n_frames + 1] prefix of describe slices per frame
   int* done;                 // [4][n_frames] completed items per (stage, frame); zero at launch
