@@ -1763,7 +1763,7 @@ ORBX_API int orbx_autotune_pairs_forms(orbx_ctx* c, int n_pairs, const orbx_imag
   for (int r : {4, 16})
     for (int m : {0, 64})
       for (int gsz : {0, 4, 16, 48})
-        for (int bps : {0, 2}) {
+        for (int bps : {0, 3}) {
           orbx_tuning t = keep;
           t.batch_form = 1;
           t.nms_rows = r;

@@ -121,7 +121,7 @@ __device__ __forceinline__ int pyr_tile_rows(const Frame& F, int local) {
 
 
 template <int WTA>
-__global__ void __launch_bounds__(kPersistThreads, 3) k_batch_persistent(PersistArgs p) {
+__global__ void __launch_bounds__(kPersistThreads, 4) k_batch_persistent(PersistArgs p) {
   __shared__ PersistSmem sm;
   __shared__ int s_item;
   const Batch& b = p.b;
