@@ -1416,7 +1416,7 @@ static int persist_prepare(orbx_ctx* c, PersistBufs& pb, const LaunchPlan& pl, c
     pyr_n[f] = F.pyr_tile_base[F.n_oct];
     det_n[f] = F.det_tiles_x * F.det_tiles_y;
     nms_n[f] = F.nms_strips;
-    desc_n[f] = std::max(1, div_up(F.w * F.h, kDescSlicePixels));
+    desc_n[f] = std::max(1, std::min(div_up(F.w * F.h, kDescSlicePixels), div_up(F.max_pts, 8)));
     desc_base[f + 1] = desc_base[f] + desc_n[f];
   }
   std::vector<PersistRun> runs;

@@ -57,14 +57,18 @@ __device__ __forceinline__ void g_mbar_init(uint32_t bar, uint32_t count) {
 __device__ __forceinline__ void g_mbar_expect_tx(uint32_t bar, uint32_t bytes) {
   asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
 }
+// A waiting thread is suspended by the barrier unit (woken when the phase
+// completes, or after this many nanoseconds) instead of spinning on the
+// ALU pipe that the epilogue warps need.
+constexpr uint32_t kTryWaitSuspendNs = 20000;
 __device__ __forceinline__ bool g_mbar_try(uint32_t bar, uint32_t parity) {
   uint32_t ok;
   asm volatile(
       "{\n\t.reg .pred p;\n\t"
-      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
       "selp.u32 %0, 1, 0, p;\n\t}"
       : "=r"(ok)
-      : "r"(bar), "r"(parity)
+      : "r"(bar), "r"(parity), "r"(kTryWaitSuspendNs)
       : "memory");
   return ok != 0;
 }

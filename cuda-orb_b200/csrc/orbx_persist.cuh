@@ -51,8 +51,9 @@ struct PersistArgs {
 };
 
 // Level-0 pixels per describe slice: a frame's keypoints are split into
-// ceil(w * h / kDescSlicePixels) slices.
-constexpr int kDescSlicePixels = 65536;
+// ceil(w * h / kDescSlicePixels) slices (at most one per 8 keypoints of its
+// cap), about one keypoint per warp at the synthetic images' density.
+constexpr int kDescSlicePixels = 8192;
 
 int persist_blocks_per_sm(int wta_k);
 cudaError_t launch_batch_persistent(const PersistArgs& p, int blocks, cudaStream_t s);
