@@ -469,13 +469,14 @@ def run_orbx(args, world, rank, local):
     hnb = np.zeros(1, dtype=np.int32)
     e2e_steps = min(max(args.steps, 200), 300)  # host-side noise: at least 200 samples
 
-    def e2e_run(bands, steps, rows=0):
-        """CUDA-event and host wall times of orbx_pair_host with the given upload banding."""
+    def e2e_run(bands, steps, rows=0, streams=0):
+        """CUDA-event and host wall times of orbx_pair_host with the given upload overlap."""
         t = ctx.get_tuning()
-        keep = (t.upload_bands, t.persist_row_deps)
+        keep = (t.upload_bands, t.persist_row_deps, t.host_overlap)
         if bands is not None:
             t.upload_bands = bands
             t.persist_row_deps = rows
+            t.host_overlap = streams
             ctx.set_tuning(t)
         with torch.cuda.stream(stream):
             for _ in range(3):
@@ -495,23 +496,26 @@ def run_orbx(args, world, rank, local):
                 ev_ms.append(ev0.elapsed_time(ev1))
             barrier(world)
         if bands is not None:
-            t.upload_bands, t.persist_row_deps = keep
+            t.upload_bands, t.persist_row_deps, t.host_overlap = keep
             ctx.set_tuning(t)
         return ev_ms, wall_ms
 
-    ctx_tuning_bands = int(ctx.get_tuning().upload_bands)
+    _t = ctx.get_tuning()
+    ctx_overlap = {"upload_bands": int(_t.upload_bands), "host_overlap": int(_t.host_overlap)}
     e_ms, e_wall = e2e_run(None, e2e_steps)
     e2e_total = max_over_ranks(sum(e_ms), world)
     e2e_variants = {}
-    for bands, rows in (() if args.no_e2e_variants else ((0, 0), (2, 0), (4, 0), (8, 0), (2, 1), (4, 1))):
-        name = f"{bands}" + ("_row_deps" if rows else "")
-        v_ev, v_wall = e2e_run(bands, min(e2e_steps, 50), rows)
+    variants = ((0, 0, 0), (0, 0, 1), (2, 0, 0), (4, 0, 0), (8, 0, 0), (4, 1, 0))
+    for bands, rows, streams in (() if args.no_e2e_variants else variants):
+        name = ("two_streams" if streams else f"bands_{bands}") + ("_row_deps" if rows else "")
+        v_ev, v_wall = e2e_run(bands, min(e2e_steps, 50), rows, streams)
         e2e_variants[name] = {"ms": statistics.median(v_ev), "host_wall_ms": statistics.median(v_wall)}
         # where the time goes: CUDA events between the phases and host clocks
         t = ctx.get_tuning()
-        keep_b = (t.upload_bands, t.persist_row_deps)
+        keep_b = (t.upload_bands, t.persist_row_deps, t.host_overlap)
         t.upload_bands = bands
         t.persist_row_deps = rows
+        t.host_overlap = streams
         ctx.set_tuning(t)
         phases = []
         with torch.cuda.stream(stream):
@@ -519,7 +523,7 @@ def run_orbx(args, world, rank, local):
                 flush.zero_()
                 stream.synchronize()
                 phases.append(ctx.profile_pair_host(ha.data_ptr(), hb.data_ptr(), W, H, pitch, hpa, hna, hpb, hnb))
-        t.upload_bands, t.persist_row_deps = keep_b
+        t.upload_bands, t.persist_row_deps, t.host_overlap = keep_b
         ctx.set_tuning(t)
         e2e_variants[name]["phases_ms"] = {k: statistics.median(p[k] for p in phases) for k in phases[0]}
     h2d = 2 * H * pitch
@@ -581,9 +585,9 @@ def run_orbx(args, world, rank, local):
             "e2e": {"value": e2e_total / (e2e_steps * world), "unit": "ms", "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h, "median_ms": statistics.median(e_ms), "steps": e2e_steps,
                     "host_wall_ms_median": statistics.median(e_wall),
-                    "upload_bands": ctx_tuning_bands,
+                    "overlap": ctx_overlap,
                     "how": "orbx_pair_host: pinned host images in, host keypoints/matches out, CUDA events",
-                    "by_upload_bands": e2e_variants},
+                    "variants": e2e_variants},
             "gpu_launches": 5 * args.steps,
             "roofline": roofline,
             "kernels": kernels,

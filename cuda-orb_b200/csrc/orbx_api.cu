@@ -150,6 +150,10 @@ struct orbx_ctx {
   int pair_form = 0;     // orbx_pair: 0 = five graph-replayed launches, 1 = one persistent launch
   int pyr_shape = 0;     // pyramid tile shape of the five-launch forms (kPyrShapeTW/TH)
   int row_deps = 0;      // persistent launches: detect waits per pyramid tile row, not per frame
+  int host_overlap = 0;  // orbx_pair_host: 1 = image B uploads while frame A's kernels run (two streams)
+  BatchSlot pair_b;      // frame B's tables for host_overlap
+  MatchWork hmw{};       // its matcher scratch
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   PairGraph ppg;         // orbx_pair's persistent graph
   int memops = -1;       // stream write-value support: -1 unknown, 0 no, 1 yes
   // device-side waits
@@ -480,11 +484,12 @@ static int upload_batch(orbx_ctx* c, BatchSlot& bs, const std::vector<Frame>& fr
   return ORBX_OK;
 }
 
-static int launch_frames(orbx_ctx* c, const LaunchPlan& pl, bool compute_desc) {
-  ORBX_CUDA(launch_pyramid_blur(pl.b, pl.pyr_tiles, c->stream));
-  ORBX_CUDA(launch_detect(pl.b, pl.det_tiles, c->stream));
-  ORBX_CUDA(launch_nms(pl.b, pl.nms_strips, c->stream));
-  if (compute_desc) ORBX_CUDA(launch_describe(pl.b, pl.total_max_pts, c->stream, c->describe_bps));
+static int launch_frames(orbx_ctx* c, const LaunchPlan& pl, bool compute_desc, cudaStream_t s = nullptr) {
+  if (!s) s = c->stream;
+  ORBX_CUDA(launch_pyramid_blur(pl.b, pl.pyr_tiles, s));
+  ORBX_CUDA(launch_detect(pl.b, pl.det_tiles, s));
+  ORBX_CUDA(launch_nms(pl.b, pl.nms_strips, s));
+  if (compute_desc) ORBX_CUDA(launch_describe(pl.b, pl.total_max_pts, s, c->describe_bps));
   return ORBX_OK;
 }
 
@@ -727,6 +732,15 @@ ORBX_API int orbx_destroy(orbx_ctx* c) {
   cudaFree(c->pho.mw.part);
   cudaFree(c->pho.mw.tile_done);
   if (c->copy_stream) cudaStreamDestroy(c->copy_stream);
+  if (c->ev_fork) cudaEventDestroy(c->ev_fork);
+  if (c->ev_join) cudaEventDestroy(c->ev_join);
+  cudaFree(c->hmw.part);
+  cudaFree(c->hmw.tile_done);
+  cudaFree(c->pair_b.d_frames);
+  cudaFree(c->pair_b.d_bases);
+  cudaFree(c->pair_b.d_ticket);
+  cudaFreeHost(c->pair_b.h_stage);
+  if (c->pair_b.uploaded) cudaEventDestroy(c->pair_b.uploaded);
   if (c->ev_reset) cudaEventDestroy(c->ev_reset);
   cudaFree(c->d_pattern);
   cudaFree(c->d_umax);
@@ -1176,6 +1190,50 @@ static int pair_host_overlap(orbx_ctx* c, const uint8_t* h_a, const uint8_t* h_b
   return ORBX_OK;
 }
 
+// orbx_pair_host with the two frames on two streams: image A is copied and
+// processed on the context's stream while image B is copied, then processed,
+// on the copy stream; matching and the export follow on the context's stream
+// once both are done.  The same five kernels per frame as orbx_pair.
+static int pair_host_streams(orbx_ctx* c, const uint8_t* h_a, const uint8_t* h_b, int w, int h, int pitch,
+                             bool with_desc, const uint8_t** res, cudaEvent_t ev_uploaded = nullptr) {
+  int rc;
+  if ((rc = ws_ensure(c, c->ws[0], w, h)) != 0) return rc;
+  if ((rc = ws_ensure(c, c->ws[1], w, h)) != 0) return rc;
+  if (!c->copy_stream) ORBX_CUDA(cudaStreamCreateWithFlags(&c->copy_stream, cudaStreamNonBlocking));
+  if (!c->ev_fork) ORBX_CUDA(cudaEventCreateWithFlags(&c->ev_fork, cudaEventDisableTiming));
+  if (!c->ev_join) ORBX_CUDA(cudaEventCreateWithFlags(&c->ev_join, cudaEventDisableTiming));
+  std::vector<Frame> fa(1), fb(1);
+  fill_frame(c, c->ws[0], c->io_img[0], pitch, c->io_pts[0], c->io_desc[0], c->io_count, fa[0], -1, c->pyr_shape);
+  fill_frame(c, c->ws[1], c->io_img[1], pitch, c->io_pts[1], c->io_desc[1], c->io_count + 1, fb[0], -1,
+             c->pyr_shape);
+  LaunchPlan pa, pb;
+  if ((rc = upload_batch(c, c->pair, fa, &pa)) != 0) return rc;
+  if ((rc = upload_batch(c, c->pair_b, fb, &pb)) != 0) return rc;
+  if ((rc = mw_ensure(c->hmw, c->p.max_pts)) != 0) return rc;
+  const size_t ibytes = (size_t)h * pitch;
+  // fork: the copy stream starts after everything queued before this call
+  ORBX_CUDA(cudaEventRecord(c->ev_fork, c->stream));
+  ORBX_CUDA(cudaStreamWaitEvent(c->copy_stream, c->ev_fork, 0));
+  ORBX_CUDA(cudaMemcpyAsync(c->io_img[0], h_a, ibytes, cudaMemcpyHostToDevice, c->stream));
+  ORBX_CUDA(cudaMemcpyAsync(c->io_img[1], h_b, ibytes, cudaMemcpyHostToDevice, c->copy_stream));
+  if (ev_uploaded) ORBX_CUDA(cudaEventRecord(ev_uploaded, c->copy_stream));
+  if ((rc = launch_frames(c, pa, true, c->stream)) != 0) return rc;
+  if ((rc = launch_frames(c, pb, true, c->copy_stream)) != 0) return rc;
+  ORBX_CUDA(cudaEventRecord(c->ev_join, c->copy_stream));
+  ORBX_CUDA(cudaStreamWaitEvent(c->stream, c->ev_join, 0));
+  MatchArgs m{};
+  m.q = c->io_desc[0];
+  m.db = c->io_desc[1];
+  m.nq = c->p.max_pts;
+  m.ndb = c->p.max_pts;
+  m.d_nq = c->io_count;
+  m.d_ndb = c->io_count + 1;
+  m.pts = c->io_pts[0];
+  ORBX_CUDA(launch_match_popc(m, c->hmw, c->stream, c->match_bps));
+  return hostio_export_pair(c, c->io_pts[0], c->io_pts[1], c->io_desc[0], c->io_desc[1], c->io_count,
+                            c->p.max_pts, with_desc, res);
+}
+
 // orbx_pair_host; with `prof`, CUDA events and host clocks between the phases.
 struct PairHostProf {
   cudaEvent_t ev[4];  // start, uploads done, kernels done, export done
@@ -1218,7 +1276,20 @@ static int pair_host_impl(orbx_ctx* c, const uint8_t* h_img_a, const uint8_t* h_
   const uint8_t* res = nullptr;
   const bool with_desc = h_desc_a || h_desc_b;
   if (prof) ORBX_CUDA(cudaEventRecord(prof->ev[0], c->stream));
-  if (c->upload_bands > 0 && mode != ORBX_MATCH_IMMA && memops_ok(c)) {
+  if (c->host_overlap == 1 && c->upload_bands == 0 && mode != ORBX_MATCH_IMMA) {
+    rc = pair_host_streams(c, h_img_a, h_img_b, w, h, pitch, with_desc, &res, prof ? prof->ev[1] : nullptr);
+    if (rc) {
+      cudaStreamSynchronize(c->copy_stream);
+      cudaStreamSynchronize(c->stream);
+      return rc;
+    }
+    if (prof) {
+      ORBX_CUDA(cudaEventRecord(prof->ev[2], c->stream));
+      ORBX_CUDA(cudaEventRecord(prof->ev[3], c->stream));
+      prof->t_enqueued = host_seconds();
+    }
+    ORBX_CUDA(cudaStreamSynchronize(c->stream));
+  } else if (c->upload_bands > 0 && mode != ORBX_MATCH_IMMA && memops_ok(c)) {
     rc = pair_host_overlap(c, h_img_a, h_img_b, w, h, pitch, with_desc, &res);
     if (rc) {
       cudaStreamSynchronize(c->copy_stream);
@@ -1355,6 +1426,7 @@ ORBX_API int orbx_get_tuning(orbx_ctx* c, orbx_tuning* t) {
   t->pair_form = c->pair_form;
   t->pyr_tile = c->pyr_shape;
   t->persist_row_deps = c->row_deps;
+  t->host_overlap = c->host_overlap;
   return ORBX_OK;
 }
 
@@ -1366,7 +1438,8 @@ ORBX_API int orbx_set_tuning(orbx_ctx* c, const orbx_tuning* t) {
       t->persist_group < 0 || t->persist_group > kMaxFramesPerLaunch || t->persist_blocks_per_sm < 0 ||
       t->persist_blocks_per_sm > 32 || t->wait_timeout_us < 1 || t->wait_timeout_us > 10000000 ||
       t->upload_bands < 0 || t->upload_bands > 16 || t->pair_form < 0 || t->pair_form > 1 ||
-      t->pyr_tile < 0 || t->pyr_tile >= kPyrShapes || t->persist_row_deps < 0 || t->persist_row_deps > 1)
+      t->pyr_tile < 0 || t->pyr_tile >= kPyrShapes || t->persist_row_deps < 0 || t->persist_row_deps > 1 ||
+      t->host_overlap < 0 || t->host_overlap > 1)
     return ORBX_ERR_ARG;
   c->nms_rows = t->nms_rows;
   c->describe_bps = t->describe_blocks_per_sm;
@@ -1380,6 +1453,7 @@ ORBX_API int orbx_set_tuning(orbx_ctx* c, const orbx_tuning* t) {
   c->pair_form = t->pair_form;
   c->pyr_shape = t->pyr_tile;
   c->row_deps = t->persist_row_deps;
+  c->host_overlap = t->host_overlap;
   c->wait_cycles = (long long)c->wait_us * c->clock_khz / 1000;
   if (c->batch_exec) {
     cudaGraphExecDestroy(c->batch_exec);

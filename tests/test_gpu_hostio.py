@@ -112,9 +112,10 @@ def test_pair_host_equals_device_pair(ctx, with_desc):
             assert np.array_equal(hda[:len(pa)], da) and np.array_equal(hdb[:len(pb)], db)
 
 
-@pytest.mark.parametrize("bands,rows", [(1, 0), (4, 0), (7, 0), (16, 0), (4, 1), (16, 1)])
+@pytest.mark.parametrize("bands,rows,streams", [(1, 0, 0), (4, 0, 0), (7, 0, 0), (16, 0, 0), (4, 1, 0), (16, 1, 0),
+                                                (0, 0, 1)])
 @pytest.mark.parametrize("w,h,seed", [(1920, 1080, 44), (333, 257, 45)])
-def test_pair_host_overlapped_upload_equals_device_pair(w, h, seed, bands, rows):
+def test_pair_host_overlapped_upload_equals_device_pair(w, h, seed, bands, rows, streams):
     """orbx_pair_host with the images copied in row bands on a second stream,
     while one persistent launch processes the bands that have arrived: the same
     results as orbx_pair on device-resident images, on repeated calls."""
@@ -131,6 +132,7 @@ def test_pair_host_overlapped_upload_equals_device_pair(w, h, seed, bands, rows)
     t = ctx.get_tuning()
     t.upload_bands = bands
     t.persist_row_deps = rows
+    t.host_overlap = streams
     ctx.set_tuning(t)
     ha, hb = torch.from_numpy(a).pin_memory(), torch.from_numpy(b).pin_memory()
     for _ in range(3):
@@ -148,8 +150,8 @@ def test_pair_host_overlapped_upload_equals_device_pair(w, h, seed, bands, rows)
     ref.close()
 
 
-@pytest.mark.parametrize("bands", [0, 4])
-def test_profile_pair_host_phases(bands):
+@pytest.mark.parametrize("bands,streams", [(0, 0), (4, 0), (0, 1)])
+def test_profile_pair_host_phases(bands, streams):
     """orbx_profile_pair_host returns the same results as orbx_pair_host and
     phase times in order: uploads end before the kernels, the kernels before
     the export, and the host wall time covers the device span."""
@@ -159,6 +161,7 @@ def test_profile_pair_host_phases(bands):
     ctx = orbx.Context(0, orbx.make_params(max_pts=10000))
     t = ctx.get_tuning()
     t.upload_bands = bands
+    t.host_overlap = streams
     ctx.set_tuning(t)
     ha, hb = torch.from_numpy(a).pin_memory(), torch.from_numpy(b).pin_memory()
     hpa, hpb = np.zeros((10000, 7), np.int32), np.zeros((10000, 7), np.int32)
