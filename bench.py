@@ -879,6 +879,11 @@ def run_batch_workload(args, world, rank, local):
             "gpu_launches": (1 if best == "persistent" else 5) * steps, "clocks": clocks}
 
 
+LEARNED_SIZES = {"db": 1 << 20, "q": 131072, "train": 262144, "cal": 32768}
+LEARNED_RECALL = 0.99
+LEARNED_CAL_TARGET = 0.992  # calibration target, above the reported bar to cover held-out variance
+
+
 def learned_view_ids(i, short):
     """Views of learned-proposal image i that are still needed: 0 = query, 1 =
     training (every 3rd image), 2 = calibration (every 24th image)."""

@@ -125,3 +125,20 @@ def test_calibrate_fallback_uses_distance():
     assert td >= 40 and frac <= 0.05 + 1e-9
     fb = (margin < tm) | (dstar > td)
     assert (fb.sum() + (correct & ~fb).sum()) / n >= 0.99
+
+
+def test_bench_names_are_defined():
+    """Every name bench.py reads is defined, imported or a builtin (a guard
+    against a definition lost in an edit; the bench only runs on a GPU box)."""
+    import ast
+    import builtins
+
+    src = open(os.path.join(os.path.dirname(__file__), "..", "bench.py")).read()
+    tree = ast.parse(src)
+    defined = {n.id for n in ast.walk(tree) if isinstance(n, ast.Name) and isinstance(n.ctx, ast.Store)}
+    defined |= {n.name for n in ast.walk(tree) if isinstance(n, (ast.FunctionDef, ast.ClassDef))}
+    defined |= {a.asname or a.name.split(".")[0] for n in ast.walk(tree) if isinstance(n, (ast.Import, ast.ImportFrom))
+                for a in n.names}
+    defined |= {a.arg for n in ast.walk(tree) if isinstance(n, ast.arguments) for a in n.args + n.kwonlyargs}
+    used = {n.id for n in ast.walk(tree) if isinstance(n, ast.Name) and isinstance(n.ctx, ast.Load)}
+    assert sorted(u for u in used - defined if not hasattr(builtins, u) and u != "__file__") == []
