@@ -6,9 +6,17 @@
 
 namespace orbx {
 
-// FAST ring (makeOffsets, orbd.cu:463-496), as (dx, dy).
-static __constant__ int8_t c_ring[16][2] = {{0, 3},  {1, 3},   {2, 2},   {3, 1},   {3, 0},  {3, -1}, {2, -2}, {1, -3},
-                                     {0, -3}, {-1, -3}, {-2, -2}, {-3, -1}, {-3, 0}, {-3, 1}, {-2, 2}, {-1, 3}};
+// FAST ring (makeOffsets, orbd.cu:463-496), as (dx, dy) of ring position k.
+// Functions of a compile-time k fold to immediates in the unrolled loops.
+__host__ __device__ constexpr int ring_dx(int k) {
+  switch (k & 15) {
+    case 0: return 0;   case 1: return 1;   case 2: return 2;   case 3: return 3;
+    case 4: return 3;   case 5: return 3;   case 6: return 2;   case 7: return 1;
+    case 8: return 0;   case 9: return -1;  case 10: return -2; case 11: return -3;
+    case 12: return -3; case 13: return -3; case 14: return -2; default: return -1;
+  }
+}
+__host__ __device__ constexpr int ring_dy(int k) { return ring_dx(k + 4); }
 
 __device__ __forceinline__ bool has_arc9(uint32_t m16) {
   uint32_t m = m16 | (m16 << 16);  // circular
@@ -69,7 +77,7 @@ __device__ __forceinline__ bool fast9_full(const uint8_t* c, int sw, int lo, int
   uint32_t dark = 0, bright = 0;
 #pragma unroll
   for (int k = 0; k < 16; k++) {
-    const int p = c[c_ring[k][1] * sw + c_ring[k][0]];
+    const int p = c[ring_dy(k) * sw + ring_dx(k)];
     dark |= (uint32_t)(p < lo) << k;
     bright |= (uint32_t)(p > hi) << k;
   }

@@ -180,7 +180,7 @@ __global__ void k_ocv_fast(OcvArgs a) {
     if (fast9_full(c, V.pitch, v - a.fast_thr, v + a.fast_thr)) {
       int d[25];
 #pragma unroll
-      for (int r = 0; r < 25; r++) d[r] = (int)(short)(v - c[c_ring[r & 15][1] * V.pitch + c_ring[r & 15][0]]);
+      for (int r = 0; r < 25; r++) d[r] = (int)(short)(v - c[ring_dy(r) * V.pitch + ring_dx(r)]);
       sc = (uint8_t)min(max((int)fast_score(d, a.fast_thr), 1), 255);
     }
   }

@@ -285,7 +285,7 @@ __device__ __forceinline__ float corner_score(const Batch& b, const uint8_t* c, 
   const int v = c[0];
   int d[25];
 #pragma unroll
-  for (int k = 0; k < 25; k++) d[k] = (int)(short)(v - c[c_ring[k & 15][1] * sw + c_ring[k & 15][0]]);
+  for (int k = 0; k < 25; k++) d[k] = (int)(short)(v - c[ring_dy(k) * sw + ring_dx(k)]);
   return fast_score(d, b.fast_thr);
 }
 
@@ -429,9 +429,9 @@ __device__ __forceinline__ void det_tile(const Batch& b, int t, DetSmem& sm) {
   {
     const int n2 = s_n[1];
     if (b.harris) {
-      // 32 groups of 8 lanes, one corner per group; lane s of a group takes
-      // window positions s, s + 8, ... of the 7x7 Harris window (the 32-bit sums
-      // wrap, so their order is free)
+      // 32 groups of 8 lanes, one corner per group; lanes 0..6 of a group take
+      // one row each of the 7x7 Harris window (the 32-bit sums wrap, so their
+      // order is free)
       const int gid = threadIdx.x >> 3, sub = threadIdx.x & 7;
       for (int j0 = 0; j0 < n2; j0 += 32) {
         if (j0 + 4 * warp >= n2) break;  // this warp's four groups have no corner (warp-uniform)
@@ -443,16 +443,20 @@ __device__ __forceinline__ void det_tile(const Batch& b, int t, DetSmem& sm) {
           const int o = e >> 11, ly = (e >> 6) & 31, lx = e & 63;
           const int sw = (kDetTW >> o) + 2 * kHalo;
           const uint8_t* c = s_stage + det_stage_off(o) + (ly + kHalo) * sw + (lx + kHalo);
-          for (int pos = sub; pos < 49; pos += 8) {
-            const int wy = pos / 7 - 3, wx = pos % 7 - 3;
-            const uint8_t* q = c + wy * sw + wx;
-            const int dx = ((int)q[1] - (int)q[-1]) * 2 + ((int)q[-sw + 1] - (int)q[-sw - 1]) +
-                           ((int)q[sw + 1] - (int)q[sw - 1]);
-            const int dy = ((int)q[sw] - (int)q[-sw]) * 2 + ((int)q[sw - 1] - (int)q[-sw - 1]) +
-                           ((int)q[sw + 1] - (int)q[-sw + 1]);
-            dxx += dx * dx;
-            dyy += dy * dy;
-            dxy += dx * dy;
+          if (sub < 7) {  // lane `sub` of the group takes window row sub - 3, its 7 columns unrolled
+            const uint8_t* r = c + (sub - 3) * sw;
+            const uint8_t* ru = r - sw;
+            const uint8_t* rd = r + sw;
+#pragma unroll
+            for (int wx = -3; wx <= 3; wx++) {
+              const int dx = ((int)r[wx + 1] - (int)r[wx - 1]) * 2 + ((int)ru[wx + 1] - (int)ru[wx - 1]) +
+                             ((int)rd[wx + 1] - (int)rd[wx - 1]);
+              const int dy = ((int)rd[wx] - (int)ru[wx]) * 2 + ((int)rd[wx - 1] - (int)ru[wx - 1]) +
+                             ((int)rd[wx + 1] - (int)ru[wx + 1]);
+              dxx += dx * dx;
+              dyy += dy * dy;
+              dxy += dx * dy;
+            }
           }
         }
 #pragma unroll
