@@ -311,6 +311,25 @@ struct DetSmem {
   int ow[kMaxOctaves], oh[kMaxOctaves];
 };
 
+// Stages octave O of a detect tile with its halo: (32 >> O) + 8 rows of
+// (64 >> O) + 8 bytes starting 4 rows above and 4 bytes left of the tile's
+// octave origin, in the pyramid's linear addressing.
+template <int O, bool P>
+__device__ __forceinline__ void stage_octave(const Frame& F, const uint8_t* pyr, int X0, int Y0, uint8_t* s_stage) {
+  constexpr int sw4 = ((kDetTW >> O) + 2 * kHalo) / 4;
+  constexpr int sh = (kDetTH >> O) + 2 * kHalo;
+  const int op = F.op[O];
+  const uint32_t* src =
+      reinterpret_cast<const uint32_t*>(pyr + F.ooff[O] + (long long)((Y0 >> O) - kHalo) * op + ((X0 >> O) - kHalo));
+  const int op4 = op >> 2;
+  uint32_t* dst = reinterpret_cast<uint32_t*>(s_stage + det_stage_off(O));
+#pragma unroll 4
+  for (int i = threadIdx.x; i < sh * sw4; i += 256) {
+    const int r = i / sw4, w = i - r * sw4;
+    dst[i] = ldx<P>(src + r * op4 + w);
+  }
+}
+
 // Pre-test of word w (four centres) of octave O of a detect tile: octave O
 // has (32 >> O) rows of (16 >> O) words.  Centres that pass are appended to
 // the tile's candidate list.
@@ -376,20 +395,14 @@ __device__ __forceinline__ void det_tile(const Batch& b, int t, DetSmem& sm) {
     s_ow[threadIdx.x] = threadIdx.x < n_oct ? F.ow[threadIdx.x] : 0;
     s_oh[threadIdx.x] = threadIdx.x < n_oct ? F.oh[threadIdx.x] : 0;
   }
-  // Stage every octave's tile with its halo, 4 bytes per load, one row per warp
-  // and step: octave offsets and pitches are multiples of 128 and (X0 >> o) - 4
-  // is a multiple of 4; a staged row is at most 18 words.
-  for (int o = 0; o < n_oct; o++) {
-    const int sw = (kDetTW >> o) + 2 * kHalo;
-    const int sh = (kDetTH >> o) + 2 * kHalo;
-    const int sw4 = sw >> 2;
-    const int op = F.op[o];
-    const long long base = F.ooff[o] + (long long)((Y0 >> o) - kHalo) * op + ((X0 >> o) - kHalo);
-    uint32_t* dst = reinterpret_cast<uint32_t*>(s_stage + det_stage_off(o));
-    if (lane < sw4)
-      for (int r = warp; r < sh; r += 8)
-        dst[r * sw4 + lane] = ldx<P>(reinterpret_cast<const uint32_t*>(pyr + base + (long long)r * op) + lane);
-  }
+  // Stage every octave's tile with its halo, 4 bytes per load (octave offsets
+  // and pitches are multiples of 128 and (X0 >> o) - 4 is a multiple of 4):
+  // the words of each octave are spread over the whole block.
+  stage_octave<0, P>(F, pyr, X0, Y0, s_stage);
+  if (n_oct > 1) stage_octave<1, P>(F, pyr, X0, Y0, s_stage);
+  if (n_oct > 2) stage_octave<2, P>(F, pyr, X0, Y0, s_stage);
+  if (n_oct > 3) stage_octave<3, P>(F, pyr, X0, Y0, s_stage);
+  if (n_oct > 4) stage_octave<4, P>(F, pyr, X0, Y0, s_stage);
   __syncthreads();
 
   // 1. cardinal pre-test, four centres per word: the 512 words of octave 0 take
