@@ -43,6 +43,14 @@ SMS = 148
 # DRAM bytes per launch measured by ncu (dram__bytes_read.sum + dram__bytes_write.sum,
 # cold cache) on the same workloads (the committed ncu summaries of the 1080p
 # pair and of 65536 x 65536 matching); kernels without a capture report None.
+# Warp instructions per launch of the five pair kernels (ncu smsp__inst_executed.sum
+# on the same 1080p pair, the committed summary of the pair's kernels): the
+# instruction roofline beside the HBM one, since these kernels are issue- and
+# latency-bound.
+NCU_WARP_INST = {"pyramid_blur": 13107574, "detect": 12141617, "nms": 2838553, "describe": 3380151,
+                 "match": 2037180}
+ISSUE_PER_CLK_PER_SM = 4  # warp instructions issued per clock per SM (one per scheduler)
+
 NCU_TRAFFIC = {"k_pyramid_blur": 4159744, "k_detect": 5656832, "k_nms": 1499392, "k_describe<2>": 5611008,
                "k_match_popc": 97792, "k_match_imma": 33602560}
 
@@ -431,14 +439,17 @@ def run_orbx(args, world, rank, local):
             imma_ms.append(e0.elapsed_time(e1))
     imma_pa, _ = A.to_host()
 
-    # both forms of the device-resident pair: five graph-replayed launches and
-    # one persistent launch with a device work queue
+    # both forms of the device-resident pair: five graph-replayed launches (as
+    # programmatic dependent launches, the default, and in plain stream order)
+    # and one persistent launch with a device work queue
     pair_forms = {}
     keep_t = ctx.get_tuning()
-    for name, form, rows in (("five_launch", 0, 0), ("persistent", 1, 0), ("persistent_row_deps", 1, 1)):
+    for name, form, rows, dep in (("five_launch", 0, 0, 1), ("five_launch_plain_order", 0, 0, 0),
+                                  ("persistent", 1, 0, 1), ("persistent_row_deps", 1, 1, 1)):
         t = ctx.get_tuning()
         t.pair_form = form
         t.persist_row_deps = rows
+        t.dependent_launch = dep
         ctx.set_tuning(t)
         f_ms = []
         with torch.cuda.stream(stream):
@@ -542,6 +553,7 @@ def run_orbx(args, world, rank, local):
     work = stage_work(oszp, n, na, nb)
     peaks, peak_kind = load_peaks()
     kernels = {}
+    clk_hz = ((clocks or {}).get("sm_mhz") or 1965.0) * 1e6
     for i, nm in enumerate(names):
         ent = {"ms": float(stage_ms[i])}
         if nm in work:
@@ -549,6 +561,13 @@ def run_orbx(args, world, rank, local):
             ent["gbs"] = work[nm] / (stage_ms[i] * 1e-3) / 1e9
         else:
             ent["popc_ops"] = na * nb * 8
+        if nm in NCU_WARP_INST:
+            # instruction roofline: warp instructions per level-0 pixel of the pair,
+            # and the fraction of the SMs' issue slots they fill in the live time
+            inst = NCU_WARP_INST[nm]
+            ent["warp_inst"] = inst
+            ent["warp_inst_per_l0_pixel"] = inst / (2.0 * W * H)
+            ent["issue_slot_frac"] = inst / (ISSUE_PER_CLK_PER_SM * SMS * clk_hz * stage_ms[i] * 1e-3)
         kernels[nm] = ent
     dom = max(names, key=lambda k: kernels[k]["ms"])
     if dom == "match":

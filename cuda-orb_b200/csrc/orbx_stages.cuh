@@ -37,23 +37,73 @@ __device__ __forceinline__ T ldx(const T* p) {
 // ---------------------------------------------------------------------------
 
 // Exact small-integer <-> float conversions on the full-rate pipes: a float
-// whose exponent field is 2^23 holds the integer in its mantissa.
-__device__ __forceinline__ float u8_to_float(uint32_t x) {  // 0 <= x < 2^23
-  return __fsub_rn(__uint_as_float(0x4B000000u | x), 8388608.0f);
+// whose exponent field is 2^23 holds the integer in its mantissa.  byte_bits:
+// the byte of `word` that selector `sel` (0x754j, j = 0..3) picks, in the low
+// mantissa byte of 2^23, i.e. the float bits of 2^23 + byte.
+__device__ __forceinline__ float byte_bits(uint32_t word, uint32_t sel) {
+  return __uint_as_float(__byte_perm(word, 0x4B000000u, sel));
 }
-__device__ __forceinline__ uint32_t float_to_u8_rne(float v) {  // 0 <= v < 2^22: round to nearest, ties to even
-  return (uint32_t)(__float_as_int(__fadd_rn(v, 12582912.0f)) - 0x4B400000);
+// Low bytes of four 32-bit words packed into one word (a | b << 8 | c << 16 | d << 24).
+__device__ __forceinline__ uint32_t pack_low_bytes(uint32_t a, uint32_t b, uint32_t c, uint32_t d) {
+  return __byte_perm(__byte_perm(a, b, 0x0040), __byte_perm(c, d, 0x0040), 0x5410);
 }
+__device__ __forceinline__ float2 pair2(float v) { return make_float2(v, v); }
+// gauss_dot4 on both lanes of a pair: the same operations in the same order,
+// each lane rounded as the scalar form (one packed sm_100 FP32 instruction per step).
+__device__ __forceinline__ float2 gauss_dot4x2(const float2* k, float2 t0, float2 t1, float2 t2, float2 t3) {
+  float2 acc = __ffma2_rn(k[0], t0, __fmul2_rn(k[1], t1));
+  acc = __ffma2_rn(k[2], t2, acc);
+  return __ffma2_rn(k[3], t3, acc);
+}
+// One 4-byte group of staged source columns cx .. cx+3 of a row (reflect-101 at
+// the octave edges).  words: the row is level 0 of a 4-byte aligned image, so
+// interior groups take two aligned words (cx is one past a multiple of 4).
+template <bool PL>
+__device__ __forceinline__ uint32_t pyr_stage_word(const uint8_t* rowp, int cx, int ow, int sh, bool words) {
+  if (words && cx >= 1 && cx + 3 < ow) {
+    // bytes cx-1 .. cx+6 lie in [0, pitch_in): cx + 3 < ow <= pitch_in and both words are aligned
+    const uint32_t* wp = reinterpret_cast<const uint32_t*>(rowp + (cx - 1));
+    return __byte_perm(ldx<PL>(wp), ldx<PL>(wp + 1), 0x4321);
+  }
+  uint32_t v[4];
+#pragma unroll
+  for (int j = 0; j < 4; j++) v[j] = ldx<PL>(rowp + (reflect101(cx + j, ow) << sh));
+  return pack_low_bytes(v[0], v[1], v[2], v[3]);
+}
+// Row-major walk over items (r, g) with W items per row: item threadIdx.x +
+// k * blockDim.x for k = 0, 1, .., stepped without a division per step.
+template <int W>
+struct RowWalk {
+  int r, g, dr, dg;
+  __device__ __forceinline__ RowWalk()
+      : r(threadIdx.x / W), g(threadIdx.x % W), dr(blockDim.x / W), dg(blockDim.x % W) {}
+  __device__ __forceinline__ void next() {
+    r += dr;
+    g += dg;
+    if (g >= W) {
+      g -= W;
+      r++;
+    }
+  }
+};
 
-// Staged source of a TW x TH tile: a 3-pixel halo on each side, the width
-// padded to a multiple of 4.
+// Staged source of a TW x TH tile.  The filters run on column pairs: pair k of a
+// row holds column k of the tile's left half and column k of its right half
+// (each half with its 3-pixel halo on both sides), so one packed instruction
+// filters two output columns.  Pairs are grouped two to a 16-byte slot, and a
+// row's even slots are stored before its odd slots: a thread that works on
+// slots 2g, 2g+1, .. reads slot 2g+m of its row at (m odd) * half + g + m/2,
+// so the lanes of a warp read consecutive 16-byte words for every m.  The raw
+// bytes are staged linearly.
 template <int TW, int TH>
 struct PyrSmem {
-  static constexpr int SW = TW + 8;
+  static constexpr int HW = TW / 2;   // columns per half
+  static constexpr int SW = TW + 8;   // staged bytes per row
+  static constexpr int SW2 = HW + 8;  // staged column pairs per row (3 + HW + 3, padded to 4)
   static constexpr int SH = TH + 6;
-  __align__(16) float src[SH * SW];
+  __align__(16) float2 src[SH * SW2];
   __align__(16) uint8_t byte[SH * SW];
-  __align__(16) float row[SH * TW];
+  __align__(16) float2 row[SH * HW];
 };
 
 // One pyramid tile (tile index t over the batch) of shape TW x TH.  PL: the
@@ -61,11 +111,14 @@ struct PyrSmem {
 // the read-only path).
 template <bool PL, int TW = kPyrTW, int TH = kPyrTH>
 __device__ __forceinline__ void pyr_tile(const Batch& b, int t, PyrSmem<TW, TH>& sm) {
-  constexpr int kPyrTW = TW, kPyrTH = TH;
-  constexpr int kPyrSW = PyrSmem<TW, TH>::SW, kPyrSH = PyrSmem<TW, TH>::SH;
-  float* s_src = sm.src;
+  using S = PyrSmem<TW, TH>;
+  constexpr int kHW = S::HW, kSW = S::SW, kSH = S::SH;
+  constexpr int kRowSlots = S::SW2 / 2;  // 16-byte slots per staged pair row (two planes)
+  constexpr int kOutSlots = kHW / 2;     // 16-byte slots per filtered pair row (two planes)
+  static_assert(TW % 16 == 0 && S::SW2 % 4 == 0, "pyramid tile width");
+  float4* s_src = reinterpret_cast<float4*>(sm.src);
+  float4* s_row = reinterpret_cast<float4*>(sm.row);
   uint8_t* s_byte = sm.byte;
-  float* s_row = sm.row;
   const int f = find_frame(b.pyr_base, b.n_frames, t);
   const Frame& F = b.frames[f];
   int lt = t - b.pyr_base[f];
@@ -73,8 +126,8 @@ __device__ __forceinline__ void pyr_tile(const Batch& b, int t, PyrSmem<TW, TH>&
   while (o + 1 < F.n_oct && lt >= F.pyr_tile_base[o + 1]) o++;
   lt -= F.pyr_tile_base[o];
   const int tiles_x = F.pyr_tiles_x[o];
-  const int x0 = (lt % tiles_x) * kPyrTW;
-  const int y0 = (lt / tiles_x) * kPyrTH;
+  const int x0 = (lt % tiles_x) * TW;
+  const int y0 = (lt / tiles_x) * TH;
   const int ow = F.ow[o], oh = F.oh[o], op = F.op[o];
   const uint8_t* __restrict__ img = F.img;
   const int pitch_in = F.pitch_in;
@@ -89,102 +142,120 @@ __device__ __forceinline__ void pyr_tile(const Batch& b, int t, PyrSmem<TW, TH>&
   }
   if (t == 0 && threadIdx.x == 0) *b.nms_ticket = 0u;
 
-  // stage: source rows y0-3 .. y0+34, columns x0-3 .. x0+132, reflect-101 at
-  // the octave edges, as floats and as bytes
+  // stage: source rows y0-3 .. y0+TH+2; item (r, g) takes columns 4g-3 .. 4g
+  // of the left half and of the right half (tile-relative), reflect-101 at the
+  // octave edges, as float pairs and as bytes
   const uint8_t* __restrict__ psrc = F.pyr_src ? F.pyr_src + F.ooff[o] : nullptr;
-  // octave 0 read from a 4-byte aligned image: interior groups take two aligned
-  // words (the group starts one byte past a word boundary, x0 being a multiple of 4)
   const bool words0 = (o == 0) && !psrc && ((reinterpret_cast<uintptr_t>(img) | (uintptr_t)pitch_in) & 3u) == 0;
-  constexpr int kGroups = kPyrSW / 4;
-  for (int it = threadIdx.x; it < kPyrSH * kGroups; it += blockDim.x) {
-    const int r = it / kGroups;
-    const int g = it - r * kGroups;
+  const int sh = psrc ? 0 : o;
+  constexpr int kGroups = S::SW2 / 4;  // staging items per row = slots per plane of a staged row
+  const float2 m23 = pair2(-8388608.0f);
+  for (RowWalk<kGroups> w; w.r < kSH; w.next()) {
+    const int r = w.r, g = w.g;
     const int y = reflect101(y0 - 3 + r, oh);
     const uint8_t* rowp = psrc ? psrc + (size_t)y * op : img + (size_t)(y << o) * pitch_in;
-    const int sh = psrc ? 0 : o;
     const int cx = x0 - 3 + 4 * g;
-    uint32_t v[4];
-    if (words0 && cx >= 1 && cx + 3 < ow) {
-      // bytes cx-1 .. cx+6 lie in [0, pitch_in): cx + 3 < ow <= pitch_in and both words are aligned
-      const uint32_t* wp = reinterpret_cast<const uint32_t*>(rowp + (cx - 1));
-      const uint32_t word = __byte_perm(ldx<PL>(wp), ldx<PL>(wp + 1), 0x4321);
-#pragma unroll
-      for (int j = 0; j < 4; j++) v[j] = (word >> (8 * j)) & 0xFFu;
-    } else {
-#pragma unroll
-      for (int j = 0; j < 4; j++) v[j] = ldx<PL>(rowp + (reflect101(cx + j, ow) << sh));
-    }
-    reinterpret_cast<float4*>(s_src)[it] = make_float4(u8_to_float(v[0]), u8_to_float(v[1]), u8_to_float(v[2]),
-                                                       u8_to_float(v[3]));
-    reinterpret_cast<uint32_t*>(s_byte)[it] = v[0] | (v[1] << 8) | (v[2] << 16) | (v[3] << 24);
+    const uint32_t wa = pyr_stage_word<PL>(rowp, cx, ow, sh, words0);
+    const uint32_t wb = pyr_stage_word<PL>(rowp, cx + kHW, ow, sh, words0);
+    // pair j = (byte j of wa, byte j of wb) as floats: 2^23 + byte, minus 2^23
+    const float2 p0 = __fadd2_rn(make_float2(byte_bits(wa, 0x7540u), byte_bits(wb, 0x7540u)), m23);
+    const float2 p1 = __fadd2_rn(make_float2(byte_bits(wa, 0x7541u), byte_bits(wb, 0x7541u)), m23);
+    const float2 p2 = __fadd2_rn(make_float2(byte_bits(wa, 0x7542u), byte_bits(wb, 0x7542u)), m23);
+    const float2 p3 = __fadd2_rn(make_float2(byte_bits(wa, 0x7543u), byte_bits(wb, 0x7543u)), m23);
+    // pairs 4g .. 4g+3 = slots 2g (even plane) and 2g+1 (odd plane) of row r
+    float4* row = s_src + r * kRowSlots + g;
+    row[0] = make_float4(p0.x, p0.y, p1.x, p1.y);
+    row[kGroups] = make_float4(p2.x, p2.y, p3.x, p3.y);
+    // the halves' halos overlap in the middle: both writes there store the same bytes
+    *reinterpret_cast<uint32_t*>(s_byte + r * kSW + 4 * g) = wa;
+    *reinterpret_cast<uint32_t*>(s_byte + r * kSW + kHW + 4 * g) = wb;
   }
   __syncthreads();
 
-  const float* k = b.gauss;
-  // horizontal pass: 4 consecutive outputs per thread; integer tap sums are
-  // exact in float, so they are summed as floats
-  for (int it = threadIdx.x; it < kPyrSH * (kPyrTW / 4); it += blockDim.x) {
-    const int r = it / (kPyrTW / 4);
-    const int g = it - r * (kPyrTW / 4);
-    const float4* q = reinterpret_cast<const float4*>(s_src + r * kPyrSW) + g;
-    const float4 a0 = q[0], a1 = q[1], a2 = q[2];
-    const float p[12] = {a0.x, a0.y, a0.z, a0.w, a1.x, a1.y, a1.z, a1.w, a2.x, a2.y, a2.z, a2.w};
-    float4 out;
-    float* op4 = &out.x;
+  float2 k[4];
 #pragma unroll
-    for (int j = 0; j < 4; j++) {
-      const float t1 = __fadd_rn(p[j + 2], p[j + 4]);
-      const float t2 = __fadd_rn(p[j + 1], p[j + 5]);
-      const float t3 = __fadd_rn(p[j], p[j + 6]);
-      op4[j] = gauss_dot4(k, p[j + 3], t1, t2, t3);
-    }
-    reinterpret_cast<float4*>(s_row + r * kPyrTW)[g] = out;
+  for (int i = 0; i < 4; i++) k[i] = pair2(b.gauss[i]);
+  // horizontal pass: 4 consecutive output pairs per thread; integer tap sums
+  // are exact in float, so they are summed as floats
+  constexpr int kHG = kHW / 4;  // items per row = slots per plane of a filtered row
+  for (RowWalk<kHG> w; w.r < kSH; w.next()) {
+    const int r = w.r, g = w.g;
+    const float4* row = s_src + r * kRowSlots + g;
+    // slots 2g .. 2g+4: even plane g, g+1, g+2 and odd plane g, g+1
+    const float4 e0 = row[0], o0 = row[kGroups], e1 = row[1], o1 = row[kGroups + 1], e2 = row[2];
+    const float2 p[10] = {make_float2(e0.x, e0.y), make_float2(e0.z, e0.w), make_float2(o0.x, o0.y),
+                          make_float2(o0.z, o0.w), make_float2(e1.x, e1.y), make_float2(e1.z, e1.w),
+                          make_float2(o1.x, o1.y), make_float2(o1.z, o1.w), make_float2(e2.x, e2.y),
+                          make_float2(e2.z, e2.w)};
+    float2 q[4];
+#pragma unroll
+    for (int j = 0; j < 4; j++)
+      q[j] = gauss_dot4x2(k, p[j + 3], __fadd2_rn(p[j + 2], p[j + 4]), __fadd2_rn(p[j + 1], p[j + 5]),
+                          __fadd2_rn(p[j], p[j + 6]));
+    float4* out = s_row + r * kOutSlots + g;
+    out[0] = make_float4(q[0].x, q[0].y, q[1].x, q[1].y);
+    out[kHG] = make_float4(q[2].x, q[2].y, q[3].x, q[3].y);
   }
   __syncthreads();
 
-  // vertical pass and stores: 4 consecutive columns of one row per thread
+  // vertical pass and stores: 4 consecutive column pairs of one row per thread
   uint8_t* P = F.pyr + F.ooff[o];
   uint8_t* B = F.blr + F.ooff[o];
   const bool copy_pad = (o == 0) && (pitch_in == op);
-  for (int it = threadIdx.x; it < kPyrTH * (kPyrTW / 4); it += blockDim.x) {
-    const int r = it / (kPyrTW / 4);
-    const int g = it - r * (kPyrTW / 4);
+  const float2 rne = pair2(12582912.0f);
+  for (RowWalk<kHG> w; w.r < TH; w.next()) {
+    const int r = w.r, g = w.g;
     const int y = y0 + r;
-    const int x = x0 + 4 * g;
-    if (y >= oh || x >= op) continue;
-    float4 h[7];
+    if (y >= oh) continue;
+    float2 h[7][4];
+    const float4* col = s_row + r * kOutSlots + g;
 #pragma unroll
-    for (int j = 0; j < 7; j++) h[j] = reinterpret_cast<const float4*>(s_row + (r + j) * kPyrTW)[g];
-    const float* hf = reinterpret_cast<const float*>(h);
-    uint32_t bw = 0;
+    for (int i = 0; i < 7; i++) {
+      const float4 v0 = col[i * kOutSlots], v1 = col[i * kOutSlots + kHG];
+      h[i][0] = make_float2(v0.x, v0.y);
+      h[i][1] = make_float2(v0.z, v0.w);
+      h[i][2] = make_float2(v1.x, v1.y);
+      h[i][3] = make_float2(v1.z, v1.w);
+    }
+    // rounded to the nearest integer, ties to even, by adding 1.5 * 2^23: the
+    // result's low byte is the blurred pixel (0 <= v <= 255)
+    uint32_t ua[4], ub[4];
 #pragma unroll
     for (int j = 0; j < 4; j++) {
-      const float t1 = __fadd_rn(hf[8 + j], hf[16 + j]);
-      const float t2 = __fadd_rn(hf[4 + j], hf[20 + j]);
-      const float t3 = __fadd_rn(hf[j], hf[24 + j]);
-      bw |= (float_to_u8_rne(gauss_dot4(k, hf[12 + j], t1, t2, t3)) & 0xFFu) << (8 * j);
+      const float2 v = __fadd2_rn(gauss_dot4x2(k, h[3][j], __fadd2_rn(h[2][j], h[4][j]),
+                                               __fadd2_rn(h[1][j], h[5][j]), __fadd2_rn(h[0][j], h[6][j])),
+                                  rne);
+      ua[j] = __float_as_uint(v.x);
+      ub[j] = __float_as_uint(v.y);
     }
-    // raw bytes of the same 4 pixels: staged columns 4g+3 .. 4g+6 of row r+3
-    const uint32_t* sb = reinterpret_cast<const uint32_t*>(s_byte + (r + 3) * kPyrSW) + g;
-    const uint32_t pw = __byte_perm(sb[0], sb[1], 0x6543);
-    const size_t a = (size_t)y * op + x;
-    if (x + 4 <= ow) {
-      *reinterpret_cast<uint32_t*>(B + a) = bw;
-      *reinterpret_cast<uint32_t*>(P + a) = pw;
-    } else {
-      // the group reaches into the row padding: octave 0 carries the caller's
-      // padding bytes (the reference copies h * pitch0 bytes, orbd.cu:1584),
-      // other octaves hold zeros
+    const uint8_t* sb = s_byte + (r + 3) * kSW + 4 * g;
 #pragma unroll
-      for (int j = 0; j < 4; j++) {
-        if (x + j < ow) {
-          B[a + j] = (uint8_t)(bw >> (8 * j));
-          P[a + j] = (uint8_t)(pw >> (8 * j));
-        } else {
-          const uint8_t v = psrc ? ldx<PL>(psrc + a + j)
-                                 : (copy_pad ? ldx<PL>(img + (size_t)y * pitch_in + x + j) : (uint8_t)0);
-          B[a + j] = v;
-          P[a + j] = v;
+    for (int half = 0; half < 2; half++) {
+      const int x = x0 + half * kHW + 4 * g;
+      if (x >= op) continue;
+      const uint32_t bw = half ? pack_low_bytes(ub[0], ub[1], ub[2], ub[3]) : pack_low_bytes(ua[0], ua[1], ua[2], ua[3]);
+      // raw bytes of the same 4 pixels: staged columns 4g+3 .. 4g+6 of the half
+      const uint32_t* sw = reinterpret_cast<const uint32_t*>(sb + half * kHW);
+      const uint32_t pw = __byte_perm(sw[0], sw[1], 0x6543);
+      const size_t a = (size_t)y * op + x;
+      if (x + 4 <= ow) {
+        *reinterpret_cast<uint32_t*>(B + a) = bw;
+        *reinterpret_cast<uint32_t*>(P + a) = pw;
+      } else {
+        // the group reaches into the row padding: octave 0 carries the caller's
+        // padding bytes (the reference copies h * pitch0 bytes, orbd.cu:1584),
+        // other octaves hold zeros
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+          if (x + j < ow) {
+            B[a + j] = (uint8_t)(bw >> (8 * j));
+            P[a + j] = (uint8_t)(pw >> (8 * j));
+          } else {
+            const uint8_t v = psrc ? ldx<PL>(psrc + a + j)
+                                   : (copy_pad ? ldx<PL>(img + (size_t)y * pitch_in + x + j) : (uint8_t)0);
+            B[a + j] = v;
+            P[a + j] = v;
+          }
         }
       }
     }
@@ -383,7 +454,6 @@ __device__ __forceinline__ void det_tile(const Batch& b, int t, DetSmem& sm) {
   const int Y0 = (lt / F.det_tiles_x) * kDetTH;
   const int n_oct = F.n_oct;
   const uint8_t* __restrict__ pyr = F.pyr;
-  const int lane = threadIdx.x & 31;
   const int warp = threadIdx.x >> 5;
   const int thr = b.fast_thr;
 
@@ -537,11 +607,15 @@ __device__ __forceinline__ void det_tile(const Batch& b, int t, DetSmem& sm) {
 // ---------------------------------------------------------------------------
 constexpr unsigned long long kFlagAgg = 1ull << 32;
 constexpr unsigned long long kFlagPre = 2ull << 32;
+constexpr int kLookPerLane = 8;  // look-back words read per lane and round: 256 predecessors
 
-// Warp 0 of a strip's block resolves the strip's exclusive prefix: it reads the
-// look-back words of up to 32 predecessors per round with acquire loads, and
-// stops at the nearest one that already carries an inclusive prefix.  The wait
-// for a predecessor is bounded by wait_cycles of clock64(); on expiry it sets
+// Warp 0 of a strip's block resolves the strip's exclusive prefix: in each round
+// lane l reads the look-back words of predecessors j - 8l .. j - 8l - 7, and the
+// warp stops at the nearest predecessor that already carries an inclusive
+// prefix.  A look-back word holds its flag and its count together and nothing
+// else is read on its strength, so relaxed loads suffice, and the eight of a
+// lane are in flight together (acquire loads would run one after another).  The wait for a
+// predecessor is bounded by wait_cycles of clock64(); on expiry it sets
 // kErrLookbackTimeout and returns the prefix found so far.
 __device__ __forceinline__ int nms_lookback(unsigned long long* st, int s, int lane, int* err,
                                             long long wait_cycles) {
@@ -549,14 +623,31 @@ __device__ __forceinline__ int nms_lookback(unsigned long long* st, int s, int l
   int j = s - 1;
   const long long t0 = clock64();
   while (j >= 0) {
-    const int idx = j - lane;
-    const unsigned long long wv = (idx >= 0) ? ld_acquire_u64(&st[idx]) : kFlagPre;
-    const unsigned long long flag = wv & (3ull << 32);
-    const unsigned pre = __ballot_sync(0xffffffffu, flag == kFlagPre);
-    const unsigned notready = __ballot_sync(0xffffffffu, flag == 0ull);
-    const int first_pre = pre ? (__ffs(pre) - 1) : 32;
-    const unsigned need = (first_pre >= 31) ? 0xffffffffu : ((2u << first_pre) - 1u);
-    if (notready & need) {
+    unsigned long long wv[kLookPerLane];
+#pragma unroll
+    for (int u = 0; u < kLookPerLane; u++) {
+      const int idx = j - lane * kLookPerLane - u;
+      wv[u] = (idx >= 0) ? ld_relaxed_u64(&st[idx]) : kFlagPre;
+    }
+    // this lane's nearest inclusive prefix, then the warp's
+    int first_u = kLookPerLane;
+#pragma unroll
+    for (int u = kLookPerLane - 1; u >= 0; u--)
+      if ((wv[u] & (3ull << 32)) == kFlagPre) first_u = u;
+    const unsigned pre = __ballot_sync(0xffffffffu, first_u < kLookPerLane);
+    const int first_lane = pre ? (__ffs(pre) - 1) : 32;
+    // words up to and including that prefix must all be published
+    bool notready = false;
+    int v = 0;
+#pragma unroll
+    for (int u = 0; u < kLookPerLane; u++) {
+      const bool need = lane < first_lane || (lane == first_lane && u <= first_u);
+      if (need) {
+        notready |= (wv[u] & (3ull << 32)) == 0ull;
+        v += (int)(unsigned)wv[u];
+      }
+    }
+    if (__any_sync(0xffffffffu, notready)) {
       if (clock64() - t0 > wait_cycles) {
         if (lane == 0) atomicOr(err, kErrLookbackTimeout);
         break;
@@ -564,12 +655,11 @@ __device__ __forceinline__ int nms_lookback(unsigned long long* st, int s, int l
       __nanosleep(20);
       continue;
     }
-    int v = ((need >> lane) & 1u) ? (int)(unsigned)wv : 0;
 #pragma unroll
     for (int d = 16; d >= 1; d >>= 1) v += __shfl_xor_sync(0xffffffffu, v, d);
     excl += v;
-    if (first_pre < 32) break;
-    j -= 32;
+    if (first_lane < 32) break;
+    j -= 32 * kLookPerLane;
   }
   return excl;
 }
@@ -581,13 +671,14 @@ __device__ __forceinline__ int nms_lookback(unsigned long long* st, int s, int l
 // bit is set.  Returns whether this lane's rows hold a suppressing position.
 // Positions are linear like the reference's (a column past the edge is the
 // adjacent row's entry); positions outside the map, reachable only with an
-// edge threshold below 2^o, are empty.
+// edge threshold below 2^o, are empty.  Occ(wi) gives occupancy word wi and
+// Score(wi, word, bit) the score of a set bit.
 constexpr int kNmsGroup = 8;
 constexpr int kNmsChunkWords = 128;  // occupancy words compacted per round: at most 4096 centres
 
-template <bool P>
-__device__ __forceinline__ bool nms_suppressed_rows(const Frame& F, long long idx, float v, int o, int p0,
-                                                    long long npx, int sub) {
+template <class Occ, class Score>
+__device__ __forceinline__ bool nms_window_suppressed(long long idx, float v, int o, int p0, long long npx, int sub,
+                                                      Occ occ, Score score) {
   const int r = 1 << o;
   for (int dyi = sub; dyi <= 2 * r; dyi += kNmsGroup) {
     const int dy = dyi - r;
@@ -598,7 +689,8 @@ __device__ __forceinline__ bool nms_suppressed_rows(const Frame& F, long long id
     if (hi >= npx) hi = npx - 1;
     for (long long wi = lo >> 5; wi <= (hi >> 5); wi++) {
       const long long base = wi << 5;
-      uint32_t m = ldx<P>(F.occ + wi);
+      const uint32_t word = occ(wi);
+      uint32_t m = word;
       if (base < lo) m &= ~0u << (int)(lo - base);
       if (hi - base < 31) m &= (2u << (int)(hi - base)) - 1u;
       while (m) {
@@ -607,7 +699,7 @@ __device__ __forceinline__ bool nms_suppressed_rows(const Frame& F, long long id
         const long long li = base + bb;
         if (li == idx) continue;
         const int dx = (int)(li - rc);
-        const float u = ldx<P>(F.vmap + li);
+        const float u = score(wi, word, bb);
         if (u > v || (u == v && dx <= 0 && dy <= 0)) return true;
       }
     }
@@ -615,16 +707,57 @@ __device__ __forceinline__ bool nms_suppressed_rows(const Frame& F, long long id
   return false;
 }
 
+// Staged form of a strip (kNmsStageWords occupancy words: the strip's rows with
+// a halo of R + 1 rows on each side; kNmsStageBits set bits with their scores
+// and octaves gathered next to them).
+constexpr int kNmsStageWords = 2048;
+constexpr int kNmsStageBits = 2048;
+
 struct NmsSmem {
   uint32_t sur[kNmsMaxWords];
   int pref[kNmsMaxWords];
-  uint16_t cand[kNmsChunkWords * 32];
-  float cv[kNmsChunkWords * 32];
-  uint8_t co[kNmsChunkWords * 32];
+  union {
+    struct {  // rounds over the maps in global memory
+      uint16_t cand[kNmsChunkWords * 32];
+      float cv[kNmsChunkWords * 32];
+      uint8_t co[kNmsChunkWords * 32];
+    } g;
+    struct {  // staged strip
+      uint32_t occ[kNmsStageWords];
+      float score[kNmsStageBits];
+      uint16_t pfx[kNmsStageWords + 1];  // set bits before each staged word
+      uint16_t idx[kNmsStageBits];       // bit offset of each set bit from the first staged word
+      uint8_t oct[kNmsStageBits];
+    } w;
+  } u;
   int ncand[2];
   int warp_tot[8];
   int base;
 };
+
+// Exclusive scan over the block (256 threads) of one count per thread; *total
+// gets the sum.  Every thread must call it.
+__device__ __forceinline__ int block_scan_excl(int local, int* s_warp_tot, int& total) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  int incl = local;
+#pragma unroll
+  for (int d = 1; d < 32; d <<= 1) {
+    const int n = __shfl_up_sync(0xffffffffu, incl, d);
+    if (lane >= d) incl += n;
+  }
+  if (lane == 31) s_warp_tot[warp] = incl;
+  __syncthreads();
+  int warp_off = 0, tot = 0;
+#pragma unroll
+  for (int w2 = 0; w2 < 8; w2++) {
+    const int t = s_warp_tot[w2];
+    if (w2 < warp) warp_off += t;
+    tot += t;
+  }
+  __syncthreads();
+  total = tot;
+  return warp_off + incl - local;
+}
 
 // One NMS strip; `ticket` is the strip's index over the batch, and strips must
 // start in ticket order (the look-back waits only on smaller tickets).  P: the
@@ -633,9 +766,6 @@ template <bool P>
 __device__ __forceinline__ void nms_strip(const Batch& b, int ticket, NmsSmem& sm) {
   uint32_t* s_sur = sm.sur;
   int* s_pref = sm.pref;
-  uint16_t* s_cand = sm.cand;
-  float* s_cv = sm.cv;
-  uint8_t* s_co = sm.co;
   int* s_ncand = sm.ncand;
   int* s_warp_tot = sm.warp_tot;
   int& s_base = sm.base;
@@ -649,60 +779,173 @@ __device__ __forceinline__ void nms_strip(const Batch& b, int ticket, NmsSmem& s
   const int wlo = xlo >> 5, whi = (xhi - 1) >> 5;
   const int nw = whi - wlo + 1;
   const int nwords = (row1 - row0) * nw;
-  const int p0 = F.op[0];
+  const int p0 = F.op[0];  // a multiple of 128
   const int wpr = p0 >> 5;  // occupancy words per row
   const long long npx = (long long)F.h * p0;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-
-  // pass 1: survivor bits of every occupancy word of the strip.  In rounds of
-  // kNmsChunkWords words: the centres of the round (with their scores) are
-  // compacted into shared memory, then checked by 32 groups of 8 lanes, so a
-  // textured patch of the strip spreads over every warp.
-  for (int k = threadIdx.x; k < nwords; k += blockDim.x) s_sur[k] = 0u;
-  if (threadIdx.x == 0) s_ncand[0] = 0;
   const int gid = warp * (32 / kNmsGroup) + (lane / kNmsGroup), sub = lane % kNmsGroup;
   const uint32_t gmask = ((1u << kNmsGroup) - 1u) << (lane & ~(kNmsGroup - 1));
-  for (int c0 = 0, round = 0; c0 < nwords; c0 += kNmsChunkWords, round++) {
-    int* cnt = &s_ncand[round & 1];
-    __syncthreads();  // the previous round's checks are done; its counter is free
-    if (threadIdx.x == 0) s_ncand[(round + 1) & 1] = 0;
-    const int k = c0 + (int)threadIdx.x;
-    if (threadIdx.x < kNmsChunkWords && k < nwords) {
-      const int row = row0 + k / nw;
-      const int wj = wlo + k % nw;
-      const int cbase = wj << 5;
-      uint32_t m = ldx<P>(F.occ + (long long)row * wpr + wj);
-      if (cbase < xlo) m &= ~0u << (xlo - cbase);
-      if (xhi - cbase < 32) m &= (xhi - cbase <= 0) ? 0u : ((xhi - cbase == 32) ? ~0u : ((1u << (xhi - cbase)) - 1u));
-      if (m) {
-        int pos = atomicAdd(cnt, __popc(m));
+  const uint32_t* occ_map = F.occ;
+  const float* score_map = F.vmap;
+  auto g_occ = [=](long long wi) { return ldx<P>(occ_map + wi); };
+  auto g_score = [=](long long wi, uint32_t, int bb) { return ldx<P>(score_map + ((wi << 5) + bb)); };
+
+  for (int k = threadIdx.x; k < nwords; k += blockDim.x) s_sur[k] = 0u;
+
+  // Staged pass 1.  The halo R is the largest window radius present (2^(n_oct-1)),
+  // halved until the strip fits the staging buffer; centres of octaves with a
+  // larger radius read their windows from global memory.
+  int R = 1 << (F.n_oct - 1);
+  while (R >= 1 && (min(F.h, row1 + R + 1) - max(0, row0 - R - 1)) * wpr > kNmsStageWords) R >>= 1;
+  const int srow0 = max(0, row0 - R - 1), srow1 = min(F.h, row1 + R + 1);
+  const int ns = (srow1 - srow0) * wpr;
+  const long long W0 = (long long)srow0 * wpr;  // first staged word
+  bool staged = R >= 1;
+  uint32_t* s_occ = sm.u.w.occ;
+  uint16_t* s_pfx = sm.u.w.pfx;
+  uint16_t* s_idx = sm.u.w.idx;
+  float* s_score = sm.u.w.score;
+  uint8_t* s_oct = sm.u.w.oct;
+  // a staged word, or the global one for a word outside the stage (not reached
+  // for radii up to R; kept so that no index leaves the buffers)
+  auto w_occ = [=](long long wi) {
+    const long long sw = wi - W0;
+    return (sw >= 0 && sw < ns) ? s_occ[sw] : ldx<P>(occ_map + wi);
+  };
+  auto w_score = [=](long long wi, uint32_t word, int bb) {
+    const long long sw = wi - W0;
+    return (sw >= 0 && sw < ns) ? s_score[s_pfx[sw] + __popc(word & ((1u << bb) - 1u))]
+                                : ldx<P>(score_map + ((wi << 5) + bb));
+  };
+  if (staged) {
+    for (int i = threadIdx.x; i < ns; i += blockDim.x) s_occ[i] = ldx<P>(F.occ + W0 + i);
+    __syncthreads();
+    // set bits before each word (contiguous runs of words per thread), and the
+    // list of set bits in raster order
+    const int per = (ns + 255) >> 8;
+    const int beg = min((int)threadIdx.x * per, ns), end = min(beg + per, ns);
+    int local = 0;
+    for (int i = beg; i < end; i++) local += __popc(s_occ[i]);
+    int total;
+    int run = block_scan_excl(local, s_warp_tot, total);
+    if (total <= kNmsStageBits) {
+      for (int i = beg; i < end; i++) {
+        s_pfx[i] = (uint16_t)run;
+        uint32_t m = s_occ[i];
         while (m) {
-          const int bit = __ffs(m) - 1;
+          const int bb = __ffs(m) - 1;
           m &= m - 1u;
-          const long long idx = (long long)row * p0 + cbase + bit;
-          s_cand[pos] = (uint16_t)(((k - c0) << 5) | bit);
-          s_cv[pos] = ldx<P>(F.vmap + idx);
-          s_co[pos] = ldx<P>(F.oct8 + idx);
-          pos++;
+          s_idx[run++] = (uint16_t)((i << 5) | bb);
         }
       }
-    }
-    __syncthreads();
-    const int nc = *cnt;
-    for (int j0 = 0; j0 < nc; j0 += 32 * 8 / kNmsGroup) {
-      const int j = j0 + gid;
-      bool sup = false;
-      int kk = 0, bit = 0;
-      if (j < nc) {
-        const int e = s_cand[j];
-        kk = c0 + (e >> 5);
-        bit = e & 31;
-        const int row = row0 + kk / nw;
-        const int cbase = (wlo + kk % nw) << 5;
-        sup = nms_suppressed_rows<P>(F, (long long)row * p0 + cbase + bit, s_cv[j], s_co[j], p0, npx, sub);
+      if (threadIdx.x == 0) s_pfx[ns] = (uint16_t)total;
+      __syncthreads();
+      // scores and octaves of the set bits, four loads in flight per thread
+      for (int r0 = threadIdx.x; r0 < total; r0 += 4 * blockDim.x) {
+        long long li[4];
+        bool ok[4];
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+          const int r = r0 + q * blockDim.x;
+          ok[q] = r < total;
+          li[q] = (W0 << 5) + (ok[q] ? s_idx[r] : 0);
+        }
+        float v[4];
+        uint8_t o[4];
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+          v[q] = ok[q] ? ldx<P>(F.vmap + li[q]) : 0.f;
+          o[q] = ok[q] ? ldx<P>(F.oct8 + li[q]) : (uint8_t)0;
+        }
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+          if (ok[q]) {
+            s_score[r0 + q * blockDim.x] = v[q];
+            s_oct[r0 + q * blockDim.x] = o[q];
+          }
+        }
       }
-      const uint32_t bal = __ballot_sync(0xffffffffu, sup);
-      if (j < nc && sub == 0 && !(bal & gmask)) atomicOr(&s_sur[kk], 1u << bit);
+      __syncthreads();
+      // the centres are the set bits of the strip's own rows (ranks c_lo ..
+      // c_hi - 1) in columns [xlo, xhi), checked by 32 groups of 8 lanes
+      const int c_lo = s_pfx[(row0 - srow0) * wpr], c_hi = s_pfx[(row1 - srow0) * wpr];
+      for (int j0 = c_lo; j0 < c_hi; j0 += 32 * 8 / kNmsGroup) {
+        const int j = j0 + gid;
+        bool sup = false;
+        int kk = -1, bit = 0;
+        if (j < c_hi) {
+          const int rel = s_idx[j];
+          const int rr = rel / p0, c = rel - rr * p0;
+          if (c >= xlo && c < xhi) {
+            const int row = srow0 + rr;
+            const long long idx = (long long)row * p0 + c;
+            const int o = s_oct[j];
+            sup = (1 << o) <= R ? nms_window_suppressed(idx, s_score[j], o, p0, npx, sub, w_occ, w_score)
+                                : nms_window_suppressed(idx, s_score[j], o, p0, npx, sub, g_occ, g_score);
+            kk = (row - row0) * nw + ((c >> 5) - wlo);
+            bit = c & 31;
+          }
+        }
+        const uint32_t bal = __ballot_sync(0xffffffffu, sup);
+        if (kk >= 0 && sub == 0 && !(bal & gmask)) atomicOr(&s_sur[kk], 1u << bit);
+      }
+    } else {
+      staged = false;
+    }
+  }
+
+  if (!staged) {
+    // pass 1 over global memory, in rounds of kNmsChunkWords words: the centres
+    // of the round (with their scores) are compacted into shared memory, then
+    // checked by 32 groups of 8 lanes, so a textured patch of the strip spreads
+    // over every warp
+    uint16_t* s_cand = sm.u.g.cand;
+    float* s_cv = sm.u.g.cv;
+    uint8_t* s_co = sm.u.g.co;
+    if (threadIdx.x == 0) s_ncand[0] = 0;
+    for (int c0 = 0, round = 0; c0 < nwords; c0 += kNmsChunkWords, round++) {
+      int* cnt = &s_ncand[round & 1];
+      __syncthreads();  // the previous round's checks are done; its counter is free
+      if (threadIdx.x == 0) s_ncand[(round + 1) & 1] = 0;
+      const int k = c0 + (int)threadIdx.x;
+      if (threadIdx.x < kNmsChunkWords && k < nwords) {
+        const int row = row0 + k / nw;
+        const int wj = wlo + k % nw;
+        const int cbase = wj << 5;
+        uint32_t m = ldx<P>(F.occ + (long long)row * wpr + wj);
+        if (cbase < xlo) m &= ~0u << (xlo - cbase);
+        if (xhi - cbase < 32) m &= (xhi - cbase <= 0) ? 0u : ((xhi - cbase == 32) ? ~0u : ((1u << (xhi - cbase)) - 1u));
+        if (m) {
+          int pos = atomicAdd(cnt, __popc(m));
+          while (m) {
+            const int bit = __ffs(m) - 1;
+            m &= m - 1u;
+            const long long idx = (long long)row * p0 + cbase + bit;
+            s_cand[pos] = (uint16_t)(((k - c0) << 5) | bit);
+            s_cv[pos] = ldx<P>(F.vmap + idx);
+            s_co[pos] = ldx<P>(F.oct8 + idx);
+            pos++;
+          }
+        }
+      }
+      __syncthreads();
+      const int nc = *cnt;
+      for (int j0 = 0; j0 < nc; j0 += 32 * 8 / kNmsGroup) {
+        const int j = j0 + gid;
+        bool sup = false;
+        int kk = 0, bit = 0;
+        if (j < nc) {
+          const int e = s_cand[j];
+          kk = c0 + (e >> 5);
+          bit = e & 31;
+          const int row = row0 + kk / nw;
+          const int cbase = (wlo + kk % nw) << 5;
+          sup = nms_window_suppressed((long long)row * p0 + cbase + bit, s_cv[j], s_co[j], p0, npx, sub, g_occ,
+                                      g_score);
+        }
+        const uint32_t bal = __ballot_sync(0xffffffffu, sup);
+        if (j < nc && sub == 0 && !(bal & gmask)) atomicOr(&s_sur[kk], 1u << bit);
+      }
     }
   }
   __syncthreads();
@@ -712,23 +955,12 @@ __device__ __forceinline__ void nms_strip(const Batch& b, int ticket, NmsSmem& s
   const int beg = min((int)threadIdx.x * per, nwords), end = min(beg + per, nwords);
   int local = 0;
   for (int i = beg; i < end; i++) local += __popc(s_sur[i]);
-  int incl = local;
-#pragma unroll
-  for (int d = 1; d < 32; d <<= 1) {
-    const int n = __shfl_up_sync(0xffffffffu, incl, d);
-    if (lane >= d) incl += n;
-  }
-  if (lane == 31) s_warp_tot[warp] = incl;
-  __syncthreads();
-  int warp_off = 0;
-  for (int w2 = 0; w2 < warp; w2++) warp_off += s_warp_tot[w2];
-  int run = warp_off + incl - local;
+  int strip_total;
+  int run = block_scan_excl(local, s_warp_tot, strip_total);
   for (int i = beg; i < end; i++) {
     s_pref[i] = run;
     run += __popc(s_sur[i]);
   }
-  int strip_total = 0;
-  for (int w2 = 0; w2 < 8; w2++) strip_total += s_warp_tot[w2];
 
   // decoupled look-back over the frame's strips (warp 0)
   if (warp == 0) {
@@ -755,12 +987,13 @@ __device__ __forceinline__ void nms_strip(const Batch& b, int ticket, NmsSmem& s
   const int base = s_base;
   if (base >= F.max_pts) return;
 
-  // pass 2: write the survivors
+  // pass 2: write the survivors (score and octave from the stage when staged)
   for (int k = threadIdx.x; k < nwords; k += blockDim.x) {
     uint32_t m = s_sur[k];
     if (!m) continue;
     const int row = row0 + k / nw;
     const int cbase = (wlo + k % nw) << 5;
+    const long long wi = ((long long)row * p0 + cbase) >> 5;
     int rank = base + s_pref[k];
     while (m) {
       const int bit = __ffs(m) - 1;
@@ -770,8 +1003,15 @@ __device__ __forceinline__ void nms_strip(const Batch& b, int ticket, NmsSmem& s
       orbx_point q;
       q.x = cbase + bit;
       q.y = row;
-      q.octave = F.oct8[idx];
-      q.score = F.vmap[idx];
+      if (staged) {
+        const int sw = (int)(wi - W0);
+        const int sr = s_pfx[sw] + __popc(s_occ[sw] & ((1u << bit) - 1u));
+        q.octave = s_oct[sr];
+        q.score = s_score[sr];
+      } else {
+        q.octave = F.oct8[idx];
+        q.score = F.vmap[idx];
+      }
       q.angle = 0.f;
       q.match = 0;
       q.distance = 0;

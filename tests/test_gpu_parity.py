@@ -132,6 +132,35 @@ def test_against_oracle_sizes(ctx, w, h, seed):
             assert same > 0.99
 
 
+@pytest.mark.parametrize("w,h,seed,nms_rows", [(640, 480, 3, 0), (1280, 720, 4, 0), (1280, 720, 4, 16)])
+def test_dense_corners_vs_oracle(ctx, w, h, seed, nms_rows):
+    """Uniform noise in the top half (corners at a large share of its pixels),
+    the synthetic scene below.  NMS strips whose window holds more set bits
+    than its shared-memory stage check their centres in rounds over global
+    memory, the others from the stage; both must give the oracle's keypoints."""
+    img, _, _ = synth.make_pair(w, h, seed)
+    rng = np.random.default_rng(seed)
+    img = img.copy()
+    img[: h // 2] = rng.integers(0, 256, size=(h // 2, img.shape[1]), dtype=np.uint8)
+    cap = w * h // 4
+    ctx.init(orbx.make_params(max_pts=cap))
+    if nms_rows:
+        t = ctx.get_tuning()
+        t.nms_rows = nms_rows
+        ctx.set_tuning(t)
+    pts, desc = run_frame(ctx, img, w, h)
+    ref = O.detect_and_compute(img, w, h, max_pts=cap, sincos=ref_sincos if R.available() else None)
+    rp = ref["points"]
+    assert ref["total"] > 2048  # far more set bits than one strip's stage holds
+    assert len(pts) == len(rp) == ref["total"]
+    for f in ("x", "y", "octave"):
+        assert np.array_equal(pts[f], rp[f]), f
+    assert np.array_equal(f32bits(pts["score"]), f32bits(rp["score"]))
+    assert np.array_equal(f32bits(pts["angle"]), f32bits(rp["angle"]))
+    if R.available():
+        assert np.array_equal(desc, ref["desc"])
+
+
 @pytest.mark.skipif(not R.available(), reason="reference build not present")
 @pytest.mark.parametrize("w,h,seed", [(1920, 1080, 0), (640, 480, 21)])
 def test_against_reference_build_live(ctx, w, h, seed):
@@ -251,6 +280,44 @@ def test_pair_api_matches_single_calls(ctx, mode):
         for f in ("x", "y", "octave"):
             assert np.array_equal(pa[f], sa[f]) and np.array_equal(pb[f], sb[f])
         assert np.array_equal(desc_a, sda) and np.array_equal(desc_b, sdb)
+        m, d = O.match(desc_a, desc_b)
+        assert np.array_equal(pa["match"], m) and np.array_equal(pa["distance"], d)
+
+
+@pytest.mark.parametrize("dependent", [0, 1])
+def test_dependent_launch_same_results(ctx, dependent):
+    """The pair graph with its kernels as programmatic dependent launches (each
+    kernel scheduled while the one before finishes, waiting on the device for
+    its results) and in plain stream order: identical keypoints, descriptors and
+    matches, equal to the oracle's, over repeated graph replays."""
+    w, h = 1920, 1080
+    a, b, _ = synth.make_pair(w, h, 8)
+    ctx.init(orbx.make_params(max_pts=10000))
+    t = ctx.get_tuning()
+    t.dependent_launch = dependent
+    ctx.set_tuning(t)
+    assert ctx.get_tuning().dependent_launch == dependent
+    ref_a = O.detect_and_compute(a, w, h, max_pts=10000, sincos=ref_sincos if R.available() else None)
+    ref_b = O.detect_and_compute(b, w, h, max_pts=10000, sincos=ref_sincos if R.available() else None)
+    da = torch.from_numpy(a).cuda()
+    db = torch.from_numpy(b).cuda()
+    A = orbx.FrameBuffers(10000)
+    B = orbx.FrameBuffers(10000)
+    for _ in range(5):
+        ctx.pair_ptr(da, db, w, h, a.shape[1], A.points, A.desc, A.count, B.points, B.desc, B.count,
+                     orbx.MATCH_POPC)
+        ctx.sync()
+        pa, desc_a = A.to_host()
+        pb, desc_b = B.to_host()
+        for p, ref in ((pa, ref_a), (pb, ref_b)):
+            rp = ref["points"]
+            assert len(p) == len(rp)
+            for f in ("x", "y", "octave"):
+                assert np.array_equal(p[f], rp[f]), f
+            assert np.array_equal(f32bits(p["score"]), f32bits(rp["score"]))
+            assert np.array_equal(f32bits(p["angle"]), f32bits(rp["angle"]))
+        if R.available():
+            assert np.array_equal(desc_a, ref_a["desc"]) and np.array_equal(desc_b, ref_b["desc"])
         m, d = O.match(desc_a, desc_b)
         assert np.array_equal(pa["match"], m) and np.array_equal(pa["distance"], d)
 
