@@ -439,17 +439,14 @@ def run_orbx(args, world, rank, local):
             imma_ms.append(e0.elapsed_time(e1))
     imma_pa, _ = A.to_host()
 
-    # both forms of the device-resident pair: five graph-replayed launches (as
-    # programmatic dependent launches, the default, and in plain stream order)
-    # and one persistent launch with a device work queue
+    # both forms of the device-resident pair: five graph-replayed launches and
+    # one persistent launch with a device work queue
     pair_forms = {}
     keep_t = ctx.get_tuning()
-    for name, form, rows, dep in (("five_launch", 0, 0, 1), ("five_launch_plain_order", 0, 0, 0),
-                                  ("persistent", 1, 0, 1), ("persistent_row_deps", 1, 1, 1)):
+    for name, form, rows in (("five_launch", 0, 0), ("persistent", 1, 0), ("persistent_row_deps", 1, 1)):
         t = ctx.get_tuning()
         t.pair_form = form
         t.persist_row_deps = rows
-        t.dependent_launch = dep
         ctx.set_tuning(t)
         f_ms = []
         with torch.cuda.stream(stream):

@@ -151,7 +151,6 @@ struct orbx_ctx {
   int pyr_shape = 0;     // pyramid tile shape of the five-launch forms (kPyrShapeTW/TH)
   int row_deps = 0;      // persistent launches: detect waits per pyramid tile row, not per frame
   int host_overlap = 0;  // orbx_pair_host: 1 = image B uploads while frame A's kernels run (two streams)
-  int pdl = 1;           // five-launch forms: kernels after the pyramid are programmatic dependent launches
   BatchSlot pair_b;      // frame B's tables for host_overlap
   MatchWork hmw{};       // its matcher scratch
   cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
@@ -469,7 +468,6 @@ static int upload_batch(orbx_ctx* c, BatchSlot& bs, const std::vector<Frame>& fr
   b.nms_ticket = bs.d_ticket;
   b.err = c->d_err;
   b.wait_cycles = c->wait_cycles;
-  b.pdl = c->pdl;
   b.pyr_shape = frames[0].pyr_shape;
   b.fast_thr = c->p.fast_threshold;
   b.harris = c->p.score_type == 0 ? 1 : 0;
@@ -889,7 +887,7 @@ static int launch_match(orbx_ctx* c, MatchWork& mw, const MatchArgs& a, int nq_c
   int rc = mw_ensure(mw, nq_cap);
   if (rc) return rc;
   if (mode == ORBX_MATCH_POPC) {
-    ORBX_CUDA(launch_match_popc(a, mw, c->stream, c->match_bps, c->pdl != 0));
+    ORBX_CUDA(launch_match_popc(a, mw, c->stream, c->match_bps));
     return ORBX_OK;
   }
   if ((rc = imma_ensure(c, nq_cap, ndb_cap)) != 0) return rc;
@@ -1429,7 +1427,6 @@ ORBX_API int orbx_get_tuning(orbx_ctx* c, orbx_tuning* t) {
   t->pyr_tile = c->pyr_shape;
   t->persist_row_deps = c->row_deps;
   t->host_overlap = c->host_overlap;
-  t->dependent_launch = c->pdl;
   return ORBX_OK;
 }
 
@@ -1442,7 +1439,7 @@ ORBX_API int orbx_set_tuning(orbx_ctx* c, const orbx_tuning* t) {
       t->persist_blocks_per_sm > 32 || t->wait_timeout_us < 1 || t->wait_timeout_us > 10000000 ||
       t->upload_bands < 0 || t->upload_bands > 16 || t->pair_form < 0 || t->pair_form > 1 ||
       t->pyr_tile < 0 || t->pyr_tile >= kPyrShapes || t->persist_row_deps < 0 || t->persist_row_deps > 1 ||
-      t->host_overlap < 0 || t->host_overlap > 1 || t->dependent_launch < 0 || t->dependent_launch > 1)
+      t->host_overlap < 0 || t->host_overlap > 1)
     return ORBX_ERR_ARG;
   c->nms_rows = t->nms_rows;
   c->describe_bps = t->describe_blocks_per_sm;
@@ -1457,7 +1454,6 @@ ORBX_API int orbx_set_tuning(orbx_ctx* c, const orbx_tuning* t) {
   c->pyr_shape = t->pyr_tile;
   c->row_deps = t->persist_row_deps;
   c->host_overlap = t->host_overlap;
-  c->pdl = t->dependent_launch;
   c->wait_cycles = (long long)c->wait_us * c->clock_khz / 1000;
   if (c->batch_exec) {
     cudaGraphExecDestroy(c->batch_exec);

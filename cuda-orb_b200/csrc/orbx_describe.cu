@@ -17,14 +17,6 @@ __global__ void __launch_bounds__(kDescWarps * 32) k_describe(Batch b) {
   __shared__ int s_wsum[kDescWarps];
   const int lane = threadIdx.x & 31;
   const int nf = b.n_frames;
-  // pattern points and the disc table (set at init) before waiting for NMS's counts
-  constexpr int PSTEP = (WTA == 3) ? 12 : 16;
-  float px[PSTEP], py[PSTEP];
-  load_pattern<WTA>(b, lane, px, py);
-  const int half_k = b.half_k;
-  if (threadIdx.x < half_k + 1) s_umax[threadIdx.x] = b.umax[threadIdx.x];
-  pdl_wait();
-  pdl_launch_dependents();
   // exclusive prefix of the per-frame keypoint counts (written by k_nms):
   // thread t scans frames [t*per, (t+1)*per)
   {
@@ -48,8 +40,14 @@ __global__ void __launch_bounds__(kDescWarps * 32) k_describe(Batch b) {
     }
     if (threadIdx.x == kDescWarps * 32 - 1) s_pref[nf] = run;
   }
+  const int half_k = b.half_k;
+  if (threadIdx.x < half_k + 1) s_umax[threadIdx.x] = b.umax[threadIdx.x];
   __syncthreads();
   const int total = s_pref[nf];
+
+  constexpr int PSTEP = (WTA == 3) ? 12 : 16;
+  float px[PSTEP], py[PSTEP];
+  load_pattern<WTA>(b, lane, px, py);
 
   const int gw = blockIdx.x * kDescWarps + (threadIdx.x >> 5);
   const int nw = gridDim.x * kDescWarps;
@@ -72,10 +70,13 @@ cudaError_t launch_describe(const Batch& b, int total_max_pts, cudaStream_t s, i
   int blocks = (warps_needed + kDescWarps - 1) / kDescWarps;
   const int cap = 148 * (blocks_per_sm > 0 ? blocks_per_sm : 8);
   if (blocks > cap) blocks = cap;
-  const bool dep = b.pdl != 0;
-  if (b.wta_k == 3) return launch_kernel(k_describe<3>, dim3(blocks), dim3(kDescWarps * 32), s, dep, b);
-  if (b.wta_k == 4) return launch_kernel(k_describe<4>, dim3(blocks), dim3(kDescWarps * 32), s, dep, b);
-  return launch_kernel(k_describe<2>, dim3(blocks), dim3(kDescWarps * 32), s, dep, b);
+  if (b.wta_k == 3)
+    k_describe<3><<<blocks, kDescWarps * 32, 0, s>>>(b);
+  else if (b.wta_k == 4)
+    k_describe<4><<<blocks, kDescWarps * 32, 0, s>>>(b);
+  else
+    k_describe<2><<<blocks, kDescWarps * 32, 0, s>>>(b);
+  return cudaGetLastError();
 }
 
 }  // namespace orbx

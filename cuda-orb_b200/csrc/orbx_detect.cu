@@ -11,33 +11,19 @@ namespace orbx {
 template <int TW, int TH>
 __global__ void __launch_bounds__(256, 4) k_pyramid_blur(Batch b) {
   __shared__ PyrSmem<TW, TH> sm;
-  pdl_launch_dependents();  // the detect grid may be scheduled; it waits for this one
   pyr_tile<false, TW, TH>(b, blockIdx.x, sm);
 }
 
 __global__ void __launch_bounds__(256, 4) k_detect(Batch b) {
   __shared__ DetSmem sm;
-  pdl_wait();
-  pdl_launch_dependents();
   det_tile<false>(b, blockIdx.x, sm);
 }
 
 __global__ void __launch_bounds__(256, 4) k_nms(Batch b) {
   __shared__ NmsSmem sm;
   __shared__ int s_ticket;
-  // The ticket counter and look-back words were reset by the pyramid kernel.
-  // As a dependent launch this grid is scheduled only after every detect block
-  // has passed its own wait, i.e. after the pyramid kernel has completed, so the
-  // ticket and the frame descriptor are fetched before the wait for detect.
   if (threadIdx.x == 0) s_ticket = (int)atomicAdd(b.nms_ticket, 1u);
   __syncthreads();
-  {
-    const Frame* fr = b.frames + find_frame(b.nms_base, b.n_frames, s_ticket);
-    if (threadIdx.x * 128 < sizeof(Frame))
-      asm volatile("prefetch.global.L1 [%0];" ::"l"(reinterpret_cast<const char*>(fr) + threadIdx.x * 128));
-  }
-  pdl_wait();
-  pdl_launch_dependents();
   nms_strip<false>(b, s_ticket, sm);
 }
 
@@ -80,12 +66,14 @@ cudaError_t launch_pyramid_blur(const Batch& b, int total_tiles, cudaStream_t s)
 
 cudaError_t launch_detect(const Batch& b, int total_tiles, cudaStream_t s) {
   if (total_tiles <= 0) return cudaSuccess;
-  return launch_kernel(k_detect, dim3(total_tiles), dim3(256), s, b.pdl != 0, b);
+  k_detect<<<total_tiles, 256, 0, s>>>(b);
+  return cudaGetLastError();
 }
 
 cudaError_t launch_nms(const Batch& b, int total_strips, cudaStream_t s) {
   if (total_strips <= 0) return cudaSuccess;
-  return launch_kernel(k_nms, dim3(total_strips), dim3(256), s, b.pdl != 0, b);
+  k_nms<<<total_strips, 256, 0, s>>>(b);
+  return cudaGetLastError();
 }
 
 }  // namespace orbx

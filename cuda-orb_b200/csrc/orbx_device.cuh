@@ -95,30 +95,16 @@ __device__ __forceinline__ float fast_atan2(float y, float x) {
   return r;
 }
 
-__device__ __forceinline__ void st_release_u64(unsigned long long* p, unsigned long long v) {
-  asm volatile("st.release.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
-}
-
-// Programmatic dependent launch.  pdl_wait: when this grid was launched as a
-// dependent of the previous kernel of its stream, wait until that kernel has
-// completed and its memory operations are visible (returns at once otherwise).
-// pdl_launch_dependents: the next kernel of the stream may be scheduled once
-// every block of this grid has issued it or exited.
-__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
-__device__ __forceinline__ void pdl_launch_dependents() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
-
-// Strong relaxed load (read at the device's coherence point, no ordering of
-// later accesses), for words that carry all the data their reader needs.
+// Strong relaxed load and store (at the device's coherence point, no ordering
+// of other accesses), for words that carry all the data their reader needs.
 __device__ __forceinline__ unsigned long long ld_relaxed_u64(const unsigned long long* p) {
   unsigned long long v;
   asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p));
   return v;
 }
 
-__device__ __forceinline__ unsigned long long ld_acquire_u64(const unsigned long long* p) {
-  unsigned long long v;
-  asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
-  return v;
+__device__ __forceinline__ void st_relaxed_u64(unsigned long long* p, unsigned long long v) {
+  asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
 }
 
 // Index of the frame whose tile range [base[f], base[f+1]) holds t.

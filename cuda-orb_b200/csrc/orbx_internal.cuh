@@ -67,7 +67,6 @@ struct Batch {
   unsigned int* nms_ticket;  // dynamic strip ticket (reset by k_pyramid_blur)
   int* err;              // sticky error word (bounded waits that gave up)
   long long wait_cycles; // bound of every device-side wait, in SM clock cycles
-  int pdl;               // launch detect, NMS and describe as programmatic dependents of the kernel before
   int pyr_shape;         // pyramid tile shape of every frame of the launch
   int describe_mode;     // 0: angle + descriptor, 1: angle only, 2: descriptor only
   // parameters (Orbor::init, orb.h:18-19)
@@ -90,27 +89,6 @@ enum : int { kDescribeBoth = 0, kDescribeAngleOnly = 1, kDescribeDescOnly = 2 };
 
 // host-side helpers implemented in orbx_api.cu
 }  // namespace orbx
-
-// Kernel launch on stream s.  dependent: programmatic stream serialization,
-// so the grid may be scheduled while the previous kernel of the stream runs
-// its last blocks; the kernel then waits for that kernel's results on the
-// device (pdl_wait).  Without a kernel before it in the stream it is an
-// ordinary launch.
-template <typename... P, typename... A>
-inline cudaError_t launch_kernel(void (*k)(P...), dim3 grid, dim3 block, cudaStream_t s, bool dependent,
-                                 A&&... args) {
-  cudaLaunchConfig_t cfg = {};
-  cfg.gridDim = grid;
-  cfg.blockDim = block;
-  cfg.dynamicSmemBytes = 0;
-  cfg.stream = s;
-  cudaLaunchAttribute at[1];
-  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
-  at[0].val.programmaticStreamSerializationAllowed = 1;
-  cfg.attrs = at;
-  cfg.numAttrs = dependent ? 1 : 0;
-  return cudaLaunchKernelEx(&cfg, k, static_cast<A&&>(args)...);
-}
 
 // kernel launchers (orbx_detect.cu / orbx_describe.cu / orbx_match.cu)
 namespace orbx {
@@ -227,8 +205,7 @@ int lower_blur(orbx_ctx* c, uint8_t* octave_images, const int* oszp, int noctave
 int lower_last_layout(orbx_ctx* c, int* oszp, int noctaves);
 int lower_describe(orbx_ctx* c, const uint8_t* octave_images, orbx_point* pts, int n_pts, uint8_t* desc, int wta_k,
                    const int* oszp, int noctaves, int* d_tmp_count);
-cudaError_t launch_match_popc(const MatchArgs& a, const MatchWork& w, cudaStream_t s, int blocks_per_sm = 8,
-                              bool dependent = false);
+cudaError_t launch_match_popc(const MatchArgs& a, const MatchWork& w, cudaStream_t s, int blocks_per_sm = 8);
 
 // one matching job of a batch (one frame pair)
 struct MatchJob {

@@ -15,8 +15,6 @@ namespace orbx {
 __global__ void __launch_bounds__(kMQ) k_match_popc(MatchArgs a, MatchWork w) {
   __shared__ uint4 s_db[kMChunk * 2];
   __shared__ unsigned int s_last;
-  pdl_wait();
-  pdl_launch_dependents();
   match_popc_block<kMQ, false>(a, w, blockIdx.x, gridDim.x, s_db, s_last);
 }
 
@@ -36,11 +34,10 @@ int match_popc_blocks(int nq_cap, int splits_cap, int blocks_per_sm) {
   return (int)blocks;
 }
 
-cudaError_t launch_match_popc(const MatchArgs& a, const MatchWork& w, cudaStream_t s, int blocks_per_sm,
-                              bool dependent) {
+cudaError_t launch_match_popc(const MatchArgs& a, const MatchWork& w, cudaStream_t s, int blocks_per_sm) {
   if (w.nq_cap <= 0) return cudaSuccess;
-  return launch_kernel(k_match_popc, dim3(match_popc_blocks(w.nq_cap, w.splits_cap, blocks_per_sm)), dim3(kMQ), s,
-                       dependent, a, w);
+  k_match_popc<<<match_popc_blocks(w.nq_cap, w.splits_cap, blocks_per_sm), kMQ, 0, s>>>(a, w);
+  return cudaGetLastError();
 }
 
 cudaError_t launch_match_popc_batch(const MatchJob* d_jobs, int n_jobs, int blocks_per_job, cudaStream_t s) {

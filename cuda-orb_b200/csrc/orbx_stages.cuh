@@ -609,13 +609,19 @@ constexpr unsigned long long kFlagAgg = 1ull << 32;
 constexpr unsigned long long kFlagPre = 2ull << 32;
 constexpr int kLookPerLane = 8;  // look-back words read per lane and round: 256 predecessors
 
-// Warp 0 of a strip's block resolves the strip's exclusive prefix: in each round
-// lane l reads the look-back words of predecessors j - 8l .. j - 8l - 7, and the
-// warp stops at the nearest predecessor that already carries an inclusive
-// prefix.  A look-back word holds its flag and its count together and nothing
-// else is read on its strength, so relaxed loads suffice, and the eight of a
-// lane are in flight together (acquire loads would run one after another).  The wait for a
-// predecessor is bounded by wait_cycles of clock64(); on expiry it sets
+// Warp 0 of a strip's block resolves the strip's exclusive prefix.  In each
+// round lane l reads the look-back words of predecessors j - l - 32u, u = 0..7
+// (each of the eight loads is 32 consecutive words, so a round touches 64
+// sectors), and the warp stops at the nearest predecessor that already carries
+// an inclusive prefix.  A look-back word holds its flag and its count together
+// and nothing else is read on its strength, so plain relaxed loads and stores
+// suffice (a release store would wait for a fence).  A published word only ever
+// changes from an aggregate to an inclusive prefix of the same strip, and
+// summing aggregates back to any prefix gives the same total, so words already
+// seen published are kept and only the pending ones are read again, after a
+// back-off that doubles from 32 ns to 1 us: the words of a frame share a few
+// L2 sectors, and a store to them completes only after the reads queued there.
+// The wait is bounded by wait_cycles of clock64(); on expiry it sets
 // kErrLookbackTimeout and returns the prefix found so far.
 __device__ __forceinline__ int nms_lookback(unsigned long long* st, int s, int lane, int* err,
                                             long long wait_cycles) {
@@ -626,40 +632,58 @@ __device__ __forceinline__ int nms_lookback(unsigned long long* st, int s, int l
     unsigned long long wv[kLookPerLane];
 #pragma unroll
     for (int u = 0; u < kLookPerLane; u++) {
-      const int idx = j - lane * kLookPerLane - u;
+      const int idx = j - lane - 32 * u;
       wv[u] = (idx >= 0) ? ld_relaxed_u64(&st[idx]) : kFlagPre;
     }
-    // this lane's nearest inclusive prefix, then the warp's
-    int first_u = kLookPerLane;
+    unsigned sleep_ns = 32;
+    bool timed_out = false;
+    for (;;) {
+      // the nearest inclusive prefix: smallest distance lane + 32u
+      int first_u = kLookPerLane, first_lane = 32;
 #pragma unroll
-    for (int u = kLookPerLane - 1; u >= 0; u--)
-      if ((wv[u] & (3ull << 32)) == kFlagPre) first_u = u;
-    const unsigned pre = __ballot_sync(0xffffffffu, first_u < kLookPerLane);
-    const int first_lane = pre ? (__ffs(pre) - 1) : 32;
-    // words up to and including that prefix must all be published
-    bool notready = false;
-    int v = 0;
-#pragma unroll
-    for (int u = 0; u < kLookPerLane; u++) {
-      const bool need = lane < first_lane || (lane == first_lane && u <= first_u);
-      if (need) {
-        notready |= (wv[u] & (3ull << 32)) == 0ull;
-        v += (int)(unsigned)wv[u];
+      for (int u = kLookPerLane - 1; u >= 0; u--) {
+        const unsigned pre = __ballot_sync(0xffffffffu, (wv[u] & (3ull << 32)) == kFlagPre);
+        if (pre) {
+          first_u = u;
+          first_lane = __ffs(pre) - 1;
+        }
       }
-    }
-    if (__any_sync(0xffffffffu, notready)) {
-      if (clock64() - t0 > wait_cycles) {
-        if (lane == 0) atomicOr(err, kErrLookbackTimeout);
+      // words up to and including that prefix must all be published
+      bool notready = false;
+#pragma unroll
+      for (int u = 0; u < kLookPerLane; u++) {
+        const bool need = u < first_u || (u == first_u && lane <= first_lane);
+        if (need && (wv[u] & (3ull << 32)) == 0ull) notready = true;
+      }
+      if (!__any_sync(0xffffffffu, notready)) {
+        int v = 0;
+#pragma unroll
+        for (int u = 0; u < kLookPerLane; u++) {
+          const bool need = u < first_u || (u == first_u && lane <= first_lane);
+          if (need) v += (int)(unsigned)wv[u];
+        }
+#pragma unroll
+        for (int d = 16; d >= 1; d >>= 1) v += __shfl_xor_sync(0xffffffffu, v, d);
+        excl += v;
+        j = (first_u < kLookPerLane) ? -1 : j - 32 * kLookPerLane;
         break;
       }
-      __nanosleep(20);
-      continue;
-    }
+      if (__any_sync(0xffffffffu, clock64() - t0 > wait_cycles)) {  // warp-uniform decision
+        timed_out = true;
+        break;
+      }
+      __nanosleep(sleep_ns);
+      if (sleep_ns < 1024) sleep_ns <<= 1;
 #pragma unroll
-    for (int d = 16; d >= 1; d >>= 1) v += __shfl_xor_sync(0xffffffffu, v, d);
-    excl += v;
-    if (first_lane < 32) break;
-    j -= 32 * kLookPerLane;
+      for (int u = 0; u < kLookPerLane; u++) {
+        const int idx = j - lane - 32 * u;
+        if (idx >= 0 && (wv[u] & (3ull << 32)) == 0ull) wv[u] = ld_relaxed_u64(&st[idx]);
+      }
+    }
+    if (timed_out) {
+      if (lane == 0) atomicOr(err, kErrLookbackTimeout);
+      break;
+    }
   }
   return excl;
 }
@@ -967,12 +991,12 @@ __device__ __forceinline__ void nms_strip(const Batch& b, int ticket, NmsSmem& s
     unsigned long long* st = F.nms_status;
     int excl = 0;
     if (s == 0) {
-      if (lane == 0) st_release_u64(&st[0], kFlagPre | (unsigned)strip_total);
+      if (lane == 0) st_relaxed_u64(&st[0], kFlagPre | (unsigned)strip_total);
     } else {
-      if (lane == 0) st_release_u64(&st[s], kFlagAgg | (unsigned)strip_total);
+      if (lane == 0) st_relaxed_u64(&st[s], kFlagAgg | (unsigned)strip_total);
       __syncwarp();
       excl = nms_lookback(st, s, lane, b.err, b.wait_cycles);
-      if (lane == 0) st_release_u64(&st[s], kFlagPre | (unsigned)(excl + strip_total));
+      if (lane == 0) st_relaxed_u64(&st[s], kFlagPre | (unsigned)(excl + strip_total));
     }
     if (lane == 0) {
       s_base = excl;

@@ -55,8 +55,7 @@ class Tuning(ctypes.Structure):
                 ("batch_form", ctypes.c_int), ("persist_group", ctypes.c_int),
                 ("persist_blocks_per_sm", ctypes.c_int), ("wait_timeout_us", ctypes.c_int),
                 ("upload_bands", ctypes.c_int), ("pair_form", ctypes.c_int), ("pyr_tile", ctypes.c_int),
-                ("persist_row_deps", ctypes.c_int), ("host_overlap", ctypes.c_int),
-                ("dependent_launch", ctypes.c_int)]
+                ("persist_row_deps", ctypes.c_int), ("host_overlap", ctypes.c_int)]
 
     def as_dict(self):
         return {f: int(getattr(self, f)) for f, _ in self._fields_}

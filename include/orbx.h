@@ -249,9 +249,6 @@ typedef struct orbx_tuning {
   int host_overlap;           /* orbx_pair_host with upload_bands = 0: 1 = image B is copied while frame A's
                                  kernels run (the frames on two streams, popcount matching), 0 = copy both,
                                  then run the pair */
-  int dependent_launch;       /* five-launch forms: 1 (default) = each kernel after the pyramid is a programmatic
-                                 dependent launch of the one before (it is scheduled while that kernel's last
-                                 blocks run and waits on the device for their results), 0 = plain stream order */
 } orbx_tuning;
 
 ORBX_API int orbx_get_tuning(orbx_ctx* ctx, orbx_tuning* t);

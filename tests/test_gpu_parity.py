@@ -284,44 +284,6 @@ def test_pair_api_matches_single_calls(ctx, mode):
         assert np.array_equal(pa["match"], m) and np.array_equal(pa["distance"], d)
 
 
-@pytest.mark.parametrize("dependent", [0, 1])
-def test_dependent_launch_same_results(ctx, dependent):
-    """The pair graph with its kernels as programmatic dependent launches (each
-    kernel scheduled while the one before finishes, waiting on the device for
-    its results) and in plain stream order: identical keypoints, descriptors and
-    matches, equal to the oracle's, over repeated graph replays."""
-    w, h = 1920, 1080
-    a, b, _ = synth.make_pair(w, h, 8)
-    ctx.init(orbx.make_params(max_pts=10000))
-    t = ctx.get_tuning()
-    t.dependent_launch = dependent
-    ctx.set_tuning(t)
-    assert ctx.get_tuning().dependent_launch == dependent
-    ref_a = O.detect_and_compute(a, w, h, max_pts=10000, sincos=ref_sincos if R.available() else None)
-    ref_b = O.detect_and_compute(b, w, h, max_pts=10000, sincos=ref_sincos if R.available() else None)
-    da = torch.from_numpy(a).cuda()
-    db = torch.from_numpy(b).cuda()
-    A = orbx.FrameBuffers(10000)
-    B = orbx.FrameBuffers(10000)
-    for _ in range(5):
-        ctx.pair_ptr(da, db, w, h, a.shape[1], A.points, A.desc, A.count, B.points, B.desc, B.count,
-                     orbx.MATCH_POPC)
-        ctx.sync()
-        pa, desc_a = A.to_host()
-        pb, desc_b = B.to_host()
-        for p, ref in ((pa, ref_a), (pb, ref_b)):
-            rp = ref["points"]
-            assert len(p) == len(rp)
-            for f in ("x", "y", "octave"):
-                assert np.array_equal(p[f], rp[f]), f
-            assert np.array_equal(f32bits(p["score"]), f32bits(rp["score"]))
-            assert np.array_equal(f32bits(p["angle"]), f32bits(rp["angle"]))
-        if R.available():
-            assert np.array_equal(desc_a, ref_a["desc"]) and np.array_equal(desc_b, ref_b["desc"])
-        m, d = O.match(desc_a, desc_b)
-        assert np.array_equal(pa["match"], m) and np.array_equal(pa["distance"], d)
-
-
 def test_determinism_repeat(ctx):
     w, h = 1920, 1080
     a, _, _ = synth.make_pair(w, h, 1)
