@@ -124,7 +124,7 @@ struct orbx_ctx {
   OcvWork* ocv = nullptr;    // orbx_ocv_detect_and_compute workspace
   // launch shapes (orbx_tuning)
   int nms_rows = kNmsRows;
-  int describe_bps = 8;
+  int describe_bps = 4;  // one wave: 64 registers x 256 threads leave room for 4 blocks per SM
   int match_bps = 8;
   int match_blocks_per_pair = 0;
   // batched pairs
@@ -1403,9 +1403,9 @@ ORBX_API int orbx_profile_pair(orbx_ctx* c, const uint8_t* d_img_a, const uint8_
   ORBX_CUDA(cudaEventRecord(c->prof_ev[2], c->stream));
   ORBX_CUDA(launch_nms(pl.b, pl.nms_strips, c->stream));
   ORBX_CUDA(cudaEventRecord(c->prof_ev[3], c->stream));
-  ORBX_CUDA(launch_describe(pl.b, pl.total_max_pts, c->stream));
+  ORBX_CUDA(launch_describe(pl.b, pl.total_max_pts, c->stream, c->describe_bps));
   ORBX_CUDA(cudaEventRecord(c->prof_ev[4], c->stream));
-  ORBX_CUDA(launch_match_popc(a, c->mw, c->stream));
+  ORBX_CUDA(launch_match_popc(a, c->mw, c->stream, c->match_bps));
   ORBX_CUDA(cudaEventRecord(c->prof_ev[5], c->stream));
   ORBX_CUDA(cudaEventSynchronize(c->prof_ev[5]));
   for (int i = 0; i < 5; i++) ORBX_CUDA(cudaEventElapsedTime(&stage_ms[i], c->prof_ev[i], c->prof_ev[i + 1]));
@@ -1824,7 +1824,7 @@ ORBX_API int orbx_autotune_pairs_forms(orbx_ctx* c, int n_pairs, const orbx_imag
   std::vector<orbx_tuning> cands;
   if (forms & 1)
   for (int r : {2, 4, 8, 16})
-    for (int d : {4, 8, 16})
+    for (int d : {3, 4, 8})
       for (int m : {0, 64, 256}) {
         orbx_tuning t = keep;
         t.batch_form = 0;

@@ -17,6 +17,15 @@ __global__ void __launch_bounds__(kDescWarps * 32) k_describe(Batch b) {
   __shared__ int s_wsum[kDescWarps];
   const int lane = threadIdx.x & 31;
   const int nf = b.n_frames;
+  // set at init: the pattern words (in flight while the counts are read) and
+  // the disc table; the frame descriptors are pulled into L1 for the keypoints
+  const PatternRaw<WTA> praw = load_pattern_raw<WTA>(b, lane);
+  const int half_k = b.half_k;
+  if (threadIdx.x < half_k + 1) s_umax[threadIdx.x] = b.umax[threadIdx.x];
+  constexpr int kFrameLines = (int)((sizeof(Frame) + 127) / 128);
+  if (nf <= 8 && (int)threadIdx.x < nf * kFrameLines)
+    asm volatile("prefetch.global.L1 [%0];" ::"l"(reinterpret_cast<const char*>(b.frames + threadIdx.x / kFrameLines) +
+                                                  128 * (threadIdx.x % kFrameLines)));
   // exclusive prefix of the per-frame keypoint counts (written by k_nms):
   // thread t scans frames [t*per, (t+1)*per)
   {
@@ -40,14 +49,12 @@ __global__ void __launch_bounds__(kDescWarps * 32) k_describe(Batch b) {
     }
     if (threadIdx.x == kDescWarps * 32 - 1) s_pref[nf] = run;
   }
-  const int half_k = b.half_k;
-  if (threadIdx.x < half_k + 1) s_umax[threadIdx.x] = b.umax[threadIdx.x];
   __syncthreads();
   const int total = s_pref[nf];
 
-  constexpr int PSTEP = (WTA == 3) ? 12 : 16;
+  constexpr int PSTEP = PatternRaw<WTA>::PSTEP;
   float px[PSTEP], py[PSTEP];
-  load_pattern<WTA>(b, lane, px, py);
+  pattern_points<WTA>(praw, px, py);
 
   const int gw = blockIdx.x * kDescWarps + (threadIdx.x >> 5);
   const int nw = gridDim.x * kDescWarps;

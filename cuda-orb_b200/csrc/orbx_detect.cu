@@ -9,7 +9,7 @@
 namespace orbx {
 
 template <int TW, int TH>
-__global__ void __launch_bounds__(256, 4) k_pyramid_blur(Batch b) {
+__global__ void __launch_bounds__(kPyrThreads, 4) k_pyramid_blur(Batch b) {
   __shared__ PyrSmem<TW, TH> sm;
   pyr_tile<false, TW, TH>(b, blockIdx.x, sm);
 }
@@ -50,16 +50,16 @@ cudaError_t launch_pyramid_blur(const Batch& b, int total_tiles, cudaStream_t s)
   if (total_tiles <= 0) return cudaSuccess;
   switch (b.pyr_shape) {
     case 1:
-      k_pyramid_blur<kPyrShapeTW[1], kPyrShapeTH[1]><<<total_tiles, 256, 0, s>>>(b);
+      k_pyramid_blur<kPyrShapeTW[1], kPyrShapeTH[1]><<<total_tiles, kPyrThreads, 0, s>>>(b);
       break;
     case 2:
-      k_pyramid_blur<kPyrShapeTW[2], kPyrShapeTH[2]><<<total_tiles, 256, 0, s>>>(b);
+      k_pyramid_blur<kPyrShapeTW[2], kPyrShapeTH[2]><<<total_tiles, kPyrThreads, 0, s>>>(b);
       break;
     case 3:
-      k_pyramid_blur<kPyrShapeTW[3], kPyrShapeTH[3]><<<total_tiles, 256, 0, s>>>(b);
+      k_pyramid_blur<kPyrShapeTW[3], kPyrShapeTH[3]><<<total_tiles, kPyrThreads, 0, s>>>(b);
       break;
     default:
-      k_pyramid_blur<kPyrShapeTW[0], kPyrShapeTH[0]><<<total_tiles, 256, 0, s>>>(b);
+      k_pyramid_blur<kPyrShapeTW[0], kPyrShapeTH[0]><<<total_tiles, kPyrThreads, 0, s>>>(b);
   }
   return cudaGetLastError();
 }

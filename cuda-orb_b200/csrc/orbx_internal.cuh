@@ -14,6 +14,7 @@ constexpr size_t kGuard = 256 * 1024; // zeroed bytes before/after each pyramid
 // Pyramid-and-blur tile (octave pixels): the default shape, which the
 // persistent kernel uses; the five-launch kernel also has the other shapes of
 // kPyrShapeTW/TH (tuning pyr_tile), one instantiation each
+constexpr int kPyrThreads = 256;  // threads of every block that runs pyramid tiles
 constexpr int kPyrTW = 128;
 constexpr int kPyrTH = 32;
 constexpr int kPyrShapes = 4;

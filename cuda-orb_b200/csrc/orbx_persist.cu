@@ -44,6 +44,7 @@ union PersistSmem {
 };
 
 constexpr int kPersistThreads = 256;
+static_assert(kPersistThreads == kPyrThreads, "pyramid tiles assume kPyrThreads threads per block");
 
 // One thread waits until *ctr >= need (acquire), bounded by wait_cycles.
 // After one wait has given up, later waits return at once so the launch drains.

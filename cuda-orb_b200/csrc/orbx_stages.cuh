@@ -71,15 +71,14 @@ __device__ __forceinline__ uint32_t pyr_stage_word(const uint8_t* rowp, int cx, 
   return pack_low_bytes(v[0], v[1], v[2], v[3]);
 }
 // Row-major walk over items (r, g) with W items per row: item threadIdx.x +
-// k * blockDim.x for k = 0, 1, .., stepped without a division per step.
-template <int W>
+// k * T for k = 0, 1, .. in a block of T threads, stepped without a division.
+template <int W, int T>
 struct RowWalk {
-  int r, g, dr, dg;
-  __device__ __forceinline__ RowWalk()
-      : r(threadIdx.x / W), g(threadIdx.x % W), dr(blockDim.x / W), dg(blockDim.x % W) {}
+  int r, g;
+  __device__ __forceinline__ RowWalk() : r(threadIdx.x / W), g(threadIdx.x % W) {}
   __device__ __forceinline__ void next() {
-    r += dr;
-    g += dg;
+    r += T / W;
+    g += T % W;
     if (g >= W) {
       g -= W;
       r++;
@@ -150,25 +149,42 @@ __device__ __forceinline__ void pyr_tile(const Batch& b, int t, PyrSmem<TW, TH>&
   const int sh = psrc ? 0 : o;
   constexpr int kGroups = S::SW2 / 4;  // staging items per row = slots per plane of a staged row
   const float2 m23 = pair2(-8388608.0f);
-  for (RowWalk<kGroups> w; w.r < kSH; w.next()) {
+  // all of a thread's staging loads are issued before any is used (one round
+  // trip per tile instead of one per item); blocks have kPyrThreads threads
+  constexpr int kStageItems = (kSH * kGroups + kPyrThreads - 1) / kPyrThreads;
+  uint32_t wa[kStageItems], wb[kStageItems];
+  {
+    RowWalk<kGroups, kPyrThreads> w;
+#pragma unroll
+    for (int q = 0; q < kStageItems; q++) {
+      wa[q] = wb[q] = 0u;
+      if (w.r < kSH) {
+        const int y = reflect101(y0 - 3 + w.r, oh);
+        const uint8_t* rowp = psrc ? psrc + (size_t)y * op : img + (size_t)(y << o) * pitch_in;
+        const int cx = x0 - 3 + 4 * w.g;
+        wa[q] = pyr_stage_word<PL>(rowp, cx, ow, sh, words0);
+        wb[q] = pyr_stage_word<PL>(rowp, cx + kHW, ow, sh, words0);
+      }
+      w.next();
+    }
+  }
+  RowWalk<kGroups, kPyrThreads> w;
+#pragma unroll
+  for (int q = 0; q < kStageItems; q++, w.next()) {
     const int r = w.r, g = w.g;
-    const int y = reflect101(y0 - 3 + r, oh);
-    const uint8_t* rowp = psrc ? psrc + (size_t)y * op : img + (size_t)(y << o) * pitch_in;
-    const int cx = x0 - 3 + 4 * g;
-    const uint32_t wa = pyr_stage_word<PL>(rowp, cx, ow, sh, words0);
-    const uint32_t wb = pyr_stage_word<PL>(rowp, cx + kHW, ow, sh, words0);
+    if (r >= kSH) break;
     // pair j = (byte j of wa, byte j of wb) as floats: 2^23 + byte, minus 2^23
-    const float2 p0 = __fadd2_rn(make_float2(byte_bits(wa, 0x7540u), byte_bits(wb, 0x7540u)), m23);
-    const float2 p1 = __fadd2_rn(make_float2(byte_bits(wa, 0x7541u), byte_bits(wb, 0x7541u)), m23);
-    const float2 p2 = __fadd2_rn(make_float2(byte_bits(wa, 0x7542u), byte_bits(wb, 0x7542u)), m23);
-    const float2 p3 = __fadd2_rn(make_float2(byte_bits(wa, 0x7543u), byte_bits(wb, 0x7543u)), m23);
+    const float2 p0 = __fadd2_rn(make_float2(byte_bits(wa[q], 0x7540u), byte_bits(wb[q], 0x7540u)), m23);
+    const float2 p1 = __fadd2_rn(make_float2(byte_bits(wa[q], 0x7541u), byte_bits(wb[q], 0x7541u)), m23);
+    const float2 p2 = __fadd2_rn(make_float2(byte_bits(wa[q], 0x7542u), byte_bits(wb[q], 0x7542u)), m23);
+    const float2 p3 = __fadd2_rn(make_float2(byte_bits(wa[q], 0x7543u), byte_bits(wb[q], 0x7543u)), m23);
     // pairs 4g .. 4g+3 = slots 2g (even plane) and 2g+1 (odd plane) of row r
     float4* row = s_src + r * kRowSlots + g;
     row[0] = make_float4(p0.x, p0.y, p1.x, p1.y);
     row[kGroups] = make_float4(p2.x, p2.y, p3.x, p3.y);
     // the halves' halos overlap in the middle: both writes there store the same bytes
-    *reinterpret_cast<uint32_t*>(s_byte + r * kSW + 4 * g) = wa;
-    *reinterpret_cast<uint32_t*>(s_byte + r * kSW + kHW + 4 * g) = wb;
+    *reinterpret_cast<uint32_t*>(s_byte + r * kSW + 4 * g) = wa[q];
+    *reinterpret_cast<uint32_t*>(s_byte + r * kSW + kHW + 4 * g) = wb[q];
   }
   __syncthreads();
 
@@ -178,7 +194,7 @@ __device__ __forceinline__ void pyr_tile(const Batch& b, int t, PyrSmem<TW, TH>&
   // horizontal pass: 4 consecutive output pairs per thread; integer tap sums
   // are exact in float, so they are summed as floats
   constexpr int kHG = kHW / 4;  // items per row = slots per plane of a filtered row
-  for (RowWalk<kHG> w; w.r < kSH; w.next()) {
+  for (RowWalk<kHG, kPyrThreads> w; w.r < kSH; w.next()) {
     const int r = w.r, g = w.g;
     const float4* row = s_src + r * kRowSlots + g;
     // slots 2g .. 2g+4: even plane g, g+1, g+2 and odd plane g, g+1
@@ -203,7 +219,7 @@ __device__ __forceinline__ void pyr_tile(const Batch& b, int t, PyrSmem<TW, TH>&
   uint8_t* B = F.blr + F.ooff[o];
   const bool copy_pad = (o == 0) && (pitch_in == op);
   const float2 rne = pair2(12582912.0f);
-  for (RowWalk<kHG> w; w.r < TH; w.next()) {
+  for (RowWalk<kHG, kPyrThreads> w; w.r < TH; w.next()) {
     const int r = w.r, g = w.g;
     const int y = y0 + r;
     if (y >= oh) continue;
@@ -1100,23 +1116,56 @@ __device__ __forceinline__ uint8_t describe_byte(const uint8_t* center, int pitc
   return val;
 }
 
-// This lane's pattern points of descriptor byte `lane` (setPattern, orbd.cu:95-410).
+// This lane's pattern points of descriptor byte `lane` (setPattern,
+// orbd.cu:95-410): PSTEP (x, y) int8 pairs, contiguous per lane, fetched as
+// raw words (load_pattern_raw) so that the loads can be in flight with other
+// work, then converted (pattern_points).
 template <int WTA>
-__device__ __forceinline__ void load_pattern(const Batch& b, int lane, float* px, float* py) {
-  constexpr int PSTEP = (WTA == 3) ? 12 : 16;
+struct PatternRaw {
+  static constexpr int PSTEP = (WTA == 3) ? 12 : 16;
+  static constexpr int WORDS = PSTEP / 2;  // 2 * PSTEP bytes
+  uint32_t w[WORDS];
+};
+template <int WTA>
+__device__ __forceinline__ PatternRaw<WTA> load_pattern_raw(const Batch& b, int lane) {
+  PatternRaw<WTA> r;
+  constexpr int W = PatternRaw<WTA>::WORDS;
+  // 2 * PSTEP * lane bytes in: a multiple of 8 (WTA 3) or 16, and the table is 16-byte aligned
+  const uint32_t* src = reinterpret_cast<const uint32_t*>(b.pattern) + W * lane;
+  if constexpr (W % 4 == 0) {
 #pragma unroll
-  for (int j = 0; j < PSTEP; j++) {
-    px[j] = (float)b.pattern[2 * (PSTEP * lane + j)];
-    py[j] = (float)b.pattern[2 * (PSTEP * lane + j) + 1];
+    for (int i = 0; i < W / 4; i++) {
+      const uint4 v = __ldg(reinterpret_cast<const uint4*>(src) + i);
+      r.w[4 * i] = v.x, r.w[4 * i + 1] = v.y, r.w[4 * i + 2] = v.z, r.w[4 * i + 3] = v.w;
+    }
+  } else {
+#pragma unroll
+    for (int i = 0; i < W / 2; i++) {
+      const uint2 v = __ldg(reinterpret_cast<const uint2*>(src) + i);
+      r.w[2 * i] = v.x, r.w[2 * i + 1] = v.y;
+    }
+  }
+  return r;
+}
+template <int WTA>
+__device__ __forceinline__ void pattern_points(const PatternRaw<WTA>& r, float* px, float* py) {
+#pragma unroll
+  for (int j = 0; j < PatternRaw<WTA>::PSTEP; j++) {
+    const uint32_t word = r.w[j >> 1];
+    const int sh = 16 * (j & 1);
+    px[j] = (float)(int)(int8_t)((word >> sh) & 0xFFu);
+    py[j] = (float)(int)(int8_t)((word >> (sh + 8)) & 0xFFu);
   }
 }
+template <int WTA>
+__device__ __forceinline__ void load_pattern(const Batch& b, int lane, float* px, float* py) {
+  pattern_points<WTA>(load_pattern_raw<WTA>(b, lane), px, py);
+}
 
-// angleIC + gDescrible for keypoint k of frame F, by one warp.
 template <int WTA, bool PL>
 __device__ __forceinline__ void describe_keypoint(const Batch& b, const Frame& F, int k, const float* px,
                                                   const float* py, const int* s_umax, int lane) {
   const int half_k = b.half_k;
-  const int u = lane - 15;
   orbx_point* P = F.pts + k;
   const int x = ldc<PL>(&P->x), y = ldc<PL>(&P->y), o = ldc<PL>(&P->octave);
   const int pitch = F.op[o];
@@ -1124,16 +1173,36 @@ __device__ __forceinline__ void describe_keypoint(const Batch& b, const Frame& F
 
   float angle;
   if (b.describe_mode != kDescribeDescOnly) {
-    // intensity centroid on the raw octave
+    // intensity centroid on the raw octave: lane v + half_k owns disc row v
+    // and reads it as nine aligned words at once (octave pitches are multiples
+    // of 128, so every row has the same alignment); the integer sums are exact
+    // in any order
     const uint8_t* center = F.pyr + coff;
     int m10 = 0, m01 = 0;
-    for (int v = -half_k; v <= half_k; v++) {
+    if (lane <= 2 * half_k) {
+      const int v = lane - half_k;
       const int um = s_umax[v < 0 ? -v : v];
-      if (lane < 31 && u >= -um && u <= um) {
-        const int val = ldc<PL>(center + (ptrdiff_t)v * pitch + u);
-        m10 += u * val;
-        m01 += v * val;
+      const uintptr_t ra = reinterpret_cast<uintptr_t>(center + (ptrdiff_t)v * pitch - half_k);  // column -half_k
+      const uint32_t* wp = reinterpret_cast<const uint32_t*>(ra & ~(uintptr_t)3);
+      const unsigned sh = 8u * (unsigned)(ra & 3);
+      uint32_t w[9];
+#pragma unroll
+      for (int i = 0; i < 9; i++) w[i] = ldc<PL>(wp + i);
+      int sum = 0;
+#pragma unroll
+      for (int i = 0; i < 8; i++) {
+        const uint32_t r = __funnelshift_r(w[i], w[i + 1], sh);  // columns 4i - half_k .. 4i + 3 - half_k
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+          const int uu = 4 * i + k - half_k;
+          if ((unsigned)(uu + um) <= (unsigned)(2 * um)) {  // |uu| <= um
+            const int val = (int)((r >> (8 * k)) & 0xFFu);
+            m10 += uu * val;
+            sum += val;
+          }
+        }
       }
+      m01 = v * sum;
     }
 #pragma unroll
     for (int d = 16; d >= 1; d >>= 1) {
