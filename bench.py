@@ -47,7 +47,7 @@ SMS = 148
 # on the same 1080p pair, the committed summary of the pair's kernels): the
 # instruction roofline beside the HBM one, since these kernels are issue- and
 # latency-bound.
-NCU_WARP_INST = {"pyramid_blur": 13107574, "detect": 12141617, "nms": 2838553, "describe": 3380151,
+NCU_WARP_INST = {"pyramid_blur": 8642876, "detect": 12141439, "nms": 3966314, "describe": 2382793,
                  "match": 2037180}
 ISSUE_PER_CLK_PER_SM = 4  # warp instructions issued per clock per SM (one per scheduler)
 

@@ -150,7 +150,7 @@ struct orbx_ctx {
   int pair_form = 0;     // orbx_pair: 0 = five graph-replayed launches, 1 = one persistent launch
   int pyr_shape = 0;     // pyramid tile shape of the five-launch forms (kPyrShapeTW/TH)
   int row_deps = 0;      // persistent launches: detect waits per pyramid tile row, not per frame
-  int host_overlap = 0;  // orbx_pair_host: 1 = image B uploads while frame A's kernels run (two streams)
+  int host_overlap = 1;  // orbx_pair_host: 1 = image B uploads while frame A's kernels run (two streams)
   BatchSlot pair_b;      // frame B's tables for host_overlap
   MatchWork hmw{};       // its matcher scratch
   cudaEvent_t ev_fork = nullptr, ev_join = nullptr;

@@ -246,9 +246,9 @@ typedef struct orbx_tuning {
                                  2 = 128 x 16, 3 = 64 x 64 octave pixels (the persistent forms use 128 x 32) */
   int persist_row_deps;       /* persistent launches: 1 = a detect tile row waits only for the pyramid tile rows
                                  it reads (a frame's stages overlap row by row), 0 = for the whole frame */
-  int host_overlap;           /* orbx_pair_host with upload_bands = 0: 1 = image B is copied while frame A's
-                                 kernels run (the frames on two streams, popcount matching), 0 = copy both,
-                                 then run the pair */
+  int host_overlap;           /* orbx_pair_host with upload_bands = 0: 1 (default) = image B is copied while
+                                 frame A's kernels run (the frames on two streams, popcount matching), 0 = copy
+                                 both, then run the pair */
 } orbx_tuning;
 
 ORBX_API int orbx_get_tuning(orbx_ctx* ctx, orbx_tuning* t);
