@@ -477,6 +477,15 @@ static int upload_batch(orbx_ctx* c, BatchSlot& bs, const std::vector<Frame>& fr
   b.harris_scale4 = c->scale4;
   b.pattern = c->d_pattern;
   b.umax = c->d_umax;
+  b.n_inline = nf <= kInlineFrames ? nf : 0;
+  for (int i = 0; i < kInlineFrames + 1; i++) {
+    const bool in = b.n_inline && i <= nf;
+    b.inl_pyr_base[i] = in ? pb[i] : 0;
+    b.inl_det_base[i] = in ? db[i] : 0;
+    b.inl_nms_base[i] = in ? nb[i] : 0;
+  }
+  std::memset(b.inl, 0, sizeof(b.inl));
+  for (int i = 0; i < b.n_inline; i++) b.inl[i] = frames[i];
   plan->pyr_tiles = pb[nf];
   plan->det_tiles = db[nf];
   plan->nms_strips = nb[nf];

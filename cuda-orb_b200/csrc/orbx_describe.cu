@@ -9,8 +9,8 @@
 
 namespace orbx {
 
-template <int WTA>
-__global__ void __launch_bounds__(kDescWarps * 32) k_describe(Batch b) {
+template <int WTA, bool INL>
+__global__ void __launch_bounds__(kDescWarps * 32) k_describe(const __grid_constant__ Batch b) {
   __shared__ int s_pref[kMaxFramesPerLaunch + 1];
   __shared__ int s_umax[32];
 
@@ -23,7 +23,7 @@ __global__ void __launch_bounds__(kDescWarps * 32) k_describe(Batch b) {
   const int half_k = b.half_k;
   if (threadIdx.x < half_k + 1) s_umax[threadIdx.x] = b.umax[threadIdx.x];
   constexpr int kFrameLines = (int)((sizeof(Frame) + 127) / 128);
-  if (nf <= 8 && (int)threadIdx.x < nf * kFrameLines)
+  if (!INL && nf <= 8 && (int)threadIdx.x < nf * kFrameLines)
     asm volatile("prefetch.global.L1 [%0];" ::"l"(reinterpret_cast<const char*>(b.frames + threadIdx.x / kFrameLines) +
                                                   128 * (threadIdx.x % kFrameLines)));
   // exclusive prefix of the per-frame keypoint counts (written by k_nms):
@@ -32,7 +32,7 @@ __global__ void __launch_bounds__(kDescWarps * 32) k_describe(Batch b) {
     const int per = (nf + kDescWarps * 32 - 1) / (kDescWarps * 32);
     const int beg = min((int)threadIdx.x * per, nf), end = min(beg + per, nf);
     int local = 0;
-    for (int f = beg; f < end; f++) local += *b.frames[f].count;
+    for (int f = beg; f < end; f++) local += *batch_frame<INL>(b, f).count;
     int incl = local;
 #pragma unroll
     for (int d = 1; d < 32; d <<= 1) {
@@ -45,7 +45,7 @@ __global__ void __launch_bounds__(kDescWarps * 32) k_describe(Batch b) {
     for (int w2 = 0; w2 < (int)(threadIdx.x >> 5); w2++) run += s_wsum[w2];
     for (int f = beg; f < end; f++) {
       s_pref[f] = run;
-      run += *b.frames[f].count;
+      run += *batch_frame<INL>(b, f).count;
     }
     if (threadIdx.x == kDescWarps * 32 - 1) s_pref[nf] = run;
   }
@@ -67,7 +67,7 @@ __global__ void __launch_bounds__(kDescWarps * 32) k_describe(Batch b) {
       else
         hi = mid - 1;
     }
-    describe_keypoint<WTA, false>(b, b.frames[lo], i - s_pref[lo], px, py, s_umax, lane);
+    describe_keypoint<WTA, false>(b, batch_frame<INL>(b, lo), i - s_pref[lo], px, py, s_umax, lane);
   }
 }
 
@@ -77,12 +77,22 @@ cudaError_t launch_describe(const Batch& b, int total_max_pts, cudaStream_t s, i
   int blocks = (warps_needed + kDescWarps - 1) / kDescWarps;
   const int cap = 148 * (blocks_per_sm > 0 ? blocks_per_sm : 8);
   if (blocks > cap) blocks = cap;
-  if (b.wta_k == 3)
-    k_describe<3><<<blocks, kDescWarps * 32, 0, s>>>(b);
-  else if (b.wta_k == 4)
-    k_describe<4><<<blocks, kDescWarps * 32, 0, s>>>(b);
-  else
-    k_describe<2><<<blocks, kDescWarps * 32, 0, s>>>(b);
+  const dim3 g(blocks), t(kDescWarps * 32);
+  if (b.n_inline > 0) {
+    if (b.wta_k == 3)
+      k_describe<3, true><<<g, t, 0, s>>>(b);
+    else if (b.wta_k == 4)
+      k_describe<4, true><<<g, t, 0, s>>>(b);
+    else
+      k_describe<2, true><<<g, t, 0, s>>>(b);
+  } else {
+    if (b.wta_k == 3)
+      k_describe<3, false><<<g, t, 0, s>>>(b);
+    else if (b.wta_k == 4)
+      k_describe<4, false><<<g, t, 0, s>>>(b);
+    else
+      k_describe<2, false><<<g, t, 0, s>>>(b);
+  }
   return cudaGetLastError();
 }
 

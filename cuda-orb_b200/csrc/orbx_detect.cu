@@ -8,23 +8,27 @@
 
 namespace orbx {
 
-template <int TW, int TH>
-__global__ void __launch_bounds__(kPyrThreads, 4) k_pyramid_blur(Batch b) {
+// Kernels take the batch as a grid constant so that, for batches whose frame
+// table travels in the launch parameters (INL), the stages read it in place.
+template <int TW, int TH, bool INL>
+__global__ void __launch_bounds__(kPyrThreads, 4) k_pyramid_blur(const __grid_constant__ Batch b) {
   __shared__ PyrSmem<TW, TH> sm;
-  pyr_tile<false, TW, TH>(b, blockIdx.x, sm);
+  pyr_tile<false, TW, TH, INL>(b, blockIdx.x, sm);
 }
 
-__global__ void __launch_bounds__(256, 4) k_detect(Batch b) {
+template <bool INL>
+__global__ void __launch_bounds__(256, 5) k_detect(const __grid_constant__ Batch b) {
   __shared__ DetSmem sm;
-  det_tile<false>(b, blockIdx.x, sm);
+  det_tile<false, INL>(b, blockIdx.x, sm);
 }
 
-__global__ void __launch_bounds__(256, 4) k_nms(Batch b) {
+template <bool INL>
+__global__ void __launch_bounds__(256, 4) k_nms(const __grid_constant__ Batch b) {
   __shared__ NmsSmem sm;
   __shared__ int s_ticket;
   if (threadIdx.x == 0) s_ticket = (int)atomicAdd(b.nms_ticket, 1u);
   __syncthreads();
-  nms_strip<false>(b, s_ticket, sm);
+  nms_strip<false, INL>(b, s_ticket, sm);
 }
 
 // Dense reference-layout maps (vmem: f32 scores then i32 octaves,
@@ -48,31 +52,42 @@ cudaError_t launch_expand_score_map(const Frame* d_frame, float* vmap_dense, int
 
 cudaError_t launch_pyramid_blur(const Batch& b, int total_tiles, cudaStream_t s) {
   if (total_tiles <= 0) return cudaSuccess;
+  const bool inl = b.n_inline > 0;
   switch (b.pyr_shape) {
     case 1:
-      k_pyramid_blur<kPyrShapeTW[1], kPyrShapeTH[1]><<<total_tiles, kPyrThreads, 0, s>>>(b);
+      if (inl) k_pyramid_blur<kPyrShapeTW[1], kPyrShapeTH[1], true><<<total_tiles, kPyrThreads, 0, s>>>(b);
+      else k_pyramid_blur<kPyrShapeTW[1], kPyrShapeTH[1], false><<<total_tiles, kPyrThreads, 0, s>>>(b);
       break;
     case 2:
-      k_pyramid_blur<kPyrShapeTW[2], kPyrShapeTH[2]><<<total_tiles, kPyrThreads, 0, s>>>(b);
+      if (inl) k_pyramid_blur<kPyrShapeTW[2], kPyrShapeTH[2], true><<<total_tiles, kPyrThreads, 0, s>>>(b);
+      else k_pyramid_blur<kPyrShapeTW[2], kPyrShapeTH[2], false><<<total_tiles, kPyrThreads, 0, s>>>(b);
       break;
     case 3:
-      k_pyramid_blur<kPyrShapeTW[3], kPyrShapeTH[3]><<<total_tiles, kPyrThreads, 0, s>>>(b);
+      if (inl) k_pyramid_blur<kPyrShapeTW[3], kPyrShapeTH[3], true><<<total_tiles, kPyrThreads, 0, s>>>(b);
+      else k_pyramid_blur<kPyrShapeTW[3], kPyrShapeTH[3], false><<<total_tiles, kPyrThreads, 0, s>>>(b);
       break;
     default:
-      k_pyramid_blur<kPyrShapeTW[0], kPyrShapeTH[0]><<<total_tiles, kPyrThreads, 0, s>>>(b);
+      if (inl) k_pyramid_blur<kPyrShapeTW[0], kPyrShapeTH[0], true><<<total_tiles, kPyrThreads, 0, s>>>(b);
+      else k_pyramid_blur<kPyrShapeTW[0], kPyrShapeTH[0], false><<<total_tiles, kPyrThreads, 0, s>>>(b);
   }
   return cudaGetLastError();
 }
 
 cudaError_t launch_detect(const Batch& b, int total_tiles, cudaStream_t s) {
   if (total_tiles <= 0) return cudaSuccess;
-  k_detect<<<total_tiles, 256, 0, s>>>(b);
+  if (b.n_inline > 0)
+    k_detect<true><<<total_tiles, 256, 0, s>>>(b);
+  else
+    k_detect<false><<<total_tiles, 256, 0, s>>>(b);
   return cudaGetLastError();
 }
 
 cudaError_t launch_nms(const Batch& b, int total_strips, cudaStream_t s) {
   if (total_strips <= 0) return cudaSuccess;
-  k_nms<<<total_strips, 256, 0, s>>>(b);
+  if (b.n_inline > 0)
+    k_nms<true><<<total_strips, 256, 0, s>>>(b);
+  else
+    k_nms<false><<<total_strips, 256, 0, s>>>(b);
   return cudaGetLastError();
 }
 

@@ -9,6 +9,7 @@ namespace orbx {
 
 constexpr int kMaxOctaves = 5;        // MAX_OCTAVE, orbd.cu:18
 constexpr int kMaxFramesPerLaunch = 1024;
+constexpr int kInlineFrames = 2;  // frames carried in the launch parameters (a pair)
 constexpr size_t kGuard = 256 * 1024; // zeroed bytes before/after each pyramid
 
 // Pyramid-and-blur tile (octave pixels): the default shape, which the
@@ -79,6 +80,12 @@ struct Batch {
   float harris_scale4;   // setScaleSqSq (orbd.cu:436-441)
   const int8_t* pattern; // [512][2] sampling points (setPattern)
   const int* umax;       // [half_k + 2] (setUmax)
+  // A batch of up to kInlineFrames frames also carries its frame table and
+  // tile prefixes in the launch parameters (n_inline = n_frames, else 0), so
+  // that the kernels read them from the constant bank instead of global memory.
+  int n_inline;
+  int inl_pyr_base[kInlineFrames + 1], inl_det_base[kInlineFrames + 1], inl_nms_base[kInlineFrames + 1];
+  Frame inl[kInlineFrames];
 };
 
 enum : int {

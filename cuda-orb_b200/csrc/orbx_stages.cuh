@@ -21,6 +21,34 @@ __device__ __forceinline__ T ldx(const T* p) {
     return __ldg(p);
 }
 
+// The frame table of a launch: from the launch parameters (INL, batches of up
+// to kInlineFrames frames, constant-bank reads) or from global memory.
+template <bool INL>
+__device__ __forceinline__ const Frame& batch_frame(const Batch& b, int f) {
+  if constexpr (INL)
+    return b.inl[f];
+  else
+    return b.frames[f];
+}
+// Index of the frame whose range [base[f], base[f+1]) holds t (base in the
+// launch parameters when INL).
+template <bool INL>
+__device__ __forceinline__ int find_frame_in(const int* base, int n, int t) {
+  int lo = 0, hi = n - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    int v;
+    if constexpr (INL)
+      v = base[mid];
+    else
+      v = __ldg(base + mid);
+    if (v <= t)
+      lo = mid;
+    else
+      hi = mid - 1;
+  }
+  return lo;
+}
 
 // ---------------------------------------------------------------------------
 // Pyramid + blur
@@ -108,7 +136,7 @@ struct PyrSmem {
 // One pyramid tile (tile index t over the batch) of shape TW x TH.  PL: the
 // level-0 image is copied in during the same launch (coherent loads instead of
 // the read-only path).
-template <bool PL, int TW = kPyrTW, int TH = kPyrTH>
+template <bool PL, int TW = kPyrTW, int TH = kPyrTH, bool INL = false>
 __device__ __forceinline__ void pyr_tile(const Batch& b, int t, PyrSmem<TW, TH>& sm) {
   using S = PyrSmem<TW, TH>;
   constexpr int kHW = S::HW, kSW = S::SW, kSH = S::SH;
@@ -118,9 +146,10 @@ __device__ __forceinline__ void pyr_tile(const Batch& b, int t, PyrSmem<TW, TH>&
   float4* s_src = reinterpret_cast<float4*>(sm.src);
   float4* s_row = reinterpret_cast<float4*>(sm.row);
   uint8_t* s_byte = sm.byte;
-  const int f = find_frame(b.pyr_base, b.n_frames, t);
-  const Frame& F = b.frames[f];
-  int lt = t - b.pyr_base[f];
+  const int* base = INL ? b.inl_pyr_base : b.pyr_base;
+  const int f = find_frame_in<INL>(base, b.n_frames, t);
+  const Frame& F = batch_frame<INL>(b, f);
+  int lt = t - (INL ? base[f] : __ldg(base + f));
   int o = 0;
   while (o + 1 < F.n_oct && lt >= F.pyr_tile_base[o + 1]) o++;
   lt -= F.pyr_tile_base[o];
@@ -453,7 +482,7 @@ __device__ __forceinline__ void pretest_word(int w, int X0, int Y0, const uint8_
 
 // One detect tile (tile index t over the batch).  P: the raw pyramid was
 // written earlier in the same launch (coherent loads instead of the read-only path).
-template <bool P>
+template <bool P, bool INL = false>
 __device__ __forceinline__ void det_tile(const Batch& b, int t, DetSmem& sm) {
   uint8_t* s_stage = sm.stage;
   unsigned long long* s_key = sm.key;
@@ -463,9 +492,10 @@ __device__ __forceinline__ void det_tile(const Batch& b, int t, DetSmem& sm) {
   uint32_t* s_occ = sm.occ;
   int* s_ow = sm.ow;
   int* s_oh = sm.oh;
-  const int f = find_frame(b.det_base, b.n_frames, t);
-  const Frame& F = b.frames[f];
-  const int lt = t - b.det_base[f];
+  const int* base = INL ? b.inl_det_base : b.det_base;
+  const int f = find_frame_in<INL>(base, b.n_frames, t);
+  const Frame& F = batch_frame<INL>(b, f);
+  const int lt = t - (INL ? base[f] : __ldg(base + f));
   const int X0 = (lt % F.det_tiles_x) * kDetTW;
   const int Y0 = (lt / F.det_tiles_x) * kDetTH;
   const int n_oct = F.n_oct;
@@ -802,16 +832,17 @@ __device__ __forceinline__ int block_scan_excl(int local, int* s_warp_tot, int& 
 // One NMS strip; `ticket` is the strip's index over the batch, and strips must
 // start in ticket order (the look-back waits only on smaller tickets).  P: the
 // score map was written earlier in the same launch.
-template <bool P>
+template <bool P, bool INL = false>
 __device__ __forceinline__ void nms_strip(const Batch& b, int ticket, NmsSmem& sm) {
   uint32_t* s_sur = sm.sur;
   int* s_pref = sm.pref;
   int* s_ncand = sm.ncand;
   int* s_warp_tot = sm.warp_tot;
   int& s_base = sm.base;
-  const int f = find_frame(b.nms_base, b.n_frames, ticket);
-  const Frame& F = b.frames[f];
-  const int s = ticket - b.nms_base[f];
+  const int* strip_base = INL ? b.inl_nms_base : b.nms_base;
+  const int f = find_frame_in<INL>(strip_base, b.n_frames, ticket);
+  const Frame& F = batch_frame<INL>(b, f);
+  const int s = ticket - (INL ? strip_base[f] : __ldg(strip_base + f));
   const int border = F.border;
   const int row0 = border + s * F.nms_rows;
   const int row1 = min(row0 + F.nms_rows, F.h - border);
