@@ -133,35 +133,80 @@ struct PyrSmem {
   __align__(16) float2 row[SH * HW];
 };
 
-// One pyramid tile (tile index t over the batch) of shape TW x TH.  PL: the
-// level-0 image is copied in during the same launch (coherent loads instead of
-// the read-only path).
-template <bool PL, int TW = kPyrTW, int TH = kPyrTH, bool INL = false>
-__device__ __forceinline__ void pyr_tile(const Batch& b, int t, PyrSmem<TW, TH>& sm) {
-  using S = PyrSmem<TW, TH>;
-  constexpr int kHW = S::HW, kSW = S::SW, kSH = S::SH;
-  constexpr int kRowSlots = S::SW2 / 2;  // 16-byte slots per staged pair row (two planes)
-  constexpr int kOutSlots = kHW / 2;     // 16-byte slots per filtered pair row (two planes)
-  static_assert(TW % 16 == 0 && S::SW2 % 4 == 0, "pyramid tile width");
-  float4* s_src = reinterpret_cast<float4*>(sm.src);
-  float4* s_row = reinterpret_cast<float4*>(sm.row);
-  uint8_t* s_byte = sm.byte;
+// Position of pyramid tile t (tile index over the batch) of shape TW x TH.
+struct PyrTile {
+  int f;       // frame
+  int o;       // octave
+  int lt;      // tile index within the octave
+  int x0, y0;  // octave-pixel origin
+};
+template <bool INL, int TW, int TH>
+__device__ __forceinline__ PyrTile pyr_tile_at(const Batch& b, int t) {
   const int* base = INL ? b.inl_pyr_base : b.pyr_base;
-  const int f = find_frame_in<INL>(base, b.n_frames, t);
-  const Frame& F = batch_frame<INL>(b, f);
-  int lt = t - (INL ? base[f] : __ldg(base + f));
+  PyrTile g;
+  g.f = find_frame_in<INL>(base, b.n_frames, t);
+  const Frame& F = batch_frame<INL>(b, g.f);
+  int lt = t - (INL ? base[g.f] : __ldg(base + g.f));
   int o = 0;
   while (o + 1 < F.n_oct && lt >= F.pyr_tile_base[o + 1]) o++;
   lt -= F.pyr_tile_base[o];
   const int tiles_x = F.pyr_tiles_x[o];
-  const int x0 = (lt % tiles_x) * TW;
-  const int y0 = (lt / tiles_x) * TH;
-  const int ow = F.ow[o], oh = F.oh[o], op = F.op[o];
+  g.o = o;
+  g.lt = lt;
+  g.x0 = (lt % tiles_x) * TW;
+  g.y0 = (lt / tiles_x) * TH;
+  return g;
+}
+
+template <int TW, int TH>
+__host__ __device__ constexpr int pyr_stage_items() {
+  return (PyrSmem<TW, TH>::SH * (PyrSmem<TW, TH>::SW2 / 4) + kPyrThreads - 1) / kPyrThreads;
+}
+
+// Staging loads of tile g: source rows y0-3 .. y0+TH+2; item (r, g) takes
+// columns 4g-3 .. 4g of the left half and of the right half (tile-relative),
+// reflect-101 at the octave edges.  All of a thread's loads are issued before
+// any is used (blocks have kPyrThreads threads).
+template <bool PL, int TW, int TH, bool INL>
+__device__ __forceinline__ void pyr_tile_load(const Batch& b, const PyrTile& g, uint32_t* wa, uint32_t* wb) {
+  using S = PyrSmem<TW, TH>;
+  constexpr int kHW = S::HW, kSH = S::SH, kGroups = S::SW2 / 4;
+  const Frame& F = batch_frame<INL>(b, g.f);
+  const int o = g.o, ow = F.ow[o], oh = F.oh[o], op = F.op[o];
   const uint8_t* __restrict__ img = F.img;
   const int pitch_in = F.pitch_in;
+  const uint8_t* __restrict__ psrc = F.pyr_src ? F.pyr_src + F.ooff[o] : nullptr;
+  const bool words0 = (o == 0) && !psrc && ((reinterpret_cast<uintptr_t>(img) | (uintptr_t)pitch_in) & 3u) == 0;
+  const int sh = psrc ? 0 : o;
+  RowWalk<kGroups, kPyrThreads> w;
+#pragma unroll
+  for (int q = 0; q < pyr_stage_items<TW, TH>(); q++) {
+    wa[q] = wb[q] = 0u;
+    if (w.r < kSH) {
+      const int y = reflect101(g.y0 - 3 + w.r, oh);
+      const uint8_t* rowp = psrc ? psrc + (size_t)y * op : img + (size_t)(y << o) * pitch_in;
+      const int cx = g.x0 - 3 + 4 * w.g;
+      wa[q] = pyr_stage_word<PL>(rowp, cx, ow, sh, words0);
+      wb[q] = pyr_stage_word<PL>(rowp, cx + kHW, ow, sh, words0);
+    }
+    w.next();
+  }
+}
 
-  // Per-frame housekeeping for the later stages of the same batch.
-  if (o == 0 && lt == 0) {
+// The staged words of tile g into shared memory, as float pairs and as bytes,
+// plus the per-frame housekeeping of the frame's first tile.  No barrier.
+template <int TW, int TH, bool INL>
+__device__ __forceinline__ void pyr_tile_stage(const Batch& b, int t, const PyrTile& g, const uint32_t* wa,
+                                               const uint32_t* wb, PyrSmem<TW, TH>& sm) {
+  using S = PyrSmem<TW, TH>;
+  constexpr int kHW = S::HW, kSW = S::SW, kSH = S::SH;
+  constexpr int kRowSlots = S::SW2 / 2;  // 16-byte slots per staged pair row (two planes)
+  constexpr int kGroups = S::SW2 / 4;    // staging items per row = slots per plane of a staged row
+  static_assert(TW % 16 == 0 && S::SW2 % 4 == 0, "pyramid tile width");
+  float4* s_src = reinterpret_cast<float4*>(sm.src);
+  uint8_t* s_byte = sm.byte;
+  const Frame& F = batch_frame<INL>(b, g.f);
+  if (g.o == 0 && g.lt == 0) {
     for (int i = threadIdx.x; i < F.nms_strips; i += blockDim.x) F.nms_status[i] = 0ull;
     if (threadIdx.x == 0) {
       *F.count = 0;
@@ -169,38 +214,11 @@ __device__ __forceinline__ void pyr_tile(const Batch& b, int t, PyrSmem<TW, TH>&
     }
   }
   if (t == 0 && threadIdx.x == 0) *b.nms_ticket = 0u;
-
-  // stage: source rows y0-3 .. y0+TH+2; item (r, g) takes columns 4g-3 .. 4g
-  // of the left half and of the right half (tile-relative), reflect-101 at the
-  // octave edges, as float pairs and as bytes
-  const uint8_t* __restrict__ psrc = F.pyr_src ? F.pyr_src + F.ooff[o] : nullptr;
-  const bool words0 = (o == 0) && !psrc && ((reinterpret_cast<uintptr_t>(img) | (uintptr_t)pitch_in) & 3u) == 0;
-  const int sh = psrc ? 0 : o;
-  constexpr int kGroups = S::SW2 / 4;  // staging items per row = slots per plane of a staged row
   const float2 m23 = pair2(-8388608.0f);
-  // all of a thread's staging loads are issued before any is used (one round
-  // trip per tile instead of one per item); blocks have kPyrThreads threads
-  constexpr int kStageItems = (kSH * kGroups + kPyrThreads - 1) / kPyrThreads;
-  uint32_t wa[kStageItems], wb[kStageItems];
-  {
-    RowWalk<kGroups, kPyrThreads> w;
-#pragma unroll
-    for (int q = 0; q < kStageItems; q++) {
-      wa[q] = wb[q] = 0u;
-      if (w.r < kSH) {
-        const int y = reflect101(y0 - 3 + w.r, oh);
-        const uint8_t* rowp = psrc ? psrc + (size_t)y * op : img + (size_t)(y << o) * pitch_in;
-        const int cx = x0 - 3 + 4 * w.g;
-        wa[q] = pyr_stage_word<PL>(rowp, cx, ow, sh, words0);
-        wb[q] = pyr_stage_word<PL>(rowp, cx + kHW, ow, sh, words0);
-      }
-      w.next();
-    }
-  }
   RowWalk<kGroups, kPyrThreads> w;
 #pragma unroll
-  for (int q = 0; q < kStageItems; q++, w.next()) {
-    const int r = w.r, g = w.g;
+  for (int q = 0; q < pyr_stage_items<TW, TH>(); q++, w.next()) {
+    const int r = w.r, gg = w.g;
     if (r >= kSH) break;
     // pair j = (byte j of wa, byte j of wb) as floats: 2^23 + byte, minus 2^23
     const float2 p0 = __fadd2_rn(make_float2(byte_bits(wa[q], 0x7540u), byte_bits(wb[q], 0x7540u)), m23);
@@ -208,13 +226,34 @@ __device__ __forceinline__ void pyr_tile(const Batch& b, int t, PyrSmem<TW, TH>&
     const float2 p2 = __fadd2_rn(make_float2(byte_bits(wa[q], 0x7542u), byte_bits(wb[q], 0x7542u)), m23);
     const float2 p3 = __fadd2_rn(make_float2(byte_bits(wa[q], 0x7543u), byte_bits(wb[q], 0x7543u)), m23);
     // pairs 4g .. 4g+3 = slots 2g (even plane) and 2g+1 (odd plane) of row r
-    float4* row = s_src + r * kRowSlots + g;
+    float4* row = s_src + r * kRowSlots + gg;
     row[0] = make_float4(p0.x, p0.y, p1.x, p1.y);
     row[kGroups] = make_float4(p2.x, p2.y, p3.x, p3.y);
     // the halves' halos overlap in the middle: both writes there store the same bytes
-    *reinterpret_cast<uint32_t*>(s_byte + r * kSW + 4 * g) = wa[q];
-    *reinterpret_cast<uint32_t*>(s_byte + r * kSW + kHW + 4 * g) = wb[q];
+    *reinterpret_cast<uint32_t*>(s_byte + r * kSW + 4 * gg) = wa[q];
+    *reinterpret_cast<uint32_t*>(s_byte + r * kSW + kHW + 4 * gg) = wb[q];
   }
+}
+
+// Blur of the staged tile g and the stores of its raw and blurred bytes:
+// a barrier, the horizontal pass, a barrier, the vertical pass.  PL: the
+// level-0 image was written earlier in the same launch.
+template <bool PL, int TW, int TH, bool INL>
+__device__ __forceinline__ void pyr_tile_filter(const Batch& b, const PyrTile& g, PyrSmem<TW, TH>& sm) {
+  using S = PyrSmem<TW, TH>;
+  constexpr int kHW = S::HW, kSW = S::SW, kSH = S::SH;
+  constexpr int kRowSlots = S::SW2 / 2;
+  constexpr int kOutSlots = kHW / 2;     // 16-byte slots per filtered pair row (two planes)
+  constexpr int kGroups = S::SW2 / 4;
+  float4* s_src = reinterpret_cast<float4*>(sm.src);
+  float4* s_row = reinterpret_cast<float4*>(sm.row);
+  uint8_t* s_byte = sm.byte;
+  const Frame& F = batch_frame<INL>(b, g.f);
+  const int o = g.o, x0 = g.x0, y0 = g.y0;
+  const int ow = F.ow[o], oh = F.oh[o], op = F.op[o];
+  const uint8_t* __restrict__ img = F.img;
+  const int pitch_in = F.pitch_in;
+  const uint8_t* __restrict__ psrc = F.pyr_src ? F.pyr_src + F.ooff[o] : nullptr;
   __syncthreads();
 
   float2 k[4];
@@ -305,6 +344,20 @@ __device__ __forceinline__ void pyr_tile(const Batch& b, int t, PyrSmem<TW, TH>&
       }
     }
   }
+}
+
+
+// One pyramid tile (tile index t over the batch) of shape TW x TH: it stages
+// the tile plus a 3-pixel reflected halo in shared memory, writes the raw
+// tile, and blurs it.  PL: the level-0 image is copied in during the same
+// launch (coherent loads instead of the read-only path).
+template <bool PL, int TW = kPyrTW, int TH = kPyrTH, bool INL = false>
+__device__ __forceinline__ void pyr_tile(const Batch& b, int t, PyrSmem<TW, TH>& sm) {
+  uint32_t wa[pyr_stage_items<TW, TH>()], wb[pyr_stage_items<TW, TH>()];
+  const PyrTile g = pyr_tile_at<INL, TW, TH>(b, t);
+  pyr_tile_load<PL, TW, TH, INL>(b, g, wa, wb);
+  pyr_tile_stage<TW, TH, INL>(b, t, g, wa, wb, sm);
+  pyr_tile_filter<PL, TW, TH, INL>(b, g, sm);
 }
 
 // ---------------------------------------------------------------------------
