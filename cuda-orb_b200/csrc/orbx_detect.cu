@@ -17,7 +17,7 @@ __global__ void __launch_bounds__(kPyrThreads, 4) k_pyramid_blur(const __grid_co
 }
 
 template <bool INL>
-__global__ void __launch_bounds__(256, 5) k_detect(const __grid_constant__ Batch b) {
+__global__ void __launch_bounds__(256, 6) k_detect(const __grid_constant__ Batch b) {
   __shared__ DetSmem sm;
   det_tile<false, INL>(b, blockIdx.x, sm);
 }
