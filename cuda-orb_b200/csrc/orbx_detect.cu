@@ -11,7 +11,7 @@ namespace orbx {
 // Kernels take the batch as a grid constant so that, for batches whose frame
 // table travels in the launch parameters (INL), the stages read it in place.
 template <int TW, int TH, bool INL>
-__global__ void __launch_bounds__(kPyrThreads, 4) k_pyramid_blur(const __grid_constant__ Batch b) {
+__global__ void __launch_bounds__(kPyrThreads, 5) k_pyramid_blur(const __grid_constant__ Batch b) {
   __shared__ PyrSmem<TW, TH> sm;
   pyr_tile<false, TW, TH, INL>(b, blockIdx.x, sm);
 }

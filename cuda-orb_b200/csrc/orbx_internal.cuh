@@ -16,11 +16,12 @@ constexpr size_t kGuard = 256 * 1024; // zeroed bytes before/after each pyramid
 // persistent kernel uses; the five-launch kernel also has the other shapes of
 // kPyrShapeTW/TH (tuning pyr_tile), one instantiation each
 constexpr int kPyrThreads = 256;  // threads of every block that runs pyramid tiles
-constexpr int kPyrTW = 128;
-constexpr int kPyrTH = 32;
 constexpr int kPyrShapes = 4;
+// 128 x 28 keeps a tile's shared memory under the 44.6 KB of five blocks per SM
 constexpr int kPyrShapeTW[kPyrShapes] = {128, 64, 128, 64};
-constexpr int kPyrShapeTH[kPyrShapes] = {32, 32, 16, 64};
+constexpr int kPyrShapeTH[kPyrShapes] = {28, 32, 16, 64};
+constexpr int kPyrTW = kPyrShapeTW[0];
+constexpr int kPyrTH = kPyrShapeTH[0];
 // Detect tile (level-0 pixels); 32 keeps octave 4/5 tiles whole
 constexpr int kDetTW = 64;
 constexpr int kDetTH = 32;
