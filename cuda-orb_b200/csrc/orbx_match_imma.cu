@@ -170,11 +170,47 @@ __device__ __forceinline__ bool any_exceeds32(const int* v, int thr) {
   return m > thr;
 }
 
+// Maxima of the column groups 0-8, 9-17, 18-26 and 27-31 of a 32-column chunk,
+// as float bit patterns (the reduction any_exceeds32 uses, for thr >= 0).
+__device__ __forceinline__ void group_max4(const int* v, float* r) {
+  float m[12];
+#pragma unroll
+  for (int i = 0; i < 10; i++)
+    m[i] = fmax3_bits(__int_as_float(v[3 * i]), __int_as_float(v[3 * i + 1]), __int_as_float(v[3 * i + 2]));
+  m[10] = __int_as_float(v[30]);
+  m[11] = __int_as_float(v[31]);
+  r[0] = fmax3_bits(m[0], m[1], m[2]);
+  r[1] = fmax3_bits(m[3], m[4], m[5]);
+  r[2] = fmax3_bits(m[6], m[7], m[8]);
+  r[3] = fmax3_bits(m[9], m[10], m[11]);
+}
+// Whether a group maximum from group_max4 exceeds thr >= 0 (a NaN maximum
+// means every value of the group was negative).
+__device__ __forceinline__ bool bits_exceed(float r, int thr) {
+  const int rb = __float_as_int(r);
+  return rb > thr && rb < 0x7F800000;
+}
+
 // Global key (distance << 22 | index) of a chunk-local key (dot << 5 | 31 - column).
 __device__ __forceinline__ uint32_t local_to_key(int lk, int g_chunk) {
   const int dot = lk >> 5;
   const int col = 31 - (lk & 31);
   return ((uint32_t)((256 - dot) >> 1) << kIdxBitsShared) | (uint32_t)(g_chunk + col);
+}
+
+// Top two of columns B .. E-1 of a chunk on local keys (dot << 5 | 31 - column),
+// ties keeping the lower column, pushed into (k1, k2).
+template <int B, int E>
+__device__ __forceinline__ void chunk_top2_push(const int* vc, int gc, uint32_t& k1, uint32_t& k2) {
+  int a1 = INT_MIN, a2 = INT_MIN;
+#pragma unroll
+  for (int j = B; j < E; j++) {
+    const int lk = (vc[j] << 5) | (31 - j);
+    a2 = max(a2, min(a1, lk));
+    a1 = max(a1, lk);
+  }
+  if ((a1 >> 5) > kMaskedDot) top2_push_shared(k1, k2, local_to_key(a1, gc));
+  if ((a2 >> 5) > kMaskedDot) top2_push_shared(k1, k2, local_to_key(a2, gc));
 }
 
 // Expand 256-bit descriptors to +-1 int8 rows; rows at or past the count are zero.
@@ -380,19 +416,35 @@ __global__ void __launch_bounds__(kIThreads, 1)
       for (int c = 0; c < 2; c++) {
         // columns arrive in increasing index order, so only a strictly larger dot
         // than the current second best can enter the top two
-        if (__any_sync(0xffffffffu, any_exceeds32(v + 32 * c, thr))) {
-          // top two of the chunk on local keys (dot << 5 | 31 - column): ties keep the lower column
-          int a1 = INT_MIN, a2 = INT_MIN;
-#pragma unroll
-          for (int j = 0; j < 32; j++) {
-            const int lk = (v[32 * c + j] << 5) | (31 - j);
-            a2 = max(a2, min(a1, lk));
-            a1 = max(a1, lk);
-          }
-          const int gc = g0 + 32 * c;
-          if ((a1 >> 5) > kMaskedDot) top2_push_shared(k1, k2, local_to_key(a1, gc));
-          if ((a2 >> 5) > kMaskedDot) top2_push_shared(k1, k2, local_to_key(a2, gc));
-          thr = (k2 == kNoKeyShared) ? kMaskedDot : 256 - 2 * (int)(k2 >> kIdxBitsShared);
+        const int* vc = v + 32 * c;
+        const int gc = g0 + 32 * c;
+        auto next_thr = [&]() { return (k2 == kNoKeyShared) ? kMaskedDot : 256 - 2 * (int)(k2 >> kIdxBitsShared); };
+        if (__any_sync(0xffffffffu, thr < 0)) {  // a lane has no second best yet: the whole chunk (warp-uniform)
+          chunk_top2_push<0, 32>(vc, gc, k1, k2);
+          thr = next_thr();
+          continue;
+        }
+        float gm[4];
+        group_max4(vc, gm);
+        const float cm = fmax3_bits(gm[0], gm[1], fmax3_bits(gm[2], gm[3], gm[3]));
+        if (!__any_sync(0xffffffffu, bits_exceed(cm, thr))) continue;
+        // only the column groups with a value above the threshold, in column
+        // order, the threshold tightening as the top two improve
+        if (__any_sync(0xffffffffu, bits_exceed(gm[0], thr))) {
+          chunk_top2_push<0, 9>(vc, gc, k1, k2);
+          thr = next_thr();
+        }
+        if (__any_sync(0xffffffffu, bits_exceed(gm[1], thr))) {
+          chunk_top2_push<9, 18>(vc, gc, k1, k2);
+          thr = next_thr();
+        }
+        if (__any_sync(0xffffffffu, bits_exceed(gm[2], thr))) {
+          chunk_top2_push<18, 27>(vc, gc, k1, k2);
+          thr = next_thr();
+        }
+        if (__any_sync(0xffffffffu, bits_exceed(gm[3], thr))) {
+          chunk_top2_push<27, 32>(vc, gc, k1, k2);
+          thr = next_thr();
         }
       }
     }
