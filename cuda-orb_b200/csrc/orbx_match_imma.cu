@@ -39,7 +39,8 @@ constexpr uint32_t kINumBars = 1 + 2 * kIStages + 4;
 // 1024 bytes of alignment slack, the query tile, the ring, the barriers, TMEM base + abort flag;
 // the end-of-block merge scratch reuses ring stage 0 (free once the last MMA completed)
 constexpr uint32_t kISmemBytes = 1024 + kIATile + kIStages * kIBTile + 8 * kINumBars + 16;
-static_assert(kISmemBytes + 16 <= 232448, "exceeds the 227 KB shared-memory opt-in");
+// dynamic tiles + the static s_last and per-row bounds (4 x kIBM 16-bit)
+static_assert(kISmemBytes + 16 + 4 * kIBM * 2 <= 232448, "exceeds the 227 KB shared-memory opt-in");
 static_assert(3 * kIBM * sizeof(uint2) <= kIBTile, "merge scratch must fit in one ring stage");
 constexpr uint32_t kITmemCols = 512;
 constexpr long long kIDeadlineCycles = 4000000000ll;  // ~2 s at 2 GHz
@@ -254,6 +255,10 @@ __global__ void __launch_bounds__(kIThreads, 1)
   uint32_t* s_tmem = reinterpret_cast<uint32_t*>(bars + kINumBars);
   volatile int* s_abort = reinterpret_cast<volatile int*>(s_tmem + 1);
   __shared__ unsigned int s_last;
+  // each column group's current second-best distance per query row (0xFFFF:
+  // none yet): two keys at or below it exist, so it bounds what the other
+  // column groups keep for that row (1 KB: the dynamic tiles leave 1.9 KB)
+  __shared__ uint16_t s_d2[4][kIBM];
 
   const int nq = min(a.d_nq ? *a.d_nq : a.nq, w.nq_cap);
   const int ndb = a.d_ndb ? *a.d_ndb : a.ndb;
@@ -279,6 +284,7 @@ __global__ void __launch_bounds__(kIThreads, 1)
 #define BAR_ACCFULL(s) (bar0 + 8u * (1 + 2 * kIStages + (s)))
 #define BAR_ACCEMPTY(s) (bar0 + 8u * (3 + 2 * kIStages + (s)))
 
+  for (int i = threadIdx.x; i < 4 * kIBM; i += blockDim.x) (&s_d2[0][0])[i] = 0xFFFFu;
   if (threadIdx.x == 0) {
     mbar_init(BAR_A, 1);
     for (int s = 0; s < kIStages; s++) {
@@ -411,14 +417,24 @@ __global__ void __launch_bounds__(kIThreads, 1)
         for (int j = 0; j < 64; j++)
           if (g0 + j >= ndb) v[j] = kMaskedDot;
       }
-      int thr = (k2 == kNoKeyShared) ? kMaskedDot : 256 - 2 * (int)(k2 >> kIdxBitsShared);
+      // the other column groups' second best for this row: a column can reach the
+      // row's final top two only at or below its distance (its index may be lower)
+      const int row = quarter * 32 + lane;
+      unsigned gbd = 0xFFFFu;
+#pragma unroll
+      for (int g = 0; g < 4; g++)
+        if (g != colgrp) gbd = min(gbd, (unsigned)reinterpret_cast<volatile uint16_t*>(&s_d2[g][0])[row]);
+      const int thr_gb = (gbd == 0xFFFFu) ? kMaskedDot : 256 - 2 * (int)gbd - 1;
+      auto next_thr = [&]() {
+        return max(thr_gb, (k2 == kNoKeyShared) ? kMaskedDot : 256 - 2 * (int)(k2 >> kIdxBitsShared));
+      };
+      int thr = next_thr();
 #pragma unroll
       for (int c = 0; c < 2; c++) {
         // columns arrive in increasing index order, so only a strictly larger dot
         // than the current second best can enter the top two
         const int* vc = v + 32 * c;
         const int gc = g0 + 32 * c;
-        auto next_thr = [&]() { return (k2 == kNoKeyShared) ? kMaskedDot : 256 - 2 * (int)(k2 >> kIdxBitsShared); };
         if (__any_sync(0xffffffffu, thr < 0)) {  // a lane has no second best yet: the whole chunk (warp-uniform)
           chunk_top2_push<0, 32>(vc, gc, k1, k2);
           thr = next_thr();
@@ -447,6 +463,7 @@ __global__ void __launch_bounds__(kIThreads, 1)
           thr = next_thr();
         }
       }
+      if (k2 != kNoKeyShared) reinterpret_cast<volatile uint16_t*>(&s_d2[colgrp][0])[row] = (uint16_t)(k2 >> kIdxBitsShared);
     }
     if (!ok) {
       *s_abort = 1;
