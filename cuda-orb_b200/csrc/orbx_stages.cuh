@@ -718,7 +718,7 @@ constexpr int kLookPerLane = 8;  // look-back words read per lane and round: 256
 // changes from an aggregate to an inclusive prefix of the same strip, and
 // summing aggregates back to any prefix gives the same total, so words already
 // seen published are kept and only the pending ones are read again, after a
-// back-off that doubles from 32 ns to 1 us: the words of a frame share a few
+// back-off that doubles from 32 ns to 256 ns: the words of a frame share a few
 // L2 sectors, and a store to them completes only after the reads queued there.
 // The wait is bounded by wait_cycles of clock64(); on expiry it sets
 // kErrLookbackTimeout and returns the prefix found so far.
@@ -772,7 +772,7 @@ __device__ __forceinline__ int nms_lookback(unsigned long long* st, int s, int l
         break;
       }
       __nanosleep(sleep_ns);
-      if (sleep_ns < 1024) sleep_ns <<= 1;
+      if (sleep_ns < 256) sleep_ns <<= 1;
 #pragma unroll
       for (int u = 0; u < kLookPerLane; u++) {
         const int idx = j - lane - 32 * u;
