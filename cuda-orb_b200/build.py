@@ -1,10 +1,13 @@
 """Build liborbx.so (the sm_100a ORB library) in place with nvcc.
 
-    python cuda-orb_b200/build.py [--force]
+    python cuda-orb_b200/build.py [--force] [--checked]
 
 Compiles every CUDA source under csrc/ for sm_100a only and links one shared
 library next to this file: the C ABI of include/orbx.h and the C++ API of
-include/orb.h / include/orbd.h.
+include/orb.h / include/orbd.h.  --checked builds the bounds-checked variant
+instead, liborbx_checked.so: the same sources with -DORBX_BOUNDS_CHECK, whose
+kernels test each global access against its buffer's extent and report the
+ones outside it (orbx_bounds_report) instead of making them.
 """
 import os
 import subprocess
@@ -13,6 +16,7 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "liborbx.so")
+LIB_CHECKED = os.path.join(HERE, "liborbx_checked.so")
 SOURCES = ["orbx_api.cu", "orbx_detect.cu", "orbx_describe.cu", "orbx_match.cu", "orbx_match_imma.cu",
            "orb_compat.cu", "orbx_static.cu", "orbx_gemm.cu", "orbx_learned.cu", "orbx_learned_api.cu",
            "orbx_hostio.cu", "orbx_ocv.cu", "orbx_persist.cu"]
@@ -28,23 +32,25 @@ def _inputs():
     return files
 
 
-def up_to_date():
-    if not os.path.exists(LIB):
+def up_to_date(lib=LIB):
+    if not os.path.exists(lib):
         return False
-    t = os.path.getmtime(LIB)
+    t = os.path.getmtime(lib)
     return all(os.path.getmtime(f) <= t for f in _inputs())
 
 
-def build(force=False, verbose=False):
-    if not force and up_to_date():
-        return LIB
-    objdir = os.path.join(HERE, "_build")
+def build(force=False, verbose=False, checked=False):
+    lib = LIB_CHECKED if checked else LIB
+    if not force and up_to_date(lib):
+        return lib
+    objdir = os.path.join(HERE, "_build_checked" if checked else "_build")
     os.makedirs(objdir, exist_ok=True)
     objs = []
     procs = []
+    flags = FLAGS + (["-DORBX_BOUNDS_CHECK"] if checked else [])
     for src in SOURCES:
         obj = os.path.join(objdir, src.replace(".cu", ".o"))
-        cmd = [NVCC] + FLAGS + ["-c", os.path.join(CSRC, src), "-o", obj]
+        cmd = [NVCC] + flags + ["-c", os.path.join(CSRC, src), "-o", obj]
         if verbose:
             print(" ".join(cmd))
         procs.append((src, subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.STDOUT)))
@@ -53,12 +59,12 @@ def build(force=False, verbose=False):
         out, _ = p.communicate()
         if p.returncode != 0:
             raise RuntimeError(f"nvcc failed on {src}:\n{out.decode(errors='replace')}")
-    tmp = LIB + ".tmp"
+    tmp = lib + ".tmp"
     cmd = [NVCC, "-gencode", "arch=compute_100a,code=sm_100a", "-shared", "-o", tmp] + objs
     subprocess.check_call(cmd)
-    os.replace(tmp, LIB)
-    return LIB
+    os.replace(tmp, lib)
+    return lib
 
 
 if __name__ == "__main__":
-    print(build(force="--force" in sys.argv, verbose=True))
+    print(build(force="--force" in sys.argv, verbose=True, checked="--checked" in sys.argv))

@@ -103,6 +103,8 @@ struct orbx_ctx {
   int8_t* d_pattern = nullptr;
   int* d_umax = nullptr;
   int* d_err = nullptr;
+  BoundsRec* d_bounds = nullptr;  // bounds-checked build only: record of skipped accesses
+  long long bounds_slack = 0;     // bytes taken off each image's checked extent (orbx_bounds_set_slack)
   Workspace ws[2];
   BatchSlot single, pair;
   MatchWork mw{};  // for orbx_match / orbx_match_knn2
@@ -161,6 +163,15 @@ struct orbx_ctx {
   long long wait_cycles = 0;
   int clock_khz = 2000000;
 };
+
+// The popcount matcher's record and row capacities (bounds-checked build; the
+// normal build leaves them null and zero, and its kernels test nothing).
+static void match_bounds(orbx_ctx* c, MatchArgs& a, int q_cap, int db_cap, int out_cap) {
+  a.bounds = c->d_bounds;
+  a.q_cap = q_cap;
+  a.db_cap = db_cap;
+  a.out_cap = out_cap;
+}
 
 #define ORBX_CUDA(x)                   \
   do {                                 \
@@ -374,6 +385,7 @@ static void fill_frame(const orbx_ctx* c, const Workspace& ws, const uint8_t* im
   F.w = ws.w;
   F.h = ws.h;
   F.pitch_in = pitch_in;
+  F.img_bytes = std::max(0LL, (long long)ws.h * pitch_in - c->bounds_slack);
   F.n_oct = n;
   for (int o = 0; o < n; o++) {
     F.ow[o] = ws.oszp[n + o];
@@ -467,6 +479,7 @@ static int upload_batch(orbx_ctx* c, BatchSlot& bs, const std::vector<Frame>& fr
   b.nms_base = bs.d_bases + 2 * (nf + 1);
   b.nms_ticket = bs.d_ticket;
   b.err = c->d_err;
+  b.bounds = c->d_bounds;
   b.wait_cycles = c->wait_cycles;
   b.pyr_shape = frames[0].pyr_shape;
   b.fast_thr = c->p.fast_threshold;
@@ -682,6 +695,14 @@ ORBX_API int orbx_create(orbx_ctx** out, int device) {
     delete c;
     return ORBX_ERR_CUDA;
   }
+#ifdef ORBX_BOUNDS_CHECK
+  if (cudaMalloc(&c->d_bounds, sizeof(BoundsRec)) != cudaSuccess ||
+      cudaMemset(c->d_bounds, 0, sizeof(BoundsRec)) != cudaSuccess) {
+    (void)cudaGetLastError();
+    delete c;
+    return ORBX_ERR_CUDA;
+  }
+#endif
   c->own_stream = true;
   int khz = 0;
   if (cudaDeviceGetAttribute(&khz, cudaDevAttrClockRate, device) != cudaSuccess || khz <= 0) {
@@ -754,6 +775,7 @@ ORBX_API int orbx_destroy(orbx_ctx* c) {
   cudaFree(c->d_pattern);
   cudaFree(c->d_umax);
   cudaFree(c->d_err);
+  cudaFree(c->d_bounds);
   if (c->own_stream) cudaStreamDestroy(c->stream);
   delete c;
   return ORBX_OK;
@@ -775,6 +797,37 @@ ORBX_API int orbx_set_stream(orbx_ctx* c, void* stream) {
 }
 
 ORBX_API void* orbx_get_stream(orbx_ctx* c) { return c ? (void*)c->stream : nullptr; }
+
+ORBX_API int orbx_bounds_checked(void) {
+#ifdef ORBX_BOUNDS_CHECK
+  return 1;
+#else
+  return 0;
+#endif
+}
+
+ORBX_API int orbx_bounds_report(orbx_ctx* c, long long* out) {
+  if (!c || !out) return ORBX_ERR_ARG;
+  if (!c->d_bounds) return ORBX_ERR_STATE;
+  DeviceGuard g(c->device);
+  ORBX_CUDA(cudaStreamSynchronize(c->stream));
+  if (c->copy_stream) ORBX_CUDA(cudaStreamSynchronize(c->copy_stream));
+  BoundsRec r{};
+  ORBX_CUDA(cudaMemcpy(&r, c->d_bounds, sizeof(r), cudaMemcpyDeviceToHost));
+  ORBX_CUDA(cudaMemset(c->d_bounds, 0, sizeof(r)));
+  out[0] = (long long)r.n;
+  out[1] = r.site;
+  out[2] = r.off;
+  out[3] = r.extent;
+  return ORBX_OK;
+}
+
+ORBX_API int orbx_bounds_set_slack(orbx_ctx* c, long long bytes) {
+  if (!c || bytes < 0) return ORBX_ERR_ARG;
+  if (!c->d_bounds) return ORBX_ERR_STATE;
+  c->bounds_slack = bytes;
+  return ORBX_OK;
+}
 
 ORBX_API int orbx_sync(orbx_ctx* c) {
   if (!c) return ORBX_ERR_ARG;
@@ -933,6 +986,7 @@ ORBX_API int orbx_match(orbx_ctx* c, orbx_point* d_points1, const int* d_n1, con
   a.d_nq = d_n1;
   a.d_ndb = d_n2;
   a.pts = d_points1;
+  match_bounds(c, a, n1_cap, n2_cap, n1_cap);
   return match_common(c, c->mw, a, n1_cap, n2_cap, mode);
 }
 
@@ -950,6 +1004,7 @@ ORBX_API int orbx_match_knn2(orbx_ctx* c, const uint8_t* d_q, int nq, const uint
   a.ndb = ndb;
   a.dist2 = d_dist2;
   a.idx2 = d_idx2;
+  match_bounds(c, a, nq, ndb, nq);
   return match_common(c, c->mw, a, nq, ndb, mode);
 }
 
@@ -1029,6 +1084,7 @@ ORBX_API int orbx_pair(orbx_ctx* c, const uint8_t* d_img_a, const uint8_t* d_img
   a.d_nq = d_n_a;
   a.d_ndb = d_n_b;
   a.pts = d_pts_a;
+  match_bounds(c, a, c->p.max_pts, c->p.max_pts, c->p.max_pts);
   if (c->pair_form == 1 && mode == ORBX_MATCH_POPC) return pair_persistent(c, pl, frames, a);
   // graph key: launch shapes and every pointer baked into the captured launches
   std::vector<uint8_t> key(sizeof(Batch) + sizeof(MatchArgs) + sizeof(LaunchPlan) + sizeof(int));
@@ -1138,6 +1194,7 @@ static int pair_host_overlap(orbx_ctx* c, const uint8_t* h_a, const uint8_t* h_b
   jobs[0].args.d_nq = c->io_count;
   jobs[0].args.d_ndb = c->io_count + 1;
   jobs[0].args.pts = c->io_pts[0];
+  match_bounds(c, jobs[0].args, c->p.max_pts, c->p.max_pts, c->p.max_pts);
   jobs[0].work = pg.mw;
   const int match_items = 2 * 148;
   PersistArgs a;
@@ -1238,6 +1295,7 @@ static int pair_host_streams(orbx_ctx* c, const uint8_t* h_a, const uint8_t* h_b
   m.d_nq = c->io_count;
   m.d_ndb = c->io_count + 1;
   m.pts = c->io_pts[0];
+  match_bounds(c, m, c->p.max_pts, c->p.max_pts, c->p.max_pts);
   ORBX_CUDA(launch_match_popc(m, c->hmw, c->stream, c->match_bps));
   return hostio_export_pair(c, c->io_pts[0], c->io_pts[1], c->io_desc[0], c->io_desc[1], c->io_count,
                             c->p.max_pts, with_desc, res);
@@ -1405,6 +1463,7 @@ ORBX_API int orbx_profile_pair(orbx_ctx* c, const uint8_t* d_img_a, const uint8_
   a.d_nq = d_n_a;
   a.d_ndb = d_n_b;
   a.pts = d_pts_a;
+  match_bounds(c, a, c->p.max_pts, c->p.max_pts, c->p.max_pts);
   ORBX_CUDA(cudaEventRecord(c->prof_ev[0], c->stream));
   ORBX_CUDA(launch_pyramid_blur(pl.b, pl.pyr_tiles, c->stream));
   ORBX_CUDA(cudaEventRecord(c->prof_ev[1], c->stream));
@@ -1709,6 +1768,7 @@ static int batch_pairs_impl(orbx_ctx* c, int n_pairs, const orbx_image* ia, cons
       J.args.d_nq = oa[i].num_pts;
       J.args.d_ndb = ob[i].num_pts;
       J.args.pts = oa[i].points;
+      match_bounds(c, J.args, oa[i].max_pts, ob[i].max_pts, oa[i].max_pts);
       J.work.part = c->batch_part + po;
       J.work.tile_done = c->batch_tile_done + to;
       J.work.nq_cap = oa[i].max_pts;

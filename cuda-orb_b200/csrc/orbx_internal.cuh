@@ -30,6 +30,40 @@ constexpr int kNmsRows = 4;
 constexpr int kNmsMaxRows = 16;
 constexpr int kNmsMaxWords = 2048;  // occupancy words per NMS strip (rows x words per row)
 
+// Bounds-checked build (the same sources compiled with -DORBX_BOUNDS_CHECK
+// into liborbx_checked.so).  Every global access of the pipeline's stage
+// bodies and of the popcount matcher is first tested against the extent of
+// the buffer it belongs to (a Span).  An access outside it is skipped, a load
+// giving zero, and counted in the launch's BoundsRec with the site, the byte
+// offset from the buffer's base and the extent of the first one.  Launches
+// without a record (bounds == nullptr) and the normal build test nothing:
+// there ORBX_IN is the constant true and the spans compile away.
+struct BoundsRec {
+  unsigned long long n;     // accesses skipped
+  long long site, off, extent;  // the first of them
+};
+struct Span {
+  const void* base;
+  long long bytes;
+};
+enum : int {
+  kSitePyrLoad = 1,  // pyramid staging: level-0 image or caller pyramid
+  kSitePyrPadLoad,   // pyramid: row padding copied from level 0
+  kSitePyrStore,     // pyramid: raw and blurred tile stores (within the octave)
+  kSiteFrameState,   // per-frame counters and NMS look-back words
+  kSiteDetLoad,      // detect: octave staging with halo (guarded pyramid)
+  kSiteDetStore,     // detect: occupancy, score and octave maps
+  kSiteNmsOcc,       // NMS: occupancy words
+  kSiteNmsScore,     // NMS: scores and octaves
+  kSiteNmsPts,       // NMS: keypoint stores
+  kSiteDescPts,      // describe: keypoint index (its loads, angle and descriptor stores)
+  kSiteDescMoment,   // describe: raw patch rows (guarded pyramid)
+  kSiteDescSample,   // describe: blurred sampling points (guarded pyramid)
+  kSiteMatchQ,       // popcount matcher: query rows
+  kSiteMatchDb,      // popcount matcher: train rows
+  kSiteMatchOut,     // matcher outputs (keypoint match fields, k = 2 lists)
+};
+
 // Per-frame state, in device memory (one entry per frame of a launch).
 struct Frame {
   const uint8_t* img;  // level-0 input, row pitch `pitch_in`
@@ -58,6 +92,7 @@ struct Frame {
   int nms_rows;      // level-0 rows per NMS strip (tunable, <= kNmsMaxRows)
   int nms_strips;
   unsigned long long* nms_status;  // look-back words, one per strip
+  long long img_bytes;  // extent of img as the bounds-checked build tests it (h * pitch_in)
 };
 
 // Per-launch view of a batch of frames.
@@ -69,6 +104,7 @@ struct Batch {
   const int* nms_base;   // [n_frames + 1] for k_nms
   unsigned int* nms_ticket;  // dynamic strip ticket (reset by k_pyramid_blur)
   int* err;              // sticky error word (bounded waits that gave up)
+  BoundsRec* bounds;     // bounds-checked build: record of skipped accesses (else null)
   long long wait_cycles; // bound of every device-side wait, in SM clock cycles
   int pyr_shape;         // pyramid tile shape of every frame of the launch
   int describe_mode;     // 0: angle + descriptor, 1: angle only, 2: descriptor only
@@ -118,6 +154,8 @@ struct MatchArgs {
   uint32_t* dist2;       // optional [nq][2]
   int32_t* idx2;         // optional [nq][2]
   orbx_point* pts;         // optional: reference-semantics match/distance (orbd.cu:1545-1557)
+  BoundsRec* bounds;       // bounds-checked build: record of skipped accesses (else null)
+  int q_cap, db_cap, out_cap;  // rows of q, db and of the outputs (checked with bounds)
 };
 struct MatchWork {          // scratch for split-train merging
   uint32_t* part;           // [splits_cap][nq_cap][2] partial top-2 keys
@@ -175,6 +213,39 @@ constexpr uint32_t kNoKeyShared = 0xFFFFFFFFu;
 constexpr int kMaxDistShared = 64;  // MAX_DIST, orbd.cu:26
 
 #ifdef __CUDACC__
+#ifdef ORBX_BOUNDS_CHECK
+// [off, off + len) within [0, extent), else recorded
+__device__ __forceinline__ bool in_range(BoundsRec* rec, int site, long long off, long long len, long long extent) {
+  if (!rec) return true;
+  if (off >= 0 && off + len <= extent) return true;
+  if (atomicAdd(&rec->n, 1ull) == 0ull) {
+    rec->site = site;
+    rec->off = off;
+    rec->extent = extent;
+  }
+  return false;
+}
+__device__ __forceinline__ bool in_span(BoundsRec* rec, int site, Span s, const void* p, int bytes) {
+  return in_range(rec, site, (long long)(reinterpret_cast<const char*>(p) - reinterpret_cast<const char*>(s.base)),
+                  bytes, s.bytes);
+}
+#define ORBX_IN(rec, site, span, p, bytes) ::orbx::in_span((rec), (site), (span), (p), (bytes))
+#define ORBX_IN_ROWS(rec, site, row, rows) ::orbx::in_range((rec), (site), (row), 1, (rows))
+#else
+#define ORBX_IN(rec, site, span, p, bytes) true
+#define ORBX_IN_ROWS(rec, site, row, rows) true
+#endif
+// Extents of a frame's buffers: the level-0 image (h rows of pitch_in bytes),
+// the pyramid with its guard zones, one octave of it, and the level-0 maps.
+__host__ __device__ __forceinline__ Span img_span(const Frame& F) { return {F.img, F.img_bytes}; }
+__host__ __device__ __forceinline__ Span guarded_span(const uint8_t* pyr, const Frame& F) {
+  return {pyr - kGuard, F.ooff[F.n_oct] + 2 * (long long)kGuard};
+}
+__host__ __device__ __forceinline__ Span octave_span(const uint8_t* pyr, const Frame& F, int o) {
+  return {pyr + F.ooff[o], F.ooff[o + 1] - F.ooff[o]};
+}
+__host__ __device__ __forceinline__ long long map_px(const Frame& F) { return (long long)F.h * F.op[0]; }
+
 __device__ __forceinline__ void top2_push_shared(uint32_t& k1, uint32_t& k2, uint32_t key) {
   k2 = min(k2, max(k1, key));
   k1 = min(k1, key);
@@ -188,6 +259,7 @@ __device__ __forceinline__ void finish_query_shared(const MatchArgs& a, int q, u
   const uint32_t d2 = (k2 == kNoKeyShared) ? kNoKeyShared : (k2 >> kIdxBitsShared);
   const int i1 = (k1 == kNoKeyShared) ? -1 : (int)(k1 & kIdxMaskShared);
   const int i2 = (k2 == kNoKeyShared) ? -1 : (int)(k2 & kIdxMaskShared);
+  if (!ORBX_IN_ROWS(a.bounds, orbx::kSiteMatchOut, q, a.out_cap)) return;
   if (a.dist2) {
     a.dist2[2 * q] = d1;
     a.dist2[2 * q + 1] = d2;

@@ -87,15 +87,20 @@ __device__ __forceinline__ float2 gauss_dot4x2(const float2* k, float2 t0, float
 // the octave edges).  words: the row is level 0 of a 4-byte aligned image, so
 // interior groups take two aligned words (cx is one past a multiple of 4).
 template <bool PL>
-__device__ __forceinline__ uint32_t pyr_stage_word(const uint8_t* rowp, int cx, int ow, int sh, bool words) {
+__device__ __forceinline__ uint32_t pyr_stage_word(const uint8_t* rowp, int cx, int ow, int sh, bool words,
+                                                   BoundsRec* rec, Span src) {
   if (words && cx >= 1 && cx + 3 < ow) {
     // bytes cx-1 .. cx+6 lie in [0, pitch_in): cx + 3 < ow <= pitch_in and both words are aligned
     const uint32_t* wp = reinterpret_cast<const uint32_t*>(rowp + (cx - 1));
+    if (!ORBX_IN(rec, kSitePyrLoad, src, wp, 8)) return 0u;
     return __byte_perm(ldx<PL>(wp), ldx<PL>(wp + 1), 0x4321);
   }
   uint32_t v[4];
 #pragma unroll
-  for (int j = 0; j < 4; j++) v[j] = ldx<PL>(rowp + (reflect101(cx + j, ow) << sh));
+  for (int j = 0; j < 4; j++) {
+    const uint8_t* p = rowp + (reflect101(cx + j, ow) << sh);
+    v[j] = ORBX_IN(rec, kSitePyrLoad, src, p, 1) ? ldx<PL>(p) : 0u;
+  }
   return pack_low_bytes(v[0], v[1], v[2], v[3]);
 }
 // Row-major walk over items (r, g) with W items per row: item threadIdx.x +
@@ -178,6 +183,7 @@ __device__ __forceinline__ void pyr_tile_load(const Batch& b, const PyrTile& g, 
   const uint8_t* __restrict__ psrc = F.pyr_src ? F.pyr_src + F.ooff[o] : nullptr;
   const bool words0 = (o == 0) && !psrc && ((reinterpret_cast<uintptr_t>(img) | (uintptr_t)pitch_in) & 3u) == 0;
   const int sh = psrc ? 0 : o;
+  const Span src = psrc ? Span{F.pyr_src, F.ooff[F.n_oct]} : img_span(F);
   RowWalk<kGroups, kPyrThreads> w;
 #pragma unroll
   for (int q = 0; q < pyr_stage_items<TW, TH>(); q++) {
@@ -186,8 +192,8 @@ __device__ __forceinline__ void pyr_tile_load(const Batch& b, const PyrTile& g, 
       const int y = reflect101(g.y0 - 3 + w.r, oh);
       const uint8_t* rowp = psrc ? psrc + (size_t)y * op : img + (size_t)(y << o) * pitch_in;
       const int cx = g.x0 - 3 + 4 * w.g;
-      wa[q] = pyr_stage_word<PL>(rowp, cx, ow, sh, words0);
-      wb[q] = pyr_stage_word<PL>(rowp, cx + kHW, ow, sh, words0);
+      wa[q] = pyr_stage_word<PL>(rowp, cx, ow, sh, words0, b.bounds, src);
+      wb[q] = pyr_stage_word<PL>(rowp, cx + kHW, ow, sh, words0, b.bounds, src);
     }
     w.next();
   }
@@ -207,7 +213,8 @@ __device__ __forceinline__ void pyr_tile_stage(const Batch& b, int t, const PyrT
   uint8_t* s_byte = sm.byte;
   const Frame& F = batch_frame<INL>(b, g.f);
   if (g.o == 0 && g.lt == 0) {
-    for (int i = threadIdx.x; i < F.nms_strips; i += blockDim.x) F.nms_status[i] = 0ull;
+    for (int i = threadIdx.x; i < F.nms_strips; i += blockDim.x)
+      if (ORBX_IN_ROWS(b.bounds, kSiteFrameState, i, F.nms_strips)) F.nms_status[i] = 0ull;
     if (threadIdx.x == 0) {
       *F.count = 0;
       if (F.total) *F.total = 0;
@@ -323,8 +330,10 @@ __device__ __forceinline__ void pyr_tile_filter(const Batch& b, const PyrTile& g
       const uint32_t pw = __byte_perm(sw[0], sw[1], 0x6543);
       const size_t a = (size_t)y * op + x;
       if (x + 4 <= ow) {
-        *reinterpret_cast<uint32_t*>(B + a) = bw;
-        *reinterpret_cast<uint32_t*>(P + a) = pw;
+        if (ORBX_IN(b.bounds, kSitePyrStore, octave_span(F.blr, F, o), B + a, 4))
+          *reinterpret_cast<uint32_t*>(B + a) = bw;
+        if (ORBX_IN(b.bounds, kSitePyrStore, octave_span(F.pyr, F, o), P + a, 4))
+          *reinterpret_cast<uint32_t*>(P + a) = pw;
       } else {
         // the group reaches into the row padding: octave 0 carries the caller's
         // padding bytes (the reference copies h * pitch0 bytes, orbd.cu:1584),
@@ -332,13 +341,21 @@ __device__ __forceinline__ void pyr_tile_filter(const Batch& b, const PyrTile& g
 #pragma unroll
         for (int j = 0; j < 4; j++) {
           if (x + j < ow) {
-            B[a + j] = (uint8_t)(bw >> (8 * j));
-            P[a + j] = (uint8_t)(pw >> (8 * j));
+            if (ORBX_IN(b.bounds, kSitePyrStore, octave_span(F.blr, F, o), B + a + j, 1))
+              B[a + j] = (uint8_t)(bw >> (8 * j));
+            if (ORBX_IN(b.bounds, kSitePyrStore, octave_span(F.pyr, F, o), P + a + j, 1))
+              P[a + j] = (uint8_t)(pw >> (8 * j));
           } else {
-            const uint8_t v = psrc ? ldx<PL>(psrc + a + j)
-                                   : (copy_pad ? ldx<PL>(img + (size_t)y * pitch_in + x + j) : (uint8_t)0);
-            B[a + j] = v;
-            P[a + j] = v;
+            const uint8_t v =
+                psrc ? (ORBX_IN(b.bounds, kSitePyrPadLoad, (Span{F.pyr_src, F.ooff[F.n_oct]}), psrc + a + j, 1)
+                            ? ldx<PL>(psrc + a + j)
+                            : (uint8_t)0)
+                     : (copy_pad ? (ORBX_IN(b.bounds, kSitePyrPadLoad, img_span(F), img + (size_t)y * pitch_in + x + j, 1)
+                                        ? ldx<PL>(img + (size_t)y * pitch_in + x + j)
+                                        : (uint8_t)0)
+                                 : (uint8_t)0);
+            if (ORBX_IN(b.bounds, kSitePyrStore, octave_span(F.blr, F, o), B + a + j, 1)) B[a + j] = v;
+            if (ORBX_IN(b.bounds, kSitePyrStore, octave_span(F.pyr, F, o), P + a + j, 1)) P[a + j] = v;
           }
         }
       }
@@ -484,7 +501,8 @@ struct DetSmem {
 // (64 >> O) + 8 bytes starting 4 rows above and 4 bytes left of the tile's
 // octave origin, in the pyramid's linear addressing.
 template <int O, bool P>
-__device__ __forceinline__ void stage_octave(const Frame& F, const uint8_t* pyr, int X0, int Y0, uint8_t* s_stage) {
+__device__ __forceinline__ void stage_octave(const Frame& F, const uint8_t* pyr, int X0, int Y0, uint8_t* s_stage,
+                                             BoundsRec* rec) {
   constexpr int sw4 = ((kDetTW >> O) + 2 * kHalo) / 4;
   constexpr int sh = (kDetTH >> O) + 2 * kHalo;
   const int op = F.op[O];
@@ -495,7 +513,8 @@ __device__ __forceinline__ void stage_octave(const Frame& F, const uint8_t* pyr,
 #pragma unroll 4
   for (int i = threadIdx.x; i < sh * sw4; i += 256) {
     const int r = i / sw4, w = i - r * sw4;
-    dst[i] = ldx<P>(src + r * op4 + w);
+    const uint32_t* sp = src + r * op4 + w;
+    dst[i] = ORBX_IN(rec, kSiteDetLoad, guarded_span(pyr, F), sp, 4) ? ldx<P>(sp) : 0u;
   }
 }
 
@@ -567,11 +586,11 @@ __device__ __forceinline__ void det_tile(const Batch& b, int t, DetSmem& sm) {
   // Stage every octave's tile with its halo, 4 bytes per load (octave offsets
   // and pitches are multiples of 128 and (X0 >> o) - 4 is a multiple of 4):
   // the words of each octave are spread over the whole block.
-  stage_octave<0, P>(F, pyr, X0, Y0, s_stage);
-  if (n_oct > 1) stage_octave<1, P>(F, pyr, X0, Y0, s_stage);
-  if (n_oct > 2) stage_octave<2, P>(F, pyr, X0, Y0, s_stage);
-  if (n_oct > 3) stage_octave<3, P>(F, pyr, X0, Y0, s_stage);
-  if (n_oct > 4) stage_octave<4, P>(F, pyr, X0, Y0, s_stage);
+  stage_octave<0, P>(F, pyr, X0, Y0, s_stage, b.bounds);
+  if (n_oct > 1) stage_octave<1, P>(F, pyr, X0, Y0, s_stage, b.bounds);
+  if (n_oct > 2) stage_octave<2, P>(F, pyr, X0, Y0, s_stage, b.bounds);
+  if (n_oct > 3) stage_octave<3, P>(F, pyr, X0, Y0, s_stage, b.bounds);
+  if (n_oct > 4) stage_octave<4, P>(F, pyr, X0, Y0, s_stage, b.bounds);
   __syncthreads();
 
   // 1. cardinal pre-test, four centres per word: the 512 words of octave 0 take
@@ -680,11 +699,12 @@ __device__ __forceinline__ void det_tile(const Batch& b, int t, DetSmem& sm) {
     if (Y < F.h) {
       uint32_t m = s_occ[threadIdx.x];
       const size_t a0 = (size_t)Y * F.op[0] + X0 + 32 * half;
-      F.occ[a0 >> 5] = m;
+      if (ORBX_IN_ROWS(b.bounds, kSiteDetStore, (long long)(a0 >> 5), map_px(F) >> 5)) F.occ[a0 >> 5] = m;
       while (m) {
         const int k = __ffs(m) - 1;
         m &= m - 1u;
         const unsigned long long key = s_key[r * kDetTW + 32 * half + k];
+        if (!ORBX_IN_ROWS(b.bounds, kSiteDetStore, (long long)(a0 + k), map_px(F))) continue;
         F.vmap[a0 + k] = __uint_as_float((uint32_t)(key >> 32));
         F.oct8[a0 + k] = (uint8_t)(7 - (int)(key & 0xFFu));
       }
@@ -911,8 +931,13 @@ __device__ __forceinline__ void nms_strip(const Batch& b, int ticket, NmsSmem& s
   const uint32_t gmask = ((1u << kNmsGroup) - 1u) << (lane & ~(kNmsGroup - 1));
   const uint32_t* occ_map = F.occ;
   const float* score_map = F.vmap;
-  auto g_occ = [=](long long wi) { return ldx<P>(occ_map + wi); };
-  auto g_score = [=](long long wi, uint32_t, int bb) { return ldx<P>(score_map + ((wi << 5) + bb)); };
+  [[maybe_unused]] BoundsRec* rec = b.bounds;
+  auto g_occ = [=](long long wi) {
+    return ORBX_IN_ROWS(rec, kSiteNmsOcc, wi, npx >> 5) ? ldx<P>(occ_map + wi) : 0u;
+  };
+  auto g_score = [=](long long wi, uint32_t, int bb) {
+    return ORBX_IN_ROWS(rec, kSiteNmsScore, (wi << 5) + bb, npx) ? ldx<P>(score_map + ((wi << 5) + bb)) : 0.f;
+  };
 
   for (int k = threadIdx.x; k < nwords; k += blockDim.x) s_sur[k] = 0u;
 
@@ -934,15 +959,15 @@ __device__ __forceinline__ void nms_strip(const Batch& b, int ticket, NmsSmem& s
   // for radii up to R; kept so that no index leaves the buffers)
   auto w_occ = [=](long long wi) {
     const long long sw = wi - W0;
-    return (sw >= 0 && sw < ns) ? s_occ[sw] : ldx<P>(occ_map + wi);
+    return (sw >= 0 && sw < ns) ? s_occ[sw] : g_occ(wi);
   };
   auto w_score = [=](long long wi, uint32_t word, int bb) {
     const long long sw = wi - W0;
     return (sw >= 0 && sw < ns) ? s_score[s_pfx[sw] + __popc(word & ((1u << bb) - 1u))]
-                                : ldx<P>(score_map + ((wi << 5) + bb));
+                                : g_score(wi, word, bb);
   };
   if (staged) {
-    for (int i = threadIdx.x; i < ns; i += blockDim.x) s_occ[i] = ldx<P>(F.occ + W0 + i);
+    for (int i = threadIdx.x; i < ns; i += blockDim.x) s_occ[i] = g_occ(W0 + i);
     __syncthreads();
     // set bits before each word (contiguous runs of words per thread), and the
     // list of set bits in raster order
@@ -978,8 +1003,9 @@ __device__ __forceinline__ void nms_strip(const Batch& b, int ticket, NmsSmem& s
         uint8_t o[4];
 #pragma unroll
         for (int q = 0; q < 4; q++) {
-          v[q] = ok[q] ? ldx<P>(F.vmap + li[q]) : 0.f;
-          o[q] = ok[q] ? ldx<P>(F.oct8 + li[q]) : (uint8_t)0;
+          const bool in = ok[q] && ORBX_IN_ROWS(rec, kSiteNmsScore, li[q], npx);
+          v[q] = in ? ldx<P>(F.vmap + li[q]) : 0.f;
+          o[q] = in ? ldx<P>(F.oct8 + li[q]) : (uint8_t)0;
         }
 #pragma unroll
         for (int q = 0; q < 4; q++) {
@@ -1036,7 +1062,7 @@ __device__ __forceinline__ void nms_strip(const Batch& b, int ticket, NmsSmem& s
         const int row = row0 + k / nw;
         const int wj = wlo + k % nw;
         const int cbase = wj << 5;
-        uint32_t m = ldx<P>(F.occ + (long long)row * wpr + wj);
+        uint32_t m = g_occ((long long)row * wpr + wj);
         if (cbase < xlo) m &= ~0u << (xlo - cbase);
         if (xhi - cbase < 32) m &= (xhi - cbase <= 0) ? 0u : ((xhi - cbase == 32) ? ~0u : ((1u << (xhi - cbase)) - 1u));
         if (m) {
@@ -1046,8 +1072,9 @@ __device__ __forceinline__ void nms_strip(const Batch& b, int ticket, NmsSmem& s
             m &= m - 1u;
             const long long idx = (long long)row * p0 + cbase + bit;
             s_cand[pos] = (uint16_t)(((k - c0) << 5) | bit);
-            s_cv[pos] = ldx<P>(F.vmap + idx);
-            s_co[pos] = ldx<P>(F.oct8 + idx);
+            const bool in = ORBX_IN_ROWS(rec, kSiteNmsScore, idx, npx);
+            s_cv[pos] = in ? ldx<P>(F.vmap + idx) : 0.f;
+            s_co[pos] = in ? ldx<P>(F.oct8 + idx) : (uint8_t)0;
             pos++;
           }
         }
@@ -1087,7 +1114,7 @@ __device__ __forceinline__ void nms_strip(const Batch& b, int ticket, NmsSmem& s
   }
 
   // decoupled look-back over the frame's strips (warp 0)
-  if (warp == 0) {
+  if (warp == 0 && ORBX_IN_ROWS(rec, kSiteFrameState, s, F.nms_strips)) {
     unsigned long long* st = F.nms_status;
     int excl = 0;
     if (s == 0) {
@@ -1133,13 +1160,14 @@ __device__ __forceinline__ void nms_strip(const Batch& b, int ticket, NmsSmem& s
         q.octave = s_oct[sr];
         q.score = s_score[sr];
       } else {
-        q.octave = F.oct8[idx];
-        q.score = F.vmap[idx];
+        const bool in = ORBX_IN_ROWS(rec, kSiteNmsScore, idx, npx);
+        q.octave = in ? F.oct8[idx] : 0;
+        q.score = in ? F.vmap[idx] : 0.f;
       }
       q.angle = 0.f;
       q.match = 0;
       q.distance = 0;
-      F.pts[rank] = q;
+      if (ORBX_IN_ROWS(rec, kSiteNmsPts, rank, F.max_pts)) F.pts[rank] = q;
       rank++;
     }
   }
@@ -1164,16 +1192,18 @@ constexpr int kDescWarps = 8;
 // (rint(x*c - y*s), rint(x*s + y*c)), evaluated by the reference build as
 // fma(x, c, -(y*s)) and fma(x, s, y*c).
 template <bool PL>
-__device__ __forceinline__ int sample_at(const uint8_t* center, int pitch, float x, float y, float s, float c) {
+__device__ __forceinline__ int sample_at(const uint8_t* center, int pitch, float x, float y, float s, float c,
+                                         BoundsRec* rec, Span blr) {
   const int ix = __float2int_rn(__fmaf_rn(x, c, -__fmul_rn(y, s)));
   const int iy = __float2int_rn(__fmaf_rn(x, s, __fmul_rn(y, c)));
-  return ldc<PL>(center + (ptrdiff_t)iy * pitch + ix);
+  const uint8_t* p = center + (ptrdiff_t)iy * pitch + ix;
+  return ORBX_IN(rec, kSiteDescSample, blr, p, 1) ? ldc<PL>(p) : 0;
 }
 
 template <int WTA, bool PL>
 __device__ __forceinline__ uint8_t describe_byte(const uint8_t* center, int pitch, const float* px, const float* py,
-                                                 float s, float c) {
-#define G(j) sample_at<PL>(center, pitch, px[j], py[j], s, c)
+                                                 float s, float c, BoundsRec* rec, Span blr) {
+#define G(j) sample_at<PL>(center, pitch, px[j], py[j], s, c, rec, blr)
   uint8_t val = 0;
   if (WTA == 2) {  // feature2 (orbd.cu:1351-1361)
 #pragma unroll
@@ -1250,6 +1280,7 @@ template <int WTA, bool PL>
 __device__ __forceinline__ void describe_keypoint(const Batch& b, const Frame& F, int k, const float* px,
                                                   const float* py, const int* s_umax, int lane) {
   const int half_k = b.half_k;
+  if (!ORBX_IN_ROWS(b.bounds, kSiteDescPts, k, F.max_pts)) return;
   orbx_point* P = F.pts + k;
   const int x = ldc<PL>(&P->x), y = ldc<PL>(&P->y), o = ldc<PL>(&P->octave);
   const int pitch = F.op[o];
@@ -1270,8 +1301,9 @@ __device__ __forceinline__ void describe_keypoint(const Batch& b, const Frame& F
       const uint32_t* wp = reinterpret_cast<const uint32_t*>(ra & ~(uintptr_t)3);
       const unsigned sh = 8u * (unsigned)(ra & 3);
       uint32_t w[9];
+      const bool in = ORBX_IN(b.bounds, kSiteDescMoment, guarded_span(F.pyr, F), wp, 36);
 #pragma unroll
-      for (int i = 0; i < 9; i++) w[i] = ldc<PL>(wp + i);
+      for (int i = 0; i < 9; i++) w[i] = in ? ldc<PL>(wp + i) : 0u;
       int sum = 0;
 #pragma unroll
       for (int i = 0; i < 8; i++) {
@@ -1303,7 +1335,7 @@ __device__ __forceinline__ void describe_keypoint(const Batch& b, const Frame& F
   // rBRIEF on the blurred octave
   const float sn = __sinf(angle);
   const float cs = __cosf(angle);
-  const uint8_t byte = describe_byte<WTA, PL>(F.blr + coff, pitch, px, py, sn, cs);
+  const uint8_t byte = describe_byte<WTA, PL>(F.blr + coff, pitch, px, py, sn, cs, b.bounds, guarded_span(F.blr, F));
   F.desc[(size_t)k * 32 + lane] = byte;
 }
 
@@ -1347,7 +1379,8 @@ __device__ __forceinline__ void match_popc_block(const MatchArgs& a, const Match
   uint32_t qw[8];
   {
     const uint4* qp = reinterpret_cast<const uint4*>(a.q) + 2 * (size_t)(active ? q : 0);
-    const uint4 v0 = ldx<P>(qp), v1 = ldx<P>(qp + 1);
+    const bool in = ORBX_IN_ROWS(a.bounds, kSiteMatchQ, active ? q : 0, a.q_cap);
+    const uint4 v0 = in ? ldx<P>(qp) : uint4{}, v1 = in ? ldx<P>(qp + 1) : uint4{};
     qw[0] = v0.x; qw[1] = v0.y; qw[2] = v0.z; qw[3] = v0.w;
     qw[4] = v1.x; qw[5] = v1.y; qw[6] = v1.z; qw[7] = v1.w;
   }
@@ -1359,7 +1392,9 @@ __device__ __forceinline__ void match_popc_block(const MatchArgs& a, const Match
   for (int r0 = r_beg; r0 < r_end; r0 += kMChunk) {
     const int rows = min(kMChunk, r_end - r0);
     __syncthreads();
-    for (int i = threadIdx.x; i < rows * 2; i += QPB) s_db[i] = ldx<P>(db4 + 2 * (size_t)r0 + i);
+    for (int i = threadIdx.x; i < rows * 2; i += QPB)
+      s_db[i] = ORBX_IN_ROWS(a.bounds, kSiteMatchDb, r0 + (i >> 1), a.db_cap) ? ldx<P>(db4 + 2 * (size_t)r0 + i)
+                                                                             : uint4{};
     __syncthreads();
     for (int j = 0; j < rows; j++) {
       const uint4 t0 = s_db[2 * j], t1 = s_db[2 * j + 1];

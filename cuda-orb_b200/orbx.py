@@ -13,7 +13,10 @@ import os
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "liborbx.so")
+# ORBX_CHECKED=1 loads the bounds-checked build (build.py --checked) instead:
+# same entry points, each kernel access tested against its buffer's extent.
+CHECKED = os.environ.get("ORBX_CHECKED", "0") == "1"
+LIB_PATH = os.path.join(HERE, "liborbx_checked.so" if CHECKED else "liborbx.so")
 
 ORBX_OK = 0
 ORBX_ERR_ARG, ORBX_ERR_CUDA, ORBX_ERR_SIZE, ORBX_ERR_STATE, ORBX_ERR_TIMEOUT, ORBX_ERR_NOMEM = 1, 2, 3, 4, 5, 6
@@ -68,7 +71,8 @@ def lib():
     global _lib
     if _lib is None:
         if not os.path.exists(LIB_PATH):
-            raise ImportError(f"liborbx.so not built: run `python {os.path.join(HERE, 'build.py')}`")
+            raise ImportError(f"{os.path.basename(LIB_PATH)} not built: run "
+                              f"`python {os.path.join(HERE, 'build.py')}{' --checked' if CHECKED else ''}`")
         L = ctypes.CDLL(LIB_PATH)
         vp, i32 = ctypes.c_void_p, ctypes.c_int
         L.orbx_version.restype = ctypes.c_char_p
@@ -103,6 +107,9 @@ def lib():
                                                 ctypes.POINTER(FrameOut), ctypes.POINTER(FrameOut), i32, i32,
                                                 ctypes.POINTER(Tuning), ctypes.POINTER(ctypes.c_float)]
         L.orbx_selftest_wait_timeout.argtypes = [vp, i32]
+        L.orbx_bounds_checked.argtypes = []
+        L.orbx_bounds_report.argtypes = [vp, ctypes.POINTER(ctypes.c_longlong)]
+        L.orbx_bounds_set_slack.argtypes = [vp, ctypes.c_longlong]
         L.orbx_profile_batch.argtypes = [vp, i32, ctypes.POINTER(Image), ctypes.POINTER(Image),
                                          ctypes.POINTER(FrameOut), ctypes.POINTER(FrameOut), vp]
         L.orbx_learned_default_params.argtypes = [ctypes.POINTER(LearnedParams)]
@@ -389,6 +396,17 @@ class Context:
     def selftest_wait_timeout(self, timeout_us):
         """Returns the status of a device wait on a counter nothing sets (ORBX_ERR_TIMEOUT expected)."""
         return int(lib().orbx_selftest_wait_timeout(self.h, int(timeout_us)))
+
+    def bounds_report(self):
+        """Bounds-checked build: (skipped accesses, site of the first, its offset,
+        its buffer's extent) since the last report; clears the record."""
+        out = (ctypes.c_longlong * 4)()
+        _check(lib().orbx_bounds_report(self.h, out), "orbx_bounds_report")
+        return tuple(int(v) for v in out)
+
+    def bounds_set_slack(self, nbytes):
+        """Bounds-checked build: later frames' image extents, as checked, end nbytes early."""
+        _check(lib().orbx_bounds_set_slack(self.h, int(nbytes)), "orbx_bounds_set_slack")
 
     def debug_buffers(self, w, h):
         n, oszp = layout(w, h, self.params.noctaves)

@@ -262,6 +262,35 @@ ORBX_API int orbx_set_tuning(orbx_ctx* ctx, const orbx_tuning* t);
  * stays usable.  For tests of the failure path. */
 ORBX_API int orbx_selftest_wait_timeout(orbx_ctx* ctx, int timeout_us);
 
+/* No counterpart in the reference (it has no checked build; its CHECK macros,
+ * cuda_utils.h:18-38, catch only failed API calls, and its kernels read past
+ * their buffers by design, orbd.cu:1001-1036 and 1437-1468).
+ * 1 in the bounds-checked build of this library (liborbx_checked.so: the same
+ * sources compiled with -DORBX_BOUNDS_CHECK), 0 in the normal build. */
+ORBX_API int orbx_bounds_checked(void);
+
+/* Bounds-checked build only.  There every global access of the pyramid,
+ * detect, NMS and describe stages (five-launch, persistent and batched forms)
+ * and of the popcount matcher is tested against the extent of its buffer
+ * (the h x pitch image, the pyramid with its guard zones, one octave for the
+ * pyramid's stores, the h x pitch0 maps, max_pts keypoints and descriptors,
+ * the match capacities).  An access outside it is skipped (a load reads zero)
+ * and counted.  This waits for the context's streams, then writes
+ * out[0] = accesses skipped since the last report, out[1] = the site of the
+ * first (kSite* in csrc/orbx_internal.cuh), out[2] = its byte (or row)
+ * offset from the buffer's base, out[3] = the buffer's extent, and clears
+ * the record.  The normal build returns ORBX_ERR_STATE. */
+ORBX_API int orbx_bounds_report(orbx_ctx* ctx, long long* out);
+
+/* Bounds-checked build only; no counterpart in the reference.  Frames set up
+ * by later calls on this context have their image's checked extent reduced by
+ * `bytes` (h x pitch - bytes), so the kernels' reads of the image's last bytes,
+ * which lie in memory the caller owns, are skipped and reported.  A test of
+ * the checker itself: it shows that a read outside a buffer's extent is caught
+ * without making any access outside an allocation.  0 restores the extent.
+ * The normal build returns ORBX_ERR_STATE. */
+ORBX_API int orbx_bounds_set_slack(orbx_ctx* ctx, long long bytes);
+
 /* Many frame pairs of any sizes and keypoint caps: every stage of every image
  * runs in shared launches (one per stage for the whole batch), then every pair
  * is matched A -> B in one launch; or, with tuning batch_form = 1, all of it

@@ -20,8 +20,8 @@ def declared_symbols():
     return sorted(set(re.findall(r"ORBX_API\s+[\w\s\*]+?\b(orbx_\w+)\s*\(", text)))
 
 
-def exported_symbols():
-    out = subprocess.check_output(["nm", "-D", "--defined-only", orbx.LIB_PATH]).decode()
+def exported_symbols(path=None):
+    out = subprocess.check_output(["nm", "-D", "--defined-only", path or orbx.LIB_PATH]).decode()
     return {line.split()[-1] for line in out.splitlines() if " T " in line}
 
 
@@ -36,6 +36,21 @@ def test_exports_every_declared_symbol():
     exp = exported_symbols()
     missing = [s for s in decl if s not in exp]
     assert not missing, missing
+
+
+def test_checked_build_exports_every_declared_symbol():
+    """The bounds-checked variant (build.py --checked) is a drop-in for the
+    normal library: same entry points, and it says which build it is."""
+    import ctypes
+
+    path = os.path.join(ROOT, "cuda-orb_b200", "liborbx_checked.so")
+    if not os.path.exists(path):
+        pytest.fail("liborbx_checked.so not built (python cuda-orb_b200/build.py --checked)")
+    exp = exported_symbols(path)
+    missing = [s for s in declared_symbols() if s not in exp]
+    assert not missing, missing
+    assert ctypes.CDLL(path).orbx_bounds_checked() == 1
+    assert orbx.lib().orbx_bounds_checked() == (1 if orbx.CHECKED else 0)
 
 
 def test_cxx_api_symbols_exported():
