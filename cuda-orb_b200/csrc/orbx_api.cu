@@ -146,6 +146,7 @@ struct orbx_ctx {
   PersistBufs pbatch;  // orbx_batch_pairs, persistent form
   PersistBufs ppair;   // orbx_pair_host with overlapped uploads
   PairGraph pho;       // its graph: persistent launch + export
+  PairGraph phs;       // orbx_pair_host on two streams from pinned images: copies, kernels, match, export
   cudaStream_t copy_stream = nullptr;
   cudaEvent_t ev_reset = nullptr;
   int upload_bands = 0;  // orbx_pair_host: 0 = copy then run; 1..16 = bands overlapped with the persistent launch
@@ -758,6 +759,7 @@ ORBX_API int orbx_destroy(orbx_ctx* c) {
   persist_free(c->pbatch);
   persist_free(c->ppair);
   if (c->pho.exec) cudaGraphExecDestroy(c->pho.exec);
+  if (c->phs.exec) cudaGraphExecDestroy(c->phs.exec);
   if (c->ppg.exec) cudaGraphExecDestroy(c->ppg.exec);
   cudaFree(c->pho.mw.part);
   cudaFree(c->pho.mw.tile_done);
@@ -877,7 +879,7 @@ ORBX_API int orbx_init(orbx_ctx* c, const orbx_params* p) {
   ORBX_CUDA(cudaMemcpy(c->d_umax, umax, sizeof(umax), cudaMemcpyHostToDevice));
   if (shape_change)
     for (auto& ws : c->ws) ws_free(ws);
-  for (PairGraph* g : {&c->pg, &c->ppg, &c->pho}) {
+  for (PairGraph* g : {&c->pg, &c->ppg, &c->pho, &c->phs}) {
     if (g->exec) {
       cudaGraphExecDestroy(g->exec);
       g->exec = nullptr;
@@ -1256,10 +1258,47 @@ static int pair_host_overlap(orbx_ctx* c, const uint8_t* h_a, const uint8_t* h_b
   return ORBX_OK;
 }
 
+static bool host_pinned(const void* p) {
+  cudaPointerAttributes at{};
+  if (cudaPointerGetAttributes(&at, p) != cudaSuccess) {
+    (void)cudaGetLastError();
+    return false;
+  }
+  return at.type == cudaMemoryTypeHost;
+}
+
+// The work of pair_host_streams from the fork on: the copies, both frames'
+// kernels on their streams, the join, matching and the export.  ev_uploaded
+// (profiling) is recorded after the copies; under capture as an external
+// event node, so that each replay records it.
+static int pair_host_streams_enqueue(orbx_ctx* c, const uint8_t* h_a, const uint8_t* h_b, size_t ibytes,
+                                     const LaunchPlan& pa, const LaunchPlan& pb, const MatchArgs& m, bool with_desc,
+                                     const uint8_t** res, cudaEvent_t ev_uploaded, bool capturing) {
+  int rc;
+  // fork: the copy stream starts after everything queued before this call
+  ORBX_CUDA(cudaEventRecord(c->ev_fork, c->stream));
+  ORBX_CUDA(cudaStreamWaitEvent(c->copy_stream, c->ev_fork, 0));
+  ORBX_CUDA(cudaMemcpyAsync(c->io_img[0], h_a, ibytes, cudaMemcpyHostToDevice, c->stream));
+  ORBX_CUDA(cudaMemcpyAsync(c->io_img[1], h_b, ibytes, cudaMemcpyHostToDevice, c->copy_stream));
+  if (ev_uploaded)
+    ORBX_CUDA(capturing ? cudaEventRecordWithFlags(ev_uploaded, c->copy_stream, cudaEventRecordExternal)
+                        : cudaEventRecord(ev_uploaded, c->copy_stream));
+  if ((rc = launch_frames(c, pa, true, c->stream)) != 0) return rc;
+  if ((rc = launch_frames(c, pb, true, c->copy_stream)) != 0) return rc;
+  ORBX_CUDA(cudaEventRecord(c->ev_join, c->copy_stream));
+  ORBX_CUDA(cudaStreamWaitEvent(c->stream, c->ev_join, 0));
+  ORBX_CUDA(launch_match_popc(m, c->hmw, c->stream, c->match_bps));
+  return hostio_export_pair(c, c->io_pts[0], c->io_pts[1], c->io_desc[0], c->io_desc[1], c->io_count,
+                            c->p.max_pts, with_desc, res);
+}
+
 // orbx_pair_host with the two frames on two streams: image A is copied and
 // processed on the context's stream while image B is copied, then processed,
 // on the copy stream; matching and the export follow on the context's stream
-// once both are done.  The same five kernels per frame as orbx_pair.
+// once both are done.  The same five kernels per frame as orbx_pair.  When
+// both images are in pinned memory the sequence is captured once into a CUDA
+// graph (keyed on the images' addresses and every launch parameter) and
+// replayed, which removes the gaps between ten separately issued launches.
 static int pair_host_streams(orbx_ctx* c, const uint8_t* h_a, const uint8_t* h_b, int w, int h, int pitch,
                              bool with_desc, const uint8_t** res, cudaEvent_t ev_uploaded = nullptr) {
   int rc;
@@ -1277,16 +1316,6 @@ static int pair_host_streams(orbx_ctx* c, const uint8_t* h_a, const uint8_t* h_b
   if ((rc = upload_batch(c, c->pair_b, fb, &pb)) != 0) return rc;
   if ((rc = mw_ensure(c->hmw, c->p.max_pts)) != 0) return rc;
   const size_t ibytes = (size_t)h * pitch;
-  // fork: the copy stream starts after everything queued before this call
-  ORBX_CUDA(cudaEventRecord(c->ev_fork, c->stream));
-  ORBX_CUDA(cudaStreamWaitEvent(c->copy_stream, c->ev_fork, 0));
-  ORBX_CUDA(cudaMemcpyAsync(c->io_img[0], h_a, ibytes, cudaMemcpyHostToDevice, c->stream));
-  ORBX_CUDA(cudaMemcpyAsync(c->io_img[1], h_b, ibytes, cudaMemcpyHostToDevice, c->copy_stream));
-  if (ev_uploaded) ORBX_CUDA(cudaEventRecord(ev_uploaded, c->copy_stream));
-  if ((rc = launch_frames(c, pa, true, c->stream)) != 0) return rc;
-  if ((rc = launch_frames(c, pb, true, c->copy_stream)) != 0) return rc;
-  ORBX_CUDA(cudaEventRecord(c->ev_join, c->copy_stream));
-  ORBX_CUDA(cudaStreamWaitEvent(c->stream, c->ev_join, 0));
   MatchArgs m{};
   m.q = c->io_desc[0];
   m.db = c->io_desc[1];
@@ -1296,9 +1325,52 @@ static int pair_host_streams(orbx_ctx* c, const uint8_t* h_a, const uint8_t* h_b
   m.d_ndb = c->io_count + 1;
   m.pts = c->io_pts[0];
   match_bounds(c, m, c->p.max_pts, c->p.max_pts, c->p.max_pts);
-  ORBX_CUDA(launch_match_popc(m, c->hmw, c->stream, c->match_bps));
-  return hostio_export_pair(c, c->io_pts[0], c->io_pts[1], c->io_desc[0], c->io_desc[1], c->io_count,
-                            c->p.max_pts, with_desc, res);
+  if (!host_pinned(h_a) || !host_pinned(h_b))
+    return pair_host_streams_enqueue(c, h_a, h_b, ibytes, pa, pb, m, with_desc, res, ev_uploaded, false);
+  const uint8_t* map_dev = nullptr;
+  if ((rc = hostio_map(c, c->p.max_pts, res, &map_dev)) != 0) return rc;
+  PairGraph& g = c->phs;
+  const void* ptrs[5] = {h_a, h_b, map_dev, c->hmw.part, ev_uploaded};
+  const long long extra[4] = {(long long)ibytes, with_desc ? 1 : 0, c->match_bps, c->describe_bps};
+  std::vector<uint8_t> key(2 * sizeof(Batch) + 6 * sizeof(int) + sizeof(MatchArgs) + sizeof(ptrs) + sizeof(extra));
+  {
+    uint8_t* k = key.data();
+    const int shapes[6] = {pa.pyr_tiles, pa.det_tiles, pa.nms_strips, pb.pyr_tiles, pb.det_tiles, pb.nms_strips};
+    std::memcpy(k, &pa.b, sizeof(Batch));
+    k += sizeof(Batch);
+    std::memcpy(k, &pb.b, sizeof(Batch));
+    k += sizeof(Batch);
+    std::memcpy(k, shapes, sizeof(shapes));
+    k += sizeof(shapes);
+    std::memcpy(k, &m, sizeof(MatchArgs));
+    k += sizeof(MatchArgs);
+    std::memcpy(k, ptrs, sizeof(ptrs));
+    k += sizeof(ptrs);
+    std::memcpy(k, extra, sizeof(extra));
+  }
+  if (!(g.valid && g.key == key)) {
+    if (g.exec) {
+      cudaGraphExecDestroy(g.exec);
+      g.exec = nullptr;
+    }
+    g.valid = false;
+    cudaGraph_t graph = nullptr;
+    ORBX_CUDA(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+    const int lrc = pair_host_streams_enqueue(c, h_a, h_b, ibytes, pa, pb, m, with_desc, res, ev_uploaded, true);
+    const cudaError_t ce = cudaStreamEndCapture(c->stream, &graph);
+    if (lrc != ORBX_OK || ce != cudaSuccess) {
+      if (graph) cudaGraphDestroy(graph);
+      (void)cudaGetLastError();
+      return lrc != ORBX_OK ? lrc : ORBX_ERR_CUDA;
+    }
+    const cudaError_t ie = cudaGraphInstantiate(&g.exec, graph, 0);
+    cudaGraphDestroy(graph);
+    ORBX_CUDA(ie);
+    g.key.swap(key);
+    g.valid = true;
+  }
+  ORBX_CUDA(cudaGraphLaunch(g.exec, c->stream));
+  return ORBX_OK;
 }
 
 // orbx_pair_host; with `prof`, CUDA events and host clocks between the phases.
@@ -1529,7 +1601,7 @@ ORBX_API int orbx_set_tuning(orbx_ctx* c, const orbx_tuning* t) {
   }
   c->batch_key.clear();
   // cached graphs baked in the old shapes
-  for (PairGraph* g : {&c->pg, &c->ppg, &c->pho}) {
+  for (PairGraph* g : {&c->pg, &c->ppg, &c->pho, &c->phs}) {
     if (g->exec) {
       cudaGraphExecDestroy(g->exec);
       g->exec = nullptr;

@@ -156,6 +156,7 @@ struct MatchArgs {
   orbx_point* pts;         // optional: reference-semantics match/distance (orbd.cu:1545-1557)
   BoundsRec* bounds;       // bounds-checked build: record of skipped accesses (else null)
   int q_cap, db_cap, out_cap;  // rows of q, db and of the outputs (checked with bounds)
+  int unused_;                 // no tail padding: whole-struct bytes key the CUDA graphs
 };
 struct MatchWork {          // scratch for split-train merging
   uint32_t* part;           // [splits_cap][nq_cap][2] partial top-2 keys

@@ -175,3 +175,43 @@ def test_profile_pair_host_phases(bands, streams):
         assert ph["host_wall"] >= ph["export_end"] * 0.9
         assert min(ph[k] for k in ("host_enqueue", "host_wait", "host_copy_out")) >= 0
     ctx.close()
+
+
+def test_pair_host_graph_follows_contents_and_addresses():
+    """orbx_pair_host on two streams replays one captured CUDA graph while the
+    pinned images keep their addresses.  New contents at the same addresses
+    must be read by the replay, and new addresses must give a new graph: each
+    call equals orbx_pair on the same images."""
+    w, h = 1280, 720
+    imgs = [synth.make_pair(w, h, seed=s)[:2] for s in (60, 61, 62)]
+    pitch = imgs[0][0].shape[1]
+    ref = orbx.Context(0, orbx.make_params(max_pts=10000))
+    want = []
+    for a, b in imgs:
+        A, B = orbx.FrameBuffers(10000), orbx.FrameBuffers(10000)
+        ref.pair_ptr(torch.from_numpy(a).cuda(), torch.from_numpy(b).cuda(), w, h, pitch, A.points, A.desc, A.count,
+                     B.points, B.desc, B.count)
+        ref.sync()
+        want.append(A.to_host() + B.to_host())
+    ref.close()
+    ctx = orbx.Context(0, orbx.make_params(max_pts=10000))
+    t = ctx.get_tuning()
+    t.upload_bands = 0
+    t.host_overlap = 1
+    ctx.set_tuning(t)
+    buf1 = [torch.empty((h, pitch), dtype=torch.uint8).pin_memory() for _ in range(2)]
+    buf2 = [torch.empty((h, pitch), dtype=torch.uint8).pin_memory() for _ in range(2)]
+    # (image set, buffers): replay, new contents at the same addresses, new addresses, back
+    for k, bufs in ((0, buf1), (0, buf1), (1, buf1), (2, buf2), (1, buf1)):
+        for dst, src in zip(bufs, imgs[k]):
+            dst.copy_(torch.from_numpy(src))
+        hpa, hpb = np.full((10000, 7), -7, np.int32), np.full((10000, 7), -7, np.int32)
+        hna, hnb = np.zeros(1, np.int32), np.zeros(1, np.int32)
+        hda, hdb = np.zeros((10000, 32), np.uint8), np.zeros((10000, 32), np.uint8)
+        ctx.pair_host(bufs[0].data_ptr(), bufs[1].data_ptr(), w, h, pitch, hpa, hna, hpb, hnb, hda, hdb)
+        pa, da, pb, db = want[k]
+        assert int(hna[0]) == len(pa) and int(hnb[0]) == len(pb), k
+        assert np.array_equal(hpa[:len(pa)].view(PT).reshape(-1), pa), k
+        assert np.array_equal(hpb[:len(pb)].view(PT).reshape(-1), pb), k
+        assert np.array_equal(hda[:len(pa)], da) and np.array_equal(hdb[:len(pb)], db), k
+    ctx.close()
