@@ -47,12 +47,12 @@ SMS = 148
 # on the same 1080p pair, the committed summary of the pair's kernels): the
 # instruction roofline beside the HBM one, since these kernels are issue- and
 # latency-bound.
-NCU_WARP_INST = {"pyramid_blur": 8642876, "detect": 12141439, "nms": 3966314, "describe": 2382793,
+NCU_WARP_INST = {"pyramid_blur": 9490774, "detect": 11897417, "nms": 3936395, "describe": 2286742,
                  "match": 2037180}
 ISSUE_PER_CLK_PER_SM = 4  # warp instructions issued per clock per SM (one per scheduler)
 
-NCU_TRAFFIC = {"k_pyramid_blur": 4159744, "k_detect": 5656832, "k_nms": 1499392, "k_describe<2>": 5611008,
-               "k_match_popc": 97792, "k_match_imma": 33602560}
+NCU_TRAFFIC = {"k_pyramid_blur": 4167936, "k_detect": 5665664, "k_nms": 1542912, "k_describe<2>": 5689472,
+               "k_match_popc": 101760, "k_match_imma": 33602560}
 
 
 def parse_args(argv=None):
