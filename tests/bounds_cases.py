@@ -90,19 +90,37 @@ def run(orbx, synth, torch):
             out[key + ".pb"], out[key + ".db"] = pb.view(np.int32).reshape(-1, 7), db
         _report(ctx, out, f"batch{form}")
         ctx.close()
-    # host buffers in and out (overlapped upload, one persistent launch)
+    # host buffers in and out: two streams (pageable images, then pinned ones
+    # replayed from a graph) and banded uploads into one persistent launch
     w, h = 1280, 720
     a, b, _ = synth.make_pair(w, h, seed=900)
+    pinned = [torch.from_numpy(np.ascontiguousarray(x)).pin_memory() for x in (a, b)]
+    for name, bands, src in (("host", 0, (np.ascontiguousarray(a), np.ascontiguousarray(b))),
+                             ("hostpinned", 0, tuple(t.data_ptr() for t in pinned)),
+                             ("hostbands", 4, tuple(t.data_ptr() for t in pinned))):
+        ctx = orbx.Context(0, orbx.make_params(max_pts=10000))
+        t = ctx.get_tuning()
+        t.upload_bands = bands
+        ctx.set_tuning(t)
+        hpa = np.zeros((10000, 7), np.int32)
+        hpb = np.zeros((10000, 7), np.int32)
+        hna, hnb = np.zeros(1, np.int32), np.zeros(1, np.int32)
+        hda, hdb = np.zeros((10000, 32), np.uint8), np.zeros((10000, 32), np.uint8)
+        for _ in range(2):
+            ctx.pair_host(src[0], src[1], w, h, a.shape[1], hpa, hna, hpb, hnb, hda, hdb)
+        na, nb = int(hna[0]), int(hnb[0])
+        out[name + ".pa"], out[name + ".da"] = hpa[:na].copy(), hda[:na].copy()
+        out[name + ".pb"], out[name + ".db"] = hpb[:nb].copy(), hdb[:nb].copy()
+        _report(ctx, out, name)
+        ctx.close()
+    # one frame (orbx_detect_and_compute) at an odd width and unaligned pitch
     ctx = orbx.Context(0, orbx.make_params(max_pts=10000))
-    hpa = np.zeros((10000, 7), np.int32)
-    hpb = np.zeros((10000, 7), np.int32)
-    hna, hnb = np.zeros(1, np.int32), np.zeros(1, np.int32)
-    hda, hdb = np.zeros((10000, 32), np.uint8), np.zeros((10000, 32), np.uint8)
-    ctx.pair_host(np.ascontiguousarray(a), np.ascontiguousarray(b), w, h, a.shape[1], hpa, hna, hpb, hnb, hda, hdb)
-    na, nb = int(hna[0]), int(hnb[0])
-    out["host.pa"], out["host.da"] = hpa[:na].copy(), hda[:na].copy()
-    out["host.pb"], out["host.db"] = hpb[:nb].copy(), hdb[:nb].copy()
-    _report(ctx, out, "host")
+    img = _padded(a, 1277, 1277)
+    bufs = orbx.detect_and_compute(ctx, torch.from_numpy(img).cuda(), 1277, h)
+    ctx.sync()
+    p1, d1 = bufs.to_host()
+    out["single.p"], out["single.d"] = p1.view(np.int32).reshape(-1, 7), d1
+    _report(ctx, out, "single")
     # k = 2 lists, popcount form, ragged sizes
     rng = np.random.default_rng(901)
     q = torch.from_numpy(rng.integers(0, 256, (1000, 32), dtype=np.uint8)).cuda()

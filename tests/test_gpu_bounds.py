@@ -52,14 +52,14 @@ def test_normal_build_has_no_record():
 
 def test_checked_build_reports_nothing(checked_run):
     recs = {k: v for k, v in checked_run.items() if k.endswith(".bounds") and not k.startswith("slack")}
-    assert len(recs) >= 14
+    assert len(recs) >= 17
     bad = {k: v.tolist() for k, v in recs.items() if v[0] != 0}
     assert not bad, bad
 
 
 def test_checked_build_equals_normal_build(checked_run):
     want = bounds_cases.run(orbx, synth, torch)
-    assert len(want) >= 60
+    assert len(want) >= 70
     for k, v in want.items():
         assert k in checked_run, k
         assert checked_run[k].shape == v.shape and np.array_equal(checked_run[k], v), k
