@@ -47,12 +47,12 @@ SMS = 148
 # on the same 1080p pair, the committed summary of the pair's kernels): the
 # instruction roofline beside the HBM one, since these kernels are issue- and
 # latency-bound.
-NCU_WARP_INST = {"pyramid_blur": 9490774, "detect": 11897417, "nms": 3936395, "describe": 2286742,
+NCU_WARP_INST = {"pyramid_blur": 9089420, "detect": 11898158, "nms": 3933009, "describe": 2286742,
                  "match": 2037180}
 ISSUE_PER_CLK_PER_SM = 4  # warp instructions issued per clock per SM (one per scheduler)
 
-NCU_TRAFFIC = {"k_pyramid_blur": 4167936, "k_detect": 5665664, "k_nms": 1542912, "k_describe<2>": 5689472,
-               "k_match_popc": 101760, "k_match_imma": 33602560}
+NCU_TRAFFIC = {"k_pyramid_blur": 4167808, "k_detect": 5666176, "k_nms": 1543552, "k_describe<2>": 5689856,
+               "k_match_popc": 99584, "k_match_imma": 33602560}
 
 
 def parse_args(argv=None):
@@ -72,7 +72,7 @@ def parse_args(argv=None):
                    help="pair1080: the 1920x1080 pair (default); match65536: k=2 matching only; "
                         "batch64: 64 pairs of mixed resolution and caps in one batch; "
                         "learned: learned-proposal k=2 search, 131072 queries x 1048576 database rows")
-    p.add_argument("--learned-spill", type=int, default=12,
+    p.add_argument("--learned-spill", type=int, default=8,
                    help="learned: clusters each database row is listed in (1..16)")
     p.add_argument("--learned-epochs", type=int, default=3, help="learned: training epochs")
     p.add_argument("--learned-labels", choices=["nearest", "listed"], default="listed",
@@ -1118,9 +1118,21 @@ def run_learned_workload(args, world, rank, local, with_cpu=True):
             e2e()
         e2e_ms = timed(e2e, steps)
         index.close()
-        # without training: the same clustering probed by nearest centroids
+        # without training: the same clustering probed by nearest centroids, alone
+        # and with the fallback rule calibrated for it the same way, timed alike
         cen = orbx.LearnedIndex(ctx, db, train, orbx.learned_params(epochs=0, spill=args.learned_spill))
         recall_centroid = float(np.mean(no_fallback(cen, q)[0] == ex_d1))
+        ccd, ccm = no_fallback(cen, cal)
+        c_tm, c_td, c_cal_fb = calibrate_fallback(ccm, ccd, ccd == cal_d1, LEARNED_CAL_TARGET)
+        cen.set_margin(c_tm)
+        cen.set_max_distance(c_td)
+        c_fbc = torch.zeros(1, dtype=torch.int32, device=dev)
+        for _ in range(warm):
+            cen.search_ptr(q, nq, dist, idx, None, c_fbc)
+        cen_ms = timed(lambda: cen.search_ptr(q, nq, dist, idx, None, c_fbc), steps)
+        untrained = {"recall_at_1": float(np.mean(dist[:, 0].cpu().numpy() == ex_d1)),
+                     "fallback_fraction": int(c_fbc.item()) / nq, "calibration_fallback_fraction": c_cal_fb,
+                     "ms": sum(cen_ms) / len(cen_ms)}
         cen.close()
         # the other training target, same data and schedule
         other = orbx.LABEL_NEAREST if label_mode == orbx.LABEL_LISTED else orbx.LABEL_LISTED
@@ -1190,6 +1202,7 @@ def run_learned_workload(args, world, rank, local, with_cpu=True):
                          "labels": args.learned_labels, "epochs": args.learned_epochs,
                          "recall_mlp_other_labels_no_fallback": recall_other_labels,
                          "recall_nearest_centroid_no_fallback": recall_centroid,
+                         "nearest_centroid_calibrated": dict(untrained, speedup_vs_exact=t_exact / untrained["ms"]),
                          "recall_lsh_no_fallback": recall_lsh,
                          "lsh_ms": statistics.median(lsh_ms), "lsh": "12 random-projection bits, 8 probes"},
             "phases_ms": phases, "proposal_tflops": proposal_tflops, "roofline": roof,

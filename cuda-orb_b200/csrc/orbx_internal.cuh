@@ -17,9 +17,10 @@ constexpr size_t kGuard = 256 * 1024; // zeroed bytes before/after each pyramid
 // kPyrShapeTW/TH (tuning pyr_tile), one instantiation each
 constexpr int kPyrThreads = 256;  // threads of every block that runs pyramid tiles
 constexpr int kPyrShapes = 4;
-// 128 x 28 keeps a tile's shared memory under the 44.6 KB of five blocks per SM
+// 128 x 30 keeps a tile's shared memory (44.1 KB) under the 44.6 KB of five
+// blocks per SM, and a 1080p pair's 1,460 tiles within two waves of them
 constexpr int kPyrShapeTW[kPyrShapes] = {128, 64, 128, 64};
-constexpr int kPyrShapeTH[kPyrShapes] = {28, 32, 16, 64};
+constexpr int kPyrShapeTH[kPyrShapes] = {30, 32, 16, 64};
 constexpr int kPyrTW = kPyrShapeTW[0];
 constexpr int kPyrTH = kPyrShapeTH[0];
 // Detect tile (level-0 pixels); 32 keeps octave 4/5 tiles whole

@@ -242,8 +242,8 @@ typedef struct orbx_tuning {
                                  already processes the bands that have arrived (popcount matching) */
   int pair_form;              /* orbx_pair: 0 = five graph-replayed launches, 1 = one persistent launch
                                  (popcount matching) */
-  int pyr_tile;               /* pyramid + blur tile of the five-launch forms: 0 = 128 x 28, 1 = 64 x 32,
-                                 2 = 128 x 16, 3 = 64 x 64 octave pixels (the persistent forms use 128 x 28) */
+  int pyr_tile;               /* pyramid + blur tile of the five-launch forms: 0 = 128 x 30, 1 = 64 x 32,
+                                 2 = 128 x 16, 3 = 64 x 64 octave pixels (the persistent forms use 128 x 30) */
   int persist_row_deps;       /* persistent launches: 1 = a detect tile row waits only for the pyramid tile rows
                                  it reads (a frame's stages overlap row by row), 0 = for the whole frame */
   int host_overlap;           /* orbx_pair_host with upload_bands = 0: 1 (default) = image B is copied while
